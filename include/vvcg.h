@@ -1,0 +1,201 @@
+/*
+ * vvcg.h - C ABI of the B200 (sm_100a) VVC reconstruction, in-loop filter and
+ * candidate-cost library (libvvcg.so).
+ *
+ * The library replaces the sample-domain half of rustmpeg-video's VVC
+ * decoder and encoder (crates/rustmpeg-video/src/vvc/). The CPU keeps CABAC
+ * parsing and syntax; after a picture has been parsed, its coding-unit
+ * records and transform levels cross this boundary and the GPU performs
+ * dequantisation, the inverse transform, intra prediction (a CTU wavefront),
+ * reconstruction, deblocking, SAO and ALF. Motion-compensation interpolation
+ * and encoder candidate-cost evaluation are exposed as batched kernels.
+ *
+ * Conventions
+ *  - Plain C types only; all sizes in samples unless stated otherwise.
+ *  - Functions named *_dev take device pointers and run asynchronously on the
+ *    context's stream; all others take host pointers and return once their
+ *    results are in host memory.
+ *  - Every function returns a vvcg_status. A failed call leaves caller output
+ *    buffers untouched; vvcg_last_error() gives a one-line reason.
+ *  - A context is bound to one CUDA device and one stream. It is not
+ *    re-entrant: one thread at a time may use it. Separate contexts are
+ *    independent.
+ *  - There is no CPU fallback inside the library: without a usable CUDA
+ *    device every call returns VVCG_UNAVAILABLE.
+ *  - Results are bit-identical to the reference CPU code for every input
+ *    the reference accepts.
+ */
+#ifndef VVCG_H
+#define VVCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VVCG_ABI_VERSION 1
+
+/* Status codes. They map one-to-one onto the reference's AcceleratorError
+ * (crates/rustmpeg-video/src/accelerator.rs:17-31): UNAVAILABLE ->
+ * Unavailable, INVALID_INPUT -> InvalidInput, LIMIT_EXCEEDED ->
+ * LimitExceeded, EXECUTION / TIMEOUT / MISMATCH -> Execution. */
+typedef enum vvcg_status {
+  VVCG_OK = 0,
+  VVCG_INVALID_INPUT = 1,
+  VVCG_LIMIT_EXCEEDED = 2,
+  VVCG_UNAVAILABLE = 3,
+  VVCG_EXECUTION = 4,
+  VVCG_TIMEOUT = 5,  /* a bounded device-side wait gave up */
+  VVCG_MISMATCH = 6  /* a device self-check disagreed */
+} vvcg_status;
+
+typedef struct vvcg_ctx vvcg_ctx;
+
+typedef struct vvcg_config {
+  int32_t device;              /* CUDA device ordinal */
+  uint32_t flags;              /* reserved, 0 */
+  uint64_t reserve_bytes;      /* device arena to reserve up front (0 = grow on demand) */
+  uint32_t spin_limit;         /* wavefront wait limit in polls (0 = library default) */
+  uint32_t reserved;
+} vvcg_config;
+
+/* Chroma format (ChromaFormatIdc, crates/rustmpeg-video/src/vvc/predict.rs:2806). */
+enum { VVCG_CHROMA_400 = 0, VVCG_CHROMA_420 = 1, VVCG_CHROMA_422 = 2, VVCG_CHROMA_444 = 3 };
+
+/* Picture tool switches that change reconstruction (SliceCodingOptions,
+ * crates/rustmpeg-video/src/vvc/slice.rs:1472-1510). */
+enum {
+  VVCG_TOOL_DEP_QUANT = 1u << 0, /* dependent quantisation (dep_quant) */
+  VVCG_TOOL_DEBLOCK = 1u << 1,   /* enable_deblock */
+  VVCG_TOOL_SAO = 1u << 2,       /* enable_sao */
+  VVCG_TOOL_ALF = 1u << 3        /* enable_alf */
+};
+
+/* One picture of the 8..12-bit frame path: the inputs of
+ * slice::decode_vvc_frame_picture_with_chroma_qp (slice.rs:4659) once CABAC
+ * has been parsed. The coding units form a uniform grid of tb x tb luma
+ * blocks, tb = min(CTU size, 32) (slice.rs:4675), coded CTU by CTU in raster
+ * order with quadtree z-order inside a CTU (slice.rs:164-187). */
+typedef struct vvcg_pic_desc {
+  uint32_t width;            /* coded width, a multiple of the CTU size */
+  uint32_t height;           /* coded height, a multiple of the CTU size */
+  uint32_t visible_width;    /* cropped output width (<= width) */
+  uint32_t visible_height;   /* cropped output height (<= height) */
+  uint8_t bit_depth;         /* 8..12 */
+  uint8_t chroma_format;     /* VVCG_CHROMA_* */
+  uint8_t ctu_log2;          /* 5..7 */
+  uint8_t slice_qp;          /* SliceQpY, 0..63 */
+  uint8_t chroma_qp_scaled;  /* Qp'C including QpBdOffset (slice.rs:4662) */
+  uint8_t tools;             /* VVCG_TOOL_* */
+  int16_t alf_aps;           /* index into vvcg_batch.aps, -1 = fixed filters */
+  uint32_t cu_offset;        /* first record of this picture in vvcg_batch.cus */
+  uint32_t ctu_offset;       /* first record of this picture in vvcg_batch.ctus */
+} vvcg_pic_desc;
+
+/* One coding unit. Records of a picture are stored in raster order of its
+ * tb grid (index gy * (width / tb) + gx), not in coding order. */
+typedef struct vvcg_cu_rec {
+  uint8_t luma_mode;    /* IntraPredModeY, 0..66 */
+  uint8_t chroma_mode;  /* 0..66, or 81 / 82 / 83 for CCLM LM / LM-L / LM-T */
+  uint8_t cbf;          /* bit0 Y, bit1 Cb, bit2 Cr */
+  uint8_t reserved;
+  int32_t level_off[3]; /* start of each TB's raster-order levels in the level
+                           pool (int16), -1 when the TB has no levels */
+} vvcg_cu_rec;
+
+/* SAO parameters of one colour component of one CTU (filter.rs:1229 SaoType). */
+typedef struct vvcg_sao {
+  uint8_t type;          /* 0 off, 1 band offset, 2 edge offset */
+  uint8_t band_or_class; /* band position 0..31, or edge class 0..3 */
+  int8_t offsets[4];
+} vvcg_sao;
+
+/* Per-CTU filter switches, in raster CTU order per picture. */
+typedef struct vvcg_ctu_filter {
+  vvcg_sao sao[3];
+  uint8_t alf_luma;      /* alf_ctb_flag of the luma CTB */
+  uint8_t reserved;
+} vvcg_ctu_filter;
+
+/* Luma ALF parameters (hls.rs:2699 VvcAlfAps, luma part). */
+typedef struct vvcg_alf_aps {
+  uint8_t num_luma_filters;    /* 0 = fixed filter of each class */
+  uint8_t luma_clip;           /* alf_luma_clip_flag */
+  uint8_t coeff_delta_idx[25]; /* class -> filter */
+  uint8_t reserved;
+  int16_t coeff[25][12];
+  uint8_t clip_idx[25][12];
+} vvcg_alf_aps;
+
+/* A batch of independent pictures (frames of one or many streams). */
+typedef struct vvcg_batch {
+  const vvcg_pic_desc* pics;
+  uint32_t num_pics;
+  uint32_t num_cus;
+  const vvcg_cu_rec* cus;
+  const int16_t* levels;
+  uint64_t num_levels;
+  const vvcg_ctu_filter* ctus;
+  uint32_t num_ctus;
+  uint32_t num_aps;
+  const vvcg_alf_aps* aps;
+} vvcg_batch;
+
+/* Destination of one output plane; stride in samples. */
+typedef struct vvcg_plane_out {
+  uint16_t* data;
+  uint32_t stride;
+  uint32_t reserved;
+} vvcg_plane_out;
+
+/* Stages of vvcg_batch_run. */
+enum {
+  VVCG_STAGE_RECON = 1u << 0,   /* dequant + inverse transform + intra + add/clip */
+  VVCG_STAGE_DEBLOCK = 1u << 1, /* pictures with VVCG_TOOL_DEBLOCK */
+  VVCG_STAGE_SAO = 1u << 2,     /* pictures with VVCG_TOOL_SAO */
+  VVCG_STAGE_ALF = 1u << 3,     /* pictures with VVCG_TOOL_ALF and an enabled CTU */
+  VVCG_STAGE_ALL = 0xFu
+};
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Replaces: constructing the reference's accelerator provider
+ * (accelerator.rs:155-200 trait objects). */
+vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out);
+void vvcg_ctx_destroy(vvcg_ctx* ctx);
+const char* vvcg_last_error(const vvcg_ctx* ctx);
+/* Use a caller-owned cudaStream_t (NULL = the context's own stream). */
+vvcg_status vvcg_set_stream(vvcg_ctx* ctx, void* cuda_stream);
+/* Number of this library's kernels launched since the context was created. */
+uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx);
+
+/* ---- picture batches (frame path) ---------------------------------------- */
+
+/* Whole call with host buffers: upload, reconstruct, filter, download.
+ * `out` holds 3 planes (Y, Cb, Cr) per picture, num_pics * 3 entries; the
+ * visible area of each plane is written.
+ * Replaces: the per-CU reconstruction loop and the picture-level loop
+ * filters of slice::decode_vvc_frame_picture_with_chroma_qp
+ * (slice.rs:4834-4988 and :4990-5072). */
+vvcg_status vvcg_decode_batch(vvcg_ctx* ctx, const vvcg_batch* batch, const vvcg_plane_out* out);
+
+/* Split form of vvcg_decode_batch, for callers that keep pictures on the GPU:
+ * prepare (validate, schedule, size the device arena), upload (records and
+ * levels to the device), run (kernels only, asynchronous on the stream),
+ * sync (wait and read the device status word), download (visible planes). */
+vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* batch);
+vvcg_status vvcg_batch_upload(vvcg_ctx* ctx, const vvcg_batch* batch);
+vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t stage_mask);
+vvcg_status vvcg_batch_sync(vvcg_ctx* ctx);
+vvcg_status vvcg_batch_download(vvcg_ctx* ctx, const vvcg_plane_out* out);
+/* Device address and stride (samples) of one reconstructed plane. */
+vvcg_status vvcg_batch_plane(vvcg_ctx* ctx, uint32_t pic, uint32_t comp, void** dev_ptr,
+                             uint32_t* stride);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VVCG_H */

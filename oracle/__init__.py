@@ -1,0 +1,380 @@
+"""CPU oracle for the VVC reconstruction / loop-filter / candidate-cost path.
+
+TEST INFRASTRUCTURE ONLY: a C++ restatement of the reference codec's CPU code
+(rustmpeg-video, crates/rustmpeg-video/src/vvc/), loaded with ctypes. Only the
+tests, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` may use it,
+and only as the checker or the timed CPU baseline; the product library never
+links or calls it.
+
+Parity pinning: the reference is Rust and cannot be built here, so the
+restatement is pinned by the reference's own known-answer and property tests
+(ported in tests/test_oracle_kats.py). Paths those tests do not reach are
+"parity unpinned".
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liborc_vvc.so")
+_lib = None
+
+DCT2, DST7, DCT8 = 0, 1, 2
+CHROMA_400, CHROMA_420, CHROMA_422, CHROMA_444 = 0, 1, 2, 3
+OPT_FULL_INTRA, OPT_CCLM, OPT_DEP_QUANT, OPT_DEBLOCK = 1, 2, 4, 8
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (g++ -O2, scalar)."""
+    if force or not os.path.exists(_LIB_PATH):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    else:
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _declare(L):
+    vp, i = C.c_void_p, C.c_int
+    for name in ("orc_forward_transform", "orc_inverse_transform"):
+        getattr(L, name).argtypes = [i, i, vp, i, i, i, i, i, vp]
+    L.orc_quantize.argtypes = [i, i, vp, i, i, i, vp]
+    L.orc_dequantize.argtypes = [i, i, vp, i, i, vp]
+    L.orc_quantize_dq.argtypes = [i, i, vp, i, i, vp]
+    L.orc_dequantize_dq.argtypes = [i, i, vp, i, i, vp]
+    L.orc_coeff_scan.argtypes = [i, i, vp]
+    L.orc_quantize_ts.argtypes = [i, i]
+    L.orc_dequantize_ts.argtypes = [i, i]
+    L.orc_scaled_luma_qp.argtypes = [i, i]
+    L.orc_chroma_qp.argtypes = [i, i, i]
+    L.orc_wide_angle.argtypes = [i, i, i]
+    L.orc_angular_params.argtypes = [i, i, i, i, vp]
+    L.orc_angular_params.restype = None
+    L.orc_predict_block.argtypes = [vp, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_predict_block.restype = None
+    L.orc_predict_coded_block.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, vp, i, i, i, vp]
+    L.orc_predict_coded_block.restype = None
+    L.orc_predict_cclm.argtypes = [vp, i, i, vp, i, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_predict_cclm.restype = None
+    L.orc_choose_intra_mode.argtypes = [vp, vp, i, i, i, i, i, i, i]
+    L.orc_deblock_luma.argtypes = [vp, i, i, i, i, i, i, i, i, i]
+    L.orc_deblock_luma.restype = None
+    L.orc_deblock_chroma.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i]
+    L.orc_deblock_chroma.restype = None
+    L.orc_sao_region.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_sao_region.restype = None
+    L.orc_alf_luma.argtypes = [vp, i, i, i, i, i, vp, vp, vp]
+    L.orc_alf_classify.argtypes = [vp, i, i, i, i, i, vp]
+    L.orc_alf_classify.restype = None
+    L.orc_mc_luma.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_mc_luma.restype = None
+    L.orc_mc_chroma.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_mc_chroma.restype = None
+    L.orc_bi_average.argtypes = [vp, vp, i, i, i, vp]
+    L.orc_bi_average.restype = None
+    L.orc_encode_frame.argtypes = [vp, vp, vp, i, i, i, i, i, i, i, vp, vp, C.c_uint64,
+                                   C.POINTER(C.c_uint64), vp, vp, vp]
+    L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+
+
+# ---------------------------------------------------------------- transforms --
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def forward_transform(res, tr_hor=DCT2, tr_ver=DCT2, skip_w=0, skip_h=0, bd=8):
+    res = _i32(res)
+    h, w = res.shape
+    out = np.zeros_like(res)
+    rc = lib().orc_forward_transform(w, h, _p(res), tr_hor, tr_ver, skip_w, skip_h, bd, _p(out))
+    if rc:
+        raise ValueError(f"forward transform rejected ({rc})")
+    return out
+
+
+def inverse_transform(co, tr_hor=DCT2, tr_ver=DCT2, skip_w=0, skip_h=0, bd=8):
+    co = _i32(co)
+    h, w = co.shape
+    out = np.zeros_like(co)
+    rc = lib().orc_inverse_transform(w, h, _p(co), tr_hor, tr_ver, skip_w, skip_h, bd, _p(out))
+    if rc:
+        raise ValueError(f"inverse transform rejected ({rc})")
+    return out
+
+
+def quantize(co, qp, bd=8, intra=True):
+    co = _i32(co)
+    h, w = co.shape
+    out = np.zeros_like(co)
+    if lib().orc_quantize(w, h, _p(co), qp, bd, int(intra), _p(out)):
+        raise ValueError("quantize rejected")
+    return out
+
+
+def dequantize(lv, qp, bd=8):
+    lv = _i32(lv)
+    h, w = lv.shape
+    out = np.zeros_like(lv)
+    if lib().orc_dequantize(w, h, _p(lv), qp, bd, _p(out)):
+        raise ValueError("dequantize rejected")
+    return out
+
+
+def quantize_dq(co, qp, bd=8):
+    co = _i32(co)
+    h, w = co.shape
+    out = np.zeros_like(co)
+    if lib().orc_quantize_dq(w, h, _p(co), qp, bd, _p(out)):
+        raise ValueError("dep quant rejected")
+    return out
+
+
+def dequantize_dq(lv, qp, bd=8):
+    lv = _i32(lv)
+    h, w = lv.shape
+    out = np.zeros_like(lv)
+    if lib().orc_dequantize_dq(w, h, _p(lv), qp, bd, _p(out)):
+        raise ValueError("dep dequant rejected")
+    return out
+
+
+def coeff_scan(w, h):
+    out = np.zeros(w * h, dtype=np.int32)
+    n = lib().orc_coeff_scan(w, h, _p(out))
+    return out[:n]
+
+
+def quantize_ts(r, qp):
+    return lib().orc_quantize_ts(int(r), qp)
+
+
+def dequantize_ts(level, qp):
+    return lib().orc_dequantize_ts(int(level), qp)
+
+
+def scaled_luma_qp(qp, bd):
+    return lib().orc_scaled_luma_qp(qp, bd)
+
+
+def chroma_qp(qp, bd, offset=0):
+    return lib().orc_chroma_qp(qp, bd, offset)
+
+
+def wide_angle(w, h, mode):
+    return lib().orc_wide_angle(w, h, mode)
+
+
+def angular_params(mode, w, h, is_luma=True):
+    out = np.zeros(8, dtype=np.int32)
+    lib().orc_angular_params(mode, w, h, int(is_luma), _p(out))
+    keys = ("pred_mode", "is_mode_ver", "intra_pred_angle", "abs_inv_angle",
+            "ref_filter_flag", "interpolation_flag", "apply_pdpc", "angular_scale")
+    return dict(zip(keys, out.tolist()))
+
+
+# --------------------------------------------------------------------- intra --
+
+def _u16(a):
+    return np.ascontiguousarray(a, dtype=np.uint16)
+
+
+def predict_block(plane, bd, x, y, w, h, mode, is_luma=True):
+    plane = _u16(plane)
+    out = np.zeros((h, w), dtype=np.uint16)
+    lib().orc_predict_block(_p(plane), plane.shape[1], plane.shape[0], bd, x, y, w, h,
+                            int(is_luma), mode, _p(out))
+    return out
+
+
+def predict_coded_block(plane, bd, x, y, w, h, mode, coded, tb, is_luma=True, sx=1, sy=1):
+    plane = _u16(plane)
+    coded = np.ascontiguousarray(coded, dtype=np.uint8)
+    out = np.zeros((h, w), dtype=np.uint16)
+    lib().orc_predict_coded_block(_p(plane), plane.shape[1], plane.shape[0], bd, x, y, w, h,
+                                  int(is_luma), mode, sx, sy, _p(coded), coded.shape[1],
+                                  coded.shape[0], tb, _p(out))
+    return out
+
+
+def predict_cclm(luma, chroma, bd, bxc, byc, cw, ch, mode, cf=CHROMA_420, ctu=32):
+    luma, chroma = _u16(luma), _u16(chroma)
+    out = np.zeros((ch, cw), dtype=np.uint16)
+    lib().orc_predict_cclm(_p(luma), luma.shape[1], luma.shape[0], _p(chroma), chroma.shape[1],
+                           chroma.shape[0], bd, bxc, byc, cw, ch, mode, cf, ctu, _p(out))
+    return out
+
+
+def choose_intra_mode(recon, src, bd, bx, by, w, h):
+    recon, src = _u16(recon), _u16(src)
+    return lib().orc_choose_intra_mode(_p(recon), _p(src), recon.shape[1], recon.shape[0], bd,
+                                       bx, by, w, h)
+
+
+# ------------------------------------------------------------------- filters --
+
+def deblock_luma(plane, bd, cu_step, ctb, qp, bs=2, beta_off=0, tc_off=0):
+    p = _u16(plane).copy()
+    lib().orc_deblock_luma(_p(p), p.shape[1], p.shape[0], bd, cu_step, ctb, qp, bs, beta_off,
+                           tc_off)
+    return p
+
+
+def deblock_chroma(plane, bd, cu_step, ctb_h, qp, bs=2, beta_off=0, tc_off=0, sub_w=2, sub_h=2):
+    p = _u16(plane).copy()
+    lib().orc_deblock_chroma(_p(p), p.shape[1], p.shape[0], bd, cu_step, ctb_h, qp, bs, beta_off,
+                             tc_off, sub_w, sub_h)
+    return p
+
+
+def sao_region(src, dst, bd, bx, by, w, h, sao_type, band_or_class, offsets):
+    src = _u16(src)
+    dst = _u16(dst).copy()
+    off = np.asarray(offsets, dtype=np.int32)
+    lib().orc_sao_region(_p(src), _p(dst), src.shape[1], src.shape[0], bd, bx, by, w, h,
+                         sao_type, band_or_class, _p(off))
+    return dst
+
+
+def alf_luma(plane, bd, aps=None):
+    """Whole-plane luma ALF. aps: dict(coeff[n,12], clip_idx[n,12], delta_idx[25], luma_clip)."""
+    p = _u16(plane).copy()
+    if aps is None:
+        rc = lib().orc_alf_luma(_p(p), p.shape[1], p.shape[0], bd, 0, 0, None, None, None)
+    else:
+        coeff = np.zeros((25, 12), dtype=np.int16)
+        clip = np.zeros((25, 12), dtype=np.uint8)
+        n = len(aps["coeff"])
+        coeff[:n] = aps["coeff"]
+        clip[:n] = aps.get("clip_idx", np.zeros((n, 12)))
+        delta = np.ascontiguousarray(aps["delta_idx"], dtype=np.uint8)
+        rc = lib().orc_alf_luma(_p(p), p.shape[1], p.shape[0], bd, n, int(aps.get("luma_clip", 0)),
+                                _p(delta), _p(coeff), _p(clip))
+    return p, rc
+
+
+def alf_classify(plane, bd, bx, by):
+    plane = _u16(plane)
+    out = np.zeros(2, dtype=np.int32)
+    lib().orc_alf_classify(_p(plane), plane.shape[1], plane.shape[0], bd, bx, by, _p(out))
+    return int(out[0]), int(out[1])
+
+
+# ----------------------------------------------------------------------- MC --
+
+def mc_luma(ref, bd, bx, by, w, h, mvx, mvy, bi=False, affine=False, alt_hpel=False):
+    ref = _u16(ref)
+    out = np.zeros((h, w), dtype=np.int32)
+    lib().orc_mc_luma(_p(ref), ref.shape[1], ref.shape[0], bd, bx, by, w, h, mvx, mvy, int(bi),
+                      int(affine), int(alt_hpel), _p(out))
+    return out
+
+
+def mc_chroma(ref, bd, bxc, byc, cw, ch, mvx, mvy, bi=False, cf=CHROMA_420):
+    ref = _u16(ref)
+    out = np.zeros((ch, cw), dtype=np.int32)
+    lib().orc_mc_chroma(_p(ref), ref.shape[1], ref.shape[0], bd, bxc, byc, cw, ch, mvx, mvy,
+                        int(bi), cf, _p(out))
+    return out
+
+
+def bi_average(p0, p1, bcw, bd):
+    p0, p1 = _i32(p0), _i32(p1)
+    out = np.zeros(p0.shape, dtype=np.uint16)
+    lib().orc_bi_average(_p(p0), _p(p1), p0.size, bcw, bd, _p(out))
+    return out
+
+
+# ------------------------------------------------------------ frame path --
+
+# Record layouts of include/vvcg.h, as numpy structured dtypes.
+CU_DTYPE = np.dtype([("luma_mode", "u1"), ("chroma_mode", "u1"), ("cbf", "u1"),
+                     ("reserved", "u1"), ("level_off", "<i4", (3,))])
+SAO_DTYPE = np.dtype([("type", "u1"), ("band_or_class", "u1"), ("offsets", "i1", (4,))])
+CTU_DTYPE = np.dtype([("sao", SAO_DTYPE, (3,)), ("alf_luma", "u1"), ("reserved", "u1")])
+PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("visible_width", "<u4"),
+                      ("visible_height", "<u4"), ("bit_depth", "u1"), ("chroma_format", "u1"),
+                      ("ctu_log2", "u1"), ("slice_qp", "u1"), ("chroma_qp_scaled", "u1"),
+                      ("tools", "u1"), ("alf_aps", "<i2"), ("cu_offset", "<u4"),
+                      ("ctu_offset", "<u4")])
+APS_DTYPE = np.dtype([("num_luma_filters", "u1"), ("luma_clip", "u1"),
+                      ("coeff_delta_idx", "u1", (25,)), ("reserved", "u1"),
+                      ("coeff", "<i2", (25, 12)), ("clip_idx", "u1", (25, 12))])
+TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
+assert CU_DTYPE.itemsize == 16 and CTU_DTYPE.itemsize == 20 and PIC_DTYPE.itemsize == 32
+
+
+def chroma_dims(w, h, cf):
+    if cf == CHROMA_400:
+        return 0, 0
+    sw = 2 if cf in (CHROMA_420, CHROMA_422) else 1
+    sh = 2 if cf == CHROMA_420 else 1
+    return (w + sw - 1) // sw, (h + sh - 1) // sh
+
+
+def encode_frame(y, u, v, bd, qp, ctu_log2=5, opts=OPT_FULL_INTRA | OPT_DEBLOCK, cf=CHROMA_420):
+    """Restated slice::encode_vvc_frame_picture on coded-size planes.
+
+    Returns (cus, levels, (rec_y, rec_u, rec_v)): cus is a CU_DTYPE array in
+    tb-grid raster order, levels the int16 pool the records index.
+    """
+    y = _u16(y)
+    h, w = y.shape
+    cw, ch = chroma_dims(w, h, cf)
+    u = _u16(u) if cf else np.zeros((1, 1), np.uint16)
+    v = _u16(v) if cf else np.zeros((1, 1), np.uint16)
+    tb = min(1 << ctu_log2, 32)
+    cus = np.zeros((h // tb) * (w // tb), dtype=CU_DTYPE)
+    cap = w * h * 2 + 64
+    levels = np.zeros(cap, dtype=np.int16)
+    used = C.c_uint64(0)
+    ry = np.zeros((h, w), np.uint16)
+    ru = np.zeros((max(ch, 1), max(cw, 1)), np.uint16)
+    rv = np.zeros((max(ch, 1), max(cw, 1)), np.uint16)
+    rc = lib().orc_encode_frame(_p(y), _p(u), _p(v), w, h, bd, cf, qp, ctu_log2, opts, _p(cus),
+                                _p(levels), cap, C.byref(used), _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"encode_frame rejected ({rc})")
+    return cus, levels[: used.value].copy(), (ry, ru, rv)
+
+
+def recon_frame(pic, cus, levels, ctus, aps=None):
+    """Restated decode_vvc_frame_picture_with_chroma_qp reconstruction + filters.
+
+    pic: one PIC_DTYPE record; cus/ctus: the picture's own records. Returns
+    (status, (y, u, v)) with coded-size planes; status -3 marks the input on
+    which the reference aborts (fixed-filter ALF reaching class >= 16).
+    """
+    pic = np.asarray(pic, dtype=PIC_DTYPE).reshape(1).copy()
+    w, h = int(pic[0]["width"]), int(pic[0]["height"])
+    cf = int(pic[0]["chroma_format"])
+    cw, ch = chroma_dims(w, h, cf)
+    cus = np.ascontiguousarray(cus, dtype=CU_DTYPE)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    if levels.size == 0:
+        levels = np.zeros(1, np.int16)
+    ctus = np.ascontiguousarray(ctus, dtype=CTU_DTYPE)
+    aps_arr = None if aps is None else np.asarray(aps, dtype=APS_DTYPE).reshape(1).copy()
+    y = np.zeros((h, w), np.uint16)
+    u = np.zeros((max(ch, 1), max(cw, 1)), np.uint16)
+    v = np.zeros((max(ch, 1), max(cw, 1)), np.uint16)
+    rc = lib().orc_recon_frame(_p(pic), _p(cus), _p(levels), _p(ctus),
+                               None if aps_arr is None else _p(aps_arr), _p(y), _p(u), _p(v))
+    return rc, (y, u, v)

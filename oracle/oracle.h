@@ -1,0 +1,145 @@
+// CPU oracle for the VVC reconstruction / loop-filter / candidate-cost path.
+//
+// TEST INFRASTRUCTURE ONLY. This is a plain C++ restatement of the reference
+// codec's single-threaded CPU code (rustmpeg-video, crates/rustmpeg-video/src/vvc/),
+// function by function, each citing the reference file:line it follows. It is
+// the checker that the CUDA path is compared against, and the timed CPU
+// baseline in bench.py. Nothing in the product library links, loads or calls
+// it: only tests/, __graft_entry__.smoke() and bench.py's CPU legs use it.
+//
+// Parity pinning: the reference is Rust and no Rust toolchain is available,
+// so the reference itself cannot be run to produce golden outputs. The
+// restatement is pinned by the reference's own known-answer and property
+// tests, ported in tests/test_oracle_kats.py (see the header of that file for
+// the list); anything those tests do not reach is "parity unpinned".
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace orc {
+
+enum TrType { kDct2 = 0, kDst7 = 1, kDct8 = 2 };
+
+// ---- dct.rs -----------------------------------------------------------------
+const int8_t* matrix_for_any(int tr, int size);
+int forward_transform_rect_bd(int w, int h, const int32_t* residual, int tr_hor, int tr_ver,
+                              int extra_skip_w, int extra_skip_h, int bd, int32_t* out);
+int inverse_transform_rect_bd(int w, int h, const int32_t* coeffs, int tr_hor, int tr_ver,
+                              int extra_skip_w, int extra_skip_h, int bd, int32_t* out);
+int quantize_rect_bd(int w, int h, const int32_t* coeffs, int qp_scaled, int bd, bool is_intra,
+                     int32_t* out);
+int dequantize_rect_bd(int w, int h, const int32_t* levels, int qp_scaled, int bd, int32_t* out);
+int dequantize_dep_quant_bd(int w, int h, const int32_t* levels, const int32_t* scan_raster,
+                            int qp_scaled, int bd, int32_t* out);
+int quantize_dep_quant_bd(int w, int h, const int32_t* coeffs, const int32_t* scan_raster,
+                          int qp_scaled, int bd, int32_t* out);
+
+// ---- transform.rs -------------------------------------------------------------
+// Grouped diagonal scan; returns the number of scan positions written.
+int coeff_scan_raster(int w, int h, int32_t* raster);
+int32_t quantize_ts(int32_t residual, int qp);
+int32_t dequantize_ts(int32_t level, int qp);
+
+// ---- lfnst.rs -----------------------------------------------------------------
+int get_lfnst_intra_mode(int mode);
+int inverse_lfnst_rect(int32_t* coeffs, int w, int h, int lfnst_idx, int intra_mode);
+int forward_lfnst_rect(int32_t* coeffs, int w, int h, int lfnst_idx, int intra_mode);
+
+// ---- predict.rs (16-bit sample planes) ----------------------------------------
+struct Plane16 {
+  uint16_t* data;
+  int width;
+  int height;
+  int bd;
+  uint16_t get(int x, int y) const { return data[(size_t)y * width + x]; }
+  void set(int x, int y, int v) {
+    int mx = (1 << bd) - 1;
+    data[(size_t)y * width + x] = (uint16_t)(v > mx ? mx : v);
+  }
+};
+
+struct Refs16 {
+  int top_left;
+  std::vector<int> above;  // 2 * width
+  std::vector<int> left;   // 2 * height
+  int bd;
+};
+
+// Coded-unit availability map of the 10-bit frame path (slice.rs CodedUnits).
+struct CodedMap {
+  const uint8_t* coded;
+  int grid_w, grid_h, tb;
+  bool is_coded_luma(int x, int y) const {
+    int gx = x / tb, gy = y / tb;
+    return gx < grid_w && gy < grid_h && coded[gy * grid_w + gx];
+  }
+};
+
+Refs16 gather_references_16(const Plane16& p, int x, int y, int w, int h);
+void predict_from_refs_16(const Refs16& refs, int w, int h, bool is_luma, int mode, uint16_t* out);
+void predict_block_16(const Plane16& p, int x, int y, int w, int h, bool is_luma, int mode,
+                      uint16_t* out);
+void predict_coded_block_16(const Plane16& p, int x, int y, int w, int h, bool is_luma, int mode,
+                            int scale_x, int scale_y, const CodedMap& cm, uint16_t* out);
+// cclm_mode: 0 = LM (LT), 1 = LM-L, 2 = LM-T; chroma_format 1 = 4:2:0, 2 = 4:2:2, 3 = 4:4:4
+void predict_cclm_with_format_16(const Plane16& luma, const Plane16& chroma, int bxc, int byc,
+                                 int cw, int ch, int cclm_mode, int chroma_format, int ctu_size,
+                                 uint16_t* out);
+int choose_intra_mode_16(const Plane16& recon, const Plane16& src, int bx, int by, int w, int h,
+                         bool is_luma);
+
+struct AngularParams {
+  int pred_mode;
+  bool is_mode_ver;
+  int intra_pred_angle;
+  int abs_inv_angle;
+  bool ref_filter_flag;
+  bool interpolation_flag;
+  bool apply_pdpc;
+  int angular_scale;
+};
+AngularParams init_angular_params(int dir_mode, int pu_w, int pu_h, int cu_w, int cu_h,
+                                  bool is_luma, int mrl_idx, bool use_isp);
+int get_modified_wide_angle(int w, int h, int mode);
+
+// ---- filter.rs (16-bit) ---------------------------------------------------------
+void deblock_luma_plane_16(Plane16& p, int cu_step, int ctb_size, int qp, int bs, int beta_off,
+                           int tc_off);
+void deblock_chroma_plane_16(Plane16& p, int cu_step, int ctb_height_c, int qp_c, int bs,
+                             int beta_off, int tc_off, int sub_w, int sub_h);
+struct Sao {
+  int type;  // 0 off, 1 band offset, 2 edge offset
+  int band_pos_or_class;
+  int offsets[4];
+};
+void apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
+                         const Sao& sao);
+struct AlfAps {
+  int num_luma_filters;  // 0 = fixed filters of the class
+  bool luma_clip;
+  uint8_t coeff_delta_idx[25];
+  int16_t coeff[25][12];
+  uint8_t clip_idx[25][12];
+};
+// Sets g_alf_status to -1 where the reference would abort (see orc_filter.cpp).
+extern int g_alf_status;
+void apply_alf_luma_plane_16(Plane16& p, const AlfAps& aps);
+void classify_alf_4x4_16(const Plane16& p, int bx, int by, int* class_idx, int* transpose_idx);
+
+// ---- inter.rs (16-bit) ----------------------------------------------------------
+void interpolate_luma_block_16(const Plane16& ref, int bx, int by, int w, int h, int mv_x,
+                               int mv_y, bool bi, bool affine, bool alt_hpel, int32_t* out);
+void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, int cw, int ch,
+                                        int mv_x, int mv_y, bool bi, int chroma_format,
+                                        int32_t* out);
+void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int bd,
+                            uint16_t* out);
+
+// ---- hls.rs ---------------------------------------------------------------------
+int scaled_luma_qp_bd(int qpy, int bd);
+int derived_chroma_qp_bd(int qpy, int bd, int chroma_qp_offset);
+int derived_chroma_qp(int qp);
+
+}  // namespace orc

@@ -1,0 +1,134 @@
+// CPU oracle (test infrastructure only; see oracle.h): flat extern "C" entry
+// points over the restated reference functions, for the Python tests and the
+// CPU legs of bench.py (loaded with ctypes). Each wraps one function of the
+// oracle with plain pointers; planes are row-major with stride = width.
+#include <string.h>
+
+#include <vector>
+
+#include "oracle.h"
+
+using namespace orc;
+
+extern "C" {
+
+int orc_forward_transform(int w, int h, const int32_t* res, int trh, int trv, int esw, int esh,
+                          int bd, int32_t* out) {
+  return forward_transform_rect_bd(w, h, res, trh, trv, esw, esh, bd, out);
+}
+int orc_inverse_transform(int w, int h, const int32_t* co, int trh, int trv, int esw, int esh,
+                          int bd, int32_t* out) {
+  return inverse_transform_rect_bd(w, h, co, trh, trv, esw, esh, bd, out);
+}
+int orc_quantize(int w, int h, const int32_t* c, int qp, int bd, int intra, int32_t* out) {
+  return quantize_rect_bd(w, h, c, qp, bd, intra != 0, out);
+}
+int orc_dequantize(int w, int h, const int32_t* l, int qp, int bd, int32_t* out) {
+  return dequantize_rect_bd(w, h, l, qp, bd, out);
+}
+int orc_quantize_dq(int w, int h, const int32_t* c, int qp, int bd, int32_t* out) {
+  std::vector<int32_t> scan(w * h);
+  coeff_scan_raster(w, h, scan.data());
+  return quantize_dep_quant_bd(w, h, c, scan.data(), qp, bd, out);
+}
+int orc_dequantize_dq(int w, int h, const int32_t* l, int qp, int bd, int32_t* out) {
+  std::vector<int32_t> scan(w * h);
+  coeff_scan_raster(w, h, scan.data());
+  return dequantize_dep_quant_bd(w, h, l, scan.data(), qp, bd, out);
+}
+int orc_coeff_scan(int w, int h, int32_t* raster) { return coeff_scan_raster(w, h, raster); }
+int orc_quantize_ts(int r, int qp) { return quantize_ts(r, qp); }
+int orc_dequantize_ts(int l, int qp) { return dequantize_ts(l, qp); }
+int orc_scaled_luma_qp(int qp, int bd) { return scaled_luma_qp_bd(qp, bd); }
+int orc_chroma_qp(int qp, int bd, int off) { return derived_chroma_qp_bd(qp, bd, off); }
+int orc_wide_angle(int w, int h, int mode) { return get_modified_wide_angle(w, h, mode); }
+void orc_angular_params(int mode, int w, int h, int is_luma, int32_t* out8) {
+  AngularParams p = init_angular_params(mode, w, h, w, h, is_luma != 0, 0, false);
+  out8[0] = p.pred_mode;
+  out8[1] = p.is_mode_ver;
+  out8[2] = p.intra_pred_angle;
+  out8[3] = p.abs_inv_angle;
+  out8[4] = p.ref_filter_flag;
+  out8[5] = p.interpolation_flag;
+  out8[6] = p.apply_pdpc;
+  out8[7] = p.angular_scale;
+}
+
+void orc_predict_block(const uint16_t* plane, int pw, int ph, int bd, int x, int y, int w, int h,
+                       int is_luma, int mode, uint16_t* out) {
+  Plane16 p{(uint16_t*)plane, pw, ph, bd};
+  predict_block_16(p, x, y, w, h, is_luma != 0, mode, out);
+}
+// `coded` is the tb-grid availability map of predict_coded_block_16.
+void orc_predict_coded_block(const uint16_t* plane, int pw, int ph, int bd, int x, int y, int w,
+                             int h, int is_luma, int mode, int sx, int sy, const uint8_t* coded,
+                             int gw, int gh, int tb, uint16_t* out) {
+  Plane16 p{(uint16_t*)plane, pw, ph, bd};
+  CodedMap cm{coded, gw, gh, tb};
+  predict_coded_block_16(p, x, y, w, h, is_luma != 0, mode, sx, sy, cm, out);
+}
+void orc_predict_cclm(const uint16_t* luma, int lw, int lh, const uint16_t* chroma, int cw_, int ch_,
+                      int bd, int bxc, int byc, int cw, int ch, int mode, int cf, int ctu,
+                      uint16_t* out) {
+  Plane16 l{(uint16_t*)luma, lw, lh, bd}, c{(uint16_t*)chroma, cw_, ch_, bd};
+  predict_cclm_with_format_16(l, c, bxc, byc, cw, ch, mode, cf, ctu, out);
+}
+int orc_choose_intra_mode(const uint16_t* recon, const uint16_t* src, int pw, int ph, int bd,
+                          int bx, int by, int w, int h) {
+  Plane16 r{(uint16_t*)recon, pw, ph, bd}, s{(uint16_t*)src, pw, ph, bd};
+  return choose_intra_mode_16(r, s, bx, by, w, h, true);
+}
+
+void orc_deblock_luma(uint16_t* plane, int pw, int ph, int bd, int cu_step, int ctb, int qp, int bs,
+                      int beta_off, int tc_off) {
+  Plane16 p{plane, pw, ph, bd};
+  deblock_luma_plane_16(p, cu_step, ctb, qp, bs, beta_off, tc_off);
+}
+void orc_deblock_chroma(uint16_t* plane, int pw, int ph, int bd, int cu_step, int ctb_h, int qp,
+                        int bs, int beta_off, int tc_off, int sub_w, int sub_h) {
+  Plane16 p{plane, pw, ph, bd};
+  deblock_chroma_plane_16(p, cu_step, ctb_h, qp, bs, beta_off, tc_off, sub_w, sub_h);
+}
+void orc_sao_region(const uint16_t* src, uint16_t* dst, int pw, int ph, int bd, int bx, int by,
+                    int w, int h, int type, int band_or_class, const int32_t* offsets) {
+  Plane16 s{(uint16_t*)src, pw, ph, bd}, d{dst, pw, ph, bd};
+  Sao sao{type, band_or_class, {offsets[0], offsets[1], offsets[2], offsets[3]}};
+  apply_sao_region_16(s, d, bx, by, w, h, sao);
+}
+// aps == NULL selects the fixed filters. Returns -1 where the reference aborts.
+int orc_alf_luma(uint16_t* plane, int pw, int ph, int bd, int num_filters, int luma_clip,
+                 const uint8_t* delta_idx, const int16_t* coeff, const uint8_t* clip_idx) {
+  Plane16 p{plane, pw, ph, bd};
+  AlfAps a;
+  memset(&a, 0, sizeof(a));
+  a.num_luma_filters = num_filters;
+  a.luma_clip = luma_clip != 0;
+  if (num_filters > 0) {
+    memcpy(a.coeff_delta_idx, delta_idx, 25);
+    memcpy(a.coeff, coeff, sizeof(int16_t) * 25 * 12);
+    memcpy(a.clip_idx, clip_idx, 25 * 12);
+  }
+  apply_alf_luma_plane_16(p, a);
+  return g_alf_status;
+}
+void orc_alf_classify(const uint16_t* plane, int pw, int ph, int bd, int bx, int by,
+                      int32_t* out2) {
+  Plane16 p{(uint16_t*)plane, pw, ph, bd};
+  classify_alf_4x4_16(p, bx, by, &out2[0], &out2[1]);
+}
+
+void orc_mc_luma(const uint16_t* ref, int pw, int ph, int bd, int bx, int by, int w, int h, int mvx,
+                 int mvy, int bi, int affine, int alt_hpel, int32_t* out) {
+  Plane16 p{(uint16_t*)ref, pw, ph, bd};
+  interpolate_luma_block_16(p, bx, by, w, h, mvx, mvy, bi != 0, affine != 0, alt_hpel != 0, out);
+}
+void orc_mc_chroma(const uint16_t* ref, int pw, int ph, int bd, int bxc, int byc, int cw, int ch,
+                   int mvx, int mvy, int bi, int cf, int32_t* out) {
+  Plane16 p{(uint16_t*)ref, pw, ph, bd};
+  interpolate_chroma_block_format_16(p, bxc, byc, cw, ch, mvx, mvy, bi != 0, cf, out);
+}
+void orc_bi_average(const int32_t* p0, const int32_t* p1, int n, int bcw, int bd, uint16_t* out) {
+  weighted_average_bi_16(p0, p1, n, bcw, bd, out);
+}
+
+}  // extern "C"

@@ -1,0 +1,180 @@
+// CPU oracle (test infrastructure only; see oracle.h): 8..12-bit motion
+// compensation interpolation. Restates crates/rustmpeg-video/src/vvc/inter.rs
+// (interpolate_luma_block_16, interpolate_chroma_block_format_16,
+// weighted_average_bi_16) of the reference, including its uni-prediction
+// second-stage shift `12 - bd` for 2-D fractional positions (inter.rs:2051,
+// :2583), which differs from the 8-bit path's `6 + headroom`.
+#include <algorithm>
+#include <vector>
+
+#include "../rustmpeg-next_b200/csrc/vvc_tables.h"
+#include "oracle.h"
+
+namespace orc {
+using namespace vvc_tables;
+
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// inter.rs:2010-2134 interpolate_luma_block_16
+void interpolate_luma_block_16(const Plane16& ref, int bx, int by, int w, int h, int mv_x, int mv_y,
+                               bool bi, bool affine, bool alt_hpel, int32_t* out) {
+  int dx = mv_x >> 4, dy = mv_y >> 4;
+  int fx = mv_x & 15, fy = mv_y & 15;
+  int bd = clampi(ref.bd, 8, 12);
+  int mx = (1 << bd) - 1;
+  auto g = [&](int x, int y) {
+    return (int)ref.get(clampi(x, 0, ref.width - 1), clampi(y, 0, ref.height - 1));
+  };
+  auto filt = [&](int frac, int* f) {
+    for (int k = 0; k < 8; k++) {
+      if (affine)
+        f[k] = kAffineTaps8[frac * 8 + k];
+      else if (alt_hpel && frac == 8)
+        f[k] = kLumaAltHpel[k];
+      else
+        f[k] = kLumaTaps8[frac * 8 + k];
+    }
+  };
+  int head = std::max(14 - bd, 2);
+  int shift1 = 6 - head;
+  int shift2 = bi ? 6 : 12 - bd;
+  int add2 = bi ? 0 : 1 << (shift2 - 1);
+  int offs = 1 << (bd + head - 1);
+  if (fx == 0 && fy == 0) {
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        int s = g(bx + x + dx, by + y + dy);
+        out[y * w + x] = bi ? (s << head) - offs : s;
+      }
+    return;
+  }
+  if (fy == 0) {
+    int f[8];
+    filt(fx, f);
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        int px = bx + x + dx, py = by + y + dy;
+        int s = 0;
+        for (int k = 0; k < 8; k++) s += f[k] * g(px + k - 3, py);
+        out[y * w + x] = bi ? (s >> shift1) - offs : clampi((s + 32) >> 6, 0, mx);
+      }
+    return;
+  }
+  if (fx == 0) {
+    int f[8];
+    filt(fy, f);
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        int px = bx + x + dx, py = by + y + dy;
+        int s = 0;
+        for (int k = 0; k < 8; k++) s += f[k] * g(px, py + k - 3);
+        out[y * w + x] = bi ? (s >> shift1) - offs : clampi((s + 32) >> 6, 0, mx);
+      }
+    return;
+  }
+  int fh[8], fv[8];
+  filt(fx, fh);
+  filt(fy, fv);
+  int th = h + 7;
+  std::vector<int> tmp((size_t)w * th);
+  for (int ty = 0; ty < th; ty++) {
+    int py = by + ty - 3 + dy;
+    for (int x = 0; x < w; x++) {
+      int px = bx + x + dx;
+      int s = 0;
+      for (int k = 0; k < 8; k++) s += fh[k] * g(px + k - 3, py);
+      tmp[ty * w + x] = s >> shift1;
+    }
+  }
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      int s = 0;
+      for (int k = 0; k < 8; k++) s += fv[k] * tmp[(y + k) * w + x];
+      out[y * w + x] = bi ? (s >> shift2) - offs : clampi((s + add2) >> shift2, 0, mx);
+    }
+}
+
+// inter.rs:2543-2672 interpolate_chroma_block_format_16 (cf: 1 = 4:2:0, 2 = 4:2:2, 3 = 4:4:4)
+void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, int cw, int ch,
+                                        int mv_x, int mv_y, bool bi, int cf, int32_t* out) {
+  if (cw == 0 || ch == 0 || cf == 0) return;
+  int sub_w = (cf == 1 || cf == 2) ? 2 : 1;
+  int sub_h = cf == 1 ? 2 : 1;
+  int mvx32 = mv_x * (sub_w == 1 ? 2 : 1);
+  int mvy32 = mv_y * (sub_h == 1 ? 2 : 1);
+  int dx = mvx32 >> 5, dy = mvy32 >> 5;
+  int fx = mvx32 & 31, fy = mvy32 & 31;
+  int bd = clampi(ref.bd, 8, 12);
+  int mx = (1 << bd) - 1;
+  auto g = [&](int x, int y) {
+    return (int)ref.get(clampi(x, 0, ref.width - 1), clampi(y, 0, ref.height - 1));
+  };
+  int head = std::max(14 - bd, 2);
+  int shift1 = 6 - head;
+  int shift2 = bi ? 6 : 12 - bd;
+  int add2 = bi ? 0 : 1 << (shift2 - 1);
+  int offs = 1 << (bd + head - 1);
+  if (fx == 0 && fy == 0) {
+    for (int y = 0; y < ch; y++)
+      for (int x = 0; x < cw; x++) {
+        int s = g(bxc + x + dx, byc + y + dy);
+        out[y * cw + x] = bi ? (s << head) - offs : s;
+      }
+    return;
+  }
+  const int8_t* fh = &kChromaTaps4[fx * 4];
+  const int8_t* fv = &kChromaTaps4[fy * 4];
+  if (fy == 0) {
+    for (int y = 0; y < ch; y++)
+      for (int x = 0; x < cw; x++) {
+        int px = bxc + x + dx, py = byc + y + dy;
+        int s = 0;
+        for (int k = 0; k < 4; k++) s += fh[k] * g(px + k - 1, py);
+        out[y * cw + x] = bi ? (s >> shift1) - offs : clampi((s + 32) >> 6, 0, mx);
+      }
+    return;
+  }
+  if (fx == 0) {
+    for (int y = 0; y < ch; y++)
+      for (int x = 0; x < cw; x++) {
+        int px = bxc + x + dx, py = byc + y + dy;
+        int s = 0;
+        for (int k = 0; k < 4; k++) s += fv[k] * g(px, py + k - 1);
+        out[y * cw + x] = bi ? (s >> shift1) - offs : clampi((s + 32) >> 6, 0, mx);
+      }
+    return;
+  }
+  int th = ch + 3;
+  std::vector<int> tmp((size_t)cw * th);
+  for (int ty = 0; ty < th; ty++) {
+    int py = byc + ty - 1 + dy;
+    for (int x = 0; x < cw; x++) {
+      int px = bxc + x + dx;
+      int s = 0;
+      for (int k = 0; k < 4; k++) s += fh[k] * g(px + k - 1, py);
+      tmp[ty * cw + x] = s >> shift1;
+    }
+  }
+  for (int y = 0; y < ch; y++)
+    for (int x = 0; x < cw; x++) {
+      int s = 0;
+      for (int k = 0; k < 4; k++) s += fv[k] * tmp[(y + k) * cw + x];
+      out[y * cw + x] = bi ? (s >> shift2) - offs : clampi((s + add2) >> shift2, 0, mx);
+    }
+}
+
+// inter.rs:2676-2698 weighted_average_bi_16
+void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int bd,
+                            uint16_t* out) {
+  bd = clampi(bd, 8, 12);
+  int mx = (1 << bd) - 1;
+  int w1 = kBcwWeights[std::min(bcw_idx, 4)];
+  int w0 = 8 - w1;
+  int head = std::max(14 - bd, 2);
+  int sn = head + 3;
+  int io = 1 << (bd + head - 1);
+  int off = (1 << (sn - 1)) + (io << 3);
+  for (int i = 0; i < n; i++) out[i] = (uint16_t)clampi((p0[i] * w0 + p1[i] * w1 + off) >> sn, 0, mx);
+}
+
+}  // namespace orc
