@@ -194,6 +194,42 @@ vvcg_status vvcg_batch_download(vvcg_ctx* ctx, const vvcg_plane_out* out);
 vvcg_status vvcg_batch_plane(vvcg_ctx* ctx, uint32_t pic, uint32_t comp, void** dev_ptr,
                              uint32_t* stride);
 
+/* ---- motion compensation (batched blocks, device pointers) --------------- */
+
+enum {
+  VVCG_MC_BI = 1u << 0,      /* emit 14-bit bi-prediction intermediates */
+  VVCG_MC_AFFINE = 1u << 1,  /* 6-tap affine luma filters */
+  VVCG_MC_ALT_HPEL = 1u << 2 /* alternative half-pel luma filter */
+};
+
+typedef struct vvcg_mc_block {
+  int32_t x, y;        /* block position in the reference plane's sample grid */
+  uint16_t w, h;       /* block size, 1..128 */
+  int32_t mv_x, mv_y;  /* motion vector in 1/16 luma sample units */
+  uint32_t flags;      /* VVCG_MC_* */
+  uint32_t reserved;
+  uint64_t out_offset; /* first int32 output element; outputs are w*h, raster */
+} vvcg_mc_block;
+
+/* Batched luma interpolation. Replaces: inter::interpolate_luma_block_16
+ * (crates/rustmpeg-video/src/vvc/inter.rs:2010). Outputs clipped samples
+ * (uni-prediction) or 14-bit intermediates (VVCG_MC_BI). */
+vvcg_status vvcg_mc_luma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t width,
+                                uint32_t height, uint32_t stride, uint8_t bit_depth,
+                                const vvcg_mc_block* blocks, uint32_t num_blocks, int32_t* out);
+/* Batched chroma interpolation (chroma_format 1..3). Replaces:
+ * inter::interpolate_chroma_block_format_16 (inter.rs:2543). Block positions
+ * are in chroma samples; motion vectors stay in 1/16 luma units. */
+vvcg_status vvcg_mc_chroma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t width,
+                                  uint32_t height, uint32_t stride, uint8_t bit_depth,
+                                  uint8_t chroma_format, const vvcg_mc_block* blocks,
+                                  uint32_t num_blocks, int32_t* out);
+/* BCW weighted bi-prediction average. Replaces: inter::weighted_average_bi_16
+ * (inter.rs:2676). */
+vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* pred0, const int32_t* pred1,
+                                      uint64_t count, uint8_t bcw_idx, uint8_t bit_depth,
+                                      uint16_t* out);
+
 #ifdef __cplusplus
 }
 #endif

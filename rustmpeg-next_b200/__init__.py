@@ -1,0 +1,305 @@
+"""rustmpeg-next_b200: B200 (sm_100a) VVC reconstruction, loop filtering and
+motion compensation behind the C ABI of include/vvcg.h (libvvcg.so).
+
+This module is the Python binding of that ABI (ctypes): the record layouts as
+numpy dtypes, a context class, and typed errors that mirror the reference's
+AcceleratorError (crates/rustmpeg-video/src/accelerator.rs:17-31). All
+computation happens in the CUDA library; there is no CPU fallback, and every
+call raises when the library or a CUDA device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "lib")
+LIB_PATH = os.path.join(LIB_DIR, "libvvcg.so")
+CSRC = os.path.join(HERE, "csrc")
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-shared"]
+
+# ------------------------------------------------------------------ records --
+CU_DTYPE = np.dtype([("luma_mode", "u1"), ("chroma_mode", "u1"), ("cbf", "u1"),
+                     ("reserved", "u1"), ("level_off", "<i4", (3,))])
+SAO_DTYPE = np.dtype([("type", "u1"), ("band_or_class", "u1"), ("offsets", "i1", (4,))])
+CTU_DTYPE = np.dtype([("sao", SAO_DTYPE, (3,)), ("alf_luma", "u1"), ("reserved", "u1")])
+PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("visible_width", "<u4"),
+                      ("visible_height", "<u4"), ("bit_depth", "u1"), ("chroma_format", "u1"),
+                      ("ctu_log2", "u1"), ("slice_qp", "u1"), ("chroma_qp_scaled", "u1"),
+                      ("tools", "u1"), ("alf_aps", "<i2"), ("cu_offset", "<u4"),
+                      ("ctu_offset", "<u4")])
+APS_DTYPE = np.dtype([("num_luma_filters", "u1"), ("luma_clip", "u1"),
+                      ("coeff_delta_idx", "u1", (25,)), ("reserved", "u1"),
+                      ("coeff", "<i2", (25, 12)), ("clip_idx", "u1", (25, 12))])
+MC_BLOCK_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<u2"), ("h", "<u2"),
+                           ("mv_x", "<i4"), ("mv_y", "<i4"), ("flags", "<u4"),
+                           ("reserved", "<u4"), ("out_offset", "<u8")], align=True)
+
+TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
+STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
+MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4
+CHROMA_400, CHROMA_420, CHROMA_422, CHROMA_444 = 0, 1, 2, 3
+
+OK, INVALID_INPUT, LIMIT_EXCEEDED, UNAVAILABLE, EXECUTION, TIMEOUT, MISMATCH = range(7)
+
+
+class AcceleratorError(RuntimeError):
+    """Base of the typed errors (reference AcceleratorError)."""
+
+    status = EXECUTION
+
+
+class Unavailable(AcceleratorError):
+    status = UNAVAILABLE
+
+
+class InvalidInput(AcceleratorError):
+    status = INVALID_INPUT
+
+
+class LimitExceeded(AcceleratorError):
+    status = LIMIT_EXCEEDED
+
+
+class Execution(AcceleratorError):
+    status = EXECUTION
+
+
+class Timeout(Execution):
+    status = TIMEOUT
+
+
+class Mismatch(Execution):
+    status = MISMATCH
+
+
+_ERRORS = {INVALID_INPUT: InvalidInput, LIMIT_EXCEEDED: LimitExceeded, UNAVAILABLE: Unavailable,
+           EXECUTION: Execution, TIMEOUT: Timeout, MISMATCH: Mismatch}
+
+
+class _Batch(C.Structure):
+    _fields_ = [("pics", C.c_void_p), ("num_pics", C.c_uint32), ("num_cus", C.c_uint32),
+                ("cus", C.c_void_p), ("levels", C.c_void_p), ("num_levels", C.c_uint64),
+                ("ctus", C.c_void_p), ("num_ctus", C.c_uint32), ("num_aps", C.c_uint32),
+                ("aps", C.c_void_p)]
+
+
+class _PlaneOut(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("stride", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _Config(C.Structure):
+    _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("reserve_bytes", C.c_uint64),
+                ("spin_limit", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize == 32
+assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40
+
+
+def build(force: bool = False) -> str:
+    """Compile csrc/vvcg.cu for sm_100a into lib/libvvcg.so (nvcc cross-compiles without a GPU)."""
+    srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    newest = max(os.path.getmtime(s) for s in srcs + [os.path.join(HERE, "..", "include", "vvcg.h")])
+    if not force and os.path.exists(LIB_PATH) and os.path.getmtime(LIB_PATH) >= newest:
+        return LIB_PATH
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = ["nvcc", *NVCC_FLAGS, "-o", LIB_PATH, os.path.join(CSRC, "vvcg.cu")]
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    """Load libvvcg.so (raises Unavailable when it was never built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise Unavailable(f"libvvcg.so is not built ({LIB_PATH}); run build()")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, u8 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint8
+        L.vvcg_ctx_create.argtypes = [vp, C.POINTER(vp)]
+        L.vvcg_ctx_destroy.argtypes = [vp]
+        L.vvcg_ctx_destroy.restype = None
+        L.vvcg_last_error.argtypes = [vp]
+        L.vvcg_last_error.restype = C.c_char_p
+        L.vvcg_set_stream.argtypes = [vp, vp]
+        L.vvcg_kernel_launches.argtypes = [vp]
+        L.vvcg_kernel_launches.restype = u64
+        for n in ("vvcg_batch_prepare", "vvcg_batch_upload"):
+            getattr(L, n).argtypes = [vp, vp]
+        L.vvcg_decode_batch.argtypes = [vp, vp, vp]
+        L.vvcg_batch_run.argtypes = [vp, u32]
+        L.vvcg_batch_sync.argtypes = [vp]
+        L.vvcg_batch_download.argtypes = [vp, vp]
+        L.vvcg_batch_plane.argtypes = [vp, u32, u32, C.POINTER(vp), C.POINTER(u32)]
+        L.vvcg_mc_luma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, vp, u32, vp]
+        L.vvcg_mc_chroma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, u8, vp, u32, vp]
+        L.vvcg_mc_bi_average_16_dev.argtypes = [vp, vp, vp, u64, u8, u8, vp]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def chroma_dims(w, h, cf):
+    if cf == CHROMA_400:
+        return 0, 0
+    sw = 2 if cf in (CHROMA_420, CHROMA_422) else 1
+    sh = 2 if cf == CHROMA_420 else 1
+    return (w + sw - 1) // sw, (h + sh - 1) // sh
+
+
+class Batch:
+    """Host-side records of a picture batch (the inputs of vvcg_batch)."""
+
+    def __init__(self, pics, cus, levels, ctus=None, aps=None):
+        self.pics = np.ascontiguousarray(pics, dtype=PIC_DTYPE)
+        self.cus = np.ascontiguousarray(cus, dtype=CU_DTYPE)
+        self.levels = levels if hasattr(levels, "data_ptr") else np.ascontiguousarray(levels, dtype=np.int16)
+        self.ctus = None if ctus is None else np.ascontiguousarray(ctus, dtype=CTU_DTYPE)
+        self.aps = None if aps is None else np.ascontiguousarray(aps, dtype=APS_DTYPE)
+
+    def as_struct(self):
+        nlev = self.levels.numel() if hasattr(self.levels, "numel") else self.levels.size
+        return _Batch(_ptr(self.pics), len(self.pics), len(self.cus), _ptr(self.cus),
+                      _ptr(self.levels), nlev,
+                      _ptr(self.ctus) if self.ctus is not None else None,
+                      0 if self.ctus is None else len(self.ctus),
+                      0 if self.aps is None else len(self.aps),
+                      _ptr(self.aps) if self.aps is not None else None)
+
+    def output_planes(self):
+        """Allocate visible-size output planes: list of (y, u, v) uint16 arrays."""
+        outs = []
+        for p in self.pics:
+            w, h, cf = int(p["visible_width"]), int(p["visible_height"]), int(p["chroma_format"])
+            cw, ch = chroma_dims(w, h, cf)
+            outs.append((np.zeros((h, w), np.uint16),
+                         np.zeros((ch, cw), np.uint16) if cf else None,
+                         np.zeros((ch, cw), np.uint16) if cf else None))
+        return outs
+
+
+class Context:
+    """One libvvcg context: a CUDA device, a stream and the device arena."""
+
+    def __init__(self, device: int = 0, spin_limit: int = 0, reserve_bytes: int = 0):
+        L = lib()
+        cfg = _Config(device, 0, reserve_bytes, spin_limit, 0)
+        h = C.c_void_p()
+        st = L.vvcg_ctx_create(C.byref(cfg), C.byref(h))
+        if st != OK:
+            raise _ERRORS.get(st, Execution)(f"vvcg_ctx_create failed with status {st}")
+        self._h = h
+        self._L = L
+        self._keep = None
+
+    def close(self):
+        if self._h:
+            self._L.vvcg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st):
+        if st != OK:
+            msg = self._L.vvcg_last_error(self._h).decode()
+            raise _ERRORS.get(st, Execution)(msg)
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self._L.vvcg_kernel_launches(self._h))
+
+    def set_stream(self, stream=None):
+        """Use a torch.cuda.Stream (or raw handle) for every launch; None = own stream."""
+        raw = None if stream is None else getattr(stream, "cuda_stream", stream)
+        self._check(self._L.vvcg_set_stream(self._h, C.c_void_p(raw) if raw else None))
+
+    # -- picture batches --
+    def decode_batch(self, batch: Batch, outs=None):
+        """Whole call with host buffers; returns [(y, u, v)] visible planes."""
+        outs = outs if outs is not None else batch.output_planes()
+        po = self._plane_outs(outs)
+        self._keep = (batch, outs, po)
+        self._check(self._L.vvcg_decode_batch(self._h, C.byref(batch.as_struct()), po))
+        return outs
+
+    def prepare(self, batch: Batch):
+        self._keep = batch
+        self._check(self._L.vvcg_batch_prepare(self._h, C.byref(batch.as_struct())))
+
+    def upload(self, batch: Batch):
+        self._check(self._L.vvcg_batch_upload(self._h, C.byref(batch.as_struct())))
+
+    def run(self, stages: int = STAGE_ALL):
+        self._check(self._L.vvcg_batch_run(self._h, stages))
+
+    def sync(self):
+        self._check(self._L.vvcg_batch_sync(self._h))
+
+    def download(self, outs):
+        po = self._plane_outs(outs)
+        self._check(self._L.vvcg_batch_download(self._h, po))
+        return outs
+
+    def plane(self, pic: int, comp: int):
+        p = C.c_void_p()
+        s = C.c_uint32()
+        self._check(self._L.vvcg_batch_plane(self._h, pic, comp, C.byref(p), C.byref(s)))
+        return p.value, s.value
+
+    @staticmethod
+    def _plane_outs(outs):
+        arr = (_PlaneOut * (3 * len(outs)))()
+        for i, planes in enumerate(outs):
+            for c in range(3):
+                a = planes[c]
+                if a is None:
+                    arr[i * 3 + c] = _PlaneOut(None, 0, 0)
+                else:
+                    stride = a.stride(0) if hasattr(a, "stride") and callable(a.stride) else a.strides[0] // 2
+                    arr[i * 3 + c] = _PlaneOut(_ptr(a), stride, 0)
+        return arr
+
+    # -- motion compensation (torch CUDA tensors) --
+    def mc_luma(self, ref, bit_depth, blocks, out):
+        """ref: (H, W) uint16-as-int16 CUDA tensor; blocks: CUDA uint8 tensor of MC_BLOCK_DTYPE bytes."""
+        h, w = ref.shape
+        n = blocks.numel() // MC_BLOCK_DTYPE.itemsize
+        self._check(self._L.vvcg_mc_luma_16_dev(self._h, _ptr(ref), w, h, ref.stride(0), bit_depth,
+                                                _ptr(blocks), n, _ptr(out)))
+
+    def mc_chroma(self, ref, bit_depth, chroma_format, blocks, out):
+        h, w = ref.shape
+        n = blocks.numel() // MC_BLOCK_DTYPE.itemsize
+        self._check(self._L.vvcg_mc_chroma_16_dev(self._h, _ptr(ref), w, h, ref.stride(0),
+                                                  bit_depth, chroma_format, _ptr(blocks), n,
+                                                  _ptr(out)))
+
+    def mc_bi_average(self, p0, p1, bcw_idx, bit_depth, out):
+        self._check(self._L.vvcg_mc_bi_average_16_dev(self._h, _ptr(p0), _ptr(p1), p0.numel(),
+                                                      bcw_idx, bit_depth, _ptr(out)))

@@ -1,0 +1,483 @@
+// In-loop filters of the frame path on 16-bit planes: deblocking (vertical
+// edges, then horizontal edges), SAO and ALF. Each follows the reference
+// function named beside it (crates/rustmpeg-video/src/vvc/filter.rs) and is
+// bit-identical to it. Edge segments of one direction never read samples that
+// another segment of the same direction writes (edges are at least 8 samples
+// apart and a segment writes at most 7 samples on each side, reading 8), so
+// each direction runs fully parallel and matches the reference's serial scan.
+#pragma once
+#include "vvcg_device.cuh"
+#include "vvcg_tables_dev.cuh"
+
+namespace vvcg {
+
+__device__ __forceinline__ int tc_for(int idx, int bd) {
+  return bd < 10 ? (c_dbf_tc[idx] + (1 << (9 - bd))) >> (10 - bd) : c_dbf_tc[idx] << (bd - 10);
+}
+
+struct LumaEdgeDec {
+  int de, len_p, len_q;
+  bool dep, deq;
+};
+
+#define LP(l, i) ((l)[7 - (i)])
+#define LQ(l, j) ((l)[8 + (j)])
+
+// filter.rs:282-305 luma_sample_decision
+__device__ __forceinline__ bool luma_sample_dec(int p0, int p3, int q0, int q3, int dpq, int sp,
+                                                int sq, int spq, bool lp, bool lq, int beta, int tc) {
+  if (lp) sp = (sp + abs(p3 - p0) + 1) >> 1;
+  if (lq) sq = (sq + abs(q3 - q0) + 1) >> 1;
+  int t1 = (lp || lq) ? (3 * beta) >> 5 : beta >> 3;
+  int t2 = (lp || lq) ? beta >> 4 : beta >> 2;
+  return dpq < t2 && sp + sq < t1 && spq < ((5 * tc + 1) >> 1);
+}
+
+// filter.rs:311-468 decide_luma_edge
+__device__ bool decide_luma(const int (*ln)[16], int beta, int tc, int lpi, int lqi, bool ctb_hor,
+                            LumaEdgeDec* e) {
+  const int* l0 = ln[0];
+  const int* l3 = ln[3];
+  int dp0 = abs(LP(l0, 2) - 2 * LP(l0, 1) + LP(l0, 0)), dp3 = abs(LP(l3, 2) - 2 * LP(l3, 1) + LP(l3, 0));
+  int dq0 = abs(LQ(l0, 2) - 2 * LQ(l0, 1) + LQ(l0, 0)), dq3 = abs(LQ(l3, 2) - 2 * LQ(l3, 1) + LQ(l3, 0));
+  int dpq0 = dp0 + dq0, dpq3 = dp3 + dq3;
+  int sp0 = abs(LP(l0, 3) - LP(l0, 0)), sp3 = abs(LP(l3, 3) - LP(l3, 0));
+  int sq0 = abs(LQ(l0, 0) - LQ(l0, 3)), sq3 = abs(LQ(l3, 0) - LQ(l3, 3));
+  int spq0 = abs(LP(l0, 0) - LQ(l0, 0)), spq3 = abs(LP(l3, 0) - LQ(l3, 0));
+  int len_p = clampi(lpi, 1, 7), len_q = clampi(lqi, 1, 7);
+  bool lp = len_p > 3 && !ctb_hor, lq = len_q > 3;
+  if (lp || lq) {
+    int dp0l = lp ? (dp0 + abs(LP(l0, 5) - 2 * LP(l0, 4) + LP(l0, 3)) + 1) >> 1 : dp0;
+    int dp3l = lp ? (dp3 + abs(LP(l3, 5) - 2 * LP(l3, 4) + LP(l3, 3)) + 1) >> 1 : dp3;
+    int dq0l = lq ? (dq0 + abs(LQ(l0, 5) - 2 * LQ(l0, 4) + LQ(l0, 3)) + 1) >> 1 : dq0;
+    int dq3l = lq ? (dq3 + abs(LQ(l3, 5) - 2 * LQ(l3, 4) + LQ(l3, 3)) + 1) >> 1 : dq3;
+    if (!lp) len_p = 3;
+    if (!lq) len_q = 3;
+    int sp0l = len_p == 7 ? sp0 + abs(LP(l0, 7) - LP(l0, 6) - LP(l0, 5) + LP(l0, 4)) : sp0;
+    int sp3l = len_p == 7 ? sp3 + abs(LP(l3, 7) - LP(l3, 6) - LP(l3, 5) + LP(l3, 4)) : sp3;
+    int sq0l = len_q == 7 ? sq0 + abs(LQ(l0, 4) - LQ(l0, 5) - LQ(l0, 6) + LQ(l0, 7)) : sq0;
+    int sq3l = len_q == 7 ? sq3 + abs(LQ(l3, 4) - LQ(l3, 5) - LQ(l3, 6) + LQ(l3, 7)) : sq3;
+    int d0l = dp0l + dq0l, d3l = dp3l + dq3l;
+    if (d0l + d3l < beta) {
+      bool s0 = luma_sample_dec(lp ? LP(l0, len_p) : 0, lp ? LP(l0, 3) : 0, lq ? LQ(l0, len_q) : 0,
+                                lq ? LQ(l0, 3) : 0, 2 * d0l, sp0l, sq0l, spq0, lp, lq, beta, tc);
+      bool s3 = luma_sample_dec(lp ? LP(l3, len_p) : 0, lp ? LP(l3, 3) : 0, lq ? LQ(l3, len_q) : 0,
+                                lq ? LQ(l3, 3) : 0, 2 * d3l, sp3l, sq3l, spq3, lp, lq, beta, tc);
+      if (s0 && s3) {
+        *e = LumaEdgeDec{3, len_p, len_q, true, true};
+        return true;
+      }
+    }
+  }
+  int dp = dp0 + dp3, dq = dq0 + dq3;
+  if (dpq0 + dpq3 >= beta) return false;
+  bool s0 = false, s3 = false;
+  if (len_p > 2 && len_q > 2) {
+    s0 = luma_sample_dec(0, 0, 0, 0, 2 * dpq0, sp0, sq0, spq0, false, false, beta, tc);
+    s3 = luma_sample_dec(0, 0, 0, 0, 2 * dpq3, sp3, sq3, spq3, false, false, beta, tc);
+  }
+  int de = 1;
+  if (s0 && s3) {
+    de = 2;
+    len_p = 3;
+    len_q = 3;
+  }
+  int thr = (beta + (beta >> 1)) >> 3;
+  bool dep = len_p > 1 && len_q > 1 && dp < thr;
+  bool deq = len_p > 1 && len_q > 1 && dq < thr;
+  if (de == 1) {
+    len_p = 1 + (dep ? 1 : 0);
+    len_q = 1 + (deq ? 1 : 0);
+  }
+  *e = LumaEdgeDec{de, len_p, len_q, dep, deq};
+  return true;
+}
+
+// filter.rs:477-582 long_tap_luma_line (in place on a 16-sample line)
+__device__ void long_tap_line(int* l, int np, int nq, int tc, int maxv) {
+  int m[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) m[i] = l[i];
+#define MP(i) m[7 - (i)]
+#define MQ(j) m[8 + (j)]
+  int rm;
+  if (np == 5 && nq == 5)
+    rm = (2 * (MP(0) + MQ(0) + MP(1) + MQ(1) + MP(2) + MQ(2)) + MP(3) + MQ(3) + MP(4) + MQ(4) + 8) >> 4;
+  else if ((np == 7 && nq == 5) || (np == 5 && nq == 7))
+    rm = (2 * (MP(0) + MQ(0) + MP(1) + MQ(1)) + MP(2) + MQ(2) + MP(3) + MQ(3) + MP(4) + MQ(4) +
+          MP(5) + MQ(5) + 8) >> 4;
+  else if ((np == 5 && nq == 3) || (np == 3 && nq == 5))
+    rm = (MP(0) + MQ(0) + MP(1) + MQ(1) + MP(2) + MQ(2) + MP(3) + MQ(3) + 4) >> 3;
+  else if (np == 7 && nq == 3)
+    rm = (2 * (MP(0) + MQ(0)) + MQ(0) + 2 * (MQ(1) + MQ(2)) + MP(1) + MQ(1) + MP(2) + MP(3) + MP(4) +
+          MP(5) + MP(6) + 8) >> 4;
+  else if (np == 3 && nq == 7)
+    rm = (2 * (MP(0) + MQ(0)) + MP(0) + 2 * (MP(1) + MP(2)) + MP(1) + MQ(1) + MQ(2) + MQ(3) + MQ(4) +
+          MQ(5) + MQ(6) + 8) >> 4;
+  else
+    rm = (2 * (MP(0) + MQ(0)) + MP(1) + MQ(1) + MP(2) + MQ(2) + MP(3) + MQ(3) + MP(4) + MQ(4) +
+          MP(5) + MQ(5) + MP(6) + MQ(6) + 8) >> 4;
+  const int ref_p = (MP(np) + MP(np - 1) + 1) >> 1;
+  const int ref_q = (MQ(nq) + MQ(nq - 1) + 1) >> 1;
+  const int c7[7] = {59, 50, 41, 32, 23, 14, 5}, t7[7] = {6, 5, 4, 3, 2, 1, 1};
+  const int c5[5] = {58, 45, 32, 19, 6}, t5[5] = {6, 5, 4, 3, 2};
+  const int c3[3] = {53, 32, 11}, t3[3] = {6, 4, 2};
+  for (int pos = 0; pos < np; pos++) {
+    int f = np == 7 ? c7[pos] : (np == 5 ? c5[pos] : c3[pos]);
+    int t = np == 7 ? t7[pos] : (np == 5 ? t5[pos] : t3[pos]);
+    int o = MP(pos), cv = (tc * t) >> 1;
+    int it = (rm * f + ref_p * (64 - f) + 32) >> 6;
+    l[7 - pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
+  }
+  for (int pos = 0; pos < nq; pos++) {
+    int f = nq == 7 ? c7[pos] : (nq == 5 ? c5[pos] : c3[pos]);
+    int t = nq == 7 ? t7[pos] : (nq == 5 ? t5[pos] : t3[pos]);
+    int o = MQ(pos), cv = (tc * t) >> 1;
+    int it = (rm * f + ref_q * (64 - f) + 32) >> 6;
+    l[8 + pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
+  }
+#undef MP
+#undef MQ
+}
+
+// filter.rs:586-631 short_filter_luma_line
+__device__ void short_line(int* l, const LumaEdgeDec& e, int tc, int maxv) {
+  int m[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) m[i] = l[i];
+  if (e.de == 2) {
+    l[7] = clampi((LP(m, 2) + 2 * LP(m, 1) + 2 * LP(m, 0) + 2 * LQ(m, 0) + LQ(m, 1) + 4) >> 3,
+                  LP(m, 0) - 3 * tc, LP(m, 0) + 3 * tc);
+    l[6] = clampi((LP(m, 2) + LP(m, 1) + LP(m, 0) + LQ(m, 0) + 2) >> 2, LP(m, 1) - 2 * tc,
+                  LP(m, 1) + 2 * tc);
+    l[5] = clampi((2 * LP(m, 3) + 3 * LP(m, 2) + LP(m, 1) + LP(m, 0) + LQ(m, 0) + 4) >> 3,
+                  LP(m, 2) - tc, LP(m, 2) + tc);
+    l[8] = clampi((LP(m, 1) + 2 * LP(m, 0) + 2 * LQ(m, 0) + 2 * LQ(m, 1) + LQ(m, 2) + 4) >> 3,
+                  LQ(m, 0) - 3 * tc, LQ(m, 0) + 3 * tc);
+    l[9] = clampi((LP(m, 0) + LQ(m, 0) + LQ(m, 1) + LQ(m, 2) + 2) >> 2, LQ(m, 1) - 2 * tc,
+                  LQ(m, 1) + 2 * tc);
+    l[10] = clampi((LP(m, 0) + LQ(m, 0) + LQ(m, 1) + 3 * LQ(m, 2) + 2 * LQ(m, 3) + 4) >> 3,
+                   LQ(m, 2) - tc, LQ(m, 2) + tc);
+    return;
+  }
+  int delta = (9 * (LQ(m, 0) - LP(m, 0)) - 3 * (LQ(m, 1) - LP(m, 1)) + 8) >> 4;
+  if (abs(delta) >= tc * 10) return;
+  delta = clampi(delta, -tc, tc);
+  l[7] = clampi(LP(m, 0) + delta, 0, maxv);
+  l[8] = clampi(LQ(m, 0) - delta, 0, maxv);
+  int tc2 = tc >> 1;
+  if (e.dep) {
+    int d = clampi((((LP(m, 2) + LP(m, 0) + 1) >> 1) - LP(m, 1) + delta) >> 1, -tc2, tc2);
+    l[6] = clampi(LP(m, 1) + d, 0, maxv);
+  }
+  if (e.deq) {
+    int d = clampi((((LQ(m, 2) + LQ(m, 0) + 1) >> 1) - LQ(m, 1) - delta) >> 1, -tc2, tc2);
+    l[9] = clampi(LQ(m, 1) + d, 0, maxv);
+  }
+}
+
+// Picture-level parameters of one deblocking pass over one plane.
+struct DbfPass {
+  uint16_t* plane;
+  int32_t stride, w, h, bd;
+  int32_t step, ctb, qp, bs, beta_off, tc_off;
+  int32_t len_p, len_q;  // luma: max filter length; chroma: lengths from the lattice
+  int32_t sub;           // chroma: SubHeightC (vertical pass) / SubWidthC (horizontal pass)
+  int32_t n_edges, n_segs;
+};
+
+// deblock_luma_edge_bd (filter.rs:638-679) on the segment's 4 lines;
+// vertical edges (filter.rs:2360-2390) or horizontal edges (:2392-2425) of
+// deblock_luma_plane_16. One thread per 4-line segment.
+template <bool kVertical>
+__global__ void k_deblock_luma(const DbfPass* __restrict__ passes, int n_pass) {
+  const DbfPass& D = passes[blockIdx.y];
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= D.n_edges * D.n_segs) return;
+  int e = idx / D.n_segs, s = idx % D.n_segs;
+  int pos = D.step * (e + 1);  // edge x (vertical) or y (horizontal)
+  int seg = s * 4;
+  int bd = D.bd, maxv = (1 << bd) - 1;
+  int qp = D.qp;
+  int idx_tc = clampi(qp + 2 * (D.bs - 1) + 2 * D.tc_off, 0, 65);
+  int idx_b = clampi(qp + 2 * D.beta_off, 0, 63);
+  int tc = tc_for(idx_tc, bd);
+  int beta = c_dbf_beta[idx_b] << (bd - 8);
+  if (D.bs == 0 || beta == 0 || tc == 0) return;
+  int ln[4][16];
+  uint16_t* pl = D.plane;
+  const int st = D.stride;
+  for (int k = 0; k < 4; k++)
+    for (int i = 0; i < 16; i++)
+      ln[k][i] = kVertical ? pl[(size_t)(seg + k) * st + pos - 8 + i] : pl[(size_t)(pos - 8 + i) * st + seg + k];
+  bool ctb_hor = !kVertical && (pos % D.ctb) == 0;
+  LumaEdgeDec dec;
+  if (!decide_luma(ln, beta, tc, D.len_p, D.len_q, ctb_hor, &dec)) return;
+  for (int k = 0; k < 4; k++) {
+    if (dec.de == 3)
+      long_tap_line(ln[k], dec.len_p, dec.len_q, tc, maxv);
+    else
+      short_line(ln[k], dec, tc, maxv);
+  }
+  for (int k = 0; k < 4; k++)
+    for (int i = 1; i < 15; i++) {
+      uint16_t v = (uint16_t)clampi(ln[k][i], 0, maxv);
+      if (kVertical)
+        pl[(size_t)(seg + k) * st + pos - 8 + i] = v;
+      else
+        pl[(size_t)(pos - 8 + i) * st + seg + k] = v;
+    }
+}
+
+// filter.rs:907-919 chroma_sample_decision
+__device__ __forceinline__ bool chroma_dec(int p0, int p3, int q0, int q3, int dpq, int beta, int tc) {
+  return dpq < (beta >> 2) && abs(p3 - p0) + abs(q0 - q3) < (beta >> 3) &&
+         abs(p0 - q0) < ((5 * tc + 1) >> 1);
+}
+
+// deblock_chroma_edge (filter.rs:935-1007) + the strong / p1q3 / weak line
+// filters (:1010-1057), driven as in deblock_chroma_plane_16 (:2433-2527).
+// One thread per 2- or 4-line group.
+template <bool kVertical>
+__global__ void k_deblock_chroma(const DbfPass* __restrict__ passes, int n_pass) {
+  const DbfPass& D = passes[blockIdx.y];
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= D.n_edges * D.n_segs) return;
+  const int e = idx / D.n_segs, s = idx % D.n_segs;
+  const int pos = D.step * (e + 1);
+  const int group = D.sub == 1 ? 4 : 2;
+  const int seg = s * group;
+  const int bd = D.bd, maxv = (1 << bd) - 1;
+  if (D.bs == 0) return;
+  int len_p = min(D.len_p, 3), len_q = min(D.len_q, 3);
+  if (!kVertical && (pos % D.ctb) == 0) len_p = 1;  // upper chroma CTB boundary
+  if (len_p == 1 && len_q == 1 && D.bs != 2) return;
+  int idx_tc = clampi(D.qp + 2 * (D.bs - 1) + 2 * D.tc_off, 0, 65);
+  int idx_b = clampi(D.qp + 2 * D.beta_off, 0, 63);
+  int tc = tc_for(idx_tc, bd);
+  int beta = c_dbf_beta[idx_b] << (bd - 8);
+  int ln[4][8];
+  uint16_t* pl = D.plane;
+  const int st = D.stride;
+  for (int k = 0; k < group; k++)
+    for (int i = 0; i < 8; i++)
+      ln[k][i] = kVertical ? pl[(size_t)(seg + k) * st + pos - 4 + i] : pl[(size_t)(pos - 4 + i) * st + seg + k];
+  if (len_q == 3) {
+    int a[8], b[8];
+    for (int i = 0; i < 8; i++) {
+      a[i] = ln[0][i];
+      b[i] = ln[group - 1][i];
+    }
+    if (len_p == 1) {
+      a[0] = a[1] = a[2];
+      b[0] = b[1] = b[2];
+    }
+    int dp0 = abs(a[1] - 2 * a[2] + a[3]), dp1 = abs(b[1] - 2 * b[2] + b[3]);
+    int dq0 = abs(a[6] - 2 * a[5] + a[4]), dq1 = abs(b[6] - 2 * b[5] + b[4]);
+    int dpq0 = dp0 + dq0, dpq1 = dp1 + dq1;
+    bool strong = (dpq0 + dpq1) < beta && chroma_dec(a[3], a[0], a[4], a[7], 2 * dpq0, beta, tc) &&
+                  chroma_dec(b[3], b[0], b[4], b[7], 2 * dpq1, beta, tc);
+    if (!strong) {
+      len_p = 1;
+      len_q = 1;
+    }
+  }
+  for (int k = 0; k < group; k++) {
+    int* l = ln[k];
+    int m[8];
+    for (int i = 0; i < 8; i++) m[i] = l[i];
+    auto cl = [&](int o, int v) { return clampi(clampi(v, o - tc, o + tc), 0, maxv); };
+    if (len_p == 3 && len_q == 3) {
+      l[1] = cl(m[1], (3 * m[0] + 2 * m[1] + m[2] + m[3] + m[4] + 4) >> 3);
+      l[2] = cl(m[2], (2 * m[0] + m[1] + 2 * m[2] + m[3] + m[4] + m[5] + 4) >> 3);
+      l[3] = cl(m[3], (m[0] + m[1] + m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
+      l[4] = cl(m[4], (m[1] + m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
+      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
+      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
+    } else if (len_p == 1 && len_q == 3) {
+      l[3] = cl(m[3], (3 * m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
+      l[4] = cl(m[4], (2 * m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
+      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
+      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
+    } else {
+      int delta = clampi((4 * (m[4] - m[3]) + m[2] - m[5] + 4) >> 3, -tc, tc);
+      l[3] = clampi(m[3] + delta, 0, maxv);
+      l[4] = clampi(m[4] - delta, 0, maxv);
+    }
+  }
+  for (int k = 0; k < group; k++)
+    for (int i = 1; i < 7; i++) {
+      uint16_t v = (uint16_t)clampi(ln[k][i], 0, maxv);
+      if (kVertical)
+        pl[(size_t)(seg + k) * st + pos - 4 + i] = v;
+      else
+        pl[(size_t)(pos - 4 + i) * st + seg + k] = v;
+    }
+}
+
+// One SAO pass over one plane of one picture.
+struct SaoPass {
+  const uint16_t* src;
+  uint16_t* dst;
+  const vvcg_ctu_filter* ctus;
+  int32_t stride, w, h, bd, comp;
+  int32_t ctu_w_s, ctu_h_s;  // CTU size in this plane's samples
+  int32_t ctu_cols;          // CTUs per row
+};
+
+// apply_sao_region_16 (filter.rs:1880-1947), every sample of the plane; the
+// CTU containing a sample supplies its parameters and unmodified samples are
+// copied (the reference filters a copy in place).
+__global__ void k_sao(const SaoPass* __restrict__ passes) {
+  const SaoPass& S = passes[blockIdx.y];
+  const int x = (blockIdx.x % ((S.w + 63) / 64)) * 64 + (threadIdx.x & 63);
+  const int y = (blockIdx.x / ((S.w + 63) / 64)) * 4 + (threadIdx.x >> 6);
+  if (x >= S.w || y >= S.h) return;
+  const int st = S.stride;
+  const int c = S.src[(size_t)y * st + x];
+  const vvcg_sao sp = S.ctus[(y / S.ctu_h_s) * S.ctu_cols + x / S.ctu_w_s].sao[S.comp];
+  const int maxv = (1 << S.bd) - 1;
+  int out = c;
+  if (sp.type == 1) {
+    int band = ((uint8_t)((uint8_t)(c >> (S.bd - 5)) - sp.band_or_class)) & 31;
+    if (band < 4) out = clampi(c + sp.offsets[band], 0, maxv);
+  } else if (sp.type == 2) {
+    int dx, dy;
+    switch (sp.band_or_class & 3) {
+      case 0: dx = 1; dy = 0; break;
+      case 1: dx = 0; dy = 1; break;
+      case 2: dx = 1; dy = 1; break;
+      default: dx = 1; dy = -1; break;
+    }
+    if (!(x - dx < 0 || x + dx >= S.w || y - dy < 0 || y + dy >= S.h)) {
+      int a = S.src[(size_t)(y - dy) * st + x - dx];
+      int b = S.src[(size_t)(y + dy) * st + x + dx];
+      int ei = 2 + ((c > a) - (c < a)) + ((c > b) - (c < b));
+      int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2] : ei == 4 ? sp.offsets[3] : 0;
+      out = clampi(c + off, 0, maxv);
+    }
+  }
+  S.dst[(size_t)y * st + x] = (uint16_t)out;
+}
+
+// One luma ALF pass (whole plane, apply_alf_luma_plane_16 of filter.rs:2045-2124).
+struct AlfPass {
+  const uint16_t* src;
+  uint16_t* dst;
+  const vvcg_alf_aps* aps;  // NULL = fixed filter of each class
+  int32_t stride, w, h, bd;
+};
+
+constexpr int kAlfTw = 64, kAlfTh = 16, kAlfHalo = 4;
+
+// Tile of 64x16 outputs: the tile plus a 4-sample halo (coordinates clamped
+// to the plane, as the reference's get_p does) is staged in shared memory;
+// each 4x4 block is classified (classify_alf_4x4_16, filter.rs:2126-2182)
+// and filtered with the 7x7 diamond.
+__global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
+  const AlfPass& A = passes[blockIdx.z];
+  __shared__ uint16_t t[kAlfTh + 2 * kAlfHalo][kAlfTw + 2 * kAlfHalo];
+  __shared__ int8_t s_cls[kAlfTh / 4][kAlfTw / 4];
+  __shared__ int8_t s_tr[kAlfTh / 4][kAlfTw / 4];
+  const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
+  if (x0 >= A.w || y0 >= A.h) return;
+  const int W = kAlfTw + 2 * kAlfHalo, H = kAlfTh + 2 * kAlfHalo;
+  for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
+    int ty = i / W, tx = i % W;
+    int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
+    t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
+  }
+  __syncthreads();
+  auto g = [&](int x, int y) -> int {  // plane coordinates, clamped
+    x = clampi(x, 0, A.w - 1);
+    y = clampi(y, 0, A.h - 1);
+    return t[y - y0 + kAlfHalo][x - x0 + kAlfHalo];
+  };
+  if (threadIdx.x < (kAlfTw / 4) * (kAlfTh / 4)) {
+    int bxi = threadIdx.x % (kAlfTw / 4), byi = threadIdx.x / (kAlfTw / 4);
+    int bx = x0 + bxi * 4, by = y0 + byi * 4;
+    int cls = 0, tr = 0;
+    if (bx < A.w && by < A.h) {
+      const int TH[16] = {0, 1, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 4};
+      int sh = 0, sv = 0, d0 = 0, d1 = 0;
+      for (int dy = 0; dy <= 4; dy += 2)
+        for (int dx = 0; dx <= 4; dx += 2) {
+          int x = bx + dx, y = by + dy;
+          int c2 = g(x, y) << 1;
+          sh += abs(c2 - g(x - 1, y) - g(x + 1, y));
+          sv += abs(c2 - g(x, y - 1) - g(x, y + 1));
+          d0 += abs(c2 - g(x - 1, y - 1) - g(x + 1, y + 1));
+          d1 += abs(c2 - g(x + 1, y - 1) - g(x - 1, y + 1));
+        }
+      long long act = ((long long)(sh + sv) * 64) >> (A.bd + 4);
+      int q_act = TH[(int)(act < 0 ? 0 : (act > 15 ? 15 : act))];
+      int hv1, hv0, dhv, dd1, dd0, ddd;
+      if (sv > sh) { hv1 = sv; hv0 = sh; dhv = 1; } else { hv1 = sh; hv0 = sv; dhv = 3; }
+      if (d0 > d1) { dd1 = d0; dd0 = d1; ddd = 0; } else { dd1 = d1; dd0 = d0; ddd = 2; }
+      int h1, h0, mdir, sdir;
+      if ((long long)dd1 * hv0 > (long long)hv1 * dd0) { h1 = dd1; h0 = dd0; mdir = ddd; sdir = dhv; }
+      else { h1 = hv1; h0 = hv0; mdir = dhv; sdir = ddd; }
+      int ds = 0;
+      if (h1 > 2 * h0) ds = (h1 * 2 > 9 * h0) ? 2 : 1;
+      const int TT[8] = {0, 1, 0, 2, 2, 3, 1, 3};
+      tr = TT[mdir * 2 + (sdir >> 1)];
+      cls = q_act;
+      if (ds) cls += (((mdir & 1) << 1) + ds - 1 + 1) * 5;
+      cls = min(cls, 24);
+    }
+    s_cls[byi][bxi] = (int8_t)cls;
+    s_tr[byi][bxi] = (int8_t)tr;
+  }
+  __syncthreads();
+  const int* ct = A.bd >= 12 ? c_alf_clip[2] : (A.bd >= 10 ? c_alf_clip[1] : c_alf_clip[0]);
+  const int maxv = (1 << A.bd) - 1;
+  for (int i = threadIdx.x; i < kAlfTw * kAlfTh; i += blockDim.x) {
+    int lx = i % kAlfTw, lyy = i / kAlfTw;
+    int x = x0 + lx, y = y0 + lyy;
+    if (x >= A.w || y >= A.h) continue;
+    int cls = s_cls[lyy >> 2][lx >> 2], tr = s_tr[lyy >> 2][lx >> 2];
+    int base_c[12], base_clip[12];
+    int filt = 0;
+    if (A.aps && A.aps->num_luma_filters > 0) {
+      filt = min((int)A.aps->coeff_delta_idx[cls], (int)A.aps->num_luma_filters - 1);
+      for (int k = 0; k < 12; k++) base_c[k] = A.aps->coeff[filt][k];
+    } else {
+      if (cls >= 16) {  // the reference indexes a [16][25] table by class and aborts
+        atomicOr(status, kStatusAlfAbort);
+        A.dst[(size_t)y * A.stride + x] = (uint16_t)g(x, y);
+        continue;
+      }
+      int fixed = c_alf_class_to_filter[cls * 25];
+      for (int k = 0; k < 12; k++) base_c[k] = c_alf_fixed[fixed * 13 + k];
+    }
+    bool use_clip = A.aps && A.aps->luma_clip && filt < (int)A.aps->num_luma_filters;
+    for (int k = 0; k < 12; k++) base_clip[k] = use_clip ? A.aps->clip_idx[filt][k] : 0;
+    int fc[12], fcl[12];
+    for (int k = 0; k < 12; k++) {
+      int p = c_alf_transpose_perm[(tr & 3) * 12 + k];
+      fc[k] = base_c[p];
+      fcl[k] = ct[base_clip[p] & 3];
+    }
+    const int c = g(x, y);
+    auto ca = [&](int cv, int p0, int p1) { return clampi(p0 - c, -cv, cv) + clampi(p1 - c, -cv, cv); };
+    int s = 0;
+    s += fc[0] * ca(fcl[0], g(x, y + 3), g(x, y - 3));
+    s += fc[1] * ca(fcl[1], g(x + 1, y + 2), g(x - 1, y - 2));
+    s += fc[2] * ca(fcl[2], g(x, y + 2), g(x, y - 2));
+    s += fc[3] * ca(fcl[3], g(x - 1, y + 2), g(x + 1, y - 2));
+    s += fc[4] * ca(fcl[4], g(x + 2, y + 1), g(x - 2, y - 1));
+    s += fc[5] * ca(fcl[5], g(x + 1, y + 1), g(x - 1, y - 1));
+    s += fc[6] * ca(fcl[6], g(x, y + 1), g(x, y - 1));
+    s += fc[7] * ca(fcl[7], g(x - 1, y + 1), g(x + 1, y - 1));
+    s += fc[8] * ca(fcl[8], g(x - 2, y + 1), g(x + 2, y - 1));
+    s += fc[9] * ca(fcl[9], g(x + 3, y), g(x - 3, y));
+    s += fc[10] * ca(fcl[10], g(x + 2, y), g(x - 2, y));
+    s += fc[11] * ca(fcl[11], g(x + 1, y), g(x - 1, y));
+    A.dst[(size_t)y * A.stride + x] = (uint16_t)clampi(c + ((s + 64) >> 7), 0, maxv);
+  }
+}
+
+#undef LP
+#undef LQ
+
+}  // namespace vvcg

@@ -1,0 +1,670 @@
+// libvvcg: C ABI of the B200 VVC reconstruction / loop-filter / MC library.
+// One translation unit: the kernels live in the included .cuh headers.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/vvcg.h"
+#include "filters.cuh"
+#include "mc.cuh"
+#include "recon.cuh"
+#include "vvc_tables.h"
+#include "vvcg_device.cuh"
+#include "vvcg_tables_dev.cuh"
+
+using namespace vvcg;
+
+namespace {
+
+// Picture size limit of the reference (mod.rs:91 MAX_LUMA_SAMPLES).
+constexpr uint64_t kMaxLumaSamples = 35651584ull;
+constexpr uint32_t kDefaultSpinLimit = 1u << 22;  // ~0.5-1 s of polling
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(bytes, (size_t)256);
+    want += want / 4;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct PicLayout {
+  uint64_t plane_off[3], scratch_off[3];  // in samples within the plane arena
+  int32_t stride[3], pw[3], ph[3];
+  int final_in_scratch[3];
+  int vis_w[3], vis_h[3];
+};
+
+}  // namespace
+
+struct vvcg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  std::string err;
+  uint64_t launches = 0;
+  uint32_t spin_limit = kDefaultSpinLimit;
+  uint32_t epoch = 0;
+  int num_sms = 0;
+  int recon_ctas_per_sm = 0;
+  size_t recon_smem = 0;
+  // batch state
+  bool prepared = false;
+  uint32_t num_pics = 0;
+  std::vector<PicLayout> layout;
+  std::vector<DevPic> pics;
+  std::vector<CtuItem> items;
+  std::vector<DbfPass> dbf[4];  // luma V, luma H, chroma V, chroma H
+  std::vector<SaoPass> sao;
+  std::vector<AlfPass> alf;
+  uint64_t num_cus = 0, num_levels = 0, num_ctus = 0, num_aps = 0;
+  // device memory
+  DevBuf planes, flags, d_pics, d_items, d_dbf[4], d_sao, d_alf, d_cus, d_levels, d_ctus, d_aps,
+      d_ctrl;  // d_ctrl: [0] queue counter, [1] status word
+  uint64_t flags_count = 0;
+};
+
+namespace {
+
+std::mutex g_tables_mu;
+bool g_tables_ready[64] = {false};
+
+vvcg_status fail(vvcg_ctx* ctx, vvcg_status st, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return st;
+}
+
+vvcg_status cuda_fail(vvcg_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, VVCG_EXECUTION, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call, what)                                   \
+  do {                                                   \
+    cudaError_t _e = (call);                             \
+    if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); \
+  } while (0)
+
+// Grouped diagonal scan of a w x h TB (VTM ScanGenerator DIAG over 4x4-style
+// coefficient groups sized by g_log2TxSubblockSize, H.266 6.5.3-6.5.4),
+// raster index per scan position, capped to the top-left 32x32.
+int build_scan(int w, int h, int16_t* out) {
+  static const uint8_t T[8][8][2] = {
+      {{0, 0}, {0, 1}, {0, 2}, {0, 3}, {0, 4}, {0, 4}, {0, 4}, {0, 4}},
+      {{1, 0}, {1, 1}, {1, 1}, {1, 3}, {1, 3}, {1, 3}, {1, 3}, {1, 3}},
+      {{2, 0}, {1, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+      {{3, 0}, {3, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+      {{4, 0}, {3, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+      {{4, 0}, {3, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+      {{4, 0}, {3, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+      {{4, 0}, {3, 1}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}, {2, 2}},
+  };
+  int a = std::min(7, __builtin_ctz(w)), b = std::min(7, __builtin_ctz(h));
+  int cgw = 1 << T[a][b][0], cgh = 1 << T[a][b][1];
+  int gw = std::min(w, 32) / cgw, gh = std::min(h, 32) / cgh;
+  auto diag = [](int W, int H, std::vector<std::pair<int, int>>& o) {
+    o.clear();
+    int line = 0, col = 0;
+    for (int i = 0; i < W * H; i++) {
+      o.push_back({col, line});
+      if (col == W - 1 || line == 0) {
+        line += col + 1;
+        col = 0;
+        if (line >= H) {
+          col += line - (H - 1);
+          line = H - 1;
+        }
+      } else {
+        col++;
+        line--;
+      }
+    }
+  };
+  std::vector<std::pair<int, int>> g, in;
+  diag(gw, gh, g);
+  diag(cgw, cgh, in);
+  int k = 0;
+  for (auto& G : g)
+    for (auto& I : in) out[k++] = (int16_t)((G.second * cgh + I.second) * w + G.first * cgw + I.first);
+  return k;
+}
+
+vvcg_status upload_tables(vvcg_ctx* ctx) {
+  std::lock_guard<std::mutex> lk(g_tables_mu);
+  if (ctx->device < 64 && g_tables_ready[ctx->device]) return VVCG_OK;
+  using namespace vvc_tables;
+  int ang[32], inv[32], thr[8];
+  for (int i = 0; i < 32; i++) {
+    ang[i] = kAngTable[i];
+    inv[i] = kInvAngTable[i];
+  }
+  for (int i = 0; i < 8; i++) thr[i] = kIntraFilterThreshold[i];
+  CK(cudaMemcpyToSymbol(c_ang_table, ang, sizeof(ang)), "tables");
+  CK(cudaMemcpyToSymbol(c_inv_ang_table, inv, sizeof(inv)), "tables");
+  CK(cudaMemcpyToSymbol(c_intra_filter_thr, thr, sizeof(thr)), "tables");
+  CK(cudaMemcpyToSymbol(c_chroma_taps4, kChromaTaps4, sizeof(kChromaTaps4)), "tables");
+  CK(cudaMemcpyToSymbol(c_cclm_div_sig, kCclmDivSig, sizeof(kCclmDivSig)), "tables");
+  CK(cudaMemcpyToSymbol(c_inv_quant_scale, kInvQuantScale, sizeof(kInvQuantScale)), "tables");
+  CK(cudaMemcpyToSymbol(c_quant_scale, kQuantScale, sizeof(kQuantScale)), "tables");
+  CK(cudaMemcpyToSymbol(c_dbf_tc, kDbfTc, sizeof(kDbfTc)), "tables");
+  CK(cudaMemcpyToSymbol(c_dbf_beta, kDbfBeta, sizeof(kDbfBeta)), "tables");
+  CK(cudaMemcpyToSymbol(c_luma_taps8, kLumaTaps8, sizeof(kLumaTaps8)), "tables");
+  CK(cudaMemcpyToSymbol(c_affine_taps8, kAffineTaps8, sizeof(kAffineTaps8)), "tables");
+  CK(cudaMemcpyToSymbol(c_luma_alt_hpel, kLumaAltHpel, sizeof(kLumaAltHpel)), "tables");
+  CK(cudaMemcpyToSymbol(c_bcw_weights, kBcwWeights, sizeof(kBcwWeights)), "tables");
+  CK(cudaMemcpyToSymbol(c_alf_clip, kAlfClip, sizeof(kAlfClip)), "tables");
+  CK(cudaMemcpyToSymbol(c_alf_fixed, kAlfFixedCoeff, sizeof(kAlfFixedCoeff)), "tables");
+  CK(cudaMemcpyToSymbol(c_alf_class_to_filter, kAlfClassToFilter, sizeof(kAlfClassToFilter)), "tables");
+  CK(cudaMemcpyToSymbol(c_alf_transpose_perm, kAlfTransposePerm, sizeof(kAlfTransposePerm)), "tables");
+  static const int8_t* d2[6] = {kDct2N2, kDct2N4, kDct2N8, kDct2N16, kDct2N32, kDct2N64};
+  for (int i = 0; i < 6; i++) {
+    int n = 2 << i;
+    CK(cudaMemcpyToSymbol(g_dct2_m, d2[i], n * n, (size_t)i * 64 * 64), "tables");
+  }
+  static const int8_t* s7[4] = {kDst7N4, kDst7N8, kDst7N16, kDst7N32};
+  static const int8_t* c8[4] = {kDct8N4, kDct8N8, kDct8N16, kDct8N32};
+  for (int i = 0; i < 4; i++) {
+    int n = 4 << i;
+    CK(cudaMemcpyToSymbol(g_dst7_m, s7[i], n * n, (size_t)i * 32 * 32), "tables");
+    CK(cudaMemcpyToSymbol(g_dct8_m, c8[i], n * n, (size_t)i * 32 * 32), "tables");
+  }
+  std::vector<int16_t> scans(36 * 1024, 0);
+  int32_t offs[36];
+  int pos = 0;
+  for (int a = 1; a <= 6; a++)
+    for (int b = 1; b <= 6; b++) {
+      offs[(a - 1) * 6 + (b - 1)] = pos;
+      pos += build_scan(1 << a, 1 << b, scans.data() + pos);
+    }
+  CK(cudaMemcpyToSymbol(g_scan, scans.data(), sizeof(int16_t) * pos), "tables");
+  CK(cudaMemcpyToSymbol(g_scan_off, offs, sizeof(offs)), "tables");
+  CK(cudaDeviceSynchronize(), "tables");
+  if (ctx->device < 64) g_tables_ready[ctx->device] = true;
+  return VVCG_OK;
+}
+
+uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+
+template <typename T>
+vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
+  if (v.empty()) return VVCG_OK;
+  CK(buf.reserve(sizeof(T) * v.size()), "cudaMalloc");
+  CK(cudaMemcpyAsync(buf.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
+  if (!out) return VVCG_INVALID_INPUT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return VVCG_UNAVAILABLE;
+  }
+  int dev = cfg ? cfg->device : 0;
+  if (dev < 0 || dev >= ndev) return VVCG_INVALID_INPUT;
+  vvcg_ctx* ctx = new vvcg_ctx();
+  ctx->device = dev;
+  if (cfg && cfg->spin_limit) ctx->spin_limit = cfg->spin_limit;
+  if (cudaSetDevice(dev) != cudaSuccess) {
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  ctx->num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  ctx->stream = ctx->own_stream;
+  ctx->recon_smem = sizeof(ReconSmem);
+  if (cudaFuncSetAttribute(k_recon_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)ctx->recon_smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->recon_ctas_per_sm, k_recon_wavefront,
+                                                    256, ctx->recon_smem) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  if (upload_tables(ctx) != VVCG_OK) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  if (cfg && cfg->reserve_bytes) ctx->planes.reserve(cfg->reserve_bytes);
+  if (ctx->d_ctrl.reserve(64) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  cudaMemset(ctx->d_ctrl.p, 0, 64);
+  *out = ctx;
+  return VVCG_OK;
+}
+
+void vvcg_ctx_destroy(vvcg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
+                    &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
+                    &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl})
+    b->release();
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+}
+
+const char* vvcg_last_error(const vvcg_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+vvcg_status vvcg_set_stream(vvcg_ctx* ctx, void* stream) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return VVCG_OK;
+}
+
+uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  ctx->prepared = false;
+  if (!b || !b->pics || b->num_pics == 0) return fail(ctx, VVCG_INVALID_INPUT, "empty batch");
+  if (b->num_cus && !b->cus) return fail(ctx, VVCG_INVALID_INPUT, "missing CU records");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const uint32_t np = b->num_pics;
+  ctx->num_pics = np;
+  ctx->layout.assign(np, PicLayout{});
+  ctx->pics.assign(np, DevPic{});
+  ctx->items.clear();
+  for (auto& v : ctx->dbf) v.clear();
+  ctx->sao.clear();
+  ctx->alf.clear();
+  ctx->num_cus = b->num_cus;
+  ctx->num_levels = b->num_levels;
+  ctx->num_ctus = b->num_ctus;
+  ctx->num_aps = b->num_aps;
+  uint64_t plane_samples = 0, total_ctus = 0;
+  std::vector<uint64_t> flag_base(np);
+  for (uint32_t i = 0; i < np; i++) {
+    const vvcg_pic_desc& d = b->pics[i];
+    if (d.ctu_log2 < 5 || d.ctu_log2 > 7)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU size outside 32..=128", i);
+    const uint32_t ctu = 1u << d.ctu_log2;
+    if (d.width < ctu || d.height < ctu || d.width % ctu || d.height % ctu)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: coded size not aligned to the CTU grid", i);
+    if ((uint64_t)d.width * d.height > kMaxLumaSamples)
+      return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture %u: %ux%u exceeds %llu luma samples", i,
+                  d.width, d.height, (unsigned long long)kMaxLumaSamples);
+    if (d.bit_depth < 8 || d.bit_depth > 12 || d.chroma_format > 3)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: bit depth or chroma format", i);
+    if (d.visible_width > d.width || d.visible_height > d.height || !d.visible_width || !d.visible_height)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: visible size", i);
+    if (d.alf_aps >= 0 && (uint32_t)d.alf_aps >= b->num_aps)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: ALF APS index", i);
+    const int tb = std::min<int>(ctu, 32);
+    const int cf = d.chroma_format;
+    const int sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
+    const int tcw = cf ? std::max(tb / sw, 2) : 0, tch = cf ? std::max(tb / sh, 2) : 0;
+    const uint32_t gw = d.width / tb, gh = d.height / tb;
+    const uint32_t cw_ = d.width / ctu, ch_ = d.height / ctu;
+    if ((uint64_t)d.cu_offset + (uint64_t)gw * gh > b->num_cus)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CU records out of range", i);
+    const bool filt = d.tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF);
+    if (filt && (!b->ctus || (uint64_t)d.ctu_offset + (uint64_t)cw_ * ch_ > b->num_ctus))
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU filter records out of range", i);
+    // level offsets
+    for (uint32_t k = 0; k < gw * gh; k++) {
+      const vvcg_cu_rec& r = b->cus[d.cu_offset + k];
+      for (int c = 0; c < (cf ? 3 : 1); c++) {
+        if (!((r.cbf >> c) & 1) || r.level_off[c] < 0) continue;
+        uint64_t n = c ? (uint64_t)tcw * tch : (uint64_t)tb * tb;
+        if (!b->levels || (uint64_t)r.level_off[c] + n > b->num_levels)
+          return fail(ctx, VVCG_INVALID_INPUT, "picture %u CU %u: level offset out of range", i, k);
+      }
+    }
+    PicLayout& L = ctx->layout[i];
+    const int ncomp = cf ? 3 : 1;
+    for (int c = 0; c < 3; c++) {
+      L.pw[c] = c == 0 ? d.width : (cf ? (d.width + sw - 1) / sw : 0);
+      L.ph[c] = c == 0 ? d.height : (cf ? (d.height + sh - 1) / sh : 0);
+      L.vis_w[c] = c == 0 ? d.visible_width : (cf ? (d.visible_width + sw - 1) / sw : 0);
+      L.vis_h[c] = c == 0 ? d.visible_height : (cf ? (d.visible_height + sh - 1) / sh : 0);
+      L.stride[c] = c < ncomp ? (int32_t)align_up(L.pw[c], 64) : 0;
+      L.plane_off[c] = plane_samples;
+      plane_samples += c < ncomp ? (uint64_t)L.stride[c] * L.ph[c] : 0;
+      L.scratch_off[c] = plane_samples;
+      plane_samples += c < ncomp ? (uint64_t)L.stride[c] * L.ph[c] : 0;
+      L.final_in_scratch[c] = 0;
+    }
+    flag_base[i] = total_ctus;
+    total_ctus += (uint64_t)cw_ * ch_;
+    DevPic& P = ctx->pics[i];
+    P.bd = d.bit_depth;
+    P.cf = cf;
+    P.ctu_log2 = d.ctu_log2;
+    P.ctu = ctu;
+    P.tb = tb;
+    P.tb_cw = tcw;
+    P.tb_ch = tch;
+    P.sub_w = sw;
+    P.sub_h = sh;
+    P.grid_w = gw;
+    P.grid_h = gh;
+    P.ctu_w = cw_;
+    P.ctu_h = ch_;
+    // slice.rs:4681-4682 Qp'Y and Qp'C, both at least 4
+    const int off = 6 * (d.bit_depth - 8);
+    P.lqp = std::max(std::min(63 + off, std::max(0, (int)d.slice_qp + off)), 4);
+    P.cqp = std::max((int)d.chroma_qp_scaled, 4);
+    P.slice_qp = d.slice_qp;
+    P.tools = d.tools;
+    P.aps = d.alf_aps;
+    for (int c = 0; c < 3; c++) {
+      P.stride[c] = L.stride[c];
+      P.pw[c] = L.pw[c];
+      P.ph[c] = L.ph[c];
+    }
+  }
+  // wavefront order: CTU diagonal t = cx + 2*cy, then picture
+  {
+    uint32_t tmax = 0;
+    for (auto& P : ctx->pics) tmax = std::max<uint32_t>(tmax, (P.ctu_w - 1) + 2 * (P.ctu_h - 1));
+    for (uint32_t t = 0; t <= tmax; t++)
+      for (uint32_t i = 0; i < np; i++) {
+        const DevPic& P = ctx->pics[i];
+        for (int cy = 0; cy < P.ctu_h; cy++) {
+          int cx = (int)t - 2 * cy;
+          if (cx < 0 || cx >= P.ctu_w) continue;
+          ctx->items.push_back(CtuItem{i, (uint16_t)cx, (uint16_t)cy});
+        }
+      }
+  }
+  // device memory
+  CK(ctx->planes.reserve(plane_samples * sizeof(uint16_t)), "cudaMalloc planes");
+  if (ctx->flags.cap < total_ctus * sizeof(uint32_t)) {
+    CK(ctx->flags.reserve(total_ctus * sizeof(uint32_t)), "cudaMalloc flags");
+    CK(cudaMemsetAsync(ctx->flags.p, 0, ctx->flags.cap, ctx->stream), "memset flags");
+  }
+  ctx->flags_count = total_ctus;
+  CK(ctx->d_cus.reserve(std::max<uint64_t>(1, b->num_cus) * sizeof(vvcg_cu_rec)), "cudaMalloc");
+  CK(ctx->d_levels.reserve(std::max<uint64_t>(1, b->num_levels) * sizeof(int16_t)), "cudaMalloc");
+  CK(ctx->d_ctus.reserve(std::max<uint64_t>(1, b->num_ctus) * sizeof(vvcg_ctu_filter)), "cudaMalloc");
+  CK(ctx->d_aps.reserve(std::max<uint64_t>(1, b->num_aps) * sizeof(vvcg_alf_aps)), "cudaMalloc");
+  uint16_t* base = (uint16_t*)ctx->planes.p;
+  for (uint32_t i = 0; i < np; i++) {
+    const vvcg_pic_desc& d = b->pics[i];
+    DevPic& P = ctx->pics[i];
+    PicLayout& L = ctx->layout[i];
+    for (int c = 0; c < 3; c++) {
+      P.plane[c] = base + L.plane_off[c];
+      P.scratch[c] = base + L.scratch_off[c];
+    }
+    P.cus = (const vvcg_cu_rec*)ctx->d_cus.p + d.cu_offset;
+    P.ctus = (const vvcg_ctu_filter*)ctx->d_ctus.p + d.ctu_offset;
+    P.ctu_done = (uint32_t*)ctx->flags.p + flag_base[i];
+    const int ncomp = P.cf ? 3 : 1;
+    if (d.tools & VVCG_TOOL_DEBLOCK) {
+      // slice.rs:4990-5020: luma lattice tb, CTB ctu, SliceQpY; chroma lattice
+      // tb_cw, CTB height ctu / SubHeightC, QP derived_chroma_qp(SliceQpY)
+      const int step = std::max(P.tb, 8), ctb = std::max(P.ctu, step);
+      const int lml = step <= 4 ? 1 : (step >= 32 ? 7 : 3);
+      DbfPass v{P.plane[0], P.stride[0], P.pw[0], P.ph[0], P.bd, step, ctb, (int)d.slice_qp, 2, 0, 0,
+                lml, lml, 1, 0, 0};
+      v.n_edges = (P.pw[0] - 8) / step;
+      v.n_segs = P.ph[0] / 4;
+      DbfPass h = v;
+      h.n_edges = (P.ph[0] - 8) / step;
+      h.n_segs = P.pw[0] / 4;
+      if (v.n_edges > 0 && v.n_segs > 0) ctx->dbf[0].push_back(v);
+      if (h.n_edges > 0 && h.n_segs > 0) ctx->dbf[1].push_back(h);
+      if (P.cf) {
+        const int cqp = std::min(63, std::max(0, (int)d.slice_qp <= 26 ? (int)d.slice_qp
+                                                                        : (int)d.slice_qp - 1));
+        const int cstep = std::max(P.tb_cw, 8);
+        const int cctb = std::max(P.ctu / P.sub_h, cstep);
+        const int clen = cstep >= 8 ? 3 : 1;
+        for (int c = 1; c <= 2; c++) {
+          DbfPass cv{P.plane[c], P.stride[c], P.pw[c], P.ph[c], P.bd, cstep, cctb, cqp, 2, 0, 0,
+                     clen, clen, P.sub_h, 0, 0};
+          cv.n_edges = P.pw[c] >= 8 ? (P.pw[c] - 4) / cstep : 0;
+          cv.n_segs = P.ph[c] / (P.sub_h == 1 ? 4 : 2);
+          DbfPass ch = cv;
+          ch.sub = P.sub_w;
+          ch.n_edges = P.ph[c] >= 8 ? (P.ph[c] - 4) / cstep : 0;
+          ch.n_segs = P.pw[c] / (P.sub_w == 1 ? 4 : 2);
+          if (cv.n_edges > 0 && cv.n_segs > 0) ctx->dbf[2].push_back(cv);
+          if (ch.n_edges > 0 && ch.n_segs > 0) ctx->dbf[3].push_back(ch);
+        }
+      }
+    }
+    bool sao_ran = false;
+    if (d.tools & VVCG_TOOL_SAO) {
+      sao_ran = true;
+      for (int c = 0; c < ncomp; c++) {
+        SaoPass s{P.plane[c], P.scratch[c], P.ctus, P.stride[c], P.pw[c], P.ph[c], P.bd, c,
+                  c ? P.ctu / P.sub_w : P.ctu, c ? P.ctu / P.sub_h : P.ctu, P.ctu_w};
+        ctx->sao.push_back(s);
+        L.final_in_scratch[c] = 1;
+      }
+    }
+    if (d.tools & VVCG_TOOL_ALF) {
+      bool any = false;
+      for (uint64_t k = 0; k < (uint64_t)P.ctu_w * P.ctu_h; k++) any |= b->ctus[d.ctu_offset + k].alf_luma != 0;
+      if (any) {
+        AlfPass a{sao_ran ? P.scratch[0] : P.plane[0], sao_ran ? P.plane[0] : P.scratch[0],
+                  d.alf_aps >= 0 ? (const vvcg_alf_aps*)ctx->d_aps.p + d.alf_aps : nullptr,
+                  P.stride[0], P.pw[0], P.ph[0], P.bd};
+        ctx->alf.push_back(a);
+        L.final_in_scratch[0] = sao_ran ? 0 : 1;
+      }
+    }
+  }
+  vvcg_status st;
+  if ((st = upload_vec(ctx, ctx->d_pics, ctx->pics)) != VVCG_OK) return st;
+  if ((st = upload_vec(ctx, ctx->d_items, ctx->items)) != VVCG_OK) return st;
+  for (int k = 0; k < 4; k++)
+    if ((st = upload_vec(ctx, ctx->d_dbf[k], ctx->dbf[k])) != VVCG_OK) return st;
+  if ((st = upload_vec(ctx, ctx->d_sao, ctx->sao)) != VVCG_OK) return st;
+  if ((st = upload_vec(ctx, ctx->d_alf, ctx->alf)) != VVCG_OK) return st;
+  CK(cudaStreamSynchronize(ctx->stream), "prepare");
+  ctx->prepared = true;
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_batch_upload(vvcg_ctx* ctx, const vvcg_batch* b) {
+  if (!ctx || !b) return VVCG_INVALID_INPUT;
+  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+  if (b->num_cus != ctx->num_cus || b->num_levels > ctx->d_levels.cap / sizeof(int16_t) ||
+      b->num_ctus != ctx->num_ctus || b->num_aps != ctx->num_aps)
+    return fail(ctx, VVCG_INVALID_INPUT, "batch shape differs from the prepared one");
+  ctx->num_levels = b->num_levels;
+  if (b->num_cus)
+    CK(cudaMemcpyAsync(ctx->d_cus.p, b->cus, sizeof(vvcg_cu_rec) * b->num_cus, cudaMemcpyHostToDevice, ctx->stream), "upload CUs");
+  if (b->num_levels)
+    CK(cudaMemcpyAsync(ctx->d_levels.p, b->levels, sizeof(int16_t) * b->num_levels, cudaMemcpyHostToDevice, ctx->stream), "upload levels");
+  if (b->num_ctus && b->ctus)
+    CK(cudaMemcpyAsync(ctx->d_ctus.p, b->ctus, sizeof(vvcg_ctu_filter) * b->num_ctus, cudaMemcpyHostToDevice, ctx->stream), "upload CTUs");
+  if (b->num_aps && b->aps)
+    CK(cudaMemcpyAsync(ctx->d_aps.p, b->aps, sizeof(vvcg_alf_aps) * b->num_aps, cudaMemcpyHostToDevice, ctx->stream), "upload APS");
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+  uint32_t* ctrl = (uint32_t*)ctx->d_ctrl.p;
+  CK(cudaMemsetAsync(ctrl, 0, 2 * sizeof(uint32_t), ctx->stream), "memset");
+  if (mask & VVCG_STAGE_RECON) {
+    ctx->epoch++;
+    const uint32_t n = (uint32_t)ctx->items.size();
+    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(ctx->num_sms * std::max(1, ctx->recon_ctas_per_sm)));
+    k_recon_wavefront<<<grid, 256, ctx->recon_smem, ctx->stream>>>(
+        (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl,
+        (const int16_t*)ctx->d_levels.p, ctx->num_levels, ctx->epoch, ctx->spin_limit, ctrl + 1);
+    CK(cudaGetLastError(), "recon launch");
+    ctx->launches++;
+  }
+  if (mask & VVCG_STAGE_DEBLOCK) {
+    for (int k = 0; k < 4; k++) {
+      const auto& v = ctx->dbf[k];
+      if (v.empty()) continue;
+      uint32_t maxw = 0;
+      for (auto& p : v) maxw = std::max<uint32_t>(maxw, (uint32_t)(p.n_edges * p.n_segs));
+      dim3 grid((maxw + 127) / 128, (unsigned)v.size());
+      const DbfPass* d = (const DbfPass*)ctx->d_dbf[k].p;
+      if (k == 0) k_deblock_luma<true><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
+      if (k == 1) k_deblock_luma<false><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
+      if (k == 2) k_deblock_chroma<true><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
+      if (k == 3) k_deblock_chroma<false><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
+      CK(cudaGetLastError(), "deblock launch");
+      ctx->launches++;
+    }
+  }
+  if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
+    uint32_t maxb = 0;
+    for (auto& s : ctx->sao) maxb = std::max<uint32_t>(maxb, (uint32_t)(((s.w + 63) / 64) * ((s.h + 3) / 4)));
+    k_sao<<<dim3(maxb, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p);
+    CK(cudaGetLastError(), "sao launch");
+    ctx->launches++;
+  }
+  if ((mask & VVCG_STAGE_ALF) && !ctx->alf.empty()) {
+    uint32_t gx = 0, gy = 0;
+    for (auto& a : ctx->alf) {
+      gx = std::max<uint32_t>(gx, (a.w + kAlfTw - 1) / kAlfTw);
+      gy = std::max<uint32_t>(gy, (a.h + kAlfTh - 1) / kAlfTh);
+    }
+    k_alf_luma<<<dim3(gx, gy, (unsigned)ctx->alf.size()), 256, 0, ctx->stream>>>(
+        (const AlfPass*)ctx->d_alf.p, ctrl + 1);
+    CK(cudaGetLastError(), "alf launch");
+    ctx->launches++;
+  }
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_batch_sync(vvcg_ctx* ctx) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  uint32_t status = 0;
+  CK(cudaMemcpyAsync(&status, (uint32_t*)ctx->d_ctrl.p + 1, sizeof(status), cudaMemcpyDeviceToHost, ctx->stream), "status");
+  CK(cudaStreamSynchronize(ctx->stream), "synchronize");
+  if (status & kStatusTimeout)
+    return fail(ctx, VVCG_TIMEOUT, "a wavefront wait gave up after %u polls", ctx->spin_limit);
+  if (status & kStatusBadRecord) return fail(ctx, VVCG_INVALID_INPUT, "a level offset was out of range");
+  if (status & kStatusAlfAbort)
+    return fail(ctx, VVCG_INVALID_INPUT,
+                "fixed-filter ALF reached a class >= 16, where the reference aborts");
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_batch_download(vvcg_ctx* ctx, const vvcg_plane_out* out) {
+  if (!ctx || !out) return VVCG_INVALID_INPUT;
+  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+  for (uint32_t i = 0; i < ctx->num_pics; i++) {
+    const PicLayout& L = ctx->layout[i];
+    const DevPic& P = ctx->pics[i];
+    for (int c = 0; c < (P.cf ? 3 : 1); c++) {
+      const vvcg_plane_out& o = out[i * 3 + c];
+      if (!o.data) continue;
+      if (o.stride < (uint32_t)L.vis_w[c]) return fail(ctx, VVCG_INVALID_INPUT, "output stride too small");
+      const uint16_t* src = L.final_in_scratch[c] ? P.scratch[c] : P.plane[c];
+      CK(cudaMemcpy2DAsync(o.data, (size_t)o.stride * 2, src, (size_t)L.stride[c] * 2,
+                           (size_t)L.vis_w[c] * 2, L.vis_h[c], cudaMemcpyDeviceToHost, ctx->stream),
+         "download");
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream), "download");
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_batch_plane(vvcg_ctx* ctx, uint32_t pic, uint32_t comp, void** ptr, uint32_t* stride) {
+  if (!ctx || !ptr || !ctx->prepared || pic >= ctx->num_pics || comp > 2) return VVCG_INVALID_INPUT;
+  const PicLayout& L = ctx->layout[pic];
+  const DevPic& P = ctx->pics[pic];
+  if (comp > 0 && !P.cf) return VVCG_INVALID_INPUT;
+  *ptr = L.final_in_scratch[comp] ? P.scratch[comp] : P.plane[comp];
+  if (stride) *stride = (uint32_t)L.stride[comp];
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_decode_batch(vvcg_ctx* ctx, const vvcg_batch* b, const vvcg_plane_out* out) {
+  vvcg_status st;
+  if ((st = vvcg_batch_prepare(ctx, b)) != VVCG_OK) return st;
+  if ((st = vvcg_batch_upload(ctx, b)) != VVCG_OK) return st;
+  if ((st = vvcg_batch_run(ctx, VVCG_STAGE_ALL)) != VVCG_OK) return st;
+  if ((st = vvcg_batch_sync(ctx)) != VVCG_OK) return st;
+  return vvcg_batch_download(ctx, out);
+}
+
+static vvcg_status mc_common(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uint32_t h,
+                             uint32_t stride, uint8_t bd, int chroma, const vvcg_mc_block* blocks,
+                             uint32_t n, int32_t* out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!ref || !out || (n && !blocks) || !w || !h || stride < w || bd < 8 || bd > 12)
+    return fail(ctx, VVCG_INVALID_INPUT, "invalid MC arguments");
+  if (n == 0) return VVCG_OK;
+  McParams pm{ref, (int32_t)w, (int32_t)h, (int32_t)stride, bd, chroma};
+  k_mc<<<n, 256, 0, ctx->stream>>>(pm, blocks, n, out, (uint32_t*)ctx->d_ctrl.p + 1);
+  CK(cudaGetLastError(), "mc launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_mc_luma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uint32_t h,
+                                uint32_t stride, uint8_t bd, const vvcg_mc_block* blocks,
+                                uint32_t n, int32_t* out) {
+  return mc_common(ctx, ref, w, h, stride, bd, 0, blocks, n, out);
+}
+
+vvcg_status vvcg_mc_chroma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uint32_t h,
+                                  uint32_t stride, uint8_t bd, uint8_t cf,
+                                  const vvcg_mc_block* blocks, uint32_t n, int32_t* out) {
+  if (cf < 1 || cf > 3) return fail(ctx, VVCG_INVALID_INPUT, "chroma format");
+  return mc_common(ctx, ref, w, h, stride, bd, cf, blocks, n, out);
+}
+
+vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* p0, const int32_t* p1,
+                                      uint64_t count, uint8_t bcw, uint8_t bd, uint16_t* out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!p0 || !p1 || !out || bd < 8 || bd > 12 || bcw > 4)
+    return fail(ctx, VVCG_INVALID_INPUT, "invalid bi-average arguments");
+  if (!count) return VVCG_OK;
+  uint32_t grid = (uint32_t)std::min<uint64_t>((count + 255) / 256, (uint64_t)ctx->num_sms * 16);
+  k_bi_average<<<grid, 256, 0, ctx->stream>>>(p0, p1, count, bcw, bd, out);
+  CK(cudaGetLastError(), "bi average launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+}  // extern "C"

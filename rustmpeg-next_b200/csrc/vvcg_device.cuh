@@ -1,0 +1,54 @@
+// Device-side data layout and helpers shared by the reconstruction and
+// loop-filter kernels of libvvcg (sm_100a).
+#pragma once
+#include <stdint.h>
+
+#include "../../include/vvcg.h"
+
+namespace vvcg {
+
+// Status word bits written by kernels (read back by vvcg_batch_sync).
+enum : uint32_t {
+  kStatusTimeout = 1u << 0,      // a wavefront wait ran out of polls
+  kStatusBadRecord = 1u << 1,    // a record or level offset was out of range
+  kStatusAlfAbort = 1u << 2,     // fixed-filter ALF reached class >= 16 (the reference aborts)
+};
+
+// One picture as the kernels see it (built on the host, copied to HBM).
+struct DevPic {
+  uint16_t* plane[3];       // coded-size reconstructed planes (Y, Cb, Cr)
+  uint16_t* scratch[3];     // same-size planes for the pre-SAO / pre-ALF copies
+  int32_t stride[3];        // samples
+  int32_t pw[3], ph[3];     // plane widths / heights
+  const vvcg_cu_rec* cus;   // the picture's records, tb-grid raster order
+  const vvcg_ctu_filter* ctus;
+  uint32_t* ctu_done;       // per-CTU epoch flags (CTU raster order)
+  int32_t bd, cf, ctu_log2, ctu, tb, tb_cw, tb_ch, sub_w, sub_h;
+  int32_t grid_w, grid_h, ctu_w, ctu_h;
+  int32_t lqp, cqp, slice_qp, tools, aps;
+};
+
+// Work item of the wavefront: a CTU of a picture.
+struct CtuItem {
+  uint32_t pic;
+  uint16_t cx, cy;
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ int ilog2(int v) { return __ffs(v) - 1; }
+__device__ __forceinline__ int floor_log2(unsigned v) { return 31 - __clz(v); }
+__device__ __forceinline__ int clip16(long long v) {
+  return (int)(v < -32768 ? -32768 : (v > 32767 ? 32767 : v));
+}
+__device__ __forceinline__ int clip16i(int v) { return v < -32768 ? -32768 : (v > 32767 ? 32767 : v); }
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+}  // namespace vvcg

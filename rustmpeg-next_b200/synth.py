@@ -1,0 +1,191 @@
+"""Seeded synthetic workloads for the frame path.
+
+- ``value_noise_frame``: the 1920x1080 10-bit 4:2:0 content of the full-frame
+  configuration (4-octave value noise with octave gains 1, .5, .25, .125,
+  amplitude 0..1023, translated by (+1.25, -0.75) px per frame, plus 8 moving
+  64x64 textured rectangles with velocities uniform in +-6 px/frame; chroma is
+  the same noise at half resolution scaled to [384, 640]).
+- ``random_records``: decoder inputs with the statistics of coded pictures
+  (per-CU intra modes, CCLM chroma modes, sparse low-frequency transform levels
+  whose density falls with frequency and QP, per-CTU SAO parameters and ALF
+  switches), for picture batches of any size, bit depth and chroma format.
+
+Seeds follow 0x5EED0000 + stream * 1000 + frame.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import (APS_DTYPE, CTU_DTYPE, CU_DTYPE, PIC_DTYPE, TOOL_ALF, TOOL_DEBLOCK, TOOL_DEP_QUANT,
+               TOOL_SAO, chroma_dims)
+
+
+def seed_for(stream: int, frame: int) -> int:
+    return 0x5EED0000 + stream * 1000 + frame
+
+
+def _value_noise(h, w, cell, rng_seed, ox=0.0, oy=0.0):
+    rng = np.random.default_rng(rng_seed)
+    gh, gw = int((h + abs(oy)) / cell) + 3, int((w + abs(ox)) / cell) + 3
+    lattice = rng.random((gh, gw))
+    ys = (np.arange(h)[:, None] + oy) / cell + 1
+    xs = (np.arange(w)[None, :] + ox) / cell + 1
+    y0 = np.floor(ys).astype(int)
+    x0 = np.floor(xs).astype(int)
+    fy = ys - y0
+    fx = xs - x0
+    fy = fy * fy * (3 - 2 * fy)
+    fx = fx * fx * (3 - 2 * fx)
+    y0 = np.clip(y0, 0, gh - 2)
+    x0 = np.clip(x0, 0, gw - 2)
+    a = lattice[y0, x0]
+    b = lattice[y0, x0 + 1]
+    c = lattice[y0 + 1, x0]
+    d = lattice[y0 + 1, x0 + 1]
+    return (a * (1 - fx) + b * fx) * (1 - fy) + (c * (1 - fx) + d * fx) * fy
+
+
+def _noise(h, w, seed, ox, oy, base_cell=128.0):
+    acc = np.zeros((h, w))
+    norm = 0.0
+    for o, g in enumerate((1.0, 0.5, 0.25, 0.125)):
+        acc += g * _value_noise(h, w, base_cell / (2 ** o), seed + 17 * o, ox / (2 ** 0), oy)
+        norm += g
+    return acc / norm
+
+
+def value_noise_frame(w=1920, h=1080, bd=10, frame=0, stream=0):
+    """One frame of the full-frame content; returns (y, u, v) uint16 planes."""
+    mx = (1 << bd) - 1
+    base = seed_for(stream, 0)
+    ox, oy = 1.25 * frame, -0.75 * frame
+    y = _noise(h, w, base, ox, oy) * mx
+    rng = np.random.default_rng(base + 7)
+    pos = rng.uniform([0, 0], [w - 64, h - 64], size=(8, 2))
+    vel = rng.uniform(-6, 6, size=(8, 2))
+    tex = [_noise(64, 64, base + 100 + k, 0, 0, base_cell=16.0) * mx for k in range(8)]
+    for k in range(8):
+        px, py = pos[k] + vel[k] * frame
+        px = int(round(px)) % max(1, w - 64)
+        py = int(round(py)) % max(1, h - 64)
+        y[py:py + 64, px:px + 64] = tex[k]
+    cw, ch = (w + 1) // 2, (h + 1) // 2
+    lo, hi = 384 << (bd - 10) if bd >= 10 else 384 >> (10 - bd), 640 << (bd - 10) if bd >= 10 else 640 >> (10 - bd)
+    u = lo + _noise(ch, cw, base + 1, ox / 2, oy / 2) * (hi - lo)
+    v = lo + _noise(ch, cw, base + 2, ox / 2, oy / 2) * (hi - lo)
+    return (np.clip(np.rint(y), 0, mx).astype(np.uint16), np.clip(np.rint(u), 0, mx).astype(np.uint16),
+            np.clip(np.rint(v), 0, mx).astype(np.uint16))
+
+
+def pad_to(plane, w, h):
+    """Edge-replicate a plane to (h, w) (mod.rs:2753 pad_vvc_frame)."""
+    ph, pw = plane.shape
+    return np.pad(plane, ((0, h - ph), (0, w - pw)), mode="edge")
+
+
+def _tb_levels(rng, w, h, qp_scaled):
+    """Sparse levels concentrated at low frequencies; density falls with QP."""
+    yy, xx = np.mgrid[0:h, 0:w]
+    freq = (xx + yy) / (w + h)
+    dens = np.clip(0.9 * np.exp(-freq * 9.0) * np.exp(-(qp_scaled - 22) / 14.0), 0.0, 0.95)
+    mask = rng.random((h, w)) < dens
+    mag = np.floor(rng.exponential(1.0 + 6.0 * np.exp(-freq * 6.0) * np.exp(-(qp_scaled - 22) / 12.0),
+                                   (h, w))).astype(np.int32) + 1
+    sign = np.where(rng.random((h, w)) < 0.5, -1, 1)
+    return (mask * mag * sign).astype(np.int16)
+
+
+def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=False):
+    """Build a batch of decoder records.
+
+    pics_spec: iterable of dicts with keys width, height (coded, CTU multiples),
+    visible_width, visible_height, bit_depth, chroma_format, ctu_log2, qp.
+    Returns (pics, cus, levels, ctus, aps).
+    """
+    rng = np.random.default_rng(seed)
+    pics, cu_chunks, lv_chunks, ctu_chunks = [], [], [], []
+    n_cu = n_lv = n_ctu = 0
+    for spec in pics_spec:
+        w, h, bd, cf = spec["width"], spec["height"], spec["bit_depth"], spec["chroma_format"]
+        ctu_log2, qp = spec.get("ctu_log2", 5), spec["qp"]
+        ctu = 1 << ctu_log2
+        tb = min(ctu, 32)
+        sw = 2 if cf in (1, 2) else 1
+        sh = 2 if cf == 1 else 1
+        tcw, tch = (max(tb // sw, 2), max(tb // sh, 2)) if cf else (0, 0)
+        off = 6 * (bd - 8)
+        lqp = max(min(63 + off, qp + off), 4)
+        qpc = min(63, max(-off, qp))
+        cqp = max(0, (qpc if qpc <= 26 else qpc - 1) + off)
+        p = np.zeros((), PIC_DTYPE)
+        p["width"], p["height"] = w, h
+        p["visible_width"] = spec.get("visible_width", w)
+        p["visible_height"] = spec.get("visible_height", h)
+        p["bit_depth"], p["chroma_format"], p["ctu_log2"] = bd, cf, ctu_log2
+        p["slice_qp"], p["chroma_qp_scaled"] = qp, cqp
+        p["tools"] = spec.get("tools", tools)
+        p["alf_aps"] = 0 if alf_aps else -1
+        p["cu_offset"], p["ctu_offset"] = n_cu, n_ctu
+        gw, gh = w // tb, h // tb
+        cus = np.zeros(gw * gh, CU_DTYPE)
+        cus["luma_mode"] = rng.integers(0, 67, gw * gh)
+        chm = rng.integers(0, 70, gw * gh)
+        chm = np.where(chm >= 67, 81 + (chm - 67), cus["luma_mode"])
+        cus["chroma_mode"] = chm if cf else 0
+        cus["level_off"] = -1
+        for k in range(gw * gh):
+            cbf = 0
+            for c in range(3 if cf else 1):
+                if rng.random() < (0.85 if c == 0 else 0.5) * np.exp(-(qp - 22) / 30.0):
+                    bw, bh = (tb, tb) if c == 0 else (tcw, tch)
+                    lv = _tb_levels(rng, bw, bh, lqp if c == 0 else cqp)
+                    if not lv.any():
+                        lv[0, 0] = 1
+                    cus["level_off"][k, c] = n_lv
+                    lv_chunks.append(lv.ravel())
+                    n_lv += lv.size
+                    cbf |= 1 << c
+            cus["cbf"][k] = cbf
+        ctus = np.zeros((h // ctu) * (w // ctu), CTU_DTYPE)
+        omax = (1 << (min(bd, 10) - 5)) - 1
+        for k in range(len(ctus)):
+            for c in range(3 if cf else 1):
+                r = rng.random()
+                if r > sao_prob:
+                    continue
+                if r < sao_prob / 2:
+                    ctus["sao"][k, c]["type"] = 1
+                    ctus["sao"][k, c]["band_or_class"] = rng.integers(0, 32)
+                    ctus["sao"][k, c]["offsets"] = rng.integers(-omax, omax + 1, 4)
+                else:
+                    ctus["sao"][k, c]["type"] = 2
+                    ctus["sao"][k, c]["band_or_class"] = rng.integers(0, 4)
+                    o = rng.integers(0, omax + 1, 4)
+                    ctus["sao"][k, c]["offsets"] = [o[0], o[1], -o[2], -o[3]]
+        ctus["alf_luma"] = rng.random(len(ctus)) < 0.7
+        pics.append(p)
+        cu_chunks.append(cus)
+        ctu_chunks.append(ctus)
+        n_cu += len(cus)
+        n_ctu += len(ctus)
+    aps = None
+    if alf_aps:
+        aps = synthetic_aps(rng)
+    levels = np.concatenate(lv_chunks) if lv_chunks else np.zeros(0, np.int16)
+    return (np.array(pics, PIC_DTYPE), np.concatenate(cu_chunks), levels,
+            np.concatenate(ctu_chunks), aps)
+
+
+def synthetic_aps(rng, n_filters=25, luma_clip=True):
+    """An ALF APS whose luma filters are fixed-filter coefficient sets of the
+    standard (clip indices uniform over 0..3)."""
+    from .tables import alf_fixed_coeff
+
+    fixed = alf_fixed_coeff()
+    aps = np.zeros(1, APS_DTYPE)
+    aps["num_luma_filters"] = n_filters
+    aps["luma_clip"] = int(luma_clip)
+    aps["coeff_delta_idx"][0] = rng.integers(0, n_filters, 25)
+    aps["coeff"][0, :n_filters] = fixed[rng.integers(0, 64, n_filters), :12]
+    aps["clip_idx"][0, :n_filters] = rng.integers(0, 4, (n_filters, 12))
+    return aps
