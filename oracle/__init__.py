@@ -79,7 +79,6 @@ def _declare(L):
     L.orc_deblock_chroma.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i]
     L.orc_deblock_chroma.restype = None
     L.orc_sao_region.argtypes = [vp, vp, i, i, i, i, i, i, i, i, i, vp]
-    L.orc_sao_region.restype = None
     L.orc_alf_luma.argtypes = [vp, i, i, i, i, i, vp, vp, vp]
     L.orc_alf_classify.argtypes = [vp, i, i, i, i, i, vp]
     L.orc_alf_classify.restype = None
@@ -248,9 +247,9 @@ def sao_region(src, dst, bd, bx, by, w, h, sao_type, band_or_class, offsets):
     src = _u16(src)
     dst = _u16(dst).copy()
     off = np.asarray(offsets, dtype=np.int32)
-    lib().orc_sao_region(_p(src), _p(dst), src.shape[1], src.shape[0], bd, bx, by, w, h,
-                         sao_type, band_or_class, _p(off))
-    return dst
+    rc = lib().orc_sao_region(_p(src), _p(dst), src.shape[1], src.shape[0], bd, bx, by, w, h,
+                              sao_type, band_or_class, _p(off))
+    return dst, rc
 
 
 def alf_luma(plane, bd, aps=None):
@@ -342,7 +341,7 @@ def encode_frame(y, u, v, bd, qp, ctu_log2=5, opts=OPT_FULL_INTRA | OPT_DEBLOCK,
     v = _u16(v) if cf else np.zeros((1, 1), np.uint16)
     tb = min(1 << ctu_log2, 32)
     cus = np.zeros((h // tb) * (w // tb), dtype=CU_DTYPE)
-    cap = w * h * 2 + 64
+    cap = w * h * 3 + 64
     levels = np.zeros(cap, dtype=np.int16)
     used = C.c_uint64(0)
     ry = np.zeros((h, w), np.uint16)

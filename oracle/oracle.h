@@ -114,8 +114,9 @@ struct Sao {
   int band_pos_or_class;
   int offsets[4];
 };
-void apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
-                         const Sao& sao);
+// Returns -1 (without writing) where the reference aborts: see orc_filter.cpp.
+int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
+                        const Sao& sao);
 struct AlfAps {
   int num_luma_filters;  // 0 = fixed filters of the class
   bool luma_clip;

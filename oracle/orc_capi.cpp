@@ -89,11 +89,11 @@ void orc_deblock_chroma(uint16_t* plane, int pw, int ph, int bd, int cu_step, in
   Plane16 p{plane, pw, ph, bd};
   deblock_chroma_plane_16(p, cu_step, ctb_h, qp, bs, beta_off, tc_off, sub_w, sub_h);
 }
-void orc_sao_region(const uint16_t* src, uint16_t* dst, int pw, int ph, int bd, int bx, int by,
-                    int w, int h, int type, int band_or_class, const int32_t* offsets) {
+int orc_sao_region(const uint16_t* src, uint16_t* dst, int pw, int ph, int bd, int bx, int by,
+                   int w, int h, int type, int band_or_class, const int32_t* offsets) {
   Plane16 s{(uint16_t*)src, pw, ph, bd}, d{dst, pw, ph, bd};
   Sao sao{type, band_or_class, {offsets[0], offsets[1], offsets[2], offsets[3]}};
-  apply_sao_region_16(s, d, bx, by, w, h, sao);
+  return apply_sao_region_16(s, d, bx, by, w, h, sao);
 }
 // aps == NULL selects the fixed filters. Returns -1 where the reference aborts.
 int orc_alf_luma(uint16_t* plane, int pw, int ph, int bd, int num_filters, int luma_clip,

@@ -368,9 +368,20 @@ void deblock_chroma_plane_16(Plane16& p, int cu_step, int ctb_height_c, int qp_c
 
 // ---------------------------------------------------------------------- SAO ---
 
-// filter.rs:1880-1947 apply_sao_region_16
-void apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
-                         const Sao& sao) {
+// filter.rs:1880-1947 apply_sao_region_16. For edge class 3 the reference uses
+// the neighbour offset (1, -1) with a bounds test written for (1, 1): on the
+// first and last picture rows it indexes row -1 / row height, which panics
+// (slice index out of bounds). This restatement returns -1 before writing
+// anything in that case.
+int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
+                        const Sao& sao) {
+  if (sao.type == 2 && (sao.band_pos_or_class & 3) == 3 && src.width >= 3) {
+    int hl_ = std::min(by + h, src.height);
+    if ((by == 0 && hl_ > 0) || (hl_ == src.height && by < hl_)) {
+      int xl = std::max(bx, 1), xr = std::min(bx + w, src.width) - 1;  // x in [1, width-2]
+      if (xl <= std::min(xr, src.width - 2)) return -1;
+    }
+  }
   int bd = clampi(src.bd, 8, 12);
   int mx = (1 << bd) - 1;
   int band_shift = bd - 5;
@@ -403,6 +414,7 @@ void apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w
         dst.set(x, y, clampi(c + off, 0, mx));
       }
   }
+  return 0;
 }
 
 // ---------------------------------------------------------------------- ALF ---

@@ -335,10 +335,10 @@ int orc_recon_frame(const vvcg_pic_desc* pic, const vvcg_cu_rec* cus, const int1
           s[c].band_pos_or_class = f.sao[c].band_or_class;
           for (int k = 0; k < 4; k++) s[c].offsets[k] = f.sao[c].offsets[k];
         }
-        apply_sao_region_16(sy, ry, xx * g.ctu, yy * g.ctu, g.ctu, g.ctu, s[0]);
+        if (apply_sao_region_16(sy, ry, xx * g.ctu, yy * g.ctu, g.ctu, g.ctu, s[0])) return -3;
         if (has_c) {
-          apply_sao_region_16(su, ru, xx * ctu_cw, yy * ctu_ch, ctu_cw, ctu_ch, s[1]);
-          apply_sao_region_16(sv, rv, xx * ctu_cw, yy * ctu_ch, ctu_cw, ctu_ch, s[2]);
+          if (apply_sao_region_16(su, ru, xx * ctu_cw, yy * ctu_ch, ctu_cw, ctu_ch, s[1])) return -3;
+          if (apply_sao_region_16(sv, rv, xx * ctu_cw, yy * ctu_ch, ctu_cw, ctu_ch, s[2])) return -3;
         }
       }
   }

@@ -38,7 +38,10 @@ void interpolate_luma_block_16(const Plane16& ref, int bx, int by, int w, int h,
   int head = std::max(14 - bd, 2);
   int shift1 = 6 - head;
   int shift2 = bi ? 6 : 12 - bd;
-  int add2 = bi ? 0 : 1 << (shift2 - 1);
+  // `1i32 << (shift2 - 1)` and `sum + add2` as the reference's release build
+  // evaluates them: the shift count is masked to 5 bits (at 12 bit shift2 is 0,
+  // giving 1 << 31) and the addition wraps.
+  int add2 = bi ? 0 : (int)(1u << ((unsigned)(shift2 - 1) & 31));
   int offs = 1 << (bd + head - 1);
   if (fx == 0 && fy == 0) {
     for (int y = 0; y < h; y++)
@@ -90,7 +93,7 @@ void interpolate_luma_block_16(const Plane16& ref, int bx, int by, int w, int h,
     for (int x = 0; x < w; x++) {
       int s = 0;
       for (int k = 0; k < 8; k++) s += fv[k] * tmp[(y + k) * w + x];
-      out[y * w + x] = bi ? (s >> shift2) - offs : clampi((s + add2) >> shift2, 0, mx);
+      out[y * w + x] = bi ? (s >> shift2) - offs : clampi((int)((unsigned)s + (unsigned)add2) >> shift2, 0, mx);
     }
 }
 
@@ -112,7 +115,10 @@ void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, in
   int head = std::max(14 - bd, 2);
   int shift1 = 6 - head;
   int shift2 = bi ? 6 : 12 - bd;
-  int add2 = bi ? 0 : 1 << (shift2 - 1);
+  // `1i32 << (shift2 - 1)` and `sum + add2` as the reference's release build
+  // evaluates them: the shift count is masked to 5 bits (at 12 bit shift2 is 0,
+  // giving 1 << 31) and the addition wraps.
+  int add2 = bi ? 0 : (int)(1u << ((unsigned)(shift2 - 1) & 31));
   int offs = 1 << (bd + head - 1);
   if (fx == 0 && fy == 0) {
     for (int y = 0; y < ch; y++)
@@ -159,7 +165,7 @@ void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, in
     for (int x = 0; x < cw; x++) {
       int s = 0;
       for (int k = 0; k < 4; k++) s += fv[k] * tmp[(y + k) * cw + x];
-      out[y * cw + x] = bi ? (s >> shift2) - offs : clampi((s + add2) >> shift2, 0, mx);
+      out[y * cw + x] = bi ? (s >> shift2) - offs : clampi((int)((unsigned)s + (unsigned)add2) >> shift2, 0, mx);
     }
 }
 

@@ -327,8 +327,11 @@ struct SaoPass {
 
 // apply_sao_region_16 (filter.rs:1880-1947), every sample of the plane; the
 // CTU containing a sample supplies its parameters and unmodified samples are
-// copied (the reference filters a copy in place).
-__global__ void k_sao(const SaoPass* __restrict__ passes) {
+// copied (the reference filters a copy in place). For edge class 3 the
+// reference pairs the neighbour offset (1, -1) with a bounds test for (1, 1),
+// so on the first and last rows it indexes row -1 / row h and panics; here
+// such a sample raises kStatusSaoAbort and nothing outside the plane is read.
+__global__ void k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
   const SaoPass& S = passes[blockIdx.y];
   const int x = (blockIdx.x % ((S.w + 63) / 64)) * 64 + (threadIdx.x & 63);
   const int y = (blockIdx.x / ((S.w + 63) / 64)) * 4 + (threadIdx.x >> 6);
@@ -349,7 +352,9 @@ __global__ void k_sao(const SaoPass* __restrict__ passes) {
       case 2: dx = 1; dy = 1; break;
       default: dx = 1; dy = -1; break;
     }
-    if (!(x - dx < 0 || x + dx >= S.w || y - dy < 0 || y + dy >= S.h)) {
+    if (dy == -1 && !(x - dx < 0 || x + dx >= S.w) && (y == 0 || y == S.h - 1)) {
+      atomicOr(status, kStatusSaoAbort);
+    } else if (!(x - dx < 0 || x + dx >= S.w || y - dy < 0 || y + dy >= S.h)) {
       int a = S.src[(size_t)(y - dy) * st + x - dx];
       int b = S.src[(size_t)(y + dy) * st + x + dx];
       int ei = 2 + ((c > a) - (c < a)) + ((c > b) - (c < b));

@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(256) k_mc(McParams Pm, const vvcg_mc_block* __
   const int head = max(14 - bd, 2);
   const int shift1 = 6 - head;
   const int shift2 = bi ? 6 : 12 - bd;
-  const int add2 = bi ? 0 : 1 << (shift2 - 1);
+  // The reference's release build masks the shift count to 5 bits (1 << 31 at
+  // 12 bit, where shift2 is 0) and wraps the addition below.
+  const int add2 = bi ? 0 : (int)(1u << ((unsigned)(shift2 - 1) & 31));
   const int offs = 1 << (bd + head - 1);
   const int bw = B.w, bh = B.h;
   int32_t* o = out + B.out_offset;
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256) k_mc(McParams Pm, const vvcg_mc_block* __
           int x = i % tw, y = i / tw;
           int s = 0;
           for (int k = 0; k < ntap; k++) s += fv[k] * tmp[y + k][x];
-          o[(size_t)(ty0 + y) * bw + tx0 + x] = bi ? (s >> shift2) - offs : clampi((s + add2) >> shift2, 0, maxv);
+          o[(size_t)(ty0 + y) * bw + tx0 + x] = bi ? (s >> shift2) - offs : clampi((int)((unsigned)s + (unsigned)add2) >> shift2, 0, maxv);
         }
       }
     }

@@ -556,7 +556,8 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
   if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
     uint32_t maxb = 0;
     for (auto& s : ctx->sao) maxb = std::max<uint32_t>(maxb, (uint32_t)(((s.w + 63) / 64) * ((s.h + 3) / 4)));
-    k_sao<<<dim3(maxb, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p);
+    k_sao<<<dim3(maxb, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p,
+                                                                            ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
     ctx->launches++;
   }
@@ -585,6 +586,9 @@ vvcg_status vvcg_batch_sync(vvcg_ctx* ctx) {
   if (status & kStatusAlfAbort)
     return fail(ctx, VVCG_INVALID_INPUT,
                 "fixed-filter ALF reached a class >= 16, where the reference aborts");
+  if (status & kStatusSaoAbort)
+    return fail(ctx, VVCG_INVALID_INPUT,
+                "SAO edge class 3 on the first or last picture row, where the reference aborts");
   return VVCG_OK;
 }
 

@@ -12,6 +12,7 @@ enum : uint32_t {
   kStatusTimeout = 1u << 0,      // a wavefront wait ran out of polls
   kStatusBadRecord = 1u << 1,    // a record or level offset was out of range
   kStatusAlfAbort = 1u << 2,     // fixed-filter ALF reached class >= 16 (the reference aborts)
+  kStatusSaoAbort = 1u << 3,     // SAO edge class 3 on the first/last row (the reference aborts)
 };
 
 // One picture as the kernels see it (built on the host, copied to HBM).

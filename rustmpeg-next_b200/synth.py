@@ -95,11 +95,14 @@ def _tb_levels(rng, w, h, qp_scaled):
     return (mask * mag * sign).astype(np.int16)
 
 
-def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=False):
+def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=False,
+                   sao_class3_on_edges=False):
     """Build a batch of decoder records.
 
     pics_spec: iterable of dicts with keys width, height (coded, CTU multiples),
     visible_width, visible_height, bit_depth, chroma_format, ctu_log2, qp.
+    SAO edge class 3 is kept off the first and last CTU rows unless
+    sao_class3_on_edges (the reference aborts on it there).
     Returns (pics, cus, levels, ctus, aps).
     """
     rng = np.random.default_rng(seed)
@@ -158,8 +161,12 @@ def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=
                     ctus["sao"][k, c]["band_or_class"] = rng.integers(0, 32)
                     ctus["sao"][k, c]["offsets"] = rng.integers(-omax, omax + 1, 4)
                 else:
+                    eo = int(rng.integers(0, 4))
+                    row = k // (w // ctu)
+                    if eo == 3 and not sao_class3_on_edges and row in (0, h // ctu - 1):
+                        eo = 2
                     ctus["sao"][k, c]["type"] = 2
-                    ctus["sao"][k, c]["band_or_class"] = rng.integers(0, 4)
+                    ctus["sao"][k, c]["band_or_class"] = eo
                     o = rng.integers(0, omax + 1, 4)
                     ctus["sao"][k, c]["offsets"] = [o[0], o[1], -o[2], -o[3]]
         ctus["alf_luma"] = rng.random(len(ctus)) < 0.7

@@ -198,6 +198,26 @@ def test_invalid_inputs_are_rejected(ctx, pkg):
     assert out[0][0].shape == (64, 128)
 
 
+def test_sao_edge_class3_on_picture_edge_aborts_like_the_reference(ctx, pkg, orc):
+    """apply_sao_region_16 indexes row -1 for edge class 3 on the first picture
+    row (a panic in the reference); the GPU rejects the same input."""
+    from rustmpeg_next_b200 import synth
+
+    spec = [dict(width=128, height=64, bit_depth=10, chroma_format=1, ctu_log2=5, qp=27)]
+    pics, cus, levels, ctus, _ = synth.random_records(spec, seed=4, tools=pkg.TOOL_SAO)
+    ctus["sao"]["type"] = 0
+    ctus["sao"][1, 0]["type"] = 2
+    ctus["sao"][1, 0]["band_or_class"] = 3
+    ref = oracle_outputs(orc, pics, cus, levels, ctus, None)
+    assert ref[0][0] == -3
+    with pytest.raises(pkg.InvalidInput):
+        ctx.decode_batch(pkg.Batch(pics, cus, levels, ctus))
+    # class 3 inside the picture is fine
+    ctus["sao"][1, 0]["band_or_class"] = 2
+    out = ctx.decode_batch(pkg.Batch(pics, cus, levels, ctus))
+    assert_same(out, oracle_outputs(orc, pics, cus, levels, ctus, None))
+
+
 def test_fixed_filter_alf_abort_matches_the_reference(ctx, pkg, orc):
     """The reference's whole-plane fixed-filter ALF aborts when a 4x4 block's
     class is 16 or more; the GPU reports that input as invalid too."""
