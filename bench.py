@@ -1,0 +1,377 @@
+"""Benchmark: VVC reconstruction + in-loop filtering throughput (Mpx/s).
+
+Workload (one step): a batch of 128 pictures of 1920x1080 (coded 1920x1088)
+10-bit 4:2:0 = 32 frames at each of QP 22, 27, 32, 37, CTU 32, reconstructed
+(dequantisation, inverse DCT-II, intra prediction as a CTU wavefront, add/clip)
+and filtered (deblocking, SAO, ALF with an APS). Decoder records are seeded
+synthetic records with coded-picture statistics (rustmpeg-next_b200/synth.py).
+The metric counts visible luma pixels (1920x1080) per second.
+
+value : device-resident throughput (records already in HBM; the 466 MB level
+        pool and 1.6 GB of planes exceed the 126 MB L2, so no flush is needed).
+e2e   : the same through the C ABI with host buffers: every step copies the
+        records from pinned host memory, runs, and copies the visible planes
+        back to pinned host memory.
+Multi-GPU: replicas (each rank reconstructs its own batch; no collective on the
+data path); time is the max over ranks.
+
+`--impl reference` times the CPU oracle (the C++ restatement of the reference's
+single-threaded CPU decoder path) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "rustmpeg-next_b200")
+PIX_W, PIX_H, CODED_H = 1920, 1080, 1088
+QPS = (22, 27, 32, 37)
+METRIC = "VVC recon+filter Mpx/s bit-exact"
+
+
+def load_pkg():
+    if "rustmpeg_next_b200" in sys.modules:
+        return sys.modules["rustmpeg_next_b200"]
+    spec = importlib.util.spec_from_file_location(
+        "rustmpeg_next_b200", os.path.join(PKG_DIR, "__init__.py"), submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["rustmpeg_next_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload_specs(frames_per_qp):
+    return [dict(width=PIX_W, height=CODED_H, visible_width=PIX_W, visible_height=PIX_H, bit_depth=10,
+                 chroma_format=1, ctu_log2=5, qp=q) for q in QPS for _ in range(frames_per_qp)]
+
+
+def build_records(pkg, frames_per_qp, seed):
+    from rustmpeg_next_b200 import synth
+
+    tools = pkg.TOOL_DEBLOCK | pkg.TOOL_SAO | pkg.TOOL_ALF
+    return synth.random_records(workload_specs(frames_per_qp), seed=seed, tools=tools, alf_aps=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        os.unlink(self.path)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, n in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_baseline_oracle(pics, cus, levels, ctus, aps, n_pics, processes=1):
+    """Time the oracle (C++ restatement of the reference CPU path) on a bounded
+    sample of the same pictures; returns (Mpx/s, seconds, pictures)."""
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    oracle.build()
+    sample = list(range(n_pics))
+    t0 = time.perf_counter()
+    if processes <= 1:
+        for i in sample:
+            _oracle_one(pics[i], cus, levels, ctus, aps)
+    else:
+        import multiprocessing as mp
+
+        ctxm = mp.get_context("spawn")
+        with ctxm.Pool(processes) as pool:
+            pool.starmap(_oracle_one, [(pics[i], cus, levels, ctus, aps) for i in sample])
+    dt = time.perf_counter() - t0
+    return n_pics * PIX_W * PIX_H / dt / 1e6, dt, n_pics
+
+
+def _oracle_one(p, cus, levels, ctus, aps):
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    tb = min(1 << int(p["ctu_log2"]), 32)
+    n = (int(p["width"]) // tb) * (int(p["height"]) // tb)
+    nc = (int(p["width"]) >> int(p["ctu_log2"])) * (int(p["height"]) >> int(p["ctu_log2"]))
+    a = None if aps is None or int(p["alf_aps"]) < 0 else aps[int(p["alf_aps"])]
+    rc, _ = oracle.recon_frame(p, cus[int(p["cu_offset"]):][:n], levels,
+                               ctus[int(p["ctu_offset"]):][:nc], a)
+    assert rc == 0
+
+
+def run_reference(args, rank):
+    """--impl reference: the oracle on all host cores (replaces the unbuildable
+    Rust reference; bounded sample per step)."""
+    if rank != 0:
+        return
+    pkg = load_pkg()
+    cores = os.cpu_count() or 1
+    n_sample = max(2, min(cores, 16))
+    pics, cus, levels, ctus, aps = build_records(pkg, 1, seed=0x5EED0000)
+    for _ in range(args.warmup):
+        cpu_baseline_oracle(pics, cus, levels, ctus, aps, min(n_sample, len(pics)), processes=cores)
+    times = []
+    for _ in range(args.steps):
+        v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, min(n_sample, len(pics)), processes=cores)
+        times.append(dt)
+    mean = sum(times) / len(times)
+    n = min(n_sample, len(pics))
+    value = n * PIX_W * PIX_H / mean / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpx/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": {"workload": "1920x1080 10-bit 4:2:0 recon+deblock+SAO+ALF (CTU 32)",
+                       "sample_pictures_per_step": n},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
+                             "sample": f"{n} pictures of 1920x1080 per step, one process per core "
+                                       "(C++ restatement of the reference CPU path, g++ -O2)"},
+            "e2e": {"value": round(value, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames-per-qp", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=4, help="pictures in the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+
+    pkg = load_pkg()
+    pkg.build()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    pics, cus, levels, ctus, aps = build_records(pkg, args.frames_per_qp, seed=0x5EED0000 + 1000 * rank)
+    n_pics = len(pics)
+    # pinned host copies for the end-to-end leg
+    pin = lambda a: torch.from_numpy(a.view(np.uint8)).pin_memory().numpy().view(a.dtype)  # noqa: E731
+    cus_p, lev_p, ctus_p, aps_p = pin(cus), pin(levels), pin(ctus), pin(aps)
+    batch = pkg.Batch(pics, cus_p, lev_p, ctus_p, aps_p)
+    outs = [(torch.empty((PIX_H, PIX_W), dtype=torch.int16).pin_memory().numpy().view(np.uint16),
+             torch.empty((PIX_H // 2, PIX_W // 2), dtype=torch.int16).pin_memory().numpy().view(np.uint16),
+             torch.empty((PIX_H // 2, PIX_W // 2), dtype=torch.int16).pin_memory().numpy().view(np.uint16))
+            for _ in range(n_pics)]
+
+    ctx = pkg.Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream)
+    ctx.prepare(batch)
+    ctx.upload(batch)
+
+    def sync_all():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, k):
+        sync_all()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(k):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / k
+        sync_all()
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # correctness of the configuration before timing (no reference aborts)
+    ctx.run(pkg.STAGE_ALL)
+    ctx.sync()
+
+    # warm-up, then the timed device-resident steps
+    for _ in range(args.warmup):
+        ctx.run(pkg.STAGE_ALL)
+    ctx.sync()
+    launches0 = ctx.kernel_launches
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms_step = timed(lambda: ctx.run(pkg.STAGE_ALL), args.steps)
+    clocks = sampler.stop()
+    launches = ctx.kernel_launches - launches0
+    ctx.sync()
+
+    # per-stage times (each stage alone, same data) for the roofline
+    stage_ms = {}
+    for name, st in (("recon", pkg.STAGE_RECON), ("deblock", pkg.STAGE_DEBLOCK),
+                     ("sao", pkg.STAGE_SAO), ("alf", pkg.STAGE_ALF)):
+        for _ in range(2):
+            ctx.run(st)
+        stage_ms[name] = timed(lambda st=st: ctx.run(st), max(3, args.steps // 2))
+    ctx.run(pkg.STAGE_ALL)
+    ctx.sync()
+
+    # end to end through the C ABI with pinned host buffers
+    h2d = cus.nbytes + levels.nbytes + ctus.nbytes + aps.nbytes
+    d2h = n_pics * PIX_W * PIX_H * 2 * 3 // 2
+
+    def e2e_step():
+        ctx.upload(batch)
+        ctx.run(pkg.STAGE_ALL)
+        ctx.download(outs)  # synchronises the stream
+
+    for _ in range(2):
+        e2e_step()
+    sync_all()
+    t0 = time.perf_counter()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    k_e2e = max(3, args.steps // 4)
+    for _ in range(k_e2e):
+        e2e_step()
+    ev1.record(stream)
+    ev1.synchronize()
+    e2e_ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3) / k_e2e
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    px_step = n_pics * PIX_W * PIX_H
+    value = world * px_step / (ms_step * 1e-3) / 1e6
+    e2e_value = world * px_step / (e2e_ms * 1e-3) / 1e6
+
+    # roofline of the dominant stage
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    coded = n_pics * PIX_W * CODED_H * 3 // 2
+    luma = n_pics * PIX_W * CODED_H
+    alg = {"recon": levels.nbytes + cus.nbytes + 2 * coded, "deblock": 4 * coded,
+           "sao": 4 * coded, "alf": 4 * luma}
+    dom = max(stage_ms, key=stage_ms.get)
+    achieved = alg[dom] / (stage_ms[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak,
+                "unit": "GB/s", "frac": round(achieved / hbm_peak, 4), "traffic": None,
+                "peak_source": "measured" if peaks else "fallback",
+                "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+                "stages_frac": {k: round(alg[k] / (stage_ms[k] * 1e-3) / 1e9 / hbm_peak, 4)
+                                for k in stage_ms}}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        try:
+            tr = json.load(open(traffic_file))
+            if dom in tr:
+                roofline["traffic"] = tr[dom]
+        except Exception:
+            pass
+
+    line = {"metric": METRIC, "value": round(value, 2), "unit": "Mpx/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": "1920x1080 10-bit 4:2:0, 32 frames x QP{22,27,32,37} = "
+                                   f"{n_pics} pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)",
+                       "pictures_per_step": n_pics, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (466 MB levels, 1.6 GB planes); no flush",
+                       "records": "seeded synthetic decoder records"},
+            "roofline": roofline,
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mpx/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, args.cpu_sample)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
+                                "sample": f"{n} pictures of 1920x1080 from the same batch, "
+                                          f"{dt:.1f} s, one thread (C++ restatement of the "
+                                          "reference CPU path, g++ -O2)",
+                                "host_cpu": _cpu_model(), "nproc": os.cpu_count()}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _cpu_model():
+    try:
+        for l in open("/proc/cpuinfo"):
+            if l.startswith("model name"):
+                return l.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return None
+
+
+if __name__ == "__main__":
+    main()

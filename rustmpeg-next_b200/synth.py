@@ -83,16 +83,20 @@ def pad_to(plane, w, h):
     return np.pad(plane, ((0, h - ph), (0, w - pw)), mode="edge")
 
 
-def _tb_levels(rng, w, h, qp_scaled):
-    """Sparse levels concentrated at low frequencies; density falls with QP."""
+def _tb_levels(rng, n, w, h, qp_scaled):
+    """n TBs of sparse levels concentrated at low frequencies; density falls
+    with QP; every TB keeps at least its DC level (it is coded, cbf = 1)."""
     yy, xx = np.mgrid[0:h, 0:w]
     freq = (xx + yy) / (w + h)
     dens = np.clip(0.9 * np.exp(-freq * 9.0) * np.exp(-(qp_scaled - 22) / 14.0), 0.0, 0.95)
-    mask = rng.random((h, w)) < dens
-    mag = np.floor(rng.exponential(1.0 + 6.0 * np.exp(-freq * 6.0) * np.exp(-(qp_scaled - 22) / 12.0),
-                                   (h, w))).astype(np.int32) + 1
-    sign = np.where(rng.random((h, w)) < 0.5, -1, 1)
-    return (mask * mag * sign).astype(np.int16)
+    scale = 1.0 + 6.0 * np.exp(-freq * 6.0) * np.exp(-(qp_scaled - 22) / 12.0)
+    mask = rng.random((n, h, w), dtype=np.float32) < dens
+    mag = np.floor(rng.standard_exponential((n, h, w), dtype=np.float32) * scale).astype(np.int16) + 1
+    sign = np.where(rng.random((n, h, w), dtype=np.float32) < 0.5, -1, 1).astype(np.int16)
+    lv = (mask * mag * sign).astype(np.int16)
+    empty = ~lv.reshape(n, -1).any(axis=1)
+    lv[empty, 0, 0] = 1
+    return lv
 
 
 def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=False,
@@ -135,41 +139,42 @@ def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=
         chm = rng.integers(0, 70, gw * gh)
         chm = np.where(chm >= 67, 81 + (chm - 67), cus["luma_mode"])
         cus["chroma_mode"] = chm if cf else 0
-        cus["level_off"] = -1
-        for k in range(gw * gh):
-            cbf = 0
-            for c in range(3 if cf else 1):
-                if rng.random() < (0.85 if c == 0 else 0.5) * np.exp(-(qp - 22) / 30.0):
-                    bw, bh = (tb, tb) if c == 0 else (tcw, tch)
-                    lv = _tb_levels(rng, bw, bh, lqp if c == 0 else cqp)
-                    if not lv.any():
-                        lv[0, 0] = 1
-                    cus["level_off"][k, c] = n_lv
-                    lv_chunks.append(lv.ravel())
-                    n_lv += lv.size
-                    cbf |= 1 << c
-            cus["cbf"][k] = cbf
-        ctus = np.zeros((h // ctu) * (w // ctu), CTU_DTYPE)
+        ncu = gw * gh
+        lo = np.full((ncu, 3), -1, np.int32)
+        cbf = np.zeros(ncu, np.uint8)
+        for c in range(3 if cf else 1):
+            coded = rng.random(ncu) < (0.85 if c == 0 else 0.5) * np.exp(-(qp - 22) / 30.0)
+            idx = np.nonzero(coded)[0]
+            bw, bh = (tb, tb) if c == 0 else (tcw, tch)
+            if len(idx):
+                lv = _tb_levels(rng, len(idx), bw, bh, lqp if c == 0 else cqp)
+                lo[idx, c] = n_lv + np.arange(len(idx), dtype=np.int64) * (bw * bh)
+                lv_chunks.append(lv.reshape(-1))
+                n_lv += lv.size
+            cbf |= (coded.astype(np.uint8) << c)
+        cus["level_off"] = lo
+        cus["cbf"] = cbf
+        nctu = (h // ctu) * (w // ctu)
+        ctus = np.zeros(nctu, CTU_DTYPE)
         omax = (1 << (min(bd, 10) - 5)) - 1
-        for k in range(len(ctus)):
-            for c in range(3 if cf else 1):
-                r = rng.random()
-                if r > sao_prob:
-                    continue
-                if r < sao_prob / 2:
-                    ctus["sao"][k, c]["type"] = 1
-                    ctus["sao"][k, c]["band_or_class"] = rng.integers(0, 32)
-                    ctus["sao"][k, c]["offsets"] = rng.integers(-omax, omax + 1, 4)
-                else:
-                    eo = int(rng.integers(0, 4))
-                    row = k // (w // ctu)
-                    if eo == 3 and not sao_class3_on_edges and row in (0, h // ctu - 1):
-                        eo = 2
-                    ctus["sao"][k, c]["type"] = 2
-                    ctus["sao"][k, c]["band_or_class"] = eo
-                    o = rng.integers(0, omax + 1, 4)
-                    ctus["sao"][k, c]["offsets"] = [o[0], o[1], -o[2], -o[3]]
-        ctus["alf_luma"] = rng.random(len(ctus)) < 0.7
+        row = np.arange(nctu) // (w // ctu)
+        edge_row = (row == 0) | (row == h // ctu - 1)
+        for c in range(3 if cf else 1):
+            r = rng.random(nctu)
+            band = r < sao_prob / 2
+            edge = (r >= sao_prob / 2) & (r <= sao_prob)
+            eo = rng.integers(0, 4, nctu)
+            if not sao_class3_on_edges:
+                eo = np.where((eo == 3) & edge_row, 2, eo)
+            o = rng.integers(0, omax + 1, (nctu, 4))
+            ob = rng.integers(-omax, omax + 1, (nctu, 4))
+            s = ctus["sao"][:, c]
+            s["type"] = np.where(band, 1, np.where(edge, 2, 0))
+            s["band_or_class"] = np.where(band, rng.integers(0, 32, nctu), np.where(edge, eo, 0))
+            s["offsets"] = np.where(band[:, None], ob,
+                                    np.where(edge[:, None], o * np.array([1, 1, -1, -1]), 0))
+            ctus["sao"][:, c] = s
+        ctus["alf_luma"] = rng.random(nctu) < 0.7
         pics.append(p)
         cu_chunks.append(cus)
         ctu_chunks.append(ctus)
