@@ -65,8 +65,7 @@ struct vvcg_ctx {
   uint32_t spin_limit = kDefaultSpinLimit;
   uint32_t epoch = 0;
   int num_sms = 0;
-  int recon_ctas_per_sm = 0;
-  size_t recon_smem = 0;
+  uint32_t recon_c_area = 2;  // largest chroma TB area of the prepared batch
   // batch state
   bool prepared = false;
   uint32_t num_pics = 0;
@@ -210,6 +209,11 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
 
 uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
+// Shared workspace of one recon warp for chroma TBs of c_area samples.
+uint32_t recon_ws_bytes(uint32_t c_area) {
+  return align_up((uint32_t)sizeof(WarpWs) + 2u * 2u * std::max(c_area, 2u), 16);
+}
+
 template <typename T>
 vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
   if (v.empty()) return VVCG_OK;
@@ -251,11 +255,9 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     return VVCG_UNAVAILABLE;
   }
   ctx->stream = ctx->own_stream;
-  ctx->recon_smem = sizeof(ReconSmem);
+  // largest per-warp workspace: 4:4:4 chroma TBs of 32x32
   if (cudaFuncSetAttribute(k_recon_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)ctx->recon_smem) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->recon_ctas_per_sm, k_recon_wavefront,
-                                                    256, ctx->recon_smem) != cudaSuccess) {
+                           (int)(kWarpsPerCta * recon_ws_bytes(32 * 32))) != cudaSuccess) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return VVCG_UNAVAILABLE;
@@ -419,6 +421,9 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     CK(cudaMemsetAsync(ctx->flags.p, 0, ctx->flags.cap, ctx->stream), "memset flags");
   }
   ctx->flags_count = total_ctus;
+  ctx->recon_c_area = 2;
+  for (auto& P : ctx->pics)
+    ctx->recon_c_area = std::max<uint32_t>(ctx->recon_c_area, (uint32_t)(P.tb_cw * P.tb_ch));
   CK(ctx->d_cus.reserve(std::max<uint64_t>(1, b->num_cus) * sizeof(vvcg_cu_rec)), "cudaMalloc");
   CK(ctx->d_levels.reserve(std::max<uint64_t>(1, b->num_levels) * sizeof(int16_t)), "cudaMalloc");
   CK(ctx->d_ctus.reserve(std::max<uint64_t>(1, b->num_ctus) * sizeof(vvcg_ctu_filter)), "cudaMalloc");
@@ -530,10 +535,17 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
   if (mask & VVCG_STAGE_RECON) {
     ctx->epoch++;
     const uint32_t n = (uint32_t)ctx->items.size();
-    const uint32_t grid = std::min<uint32_t>(n, (uint32_t)(ctx->num_sms * std::max(1, ctx->recon_ctas_per_sm)));
-    k_recon_wavefront<<<grid, 256, ctx->recon_smem, ctx->stream>>>(
+    const uint32_t ws = recon_ws_bytes(ctx->recon_c_area);
+    const size_t smem = (size_t)kWarpsPerCta * ws;
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32, smem),
+       "occupancy");
+    const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kWarpsPerCta;
+    const uint32_t grid = (std::min<uint32_t>(n, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
+    k_recon_wavefront<<<grid, kWarpsPerCta * 32, smem, ctx->stream>>>(
         (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl,
-        (const int16_t*)ctx->d_levels.p, ctx->num_levels, ctx->epoch, ctx->spin_limit, ctrl + 1);
+        (const int16_t*)ctx->d_levels.p, ctx->num_levels, ctx->epoch, ctx->spin_limit, ctrl + 1, ws,
+        ctx->recon_c_area);
     CK(cudaGetLastError(), "recon launch");
     ctx->launches++;
   }
