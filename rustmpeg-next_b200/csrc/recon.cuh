@@ -28,6 +28,7 @@ constexpr int kTS = 34;  // row stride (int16) of the transposed coefficient til
 // Per-warp shared workspace. res_c holds two chroma TBs of up to kMaxCArea
 // samples; the coefficient tiles are reused as the CU's luma tile for CCLM.
 struct WarpWs {
+  DevPic P;  // the item's picture, copied once per item
   int16_t res_y[32 * 32];
   int16_t ct[32 * kTS];  // coefficients, transposed: ct[col * kTS + row]
   int16_t tt[32 * kTS];  // stage-1 output, transposed: tt[row * kTS + col]
@@ -98,6 +99,17 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   const bool s2 = ((lw + lh) & 1) != 0;
   const int tr_shift = 15 - bd - ((lw + lh) >> 1) - (s2 ? 1 : 0);
   int maxr = -1, maxc = -1;
+  // All of the TB's levels are fetched up front (streaming 16-byte loads, one
+  // round trip), while the coefficient tile is cleared.
+  uint4 buf[4];
+  const int nvec = n >> 8;  // uint4 per lane: 4 (1024 levels), 2 (512), 1 (256)
+  const bool vec_ok = ((reinterpret_cast<uintptr_t>(lv) & 15) == 0) && (n & 255) == 0;
+  if (vec_ok) {
+    const uint4* lv4 = reinterpret_cast<const uint4*>(lv);
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+      if (v < nvec) buf[v] = __ldcs(lv4 + lane + 32 * v);
+  }
   // clear the coefficient tile rows that the dot products read (k < 32)
   for (int i = lane; i < w * (kTS / 2); i += 32) reinterpret_cast<uint32_t*>(W.ct)[i] = 0;
   __syncwarp();
@@ -106,15 +118,29 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     const int qp_per = qp / 6, qp_rem = qp % 6;
     const int rs = 6 - (tr_shift + qp_per);
     const long long scale = c_inv_quant_scale[s2 ? 1 : 0][qp_rem];
-    for (int i = lane; i < n; i += 32) {
-      int L = lv[i];
-      if (L != 0) {
-        int r = i >> lw, c = i & (w - 1);
-        maxr = max(maxr, r);
-        maxc = max(maxc, c);
-        long long val = (long long)L * scale;
-        long long sc = rs > 0 ? (val + (1ll << (rs - 1))) >> rs : val << (-rs);
-        W.ct[c * kTS + r] = (int16_t)clip16(sc);
+    auto put = [&](int i, int L) {
+      int r = i >> lw, c = i & (w - 1);
+      maxr = max(maxr, r);
+      maxc = max(maxc, c);
+      long long val = (long long)L * scale;
+      long long sc = rs > 0 ? (val + (1ll << (rs - 1))) >> rs : val << (-rs);
+      W.ct[c * kTS + r] = (int16_t)clip16(sc);
+    };
+    if (vec_ok) {
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        if (v < nvec) {
+          const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
+            if (L != 0) put(8 * (lane + 32 * v) + e, L);
+          }
+        }
+    } else {
+      for (int i = lane; i < n; i += 32) {
+        int L = lv[i];
+        if (L != 0) put(i, L);
       }
     }
   } else {
@@ -126,13 +152,27 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     const int16_t* scan = g_scan + g_scan_off[(lw - 1) * 6 + (lh - 1)];
     const int ns = min(w, 32) * min(h, 32);
     int last = -1;
-    for (int i = lane; i < n; i += 32) {
-      int L = lv[i];
-      if (L != 0) {
-        int r = i >> lw, c = i & (w - 1);
-        maxr = max(maxr, r);
-        maxc = max(maxc, c);
-        W.ct[c * kTS + r] = (int16_t)L;
+    auto put = [&](int i, int L) {
+      int r = i >> lw, c = i & (w - 1);
+      maxr = max(maxr, r);
+      maxc = max(maxc, c);
+      W.ct[c * kTS + r] = (int16_t)L;
+    };
+    if (vec_ok) {
+#pragma unroll
+      for (int v = 0; v < 4; v++)
+        if (v < nvec) {
+          const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
+#pragma unroll
+          for (int e = 0; e < 8; e++) {
+            int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
+            if (L != 0) put(8 * (lane + 32 * v) + e, L);
+          }
+        }
+    } else {
+      for (int i = lane; i < n; i += 32) {
+        int L = lv[i];
+        if (L != 0) put(i, L);
       }
     }
     __syncwarp();
@@ -266,7 +306,11 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
     it = __shfl_sync(0xffffffffu, it, 0);
     if (it >= n_items) break;
     const CtuItem item = items[it];
-    const DevPic& P = pics[item.pic];
+    static_assert(sizeof(DevPic) % 4 == 0 && sizeof(DevPic) <= 64 * 4, "DevPic copy");
+    for (int i = lane; i < (int)(sizeof(DevPic) / 4); i += 32)
+      reinterpret_cast<uint32_t*>(&W.P)[i] = reinterpret_cast<const uint32_t*>(&pics[item.pic])[i];
+    __syncwarp();
+    const DevPic& P = W.P;
     const int cx = item.cx, cy = item.cy;
     const int tb = P.tb, ctu_log2 = P.ctu_log2, sh = ctu_log2 - ilog2(tb);
     const int ncu = 1 << (2 * sh);
