@@ -163,15 +163,21 @@ __device__ void warp_filter_refs(int w, int h, IntraWs& S) {
   __syncwarp();
 }
 
-// Writes clip(pred + res) for sample pairs (x, x+1) of row y as one 32-bit store.
+// Writes clip(pred + res) for sample pairs (x, x+1) of row y as one 32-bit
+// store. `res` (nullable) points at the block's residual in a plane-strided
+// int16 buffer; `keep` (nullable) receives the block (int16 raster, width w).
 __device__ __forceinline__ void store_pair(const DevPic& P, int comp, int x0, int y0, int w, int x,
                                            int y, int p0, int p1, const int16_t* res, int16_t* keep,
                                            int maxv) {
-  int v0 = clampi(p0 + res[y * w + x], 0, maxv);
-  int v1 = clampi(p1 + res[y * w + x + 1], 0, maxv);
+  if (res) {
+    uint32_t rv = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * P.stride[comp] + x));
+    p0 += (int)(int16_t)(rv & 0xFFFFu);
+    p1 += (int)(int16_t)(rv >> 16);
+  }
+  const int v0 = clampi(p0, 0, maxv), v1 = clampi(p1, 0, maxv);
   uint16_t* dst = P.plane[comp] + (size_t)(y0 + y) * P.stride[comp] + x0 + x;
   *reinterpret_cast<uint32_t*>(dst) = (uint32_t)v0 | ((uint32_t)v1 << 16);
-  if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = (uint32_t)(uint16_t)v0 | ((uint32_t)v1 << 16);
+  if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = (uint32_t)v0 | ((uint32_t)v1 << 16);
 }
 
 // Intra prediction of one block fused with reconstruction: gathers the
@@ -299,60 +305,72 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
   const int16_t* rm = p.is_ver ? S.ref_above : S.ref_left;
   const int16_t* rs = p.is_ver ? S.ref_left : S.ref_above;
   const int ww = p.is_ver ? w : h, wh = p.is_ver ? h : w;
-  const bool int_slope = (abs(p.angle) & 0x1F) == 0;
-  const int sc0 = (ilog2(ww) + ilog2(wh) - 2) >> 2;
-  const int sca = max(0, p.scale);
-  for (int q = lane; q < npair; q += 32) {
-    const int oy = (2 * q) >> lw, ox0 = (2 * q) & (w - 1);
-    int v[2];
+  if (p.angle == 0) {
+    const int sc0 = (ilog2(ww) + ilog2(wh) - 2) >> 2;
+    const int lim = p.pdpc ? min(3 << sc0, ww) : 0;
+    for (int q = lane; q < npair; q += 32) {
+      const int oy = (2 * q) >> lw, ox0 = (2 * q) & (w - 1);
+      int v[2];
 #pragma unroll
-    for (int t = 0; t < 2; t++) {
-      const int ox = ox0 + t;
-      const int x = p.is_ver ? ox : oy, yy = p.is_ver ? oy : ox;  // work coordinates
-      int val;
-      if (p.angle == 0) {
-        val = rm[base + x + 1];
-        if (p.pdpc && x < min(3 << sc0, ww)) {
+      for (int t = 0; t < 2; t++) {
+        const int ox = ox0 + t;
+        const int x = p.is_ver ? ox : oy, yy = p.is_ver ? oy : ox;  // work coordinates
+        int val = rm[base + x + 1];
+        if (x < lim) {
           int wl = 32 >> ((2 * x) >> sc0);
           val = clampi(val + ((wl * (rs[base + 1 + yy] - rm[base]) + 32) >> 6), 0, maxv);
         }
-      } else {
-        const int dp = p.angle * (yy + 1);
-        const int di = dp >> 5, fr = dp & 31;
-        if (!int_slope) {
-          if (is_luma) {
-            int f0, f1, f2, f3;
-            if (p.interp) {
-              f0 = 16 - (fr >> 1);
-              f1 = 32 - (fr >> 1);
-              f2 = 16 + (fr >> 1);
-              f3 = fr >> 1;
-            } else {
-              f0 = c_chroma_taps4[fr * 4 + 0];
-              f1 = c_chroma_taps4[fr * 4 + 1];
-              f2 = c_chroma_taps4[fr * 4 + 2];
-              f3 = c_chroma_taps4[fr * 4 + 3];
-            }
-            const int j = base + di + x;
-            val = clampi((f0 * rm[j] + f1 * rm[j + 1] + f2 * rm[j + 2] + f3 * rm[j + 3] + 32) >> 6, 0, maxv);
-          } else {
-            const int j = base + di + x + 1;
-            const int p0 = rm[j], p1 = rm[j + 1];
-            val = clampi(p0 + ((fr * (p1 - p0) + 16) >> 5), 0, maxv);
-          }
-        } else {
-          val = clampi(rm[base + di + x + 1], 0, maxv);
-        }
-        if (p.pdpc && x < min(3 << sca, ww)) {
-          const int inv_sum = 256 + (x + 1) * p.abs_inv;
-          const int wl = 32 >> ((2 * x) >> sca);
-          const int li = min(base + yy + (inv_sum >> 9) + 1, buf_len - 1);
-          val = clampi(val + ((wl * (rs[li] - val) + 32) >> 6), 0, maxv);
-        }
+        v[t] = val;
       }
-      v[t] = val;
+      store_pair(P, comp, x0, y0, w, ox0, oy, v[0], v[1], res, keep, maxv);
     }
-    store_pair(P, comp, x0, y0, w, ox0, oy, v[0], v[1], res, keep, maxv);
+    __syncwarp();
+    return;
+  }
+  // Every non-zero-angle case is one 4-tap filter over rm[j..j+3], j = base + di + x:
+  // integer slopes take rm[j+1] (taps 0,64,0,0: (64v + 32) >> 6 == v); chroma's
+  // linear p0 + ((f (p1 - p0) + 16) >> 5) with p0 = rm[j+1] equals taps
+  // 0, 2(32-f), 2f, 0; luma non-integer slopes use the Gaussian or cubic taps.
+  const int kind = (abs(p.angle) & 0x1F) == 0 ? 0 : (!is_luma ? 1 : (p.interp ? 2 : 3));
+  const int sca = max(0, p.scale);
+  const int lim = p.pdpc ? min(3 << sca, ww) : 0;
+  auto sample = [&](int x, int yy) -> int {
+    const int dp = p.angle * (yy + 1);
+    const int di = dp >> 5, fr = dp & 31;
+    int f0, f1, f2, f3;
+    if (kind == 0) {
+      f0 = 0; f1 = 64; f2 = 0; f3 = 0;
+    } else if (kind == 1) {
+      f0 = 0; f1 = 2 * (32 - fr); f2 = 2 * fr; f3 = 0;
+    } else if (kind == 2) {
+      f0 = 16 - (fr >> 1); f1 = 32 - (fr >> 1); f2 = 16 + (fr >> 1); f3 = fr >> 1;
+    } else {
+      f0 = c_chroma_taps4[fr * 4 + 0];
+      f1 = c_chroma_taps4[fr * 4 + 1];
+      f2 = c_chroma_taps4[fr * 4 + 2];
+      f3 = c_chroma_taps4[fr * 4 + 3];
+    }
+    const int j = base + di + x;
+    int val = clampi((f0 * rm[j] + f1 * rm[j + 1] + f2 * rm[j + 2] + f3 * rm[j + 3] + 32) >> 6, 0, maxv);
+    if (x < lim) {
+      const int inv_sum = 256 + (x + 1) * p.abs_inv;
+      const int wl = 32 >> ((2 * x) >> sca);
+      const int li = min(base + yy + (inv_sum >> 9) + 1, buf_len - 1);
+      val = clampi(val + ((wl * (rs[li] - val) + 32) >> 6), 0, maxv);
+    }
+    return val;
+  };
+  for (int q = lane; q < npair; q += 32) {
+    const int oy = (2 * q) >> lw, ox0 = (2 * q) & (w - 1);
+    int v0, v1;
+    if (p.is_ver) {
+      v0 = sample(ox0, oy);
+      v1 = sample(ox0 + 1, oy);
+    } else {
+      v0 = sample(oy, ox0);
+      v1 = sample(oy, ox0 + 1);
+    }
+    store_pair(P, comp, x0, y0, w, ox0, oy, v0, v1, res, keep, maxv);
   }
   __syncwarp();
 }

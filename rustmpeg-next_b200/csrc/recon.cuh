@@ -1,20 +1,22 @@
-// Reconstruction of the 8..12-bit frame path on the GPU: a persistent
-// wavefront kernel in which every warp works on its own CTU.
+// Reconstruction of the 8..12-bit frame path on the GPU, in two kernels.
 //
-// Work items are CTUs handed out by an atomic counter in wavefront order
+// k_residual: every coded TB of the batch is dequantised and inverse
+// transformed by one warp, with no dependencies between TBs; the int16
+// residual goes to the picture's scratch planes (free until SAO runs).
+//
+// k_recon_wavefront: a persistent kernel in which every warp works on its own
+// CTU. Work items are CTUs handed out by an atomic counter in wavefront order
 // (diagonal t = cx + 2*cy, across all pictures of the batch), so a warp only
-// ever waits on items that running warps already hold and the schedule
-// cannot deadlock. For each coding unit the warp first dequantises and
-// inverse-transforms the residuals of its three TBs (independent of the
-// neighbours, so this overlaps the wait), then waits (bounded) for the left
-// and top-right CTUs, then predicts, adds, clips and stores.
+// ever waits on items that running warps already hold and the schedule cannot
+// deadlock. For each coding unit the warp waits (bounded) for the left and
+// top-right CTUs, then predicts, adds the residual, clips and stores.
 //
 // Follows slice::decode_vvc_frame_picture_with_chroma_qp (slice.rs:4834-4988):
-// predict_coded_block_16 / predict_cclm_with_format_16 prediction (see
-// intra.cuh), dequantize_rect_bd or dequantize_dep_quant_bd (dct.rs:1151,
-// :1191), inverse_transform_rect_bd (dct.rs:996) with DCT-II both ways, and the
-// add/clip to 0..2^bd-1. All sums are exact in int32, so reassociating the
-// matrix products (dp2a pairs) gives the reference's results bit for bit.
+// predict_coded_block_16 / predict_cclm_with_format_16 prediction (intra.cuh),
+// dequantize_rect_bd or dequantize_dep_quant_bd (dct.rs:1151, :1191),
+// inverse_transform_rect_bd (dct.rs:996) with DCT-II both ways, and the add /
+// clip to 0..2^bd-1. All sums are exact in int32, so reassociating the matrix
+// products (dp2a pairs) gives the reference's results bit for bit.
 #pragma once
 #include "intra.cuh"
 #include "vvcg_device.cuh"
@@ -25,15 +27,9 @@ namespace vvcg {
 constexpr int kWarpsPerCta = 8;
 constexpr int kTS = 34;  // row stride (int16) of the transposed coefficient tiles
 
-// Per-warp shared workspace. res_c holds two chroma TBs of up to kMaxCArea
-// samples; the coefficient tiles are reused as the CU's luma tile for CCLM.
-struct WarpWs {
-  DevPic P;  // the item's picture, copied once per item
-  int16_t res_y[32 * 32];
+struct ResidWs {
   int16_t ct[32 * kTS];  // coefficients, transposed: ct[col * kTS + row]
   int16_t tt[32 * kTS];  // stage-1 output, transposed: tt[row * kTS + col]
-  IntraWs in;
-  // followed by int16_t res_c[2][max chroma TB area]
 };
 
 // Matrix columns held in registers: lane j keeps M[k][j] of the 32-point
@@ -64,8 +60,8 @@ __device__ __forceinline__ void load_mat_regs(MatRegs& R) {
   }
 }
 
-// sum_k M[k][j] * v[k] for k < 4*ng, with v given as int16 pairs in a
-// transposed tile row (v[k] at row[k]); M from the lane's registers.
+// sum_k M[k][j] * v[k] for k < 4*ng, v given as int16 pairs (a transposed tile
+// row, v[k] at row[k]), M from the lane's registers.
 template <int N>
 __device__ __forceinline__ int dot_col(const MatRegs& R, const int16_t* row, int ng) {
   const uint32_t* r2 = reinterpret_cast<const uint32_t*>(row);
@@ -90,10 +86,10 @@ __device__ __forceinline__ int dot_col(const MatRegs& R, const int16_t* row, int
 
 // Dequantisation (regular or dependent) and 2-D inverse DCT-II of a w x h TB
 // (w, h in {16, 32}) whose int16 raster levels start at `lv`; the residual is
-// written to `res` (int16, raster). Rows/columns past the last nonzero level
-// hold zeros and are skipped without changing any sum.
+// stored to `out` (int16, row stride `ostride`). Rows/columns past the last
+// nonzero level hold zeros and are skipped without changing any sum.
 __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int qp_scaled, int bd,
-                              bool dq, const MatRegs& R, WarpWs& W, int16_t* res) {
+                              bool dq, const MatRegs& R, ResidWs& W, int16_t* out, int ostride) {
   const int lane = threadIdx.x & 31;
   const int n = w * h, lw = ilog2(w), lh = ilog2(h);
   const bool s2 = ((lw + lh) & 1) != 0;
@@ -110,72 +106,50 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     for (int v = 0; v < 4; v++)
       if (v < nvec) buf[v] = __ldcs(lv4 + lane + 32 * v);
   }
-  // clear the coefficient tile rows that the dot products read (k < 32)
   for (int i = lane; i < w * (kTS / 2); i += 32) reinterpret_cast<uint32_t*>(W.ct)[i] = 0;
   __syncwarp();
-  if (!dq) {
-    const int qp = max(4, qp_scaled);
-    const int qp_per = qp / 6, qp_rem = qp % 6;
-    const int rs = 6 - (tr_shift + qp_per);
-    const long long scale = c_inv_quant_scale[s2 ? 1 : 0][qp_rem];
-    auto put = [&](int i, int L) {
-      int r = i >> lw, c = i & (w - 1);
-      maxr = max(maxr, r);
-      maxc = max(maxc, c);
+  // level -> tile (regular dequantisation applied here, dct.rs:1151-1187)
+  const int qp = max(4, qp_scaled);
+  const int rs = 6 - (tr_shift + qp / 6);
+  const int scale = c_inv_quant_scale[s2 ? 1 : 0][qp % 6];
+  auto put = [&](int i, int L) {
+    int r = i >> lw, c = i & (w - 1);
+    maxr = max(maxr, r);
+    maxc = max(maxc, c);
+    int v = L;
+    if (!dq) {
       long long val = (long long)L * scale;
-      long long sc = rs > 0 ? (val + (1ll << (rs - 1))) >> rs : val << (-rs);
-      W.ct[c * kTS + r] = (int16_t)clip16(sc);
-    };
-    if (vec_ok) {
-#pragma unroll
-      for (int v = 0; v < 4; v++)
-        if (v < nvec) {
-          const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
-            if (L != 0) put(8 * (lane + 32 * v) + e, L);
-          }
-        }
-    } else {
-      for (int i = lane; i < n; i += 32) {
-        int L = lv[i];
-        if (L != 0) put(i, L);
-      }
+      v = clip16(rs > 0 ? (val + (1ll << (rs - 1))) >> rs : val << (-rs));
     }
+    W.ct[c * kTS + r] = (int16_t)v;
+  };
+  if (vec_ok) {
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+      if (v < nvec) {
+        const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+          int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
+          if (L != 0) put(8 * (lane + 32 * v) + e, L);
+        }
+      }
   } else {
+    for (int i = lane; i < n; i += 32) {
+      int L = lv[i];
+      if (L != 0) put(i, L);
+    }
+  }
+  if (dq) {
     // dequantize_dep_quant_bd (dct.rs:1191-1248): the 4-state machine walks the
     // grouped diagonal scan backwards from the last nonzero level. The walk is
     // split into 32 chunks; each lane composes its chunk's state transitions,
     // a warp scan of the compositions gives each chunk's entry state, then
     // every lane replays its chunk.
+    __syncwarp();
     const int16_t* scan = g_scan + g_scan_off[(lw - 1) * 6 + (lh - 1)];
     const int ns = min(w, 32) * min(h, 32);
     int last = -1;
-    auto put = [&](int i, int L) {
-      int r = i >> lw, c = i & (w - 1);
-      maxr = max(maxr, r);
-      maxc = max(maxc, c);
-      W.ct[c * kTS + r] = (int16_t)L;
-    };
-    if (vec_ok) {
-#pragma unroll
-      for (int v = 0; v < 4; v++)
-        if (v < nvec) {
-          const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
-#pragma unroll
-          for (int e = 0; e < 8; e++) {
-            int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
-            if (L != 0) put(8 * (lane + 32 * v) + e, L);
-          }
-        }
-    } else {
-      for (int i = lane; i < n; i += 32) {
-        int L = lv[i];
-        if (L != 0) put(i, L);
-      }
-    }
-    __syncwarp();
     for (int s = lane; s < ns; s += 32) {
       int r = scan[s];
       if (W.ct[(r & (w - 1)) * kTS + (r >> lw)] != 0) last = max(last, s);
@@ -229,9 +203,11 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   maxr = __reduce_max_sync(0xffffffffu, maxr);
   maxc = __reduce_max_sync(0xffffffffu, maxc);
   __syncwarp();
-  if (maxr < 0) {
-    for (int i = lane; i < n / 2; i += 32) reinterpret_cast<uint32_t*>(res)[i] = 0;
-    __syncwarp();
+  if (maxr < 0) {  // all levels zero (cbf set without levels): residual 0
+    for (int i = lane; i < n / 2; i += 32) {
+      int y = (2 * i) >> lw, x = (2 * i) & (w - 1);
+      *reinterpret_cast<uint32_t*>(&out[(size_t)y * ostride + x]) = 0;
+    }
     return;
   }
   // Stage 1, columns (dct.rs:1075-1087): tt[j][i] = clip16((sum_k Mv[k][j] ct[i][k] + 64) >> 7)
@@ -251,7 +227,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
       }
     }
   }
-  // tt columns past maxc must read as zero in stage 2
+  // tt columns past maxc that stage 2 reads must be zero
   if (maxc + 1 < w)
     for (int i = lane; i < h * 4; i += 32) {
       int row = i >> 2, c = maxc + 1 + (i & 3);
@@ -264,18 +240,56 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   if (w == 32) {
     for (int y = 0; y < h; y++) {
       int acc = dot_col<32>(R, &W.tt[y * kTS], ngc);
-      res[y * 32 + lane] = (int16_t)clip16i((acc + add2) >> sh2);
+      out[(size_t)y * ostride + lane] = (int16_t)clip16i((acc + add2) >> sh2);
     }
   } else {
     const int x = lane & 15;
     for (int y0 = 0; y0 < h; y0 += 2) {
       int y = y0 + (lane >> 4);
       int acc = dot_col<16>(R, &W.tt[y * kTS], ngc);
-      res[y * 16 + x] = (int16_t)clip16i((acc + add2) >> sh2);
+      out[(size_t)y * ostride + x] = (int16_t)clip16i((acc + add2) >> sh2);
     }
   }
   __syncwarp();
 }
+
+// One warp per coding unit: the residuals of its coded TBs go to the scratch
+// planes at the TB's position. Grid: (ceil(max CUs per picture / 8), pictures).
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
+k_residual(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels,
+           uint32_t* status) {
+  __shared__ ResidWs ws[kWarpsPerCta];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const DevPic& P = pics[blockIdx.y];
+  const int cu = blockIdx.x * kWarpsPerCta + wid;
+  if (cu >= P.grid_w * P.grid_h) return;
+  MatRegs R;
+  load_mat_regs(R);
+  const vvcg_cu_rec rec = P.cus[cu];
+  const int gx = cu % P.grid_w, gy = cu / P.grid_w;
+  const bool dq = (P.tools & VVCG_TOOL_DEP_QUANT) != 0;
+  for (int c = 0; c < (P.cf ? 3 : 1); c++) {
+    if (!((rec.cbf >> c) & 1)) continue;
+    const int off = rec.level_off[c];
+    if (off < 0) continue;
+    const int w = c ? P.tb_cw : P.tb, h = c ? P.tb_ch : P.tb;
+    if ((uint64_t)off + (uint64_t)(w * h) > n_levels) {
+      if (lane == 0) atomicOr(status, kStatusBadRecord);
+      continue;
+    }
+    const int x0 = c ? gx * P.tb / P.sub_w : gx * P.tb, y0 = c ? gy * P.tb / P.sub_h : gy * P.tb;
+    int16_t* out = reinterpret_cast<int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0;
+    warp_residual(levels + off, w, h, c ? P.cqp : P.lqp, P.bd, dq, R, ws[wid], out, P.stride[c]);
+  }
+}
+
+// Per-warp shared workspace of the wavefront kernel.
+struct WaveWs {
+  DevPic P;                        // the item's picture, copied once per item
+  IntraWs in;                      // reference samples of the current block
+  int16_t luma[32 * 32];           // the CU's reconstructed luma (for CCLM)
+  int16_t ds[32 * 32];             // CCLM downsampled luma
+};
 
 // Bounded wait for a CTU flag; returns false when the poll limit ran out.
 __device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t epoch, uint32_t limit) {
@@ -288,18 +302,13 @@ __device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t epoch, 
   return ld_acquire(flag) == epoch;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 3)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items,
-                  uint32_t n_items, uint32_t* counter, const int16_t* __restrict__ levels,
-                  uint64_t n_levels, uint32_t epoch, uint32_t spin_limit, uint32_t* status,
-                  uint32_t ws_bytes, uint32_t c_area) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+                  uint32_t n_items, uint32_t* counter, uint32_t epoch, uint32_t spin_limit,
+                  uint32_t* status) {
+  __shared__ WaveWs wsa[kWarpsPerCta];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  WarpWs& W = *reinterpret_cast<WarpWs*>(smem_raw + (size_t)wid * ws_bytes);
-  int16_t* res_c0 = reinterpret_cast<int16_t*>(smem_raw + (size_t)wid * ws_bytes + sizeof(WarpWs));
-  int16_t* res_c1 = res_c0 + c_area;
-  MatRegs R;
-  load_mat_regs(R);
+  WaveWs& W = wsa[wid];
   for (;;) {
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(counter, 1u);
@@ -312,10 +321,22 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
     __syncwarp();
     const DevPic& P = W.P;
     const int cx = item.cx, cy = item.cy;
-    const int tb = P.tb, ctu_log2 = P.ctu_log2, sh = ctu_log2 - ilog2(tb);
+    const int tb = P.tb, sh = P.ctu_log2 - ilog2(tb);
     const int ncu = 1 << (2 * sh);
-    const int cf = P.cf, bd = P.bd;
-    const bool dq = (P.tools & VVCG_TOOL_DEP_QUANT) != 0;
+    {
+      int ok = 1;
+      if (lane == 0) {
+        // once any wait has given up the batch result is void: skip the rest
+        ok = (ld_acquire(status) & kStatusTimeout) == 0;
+        if (ok && cx > 0) ok = wait_flag(&P.ctu_done[cy * P.ctu_w + cx - 1], epoch, spin_limit);
+        if (ok && cy > 0) {
+          int tx = cx + 1 < P.ctu_w ? cx + 1 : cx;
+          ok = wait_flag(&P.ctu_done[(cy - 1) * P.ctu_w + tx], epoch, spin_limit);
+        }
+        if (!ok) atomicOr(status, kStatusTimeout);
+      }
+      __syncwarp();
+    }
     for (int k = 0; k < ncu; k++) {
       int lx = 0, ly = 0;
       for (int b = 0; b < sh; b++) {
@@ -324,52 +345,27 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
       }
       const int gx = (cx << sh) + lx, gy = (cy << sh) + ly;
       const vvcg_cu_rec rec = P.cus[gy * P.grid_w + gx];
-      // residuals of the three TBs
-      for (int c = 0; c < (cf ? 3 : 1); c++) {
-        const int w = c ? P.tb_cw : tb, h = c ? P.tb_ch : tb;
-        int16_t* res = c == 0 ? W.res_y : (c == 1 ? res_c0 : res_c1);
-        const int off = rec.level_off[c];
-        const bool has = ((rec.cbf >> c) & 1) && off >= 0;
-        if (has && (uint64_t)off + (uint64_t)(w * h) <= n_levels) {
-          warp_residual(levels + off, w, h, c ? P.cqp : P.lqp, bd, dq, R, W, res);
-        } else {
-          if (has && lane == 0) atomicOr(status, kStatusBadRecord);
-          for (int i = lane; i < w * h / 2; i += 32) reinterpret_cast<uint32_t*>(res)[i] = 0;
-          __syncwarp();
-        }
-      }
-      if (k == 0) {
-        int ok = 1;
-        if (lane == 0) {
-          // once any wait has given up the batch result is void: skip the rest
-          ok = (ld_acquire(status) & kStatusTimeout) == 0;
-          if (ok && cx > 0) ok = wait_flag(&P.ctu_done[cy * P.ctu_w + cx - 1], epoch, spin_limit);
-          if (ok && cy > 0) {
-            int tx = cx + 1 < P.ctu_w ? cx + 1 : cx;
-            ok = wait_flag(&P.ctu_done[(cy - 1) * P.ctu_w + tx], epoch, spin_limit);
-          }
-          if (!ok) atomicOr(status, kStatusTimeout);
-        }
-        __syncwarp();
-      }
       const int bx = gx * tb, by = gy * tb;
       const uint32_t order = cu_order(P, gx, gy);
-      // luma; the reconstructed block is also kept in W.ct for CCLM
-      int16_t* luma_tile = W.ct;
-      warp_predict_store(P, 0, bx, by, tb, tb, true, rec.luma_mode <= 69 ? rec.luma_mode : 0, order,
-                         W.in, W.res_y, luma_tile);
-      if (cf) {
+      auto resid = [&](int c, int x0, int y0) -> const int16_t* {
+        return ((rec.cbf >> c) & 1) && rec.level_off[c] >= 0
+                   ? reinterpret_cast<const int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0
+                   : nullptr;
+      };
+      warp_predict_store(P, 0, bx, by, tb, tb, true, rec.luma_mode <= 69 ? rec.luma_mode : 0,
+                         order, W.in, resid(0, bx, by), W.luma);
+      if (P.cf) {
         const int cxp = bx / P.sub_w, cyp = by / P.sub_h;
         const int chm = rec.chroma_mode;
         if (chm >= 81 && chm <= 83) {
-          warp_cclm_downsample(P, cxp, cyp, P.tb_cw, P.tb_ch, bx, by, tb, luma_tile, W.in, W.tt);
+          warp_cclm_downsample(P, cxp, cyp, P.tb_cw, P.tb_ch, bx, by, tb, W.luma, W.in, W.ds);
           for (int c = 1; c <= 2; c++)
-            warp_cclm_predict_store(P, c, cxp, cyp, P.tb_cw, P.tb_ch, chm - 81, W.in, W.tt,
-                                    c == 1 ? res_c0 : res_c1);
+            warp_cclm_predict_store(P, c, cxp, cyp, P.tb_cw, P.tb_ch, chm - 81, W.in, W.ds,
+                                    resid(c, cxp, cyp));
         } else {
           for (int c = 1; c <= 2; c++)
             warp_predict_store(P, c, cxp, cyp, P.tb_cw, P.tb_ch, false, chm <= 69 ? chm : 0, order,
-                               W.in, c == 1 ? res_c0 : res_c1, nullptr);
+                               W.in, resid(c, cxp, cyp), nullptr);
         }
       }
     }

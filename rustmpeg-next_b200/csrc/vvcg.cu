@@ -65,7 +65,6 @@ struct vvcg_ctx {
   uint32_t spin_limit = kDefaultSpinLimit;
   uint32_t epoch = 0;
   int num_sms = 0;
-  uint32_t recon_c_area = 2;  // largest chroma TB area of the prepared batch
   // batch state
   bool prepared = false;
   uint32_t num_pics = 0;
@@ -209,11 +208,6 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
 
 uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
-// Shared workspace of one recon warp for chroma TBs of c_area samples.
-uint32_t recon_ws_bytes(uint32_t c_area) {
-  return align_up((uint32_t)sizeof(WarpWs) + 2u * 2u * std::max(c_area, 2u), 16);
-}
-
 template <typename T>
 vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
   if (v.empty()) return VVCG_OK;
@@ -255,13 +249,6 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     return VVCG_UNAVAILABLE;
   }
   ctx->stream = ctx->own_stream;
-  // largest per-warp workspace: 4:4:4 chroma TBs of 32x32
-  if (cudaFuncSetAttribute(k_recon_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)(kWarpsPerCta * recon_ws_bytes(32 * 32))) != cudaSuccess) {
-    cudaStreamDestroy(ctx->own_stream);
-    delete ctx;
-    return VVCG_UNAVAILABLE;
-  }
   if (upload_tables(ctx) != VVCG_OK) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -421,9 +408,6 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     CK(cudaMemsetAsync(ctx->flags.p, 0, ctx->flags.cap, ctx->stream), "memset flags");
   }
   ctx->flags_count = total_ctus;
-  ctx->recon_c_area = 2;
-  for (auto& P : ctx->pics)
-    ctx->recon_c_area = std::max<uint32_t>(ctx->recon_c_area, (uint32_t)(P.tb_cw * P.tb_ch));
   CK(ctx->d_cus.reserve(std::max<uint64_t>(1, b->num_cus) * sizeof(vvcg_cu_rec)), "cudaMalloc");
   CK(ctx->d_levels.reserve(std::max<uint64_t>(1, b->num_levels) * sizeof(int16_t)), "cudaMalloc");
   CK(ctx->d_ctus.reserve(std::max<uint64_t>(1, b->num_ctus) * sizeof(vvcg_ctu_filter)), "cudaMalloc");
@@ -534,18 +518,24 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
   CK(cudaMemsetAsync(ctrl, 0, 2 * sizeof(uint32_t), ctx->stream), "memset");
   if (mask & VVCG_STAGE_RECON) {
     ctx->epoch++;
+    // residuals of every coded TB (no dependencies), into the scratch planes
+    uint32_t max_cus = 0;
+    for (auto& P : ctx->pics) max_cus = std::max<uint32_t>(max_cus, (uint32_t)(P.grid_w * P.grid_h));
+    k_residual<<<dim3((max_cus + kWarpsPerCta - 1) / kWarpsPerCta, ctx->num_pics), kWarpsPerCta * 32, 0,
+                 ctx->stream>>>((const DevPic*)ctx->d_pics.p, (const int16_t*)ctx->d_levels.p,
+                                ctx->num_levels, ctrl + 1);
+    CK(cudaGetLastError(), "residual launch");
+    ctx->launches++;
+    // prediction + reconstruction in CTU wavefront order
     const uint32_t n = (uint32_t)ctx->items.size();
-    const uint32_t ws = recon_ws_bytes(ctx->recon_c_area);
-    const size_t smem = (size_t)kWarpsPerCta * ws;
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32, smem),
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32, 0),
        "occupancy");
     const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kWarpsPerCta;
     const uint32_t grid = (std::min<uint32_t>(n, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
-    k_recon_wavefront<<<grid, kWarpsPerCta * 32, smem, ctx->stream>>>(
-        (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl,
-        (const int16_t*)ctx->d_levels.p, ctx->num_levels, ctx->epoch, ctx->spin_limit, ctrl + 1, ws,
-        ctx->recon_c_area);
+    k_recon_wavefront<<<grid, kWarpsPerCta * 32, 0, ctx->stream>>>(
+        (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
+        ctx->spin_limit, ctrl + 1);
     CK(cudaGetLastError(), "recon launch");
     ctx->launches++;
   }
