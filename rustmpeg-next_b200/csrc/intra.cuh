@@ -93,12 +93,14 @@ __device__ __forceinline__ AngP angular_params(int dir, int w, int h, bool is_lu
   return p;
 }
 
+
 __device__ __forceinline__ int ldp(const uint16_t* p) { return __ldcg(p); }
 
 // Reference samples with the frame path's availability rules:
 // gather_references_16 (predict.rs:3016-3076) followed by the coded-unit
-// substitution of predict_coded_block_16 (predict.rs:3101-3135). Reads go to
-// L2 (ld.cg): the samples were written by other SMs.
+// substitution of predict_coded_block_16 (predict.rs:3101-3135). All loads of a
+// lane are issued before any is used (one L2 round trip); reads go to L2
+// (ld.cg) because the samples were written by other SMs.
 __device__ void warp_gather_refs(const DevPic& P, int comp, int x, int y, int w, int h,
                                  uint32_t cur_order, IntraWs& S) {
   const int lane = threadIdx.x & 31;
@@ -107,40 +109,43 @@ __device__ void warp_gather_refs(const DevPic& P, int comp, int x, int y, int w,
   const int def = 1 << (P.bd - 1);
   const bool ha = y > 0, hl = x > 0;
   const int sx = comp ? P.sub_w : 1, sy = comp ? P.sub_h : 1;
-  for (int i = lane; i < 2 * w; i += 32) {
-    int v = def;
-    if (ha) {
+  // positions: up to 2 above and 2 left samples per lane (2w, 2h <= 64), and the corner
+  const uint16_t* pa[2] = {nullptr, nullptr};
+  const uint16_t* pll[2] = {nullptr, nullptr};
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int i = lane + 32 * t;
+    if (ha && i < 2 * w) {
       int avail = min(pw - x, 2 * w);
-      v = ldp(&pl[(size_t)(y - 1) * st + x + (i < avail ? i : avail - 1)]);
-      if (i >= w && x + i < pw && !is_coded_luma(P, (x + i) * sx, (y - 1) * sy, cur_order))
-        v = ldp(&pl[(size_t)(y - 1) * st + x + w - 1]);
+      int px = x + (i < avail ? i : avail - 1);
+      if (i >= w && x + i < pw && !is_coded_luma(P, (x + i) * sx, (y - 1) * sy, cur_order)) px = x + w - 1;
+      pa[t] = &pl[(size_t)(y - 1) * st + px];
     }
-    S.above[i] = (int16_t)v;
-  }
-  for (int j = lane; j < 2 * h; j += 32) {
-    int v = def;
-    if (hl) {
+    const int j = lane + 32 * t;
+    if (hl && j < 2 * h) {
       int avail = min(ph - y, h);
-      v = ldp(&pl[(size_t)(y + (j < avail ? j : avail - 1)) * st + x - 1]);
-      if (j >= h && y + j < ph && is_coded_luma(P, (x - 1) * sx, (y + j) * sy, cur_order))
-        v = ldp(&pl[(size_t)(y + j) * st + x - 1]);
+      int py = y + (j < avail ? j : avail - 1);
+      if (j >= h && y + j < ph && is_coded_luma(P, (x - 1) * sx, (y + j) * sy, cur_order)) py = y + j;
+      pll[t] = &pl[(size_t)py * st + x - 1];
     }
-    S.left[j] = (int16_t)v;
   }
-  int tl = def;
-  if (ha && hl)
-    tl = ldp(&pl[(size_t)(y - 1) * st + x - 1]);
-  else if (ha)
-    tl = ldp(&pl[(size_t)(y - 1) * st + x]);
-  else if (hl)
-    tl = ldp(&pl[(size_t)y * st + x - 1]);
-  __syncwarp();
-  if (ha && !hl) {
-    int16_t a0 = S.above[0];
-    for (int j = lane; j < 2 * h; j += 32) S.left[j] = a0;
-  } else if (!ha && hl) {
-    int16_t l0 = S.left[0];
-    for (int i = lane; i < 2 * w; i += 32) S.above[i] = l0;
+  const uint16_t* ptl = ha && hl ? &pl[(size_t)(y - 1) * st + x - 1]
+                                 : (ha ? &pl[(size_t)(y - 1) * st + x] : (hl ? &pl[(size_t)y * st + x - 1] : nullptr));
+  int va[2], vl[2], tl;
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    va[t] = pa[t] ? ldp(pa[t]) : def;
+    vl[t] = pll[t] ? ldp(pll[t]) : def;
+  }
+  tl = ptl ? ldp(ptl) : def;
+  // gather_references_16's fills when only one side exists
+  const int a0 = __shfl_sync(0xffffffffu, va[0], 0);
+  const int l0 = __shfl_sync(0xffffffffu, vl[0], 0);
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int i = lane + 32 * t;
+    if (i < 2 * w) S.above[i] = (int16_t)(!ha && hl ? l0 : va[t]);
+    if (i < 2 * h) S.left[i] = (int16_t)(ha && !hl ? a0 : vl[t]);
   }
   if (lane == 0) S.top_left = tl;
   __syncwarp();
@@ -163,21 +168,46 @@ __device__ void warp_filter_refs(int w, int h, IntraWs& S) {
   __syncwarp();
 }
 
-// Writes clip(pred + res) for sample pairs (x, x+1) of row y as one 32-bit
-// store. `res` (nullable) points at the block's residual in a plane-strided
-// int16 buffer; `keep` (nullable) receives the block (int16 raster, width w).
-__device__ __forceinline__ void store_pair(const DevPic& P, int comp, int x0, int y0, int w, int x,
-                                           int y, int p0, int p1, const int16_t* res, int16_t* keep,
-                                           int maxv) {
-  if (res) {
-    uint32_t rv = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * P.stride[comp] + x));
-    p0 += (int)(int16_t)(rv & 0xFFFFu);
-    p1 += (int)(int16_t)(rv >> 16);
+// Reconstruction of one w x h block: `pred(x, y, v0, v1)` gives the prediction
+// of the sample pair (x, x+1) of row y; the residual pairs of the lane (int16 in
+// a plane-strided buffer, nullable) are all fetched before the first is used,
+// then clip(pred + res) is stored with 32-bit stores. `keep` (nullable)
+// receives the block (int16 raster, width w).
+constexpr int kMaxPairsPerLane = (kMaxBlk * kMaxBlk / 2) / 32;
+template <class F>
+__device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, int y0, int w, int h,
+                                           const int16_t* res, int16_t* keep, F&& pred) {
+  const int lane = threadIdx.x & 31;
+  const int maxv = (1 << P.bd) - 1;
+  const int lw = ilog2(w);
+  const int npair = (w * h) >> 1;
+  const int st = P.stride[comp];
+  uint32_t rv[kMaxPairsPerLane];
+#pragma unroll
+  for (int k = 0; k < kMaxPairsPerLane; k++) {
+    const int q = lane + 32 * k;
+    rv[k] = 0;
+    if (res && q < npair) {
+      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+      rv[k] = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * st + x));
+    }
   }
-  const int v0 = clampi(p0, 0, maxv), v1 = clampi(p1, 0, maxv);
-  uint16_t* dst = P.plane[comp] + (size_t)(y0 + y) * P.stride[comp] + x0 + x;
-  *reinterpret_cast<uint32_t*>(dst) = (uint32_t)v0 | ((uint32_t)v1 << 16);
-  if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = (uint32_t)v0 | ((uint32_t)v1 << 16);
+  uint16_t* base = P.plane[comp] + (size_t)y0 * st + x0;
+#pragma unroll
+  for (int k = 0; k < kMaxPairsPerLane; k++) {
+    const int q = lane + 32 * k;
+    if (q < npair) {
+      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+      int v0, v1;
+      pred(x, y, v0, v1);
+      v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
+      v1 = clampi(v1 + (int)(int16_t)(rv[k] >> 16), 0, maxv);
+      const uint32_t pk = (uint32_t)v0 | ((uint32_t)v1 << 16);
+      *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
+      if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = pk;
+    }
+  }
+  __syncwarp();
 }
 
 // Intra prediction of one block fused with reconstruction: gathers the
@@ -191,7 +221,6 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
   const int lane = threadIdx.x & 31;
   const int bd = P.bd, maxv = (1 << bd) - 1;
   const int lw = ilog2(w), lh = ilog2(h);
-  const int npair = (w * h) >> 1;
   warp_gather_refs(P, comp, x0, y0, w, h, order, S);
   if (mode == 0) {
     const bool filt = is_luma && w * h > 32;
@@ -201,25 +230,23 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
     const int shift = lw + lh + 1;
     const int tr = A[w], bl = L[h];
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    for (int q = lane; q < npair; q += 32) {
-      const int ry = (2 * q) >> lw, rx0 = (2 * q) & (w - 1);
+    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int rx0, int ry, int& v0, int& v1) {
       const int left = L[ry];
       const int wt = 32 >> min(31, (ry * 2) >> sc);
       int v[2];
 #pragma unroll
       for (int t = 0; t < 2; t++) {
         const int rx = rx0 + t;
-        // (h-1-ry)*A + (ry+1)*bl and (w-1-rx)*L + (rx+1)*tr fit in int32 for bd <= 12, w,h <= 64
+        // exact in int32 for bd <= 12 and w, h <= 64
         int ver = (h - 1 - ry) * A[rx] + (ry + 1) * bl;
         int hor = (w - 1 - rx) * left + (rx + 1) * tr;
-        int val = ((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift;
-        val = clampi(val, 0, maxv);
+        int val = clampi(((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift, 0, maxv);
         int wl = 32 >> min(31, (rx * 2) >> sc);
         v[t] = clampi(val + ((wl * (left - val) + wt * (A[rx] - val) + 32) >> 6), 0, maxv);
       }
-      store_pair(P, comp, x0, y0, w, rx0, ry, v[0], v[1], res, keep, maxv);
-    }
-    __syncwarp();
+      v0 = v[0];
+      v1 = v[1];
+    });
     return;
   }
   if (mode == 1) {
@@ -237,27 +264,19 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
       dcu = (sl + ((unsigned)h >> 1)) >> lh;
     const int dc = (int)min(dcu & 0xFFFFu, (unsigned)maxv);
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    for (int q = lane; q < npair; q += 32) {
-      const int ry = (2 * q) >> lw, rx0 = (2 * q) & (w - 1);
+    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int rx0, int ry, int& v0, int& v1) {
       const int wt = 32 >> min(31, (ry * 2) >> sc);
-      int v[2];
-#pragma unroll
-      for (int t = 0; t < 2; t++) {
-        const int rx = rx0 + t;
-        int wl = 32 >> min(31, (rx * 2) >> sc);
-        v[t] = clampi(dc + ((wl * (S.left[ry] - dc) + wt * (S.above[rx] - dc) + 32) >> 6), 0, maxv);
-      }
-      store_pair(P, comp, x0, y0, w, rx0, ry, v[0], v[1], res, keep, maxv);
-    }
-    __syncwarp();
+      int wl0 = 32 >> min(31, (rx0 * 2) >> sc), wl1 = 32 >> min(31, ((rx0 + 1) * 2) >> sc);
+      v0 = clampi(dc + ((wl0 * (S.left[ry] - dc) + wt * (S.above[rx0] - dc) + 32) >> 6), 0, maxv);
+      v1 = clampi(dc + ((wl1 * (S.left[ry] - dc) + wt * (S.above[rx0 + 1] - dc) + 32) >> 6), 0, maxv);
+    });
     return;
   }
   if (mode < 2 || mode > 66) {
-    for (int q = lane; q < npair; q += 32) {
-      const int ry = (2 * q) >> lw, rx0 = (2 * q) & (w - 1);
-      store_pair(P, comp, x0, y0, w, rx0, ry, 0, 0, res, keep, maxv);
-    }
-    __syncwarp();
+    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int, int, int& v0, int& v1) {
+      v0 = 0;
+      v1 = 0;
+    });
     return;
   }
   // ---- angular ----
@@ -308,23 +327,23 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
   if (p.angle == 0) {
     const int sc0 = (ilog2(ww) + ilog2(wh) - 2) >> 2;
     const int lim = p.pdpc ? min(3 << sc0, ww) : 0;
-    for (int q = lane; q < npair; q += 32) {
-      const int oy = (2 * q) >> lw, ox0 = (2 * q) & (w - 1);
-      int v[2];
-#pragma unroll
-      for (int t = 0; t < 2; t++) {
-        const int ox = ox0 + t;
-        const int x = p.is_ver ? ox : oy, yy = p.is_ver ? oy : ox;  // work coordinates
-        int val = rm[base + x + 1];
-        if (x < lim) {
-          int wl = 32 >> ((2 * x) >> sc0);
-          val = clampi(val + ((wl * (rs[base + 1 + yy] - rm[base]) + 32) >> 6), 0, maxv);
-        }
-        v[t] = val;
+    auto sample = [&](int x, int yy) -> int {
+      int val = rm[base + x + 1];
+      if (x < lim) {
+        int wl = 32 >> ((2 * x) >> sc0);
+        val = clampi(val + ((wl * (rs[base + 1 + yy] - rm[base]) + 32) >> 6), 0, maxv);
       }
-      store_pair(P, comp, x0, y0, w, ox0, oy, v[0], v[1], res, keep, maxv);
-    }
-    __syncwarp();
+      return val;
+    };
+    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int ox0, int oy, int& v0, int& v1) {
+      if (p.is_ver) {
+        v0 = sample(ox0, oy);
+        v1 = sample(ox0 + 1, oy);
+      } else {
+        v0 = sample(oy, ox0);
+        v1 = sample(oy, ox0 + 1);
+      }
+    });
     return;
   }
   // Every non-zero-angle case is one 4-tap filter over rm[j..j+3], j = base + di + x:
@@ -360,9 +379,7 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
     }
     return val;
   };
-  for (int q = lane; q < npair; q += 32) {
-    const int oy = (2 * q) >> lw, ox0 = (2 * q) & (w - 1);
-    int v0, v1;
+  emit_block(P, comp, x0, y0, w, h, res, keep, [&](int ox0, int oy, int& v0, int& v1) {
     if (p.is_ver) {
       v0 = sample(ox0, oy);
       v1 = sample(ox0 + 1, oy);
@@ -370,15 +387,15 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
       v0 = sample(oy, ox0);
       v1 = sample(oy, ox0 + 1);
     }
-    store_pair(P, comp, x0, y0, w, ox0, oy, v0, v1, res, keep, maxv);
-  }
-  __syncwarp();
+  });
 }
 
 // CCLM luma downsampling (downsample_luma_for_cclm_format_16, predict.rs:3869-3990)
 // for the chroma block at (bxc, byc): `ds` (cw*ch int16) gets the block, S.ds_top /
 // S.ds_left the templates. The CU's own reconstructed luma comes from `tile`
-// (tb x tb at luma (lbx, lby)); everything else is read from the plane.
+// (tb x tb at luma (lbx, lby)); the luma column left of it is prefetched into
+// S.fleft first, so the block pass reads shared memory only; the templates
+// read the plane (one round trip per lane).
 __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, int ch, int lbx,
                                      int lby, int tb, const int16_t* tile, IntraWs& S, int16_t* ds) {
   const int lane = threadIdx.x & 31;
@@ -387,11 +404,19 @@ __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, 
   const int mid = 1 << (P.bd - 1);
   const int cf = P.cf;
   const int bx = bxc * P.sub_w, by = byc * P.sub_h;
-  auto gy = [&](int x, int y) -> int {
+  auto gp = [&](int x, int y) -> int {  // plane read, coordinates clamped
+    return ldp(&lp[(size_t)clampi(y, 0, lhei - 1) * lst + clampi(x, 0, lwid - 1)]);
+  };
+  // luma column lbx - 1 next to the tile, rows lby .. lby + tb - 1
+  if (lbx > 0)
+    for (int r = lane; r < tb; r += 32) S.fleft[r] = (int16_t)gp(lbx - 1, lby + r);
+  __syncwarp();
+  auto gy = [&](int x, int y) -> int {  // block pass: tile or the prefetched column
     x = clampi(x, 0, lwid - 1);
     y = clampi(y, 0, lhei - 1);
     if (x >= lbx && x < lbx + tb && y >= lby && y < lby + tb) return tile[(y - lby) * tb + (x - lbx)];
-    return ldp(&lp[(size_t)y * lst + x]);
+    if (x == lbx - 1 && y >= lby && y < lby + tb) return S.fleft[y - lby];
+    return gp(x, y);
   };
   for (int i = lane; i < cw * ch; i += 32) {
     int x = i % cw, y = i / cw;
@@ -411,53 +436,57 @@ __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, 
     }
     ds[i] = (int16_t)v;
   }
-  for (int x = lane; x < cw; x += 32) {
-    int v = mid;
+  // templates: each lane computes at most one top and one left entry
+  int vt = mid, vl = mid;
+  const int x = lane, y = lane;
+  if (x < cw) {
     if (cf == 1) {
       const bool first_row = (by & (P.ctu - 1)) == 0;
       if (by > 0 && first_row) {
         int lx = bx + 2 * x, yy = by - 1;
         int x0 = clampi(lx, 0, lwid - 1), xr = clampi(lx + 1, 0, lwid - 1);
         int xl = ((x == 0 && bx == 0) || x0 == 0) ? x0 : x0 - 1;
-        v = (2 * gy(x0, yy) + gy(xl, yy) + gy(xr, yy) + 2) >> 2;
+        int a = gp(x0, yy), b = gp(xl, yy), c = gp(xr, yy);
+        vt = (2 * a + b + c + 2) >> 2;
       } else if (by >= 2) {
         int lx = bx + 2 * x, ly = by - 2;
         int lxl = (x == 0 && !(bx > 0)) ? lx : lx - 1;
-        int r0 = 2 * gy(lx, ly) + gy(lxl, ly) + gy(lx + 1, ly);
-        int r1 = 2 * gy(lx, ly + 1) + gy(lxl, ly + 1) + gy(lx + 1, ly + 1);
-        v = (r0 + r1 + 4) >> 3;
+        int a = gp(lx, ly), b = gp(lxl, ly), c = gp(lx + 1, ly);
+        int d = gp(lx, ly + 1), e = gp(lxl, ly + 1), f = gp(lx + 1, ly + 1);
+        vt = (2 * a + b + c + 2 * d + e + f + 4) >> 3;
       }
     } else if (cf == 2) {
       if (by > 0) {
         int lx = bx + 2 * x, ly = by - 1;
         int lxl = (x == 0 && bx == 0) ? lx : lx - 1;
-        v = (2 * gy(lx, ly) + gy(lxl, ly) + gy(lx + 1, ly) + 2) >> 2;
+        int a = gp(lx, ly), b = gp(lxl, ly), c = gp(lx + 1, ly);
+        vt = (2 * a + b + c + 2) >> 2;
       }
     } else if (by > 0) {
-      v = gy(bx + x, by - 1);
+      vt = gp(bx + x, by - 1);
     }
-    S.ds_top[x] = (int16_t)v;
   }
-  for (int y = lane; y < ch; y += 32) {
-    int v = mid;
+  if (y < ch) {
     if (cf == 1) {
       if (bx >= 2) {
         int lx = bx - 2, ly = by + 2 * y;
-        int r0 = 2 * gy(lx, ly) + gy(lx - 1, ly) + gy(lx + 1, ly);
-        int r1 = 2 * gy(lx, ly + 1) + gy(lx - 1, ly + 1) + gy(lx + 1, ly + 1);
-        v = (r0 + r1 + 4) >> 3;
+        int a = gp(lx, ly), b = gp(lx - 1, ly), c = gp(lx + 1, ly);
+        int d = gp(lx, ly + 1), e = gp(lx - 1, ly + 1), f = gp(lx + 1, ly + 1);
+        vl = (2 * a + b + c + 2 * d + e + f + 4) >> 3;
       }
     } else if (cf == 2) {
       if (bx > 0) {
         int ly = by + y, lx = bx - 2;
         int lxl = bx >= 2 ? lx - 1 : lx;
-        v = (2 * gy(max(0, lx), ly) + gy(max(0, lxl), ly) + gy(bx - 1, ly) + 2) >> 2;
+        int a = gp(max(0, lx), ly), b = gp(max(0, lxl), ly), c = gp(bx - 1, ly);
+        vl = (2 * a + b + c + 2) >> 2;
       }
     } else if (bx > 0) {
-      v = gy(bx - 1, by + y);
+      vl = gp(bx - 1, by + y);
     }
-    S.ds_left[y] = (int16_t)v;
   }
+  if (x < cw) S.ds_top[x] = (int16_t)vt;
+  if (y < ch) S.ds_left[y] = (int16_t)vl;
   __syncwarp();
 }
 
@@ -467,12 +496,10 @@ __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, 
 __device__ void warp_cclm_predict_store(const DevPic& P, int comp, int bxc, int byc, int cw, int ch,
                                         int cclm_mode, IntraWs& S, const int16_t* ds,
                                         const int16_t* res) {
-  const int lane = threadIdx.x & 31;
   const int bd = P.bd, maxv = (1 << bd) - 1, mid = 1 << (bd - 1);
   const uint16_t* pl = P.plane[comp];
   const int st = P.stride[comp], pw = P.pw[comp], ph = P.ph[comp];
   const bool ha = byc > 0, hl = bxc > 0;
-  // template samples at the positions the LM derivation reads
   auto above = [&](int i) -> int {
     if (ha) return ldp(&pl[(size_t)(byc - 1) * st + min(bxc + i, pw - 1)]);
     if (hl) return ldp(&pl[(size_t)byc * st + bxc - 1]);
@@ -555,14 +582,10 @@ __device__ void warp_cclm_predict_store(const DevPic& P, int comp, int bxc, int 
       }
     }
   }
-  const int lw = ilog2(cw);
-  for (int q = lane; q < (cw * ch) >> 1; q += 32) {
-    const int y = (2 * q) >> lw, x = (2 * q) & (cw - 1);
-    int p0 = clampi(((ds[y * cw + x] * a) >> shift) + b, 0, maxv);
-    int p1 = clampi(((ds[y * cw + x + 1] * a) >> shift) + b, 0, maxv);
-    store_pair(P, comp, bxc, byc, cw, x, y, p0, p1, res, nullptr, maxv);
-  }
-  __syncwarp();
+  emit_block(P, comp, bxc, byc, cw, ch, res, nullptr, [&](int x, int y, int& v0, int& v1) {
+    v0 = clampi(((ds[y * cw + x] * a) >> shift) + b, 0, maxv);
+    v1 = clampi(((ds[y * cw + x + 1] * a) >> shift) + b, 0, maxv);
+  });
 }
 
 }  // namespace vvcg

@@ -302,7 +302,7 @@ __device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t epoch, 
   return ld_acquire(flag) == epoch;
 }
 
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 2)
 k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items,
                   uint32_t n_items, uint32_t* counter, uint32_t epoch, uint32_t spin_limit,
                   uint32_t* status) {
