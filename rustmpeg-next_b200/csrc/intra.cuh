@@ -22,6 +22,7 @@ struct IntraWs {
   int16_t ds_top[kMaxBlk];
   int16_t ds_left[kMaxBlk];
   int top_left, ftop_left;
+  int dc;
 };
 
 // Position of the CU at tb-grid cell (gx, gy) in the coding order of the
@@ -168,15 +169,28 @@ __device__ void warp_filter_refs(int w, int h, IntraWs& S) {
   __syncwarp();
 }
 
-// Reconstruction of one w x h block: `pred(x, y, v0, v1)` gives the prediction
-// of the sample pair (x, x+1) of row y; the residual pairs of the lane (int16 in
-// a plane-strided buffer, nullable) are all fetched before the first is used,
-// then clip(pred + res) is stored with 32-bit stores. `keep` (nullable)
-// receives the block (int16 raster, width w).
+// The samples of a block that other blocks read while they are predicted:
+// the bottom `rows` rows and the right `cols` columns. For luma that is 2 rows
+// and 5 columns: the above/left reference samples and the corner, the 2 rows /
+// 3 columns the neighbours' CCLM templates downsample, and the columns this
+// CU's own CCLM needs for its right chroma column pair; for chroma 1 and 1. Phase 1 reconstructs
+// those, phase 2 the rest, phase 0 everything.
+__device__ __forceinline__ bool in_phase(int phase, int x, int y, int w, int h, int rows, int cols) {
+  if (phase == 0) return true;
+  const bool edge = y >= h - rows || x + 1 >= w - cols;  // pair (x, x+1)
+  return phase == 1 ? edge : !edge;
+}
+
+// Reconstruction of the pairs of one w x h block that belong to `phase`:
+// `pred(x, y, v0, v1)` gives the prediction of the pair (x, x+1) of row y; the
+// lane's residual pairs (int16 in a plane-strided buffer, nullable) are all
+// fetched before the first is used, then clip(pred + res) is stored with
+// 32-bit stores. `keep` (nullable) receives the samples (int16 raster, width w).
 constexpr int kMaxPairsPerLane = (kMaxBlk * kMaxBlk / 2) / 32;
 template <class F>
 __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, int y0, int w, int h,
-                                           const int16_t* res, int16_t* keep, F&& pred) {
+                                           const int16_t* res, int16_t* keep, int phase, int rows,
+                                           int cols, F&& pred) {
   const int lane = threadIdx.x & 31;
   const int maxv = (1 << P.bd) - 1;
   const int lw = ilog2(w);
@@ -186,18 +200,17 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
 #pragma unroll
   for (int k = 0; k < kMaxPairsPerLane; k++) {
     const int q = lane + 32 * k;
+    const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
     rv[k] = 0;
-    if (res && q < npair) {
-      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+    if (res && q < npair && in_phase(phase, x, y, w, h, rows, cols))
       rv[k] = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * st + x));
-    }
   }
   uint16_t* base = P.plane[comp] + (size_t)y0 * st + x0;
 #pragma unroll
   for (int k = 0; k < kMaxPairsPerLane; k++) {
     const int q = lane + 32 * k;
-    if (q < npair) {
-      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+    const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+    if (q < npair && in_phase(phase, x, y, w, h, rows, cols)) {
       int v0, v1;
       pred(x, y, v0, v1);
       v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
@@ -210,43 +223,18 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
   __syncwarp();
 }
 
-// Intra prediction of one block fused with reconstruction: gathers the
-// references, predicts (planar / DC: predict_from_refs_16 + apply_pdpc_16,
-// predict.rs:3138-3215; angular: predict_angular_16, :3223-3410; other mode
-// values predict zeros as in predict.rs:3194), adds the residual, clips and
-// stores. `keep` (optional) receives the reconstructed block (int16 raster).
-__device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, int w, int h,
-                                   bool is_luma, int mode, uint32_t order, IntraWs& S,
-                                   const int16_t* res, int16_t* keep) {
+// Gathers the references of one block and prepares what its prediction needs
+// in S: filtered references (planar, angular with the [1 2 1] filter), the DC
+// value, and the extended main/side reference arrays of angular modes
+// (predict_angular_16, predict.rs:3240-3305).
+__device__ __noinline__ void prep_intra(const DevPic& P, int comp, int x0, int y0, int w, int h, bool is_luma,
+                           int mode, uint32_t order, IntraWs& S) {
   const int lane = threadIdx.x & 31;
   const int bd = P.bd, maxv = (1 << bd) - 1;
   const int lw = ilog2(w), lh = ilog2(h);
   warp_gather_refs(P, comp, x0, y0, w, h, order, S);
   if (mode == 0) {
-    const bool filt = is_luma && w * h > 32;
-    if (filt) warp_filter_refs(w, h, S);
-    const int16_t* A = filt ? S.fabove : S.above;
-    const int16_t* L = filt ? S.fleft : S.left;
-    const int shift = lw + lh + 1;
-    const int tr = A[w], bl = L[h];
-    const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int rx0, int ry, int& v0, int& v1) {
-      const int left = L[ry];
-      const int wt = 32 >> min(31, (ry * 2) >> sc);
-      int v[2];
-#pragma unroll
-      for (int t = 0; t < 2; t++) {
-        const int rx = rx0 + t;
-        // exact in int32 for bd <= 12 and w, h <= 64
-        int ver = (h - 1 - ry) * A[rx] + (ry + 1) * bl;
-        int hor = (w - 1 - rx) * left + (rx + 1) * tr;
-        int val = clampi(((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift, 0, maxv);
-        int wl = 32 >> min(31, (rx * 2) >> sc);
-        v[t] = clampi(val + ((wl * (left - val) + wt * (A[rx] - val) + 32) >> 6), 0, maxv);
-      }
-      v0 = v[0];
-      v1 = v[1];
-    });
+    if (is_luma && w * h > 32) warp_filter_refs(w, h, S);
     return;
   }
   if (mode == 1) {
@@ -262,24 +250,11 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
       dcu = (st + ((unsigned)w >> 1)) >> lw;
     else
       dcu = (sl + ((unsigned)h >> 1)) >> lh;
-    const int dc = (int)min(dcu & 0xFFFFu, (unsigned)maxv);
-    const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int rx0, int ry, int& v0, int& v1) {
-      const int wt = 32 >> min(31, (ry * 2) >> sc);
-      int wl0 = 32 >> min(31, (rx0 * 2) >> sc), wl1 = 32 >> min(31, ((rx0 + 1) * 2) >> sc);
-      v0 = clampi(dc + ((wl0 * (S.left[ry] - dc) + wt * (S.above[rx0] - dc) + 32) >> 6), 0, maxv);
-      v1 = clampi(dc + ((wl1 * (S.left[ry] - dc) + wt * (S.above[rx0 + 1] - dc) + 32) >> 6), 0, maxv);
-    });
+    if (lane == 0) S.dc = (int)min(dcu & 0xFFFFu, (unsigned)maxv);
+    __syncwarp();
     return;
   }
-  if (mode < 2 || mode > 66) {
-    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int, int, int& v0, int& v1) {
-      v0 = 0;
-      v1 = 0;
-    });
-    return;
-  }
-  // ---- angular ----
+  if (mode < 2 || mode > 66) return;
   const AngP p = angular_params(mode, w, h, is_luma);
   if (p.ref_filter) warp_filter_refs(w, h, S);
   const int16_t* A = p.ref_filter ? S.fabove : S.above;
@@ -321,6 +296,66 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
     }
   }
   __syncwarp();
+}
+
+// Intra prediction of one block (prepared by prep_intra) fused with
+// reconstruction, for the pairs of `phase`: planar / DC are
+// predict_from_refs_16 + apply_pdpc_16 (predict.rs:3138-3215), angular is
+// predict_angular_16 (:3223-3410), other mode values predict zeros
+// (predict.rs:3194). `keep` (optional) receives the reconstructed samples.
+__device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y0, int w, int h, bool is_luma,
+                           int mode, const IntraWs& S, const int16_t* res, int16_t* keep, int phase,
+                           int rows, int cols) {
+  const int bd = P.bd, maxv = (1 << bd) - 1;
+  const int lw = ilog2(w), lh = ilog2(h);
+  if (mode == 0) {
+    const bool filt = is_luma && w * h > 32;
+    const int16_t* A = filt ? S.fabove : S.above;
+    const int16_t* L = filt ? S.fleft : S.left;
+    const int shift = lw + lh + 1;
+    const int tr = A[w], bl = L[h];
+    const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
+    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+      const int left = L[ry];
+      const int wt = 32 >> min(31, (ry * 2) >> sc);
+      int v[2];
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const int rx = rx0 + t;
+        // exact in int32 for bd <= 12 and w, h <= 64
+        int ver = (h - 1 - ry) * A[rx] + (ry + 1) * bl;
+        int hor = (w - 1 - rx) * left + (rx + 1) * tr;
+        int val = clampi(((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift, 0, maxv);
+        int wl = 32 >> min(31, (rx * 2) >> sc);
+        v[t] = clampi(val + ((wl * (left - val) + wt * (A[rx] - val) + 32) >> 6), 0, maxv);
+      }
+      v0 = v[0];
+      v1 = v[1];
+    });
+    return;
+  }
+  if (mode == 1) {
+    const int dc = S.dc;
+    const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
+    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+      const int wt = 32 >> min(31, (ry * 2) >> sc);
+      int wl0 = 32 >> min(31, (rx0 * 2) >> sc), wl1 = 32 >> min(31, ((rx0 + 1) * 2) >> sc);
+      v0 = clampi(dc + ((wl0 * (S.left[ry] - dc) + wt * (S.above[rx0] - dc) + 32) >> 6), 0, maxv);
+      v1 = clampi(dc + ((wl1 * (S.left[ry] - dc) + wt * (S.above[rx0 + 1] - dc) + 32) >> 6), 0, maxv);
+    });
+    return;
+  }
+  if (mode < 2 || mode > 66) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int, int, int& v0, int& v1) {
+      v0 = 0;
+      v1 = 0;
+    });
+    return;
+  }
+  const AngP p = angular_params(mode, w, h, is_luma);
+  const int mx = max(w, h);
+  const int base = mx + 4;
+  const int buf_len = base + 2 * mx + 64;
   const int16_t* rm = p.is_ver ? S.ref_above : S.ref_left;
   const int16_t* rs = p.is_ver ? S.ref_left : S.ref_above;
   const int ww = p.is_ver ? w : h, wh = p.is_ver ? h : w;
@@ -335,7 +370,7 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
       }
       return val;
     };
-    emit_block(P, comp, x0, y0, w, h, res, keep, [&](int ox0, int oy, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
       if (p.is_ver) {
         v0 = sample(ox0, oy);
         v1 = sample(ox0 + 1, oy);
@@ -379,7 +414,7 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
     }
     return val;
   };
-  emit_block(P, comp, x0, y0, w, h, res, keep, [&](int ox0, int oy, int& v0, int& v1) {
+  emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
     if (p.is_ver) {
       v0 = sample(ox0, oy);
       v1 = sample(ox0 + 1, oy);
@@ -390,18 +425,19 @@ __device__ void warp_predict_store(const DevPic& P, int comp, int x0, int y0, in
   });
 }
 
-// CCLM luma downsampling (downsample_luma_for_cclm_format_16, predict.rs:3869-3990)
-// for the chroma block at (bxc, byc): `ds` (cw*ch int16) gets the block, S.ds_top /
-// S.ds_left the templates. The CU's own reconstructed luma comes from `tile`
-// (tb x tb at luma (lbx, lby)); the luma column left of it is prefetched into
-// S.fleft first, so the block pass reads shared memory only; the templates
-// read the plane (one round trip per lane).
-__device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, int ch, int lbx,
-                                     int lby, int tb, const int16_t* tile, IntraWs& S, int16_t* ds) {
+// CCLM templates and linear models for both chroma components of the chroma
+// block at (bxc, byc): the luma templates of downsample_luma_for_cclm_format_16
+// (predict.rs:3869-3990) go to L.ds_top / L.ds_left, the luma column left of the
+// CU (x = lbx - 1) to L.fleft, and each component's (a, b, shift) of
+// predict_cclm_with_format_16 (predict.rs:3996-4066) and
+// derive_cclm_params_from_4_samples (:2088-2177) to Sc[c].dc / ftop_left /
+// top_left. All plane loads of a lane are independent (one round trip).
+__device__ __noinline__ void prep_cclm(const DevPic& P, int bxc, int byc, int cw, int ch, int lbx, int lby, int tb,
+                          int cclm_mode, IntraWs& L, IntraWs* Sc) {
   const int lane = threadIdx.x & 31;
   const uint16_t* lp = P.plane[0];
   const int lst = P.stride[0], lwid = P.pw[0], lhei = P.ph[0];
-  const int mid = 1 << (P.bd - 1);
+  const int bd = P.bd, mid = 1 << (bd - 1);
   const int cf = P.cf;
   const int bx = bxc * P.sub_w, by = byc * P.sub_h;
   auto gp = [&](int x, int y) -> int {  // plane read, coordinates clamped
@@ -409,34 +445,7 @@ __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, 
   };
   // luma column lbx - 1 next to the tile, rows lby .. lby + tb - 1
   if (lbx > 0)
-    for (int r = lane; r < tb; r += 32) S.fleft[r] = (int16_t)gp(lbx - 1, lby + r);
-  __syncwarp();
-  auto gy = [&](int x, int y) -> int {  // block pass: tile or the prefetched column
-    x = clampi(x, 0, lwid - 1);
-    y = clampi(y, 0, lhei - 1);
-    if (x >= lbx && x < lbx + tb && y >= lby && y < lby + tb) return tile[(y - lby) * tb + (x - lbx)];
-    if (x == lbx - 1 && y >= lby && y < lby + tb) return S.fleft[y - lby];
-    return gp(x, y);
-  };
-  for (int i = lane; i < cw * ch; i += 32) {
-    int x = i % cw, y = i / cw;
-    int v;
-    if (cf == 1) {
-      int lx = bx + 2 * x, ly = by + 2 * y;
-      int lxl = (x == 0 && !(bx > 0)) ? lx : lx - 1;
-      int r0 = 2 * gy(lx, ly) + gy(lxl, ly) + gy(lx + 1, ly);
-      int r1 = 2 * gy(lx, ly + 1) + gy(lxl, ly + 1) + gy(lx + 1, ly + 1);
-      v = (r0 + r1 + 4) >> 3;
-    } else if (cf == 2) {
-      int lx = bx + 2 * x, ly = by + y;
-      int lxl = (x == 0 && bx == 0) ? lx : lx - 1;
-      v = (2 * gy(lx, ly) + gy(lxl, ly) + gy(lx + 1, ly) + 2) >> 2;
-    } else {
-      v = gy(bx + x, by + y);
-    }
-    ds[i] = (int16_t)v;
-  }
-  // templates: each lane computes at most one top and one left entry
+    for (int r = lane; r < tb; r += 32) L.fleft[r] = (int16_t)gp(lbx - 1, lby + r);
   int vt = mid, vl = mid;
   const int x = lane, y = lane;
   if (x < cw) {
@@ -485,59 +494,56 @@ __device__ void warp_cclm_downsample(const DevPic& P, int bxc, int byc, int cw, 
       vl = gp(bx - 1, by + y);
     }
   }
-  if (x < cw) S.ds_top[x] = (int16_t)vt;
-  if (y < ch) S.ds_left[y] = (int16_t)vl;
+  if (x < cw) L.ds_top[x] = (int16_t)vt;
+  if (y < ch) L.ds_left[y] = (int16_t)vl;
   __syncwarp();
-}
-
-// predict_cclm_with_format_16 (predict.rs:3996-4066) for one chroma component
-// from a prepared downsampling, fused with add / clip / store.
-// cclm_mode 0 LM, 1 LM-L, 2 LM-T. Chroma templates come from a plain gather.
-__device__ void warp_cclm_predict_store(const DevPic& P, int comp, int bxc, int byc, int cw, int ch,
-                                        int cclm_mode, IntraWs& S, const int16_t* ds,
-                                        const int16_t* res) {
-  const int bd = P.bd, maxv = (1 << bd) - 1, mid = 1 << (bd - 1);
-  const uint16_t* pl = P.plane[comp];
-  const int st = P.stride[comp], pw = P.pw[comp], ph = P.ph[comp];
   const bool ha = byc > 0, hl = bxc > 0;
-  auto above = [&](int i) -> int {
-    if (ha) return ldp(&pl[(size_t)(byc - 1) * st + min(bxc + i, pw - 1)]);
-    if (hl) return ldp(&pl[(size_t)byc * st + bxc - 1]);
-    return mid;
-  };
-  auto left = [&](int j) -> int {
-    if (hl) return ldp(&pl[(size_t)min(byc + j, ph - 1) * st + bxc - 1]);
-    if (ha) return ldp(&pl[(size_t)(byc - 1) * st + bxc]);
-    return mid;
-  };
-  int a = 0, b = mid, shift = 0;
-  {
-    const bool has_top = byc > 0 && cclm_mode != 1;
-    const bool has_left = bxc > 0 && cclm_mode != 2;
-    int sl[4] = {mid, mid, mid, mid}, sc[4] = {mid, mid, mid, mid};
-    int cnt = 0;
-    if (has_top && has_left) {
-      int x0 = cw / 4, x1 = (3 * cw) / 4, y0 = ch / 4, y1 = (3 * ch) / 4;
-      sl[0] = S.ds_top[x0]; sl[1] = S.ds_top[x1]; sl[2] = S.ds_left[y0]; sl[3] = S.ds_left[y1];
-      sc[0] = above(x0); sc[1] = above(x1); sc[2] = left(y0); sc[3] = left(y1);
-      cnt = 4;
-    } else if (has_top) {
-      for (int i = 0; i < min(4, cw); i++) {
-        int idx = min(((2 * i + 1) * cw) / 8, cw - 1);
-        sl[i] = S.ds_top[idx];
-        sc[i] = above(idx);
-        cnt++;
-      }
-    } else if (has_left) {
-      for (int i = 0; i < min(4, ch); i++) {
-        int idx = min(((2 * i + 1) * ch) / 8, ch - 1);
-        sl[i] = S.ds_left[idx];
-        sc[i] = left(idx);
-        cnt++;
+  const bool has_top = ha && cclm_mode != 1;
+  const bool has_left = hl && cclm_mode != 2;
+  // template positions of the LM derivation (same for both components)
+  int idx[4] = {0, 0, 0, 0}, from_top[4] = {0, 0, 0, 0};
+  int cnt = 0;
+  if (has_top && has_left) {
+    idx[0] = cw / 4; idx[1] = (3 * cw) / 4; idx[2] = ch / 4; idx[3] = (3 * ch) / 4;
+    from_top[0] = from_top[1] = 1;
+    cnt = 4;
+  } else if (has_top) {
+    for (int i = 0; i < min(4, cw); i++) {
+      idx[i] = min(((2 * i + 1) * cw) / 8, cw - 1);
+      from_top[i] = 1;
+      cnt++;
+    }
+  } else if (has_left) {
+    for (int i = 0; i < min(4, ch); i++) {
+      idx[i] = min(((2 * i + 1) * ch) / 8, ch - 1);
+      cnt++;
+    }
+  }
+  // lanes 0..3: component 1, lanes 4..7: component 2 fetch one chroma template sample
+  int tv = mid;
+  if (lane < 8) {
+    const int c = 1 + (lane >> 2), i = lane & 3;
+    const uint16_t* pl = P.plane[c];
+    const int st = P.stride[c], pw = P.pw[c], ph = P.ph[c];
+    if (i < cnt) {
+      if (from_top[i]) {  // gather_references_16 above row
+        tv = ha ? ldp(&pl[(size_t)(byc - 1) * st + min(bxc + idx[i], pw - 1)])
+                : (hl ? ldp(&pl[(size_t)byc * st + bxc - 1]) : mid);
+      } else {  // left column
+        tv = hl ? ldp(&pl[(size_t)min(byc + idx[i], ph - 1) * st + bxc - 1])
+                : (ha ? ldp(&pl[(size_t)(byc - 1) * st + bxc]) : mid);
       }
     }
-    // derive_cclm_params_from_4_samples (predict.rs:2088-2177); every lane
-    // evaluates it on the same values
+  }
+  for (int c = 1; c <= 2; c++) {
+    int sl[4], sc[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      sl[i] = i < cnt ? (from_top[i] ? L.ds_top[idx[i]] : L.ds_left[idx[i]]) : mid;
+      sc[i] = __shfl_sync(0xffffffffu, tv, (c - 1) * 4 + i);
+      if (i >= cnt) sc[i] = mid;
+    }
+    int a = 0, b = mid, shift = 0;
     if (cnt == 0) {
       a = 0;
       b = 1 << (bd - 1);
@@ -581,10 +587,47 @@ __device__ void warp_cclm_predict_store(const DevPic& P, int comp, int bxc, int 
         shift = 0;
       }
     }
+    if (lane == 0) {
+      Sc[c - 1].dc = a;
+      Sc[c - 1].ftop_left = b;
+      Sc[c - 1].top_left = shift;
+    }
   }
-  emit_block(P, comp, bxc, byc, cw, ch, res, nullptr, [&](int x, int y, int& v0, int& v1) {
-    v0 = clampi(((ds[y * cw + x] * a) >> shift) + b, 0, maxv);
-    v1 = clampi(((ds[y * cw + x + 1] * a) >> shift) + b, 0, maxv);
+  __syncwarp();
+}
+
+// CCLM prediction of one chroma component fused with reconstruction, for the
+// pairs of `phase`; the downsampled luma of each sample is formed from the
+// CU's reconstructed luma tile (tb x tb at (lbx, lby)) and the prefetched
+// column left of it (L.fleft), as downsample_luma_for_cclm_format_16 does.
+__device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int byc, int cw, int ch, int lbx,
+                          int lby, int tb, const IntraWs& L, const IntraWs& S, const int16_t* tile,
+                          const int16_t* res, int phase) {
+  const int maxv = (1 << P.bd) - 1;
+  const int cf = P.cf;
+  const int a = S.dc, b = S.ftop_left, shift = S.top_left;
+  const int bx = bxc * P.sub_w, by = byc * P.sub_h;
+  auto T = [&](int x, int y) -> int {  // x >= lbx - 1; y inside the tile
+    return x < lbx ? L.fleft[y - lby] : tile[(y - lby) * tb + (x - lbx)];
+  };
+  auto ds = [&](int x, int y) -> int {
+    if (cf == 1) {
+      int lx = bx + 2 * x, ly = by + 2 * y;
+      int lxl = (x == 0 && bx == 0) ? lx : lx - 1;
+      int r0 = 2 * T(lx, ly) + T(lxl, ly) + T(lx + 1, ly);
+      int r1 = 2 * T(lx, ly + 1) + T(lxl, ly + 1) + T(lx + 1, ly + 1);
+      return (r0 + r1 + 4) >> 3;
+    }
+    if (cf == 2) {
+      int lx = bx + 2 * x, ly = by + y;
+      int lxl = (x == 0 && bx == 0) ? lx : lx - 1;
+      return (2 * T(lx, ly) + T(lxl, ly) + T(lx + 1, ly) + 2) >> 2;
+    }
+    return T(bx + x, by + y);
+  };
+  emit_block(P, comp, bxc, byc, cw, ch, res, nullptr, phase, 1, 1, [&](int x, int y, int& v0, int& v1) {
+    v0 = clampi(((ds(x, y) * a) >> shift) + b, 0, maxv);
+    v1 = clampi(((ds(x + 1, y) * a) >> shift) + b, 0, maxv);
   });
 }
 

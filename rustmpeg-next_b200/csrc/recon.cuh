@@ -286,9 +286,8 @@ k_residual(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, 
 // Per-warp shared workspace of the wavefront kernel.
 struct WaveWs {
   DevPic P;                        // the item's picture, copied once per item
-  IntraWs in;                      // reference samples of the current block
+  IntraWs in[3];                   // prediction state per colour component
   int16_t luma[32 * 32];           // the CU's reconstructed luma (for CCLM)
-  int16_t ds[32 * 32];             // CCLM downsampled luma
 };
 
 // Bounded wait for a CTU flag; returns false when the poll limit ran out.
@@ -302,13 +301,56 @@ __device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t epoch, 
   return ld_acquire(flag) == epoch;
 }
 
+// Luma keeps 2 rows / 5 columns for neighbours and CCLM; chroma 1 / 1.
+constexpr int kLumaRows = 2, kLumaCols = 5, kChromaRows = 1, kChromaCols = 1;
+
+// Reconstructs one coding unit in `phase` (0 all samples, 1 the samples other
+// CUs read, 2 the rest). Phase 1 also prepares the prediction state (refs,
+// CCLM models) that phase 2 reuses.
+__device__ void recon_cu(const DevPic& P, const vvcg_cu_rec& rec, int gx, int gy, WaveWs& W, int phase) {
+  const int tb = P.tb;
+  const int bx = gx * tb, by = gy * tb;
+  const uint32_t order = cu_order(P, gx, gy);
+  auto resid = [&](int c, int x0, int y0) -> const int16_t* {
+    return ((rec.cbf >> c) & 1) && rec.level_off[c] >= 0
+               ? reinterpret_cast<const int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0
+               : nullptr;
+  };
+  const int lm = rec.luma_mode <= 69 ? rec.luma_mode : 0;
+  if (phase != 2) prep_intra(P, 0, bx, by, tb, tb, true, lm, order, W.in[0]);
+  emit_intra(P, 0, bx, by, tb, tb, true, lm, W.in[0], resid(0, bx, by), W.luma, phase, kLumaRows,
+             kLumaCols);
+  if (!P.cf) return;
+  const int cxp = bx / P.sub_w, cyp = by / P.sub_h;
+  const int cw = P.tb_cw, ch = P.tb_ch;
+  const int chm = rec.chroma_mode;
+  if (chm >= 81 && chm <= 83) {
+    if (phase != 2) prep_cclm(P, cxp, cyp, cw, ch, bx, by, tb, chm - 81, W.in[0], &W.in[1]);
+    for (int c = 1; c <= 2; c++)
+      emit_cclm(P, c, cxp, cyp, cw, ch, bx, by, tb, W.in[0], W.in[c], W.luma, resid(c, cxp, cyp), phase);
+  } else {
+    const int cm = chm <= 69 ? chm : 0;
+    for (int c = 1; c <= 2; c++) {
+      if (phase != 2) prep_intra(P, c, cxp, cyp, cw, ch, false, cm, order, W.in[c]);
+      emit_intra(P, c, cxp, cyp, cw, ch, false, cm, W.in[c], resid(c, cxp, cyp), nullptr, phase,
+                 kChromaRows, kChromaCols);
+    }
+  }
+}
+
+__device__ __forceinline__ void publish(uint32_t* flag, uint32_t epoch) {
+  __threadfence();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) st_release(flag, epoch);
+}
+
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 2)
 k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items,
                   uint32_t n_items, uint32_t* counter, uint32_t epoch, uint32_t spin_limit,
                   uint32_t* status) {
-  __shared__ WaveWs wsa[kWarpsPerCta];
+  extern __shared__ __align__(16) unsigned char wave_smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  WaveWs& W = wsa[wid];
+  WaveWs& W = reinterpret_cast<WaveWs*>(wave_smem)[wid];
   for (;;) {
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(counter, 1u);
@@ -321,7 +363,7 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
     __syncwarp();
     const DevPic& P = W.P;
     const int cx = item.cx, cy = item.cy;
-    const int tb = P.tb, sh = P.ctu_log2 - ilog2(tb);
+    const int sh = P.ctu_log2 - ilog2(P.tb);
     const int ncu = 1 << (2 * sh);
     {
       int ok = 1;
@@ -337,41 +379,26 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
       }
       __syncwarp();
     }
-    for (int k = 0; k < ncu; k++) {
-      int lx = 0, ly = 0;
-      for (int b = 0; b < sh; b++) {
-        lx |= ((k >> (2 * b)) & 1) << b;
-        ly |= ((k >> (2 * b + 1)) & 1) << b;
-      }
-      const int gx = (cx << sh) + lx, gy = (cy << sh) + ly;
-      const vvcg_cu_rec rec = P.cus[gy * P.grid_w + gx];
-      const int bx = gx * tb, by = gy * tb;
-      const uint32_t order = cu_order(P, gx, gy);
-      auto resid = [&](int c, int x0, int y0) -> const int16_t* {
-        return ((rec.cbf >> c) & 1) && rec.level_off[c] >= 0
-                   ? reinterpret_cast<const int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0
-                   : nullptr;
-      };
-      warp_predict_store(P, 0, bx, by, tb, tb, true, rec.luma_mode <= 69 ? rec.luma_mode : 0,
-                         order, W.in, resid(0, bx, by), W.luma);
-      if (P.cf) {
-        const int cxp = bx / P.sub_w, cyp = by / P.sub_h;
-        const int chm = rec.chroma_mode;
-        if (chm >= 81 && chm <= 83) {
-          warp_cclm_downsample(P, cxp, cyp, P.tb_cw, P.tb_ch, bx, by, tb, W.luma, W.in, W.ds);
-          for (int c = 1; c <= 2; c++)
-            warp_cclm_predict_store(P, c, cxp, cyp, P.tb_cw, P.tb_ch, chm - 81, W.in, W.ds,
-                                    resid(c, cxp, cyp));
-        } else {
-          for (int c = 1; c <= 2; c++)
-            warp_predict_store(P, c, cxp, cyp, P.tb_cw, P.tb_ch, false, chm <= 69 ? chm : 0, order,
-                               W.in, resid(c, cxp, cyp), nullptr);
+    uint32_t* flag = &P.ctu_done[cy * P.ctu_w + cx];
+    if (ncu == 1) {
+      // one CU per CTU: publish once the samples other CUs read are stored,
+      // then finish the interior off the wavefront's critical path
+      const vvcg_cu_rec rec = P.cus[cy * P.grid_w + cx];
+      recon_cu(P, rec, cx, cy, W, 1);
+      publish(flag, epoch);
+      recon_cu(P, rec, cx, cy, W, 2);
+    } else {
+      for (int k = 0; k < ncu; k++) {
+        int lx = 0, ly = 0;
+        for (int b = 0; b < sh; b++) {
+          lx |= ((k >> (2 * b)) & 1) << b;
+          ly |= ((k >> (2 * b + 1)) & 1) << b;
         }
+        const int gx = (cx << sh) + lx, gy = (cy << sh) + ly;
+        recon_cu(P, P.cus[gy * P.grid_w + gx], gx, gy, W, 0);
       }
+      publish(flag, epoch);
     }
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release(&P.ctu_done[cy * P.ctu_w + cx], epoch);
   }
 }
 

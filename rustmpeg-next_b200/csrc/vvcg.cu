@@ -249,6 +249,12 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     return VVCG_UNAVAILABLE;
   }
   ctx->stream = ctx->own_stream;
+  if (cudaFuncSetAttribute(k_recon_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kWarpsPerCta * sizeof(WaveWs))) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
   if (upload_tables(ctx) != VVCG_OK) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -529,11 +535,13 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     // prediction + reconstruction in CTU wavefront order
     const uint32_t n = (uint32_t)ctx->items.size();
     int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32, 0),
+    const size_t wave_smem = kWarpsPerCta * sizeof(WaveWs);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32,
+                                                     wave_smem),
        "occupancy");
     const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kWarpsPerCta;
     const uint32_t grid = (std::min<uint32_t>(n, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
-    k_recon_wavefront<<<grid, kWarpsPerCta * 32, 0, ctx->stream>>>(
+    k_recon_wavefront<<<grid, kWarpsPerCta * 32, wave_smem, ctx->stream>>>(
         (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
         ctx->spin_limit, ctrl + 1);
     CK(cudaGetLastError(), "recon launch");
