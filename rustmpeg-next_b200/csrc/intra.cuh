@@ -19,8 +19,9 @@ struct IntraWs {
   int16_t fleft[2 * kMaxBlk];
   int16_t ref_above[kRefBuf];
   int16_t ref_left[kRefBuf];
-  int16_t ds_top[kMaxBlk];
+  int16_t ds_top[kMaxBlk];   // CCLM luma templates
   int16_t ds_left[kMaxBlk];
+  int16_t lcol[kMaxBlk];      // CCLM: luma column left of the CU
   int top_left, ftop_left;
   int dc;
 };
@@ -428,7 +429,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
 // CCLM templates and linear models for both chroma components of the chroma
 // block at (bxc, byc): the luma templates of downsample_luma_for_cclm_format_16
 // (predict.rs:3869-3990) go to L.ds_top / L.ds_left, the luma column left of the
-// CU (x = lbx - 1) to L.fleft, and each component's (a, b, shift) of
+// CU (x = lbx - 1) to L.lcol, and each component's (a, b, shift) of
 // predict_cclm_with_format_16 (predict.rs:3996-4066) and
 // derive_cclm_params_from_4_samples (:2088-2177) to Sc[c].dc / ftop_left /
 // top_left. All plane loads of a lane are independent (one round trip).
@@ -445,7 +446,7 @@ __device__ __noinline__ void prep_cclm(const DevPic& P, int bxc, int byc, int cw
   };
   // luma column lbx - 1 next to the tile, rows lby .. lby + tb - 1
   if (lbx > 0)
-    for (int r = lane; r < tb; r += 32) L.fleft[r] = (int16_t)gp(lbx - 1, lby + r);
+    for (int r = lane; r < tb; r += 32) L.lcol[r] = (int16_t)gp(lbx - 1, lby + r);
   int vt = mid, vl = mid;
   const int x = lane, y = lane;
   if (x < cw) {
@@ -599,7 +600,7 @@ __device__ __noinline__ void prep_cclm(const DevPic& P, int bxc, int byc, int cw
 // CCLM prediction of one chroma component fused with reconstruction, for the
 // pairs of `phase`; the downsampled luma of each sample is formed from the
 // CU's reconstructed luma tile (tb x tb at (lbx, lby)) and the prefetched
-// column left of it (L.fleft), as downsample_luma_for_cclm_format_16 does.
+// column left of it (L.lcol), as downsample_luma_for_cclm_format_16 does.
 __device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int byc, int cw, int ch, int lbx,
                           int lby, int tb, const IntraWs& L, const IntraWs& S, const int16_t* tile,
                           const int16_t* res, int phase) {
@@ -608,7 +609,7 @@ __device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int b
   const int a = S.dc, b = S.ftop_left, shift = S.top_left;
   const int bx = bxc * P.sub_w, by = byc * P.sub_h;
   auto T = [&](int x, int y) -> int {  // x >= lbx - 1; y inside the tile
-    return x < lbx ? L.fleft[y - lby] : tile[(y - lby) * tb + (x - lbx)];
+    return x < lbx ? L.lcol[y - lby] : tile[(y - lby) * tb + (x - lbx)];
   };
   auto ds = [&](int x, int y) -> int {
     if (cf == 1) {
