@@ -290,17 +290,6 @@ struct WaveWs {
   int16_t luma[32 * 32];           // the CU's reconstructed luma (for CCLM)
 };
 
-// Bounded wait for a CTU flag; returns false when the poll limit ran out.
-__device__ __forceinline__ bool wait_flag(const uint32_t* flag, uint32_t epoch, uint32_t limit) {
-  uint32_t ns = 32;
-  for (uint32_t it = 0; it < limit; it++) {
-    if (ld_acquire(flag) == epoch) return true;
-    __nanosleep(ns);
-    if (ns < 256) ns <<= 1;
-  }
-  return ld_acquire(flag) == epoch;
-}
-
 // Luma keeps 2 rows / 5 columns for neighbours and CCLM; chroma 1 / 1.
 constexpr int kLumaRows = 2, kLumaCols = 5, kChromaRows = 1, kChromaCols = 1;
 
@@ -338,16 +327,33 @@ __device__ void recon_cu(const DevPic& P, const vvcg_cu_rec& rec, int gx, int gy
   }
 }
 
-__device__ __forceinline__ void publish(uint32_t* flag, uint32_t epoch) {
-  __threadfence();
-  __syncwarp();
-  if ((threadIdx.x & 31) == 0) st_release(flag, epoch);
+// Bounded wait until the CTU row above has finished `need` CTUs in this run
+// (its progress word is (epoch << 32) | count); false when the poll limit ran out.
+__device__ __forceinline__ bool wait_row(const uint64_t* row, uint32_t epoch, uint32_t need,
+                                         uint32_t limit) {
+  uint32_t ns = 64;
+  for (uint32_t it = 0;; it++) {
+    const uint64_t v = ld_relaxed64(row);
+    if ((uint32_t)(v >> 32) == epoch && (uint32_t)v >= need) {
+      fence_acq_rel();
+      return true;
+    }
+    if (it >= limit) return false;
+    __nanosleep(ns);
+    if (ns < 1024) ns <<= 1;
+  }
 }
 
+// The wavefront kernel: one warp per CTU row. Rows are handed out by an atomic
+// counter row-major across the pictures of the batch, so a warp only ever waits
+// on the row above, which a running warp took earlier, and the schedule cannot
+// deadlock. Walking its row left to right, the warp reconstructs a CTU once
+// the row above has finished the CTU above-right of it (or the last CTU of the
+// row), then publishes its own progress. The left neighbour is the warp's own
+// previous CTU, so only the row above needs synchronisation.
 __global__ void __launch_bounds__(kWarpsPerCta * 32, 2)
-k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ items,
-                  uint32_t n_items, uint32_t* counter, uint32_t epoch, uint32_t spin_limit,
-                  uint32_t* status) {
+k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, uint32_t n_rows,
+             uint32_t* counter, uint32_t epoch, uint32_t spin_limit, uint32_t* status) {
   extern __shared__ __align__(16) unsigned char wave_smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   WaveWs& W = reinterpret_cast<WaveWs*>(wave_smem)[wid];
@@ -355,39 +361,34 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(counter, 1u);
     it = __shfl_sync(0xffffffffu, it, 0);
-    if (it >= n_items) break;
-    const CtuItem item = items[it];
+    if (it >= n_rows) break;
+    const RowItem item = rows[it];
     static_assert(sizeof(DevPic) % 4 == 0 && sizeof(DevPic) <= 64 * 4, "DevPic copy");
     for (int i = lane; i < (int)(sizeof(DevPic) / 4); i += 32)
       reinterpret_cast<uint32_t*>(&W.P)[i] = reinterpret_cast<const uint32_t*>(&pics[item.pic])[i];
     __syncwarp();
     const DevPic& P = W.P;
-    const int cx = item.cx, cy = item.cy;
+    const int cy = (int)item.cy;
     const int sh = P.ctu_log2 - ilog2(P.tb);
     const int ncu = 1 << (2 * sh);
-    {
-      int ok = 1;
-      if (lane == 0) {
-        // once any wait has given up the batch result is void: skip the rest
-        ok = (ld_acquire(status) & kStatusTimeout) == 0;
-        if (ok && cx > 0) ok = wait_flag(&P.ctu_done[cy * P.ctu_w + cx - 1], epoch, spin_limit);
-        if (ok && cy > 0) {
-          int tx = cx + 1 < P.ctu_w ? cx + 1 : cx;
-          ok = wait_flag(&P.ctu_done[(cy - 1) * P.ctu_w + tx], epoch, spin_limit);
+    const uint64_t* above = cy > 0 ? P.row_done + (size_t)(cy - 1) * kRowFlagStride : nullptr;
+    uint64_t* mine = P.row_done + (size_t)cy * kRowFlagStride;
+    uint32_t have = 0;  // CTUs of the row above known to be finished
+    for (int cx = 0; cx < P.ctu_w; cx++) {
+      if (above) {
+        const uint32_t need = (uint32_t)min(cx + 2, P.ctu_w);
+        if (have < need) {
+          int ok = 1;
+          if (lane == 0) {
+            // once any wait has given up the batch result is void: skip the rest
+            ok = (ld_acquire(status) & kStatusTimeout) == 0 && wait_row(above, epoch, need, spin_limit);
+            if (!ok) atomicOr(status, kStatusTimeout);
+          }
+          ok = __shfl_sync(0xffffffffu, ok, 0);
+          __syncwarp();
+          have = ok ? need : (uint32_t)P.ctu_w;
         }
-        if (!ok) atomicOr(status, kStatusTimeout);
       }
-      __syncwarp();
-    }
-    uint32_t* flag = &P.ctu_done[cy * P.ctu_w + cx];
-    if (ncu == 1) {
-      // one CU per CTU: publish once the samples other CUs read are stored,
-      // then finish the interior off the wavefront's critical path
-      const vvcg_cu_rec rec = P.cus[cy * P.grid_w + cx];
-      recon_cu(P, rec, cx, cy, W, 1);
-      publish(flag, epoch);
-      recon_cu(P, rec, cx, cy, W, 2);
-    } else {
       for (int k = 0; k < ncu; k++) {
         int lx = 0, ly = 0;
         for (int b = 0; b < sh; b++) {
@@ -397,7 +398,10 @@ k_recon_wavefront(const DevPic* __restrict__ pics, const CtuItem* __restrict__ i
         const int gx = (cx << sh) + lx, gy = (cy << sh) + ly;
         recon_cu(P, P.cus[gy * P.grid_w + gx], gx, gy, W, 0);
       }
-      publish(flag, epoch);
+      // publish: every lane's stores are ordered before the progress word
+      __threadfence();
+      __syncwarp();
+      if (lane == 0) st_release64(mine, ((uint64_t)epoch << 32) | (uint32_t)(cx + 1));
     }
   }
 }

@@ -70,7 +70,7 @@ struct vvcg_ctx {
   uint32_t num_pics = 0;
   std::vector<PicLayout> layout;
   std::vector<DevPic> pics;
-  std::vector<CtuItem> items;
+  std::vector<RowItem> items;
   std::vector<DbfPass> dbf[4];  // luma V, luma H, chroma V, chroma H
   std::vector<SaoPass> sao;
   std::vector<AlfPass> alf;
@@ -249,7 +249,7 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     return VVCG_UNAVAILABLE;
   }
   ctx->stream = ctx->own_stream;
-  if (cudaFuncSetAttribute(k_recon_wavefront, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if (cudaFuncSetAttribute(k_recon_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(kWarpsPerCta * sizeof(WaveWs))) != cudaSuccess) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -311,8 +311,7 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   ctx->num_levels = b->num_levels;
   ctx->num_ctus = b->num_ctus;
   ctx->num_aps = b->num_aps;
-  uint64_t plane_samples = 0, total_ctus = 0;
-  std::vector<uint64_t> flag_base(np);
+  uint64_t plane_samples = 0;
   for (uint32_t i = 0; i < np; i++) {
     const vvcg_pic_desc& d = b->pics[i];
     if (d.ctu_log2 < 5 || d.ctu_log2 > 7)
@@ -364,8 +363,6 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
       plane_samples += c < ncomp ? (uint64_t)L.stride[c] * L.ph[c] : 0;
       L.final_in_scratch[c] = 0;
     }
-    flag_base[i] = total_ctus;
-    total_ctus += (uint64_t)cw_ * ch_;
     DevPic& P = ctx->pics[i];
     P.bd = d.bit_depth;
     P.cf = cf;
@@ -393,27 +390,29 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
       P.ph[c] = L.ph[c];
     }
   }
-  // wavefront order: CTU diagonal t = cx + 2*cy, then picture
+  // wavefront work: CTU rows, row-major across the pictures, so a row is only
+  // handed out after the row above it
+  uint64_t total_rows = 0;
+  std::vector<uint64_t> row_base(np);
   {
-    uint32_t tmax = 0;
-    for (auto& P : ctx->pics) tmax = std::max<uint32_t>(tmax, (P.ctu_w - 1) + 2 * (P.ctu_h - 1));
-    for (uint32_t t = 0; t <= tmax; t++)
-      for (uint32_t i = 0; i < np; i++) {
-        const DevPic& P = ctx->pics[i];
-        for (int cy = 0; cy < P.ctu_h; cy++) {
-          int cx = (int)t - 2 * cy;
-          if (cx < 0 || cx >= P.ctu_w) continue;
-          ctx->items.push_back(CtuItem{i, (uint16_t)cx, (uint16_t)cy});
-        }
-      }
+    int hmax = 0;
+    for (uint32_t i = 0; i < np; i++) {
+      row_base[i] = total_rows;
+      total_rows += ctx->pics[i].ctu_h;
+      hmax = std::max(hmax, ctx->pics[i].ctu_h);
+    }
+    for (int cy = 0; cy < hmax; cy++)
+      for (uint32_t i = 0; i < np; i++)
+        if (cy < ctx->pics[i].ctu_h) ctx->items.push_back(RowItem{i, (uint32_t)cy});
   }
   // device memory
   CK(ctx->planes.reserve(plane_samples * sizeof(uint16_t)), "cudaMalloc planes");
-  if (ctx->flags.cap < total_ctus * sizeof(uint32_t)) {
-    CK(ctx->flags.reserve(total_ctus * sizeof(uint32_t)), "cudaMalloc flags");
+  const size_t flag_bytes = total_rows * kRowFlagStride * sizeof(uint64_t);
+  if (ctx->flags.cap < flag_bytes) {
+    CK(ctx->flags.reserve(flag_bytes), "cudaMalloc flags");
     CK(cudaMemsetAsync(ctx->flags.p, 0, ctx->flags.cap, ctx->stream), "memset flags");
   }
-  ctx->flags_count = total_ctus;
+  ctx->flags_count = total_rows;
   CK(ctx->d_cus.reserve(std::max<uint64_t>(1, b->num_cus) * sizeof(vvcg_cu_rec)), "cudaMalloc");
   CK(ctx->d_levels.reserve(std::max<uint64_t>(1, b->num_levels) * sizeof(int16_t)), "cudaMalloc");
   CK(ctx->d_ctus.reserve(std::max<uint64_t>(1, b->num_ctus) * sizeof(vvcg_ctu_filter)), "cudaMalloc");
@@ -429,7 +428,7 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     }
     P.cus = (const vvcg_cu_rec*)ctx->d_cus.p + d.cu_offset;
     P.ctus = (const vvcg_ctu_filter*)ctx->d_ctus.p + d.ctu_offset;
-    P.ctu_done = (uint32_t*)ctx->flags.p + flag_base[i];
+    P.row_done = (uint64_t*)ctx->flags.p + row_base[i] * kRowFlagStride;
     const int ncomp = P.cf ? 3 : 1;
     if (d.tools & VVCG_TOOL_DEBLOCK) {
       // slice.rs:4990-5020: luma lattice tb, CTB ctu, SliceQpY; chroma lattice
@@ -536,13 +535,13 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     const uint32_t n = (uint32_t)ctx->items.size();
     int per_sm = 0;
     const size_t wave_smem = kWarpsPerCta * sizeof(WaveWs);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_wavefront, kWarpsPerCta * 32,
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_rows, kWarpsPerCta * 32,
                                                      wave_smem),
        "occupancy");
     const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kWarpsPerCta;
     const uint32_t grid = (std::min<uint32_t>(n, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
-    k_recon_wavefront<<<grid, kWarpsPerCta * 32, wave_smem, ctx->stream>>>(
-        (const DevPic*)ctx->d_pics.p, (const CtuItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
+    k_recon_rows<<<grid, kWarpsPerCta * 32, wave_smem, ctx->stream>>>(
+        (const DevPic*)ctx->d_pics.p, (const RowItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
         ctx->spin_limit, ctrl + 1);
     CK(cudaGetLastError(), "recon launch");
     ctx->launches++;

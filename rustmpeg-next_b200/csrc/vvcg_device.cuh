@@ -23,17 +23,19 @@ struct DevPic {
   int32_t pw[3], ph[3];     // plane widths / heights
   const vvcg_cu_rec* cus;   // the picture's records, tb-grid raster order
   const vvcg_ctu_filter* ctus;
-  uint32_t* ctu_done;       // per-CTU epoch flags (CTU raster order)
+  uint64_t* row_done;       // per CTU row: (epoch << 32) | CTUs finished; 128-byte stride
   int32_t bd, cf, ctu_log2, ctu, tb, tb_cw, tb_ch, sub_w, sub_h;
   int32_t grid_w, grid_h, ctu_w, ctu_h;
   int32_t lqp, cqp, slice_qp, tools, aps;
 };
 
-// Work item of the wavefront: a CTU of a picture.
-struct CtuItem {
+// Work item of the wavefront: one CTU row of a picture.
+struct RowItem {
   uint32_t pic;
-  uint16_t cx, cy;
+  uint32_t cy;
 };
+
+constexpr int kRowFlagStride = 16;  // uint64 per row flag: one 128-byte line each
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 __device__ __forceinline__ int ilog2(int v) { return __ffs(v) - 1; }
@@ -51,5 +53,14 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
 __device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release64(uint64_t* p, uint64_t v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 
 }  // namespace vvcg
