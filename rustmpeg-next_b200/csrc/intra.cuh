@@ -10,6 +10,18 @@
 namespace vvcg {
 
 constexpr int kMaxBlk = 32;                                // largest TB of the frame path
+
+// 4-tap cubic intra interpolation taps, one packed word per 1/32 position,
+// staged in shared memory by the kernels that predict (lane-divergent indices
+// would serialise constant-memory reads).
+__shared__ uint32_t s_cubic_taps[32];
+__device__ __forceinline__ void load_cubic_taps() {
+  for (int i = threadIdx.x; i < 32; i += blockDim.x)
+    s_cubic_taps[i] = (uint32_t)(uint8_t)c_chroma_taps4[4 * i] | ((uint32_t)(uint8_t)c_chroma_taps4[4 * i + 1] << 8) |
+                      ((uint32_t)(uint8_t)c_chroma_taps4[4 * i + 2] << 16) |
+                      ((uint32_t)(uint8_t)c_chroma_taps4[4 * i + 3] << 24);
+  __syncthreads();
+}
 constexpr int kRefBuf = (kMaxBlk + 4) + 2 * kMaxBlk + 64;  // predict.rs:3251 buf_len
 
 struct IntraWs {
@@ -187,7 +199,7 @@ __device__ __forceinline__ bool in_phase(int phase, int x, int y, int w, int h, 
 // lane's residual pairs (int16 in a plane-strided buffer, nullable) are all
 // fetched before the first is used, then clip(pred + res) is stored with
 // 32-bit stores. `keep` (nullable) receives the samples (int16 raster, width w).
-constexpr int kMaxPairsPerLane = (kMaxBlk * kMaxBlk / 2) / 32;
+constexpr int kPairChunk = 4;  // pairs per lane fetched and emitted together
 template <class F>
 __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, int y0, int w, int h,
                                            const int16_t* res, int16_t* keep, int phase, int rows,
@@ -197,28 +209,31 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
   const int lw = ilog2(w);
   const int npair = (w * h) >> 1;
   const int st = P.stride[comp];
-  uint32_t rv[kMaxPairsPerLane];
-#pragma unroll
-  for (int k = 0; k < kMaxPairsPerLane; k++) {
-    const int q = lane + 32 * k;
-    const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
-    rv[k] = 0;
-    if (res && q < npair && in_phase(phase, x, y, w, h, rows, cols))
-      rv[k] = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * st + x));
-  }
   uint16_t* base = P.plane[comp] + (size_t)y0 * st + x0;
+#pragma unroll 1
+  for (int k0 = 0; 32 * k0 < npair; k0 += kPairChunk) {
+    uint32_t rv[kPairChunk];
 #pragma unroll
-  for (int k = 0; k < kMaxPairsPerLane; k++) {
-    const int q = lane + 32 * k;
-    const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
-    if (q < npair && in_phase(phase, x, y, w, h, rows, cols)) {
-      int v0, v1;
-      pred(x, y, v0, v1);
-      v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
-      v1 = clampi(v1 + (int)(int16_t)(rv[k] >> 16), 0, maxv);
-      const uint32_t pk = (uint32_t)v0 | ((uint32_t)v1 << 16);
-      *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
-      if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = pk;
+    for (int k = 0; k < kPairChunk; k++) {
+      const int q = lane + 32 * (k0 + k);
+      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+      rv[k] = 0;
+      if (res && q < npair && in_phase(phase, x, y, w, h, rows, cols))
+        rv[k] = __ldcs(reinterpret_cast<const unsigned int*>(res + (size_t)y * st + x));
+    }
+#pragma unroll
+    for (int k = 0; k < kPairChunk; k++) {
+      const int q = lane + 32 * (k0 + k);
+      const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
+      if (q < npair && in_phase(phase, x, y, w, h, rows, cols)) {
+        int v0, v1;
+        pred(x, y, v0, v1);
+        v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
+        v1 = clampi(v1 + (int)(int16_t)(rv[k] >> 16), 0, maxv);
+        const uint32_t pk = (uint32_t)v0 | ((uint32_t)v1 << 16);
+        *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
+        if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = pk;
+      }
     }
   }
   __syncwarp();
@@ -400,10 +415,11 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     } else if (kind == 2) {
       f0 = 16 - (fr >> 1); f1 = 32 - (fr >> 1); f2 = 16 + (fr >> 1); f3 = fr >> 1;
     } else {
-      f0 = c_chroma_taps4[fr * 4 + 0];
-      f1 = c_chroma_taps4[fr * 4 + 1];
-      f2 = c_chroma_taps4[fr * 4 + 2];
-      f3 = c_chroma_taps4[fr * 4 + 3];
+      const uint32_t t = s_cubic_taps[fr];
+      f0 = (int8_t)t;
+      f1 = (int8_t)(t >> 8);
+      f2 = (int8_t)(t >> 16);
+      f3 = (int8_t)(t >> 24);
     }
     const int j = base + di + x;
     int val = clampi((f0 * rm[j] + f1 * rm[j + 1] + f2 * rm[j + 2] + f3 * rm[j + 3] + 32) >> 6, 0, maxv);

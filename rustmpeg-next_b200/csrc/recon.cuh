@@ -351,12 +351,13 @@ __device__ __forceinline__ bool wait_row(const uint64_t* row, uint32_t epoch, ui
 // the row above has finished the CTU above-right of it (or the last CTU of the
 // row), then publishes its own progress. The left neighbour is the warp's own
 // previous CTU, so only the row above needs synchronisation.
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 2)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 3)
 k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, uint32_t n_rows,
              uint32_t* counter, uint32_t epoch, uint32_t spin_limit, uint32_t* status) {
   extern __shared__ __align__(16) unsigned char wave_smem[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   WaveWs& W = reinterpret_cast<WaveWs*>(wave_smem)[wid];
+  load_cubic_taps();
   for (;;) {
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(counter, 1u);
