@@ -230,6 +230,47 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* pred0, const
                                       uint64_t count, uint8_t bcw_idx, uint8_t bit_depth,
                                       uint16_t* out);
 
+/* ---- allocation-free single picture --------------------------------------- */
+
+/* Largest picture height, in CTU rows, that vvcg_recon_picture_static takes
+ * (8192 luma rows with 32x32 CTUs). */
+#define VVCG_STATIC_MAX_CTU_ROWS 256u
+
+/* Reconstructs one picture, and deblocks it when its tools ask for that,
+ * without allocating any memory. No counterpart in the reference: it is a
+ * variant of vvcg_decode_batch for callers that must not allocate, such as a
+ * decoder whose device memory is fixed when it starts, code that must not let
+ * cudaMalloc/cudaFree stall other work queued on the device, or a host whose
+ * own allocator owns all device memory.
+ *
+ * Inputs and outputs are the caller's device memory: `cus` holds the
+ * picture's records from pic->cu_offset on (num_cus entries in all), `levels`
+ * the level pool (num_levels int16 values), and planes[0..2] the Y, Cb and Cr
+ * planes at coded size (width x height, 4:0:0 uses planes[0] only), each
+ * 16-byte aligned with an even stride of at least the plane width. The planes
+ * are also the work space: they first receive the residuals, then the
+ * reconstructed samples. pic is host memory. SAO and ALF are rejected
+ * (VVCG_INVALID_INPUT): they need a second set of planes.
+ *
+ * The library's bookkeeping (queue counter, status word, row progress words,
+ * the picture's descriptor and deblocking passes) lives in one fixed array of
+ * 40 KB in device memory, one per device, which holds up to
+ * VVCG_STATIC_MAX_CTU_ROWS CTU rows; taller pictures return
+ * VVCG_LIMIT_EXCEEDED. The call runs on the calling thread's current device
+ * and on `cuda_stream` (NULL = the legacy default stream), and returns after
+ * the stream has finished the picture.
+ *
+ * The first call on a device does the set-up (it loads the tables, finds the
+ * array's address and sets the kernels' attributes), so make it before any
+ * stream capture. Every call shares the array and leaves the previous call's
+ * contents in it; each call clears the parts that must start at zero. Calls
+ * that overlap in time on one device, from several host threads, race on the
+ * array: serialise them. `err` (may be NULL) receives a message on failure. */
+vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const vvcg_cu_rec* cus,
+                                      uint32_t num_cus, const int16_t* levels,
+                                      uint64_t num_levels, const vvcg_plane_out* planes,
+                                      void* cuda_stream, char* err, size_t err_cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,6 +143,7 @@ def lib():
         L.vvcg_mc_luma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, vp, u32, vp]
         L.vvcg_mc_chroma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, u8, vp, u32, vp]
         L.vvcg_mc_bi_average_16_dev.argtypes = [vp, vp, vp, u64, u8, u8, vp]
+        L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
 
@@ -303,3 +304,27 @@ class Context:
     def mc_bi_average(self, p0, p1, bcw_idx, bit_depth, out):
         self._check(self._L.vvcg_mc_bi_average_16_dev(self._h, _ptr(p0), _ptr(p1), p0.numel(),
                                                       bcw_idx, bit_depth, _ptr(out)))
+
+
+def recon_picture_static(pic, cus, levels, planes, stream=None):
+    """Allocation-free reconstruction (+ deblocking) of one picture in place.
+
+    `pic` is one PIC_DTYPE record; `cus` a CUDA uint8 tensor of CU_DTYPE
+    records; `levels` a CUDA int16 tensor; `planes` the coded-size (Y, Cb, Cr)
+    CUDA int16 tensors the library writes (None for absent chroma). Runs on
+    the current device and `stream` (a torch.cuda.Stream, a raw handle, or
+    None for the legacy default stream) and returns when it has finished.
+    """
+    L = lib()
+    desc = np.asarray(pic, dtype=PIC_DTYPE).reshape(1).copy()
+    arr = (_PlaneOut * 3)()
+    for c in range(3):
+        a = planes[c] if c < len(planes) else None
+        arr[c] = _PlaneOut(None, 0, 0) if a is None else _PlaneOut(_ptr(a), a.stride(0), 0)
+    raw = None if stream is None else getattr(stream, "cuda_stream", stream)
+    err = C.create_string_buffer(512)
+    st = L.vvcg_recon_picture_static(_ptr(desc), _ptr(cus), cus.numel() // CU_DTYPE.itemsize,
+                                     _ptr(levels), levels.numel(), arr,
+                                     C.c_void_p(raw) if raw else None, err, len(err))
+    if st != OK:
+        raise _ERRORS.get(st, Execution)(err.value.decode())

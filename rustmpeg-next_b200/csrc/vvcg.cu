@@ -2,6 +2,7 @@
 // One translation unit: the kernels live in the included .cuh headers.
 #include <cuda_runtime.h>
 #include <stdarg.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -681,3 +682,256 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* p0, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free single-picture reconstruction (vvcg_recon_picture_static).
+//
+// The context entry points above grow their device buffers with cudaMalloc.
+// This one takes records, levels and planes in the caller's device memory and
+// keeps its own bookkeeping in the fixed array g_static_scratch below, which
+// is part of the library's module image: nothing is allocated per call. The
+// residuals go into the caller's planes (DevPic::scratch aliases
+// DevPic::plane): the wavefront kernel reads each sample's residual in the
+// same lane, just before it stores that sample's reconstruction, and
+// neighbouring blocks only read samples that are already reconstructed.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kStaticMaxCtuRows = VVCG_STATIC_MAX_CTU_ROWS;
+
+// Written from the host on every call.
+struct StaticHeader {
+  DevPic pic;
+  DbfPass dbf[6];  // luma V, luma H, Cb V, Cr V, Cb H, Cr H
+  RowItem rows[kStaticMaxCtuRows];
+};
+
+// Byte layout of the array: [0, 256) control words ([0] row queue counter,
+// [1] status word), then one 128-byte progress line per CTU row, then the
+// header. The control words and the progress lines must start at zero.
+constexpr size_t kStaticFlagsOff = 256;
+constexpr size_t kStaticFlagsBytes = (size_t)kStaticMaxCtuRows * kRowFlagStride * sizeof(uint64_t);
+constexpr size_t kStaticHeaderOff = kStaticFlagsOff + kStaticFlagsBytes;
+constexpr size_t kStaticScratchBytes = 40960;
+static_assert(kStaticHeaderOff % 256 == 0, "header alignment");
+static_assert(kStaticHeaderOff + sizeof(StaticHeader) <= kStaticScratchBytes, "scratch array too small");
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+struct StaticDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;  // device address of g_static_scratch
+  int num_sms = 0;
+  int recon_ctas_per_sm = 0;
+};
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mu;
+StaticDevice g_static_dev[kStaticMaxDevices];
+
+vvcg_status static_fail(char* err, size_t cap, vvcg_status st, const char* fmt, ...) {
+  if (err && cap) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, cap, fmt, ap);
+    va_end(ap);
+  }
+  return st;
+}
+
+#define SCK(call, what)                                                                 \
+  do {                                                                                  \
+    cudaError_t _e = (call);                                                            \
+    if (_e != cudaSuccess)                                                              \
+      return static_fail(err, err_cap, VVCG_EXECUTION, "%s: %s", what, cudaGetErrorString(_e)); \
+  } while (0)
+
+// Once per device, with that device current: tables, kernel attributes, the
+// array's device address and the wavefront grid size.
+vvcg_status static_setup(int dev, const StaticDevice** out, char* err, size_t err_cap) {
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (dev < 0 || dev >= kStaticMaxDevices)
+    return static_fail(err, err_cap, VVCG_UNAVAILABLE, "device %d is beyond the %d this entry point tracks",
+                       dev, kStaticMaxDevices);
+  StaticDevice& S = g_static_dev[dev];
+  if (!S.ready) {
+    vvcg_ctx tables_ctx;  // host-side only: carries the device number and an error message
+    tables_ctx.device = dev;
+    if (upload_tables(&tables_ctx) != VVCG_OK)
+      return static_fail(err, err_cap, VVCG_UNAVAILABLE, "%s", tables_ctx.err.c_str());
+    const int wave_smem = (int)(kWarpsPerCta * sizeof(WaveWs));
+    SCK(cudaFuncSetAttribute(k_recon_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, wave_smem),
+        "cudaFuncSetAttribute");
+    void* p = nullptr;
+    SCK(cudaGetSymbolAddress(&p, g_static_scratch), "cudaGetSymbolAddress");
+    SCK(cudaDeviceGetAttribute(&S.num_sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    SCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&S.recon_ctas_per_sm, k_recon_rows,
+                                                      kWarpsPerCta * 32, wave_smem),
+        "occupancy");
+    S.scratch = (unsigned char*)p;
+    S.ready = true;
+  }
+  *out = &S;
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const vvcg_cu_rec* cus,
+                                                 uint32_t num_cus, const int16_t* levels,
+                                                 uint64_t num_levels, const vvcg_plane_out* planes,
+                                                 void* cuda_stream, char* err, size_t err_cap) {
+  if (err && err_cap) err[0] = 0;
+  if (!pic || !planes || !cus) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "missing picture, records or planes");
+  const vvcg_pic_desc& d = *pic;
+  if (d.ctu_log2 < 5 || d.ctu_log2 > 7)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "CTU size outside 32..=128");
+  const uint32_t ctu = 1u << d.ctu_log2;
+  if (d.width < ctu || d.height < ctu || d.width % ctu || d.height % ctu)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "coded size not aligned to the CTU grid");
+  if ((uint64_t)d.width * d.height > kMaxLumaSamples)
+    return static_fail(err, err_cap, VVCG_LIMIT_EXCEEDED, "%ux%u exceeds %llu luma samples", d.width,
+                       d.height, (unsigned long long)kMaxLumaSamples);
+  if (d.height / ctu > kStaticMaxCtuRows)
+    return static_fail(err, err_cap, VVCG_LIMIT_EXCEEDED,
+                       "%u CTU rows; this entry point holds at most %u (use vvcg_decode_batch)",
+                       d.height / ctu, kStaticMaxCtuRows);
+  if (d.bit_depth < 8 || d.bit_depth > 12 || d.chroma_format > 3)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "bit depth or chroma format");
+  if (d.tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF))
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT,
+                       "SAO and ALF need a second set of planes (use vvcg_decode_batch)");
+  const int tb = std::min<int>(ctu, 32);
+  const int cf = d.chroma_format;
+  const int sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
+  const uint32_t gw = d.width / tb, gh = d.height / tb;
+  if ((uint64_t)d.cu_offset + (uint64_t)gw * gh > num_cus)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "CU records out of range");
+  if (num_levels && !levels) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "missing levels");
+  const int ncomp = cf ? 3 : 1;
+
+  StaticHeader h;
+  memset(&h, 0, sizeof(h));
+  DevPic& P = h.pic;
+  for (int c = 0; c < 3; c++) {
+    P.pw[c] = c == 0 ? d.width : (cf ? (d.width + sw - 1) / sw : 0);
+    P.ph[c] = c == 0 ? d.height : (cf ? (d.height + sh - 1) / sh : 0);
+    if (c >= ncomp) continue;
+    const vvcg_plane_out& o = planes[c];
+    if (!o.data || (reinterpret_cast<uintptr_t>(o.data) & 15) || (o.stride & 1) || o.stride < (uint32_t)P.pw[c])
+      return static_fail(err, err_cap, VVCG_INVALID_INPUT,
+                         "plane %d: needs a 16-byte aligned pointer and an even stride >= %d", c, P.pw[c]);
+    P.plane[c] = o.data;
+    P.scratch[c] = o.data;  // residuals first, reconstruction over them
+    P.stride[c] = (int32_t)o.stride;
+  }
+  P.bd = d.bit_depth;
+  P.cf = cf;
+  P.ctu_log2 = d.ctu_log2;
+  P.ctu = ctu;
+  P.tb = tb;
+  P.tb_cw = cf ? std::max(tb / sw, 2) : 0;
+  P.tb_ch = cf ? std::max(tb / sh, 2) : 0;
+  P.sub_w = sw;
+  P.sub_h = sh;
+  P.grid_w = gw;
+  P.grid_h = gh;
+  P.ctu_w = d.width / ctu;
+  P.ctu_h = d.height / ctu;
+  // slice.rs:4681-4682 Qp'Y and Qp'C, both at least 4
+  const int off = 6 * (d.bit_depth - 8);
+  P.lqp = std::max(std::min(63 + off, std::max(0, (int)d.slice_qp + off)), 4);
+  P.cqp = std::max((int)d.chroma_qp_scaled, 4);
+  P.slice_qp = d.slice_qp;
+  P.tools = d.tools;
+  P.aps = -1;
+  P.cus = cus + d.cu_offset;
+  P.ctus = nullptr;
+  for (int cy = 0; cy < P.ctu_h; cy++) h.rows[cy] = RowItem{0, (uint32_t)cy};
+
+  // Deblocking passes: the same lattice, CTB and QP rules as vvcg_batch_prepare
+  // (slice.rs:4990-5020).
+  int n_dbf[4] = {0, 0, 0, 0};  // luma V, luma H, chroma V, chroma H
+  if (d.tools & VVCG_TOOL_DEBLOCK) {
+    const int step = std::max(P.tb, 8), ctb = std::max(P.ctu, step);
+    const int lml = step <= 4 ? 1 : (step >= 32 ? 7 : 3);
+    DbfPass v{P.plane[0], P.stride[0], P.pw[0], P.ph[0], P.bd, step, ctb, (int)d.slice_qp, 2, 0, 0,
+              lml, lml, 1, 0, 0};
+    v.n_edges = (P.pw[0] - 8) / step;
+    v.n_segs = P.ph[0] / 4;
+    DbfPass hz = v;
+    hz.n_edges = (P.ph[0] - 8) / step;
+    hz.n_segs = P.pw[0] / 4;
+    if (v.n_edges > 0 && v.n_segs > 0) h.dbf[n_dbf[0]++] = v;
+    if (hz.n_edges > 0 && hz.n_segs > 0) h.dbf[1 + n_dbf[1]++] = hz;
+    if (cf) {
+      const int cqp = std::min(63, std::max(0, (int)d.slice_qp <= 26 ? (int)d.slice_qp : (int)d.slice_qp - 1));
+      const int cstep = std::max(P.tb_cw, 8);
+      const int cctb = std::max(P.ctu / P.sub_h, cstep);
+      const int clen = cstep >= 8 ? 3 : 1;
+      for (int c = 1; c <= 2; c++) {
+        DbfPass cv{P.plane[c], P.stride[c], P.pw[c], P.ph[c], P.bd, cstep, cctb, cqp, 2, 0, 0,
+                   clen, clen, P.sub_h, 0, 0};
+        cv.n_edges = P.pw[c] >= 8 ? (P.pw[c] - 4) / cstep : 0;
+        cv.n_segs = P.ph[c] / (P.sub_h == 1 ? 4 : 2);
+        DbfPass ch = cv;
+        ch.sub = P.sub_w;
+        ch.n_edges = P.ph[c] >= 8 ? (P.ph[c] - 4) / cstep : 0;
+        ch.n_segs = P.pw[c] / (P.sub_w == 1 ? 4 : 2);
+        if (cv.n_edges > 0 && cv.n_segs > 0) h.dbf[2 + n_dbf[2]++] = cv;
+        if (ch.n_edges > 0 && ch.n_segs > 0) h.dbf[4 + n_dbf[3]++] = ch;
+      }
+    }
+  }
+
+  int dev = 0;
+  SCK(cudaGetDevice(&dev), "cudaGetDevice");
+  const StaticDevice* S = nullptr;
+  vvcg_status st = static_setup(dev, &S, err, err_cap);
+  if (st != VVCG_OK) return st;
+  cudaStream_t s = (cudaStream_t)cuda_stream;
+  unsigned char* base = S->scratch;
+  uint32_t* ctrl = reinterpret_cast<uint32_t*>(base);
+  P.row_done = reinterpret_cast<uint64_t*>(base + kStaticFlagsOff);
+  const DevPic* d_pic = reinterpret_cast<const DevPic*>(base + kStaticHeaderOff + offsetof(StaticHeader, pic));
+  const DbfPass* d_dbf = reinterpret_cast<const DbfPass*>(base + kStaticHeaderOff + offsetof(StaticHeader, dbf));
+  const RowItem* d_rows = reinterpret_cast<const RowItem*>(base + kStaticHeaderOff + offsetof(StaticHeader, rows));
+
+  // control words and this picture's progress lines start at zero; the header
+  // is rewritten whole up to the last row item in use
+  SCK(cudaMemsetAsync(base, 0, kStaticFlagsOff + (size_t)P.ctu_h * kRowFlagStride * sizeof(uint64_t), s),
+      "clear scratch");
+  SCK(cudaMemcpyAsync(base + kStaticHeaderOff, &h, offsetof(StaticHeader, rows) + sizeof(RowItem) * P.ctu_h,
+                      cudaMemcpyHostToDevice, s),
+      "header upload");
+  const uint32_t ncus = gw * gh;
+  k_residual<<<dim3((ncus + kWarpsPerCta - 1) / kWarpsPerCta, 1), kWarpsPerCta * 32, 0, s>>>(
+      d_pic, levels, num_levels, ctrl + 1);
+  SCK(cudaGetLastError(), "residual launch");
+  const uint32_t warps = (uint32_t)S->num_sms * std::max(1, S->recon_ctas_per_sm) * kWarpsPerCta;
+  const uint32_t grid = (std::min<uint32_t>((uint32_t)P.ctu_h, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
+  const uint32_t epoch = 1;  // progress lines were cleared above
+  k_recon_rows<<<grid, kWarpsPerCta * 32, kWarpsPerCta * sizeof(WaveWs), s>>>(
+      d_pic, d_rows, (uint32_t)P.ctu_h, ctrl, epoch, kDefaultSpinLimit, ctrl + 1);
+  SCK(cudaGetLastError(), "recon launch");
+  for (int k = 0; k < 4; k++) {
+    const int n = n_dbf[k];
+    if (!n) continue;
+    const int first = k == 0 ? 0 : (k == 1 ? 1 : (k == 2 ? 2 : 4));
+    uint32_t maxw = 0;
+    for (int i = 0; i < n; i++) maxw = std::max<uint32_t>(maxw, (uint32_t)(h.dbf[first + i].n_edges * h.dbf[first + i].n_segs));
+    dim3 g((maxw + 127) / 128, (unsigned)n);
+    if (k == 0) k_deblock_luma<true><<<g, 128, 0, s>>>(d_dbf + first, n);
+    if (k == 1) k_deblock_luma<false><<<g, 128, 0, s>>>(d_dbf + first, n);
+    if (k == 2) k_deblock_chroma<true><<<g, 128, 0, s>>>(d_dbf + first, n);
+    if (k == 3) k_deblock_chroma<false><<<g, 128, 0, s>>>(d_dbf + first, n);
+    SCK(cudaGetLastError(), "deblock launch");
+  }
+  uint32_t status = 0;
+  SCK(cudaMemcpyAsync(&status, ctrl + 1, sizeof(status), cudaMemcpyDeviceToHost, s), "status");
+  SCK(cudaStreamSynchronize(s), "synchronize");
+  if (status & kStatusTimeout)
+    return static_fail(err, err_cap, VVCG_TIMEOUT, "a wavefront wait gave up after %u polls", kDefaultSpinLimit);
+  if (status & kStatusBadRecord) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "a level offset was out of range");
+  return VVCG_OK;
+}
