@@ -230,6 +230,51 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* pred0, const
                                       uint64_t count, uint8_t bcw_idx, uint8_t bit_depth,
                                       uint16_t* out);
 
+/* ---- transform units (function level, batched, device buffers) ---------- */
+
+enum {
+  VVCG_TU_DEP_QUANT = 1u << 0,      /* dependent quantisation (4-state) */
+  VVCG_TU_TRANSFORM_SKIP = 1u << 1, /* transform skip: per-sample (de)quantisation */
+  VVCG_TU_BDPCM_HOR = 1u << 2,      /* inverse only: BDPCM accumulation along rows */
+  VVCG_TU_BDPCM_VER = 1u << 3,      /* inverse only: BDPCM accumulation along columns */
+  VVCG_TU_IMPLICIT_MTS = 1u << 4,   /* DST-7 for a dimension in 4..16 when mts_idx and
+                                       lfnst_idx are 0 (luma, no MIP) */
+  VVCG_TU_INTER = 1u << 5           /* forward only: inter rounding offset (85, not 171) */
+};
+
+typedef struct vvcg_tu_rec {
+  uint8_t log2_w, log2_h; /* 0..6 each, w * h >= 2 */
+  uint8_t bit_depth;      /* 8..12 */
+  uint8_t qp;             /* Qp' = QP + QpBdOffset, 0..87 */
+  uint8_t flags;          /* VVCG_TU_* */
+  uint8_t mts_idx;        /* 0, or 1..4: (DST7,DST7) (DCT8,DST7) (DST7,DCT8) (DCT8,DCT8) */
+  uint8_t lfnst_idx;      /* 0..2 (ignored by the inverse when mts_idx != 0) */
+  uint8_t lfnst_mode;     /* LFNST intra mode index 0..94 (lfnst::get_lfnst_intra_mode of the
+                             wide-angle mode) */
+  uint32_t in_off;        /* first int16 input element (raster, w*h) */
+  uint32_t out_off;       /* first int16 output element (raster, w*h) */
+} vvcg_tu_rec;            /* 16 bytes */
+
+/* Levels -> residual of each transform unit: transform-skip or regular /
+ * dependent dequantisation, inverse LFNST, inverse DCT-2 / DST-7 / DCT-8 with
+ * the zero-out rules, then BDPCM. Replaces: residual_of + inverse_residual
+ * (crates/rustmpeg-video/src/vvc/decode_general.rs:4100-4199) and the BDPCM
+ * step of reconstruct_tu (decode_general.rs:4055-4060, predict.rs:4224). `recs`
+ * is host memory; `in`/`out` are device buffers of in_count / out_count int16.
+ * Asynchronous on the context's stream. */
+vvcg_status vvcg_tu_inverse_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
+                                  const int16_t* in, uint64_t in_count, int16_t* out,
+                                  uint64_t out_count);
+/* Residual -> levels: forward transform, forward LFNST and regular / dependent
+ * / transform-skip quantisation. Replaces: the level side of plan_primary and
+ * plan_transform_skip (slice.rs:690-760) over dct::forward_transform_rect_bd
+ * (dct.rs:865), lfnst::forward_lfnst_rect (lfnst.rs:131), quantize_rect_bd
+ * (dct.rs:1113), quantize_dep_quant_bd (dct.rs:1252), quantize_ts
+ * (transform.rs:214). */
+vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
+                                  const int16_t* in, uint64_t in_count, int16_t* out,
+                                  uint64_t out_count);
+
 /* ---- allocation-free single picture --------------------------------------- */
 
 /* Largest picture height, in CTU rows, that vvcg_recon_picture_static takes

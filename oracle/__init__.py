@@ -91,6 +91,7 @@ def _declare(L):
     L.orc_encode_frame.argtypes = [vp, vp, vp, i, i, i, i, i, i, i, vp, vp, C.c_uint64,
                                    C.POINTER(C.c_uint64), vp, vp, vp]
     L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    L.orc_tu_batch.argtypes = [i, vp, i, vp, vp]
 
 
 # ---------------------------------------------------------------- transforms --
@@ -377,3 +378,24 @@ def recon_frame(pic, cus, levels, ctus, aps=None):
     rc = lib().orc_recon_frame(_p(pic), _p(cus), _p(levels), _p(ctus),
                                None if aps_arr is None else _p(aps_arr), _p(y), _p(u), _p(v))
     return rc, (y, u, v)
+
+
+# ------------------------------------------------------------ transform units --
+
+TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("qp", "u1"),
+                     ("flags", "u1"), ("mts_idx", "u1"), ("lfnst_idx", "u1"),
+                     ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
+TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
+
+
+def tu_batch(recs, data, out_count, forward=False):
+    """Run a transform-unit batch (TU_DTYPE records) over int16 `data`.
+
+    Returns (rc, out): rc is 0, or -(i + 1) for the first record the
+    reference rejects (later records are not run).
+    """
+    recs = np.ascontiguousarray(recs, dtype=TU_DTYPE)
+    data = np.ascontiguousarray(data, dtype=np.int16)
+    out = np.zeros(out_count, np.int16)
+    rc = lib().orc_tu_batch(1 if forward else 0, _p(recs), len(recs), _p(data), _p(out))
+    return rc, out

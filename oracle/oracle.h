@@ -138,6 +138,25 @@ void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, in
 void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int bd,
                             uint16_t* out);
 
+// ---- transform units (orc_tu.cpp) ------------------------------------------------
+// Same layout and flag values as vvcg_tu_rec / VVCG_TU_* of the C ABI.
+enum : uint8_t {
+  kTuDepQuant = 1,
+  kTuTransformSkip = 2,
+  kTuBdpcmHor = 4,
+  kTuBdpcmVer = 8,
+  kTuImplicitMts = 16,
+  kTuInter = 32,
+};
+struct TuRec {
+  uint8_t log2_w, log2_h, bit_depth, qp, flags, mts_idx, lfnst_idx, lfnst_mode;
+  uint32_t in_off, out_off;
+};
+static_assert(sizeof(TuRec) == 16, "TuRec layout");
+// Return 0, or a negative code where the reference returns an error.
+int tu_inverse(const TuRec& r, const int16_t* in, int16_t* out);
+int tu_forward(const TuRec& r, const int16_t* in, int16_t* out);
+
 // ---- hls.rs ---------------------------------------------------------------------
 int scaled_luma_qp_bd(int qpy, int bd);
 int derived_chroma_qp_bd(int qpy, int bd, int chroma_qp_offset);

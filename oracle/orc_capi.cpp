@@ -131,4 +131,16 @@ void orc_bi_average(const int32_t* p0, const int32_t* p1, int n, int bcw, int bd
   weighted_average_bi_16(p0, p1, n, bcw, bd, out);
 }
 
+// Runs every record of a transform-unit batch; returns 0, or -(i + 1) for
+// the first record the reference rejects.
+int orc_tu_batch(int forward, const void* recs, int n, const int16_t* in, int16_t* out) {
+  const TuRec* r = (const TuRec*)recs;
+  for (int i = 0; i < n; i++) {
+    int rc = forward ? tu_forward(r[i], in + r[i].in_off, out + r[i].out_off)
+                     : tu_inverse(r[i], in + r[i].in_off, out + r[i].out_off);
+    if (rc) return -(i + 1);
+  }
+  return 0;
+}
+
 }  // extern "C"

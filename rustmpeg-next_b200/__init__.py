@@ -40,7 +40,12 @@ MC_BLOCK_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<u2"), ("h", "<u2"
                            ("mv_x", "<i4"), ("mv_y", "<i4"), ("flags", "<u4"),
                            ("reserved", "<u4"), ("out_offset", "<u8")], align=True)
 
+TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("qp", "u1"),
+                     ("flags", "u1"), ("mts_idx", "u1"), ("lfnst_idx", "u1"),
+                     ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
+
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
+TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
 MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4
 CHROMA_400, CHROMA_420, CHROMA_422, CHROMA_444 = 0, 1, 2, 3
@@ -99,7 +104,7 @@ class _Config(C.Structure):
 
 
 assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize == 32
-assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40
+assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.itemsize == 16
 
 
 def build(force: bool = False) -> str:
@@ -143,6 +148,8 @@ def lib():
         L.vvcg_mc_luma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, vp, u32, vp]
         L.vvcg_mc_chroma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, u8, vp, u32, vp]
         L.vvcg_mc_bi_average_16_dev.argtypes = [vp, vp, vp, u64, u8, u8, vp]
+        for n in ("vvcg_tu_inverse_batch", "vvcg_tu_forward_batch"):
+            getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -300,6 +307,21 @@ class Context:
         self._check(self._L.vvcg_mc_chroma_16_dev(self._h, _ptr(ref), w, h, ref.stride(0),
                                                   bit_depth, chroma_format, _ptr(blocks), n,
                                                   _ptr(out)))
+
+    # -- transform units (records on the host, int16 CUDA tensors) --
+    def tu_inverse(self, recs, data, out):
+        """Levels -> residual for every TU_DTYPE record (asynchronous on the stream)."""
+        recs = np.ascontiguousarray(recs, dtype=TU_DTYPE)
+        self._keep = recs
+        self._check(self._L.vvcg_tu_inverse_batch(self._h, _ptr(recs), len(recs), _ptr(data),
+                                                  data.numel(), _ptr(out), out.numel()))
+
+    def tu_forward(self, recs, data, out):
+        """Residual -> levels for every TU_DTYPE record (asynchronous on the stream)."""
+        recs = np.ascontiguousarray(recs, dtype=TU_DTYPE)
+        self._keep = recs
+        self._check(self._L.vvcg_tu_forward_batch(self._h, _ptr(recs), len(recs), _ptr(data),
+                                                  data.numel(), _ptr(out), out.numel()))
 
     def mc_bi_average(self, p0, p1, bcw_idx, bit_depth, out):
         self._check(self._L.vvcg_mc_bi_average_16_dev(self._h, _ptr(p0), _ptr(p1), p0.numel(),

@@ -15,6 +15,7 @@
 #include "filters.cuh"
 #include "mc.cuh"
 #include "recon.cuh"
+#include "tu.cuh"
 #include "vvc_tables.h"
 #include "vvcg_device.cuh"
 #include "vvcg_tables_dev.cuh"
@@ -79,6 +80,9 @@ struct vvcg_ctx {
   // device memory
   DevBuf planes, flags, d_pics, d_items, d_dbf[4], d_sao, d_alf, d_cus, d_levels, d_ctus, d_aps,
       d_ctrl;  // d_ctrl: [0] queue counter, [1] status word
+  // transform-unit batches
+  std::vector<uint32_t> tu_idx;
+  DevBuf d_tu_recs, d_tu_idx;
   uint64_t flags_count = 0;
 };
 
@@ -202,6 +206,21 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
     }
   CK(cudaMemcpyToSymbol(g_scan, scans.data(), sizeof(int16_t) * pos), "tables");
   CK(cudaMemcpyToSymbol(g_scan_off, offs, sizeof(offs)), "tables");
+  // every (log2 w, log2 h) in 0..6 for the transform-unit kernels
+  std::vector<int16_t> tu_scans(kTuScanTotal, 0);
+  int32_t tu_offs[49];
+  pos = 0;
+  for (int a = 0; a <= 6; a++)
+    for (int b = 0; b <= 6; b++) {
+      tu_offs[a * 7 + b] = pos;
+      pos += build_scan(1 << a, 1 << b, tu_scans.data() + pos);
+    }
+  if (pos != kTuScanTotal) return fail(ctx, VVCG_EXECUTION, "scan table size %d", pos);
+  CK(cudaMemcpyToSymbol(g_tu_scan, tu_scans.data(), sizeof(int16_t) * pos), "tables");
+  CK(cudaMemcpyToSymbol(g_tu_scan_off, tu_offs, sizeof(tu_offs)), "tables");
+  CK(cudaMemcpyToSymbol(g_lfnst8, kLfnst8x8, sizeof(kLfnst8x8)), "tables");
+  CK(cudaMemcpyToSymbol(g_lfnst4, kLfnst4x4, sizeof(kLfnst4x4)), "tables");
+  CK(cudaMemcpyToSymbol(g_lfnst_lut, kLfnstLut, sizeof(kLfnstLut)), "tables");
   CK(cudaDeviceSynchronize(), "tables");
   if (ctx->device < 64) g_tables_ready[ctx->device] = true;
   return VVCG_OK;
@@ -256,6 +275,14 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     delete ctx;
     return VVCG_UNAVAILABLE;
   }
+  if (cudaFuncSetAttribute(k_tu<4096, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tu_smem_bytes<4096, 2>()) != cudaSuccess ||
+      cudaFuncSetAttribute(k_tu<4096, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tu_smem_bytes<4096, 2>()) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
   if (upload_tables(ctx) != VVCG_OK) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -278,7 +305,8 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
-                    &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl})
+                    &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
+                    &ctx->d_tu_recs, &ctx->d_tu_idx})
     b->release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -682,6 +710,100 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* p0, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Transform-unit batches (vvcg_tu_inverse_batch / vvcg_tu_forward_batch).
+// ---------------------------------------------------------------------------
+namespace {
+
+// Why the reference would reject a unit (dct.rs matrix_for_any / zero-out
+// checks, lfnst.rs parameters_rect, slice.rs:701 MTS with LFNST), or nullptr.
+const char* tu_reject(const vvcg_tu_rec& r, bool forward, uint64_t in_count, uint64_t out_count) {
+  if (r.log2_w > 6 || r.log2_h > 6 || r.log2_w + r.log2_h == 0) return "size outside 1x2..64x64";
+  const uint32_t n = 1u << (r.log2_w + r.log2_h);
+  if (r.bit_depth < 8 || r.bit_depth > 12) return "bit depth outside 8..=12";
+  if (r.qp > 87) return "Qp' above 87";
+  if ((uint64_t)r.in_off + n > in_count) return "input range past the buffer";
+  if ((uint64_t)r.out_off + n > out_count) return "output range past the buffer";
+  if (forward && (r.flags & (VVCG_TU_BDPCM_HOR | VVCG_TU_BDPCM_VER))) return "BDPCM is inverse only";
+  if ((r.flags & VVCG_TU_BDPCM_HOR) && (r.flags & VVCG_TU_BDPCM_VER)) return "two BDPCM directions";
+  if (r.flags & VVCG_TU_TRANSFORM_SKIP) return nullptr;
+  if (r.mts_idx > 4) return "mts_idx above 4";
+  if (r.lfnst_idx > 2) return "lfnst_idx above 2";
+  if (forward && r.lfnst_idx && r.mts_idx) return "MTS combined with LFNST";
+  TuShape S;
+  tu_shape(r, S);
+  auto has = [](int tr, int lg) { return tr == 0 ? (lg >= 1 && lg <= 6) : (lg >= 2 && lg <= 5); };
+  if (S.w > 1 && (!has(S.th, S.lw) || S.sw >= S.w)) return "unsupported horizontal transform";
+  if (S.h > 1 && (!has(S.tv, S.lh) || S.sh >= S.h)) return "unsupported vertical transform";
+  if (r.lfnst_idx > 0 && r.mts_idx == 0 && (S.w < 4 || S.h < 4 || r.lfnst_mode >= 95)) return "unsupported LFNST";
+  return nullptr;
+}
+
+vvcg_status tu_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t n, const int16_t* in,
+                     uint64_t in_count, int16_t* out, uint64_t out_count, bool forward) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (n == 0) return VVCG_OK;
+  if (!recs || !in || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing records or buffers");
+  uint32_t count[3] = {0, 0, 0};
+  for (uint32_t i = 0; i < n; i++) {
+    if (const char* why = tu_reject(recs[i], forward, in_count, out_count))
+      return fail(ctx, VVCG_INVALID_INPUT, "transform unit %u: %s", i, why);
+    const uint32_t el = 1u << (recs[i].log2_w + recs[i].log2_h);
+    count[el <= 256 ? 0 : (el <= 1024 ? 1 : 2)]++;
+  }
+  // units grouped by size bin
+  ctx->tu_idx.resize(n);
+  uint32_t at[3] = {0, count[0], count[0] + count[1]};
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t el = 1u << (recs[i].log2_w + recs[i].log2_h);
+    ctx->tu_idx[at[el <= 256 ? 0 : (el <= 1024 ? 1 : 2)]++] = i;
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_tu_rec) * n), "cudaMalloc");
+  CK(ctx->d_tu_idx.reserve(sizeof(uint32_t) * n), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, recs, sizeof(vvcg_tu_rec) * n, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  CK(cudaMemcpyAsync(ctx->d_tu_idx.p, ctx->tu_idx.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  const vvcg_tu_rec* d_recs = (const vvcg_tu_rec*)ctx->d_tu_recs.p;
+  const uint32_t* d_idx = (const uint32_t*)ctx->d_tu_idx.p;
+  if (count[0]) {
+    auto k = forward ? k_tu<256, kTuWarps, true> : k_tu<256, kTuWarps, false>;
+    k<<<(count[0] + kTuWarps - 1) / kTuWarps, kTuWarps * 32, tu_smem_bytes<256, kTuWarps>(), ctx->stream>>>(
+        d_recs, d_idx, count[0], in, out);
+    CK(cudaGetLastError(), "transform-unit launch");
+    ctx->launches++;
+  }
+  if (count[1]) {
+    auto k = forward ? k_tu<1024, kTuWarps, true> : k_tu<1024, kTuWarps, false>;
+    k<<<(count[1] + kTuWarps - 1) / kTuWarps, kTuWarps * 32, tu_smem_bytes<1024, kTuWarps>(), ctx->stream>>>(
+        d_recs, d_idx + count[0], count[1], in, out);
+    CK(cudaGetLastError(), "transform-unit launch");
+    ctx->launches++;
+  }
+  if (count[2]) {
+    auto k = forward ? k_tu<4096, 2, true> : k_tu<4096, 2, false>;
+    k<<<(count[2] + 1) / 2, 64, tu_smem_bytes<4096, 2>(), ctx->stream>>>(d_recs, d_idx + count[0] + count[1],
+                                                                         count[2], in, out);
+    CK(cudaGetLastError(), "transform-unit launch");
+    ctx->launches++;
+  }
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_tu_inverse_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
+                                             const int16_t* in, uint64_t in_count, int16_t* out,
+                                             uint64_t out_count) {
+  return tu_batch(ctx, recs, num_recs, in, in_count, out, out_count, false);
+}
+
+extern "C" vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
+                                             const int16_t* in, uint64_t in_count, int16_t* out,
+                                             uint64_t out_count) {
+  return tu_batch(ctx, recs, num_recs, in, in_count, out, out_count, true);
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free single-picture reconstruction (vvcg_recon_picture_static).

@@ -201,3 +201,84 @@ def synthetic_aps(rng, n_filters=25, luma_clip=True):
     aps["coeff"][0, :n_filters] = fixed[rng.integers(0, 64, n_filters), :12]
     aps["clip_idx"][0, :n_filters] = rng.integers(0, 4, (n_filters, 12))
     return aps
+
+
+# Shapes (log2 w, log2 h) of the transform units a random QT/MT tiling of
+# 4x4..64x64 blocks produces, with the luma/chroma weights of 4:2:0, plus the
+# narrow shapes ISP and 2xN chroma give.
+_TU_SHAPES = [(a, b) for a in range(2, 7) for b in range(2, 7) if abs(a - b) <= 2]
+_TU_ODD_SHAPES = [(0, 4), (4, 0), (0, 3), (1, 3), (3, 1), (1, 2), (2, 1), (1, 1), (0, 1), (1, 0), (1, 4),
+                  (0, 6), (6, 0), (1, 5), (5, 1)]
+
+
+def random_tu_records(n, seed=0, forward=False, bit_depths=(8, 10), qp_range=(22, 37), odd_frac=0.05,
+                      tools=True):
+    """Seeded transform-unit records (TU_DTYPE) and their int16 inputs.
+
+    Inverse (forward=False): sparse low-frequency levels, a few at the int16
+    limits. Forward: residuals of +-2^bd range with a smooth component.
+    `tools` mixes in DQ, transform skip, BDPCM, implicit / explicit MTS and
+    LFNST where the unit's shape allows them. Returns (recs, data, out_count).
+    """
+    from . import TU_DTYPE, TU_BDPCM_HOR, TU_BDPCM_VER, TU_DEP_QUANT, TU_IMPLICIT_MTS, TU_INTER, \
+        TU_TRANSFORM_SKIP
+
+    rng = np.random.default_rng(seed)
+    recs = np.zeros(n, TU_DTYPE)
+    shapes = np.array(_TU_SHAPES)[rng.integers(0, len(_TU_SHAPES), n)]
+    odd = rng.random(n) < odd_frac
+    shapes[odd] = np.array(_TU_ODD_SHAPES)[rng.integers(0, len(_TU_ODD_SHAPES), int(odd.sum()))]
+    recs["log2_w"], recs["log2_h"] = shapes[:, 0], shapes[:, 1]
+    bd = np.array(bit_depths)[rng.integers(0, len(bit_depths), n)]
+    recs["bit_depth"] = bd
+    qp = rng.integers(qp_range[0], qp_range[1] + 1, n) + 6 * (bd - 8)
+    recs["qp"] = np.clip(qp, 0, 87)
+    w, h = 1 << shapes[:, 0], 1 << shapes[:, 1]
+    size = w * h
+    if tools:
+        r = rng.random(n)
+        mts_ok = (w >= 4) & (h >= 4) & (w <= 32) & (h <= 32)
+        lfnst_ok = (w >= 4) & (h >= 4)
+        ts_ok = (w <= 32) & (h <= 32)
+        flags = np.where(rng.random(n) < 0.5, TU_DEP_QUANT, 0)
+        ts = ts_ok & (r < 0.15)
+        flags = np.where(ts, TU_TRANSFORM_SKIP, flags)
+        if not forward:
+            bd_dir = rng.integers(0, 3, n)
+            flags = np.where(ts & (bd_dir == 1), flags | TU_BDPCM_HOR, flags)
+            flags = np.where(ts & (bd_dir == 2), flags | TU_BDPCM_VER, flags)
+        mts = mts_ok & ~ts & (r >= 0.15) & (r < 0.4)
+        recs["mts_idx"] = np.where(mts, rng.integers(1, 5, n), 0)
+        lf = lfnst_ok & ~ts & (r >= 0.4) & (r < 0.65)
+        recs["lfnst_idx"] = np.where(lf, rng.integers(1, 3, n), 0)
+        recs["lfnst_mode"] = rng.integers(0, 95, n)
+        imp = ~ts & (r >= 0.65) & (r < 0.8)
+        flags = np.where(imp, flags | TU_IMPLICIT_MTS, flags)
+        if forward:
+            flags = np.where(rng.random(n) < 0.3, flags | TU_INTER, flags)
+        recs["flags"] = flags
+    offs = np.zeros(n + 1, np.int64)
+    offs[1:] = np.cumsum(size)
+    recs["in_off"] = offs[:-1]
+    recs["out_off"] = offs[:-1]
+    total = int(offs[-1])
+    data = np.zeros(total, np.int16)
+    for i in range(n):
+        ww, hh, o = int(w[i]), int(h[i]), int(offs[i])
+        if forward:
+            amp = 1 << int(bd[i])
+            yy, xx = np.mgrid[0:hh, 0:ww]
+            smooth = (amp // 4) * np.sin(xx * rng.random() + yy * rng.random() + rng.random() * 6)
+            v = smooth + rng.integers(-amp // 2, amp // 2 + 1, (hh, ww))
+            data[o:o + ww * hh] = np.clip(v, -amp, amp).astype(np.int16).reshape(-1)
+        else:
+            k = min(ww * hh, 1 + int(rng.geometric(0.15)))
+            ys = np.minimum((rng.exponential(hh / 6, k)).astype(int), hh - 1)
+            xs = np.minimum((rng.exponential(ww / 6, k)).astype(int), ww - 1)
+            mag = rng.geometric(0.35, k) * rng.choice([-1, 1], k)
+            big = rng.random(k) < 0.01
+            mag = np.where(big, rng.choice([-32768, 32767], k), mag)
+            blk = np.zeros((hh, ww), np.int32)
+            blk[ys, xs] = mag
+            data[o:o + ww * hh] = np.clip(blk, -32768, 32767).astype(np.int16).reshape(-1)
+    return recs, data, total
