@@ -70,7 +70,10 @@ enum {
   VVCG_TOOL_DEP_QUANT = 1u << 0, /* dependent quantisation (dep_quant) */
   VVCG_TOOL_DEBLOCK = 1u << 1,   /* enable_deblock */
   VVCG_TOOL_SAO = 1u << 2,       /* enable_sao */
-  VVCG_TOOL_ALF = 1u << 3        /* enable_alf */
+  VVCG_TOOL_ALF = 1u << 3,       /* enable_alf */
+  /* encoder only (vvcg_encode_batch): */
+  VVCG_TOOL_ENC_FULL_INTRA = 1u << 4, /* all 7 searched luma modes, not only Planar / DC */
+  VVCG_TOOL_ENC_CCLM = 1u << 5        /* chroma mode by SAD among DM and the 3 CCLM modes */
 };
 
 /* One picture of the 8..12-bit frame path: the inputs of
@@ -229,6 +232,38 @@ vvcg_status vvcg_mc_chroma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w
 vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* pred0, const int32_t* pred1,
                                       uint64_t count, uint8_t bcw_idx, uint8_t bit_depth,
                                       uint16_t* out);
+
+/* ---- encoder (frame path) ------------------------------------------------ */
+
+/* Source planes of one picture for vvcg_encode_batch: coded size, host or
+ * device memory (the copy direction is inferred). */
+typedef struct vvcg_plane_in {
+  const uint16_t* data;
+  uint32_t stride; /* samples */
+  uint32_t reserved;
+} vvcg_plane_in;
+
+/* Encodes a batch of pictures: per CU the 7-mode SAD intra decision, the
+ * prediction, forward DCT-2, regular or dependent quantisation and the
+ * encoder's own reconstruction, in CTU wavefront order, then deblocking when
+ * the picture asks for it. Replaces: slice::encode_vvc_frame_picture
+ * (crates/rustmpeg-video/src/vvc/slice.rs:4171-4634) without the CABAC
+ * writes. pics[i].chroma_qp_scaled is derived from slice_qp here
+ * (hls.rs:796 derived_chroma_qp_bd); tools may hold DEP_QUANT, DEBLOCK,
+ * ENC_FULL_INTRA and ENC_CCLM. `src` holds 3 planes per picture.
+ * Outputs (host or device memory): one record per tb-grid cell (cu_offset is
+ * assigned in picture order; level_off indexes `levels`, -1 when the TB has no
+ * nonzero level) and the level pool, where each CU owns a slot of
+ * tb*tb + 2*tb_cw*tb_ch levels (see vvcg_encode_levels_size). The
+ * reconstructed pictures stay in the context: vvcg_batch_plane and
+ * vvcg_batch_download read them, and vvcg_batch_run(VVCG_STAGE_RECON) decodes
+ * the emitted records again. Synchronous. */
+vvcg_status vvcg_encode_batch(vvcg_ctx* ctx, const vvcg_pic_desc* pics, uint32_t num_pics,
+                              const vvcg_plane_in* src, vvcg_cu_rec* cus, uint32_t cus_cap,
+                              int16_t* levels, uint64_t levels_cap);
+/* Records and level-pool entries vvcg_encode_batch writes for these pictures. */
+vvcg_status vvcg_encode_sizes(const vvcg_pic_desc* pics, uint32_t num_pics, uint32_t* num_cus,
+                              uint64_t* num_levels);
 
 /* ---- transform units (function level, batched, device buffers) ---------- */
 

@@ -45,6 +45,7 @@ TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("
                      ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
 
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
+TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM = 16, 32
 TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
 MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4
@@ -95,6 +96,10 @@ class _Batch(C.Structure):
 
 
 class _PlaneOut(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("stride", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _PlaneIn(C.Structure):
     _fields_ = [("data", C.c_void_p), ("stride", C.c_uint32), ("reserved", C.c_uint32)]
 
 
@@ -150,6 +155,8 @@ def lib():
         L.vvcg_mc_bi_average_16_dev.argtypes = [vp, vp, vp, u64, u8, u8, vp]
         for n in ("vvcg_tu_inverse_batch", "vvcg_tu_forward_batch"):
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
+        L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
+        L.vvcg_encode_batch.argtypes = [vp, vp, u32, vp, vp, u32, vp, u64]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -307,6 +314,36 @@ class Context:
         self._check(self._L.vvcg_mc_chroma_16_dev(self._h, _ptr(ref), w, h, ref.stride(0),
                                                   bit_depth, chroma_format, _ptr(blocks), n,
                                                   _ptr(out)))
+
+    # -- encoder --
+    def encode_batch(self, pics, srcs):
+        """Encode pictures (PIC_DTYPE; srcs: [(y, u, v)] coded-size uint16 arrays
+        or CUDA tensors). Returns (cus, levels) as host arrays; the
+        reconstruction stays in the context (download / plane)."""
+        pics = np.ascontiguousarray(pics, dtype=PIC_DTYPE)
+        nc, nl = C.c_uint32(), C.c_uint64()
+        st = self._L.vvcg_encode_sizes(_ptr(pics), len(pics), C.byref(nc), C.byref(nl))
+        if st != OK:
+            raise _ERRORS.get(st, Execution)("invalid picture geometry")
+        arr = (_PlaneIn * (3 * len(pics)))()
+        keep = []
+        for i, planes in enumerate(srcs):
+            for c in range(3):
+                a = planes[c] if c < len(planes) else None
+                if a is None:
+                    arr[i * 3 + c] = _PlaneIn(None, 0, 0)
+                    continue
+                if not hasattr(a, "data_ptr"):
+                    a = np.ascontiguousarray(a, dtype=np.uint16)
+                keep.append(a)
+                stride = a.stride(0) if hasattr(a, "data_ptr") else a.strides[0] // 2
+                arr[i * 3 + c] = _PlaneIn(_ptr(a), stride, 0)
+        cus = np.zeros(nc.value, CU_DTYPE)
+        levels = np.zeros(max(1, nl.value), np.int16)
+        self._keep = (pics, keep, arr)
+        self._check(self._L.vvcg_encode_batch(self._h, _ptr(pics), len(pics), arr, _ptr(cus), nc.value,
+                                              _ptr(levels), nl.value))
+        return cus, levels[:nl.value]
 
     # -- transform units (records on the host, int16 CUDA tensors) --
     def tu_inverse(self, recs, data, out):

@@ -112,11 +112,13 @@ __device__ __forceinline__ int ldp(const uint16_t* p) { return __ldcg(p); }
 
 // Reference samples with the frame path's availability rules:
 // gather_references_16 (predict.rs:3016-3076) followed by the coded-unit
-// substitution of predict_coded_block_16 (predict.rs:3101-3135). All loads of a
-// lane are issued before any is used (one L2 round trip); reads go to L2
-// (ld.cg) because the samples were written by other SMs.
+// substitution of predict_coded_block_16 (predict.rs:3101-3135); `plain`
+// leaves the substitution out (predict_block_16, which the encoder's mode
+// decisions use: h left samples, 2w above whether coded or not).
+// All loads of a lane are issued before any is used (one L2 round trip);
+// reads go to L2 (ld.cg) because the samples were written by other SMs.
 __device__ void warp_gather_refs(const DevPic& P, int comp, int x, int y, int w, int h,
-                                 uint32_t cur_order, IntraWs& S) {
+                                 uint32_t cur_order, IntraWs& S, bool plain) {
   const int lane = threadIdx.x & 31;
   const uint16_t* pl = P.plane[comp];
   const int st = P.stride[comp], pw = P.pw[comp], ph = P.ph[comp];
@@ -132,14 +134,16 @@ __device__ void warp_gather_refs(const DevPic& P, int comp, int x, int y, int w,
     if (ha && i < 2 * w) {
       int avail = min(pw - x, 2 * w);
       int px = x + (i < avail ? i : avail - 1);
-      if (i >= w && x + i < pw && !is_coded_luma(P, (x + i) * sx, (y - 1) * sy, cur_order)) px = x + w - 1;
+      if (!plain && i >= w && x + i < pw && !is_coded_luma(P, (x + i) * sx, (y - 1) * sy, cur_order))
+        px = x + w - 1;
       pa[t] = &pl[(size_t)(y - 1) * st + px];
     }
     const int j = lane + 32 * t;
     if (hl && j < 2 * h) {
       int avail = min(ph - y, h);
       int py = y + (j < avail ? j : avail - 1);
-      if (j >= h && y + j < ph && is_coded_luma(P, (x - 1) * sx, (y + j) * sy, cur_order)) py = y + j;
+      if (!plain && j >= h && y + j < ph && is_coded_luma(P, (x - 1) * sx, (y + j) * sy, cur_order))
+        py = y + j;
       pll[t] = &pl[(size_t)py * st + x - 1];
     }
   }
@@ -198,12 +202,13 @@ __device__ __forceinline__ bool in_phase(int phase, int x, int y, int w, int h, 
 // `pred(x, y, v0, v1)` gives the prediction of the pair (x, x+1) of row y; the
 // lane's residual pairs (int16 in a plane-strided buffer, nullable) are all
 // fetched before the first is used, then clip(pred + res) is stored with
-// 32-bit stores. `keep` (nullable) receives the samples (int16 raster, width w).
+// 32-bit stores (into the plane when `store`). `keep` (nullable) receives the
+// samples (int16 raster, width w).
 constexpr int kPairChunk = 4;  // pairs per lane fetched and emitted together
 template <class F>
 __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, int y0, int w, int h,
-                                           const int16_t* res, int16_t* keep, int phase, int rows,
-                                           int cols, F&& pred) {
+                                           const int16_t* res, int16_t* keep, bool store, int phase,
+                                           int rows, int cols, F&& pred) {
   const int lane = threadIdx.x & 31;
   const int maxv = (1 << P.bd) - 1;
   const int lw = ilog2(w);
@@ -231,7 +236,7 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
         v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
         v1 = clampi(v1 + (int)(int16_t)(rv[k] >> 16), 0, maxv);
         const uint32_t pk = (uint32_t)v0 | ((uint32_t)v1 << 16);
-        *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
+        if (store) *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
         if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = pk;
       }
     }
@@ -244,11 +249,11 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
 // value, and the extended main/side reference arrays of angular modes
 // (predict_angular_16, predict.rs:3240-3305).
 __device__ __noinline__ void prep_intra(const DevPic& P, int comp, int x0, int y0, int w, int h, bool is_luma,
-                           int mode, uint32_t order, IntraWs& S) {
+                           int mode, uint32_t order, IntraWs& S, bool plain = false) {
   const int lane = threadIdx.x & 31;
   const int bd = P.bd, maxv = (1 << bd) - 1;
   const int lw = ilog2(w), lh = ilog2(h);
-  warp_gather_refs(P, comp, x0, y0, w, h, order, S);
+  warp_gather_refs(P, comp, x0, y0, w, h, order, S, plain);
   if (mode == 0) {
     if (is_luma && w * h > 32) warp_filter_refs(w, h, S);
     return;
@@ -318,10 +323,11 @@ __device__ __noinline__ void prep_intra(const DevPic& P, int comp, int x0, int y
 // reconstruction, for the pairs of `phase`: planar / DC are
 // predict_from_refs_16 + apply_pdpc_16 (predict.rs:3138-3215), angular is
 // predict_angular_16 (:3223-3410), other mode values predict zeros
-// (predict.rs:3194). `keep` (optional) receives the reconstructed samples.
+// (predict.rs:3194). `keep` (optional) receives the reconstructed samples;
+// without `store` only `keep` is written (a prediction, when `res` is null).
 __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y0, int w, int h, bool is_luma,
                            int mode, const IntraWs& S, const int16_t* res, int16_t* keep, int phase,
-                           int rows, int cols) {
+                           int rows, int cols, bool store = true) {
   const int bd = P.bd, maxv = (1 << bd) - 1;
   const int lw = ilog2(w), lh = ilog2(h);
   if (mode == 0) {
@@ -331,7 +337,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     const int shift = lw + lh + 1;
     const int tr = A[w], bl = L[h];
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
       const int left = L[ry];
       const int wt = 32 >> min(31, (ry * 2) >> sc);
       int v[2];
@@ -353,7 +359,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
   if (mode == 1) {
     const int dc = S.dc;
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
       const int wt = 32 >> min(31, (ry * 2) >> sc);
       int wl0 = 32 >> min(31, (rx0 * 2) >> sc), wl1 = 32 >> min(31, ((rx0 + 1) * 2) >> sc);
       v0 = clampi(dc + ((wl0 * (S.left[ry] - dc) + wt * (S.above[rx0] - dc) + 32) >> 6), 0, maxv);
@@ -362,7 +368,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     return;
   }
   if (mode < 2 || mode > 66) {
-    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int, int, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int, int, int& v0, int& v1) {
       v0 = 0;
       v1 = 0;
     });
@@ -386,7 +392,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
       }
       return val;
     };
-    emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
       if (p.is_ver) {
         v0 = sample(ox0, oy);
         v1 = sample(ox0 + 1, oy);
@@ -431,7 +437,7 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     }
     return val;
   };
-  emit_block(P, comp, x0, y0, w, h, res, keep, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
+  emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
     if (p.is_ver) {
       v0 = sample(ox0, oy);
       v1 = sample(ox0 + 1, oy);
@@ -619,7 +625,7 @@ __device__ __noinline__ void prep_cclm(const DevPic& P, int bxc, int byc, int cw
 // column left of it (L.lcol), as downsample_luma_for_cclm_format_16 does.
 __device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int byc, int cw, int ch, int lbx,
                           int lby, int tb, const IntraWs& L, const IntraWs& S, const int16_t* tile,
-                          const int16_t* res, int phase) {
+                          const int16_t* res, int phase, int16_t* keep = nullptr, bool store = true) {
   const int maxv = (1 << P.bd) - 1;
   const int cf = P.cf;
   const int a = S.dc, b = S.ftop_left, shift = S.top_left;
@@ -642,7 +648,7 @@ __device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int b
     }
     return T(bx + x, by + y);
   };
-  emit_block(P, comp, bxc, byc, cw, ch, res, nullptr, phase, 1, 1, [&](int x, int y, int& v0, int& v1) {
+  emit_block(P, comp, bxc, byc, cw, ch, res, keep, store, phase, 1, 1, [&](int x, int y, int& v0, int& v1) {
     v0 = clampi(((ds(x, y) * a) >> shift) + b, 0, maxv);
     v1 = clampi(((ds(x + 1, y) * a) >> shift) + b, 0, maxv);
   });

@@ -344,20 +344,19 @@ __device__ __forceinline__ bool wait_row(const uint64_t* row, uint32_t epoch, ui
   }
 }
 
-// The wavefront kernel: one warp per CTU row. Rows are handed out by an atomic
-// counter row-major across the pictures of the batch, so a warp only ever waits
-// on the row above, which a running warp took earlier, and the schedule cannot
-// deadlock. Walking its row left to right, the warp reconstructs a CTU once
-// the row above has finished the CTU above-right of it (or the last CTU of the
-// row), then publishes its own progress. The left neighbour is the warp's own
-// previous CTU, so only the row above needs synchronisation.
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 3)
-k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, uint32_t n_rows,
-             uint32_t* counter, uint32_t epoch, uint32_t spin_limit, uint32_t* status) {
-  extern __shared__ __align__(16) unsigned char wave_smem[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  WaveWs& W = reinterpret_cast<WaveWs*>(wave_smem)[wid];
-  load_cubic_taps();
+// The CTU-row wavefront, shared by reconstruction and encoding: one warp per
+// CTU row. Rows are handed out by an atomic counter row-major across the
+// pictures of the batch, so a warp only ever waits on the row above, which a
+// running warp took earlier, and the schedule cannot deadlock. Walking its row
+// left to right, the warp codes a CTU once the row above has finished the CTU
+// above-right of it (or the last CTU of the row), then publishes its own
+// progress. The left neighbour is the warp's own previous CTU, so only the row
+// above needs synchronisation. `cu(gx, gy)` codes one CU with W.P set.
+template <class Ws, class CuFn>
+__device__ __forceinline__ void wavefront_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows,
+                                               uint32_t n_rows, uint32_t* counter, uint32_t epoch,
+                                               uint32_t spin_limit, uint32_t* status, Ws& W, CuFn&& cu) {
+  const int lane = threadIdx.x & 31;
   for (;;) {
     uint32_t it = 0;
     if (lane == 0) it = atomicAdd(counter, 1u);
@@ -396,8 +395,7 @@ k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, 
           lx |= ((k >> (2 * b)) & 1) << b;
           ly |= ((k >> (2 * b + 1)) & 1) << b;
         }
-        const int gx = (cx << sh) + lx, gy = (cy << sh) + ly;
-        recon_cu(P, P.cus[gy * P.grid_w + gx], gx, gy, W, 0);
+        cu((cx << sh) + lx, (cy << sh) + ly);
       }
       // publish: every lane's stores are ordered before the progress word
       __threadfence();
@@ -405,6 +403,19 @@ k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, 
       if (lane == 0) st_release64(mine, ((uint64_t)epoch << 32) | (uint32_t)(cx + 1));
     }
   }
+}
+
+// Reconstruction wavefront over the batch's CTU rows.
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 3)
+k_recon_rows(const DevPic* __restrict__ pics, const RowItem* __restrict__ rows, uint32_t n_rows,
+             uint32_t* counter, uint32_t epoch, uint32_t spin_limit, uint32_t* status) {
+  extern __shared__ __align__(16) unsigned char wave_smem[];
+  const int wid = threadIdx.x >> 5;
+  WaveWs& W = reinterpret_cast<WaveWs*>(wave_smem)[wid];
+  load_cubic_taps();
+  wavefront_rows(pics, rows, n_rows, counter, epoch, spin_limit, status, W, [&](int gx, int gy) {
+    recon_cu(W.P, W.P.cus[gy * W.P.grid_w + gx], gx, gy, W, 0);
+  });
 }
 
 }  // namespace vvcg

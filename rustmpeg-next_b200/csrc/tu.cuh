@@ -182,8 +182,10 @@ __device__ void tu_dq_dequant(int32_t* A, const TuShape& S, int qp_scaled, int b
 }
 
 // dct.rs:1252-1301 quantize_dep_quant_bd: coefficients A (raster) -> levels,
-// written to `out` (global, raster; zero outside the scan).
-__device__ void tu_dq_quant(const int32_t* A, const TuShape& S, int qp_scaled, int bd, int16_t* out,
+// written to `out` (raster; zero outside the scan). `out` may be A itself:
+// each lane reads a coefficient before it writes that position's level.
+template <class OutT>
+__device__ void tu_dq_quant(const int32_t* A, const TuShape& S, int qp_scaled, int bd, OutT* out,
                             int lane) {
   const int16_t* scan = tu_scan(S.lw, S.lh);
   const int ns = min(S.w, 32) * min(S.h, 32);
@@ -214,7 +216,7 @@ __device__ void tu_dq_quant(const int32_t* A, const TuShape& S, int qp_scaled, i
   for (int s = hi; s >= lo; s--) {
     const int c = A[scan[s]];
     const int L = level_of(qest(c), c, st);
-    out[scan[s]] = (int16_t)L;
+    out[scan[s]] = (OutT)L;
     st = dq_next(st, L);
   }
   if (ns < S.n)

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/vvcg.h"
+#include "enc.cuh"
 #include "filters.cuh"
 #include "mc.cuh"
 #include "recon.cuh"
@@ -271,6 +272,12 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
   ctx->stream = ctx->own_stream;
   if (cudaFuncSetAttribute(k_recon_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(kWarpsPerCta * sizeof(WaveWs))) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  if (cudaFuncSetAttribute(k_encode_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(kEncWarps * sizeof(EncWs))) != cudaSuccess) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return VVCG_UNAVAILABLE;
@@ -710,6 +717,136 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* p0, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Encoder (vvcg_encode_batch).
+// ---------------------------------------------------------------------------
+namespace {
+
+// hls.rs:796-802 derived_chroma_qp_bd with a zero chroma QP offset.
+int derived_chroma_qp_bd_host(int qpy, int bd) {
+  const int off = 6 * (bd - 8);
+  const int qpi = std::min(63, std::max(-off, qpy));
+  const int mapped = qpi <= 26 ? qpi : qpi - 1;
+  const int base = std::min(63, std::max(-off, mapped)) + off;
+  return std::min(63 + off, std::max(0, base));
+}
+
+// CU records and level-pool entries of one picture (one slot of
+// tb*tb + 2*tb_cw*tb_ch levels per CU); false for a geometry the frame path
+// rejects (slice.rs:129-160).
+bool encode_geometry(const vvcg_pic_desc& d, uint32_t* cus, uint64_t* levels) {
+  if (d.ctu_log2 < 5 || d.ctu_log2 > 7 || d.chroma_format > 3) return false;
+  const uint32_t ctu = 1u << d.ctu_log2;
+  if (d.width < ctu || d.height < ctu || d.width % ctu || d.height % ctu) return false;
+  const int tb = std::min<int>(ctu, 32), cf = d.chroma_format;
+  const int sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
+  const int tcw = cf ? std::max(tb / sw, 2) : 0, tch = cf ? std::max(tb / sh, 2) : 0;
+  *cus = (d.width / tb) * (d.height / tb);
+  *levels = (uint64_t)*cus * (uint64_t)(tb * tb + 2 * tcw * tch);
+  return true;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_encode_sizes(const vvcg_pic_desc* pics, uint32_t num_pics, uint32_t* num_cus,
+                                         uint64_t* num_levels) {
+  if (!pics || !num_cus || !num_levels) return VVCG_INVALID_INPUT;
+  uint64_t c = 0, l = 0;
+  for (uint32_t i = 0; i < num_pics; i++) {
+    uint32_t pc;
+    uint64_t pl;
+    if (!encode_geometry(pics[i], &pc, &pl)) return VVCG_INVALID_INPUT;
+    c += pc;
+    l += pl;
+  }
+  if (c > 0xffffffffull || l > 0x7fffffffull) return VVCG_LIMIT_EXCEEDED;
+  *num_cus = (uint32_t)c;
+  *num_levels = l;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_encode_batch(vvcg_ctx* ctx, const vvcg_pic_desc* pics, uint32_t num_pics,
+                                         const vvcg_plane_in* src, vvcg_cu_rec* cus, uint32_t cus_cap,
+                                         int16_t* levels, uint64_t levels_cap) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!pics || !num_pics || !src || !cus || !levels) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  uint32_t total_cus = 0;
+  uint64_t total_levels = 0;
+  vvcg_status st = vvcg_encode_sizes(pics, num_pics, &total_cus, &total_levels);
+  if (st != VVCG_OK) return fail(ctx, st, "picture geometry outside the frame path or too many levels");
+  if (cus_cap < total_cus || levels_cap < total_levels)
+    return fail(ctx, VVCG_INVALID_INPUT, "outputs need %u records and %llu levels", total_cus,
+                (unsigned long long)total_levels);
+  std::vector<vvcg_pic_desc> d(pics, pics + num_pics);
+  std::vector<uint32_t> lv_base(num_pics);
+  uint32_t cu_at = 0;
+  uint64_t lv_at = 0;
+  for (uint32_t i = 0; i < num_pics; i++) {
+    if (d[i].tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF))
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: the encoder does not apply SAO or ALF", i);
+    if (d[i].slice_qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "picture %u: slice QP above 63", i);
+    for (int c = 0; c < (d[i].chroma_format ? 3 : 1); c++)
+      if (!src[i * 3 + c].data) return fail(ctx, VVCG_INVALID_INPUT, "picture %u: missing source plane %d", i, c);
+    uint32_t pc;
+    uint64_t pl;
+    encode_geometry(d[i], &pc, &pl);
+    d[i].chroma_qp_scaled = (uint8_t)derived_chroma_qp_bd_host(d[i].slice_qp, d[i].bit_depth);
+    d[i].cu_offset = cu_at;
+    d[i].ctu_offset = 0;
+    d[i].alf_aps = -1;
+    lv_base[i] = (uint32_t)lv_at;
+    cu_at += pc;
+    lv_at += pl;
+  }
+  std::vector<vvcg_cu_rec> none(total_cus);
+  for (auto& r : none) r = vvcg_cu_rec{0, 0, 0, 0, {-1, -1, -1}};
+  vvcg_batch b{d.data(), num_pics, total_cus, none.data(), nullptr, 0, nullptr, 0, 0, nullptr};
+  if ((st = vvcg_batch_prepare(ctx, &b)) != VVCG_OK) return st;
+  ctx->prepared = false;  // until the encode has finished
+  CK(ctx->d_levels.reserve(std::max<uint64_t>(1, total_levels) * sizeof(int16_t)), "cudaMalloc levels");
+  ctx->num_levels = total_levels;
+  for (uint32_t i = 0; i < num_pics; i++) {
+    ctx->pics[i].lv_pool = (int16_t*)ctx->d_levels.p;
+    ctx->pics[i].lv_base = (int32_t)lv_base[i];
+  }
+  if ((st = upload_vec(ctx, ctx->d_pics, ctx->pics)) != VVCG_OK) return st;
+  CK(cudaMemsetAsync(ctx->d_levels.p, 0, total_levels * sizeof(int16_t), ctx->stream), "memset levels");
+  for (uint32_t i = 0; i < num_pics; i++) {
+    const DevPic& P = ctx->pics[i];
+    for (int c = 0; c < (P.cf ? 3 : 1); c++) {
+      // the mode decisions read not-yet-coded samples as 0 (zeroed planes)
+      CK(cudaMemsetAsync(P.plane[c], 0, (size_t)P.stride[c] * P.ph[c] * sizeof(uint16_t), ctx->stream), "memset");
+      const vvcg_plane_in& in = src[i * 3 + c];
+      if (in.stride < (uint32_t)P.pw[c]) return fail(ctx, VVCG_INVALID_INPUT, "picture %u: source stride", i);
+      CK(cudaMemcpy2DAsync(P.scratch[c], (size_t)P.stride[c] * 2, in.data, (size_t)in.stride * 2,
+                           (size_t)P.pw[c] * 2, P.ph[c], cudaMemcpyDefault, ctx->stream),
+         "source upload");
+    }
+  }
+  uint32_t* ctrl = (uint32_t*)ctx->d_ctrl.p;
+  CK(cudaMemsetAsync(ctrl, 0, 2 * sizeof(uint32_t), ctx->stream), "memset");
+  ctx->epoch++;
+  const uint32_t n = (uint32_t)ctx->items.size();
+  const size_t smem = kEncWarps * sizeof(EncWs);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_encode_rows, kEncWarps * 32, smem), "occupancy");
+  const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kEncWarps;
+  const uint32_t grid = (std::min<uint32_t>(n, warps) + kEncWarps - 1) / kEncWarps;
+  k_encode_rows<<<grid, kEncWarps * 32, smem, ctx->stream>>>((const DevPic*)ctx->d_pics.p,
+                                                            (const RowItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
+                                                            ctx->spin_limit, ctrl + 1);
+  CK(cudaGetLastError(), "encode launch");
+  ctx->launches++;
+  ctx->prepared = true;
+  if ((st = vvcg_batch_sync(ctx)) != VVCG_OK) return st;
+  if ((st = vvcg_batch_run(ctx, VVCG_STAGE_DEBLOCK)) != VVCG_OK) return st;
+  CK(cudaMemcpyAsync(cus, ctx->d_cus.p, sizeof(vvcg_cu_rec) * total_cus, cudaMemcpyDefault, ctx->stream),
+     "records download");
+  CK(cudaMemcpyAsync(levels, ctx->d_levels.p, sizeof(int16_t) * total_levels, cudaMemcpyDefault, ctx->stream),
+     "levels download");
+  return vvcg_batch_sync(ctx);
+}
 
 // ---------------------------------------------------------------------------
 // Transform-unit batches (vvcg_tu_inverse_batch / vvcg_tu_forward_batch).

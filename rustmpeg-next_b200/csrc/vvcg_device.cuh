@@ -27,6 +27,10 @@ struct DevPic {
   int32_t bd, cf, ctu_log2, ctu, tb, tb_cw, tb_ch, sub_w, sub_h;
   int32_t grid_w, grid_h, ctu_w, ctu_h;
   int32_t lqp, cqp, slice_qp, tools, aps;
+  // encoder: level pool and the picture's first slot in it (one slot of
+  // tb*tb + 2*tb_cw*tb_ch levels per CU, raster order)
+  int16_t* lv_pool;
+  int32_t lv_base;
 };
 
 // Work item of the wavefront: one CTU row of a picture.

@@ -282,3 +282,29 @@ def random_tu_records(n, seed=0, forward=False, bit_depths=(8, 10), qp_range=(22
             blk[ys, xs] = mag
             data[o:o + ww * hh] = np.clip(blk, -32768, 32767).astype(np.int16).reshape(-1)
     return recs, data, total
+
+
+def source_planes(w, h, bd=10, cf=1, seed=0, vis=None):
+    """Coded-size (w x h) source planes of value-noise content at bit depth bd
+    and chroma format cf; the visible part is vis = (vw, vh), the rest is the
+    reference's edge padding."""
+    vw, vh = vis or (w, h)
+    y, u, v = value_noise_frame(vw, vh, 10, frame=seed)
+
+    def scale(p):
+        return (p.astype(np.int32) << bd >> 10).astype(np.uint16) if bd > 10 else (p >> (10 - bd)).astype(np.uint16)
+
+    if bd != 10:
+        y, u, v = scale(y), scale(u), scale(v)
+    if cf == 0:
+        return pad_to(y, w, h), None, None
+    sw = 2 if cf in (1, 2) else 1
+    sh = 2 if cf == 1 else 1
+    cw, ch = (w + sw - 1) // sw, (h + sh - 1) // sh
+    if cf == 3:
+        u = np.kron(u, np.ones((2, 2), np.uint16))[:vh, :vw]
+        v = np.kron(v, np.ones((2, 2), np.uint16))[:vh, :vw]
+    elif cf == 2:
+        u = np.repeat(u, 2, axis=0)[:vh]
+        v = np.repeat(v, 2, axis=0)[:vh]
+    return pad_to(y, w, h), pad_to(u, cw, ch), pad_to(v, cw, ch)
