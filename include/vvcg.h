@@ -327,7 +327,8 @@ vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32
  * picture's records from pic->cu_offset on (num_cus entries in all), `levels`
  * the level pool (num_levels int16 values), and planes[0..2] the Y, Cb and Cr
  * planes at coded size (width x height, 4:0:0 uses planes[0] only), each
- * 16-byte aligned with an even stride of at least the plane width. The planes
+ * 16-byte aligned with a stride of at least the plane width that is a
+ * multiple of 8 samples. The planes
  * are also the work space: they first receive the residuals, then the
  * reconstructed samples. pic is host memory. SAO and ALF are rejected
  * (VVCG_INVALID_INPUT): they need a second set of planes.

@@ -34,7 +34,7 @@ __device__ __forceinline__ bool luma_sample_dec(int p0, int p3, int q0, int q3, 
 }
 
 // filter.rs:311-468 decide_luma_edge
-__device__ bool decide_luma(const int (*ln)[16], int beta, int tc, int lpi, int lqi, bool ctb_hor,
+__device__ __forceinline__ bool decide_luma(const int (*ln)[16], int beta, int tc, int lpi, int lqi, bool ctb_hor,
                             LumaEdgeDec* e) {
   const int* l0 = ln[0];
   const int* l3 = ln[3];
@@ -59,9 +59,12 @@ __device__ bool decide_luma(const int (*ln)[16], int beta, int tc, int lpi, int 
     int sq3l = len_q == 7 ? sq3 + abs(LQ(l3, 4) - LQ(l3, 5) - LQ(l3, 6) + LQ(l3, 7)) : sq3;
     int d0l = dp0l + dq0l, d3l = dp3l + dq3l;
     if (d0l + d3l < beta) {
-      bool s0 = luma_sample_dec(lp ? LP(l0, len_p) : 0, lp ? LP(l0, 3) : 0, lq ? LQ(l0, len_q) : 0,
+      // len_p / len_q are 3, 5 or 7 here
+      auto at_p = [&](const int* l) { return len_p == 7 ? LP(l, 7) : len_p == 5 ? LP(l, 5) : LP(l, 3); };
+      auto at_q = [&](const int* l) { return len_q == 7 ? LQ(l, 7) : len_q == 5 ? LQ(l, 5) : LQ(l, 3); };
+      bool s0 = luma_sample_dec(lp ? at_p(l0) : 0, lp ? LP(l0, 3) : 0, lq ? at_q(l0) : 0,
                                 lq ? LQ(l0, 3) : 0, 2 * d0l, sp0l, sq0l, spq0, lp, lq, beta, tc);
-      bool s3 = luma_sample_dec(lp ? LP(l3, len_p) : 0, lp ? LP(l3, 3) : 0, lq ? LQ(l3, len_q) : 0,
+      bool s3 = luma_sample_dec(lp ? at_p(l3) : 0, lp ? LP(l3, 3) : 0, lq ? at_q(l3) : 0,
                                 lq ? LQ(l3, 3) : 0, 2 * d3l, sp3l, sq3l, spq3, lp, lq, beta, tc);
       if (s0 && s3) {
         *e = LumaEdgeDec{3, len_p, len_q, true, true};
@@ -94,7 +97,7 @@ __device__ bool decide_luma(const int (*ln)[16], int beta, int tc, int lpi, int 
 }
 
 // filter.rs:477-582 long_tap_luma_line (in place on a 16-sample line)
-__device__ void long_tap_line(int* l, int np, int nq, int tc, int maxv) {
+__device__ __forceinline__ void long_tap_line(int* l, int np, int nq, int tc, int maxv) {
   int m[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) m[i] = l[i];
@@ -117,31 +120,35 @@ __device__ void long_tap_line(int* l, int np, int nq, int tc, int maxv) {
   else
     rm = (2 * (MP(0) + MQ(0)) + MP(1) + MQ(1) + MP(2) + MQ(2) + MP(3) + MQ(3) + MP(4) + MQ(4) +
           MP(5) + MQ(5) + MP(6) + MQ(6) + 8) >> 4;
-  const int ref_p = (MP(np) + MP(np - 1) + 1) >> 1;
-  const int ref_q = (MQ(nq) + MQ(nq - 1) + 1) >> 1;
+  // lengths are 3, 5 or 7: every index below is a compile-time constant
+  const int ref_p = np == 7 ? (MP(7) + MP(6) + 1) >> 1 : np == 5 ? (MP(5) + MP(4) + 1) >> 1 : (MP(3) + MP(2) + 1) >> 1;
+  const int ref_q = nq == 7 ? (MQ(7) + MQ(6) + 1) >> 1 : nq == 5 ? (MQ(5) + MQ(4) + 1) >> 1 : (MQ(3) + MQ(2) + 1) >> 1;
   const int c7[7] = {59, 50, 41, 32, 23, 14, 5}, t7[7] = {6, 5, 4, 3, 2, 1, 1};
-  const int c5[5] = {58, 45, 32, 19, 6}, t5[5] = {6, 5, 4, 3, 2};
-  const int c3[3] = {53, 32, 11}, t3[3] = {6, 4, 2};
-  for (int pos = 0; pos < np; pos++) {
-    int f = np == 7 ? c7[pos] : (np == 5 ? c5[pos] : c3[pos]);
-    int t = np == 7 ? t7[pos] : (np == 5 ? t5[pos] : t3[pos]);
-    int o = MP(pos), cv = (tc * t) >> 1;
-    int it = (rm * f + ref_p * (64 - f) + 32) >> 6;
-    l[7 - pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
-  }
-  for (int pos = 0; pos < nq; pos++) {
-    int f = nq == 7 ? c7[pos] : (nq == 5 ? c5[pos] : c3[pos]);
-    int t = nq == 7 ? t7[pos] : (nq == 5 ? t5[pos] : t3[pos]);
-    int o = MQ(pos), cv = (tc * t) >> 1;
-    int it = (rm * f + ref_q * (64 - f) + 32) >> 6;
-    l[8 + pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
+  const int c5[7] = {58, 45, 32, 19, 6, 0, 0}, t5[7] = {6, 5, 4, 3, 2, 0, 0};
+  const int c3[7] = {53, 32, 11, 0, 0, 0, 0}, t3[7] = {6, 4, 2, 0, 0, 0, 0};
+#pragma unroll
+  for (int pos = 0; pos < 7; pos++) {
+    if (pos < np) {
+      int f = np == 7 ? c7[pos] : (np == 5 ? c5[pos] : c3[pos]);
+      int t = np == 7 ? t7[pos] : (np == 5 ? t5[pos] : t3[pos]);
+      int o = MP(pos), cv = (tc * t) >> 1;
+      int it = (rm * f + ref_p * (64 - f) + 32) >> 6;
+      l[7 - pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
+    }
+    if (pos < nq) {
+      int f = nq == 7 ? c7[pos] : (nq == 5 ? c5[pos] : c3[pos]);
+      int t = nq == 7 ? t7[pos] : (nq == 5 ? t5[pos] : t3[pos]);
+      int o = MQ(pos), cv = (tc * t) >> 1;
+      int it = (rm * f + ref_q * (64 - f) + 32) >> 6;
+      l[8 + pos] = clampi(clampi(it, o - cv, o + cv), 0, maxv);
+    }
   }
 #undef MP
 #undef MQ
 }
 
 // filter.rs:586-631 short_filter_luma_line
-__device__ void short_line(int* l, const LumaEdgeDec& e, int tc, int maxv) {
+__device__ __forceinline__ void short_line(int* l, const LumaEdgeDec& e, int tc, int maxv) {
   int m[16];
 #pragma unroll
   for (int i = 0; i < 16; i++) m[i] = l[i];
@@ -207,26 +214,62 @@ __global__ void k_deblock_luma(const DbfPass* __restrict__ passes, int n_pass) {
   int ln[4][16];
   uint16_t* pl = D.plane;
   const int st = D.stride;
-  for (int k = 0; k < 4; k++)
-    for (int i = 0; i < 16; i++)
-      ln[k][i] = kVertical ? pl[(size_t)(seg + k) * st + pos - 8 + i] : pl[(size_t)(pos - 8 + i) * st + seg + k];
+  // vertical edges: one row of 16 samples is two 16-byte loads (pos - 8 is a
+  // multiple of 8); horizontal edges: the 4 columns of a row are one 8-byte load
+  if (kVertical) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint4* r = reinterpret_cast<const uint4*>(pl + (size_t)(seg + k) * st + pos - 8);
+      const uint4 a = r[0], b = r[1];
+      const uint32_t wv[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        ln[k][2 * i] = (int)(wv[i] & 0xFFFFu);
+        ln[k][2 * i + 1] = (int)(wv[i] >> 16);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+      const uint2 v = *reinterpret_cast<const uint2*>(pl + (size_t)(pos - 8 + i) * st + seg);
+      ln[0][i] = (int)(v.x & 0xFFFFu);
+      ln[1][i] = (int)(v.x >> 16);
+      ln[2][i] = (int)(v.y & 0xFFFFu);
+      ln[3][i] = (int)(v.y >> 16);
+    }
+  }
   bool ctb_hor = !kVertical && (pos % D.ctb) == 0;
   LumaEdgeDec dec;
   if (!decide_luma(ln, beta, tc, D.len_p, D.len_q, ctb_hor, &dec)) return;
+#pragma unroll
   for (int k = 0; k < 4; k++) {
     if (dec.de == 3)
       long_tap_line(ln[k], dec.len_p, dec.len_q, tc, maxv);
     else
       short_line(ln[k], dec, tc, maxv);
   }
-  for (int k = 0; k < 4; k++)
-    for (int i = 1; i < 15; i++) {
-      uint16_t v = (uint16_t)clampi(ln[k][i], 0, maxv);
-      if (kVertical)
-        pl[(size_t)(seg + k) * st + pos - 8 + i] = v;
-      else
-        pl[(size_t)(pos - 8 + i) * st + seg + k] = v;
+  // positions 0 and 15 are never modified; rewriting them is safe because
+  // edges of one pass are at least 16 samples apart on this path's lattice
+  if (kVertical) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t wv[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        wv[i] = (uint32_t)clampi(ln[k][2 * i], 0, maxv) | ((uint32_t)clampi(ln[k][2 * i + 1], 0, maxv) << 16);
+      uint4* r = reinterpret_cast<uint4*>(pl + (size_t)(seg + k) * st + pos - 8);
+      r[0] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+      r[1] = make_uint4(wv[4], wv[5], wv[6], wv[7]);
     }
+  } else {
+#pragma unroll
+    for (int i = 1; i < 15; i++) {
+      uint2 v;
+      v.x = (uint32_t)clampi(ln[0][i], 0, maxv) | ((uint32_t)clampi(ln[1][i], 0, maxv) << 16);
+      v.y = (uint32_t)clampi(ln[2][i], 0, maxv) | ((uint32_t)clampi(ln[3][i], 0, maxv) << 16);
+      *reinterpret_cast<uint2*>(pl + (size_t)(pos - 8 + i) * st + seg) = v;
+    }
+  }
 }
 
 // filter.rs:907-919 chroma_sample_decision
@@ -259,9 +302,36 @@ __global__ void k_deblock_chroma(const DbfPass* __restrict__ passes, int n_pass)
   int ln[4][8];
   uint16_t* pl = D.plane;
   const int st = D.stride;
-  for (int k = 0; k < group; k++)
-    for (int i = 0; i < 8; i++)
-      ln[k][i] = kVertical ? pl[(size_t)(seg + k) * st + pos - 4 + i] : pl[(size_t)(pos - 4 + i) * st + seg + k];
+  // vertical edges: a row of 8 samples is two 8-byte loads (pos - 4 is a
+  // multiple of 4); horizontal edges: the group's columns of a row in one load
+  if (kVertical) {
+    for (int k = 0; k < group; k++) {
+      const uint2* r = reinterpret_cast<const uint2*>(pl + (size_t)(seg + k) * st + pos - 4);
+      const uint2 a = r[0], b = r[1];
+      const uint32_t wv[4] = {a.x, a.y, b.x, b.y};
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        ln[k][2 * i] = (int)(wv[i] & 0xFFFFu);
+        ln[k][2 * i + 1] = (int)(wv[i] >> 16);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const uint16_t* rp = pl + (size_t)(pos - 4 + i) * st + seg;
+      if (group == 4) {
+        const uint2 v = *reinterpret_cast<const uint2*>(rp);
+        ln[0][i] = (int)(v.x & 0xFFFFu);
+        ln[1][i] = (int)(v.x >> 16);
+        ln[2][i] = (int)(v.y & 0xFFFFu);
+        ln[3][i] = (int)(v.y >> 16);
+      } else {
+        const uint32_t v = *reinterpret_cast<const uint32_t*>(rp);
+        ln[0][i] = (int)(v & 0xFFFFu);
+        ln[1][i] = (int)(v >> 16);
+      }
+    }
+  }
   if (len_q == 3) {
     int a[8], b[8];
     for (int i = 0; i < 8; i++) {
@@ -305,14 +375,30 @@ __global__ void k_deblock_chroma(const DbfPass* __restrict__ passes, int n_pass)
       l[4] = clampi(m[4] - delta, 0, maxv);
     }
   }
-  for (int k = 0; k < group; k++)
-    for (int i = 1; i < 7; i++) {
-      uint16_t v = (uint16_t)clampi(ln[k][i], 0, maxv);
-      if (kVertical)
-        pl[(size_t)(seg + k) * st + pos - 4 + i] = v;
-      else
-        pl[(size_t)(pos - 4 + i) * st + seg + k] = v;
+  // positions 0 and 7 are never modified; rewriting them is safe because
+  // edges of one pass are at least 8 samples apart
+  if (kVertical) {
+    for (int k = 0; k < group; k++) {
+      uint32_t wv[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        wv[i] = (uint32_t)clampi(ln[k][2 * i], 0, maxv) | ((uint32_t)clampi(ln[k][2 * i + 1], 0, maxv) << 16);
+      uint2* r = reinterpret_cast<uint2*>(pl + (size_t)(seg + k) * st + pos - 4);
+      r[0] = make_uint2(wv[0], wv[1]);
+      r[1] = make_uint2(wv[2], wv[3]);
     }
+  } else {
+#pragma unroll
+    for (int i = 1; i < 7; i++) {
+      uint16_t* rp = pl + (size_t)(pos - 4 + i) * st + seg;
+      const uint32_t v0 = (uint32_t)clampi(ln[0][i], 0, maxv) | ((uint32_t)clampi(ln[1][i], 0, maxv) << 16);
+      if (group == 4)
+        *reinterpret_cast<uint2*>(rp) =
+            make_uint2(v0, (uint32_t)clampi(ln[2][i], 0, maxv) | ((uint32_t)clampi(ln[3][i], 0, maxv) << 16));
+      else
+        *reinterpret_cast<uint32_t*>(rp) = v0;
+    }
+  }
 }
 
 // One SAO pass over one plane of one picture.
@@ -331,19 +417,37 @@ struct SaoPass {
 // reference pairs the neighbour offset (1, -1) with a bounds test for (1, 1),
 // so on the first and last rows it indexes row -1 / row h and panics; here
 // such a sample raises kStatusSaoAbort and nothing outside the plane is read.
-__global__ void k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
+// One thread per 4 consecutive samples of a row (plane widths are multiples of
+// 16 on this path, CTU widths multiples of 4): 8-byte loads and stores, the
+// two outer neighbours of edge classes as single loads.
+__device__ __forceinline__ void unpack4(uint2 v, int* o) {
+  o[0] = (int)(v.x & 0xFFFFu);
+  o[1] = (int)(v.x >> 16);
+  o[2] = (int)(v.y & 0xFFFFu);
+  o[3] = (int)(v.y >> 16);
+}
+
+__global__ void __launch_bounds__(256) k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
   const SaoPass& S = passes[blockIdx.y];
-  const int x = (blockIdx.x % ((S.w + 63) / 64)) * 64 + (threadIdx.x & 63);
-  const int y = (blockIdx.x / ((S.w + 63) / 64)) * 4 + (threadIdx.x >> 6);
-  if (x >= S.w || y >= S.h) return;
-  const int st = S.stride;
-  const int c = S.src[(size_t)y * st + x];
+  const int qw = (S.w + 3) >> 2;
+  const int bxn = (qw + 63) >> 6;
+  const int gx = (blockIdx.x % bxn) * 64 + (threadIdx.x & 63);
+  const int y = (blockIdx.x / bxn) * 4 + (threadIdx.x >> 6);
+  if (gx >= qw || y >= S.h) return;
+  const int x = gx * 4;
+  const int st = S.stride, w = S.w, h = S.h;
+  const uint16_t* src = S.src;
+  int c[4];
+  unpack4(*reinterpret_cast<const uint2*>(src + (size_t)y * st + x), c);
   const vvcg_sao sp = S.ctus[(y / S.ctu_h_s) * S.ctu_cols + x / S.ctu_w_s].sao[S.comp];
   const int maxv = (1 << S.bd) - 1;
-  int out = c;
+  int out[4] = {c[0], c[1], c[2], c[3]};
   if (sp.type == 1) {
-    int band = ((uint8_t)((uint8_t)(c >> (S.bd - 5)) - sp.band_or_class)) & 31;
-    if (band < 4) out = clampi(c + sp.offsets[band], 0, maxv);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int band = ((uint8_t)((uint8_t)(c[i] >> (S.bd - 5)) - sp.band_or_class)) & 31;
+      if (band < 4) out[i] = clampi(c[i] + sp.offsets[band], 0, maxv);
+    }
   } else if (sp.type == 2) {
     int dx, dy;
     switch (sp.band_or_class & 3) {
@@ -352,17 +456,41 @@ __global__ void k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
       case 2: dx = 1; dy = 1; break;
       default: dx = 1; dy = -1; break;
     }
-    if (dy == -1 && !(x - dx < 0 || x + dx >= S.w) && (y == 0 || y == S.h - 1)) {
-      atomicOr(status, kStatusSaoAbort);
-    } else if (!(x - dx < 0 || x + dx >= S.w || y - dy < 0 || y + dy >= S.h)) {
-      int a = S.src[(size_t)(y - dy) * st + x - dx];
-      int b = S.src[(size_t)(y + dy) * st + x + dx];
-      int ei = 2 + ((c > a) - (c < a)) + ((c > b) - (c < b));
-      int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2] : ei == 4 ? sp.offsets[3] : 0;
-      out = clampi(c + off, 0, maxv);
+    // neighbours a (at -dx, -dy) and b (at +dx, +dy) of the 4 samples
+    int a[6], b[6];  // a[i + 1] / b[i + 1] for columns x + i - 1 .. x + i + 4
+    const int ya = y - dy, yb = y + dy;
+    const bool ra = ya >= 0 && ya < h, rb = yb >= 0 && yb < h;
+    for (int i = 0; i < 6; i++) a[i] = b[i] = 0;
+    if (ra) {
+      const uint16_t* r = src + (size_t)ya * st;
+      unpack4(*reinterpret_cast<const uint2*>(r + x), a + 1);
+      if (x > 0) a[0] = r[x - 1];
+      if (x + 4 < w) a[5] = r[x + 4];
     }
+    if (rb) {
+      const uint16_t* r = src + (size_t)yb * st;
+      unpack4(*reinterpret_cast<const uint2*>(r + x), b + 1);
+      if (x > 0) b[0] = r[x - 1];
+      if (x + 4 < w) b[5] = r[x + 4];
+    }
+    bool abort = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int xi = x + i;
+      if (dy == -1 && !(xi - dx < 0 || xi + dx >= w) && (y == 0 || y == h - 1)) {
+        abort = true;
+      } else if (!(xi - dx < 0 || xi + dx >= w || ya < 0 || yb >= h || yb < 0 || ya >= h)) {
+        const int av = dx ? a[i] : a[i + 1], bv = dx ? b[i + 2] : b[i + 1];
+        const int ei = 2 + ((c[i] > av) - (c[i] < av)) + ((c[i] > bv) - (c[i] < bv));
+        const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
+                        : ei == 4 ? sp.offsets[3] : 0;
+        out[i] = clampi(c[i] + off, 0, maxv);
+      }
+    }
+    if (abort) atomicOr(status, kStatusSaoAbort);
   }
-  S.dst[(size_t)y * st + x] = (uint16_t)out;
+  *reinterpret_cast<uint2*>(S.dst + (size_t)y * st + x) =
+      make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
 }
 
 // One luma ALF pass (whole plane, apply_alf_luma_plane_16 of filter.rs:2045-2124).
@@ -374,48 +502,53 @@ struct AlfPass {
 };
 
 constexpr int kAlfTw = 64, kAlfTh = 16, kAlfHalo = 4;
+constexpr int kAlfBlocks = (kAlfTw / 4) * (kAlfTh / 4);
 
 // Tile of 64x16 outputs: the tile plus a 4-sample halo (coordinates clamped
-// to the plane, as the reference's get_p does) is staged in shared memory;
-// each 4x4 block is classified (classify_alf_4x4_16, filter.rs:2126-2182)
-// and filtered with the 7x7 diamond.
+// to the plane, as the reference's get_p does, so reads inside the staged
+// tile need no further clamping) is staged in shared memory. Each 4x4 block is
+// classified (classify_alf_4x4_16, filter.rs:2126-2182) and its transposed
+// coefficients and clip values are formed once; then each thread filters one
+// 4-sample row of a block with the 7x7 diamond.
 __global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
   const AlfPass& A = passes[blockIdx.z];
-  __shared__ uint16_t t[kAlfTh + 2 * kAlfHalo][kAlfTw + 2 * kAlfHalo];
-  __shared__ int8_t s_cls[kAlfTh / 4][kAlfTw / 4];
-  __shared__ int8_t s_tr[kAlfTh / 4][kAlfTw / 4];
+  constexpr int W = kAlfTw + 2 * kAlfHalo, H = kAlfTh + 2 * kAlfHalo;
+  __shared__ uint16_t t[H][W];
+  __shared__ int16_t s_fc[kAlfBlocks][12];
+  __shared__ int16_t s_fcl[kAlfBlocks][12];
+  __shared__ uint8_t s_abort[kAlfBlocks];
   const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
   if (x0 >= A.w || y0 >= A.h) return;
-  const int W = kAlfTw + 2 * kAlfHalo, H = kAlfTh + 2 * kAlfHalo;
   for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
     int ty = i / W, tx = i % W;
     int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
     t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
   }
   __syncthreads();
-  auto g = [&](int x, int y) -> int {  // plane coordinates, clamped
-    x = clampi(x, 0, A.w - 1);
-    y = clampi(y, 0, A.h - 1);
-    return t[y - y0 + kAlfHalo][x - x0 + kAlfHalo];
-  };
-  if (threadIdx.x < (kAlfTw / 4) * (kAlfTh / 4)) {
-    int bxi = threadIdx.x % (kAlfTw / 4), byi = threadIdx.x / (kAlfTw / 4);
-    int bx = x0 + bxi * 4, by = y0 + byi * 4;
+  // tile coordinates of plane position (x, y) inside the staged region
+  auto g = [&](int tx, int ty) -> int { return t[ty][tx]; };
+  const int* ct = A.bd >= 12 ? c_alf_clip[2] : (A.bd >= 10 ? c_alf_clip[1] : c_alf_clip[0]);
+  if (threadIdx.x < kAlfBlocks) {
+    const int bxi = threadIdx.x % (kAlfTw / 4), byi = threadIdx.x / (kAlfTw / 4);
+    const int bx = x0 + bxi * 4, by = y0 + byi * 4;
     int cls = 0, tr = 0;
     if (bx < A.w && by < A.h) {
-      const int TH[16] = {0, 1, 2, 2, 2, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3, 4};
       int sh = 0, sv = 0, d0 = 0, d1 = 0;
       for (int dy = 0; dy <= 4; dy += 2)
         for (int dx = 0; dx <= 4; dx += 2) {
-          int x = bx + dx, y = by + dy;
-          int c2 = g(x, y) << 1;
-          sh += abs(c2 - g(x - 1, y) - g(x + 1, y));
-          sv += abs(c2 - g(x, y - 1) - g(x, y + 1));
-          d0 += abs(c2 - g(x - 1, y - 1) - g(x + 1, y + 1));
-          d1 += abs(c2 - g(x + 1, y - 1) - g(x - 1, y + 1));
+          // plane positions bx + dx, by + dy and their +-1 neighbours, clamped as
+          // the staged halo is (the tile covers -4 .. +4 around the outputs)
+          const int tx = bxi * 4 + dx + kAlfHalo, ty = byi * 4 + dy + kAlfHalo;
+          const int c2 = g(tx, ty) << 1;
+          sh += abs(c2 - g(tx - 1, ty) - g(tx + 1, ty));
+          sv += abs(c2 - g(tx, ty - 1) - g(tx, ty + 1));
+          d0 += abs(c2 - g(tx - 1, ty - 1) - g(tx + 1, ty + 1));
+          d1 += abs(c2 - g(tx + 1, ty - 1) - g(tx - 1, ty + 1));
         }
       long long act = ((long long)(sh + sv) * 64) >> (A.bd + 4);
-      int q_act = TH[(int)(act < 0 ? 0 : (act > 15 ? 15 : act))];
+      // activity quantiser {0, 1, 2 x5, 3 x8, 4} of filter.rs:2163
+      const int ac = (int)(act < 0 ? 0 : (act > 15 ? 15 : act));
+      int q_act = ac == 0 ? 0 : ac == 1 ? 1 : ac <= 6 ? 2 : ac <= 14 ? 3 : 4;
       int hv1, hv0, dhv, dd1, dd0, ddd;
       if (sv > sh) { hv1 = sv; hv0 = sh; dhv = 1; } else { hv1 = sh; hv0 = sv; dhv = 3; }
       if (d0 > d1) { dd1 = d0; dd0 = d1; ddd = 0; } else { dd1 = d1; dd0 = d0; ddd = 2; }
@@ -424,62 +557,67 @@ __global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ pa
       else { h1 = hv1; h0 = hv0; mdir = dhv; sdir = ddd; }
       int ds = 0;
       if (h1 > 2 * h0) ds = (h1 * 2 > 9 * h0) ? 2 : 1;
-      const int TT[8] = {0, 1, 0, 2, 2, 3, 1, 3};
-      tr = TT[mdir * 2 + (sdir >> 1)];
+      // transpose index {0, 1, 0, 2, 2, 3, 1, 3}[mdir * 2 + sdir / 2], 2 bits each
+      tr = (0xDE84 >> (2 * (mdir * 2 + (sdir >> 1)))) & 3;
       cls = q_act;
       if (ds) cls += (((mdir & 1) << 1) + ds - 1 + 1) * 5;
       cls = min(cls, 24);
     }
-    s_cls[byi][bxi] = (int8_t)cls;
-    s_tr[byi][bxi] = (int8_t)tr;
+    // filter of the class: APS filter (coeff_delta_idx) or the fixed filter
+    // (the reference indexes a [16][25] table by class and aborts for >= 16)
+    const bool aps = A.aps && A.aps->num_luma_filters > 0;
+    const int filt = aps ? min((int)A.aps->coeff_delta_idx[cls], (int)A.aps->num_luma_filters - 1) : 0;
+    const bool abort = !aps && cls >= 16;
+    const bool use_clip = A.aps && A.aps->luma_clip && filt < (int)A.aps->num_luma_filters;
+    const int fixed = abort ? 0 : c_alf_class_to_filter[cls * 25];
+    for (int k = 0; k < 12; k++) {
+      const int p = c_alf_transpose_perm[(tr & 3) * 12 + k];
+      s_fc[threadIdx.x][k] = (int16_t)(aps ? A.aps->coeff[filt][p] : (abort ? 0 : c_alf_fixed[fixed * 13 + p]));
+      s_fcl[threadIdx.x][k] = (int16_t)ct[(use_clip ? A.aps->clip_idx[filt][p] : 0) & 3];
+    }
+    s_abort[threadIdx.x] = abort ? 1 : 0;
   }
   __syncthreads();
-  const int* ct = A.bd >= 12 ? c_alf_clip[2] : (A.bd >= 10 ? c_alf_clip[1] : c_alf_clip[0]);
-  const int maxv = (1 << A.bd) - 1;
-  for (int i = threadIdx.x; i < kAlfTw * kAlfTh; i += blockDim.x) {
-    int lx = i % kAlfTw, lyy = i / kAlfTw;
-    int x = x0 + lx, y = y0 + lyy;
-    if (x >= A.w || y >= A.h) continue;
-    int cls = s_cls[lyy >> 2][lx >> 2], tr = s_tr[lyy >> 2][lx >> 2];
-    int base_c[12], base_clip[12];
-    int filt = 0;
-    if (A.aps && A.aps->num_luma_filters > 0) {
-      filt = min((int)A.aps->coeff_delta_idx[cls], (int)A.aps->num_luma_filters - 1);
-      for (int k = 0; k < 12; k++) base_c[k] = A.aps->coeff[filt][k];
-    } else {
-      if (cls >= 16) {  // the reference indexes a [16][25] table by class and aborts
-        atomicOr(status, kStatusAlfAbort);
-        A.dst[(size_t)y * A.stride + x] = (uint16_t)g(x, y);
-        continue;
-      }
-      int fixed = c_alf_class_to_filter[cls * 25];
-      for (int k = 0; k < 12; k++) base_c[k] = c_alf_fixed[fixed * 13 + k];
-    }
-    bool use_clip = A.aps && A.aps->luma_clip && filt < (int)A.aps->num_luma_filters;
-    for (int k = 0; k < 12; k++) base_clip[k] = use_clip ? A.aps->clip_idx[filt][k] : 0;
+  const int b = threadIdx.x >> 2, r = threadIdx.x & 3;
+  const int bxi = b % (kAlfTw / 4), byi = b / (kAlfTw / 4);
+  const int x = x0 + bxi * 4, y = y0 + byi * 4 + r;
+  if (x >= A.w || y >= A.h) return;
+  const int tx0 = bxi * 4 + kAlfHalo, ty = byi * 4 + r + kAlfHalo;
+  int out[4];
+  if (s_abort[b]) {
+    atomicOr(status, kStatusAlfAbort);
+    for (int i = 0; i < 4; i++) out[i] = g(tx0 + i, ty);
+  } else {
     int fc[12], fcl[12];
+#pragma unroll
     for (int k = 0; k < 12; k++) {
-      int p = c_alf_transpose_perm[(tr & 3) * 12 + k];
-      fc[k] = base_c[p];
-      fcl[k] = ct[base_clip[p] & 3];
+      fc[k] = s_fc[b][k];
+      fcl[k] = s_fcl[b][k];
     }
-    const int c = g(x, y);
-    auto ca = [&](int cv, int p0, int p1) { return clampi(p0 - c, -cv, cv) + clampi(p1 - c, -cv, cv); };
-    int s = 0;
-    s += fc[0] * ca(fcl[0], g(x, y + 3), g(x, y - 3));
-    s += fc[1] * ca(fcl[1], g(x + 1, y + 2), g(x - 1, y - 2));
-    s += fc[2] * ca(fcl[2], g(x, y + 2), g(x, y - 2));
-    s += fc[3] * ca(fcl[3], g(x - 1, y + 2), g(x + 1, y - 2));
-    s += fc[4] * ca(fcl[4], g(x + 2, y + 1), g(x - 2, y - 1));
-    s += fc[5] * ca(fcl[5], g(x + 1, y + 1), g(x - 1, y - 1));
-    s += fc[6] * ca(fcl[6], g(x, y + 1), g(x, y - 1));
-    s += fc[7] * ca(fcl[7], g(x - 1, y + 1), g(x + 1, y - 1));
-    s += fc[8] * ca(fcl[8], g(x - 2, y + 1), g(x + 2, y - 1));
-    s += fc[9] * ca(fcl[9], g(x + 3, y), g(x - 3, y));
-    s += fc[10] * ca(fcl[10], g(x + 2, y), g(x - 2, y));
-    s += fc[11] * ca(fcl[11], g(x + 1, y), g(x - 1, y));
-    A.dst[(size_t)y * A.stride + x] = (uint16_t)clampi(c + ((s + 64) >> 7), 0, maxv);
+    const int maxv = (1 << A.bd) - 1;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int tx = tx0 + i;
+      const int c = g(tx, ty);
+      auto ca = [&](int cv, int p0, int p1) { return clampi(p0 - c, -cv, cv) + clampi(p1 - c, -cv, cv); };
+      int s = 0;
+      s += fc[0] * ca(fcl[0], g(tx, ty + 3), g(tx, ty - 3));
+      s += fc[1] * ca(fcl[1], g(tx + 1, ty + 2), g(tx - 1, ty - 2));
+      s += fc[2] * ca(fcl[2], g(tx, ty + 2), g(tx, ty - 2));
+      s += fc[3] * ca(fcl[3], g(tx - 1, ty + 2), g(tx + 1, ty - 2));
+      s += fc[4] * ca(fcl[4], g(tx + 2, ty + 1), g(tx - 2, ty - 1));
+      s += fc[5] * ca(fcl[5], g(tx + 1, ty + 1), g(tx - 1, ty - 1));
+      s += fc[6] * ca(fcl[6], g(tx, ty + 1), g(tx, ty - 1));
+      s += fc[7] * ca(fcl[7], g(tx - 1, ty + 1), g(tx + 1, ty - 1));
+      s += fc[8] * ca(fcl[8], g(tx - 2, ty + 1), g(tx + 2, ty - 1));
+      s += fc[9] * ca(fcl[9], g(tx + 3, ty), g(tx - 3, ty));
+      s += fc[10] * ca(fcl[10], g(tx + 2, ty), g(tx - 2, ty));
+      s += fc[11] * ca(fcl[11], g(tx + 1, ty), g(tx - 1, ty));
+      out[i] = clampi(c + ((s + 64) >> 7), 0, maxv);
+    }
   }
+  *reinterpret_cast<uint2*>(A.dst + (size_t)y * A.stride + x) =
+      make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
 }
 
 #undef LP

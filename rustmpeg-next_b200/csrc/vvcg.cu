@@ -600,7 +600,7 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
   }
   if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
     uint32_t maxb = 0;
-    for (auto& s : ctx->sao) maxb = std::max<uint32_t>(maxb, (uint32_t)(((s.w + 63) / 64) * ((s.h + 3) / 4)));
+    for (auto& s : ctx->sao) maxb = std::max<uint32_t>(maxb, (uint32_t)((((s.w + 3) / 4 + 63) / 64) * ((s.h + 3) / 4)));
     k_sao<<<dim3(maxb, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p,
                                                                             ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
@@ -1077,9 +1077,10 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
     P.ph[c] = c == 0 ? d.height : (cf ? (d.height + sh - 1) / sh : 0);
     if (c >= ncomp) continue;
     const vvcg_plane_out& o = planes[c];
-    if (!o.data || (reinterpret_cast<uintptr_t>(o.data) & 15) || (o.stride & 1) || o.stride < (uint32_t)P.pw[c])
+    if (!o.data || (reinterpret_cast<uintptr_t>(o.data) & 15) || (o.stride & 7) || o.stride < (uint32_t)P.pw[c])
       return static_fail(err, err_cap, VVCG_INVALID_INPUT,
-                         "plane %d: needs a 16-byte aligned pointer and an even stride >= %d", c, P.pw[c]);
+                         "plane %d: needs a 16-byte aligned pointer and a stride >= %d that is a multiple of 8",
+                         c, P.pw[c]);
     P.plane[c] = o.data;
     P.scratch[c] = o.data;  // residuals first, reconstruction over them
     P.stride[c] = (int32_t)o.stride;
