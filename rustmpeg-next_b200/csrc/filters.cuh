@@ -407,8 +407,8 @@ struct SaoPass {
   uint16_t* dst;
   const vvcg_ctu_filter* ctus;
   int32_t stride, w, h, bd, comp;
-  int32_t ctu_w_s, ctu_h_s;  // CTU size in this plane's samples
-  int32_t ctu_cols;          // CTUs per row
+  int32_t ctu_w_log2, ctu_h_log2;  // CTU size in this plane's samples (powers of 2)
+  int32_t ctu_cols;                // CTUs per row
 };
 
 // apply_sao_region_16 (filter.rs:1880-1947), every sample of the plane; the
@@ -427,70 +427,71 @@ __device__ __forceinline__ void unpack4(uint2 v, int* o) {
   o[3] = (int)(v.y >> 16);
 }
 
+// Grid: (64-group columns, row quads, passes); rows beyond gridDim.y * 4
+// are walked by the same threads.
 __global__ void __launch_bounds__(256) k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
-  const SaoPass& S = passes[blockIdx.y];
-  const int qw = (S.w + 3) >> 2;
-  const int bxn = (qw + 63) >> 6;
-  const int gx = (blockIdx.x % bxn) * 64 + (threadIdx.x & 63);
-  const int y = (blockIdx.x / bxn) * 4 + (threadIdx.x >> 6);
-  if (gx >= qw || y >= S.h) return;
-  const int x = gx * 4;
-  const int st = S.stride, w = S.w, h = S.h;
-  const uint16_t* src = S.src;
-  int c[4];
-  unpack4(*reinterpret_cast<const uint2*>(src + (size_t)y * st + x), c);
-  const vvcg_sao sp = S.ctus[(y / S.ctu_h_s) * S.ctu_cols + x / S.ctu_w_s].sao[S.comp];
-  const int maxv = (1 << S.bd) - 1;
-  int out[4] = {c[0], c[1], c[2], c[3]};
-  if (sp.type == 1) {
+  const SaoPass& S = passes[blockIdx.z];
+  const int gx = blockIdx.x * 64 + (threadIdx.x & 63);
+  if (gx >= ((S.w + 3) >> 2)) return;
+  for (int y = blockIdx.y * 4 + (threadIdx.x >> 6); y < S.h; y += gridDim.y * 4) {
+    const int x = gx * 4;
+    const int st = S.stride, w = S.w, h = S.h;
+    const uint16_t* src = S.src;
+    int c[4];
+    unpack4(*reinterpret_cast<const uint2*>(src + (size_t)y * st + x), c);
+    const vvcg_sao sp = S.ctus[(y >> S.ctu_h_log2) * S.ctu_cols + (x >> S.ctu_w_log2)].sao[S.comp];
+    const int maxv = (1 << S.bd) - 1;
+    int out[4] = {c[0], c[1], c[2], c[3]};
+    if (sp.type == 1) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int band = ((uint8_t)((uint8_t)(c[i] >> (S.bd - 5)) - sp.band_or_class)) & 31;
-      if (band < 4) out[i] = clampi(c[i] + sp.offsets[band], 0, maxv);
-    }
-  } else if (sp.type == 2) {
-    int dx, dy;
-    switch (sp.band_or_class & 3) {
-      case 0: dx = 1; dy = 0; break;
-      case 1: dx = 0; dy = 1; break;
-      case 2: dx = 1; dy = 1; break;
-      default: dx = 1; dy = -1; break;
-    }
-    // neighbours a (at -dx, -dy) and b (at +dx, +dy) of the 4 samples
-    int a[6], b[6];  // a[i + 1] / b[i + 1] for columns x + i - 1 .. x + i + 4
-    const int ya = y - dy, yb = y + dy;
-    const bool ra = ya >= 0 && ya < h, rb = yb >= 0 && yb < h;
-    for (int i = 0; i < 6; i++) a[i] = b[i] = 0;
-    if (ra) {
-      const uint16_t* r = src + (size_t)ya * st;
-      unpack4(*reinterpret_cast<const uint2*>(r + x), a + 1);
-      if (x > 0) a[0] = r[x - 1];
-      if (x + 4 < w) a[5] = r[x + 4];
-    }
-    if (rb) {
-      const uint16_t* r = src + (size_t)yb * st;
-      unpack4(*reinterpret_cast<const uint2*>(r + x), b + 1);
-      if (x > 0) b[0] = r[x - 1];
-      if (x + 4 < w) b[5] = r[x + 4];
-    }
-    bool abort = false;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      const int xi = x + i;
-      if (dy == -1 && !(xi - dx < 0 || xi + dx >= w) && (y == 0 || y == h - 1)) {
-        abort = true;
-      } else if (!(xi - dx < 0 || xi + dx >= w || ya < 0 || yb >= h || yb < 0 || ya >= h)) {
-        const int av = dx ? a[i] : a[i + 1], bv = dx ? b[i + 2] : b[i + 1];
-        const int ei = 2 + ((c[i] > av) - (c[i] < av)) + ((c[i] > bv) - (c[i] < bv));
-        const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
-                        : ei == 4 ? sp.offsets[3] : 0;
-        out[i] = clampi(c[i] + off, 0, maxv);
+      for (int i = 0; i < 4; i++) {
+        const int band = ((uint8_t)((uint8_t)(c[i] >> (S.bd - 5)) - sp.band_or_class)) & 31;
+        if (band < 4) out[i] = clampi(c[i] + sp.offsets[band], 0, maxv);
       }
+    } else if (sp.type == 2) {
+      int dx, dy;
+      switch (sp.band_or_class & 3) {
+        case 0: dx = 1; dy = 0; break;
+        case 1: dx = 0; dy = 1; break;
+        case 2: dx = 1; dy = 1; break;
+        default: dx = 1; dy = -1; break;
+      }
+      // neighbours a (at -dx, -dy) and b (at +dx, +dy) of the 4 samples
+      int a[6], b[6];  // a[i + 1] / b[i + 1] for columns x + i - 1 .. x + i + 4
+      const int ya = y - dy, yb = y + dy;
+      const bool ra = ya >= 0 && ya < h, rb = yb >= 0 && yb < h;
+      for (int i = 0; i < 6; i++) a[i] = b[i] = 0;
+      if (ra) {
+        const uint16_t* r = src + (size_t)ya * st;
+        unpack4(*reinterpret_cast<const uint2*>(r + x), a + 1);
+        if (x > 0) a[0] = r[x - 1];
+        if (x + 4 < w) a[5] = r[x + 4];
+      }
+      if (rb) {
+        const uint16_t* r = src + (size_t)yb * st;
+        unpack4(*reinterpret_cast<const uint2*>(r + x), b + 1);
+        if (x > 0) b[0] = r[x - 1];
+        if (x + 4 < w) b[5] = r[x + 4];
+      }
+      bool abort = false;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int xi = x + i;
+        if (dy == -1 && !(xi - dx < 0 || xi + dx >= w) && (y == 0 || y == h - 1)) {
+          abort = true;
+        } else if (!(xi - dx < 0 || xi + dx >= w || ya < 0 || yb >= h || yb < 0 || ya >= h)) {
+          const int av = dx ? a[i] : a[i + 1], bv = dx ? b[i + 2] : b[i + 1];
+          const int ei = 2 + ((c[i] > av) - (c[i] < av)) + ((c[i] > bv) - (c[i] < bv));
+          const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
+                          : ei == 4 ? sp.offsets[3] : 0;
+          out[i] = clampi(c[i] + off, 0, maxv);
+        }
+      }
+      if (abort) atomicOr(status, kStatusSaoAbort);
     }
-    if (abort) atomicOr(status, kStatusSaoAbort);
+    *reinterpret_cast<uint2*>(S.dst + (size_t)y * st + x) =
+        make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
   }
-  *reinterpret_cast<uint2*>(S.dst + (size_t)y * st + x) =
-      make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
 }
 
 // One luma ALF pass (whole plane, apply_alf_luma_plane_16 of filter.rs:2045-2124).

@@ -228,6 +228,7 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
 }
 
 uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+int ilog2_host(int v) { return __builtin_ctz((unsigned)v); }
 
 template <typename T>
 vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
@@ -505,7 +506,7 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
       sao_ran = true;
       for (int c = 0; c < ncomp; c++) {
         SaoPass s{P.plane[c], P.scratch[c], P.ctus, P.stride[c], P.pw[c], P.ph[c], P.bd, c,
-                  c ? P.ctu / P.sub_w : P.ctu, c ? P.ctu / P.sub_h : P.ctu, P.ctu_w};
+                  ilog2_host(c ? P.ctu / P.sub_w : P.ctu), ilog2_host(c ? P.ctu / P.sub_h : P.ctu), P.ctu_w};
         ctx->sao.push_back(s);
         L.final_in_scratch[c] = 1;
       }
@@ -599,10 +600,13 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     }
   }
   if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
-    uint32_t maxb = 0;
-    for (auto& s : ctx->sao) maxb = std::max<uint32_t>(maxb, (uint32_t)((((s.w + 3) / 4 + 63) / 64) * ((s.h + 3) / 4)));
-    k_sao<<<dim3(maxb, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p,
-                                                                            ctrl + 1);
+    uint32_t gx = 0, gy = 0;
+    for (auto& s : ctx->sao) {
+      gx = std::max<uint32_t>(gx, (uint32_t)(((s.w + 3) / 4 + 63) / 64));
+      gy = std::max<uint32_t>(gy, (uint32_t)std::min((s.h + 3) / 4, 65535));
+    }
+    k_sao<<<dim3(gx, gy, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p,
+                                                                             ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
     ctx->launches++;
   }
