@@ -310,6 +310,62 @@ vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32
                                   const int16_t* in, uint64_t in_count, int16_t* out,
                                   uint64_t out_count);
 
+/* ---- encoder candidate cost: luma transform search ----------------------- */
+
+enum {
+  VVCG_TXS_TRANSFORM_SKIP = 1u << 0, /* code the block with transform skip only (QP 4 path) */
+  VVCG_TXS_LFNST = 1u << 1           /* also try LFNST 1 and 2 (chroma_can_lfnst) */
+};
+
+typedef struct vvcg_tx_search_req {
+  uint8_t log2_size; /* 2..5: square blocks 4x4 .. 32x32 */
+  uint8_t qp;        /* QP of the 8-bit strict encoder, 0..63 */
+  uint8_t mode;      /* the block's intra mode: 0 Planar, 1 DC, 2..66 (LFNST set) */
+  uint8_t flags;     /* VVCG_TXS_* */
+  uint32_t in_off;   /* first of the n*n prediction / source samples (int16 raster) */
+  uint32_t out_off;  /* first of the n*n output levels / samples (int16 raster) */
+  uint32_t reserved;
+} vvcg_tx_search_req; /* 16 bytes */
+
+typedef struct vvcg_tx_search_res {
+  uint64_t sse;           /* reconstruction SSE of the chosen candidate */
+  uint8_t mts_idx;        /* 0..4 */
+  uint8_t lfnst_idx;      /* 0..2 */
+  uint8_t transform_skip; /* 1 when coded with transform skip */
+  uint8_t cbf;            /* any nonzero level */
+  uint32_t reserved;
+} vvcg_tx_search_res; /* 16 bytes */
+
+/* Transform choice of each 8-bit luma block by reconstruction SSE: DCT-2,
+ * then MTS 1..4, then (VVCG_TXS_LFNST) LFNST 1..2, each replacing the best
+ * only when it can be signalled and its SSE is strictly lower; writes the
+ * winner's levels and reconstructed samples. Replaces: slice::encode_luma
+ * after the prediction (crates/rustmpeg-video/src/vvc/slice.rs:810-874, with
+ * plan_primary :699, plan_transform_skip :671, mts_candidate_ok /
+ * lfnst_candidate_ok :877-896, block_sse :908). `reqs` is host memory; pred,
+ * src, levels, samples (int16, counts in_count / out_count) and `res`
+ * (num_reqs entries) are device memory. Asynchronous on the stream. */
+vvcg_status vvcg_luma_tx_search_dev(vvcg_ctx* ctx, const vvcg_tx_search_req* reqs, uint32_t num_reqs,
+                                    const int16_t* pred, const int16_t* src, uint64_t in_count,
+                                    int16_t* levels, int16_t* samples, uint64_t out_count,
+                                    vvcg_tx_search_res* res);
+
+/* ---- plane metrics ---------------------------------------------------------- */
+
+/* Sum of squared errors, sum of absolute differences and sample count of one
+ * plane pair (device pointers, strides in samples), written to out[0..2]
+ * (device memory, 3 x uint64). Replaces: CpuFrameMetrics::plane_metrics
+ * (crates/rustmpeg-video/src/accelerator.rs:258-292); PSNR and MSE follow
+ * from these on the host (PlaneMetrics::psnr, accelerator.rs:111-118).
+ * Asynchronous on the context's stream. */
+vvcg_status vvcg_plane_metrics_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint64_t ref_stride,
+                                     const uint8_t* dist, uint64_t dist_stride, uint32_t width,
+                                     uint32_t height, uint64_t* out);
+/* The same sums for 16-bit planes (the library's 8..12-bit sample planes). */
+vvcg_status vvcg_plane_metrics_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint64_t ref_stride,
+                                      const uint16_t* dist, uint64_t dist_stride, uint32_t width,
+                                      uint32_t height, uint64_t* out);
+
 /* ---- allocation-free single picture --------------------------------------- */
 
 /* Largest picture height, in CTU rows, that vvcg_recon_picture_static takes

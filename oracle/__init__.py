@@ -92,6 +92,8 @@ def _declare(L):
                                    C.POINTER(C.c_uint64), vp, vp, vp]
     L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     L.orc_tu_batch.argtypes = [i, vp, i, vp, vp]
+    L.orc_luma_tx_search.argtypes = [i, vp, vp, i, i, i, i, vp, vp, C.POINTER(C.c_uint64)]
+    L.orc_plane_metrics.argtypes = [vp, C.c_uint64, vp, C.c_uint64, C.c_uint32, C.c_uint32, i, vp]
 
 
 # ---------------------------------------------------------------- transforms --
@@ -399,3 +401,31 @@ def tu_batch(recs, data, out_count, forward=False):
     out = np.zeros(out_count, np.int16)
     rc = lib().orc_tu_batch(1 if forward else 0, _p(recs), len(recs), _p(data), _p(out))
     return rc, out
+
+
+def plane_metrics(a, b):
+    """(sse, sad, samples) of two equally sized 2-D uint8 / uint16 arrays
+    (accelerator.rs:258-292 CpuFrameMetrics::plane_metrics)."""
+    assert a.shape == b.shape and a.dtype == b.dtype
+    elem = a.dtype.itemsize
+    h, w = a.shape
+    out = np.zeros(3, np.uint64)
+    rc = lib().orc_plane_metrics(a.ctypes.data_as(C.c_void_p), a.strides[0] // elem,
+                                 b.ctypes.data_as(C.c_void_p), b.strides[0] // elem, w, h, elem, _p(out))
+    assert rc == 0
+    return int(out[0]), int(out[1]), int(out[2])
+
+
+def luma_tx_search(pred, src, qp, mode, use_ts=False, lfnst=False):
+    """slice.rs:810-874 encode_luma's transform choice for one square block.
+
+    Returns (mts_idx, lfnst_idx, ts, cbf, sse, levels, samples)."""
+    pred = np.ascontiguousarray(pred, dtype=np.int32)
+    src = np.ascontiguousarray(src, dtype=np.int32)
+    n = pred.shape[0]
+    lv = np.zeros(n * n, np.int16)
+    sm = np.zeros(n * n, np.int16)
+    sse = C.c_uint64(0)
+    r = lib().orc_luma_tx_search(n, _p(pred), _p(src), qp, mode, int(use_ts), int(lfnst), _p(lv), _p(sm),
+                                 C.byref(sse))
+    return (r >> 8) & 0xF, (r >> 4) & 0xF, (r >> 1) & 1, r & 1, sse.value, lv, sm

@@ -144,3 +144,25 @@ int orc_tu_batch(int forward, const void* recs, int n, const int16_t* in, int16_
 }
 
 }  // extern "C"
+
+// crates/rustmpeg-video/src/accelerator.rs:258-292 CpuFrameMetrics::plane_metrics
+// over `elem`-byte samples (1 or 2), strides in samples; out = {sse, sad, samples}.
+extern "C" int orc_plane_metrics(const void* a, uint64_t sa, const void* b, uint64_t sb, uint32_t w,
+                                 uint32_t h, int elem, uint64_t* out) {
+  out[0] = out[1] = out[2] = 0;
+  if (w == 0 || h == 0) return 0;
+  if (sa < w || sb < w) return -1;
+  uint64_t sse = 0, sad = 0;
+  for (uint32_t y = 0; y < h; y++)
+    for (uint32_t x = 0; x < w; x++) {
+      int l = elem == 1 ? ((const uint8_t*)a)[y * sa + x] : ((const uint16_t*)a)[y * sa + x];
+      int r = elem == 1 ? ((const uint8_t*)b)[y * sb + x] : ((const uint16_t*)b)[y * sb + x];
+      uint64_t d = (uint64_t)(l > r ? l - r : r - l);
+      sse += d * d;
+      sad += d;
+    }
+  out[0] = sse;
+  out[1] = sad;
+  out[2] = (uint64_t)w * h;
+  return 0;
+}

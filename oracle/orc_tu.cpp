@@ -111,3 +111,137 @@ int tu_forward(const TuRec& r, const int16_t* in, int16_t* out) {
 }
 
 }  // namespace orc
+
+namespace orc {
+
+// slice.rs:699-760 plan_primary / :671-697 plan_transform_skip on one square
+// block of the 8-bit strict encoder: levels and reconstructed samples.
+struct BlockPlan {
+  std::vector<int32_t> levels;
+  std::vector<int32_t> samples;
+  bool cbf = false;
+};
+
+static void slice_lfnst_skips(int w, int h, int* sw, int* sh) {  // slice.rs:674-682
+  if ((w == 4 && h > 4) || (w > 4 && h == 4)) {
+    *sw = w - 4;
+    *sh = h - 4;
+  } else if (w >= 8 && h >= 8) {
+    *sw = w - 8;
+    *sh = h - 8;
+  } else {
+    *sw = *sh = 0;
+  }
+}
+
+static BlockPlan plan_primary(const int32_t* pred, const int32_t* res, int n, int qp, int mts, int lfnst,
+                              int mode) {
+  BlockPlan p;
+  int th, tv;
+  mts_types(mts, &th, &tv);
+  int sw, sh;
+  if (lfnst > 0)
+    slice_lfnst_skips(n, n, &sw, &sh);
+  else {
+    sw = (n == 32 && th != kDct2) ? 16 : 0;  // slice.rs:659-670
+    sh = (n == 32 && tv != kDct2) ? 16 : 0;
+  }
+  std::vector<int32_t> co(n * n), deq(n * n), rec(n * n);
+  forward_transform_rect_bd(n, n, res, th, tv, sw, sh, 8, co.data());
+  if (lfnst > 0) forward_lfnst_rect(co.data(), n, n, lfnst, mode);
+  p.levels.assign(n * n, 0);
+  quantize_rect_bd(n, n, co.data(), qp, 8, true, p.levels.data());
+  for (int v : p.levels) p.cbf |= v != 0;
+  dequantize_rect_bd(n, n, p.levels.data(), qp, 8, deq.data());
+  if (lfnst > 0) inverse_lfnst_rect(deq.data(), n, n, lfnst, mode);
+  inverse_transform_rect_bd(n, n, deq.data(), th, tv, sw, sh, 8, rec.data());
+  p.samples.resize(n * n);
+  for (int i = 0; i < n * n; i++) p.samples[i] = std::min(255, std::max(0, pred[i] + rec[i]));
+  return p;
+}
+
+// slice.rs:935-939 scan_pos_last over CoeffScan(n, n)
+static int scan_pos_last(const std::vector<int32_t>& lv, int n) {
+  std::vector<int32_t> scan(n * n);
+  int ns = coeff_scan_raster(n, n, scan.data());
+  for (int s = ns - 1; s >= 0; s--)
+    if (lv[scan[s]] != 0) return s;
+  return -1;
+}
+
+}  // namespace orc
+
+// slice.rs:810-874 encode_luma (after the prediction): the transform choice of
+// one n x n luma block by reconstruction SSE. pred / src are n*n raster
+// samples; writes the winner's levels and samples; returns (mts_idx << 8) |
+// (lfnst_idx << 4) | (ts << 1) | cbf, and the winner's SSE.
+extern "C" int orc_luma_tx_search(int n, const int32_t* pred, const int32_t* src, int qp, int mode, int use_ts,
+                                  int chroma_can_lfnst, int16_t* levels, int16_t* samples, uint64_t* sse_out) {
+  using namespace orc;
+  std::vector<int32_t> res(n * n);
+  for (int i = 0; i < n * n; i++) res[i] = src[i] - pred[i];
+  auto sse_of = [&](const BlockPlan& p) {
+    uint64_t s = 0;
+    for (int i = 0; i < n * n; i++) {
+      int64_t d = (int64_t)src[i] - p.samples[i];
+      s += (uint64_t)(d * d);
+    }
+    return s;
+  };
+  BlockPlan best;
+  int best_mts = 0, best_lfnst = 0, ts = 0;
+  uint64_t best_sse;
+  if (use_ts) {  // slice.rs:671-697 plan_transform_skip
+    best.levels.resize(n * n);
+    best.samples.resize(n * n);
+    for (int i = 0; i < n * n; i++) {
+      int l = quantize_ts(res[i], qp);
+      best.levels[i] = l;
+      best.cbf |= l != 0;
+      best.samples[i] = std::min(255, std::max(0, pred[i] + dequantize_ts(l, qp)));
+    }
+    best_sse = sse_of(best);
+    ts = 1;
+  } else {
+    best = plan_primary(pred, res.data(), n, qp, 0, 0, mode);
+    best_sse = sse_of(best);
+    for (int m = 1; m <= 4; m++) {
+      BlockPlan p = plan_primary(pred, res.data(), n, qp, m, 0, mode);
+      // slice.rs:877-885 mts_candidate_ok
+      if (!p.cbf) continue;
+      int last = scan_pos_last(p.levels, n);
+      bool violates = false;
+      for (int i = 0; i < n * n; i++)
+        if (p.levels[i] != 0 && ((i % n) / 4 > 3 || (i / n) / 4 > 3)) violates = true;
+      if (!(last >= 1 && !violates)) continue;
+      uint64_t s = sse_of(p);
+      if (s < best_sse) {
+        best_sse = s;
+        best = p;
+        best_mts = m;
+      }
+    }
+    if (chroma_can_lfnst)
+      for (int l = 1; l <= 2; l++) {
+        BlockPlan p = plan_primary(pred, res.data(), n, qp, 0, l, mode);
+        // slice.rs:888-896 lfnst_candidate_ok
+        if (!p.cbf) continue;
+        int last = scan_pos_last(p.levels, n);
+        int max_pos = (n == 4 || n == 8) ? 7 : 15;
+        if (!(last >= 1 && last <= max_pos)) continue;
+        uint64_t s = sse_of(p);
+        if (s < best_sse) {
+          best_sse = s;
+          best = p;
+          best_mts = 0;
+          best_lfnst = l;
+        }
+      }
+  }
+  for (int i = 0; i < n * n; i++) {
+    levels[i] = (int16_t)best.levels[i];
+    samples[i] = (int16_t)best.samples[i];
+  }
+  *sse_out = best_sse;
+  return (best_mts << 8) | (best_lfnst << 4) | (ts << 1) | (best.cbf ? 1 : 0);
+}

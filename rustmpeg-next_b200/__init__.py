@@ -40,6 +40,11 @@ MC_BLOCK_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<u2"), ("h", "<u2"
                            ("mv_x", "<i4"), ("mv_y", "<i4"), ("flags", "<u4"),
                            ("reserved", "<u4"), ("out_offset", "<u8")], align=True)
 
+TXS_REQ_DTYPE = np.dtype([("log2_size", "u1"), ("qp", "u1"), ("mode", "u1"), ("flags", "u1"),
+                          ("in_off", "<u4"), ("out_off", "<u4"), ("reserved", "<u4")])
+TXS_RES_DTYPE = np.dtype([("sse", "<u8"), ("mts_idx", "u1"), ("lfnst_idx", "u1"), ("transform_skip", "u1"),
+                          ("cbf", "u1"), ("reserved", "<u4")])
+TXS_TRANSFORM_SKIP, TXS_LFNST = 1, 2
 TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("qp", "u1"),
                      ("flags", "u1"), ("mts_idx", "u1"), ("lfnst_idx", "u1"),
                      ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
@@ -110,6 +115,7 @@ class _Config(C.Structure):
 
 assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize == 32
 assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.itemsize == 16
+assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
 
 
 def build(force: bool = False) -> str:
@@ -157,6 +163,9 @@ def lib():
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
         L.vvcg_encode_batch.argtypes = [vp, vp, u32, vp, vp, u32, vp, u64]
+        for n in ("vvcg_plane_metrics_8_dev", "vvcg_plane_metrics_16_dev"):
+            getattr(L, n).argtypes = [vp, vp, u64, vp, u64, u32, u32, vp]
+        L.vvcg_luma_tx_search_dev.argtypes = [vp, vp, u32, vp, vp, u64, vp, vp, u64, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -344,6 +353,47 @@ class Context:
         self._check(self._L.vvcg_encode_batch(self._h, _ptr(pics), len(pics), arr, _ptr(cus), nc.value,
                                               _ptr(levels), nl.value))
         return cus, levels[:nl.value]
+
+    # -- luma transform search --
+    def luma_tx_search(self, reqs, pred, src, levels, samples):
+        """TXS_REQ_DTYPE requests (host) over int16 CUDA tensors; returns the
+        TXS_RES_DTYPE results (synchronises)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=TXS_REQ_DTYPE)
+        res = torch.zeros(len(reqs) * TXS_RES_DTYPE.itemsize, dtype=torch.uint8, device=pred.device)
+        self._keep = reqs
+        self._check(self._L.vvcg_luma_tx_search_dev(self._h, _ptr(reqs), len(reqs), _ptr(pred), _ptr(src),
+                                                    pred.numel(), _ptr(levels), _ptr(samples), levels.numel(),
+                                                    _ptr(res)))
+        torch.cuda.synchronize(pred.device)
+        return res.cpu().numpy().view(TXS_RES_DTYPE)
+
+    # -- metrics --
+    def plane_metrics(self, ref, dist):
+        """(sse, sad, samples) of two equally shaped 2-D CUDA tensors (uint8, or
+        int16 holding 16-bit samples); synchronises the stream."""
+        import torch
+
+        if tuple(ref.shape) != tuple(dist.shape):
+            raise InvalidInput(f"plane dimensions differ: {tuple(ref.shape)} and {tuple(dist.shape)}")
+        out = torch.zeros(3, dtype=torch.int64, device=ref.device)
+        h, w = ref.shape
+        fn = self._L.vvcg_plane_metrics_8_dev if ref.element_size() == 1 else self._L.vvcg_plane_metrics_16_dev
+        self._check(fn(self._h, _ptr(ref), ref.stride(0), _ptr(dist), dist.stride(0), w, h, _ptr(out)))
+        torch.cuda.synchronize(ref.device)
+        return tuple(int(v) for v in out.cpu())
+
+    @staticmethod
+    def psnr(sse, samples, bit_depth):
+        """PlaneMetrics::psnr (accelerator.rs:111-118): 100 dB for a zero error."""
+        import math
+
+        mse = sse / samples if samples else 0.0
+        if mse <= 1e-12:
+            return 100.0
+        peak = float((1 << min(bit_depth, 16)) - 1)
+        return 10.0 * math.log10(peak * peak / mse)
 
     # -- transform units (records on the host, int16 CUDA tensors) --
     def tu_inverse(self, recs, data, out):

@@ -427,71 +427,79 @@ __device__ __forceinline__ void unpack4(uint2 v, int* o) {
   o[3] = (int)(v.y >> 16);
 }
 
-// Grid: (64-group columns, row quads, passes); rows beyond gridDim.y * 4
-// are walked by the same threads.
+// Work split: each warp takes one CTU and a group of its rows, lanes on 4
+// consecutive samples of a row (a CTU row of ctu_w samples is ctu_w / 4
+// lanes), so the CTU's parameters and the branch on its type are uniform
+// across the warp. Coded sizes are CTU multiples: no partial CTUs.
+// Grid: (ceil(items / 8), passes) with 8 warps per CTA; item = CTU x group.
 __global__ void __launch_bounds__(256) k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
-  const SaoPass& S = passes[blockIdx.z];
-  const int gx = blockIdx.x * 64 + (threadIdx.x & 63);
-  if (gx >= ((S.w + 3) >> 2)) return;
-  for (int y = blockIdx.y * 4 + (threadIdx.x >> 6); y < S.h; y += gridDim.y * 4) {
-    const int x = gx * 4;
-    const int st = S.stride, w = S.w, h = S.h;
-    const uint16_t* src = S.src;
-    int c[4];
-    unpack4(*reinterpret_cast<const uint2*>(src + (size_t)y * st + x), c);
-    const vvcg_sao sp = S.ctus[(y >> S.ctu_h_log2) * S.ctu_cols + (x >> S.ctu_w_log2)].sao[S.comp];
-    const int maxv = (1 << S.bd) - 1;
-    int out[4] = {c[0], c[1], c[2], c[3]};
-    if (sp.type == 1) {
+  const SaoPass& S = passes[blockIdx.y];
+  const int lane = threadIdx.x & 31;
+  const int tpr = max(1, (1 << S.ctu_w_log2) >> 2);   // lanes per CTU row
+  const int rpw = 32 / tpr;                            // CTU rows per warp
+  const int ctu_h = 1 << S.ctu_h_log2;
+  const int groups = (ctu_h + rpw - 1) / rpw;
+  const int n_ctu = S.ctu_cols * ((S.h + ctu_h - 1) >> S.ctu_h_log2);
+  const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (item >= n_ctu * groups) return;
+  const int ctu = item / groups, grp = item - ctu * groups;
+  const int cxs = (ctu % S.ctu_cols) << S.ctu_w_log2, cys = (ctu / S.ctu_cols) << S.ctu_h_log2;
+  const int x = cxs + (lane % tpr) * 4;
+  const int y = cys + grp * rpw + lane / tpr;
+  if (lane >= tpr * rpw || x >= S.w || y >= S.h || y >= cys + ctu_h) return;
+  const int st = S.stride, w = S.w, h = S.h;
+  const uint16_t* src = S.src;
+  int c[4];
+  unpack4(*reinterpret_cast<const uint2*>(src + (size_t)y * st + x), c);
+  const vvcg_sao sp = S.ctus[ctu].sao[S.comp];
+  const int maxv = (1 << S.bd) - 1;
+  int out[4] = {c[0], c[1], c[2], c[3]};
+  if (sp.type == 1) {
+    const int o0 = sp.offsets[0], o1 = sp.offsets[1], o2 = sp.offsets[2], o3 = sp.offsets[3];
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int band = ((uint8_t)((uint8_t)(c[i] >> (S.bd - 5)) - sp.band_or_class)) & 31;
-        if (band < 4) out[i] = clampi(c[i] + sp.offsets[band], 0, maxv);
-      }
-    } else if (sp.type == 2) {
-      int dx, dy;
-      switch (sp.band_or_class & 3) {
-        case 0: dx = 1; dy = 0; break;
-        case 1: dx = 0; dy = 1; break;
-        case 2: dx = 1; dy = 1; break;
-        default: dx = 1; dy = -1; break;
-      }
-      // neighbours a (at -dx, -dy) and b (at +dx, +dy) of the 4 samples
-      int a[6], b[6];  // a[i + 1] / b[i + 1] for columns x + i - 1 .. x + i + 4
-      const int ya = y - dy, yb = y + dy;
-      const bool ra = ya >= 0 && ya < h, rb = yb >= 0 && yb < h;
-      for (int i = 0; i < 6; i++) a[i] = b[i] = 0;
-      if (ra) {
-        const uint16_t* r = src + (size_t)ya * st;
-        unpack4(*reinterpret_cast<const uint2*>(r + x), a + 1);
-        if (x > 0) a[0] = r[x - 1];
-        if (x + 4 < w) a[5] = r[x + 4];
-      }
-      if (rb) {
-        const uint16_t* r = src + (size_t)yb * st;
-        unpack4(*reinterpret_cast<const uint2*>(r + x), b + 1);
-        if (x > 0) b[0] = r[x - 1];
-        if (x + 4 < w) b[5] = r[x + 4];
-      }
-      bool abort = false;
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int xi = x + i;
-        if (dy == -1 && !(xi - dx < 0 || xi + dx >= w) && (y == 0 || y == h - 1)) {
-          abort = true;
-        } else if (!(xi - dx < 0 || xi + dx >= w || ya < 0 || yb >= h || yb < 0 || ya >= h)) {
-          const int av = dx ? a[i] : a[i + 1], bv = dx ? b[i + 2] : b[i + 1];
-          const int ei = 2 + ((c[i] > av) - (c[i] < av)) + ((c[i] > bv) - (c[i] < bv));
-          const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
-                          : ei == 4 ? sp.offsets[3] : 0;
-          out[i] = clampi(c[i] + off, 0, maxv);
-        }
-      }
-      if (abort) atomicOr(status, kStatusSaoAbort);
+    for (int i = 0; i < 4; i++) {
+      const int band = ((uint8_t)((uint8_t)(c[i] >> (S.bd - 5)) - sp.band_or_class)) & 31;
+      const int off = band == 0 ? o0 : band == 1 ? o1 : band == 2 ? o2 : o3;
+      if (band < 4) out[i] = clampi(c[i] + off, 0, maxv);
     }
-    *reinterpret_cast<uint2*>(S.dst + (size_t)y * st + x) =
-        make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
+  } else if (sp.type == 2) {
+    const int cls = sp.band_or_class & 3;
+    const int dx = cls == 1 ? 0 : 1, dy = cls == 0 ? 0 : (cls == 3 ? -1 : 1);
+    // neighbours a (at -dx, -dy) and b (at +dx, +dy): a[k] / b[k] hold columns x + k - 1
+    int a[6], b[6];
+    const int ya = y - dy, yb = y + dy;
+    const bool ra = ya >= 0 && ya < h, rb = yb >= 0 && yb < h;
+#pragma unroll
+    for (int i = 0; i < 6; i++) a[i] = b[i] = 0;
+    if (ra) {
+      const uint16_t* r = src + (size_t)ya * st;
+      unpack4(*reinterpret_cast<const uint2*>(r + x), a + 1);
+      if (dx && x > 0) a[0] = r[x - 1];
+    }
+    if (rb) {
+      const uint16_t* r = src + (size_t)yb * st;
+      unpack4(*reinterpret_cast<const uint2*>(r + x), b + 1);
+      if (dx && x + 4 < w) b[5] = r[x + 4];
+    }
+    const int o0 = sp.offsets[0], o1 = sp.offsets[1], o2 = sp.offsets[2], o3 = sp.offsets[3];
+    bool abort = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int xi = x + i;
+      const bool xin = !(xi - dx < 0 || xi + dx >= w);
+      if (dy == -1 && xin && (y == 0 || y == h - 1)) {
+        abort = true;
+      } else if (xin && ra && rb) {
+        const int av = dx ? a[i] : a[i + 1], bv = dx ? b[i + 2] : b[i + 1];
+        const int ei = 2 + ((c[i] > av) - (c[i] < av)) + ((c[i] > bv) - (c[i] < bv));
+        const int off = ei == 0 ? o0 : ei == 1 ? o1 : ei == 3 ? o2 : ei == 4 ? o3 : 0;
+        out[i] = clampi(c[i] + off, 0, maxv);
+      }
+    }
+    if (abort) atomicOr(status, kStatusSaoAbort);
   }
+  *reinterpret_cast<uint2*>(S.dst + (size_t)y * st + x) =
+      make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
 }
 
 // One luma ALF pass (whole plane, apply_alf_luma_plane_16 of filter.rs:2045-2124).

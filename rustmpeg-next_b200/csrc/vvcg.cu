@@ -15,8 +15,10 @@
 #include "enc.cuh"
 #include "filters.cuh"
 #include "mc.cuh"
+#include "metrics.cuh"
 #include "recon.cuh"
 #include "tu.cuh"
+#include "txsearch.cuh"
 #include "vvc_tables.h"
 #include "vvcg_device.cuh"
 #include "vvcg_tables_dev.cuh"
@@ -279,6 +281,12 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
   }
   if (cudaFuncSetAttribute(k_encode_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)(kEncWarps * sizeof(EncWs))) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
+  if (cudaFuncSetAttribute(k_luma_tx_search, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(TxsWs)) != cudaSuccess) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return VVCG_UNAVAILABLE;
@@ -600,13 +608,15 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     }
   }
   if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
-    uint32_t gx = 0, gy = 0;
+    // warps: one per (CTU, group of rows), see k_sao
+    uint64_t items = 0;
     for (auto& s : ctx->sao) {
-      gx = std::max<uint32_t>(gx, (uint32_t)(((s.w + 3) / 4 + 63) / 64));
-      gy = std::max<uint32_t>(gy, (uint32_t)std::min((s.h + 3) / 4, 65535));
+      const int tpr = std::max(1, (1 << s.ctu_w_log2) >> 2), rpw = 32 / tpr, ctu_h = 1 << s.ctu_h_log2;
+      const uint64_t n_ctu = (uint64_t)s.ctu_cols * ((s.h + ctu_h - 1) / ctu_h);
+      items = std::max<uint64_t>(items, n_ctu * ((ctu_h + rpw - 1) / rpw));
     }
-    k_sao<<<dim3(gx, gy, (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>((const SaoPass*)ctx->d_sao.p,
-                                                                             ctrl + 1);
+    k_sao<<<dim3((unsigned)((items + 7) / 8), (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>(
+        (const SaoPass*)ctx->d_sao.p, ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
     ctx->launches++;
   }
@@ -721,6 +731,80 @@ vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* p0, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Luma transform search (vvcg_luma_tx_search_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_luma_tx_search_dev(vvcg_ctx* ctx, const vvcg_tx_search_req* reqs, uint32_t num_reqs,
+                                               const int16_t* pred, const int16_t* src, uint64_t in_count,
+                                               int16_t* levels, int16_t* samples, uint64_t out_count,
+                                               vvcg_tx_search_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (num_reqs == 0) return VVCG_OK;
+  if (!reqs || !pred || !src || !levels || !samples || !res)
+    return fail(ctx, VVCG_INVALID_INPUT, "missing requests or buffers");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_tx_search_req& q = reqs[i];
+    if (q.log2_size < 2 || q.log2_size > 5) return fail(ctx, VVCG_INVALID_INPUT, "request %u: size outside 4..32", i);
+    if (q.qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "request %u: QP above 63", i);
+    if (q.mode > 66) return fail(ctx, VVCG_INVALID_INPUT, "request %u: intra mode above 66", i);
+    const uint64_t nn = 1ull << (2 * q.log2_size);
+    if (q.in_off + nn > in_count || q.out_off + nn > out_count)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: sample range past the buffers", i);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_tx_search_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(vvcg_tx_search_req) * num_reqs, cudaMemcpyHostToDevice,
+                     ctx->stream),
+     "upload");
+  k_luma_tx_search<<<num_reqs, kTxsWarps * 32, sizeof(TxsWs), ctx->stream>>>(
+      (const vvcg_tx_search_req*)ctx->d_tu_recs.p, pred, src, levels, samples, res);
+  CK(cudaGetLastError(), "transform search launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Plane metrics (vvcg_plane_metrics_8_dev / vvcg_plane_metrics_16_dev).
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+vvcg_status plane_metrics(vvcg_ctx* ctx, const T* ref, uint64_t ref_stride, const T* dist, uint64_t dist_stride,
+                          uint32_t w, uint32_t h, uint64_t* out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!out) return fail(ctx, VVCG_INVALID_INPUT, "missing output");
+  if (w && h && (!ref || !dist)) return fail(ctx, VVCG_INVALID_INPUT, "missing plane");
+  if (w && h && (ref_stride < w || dist_stride < w))
+    return fail(ctx, VVCG_INVALID_INPUT, "plane view exceeds its backing buffer");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  // out[0] SSE, out[1] SAD, out[2] samples (accelerator.rs:258-292)
+  CK(cudaMemsetAsync(out, 0, 2 * sizeof(uint64_t), ctx->stream), "memset");
+  const uint64_t samples = (uint64_t)w * h;
+  CK(cudaMemcpyAsync(out + 2, &samples, sizeof(samples), cudaMemcpyHostToDevice, ctx->stream), "samples");
+  if (samples == 0) return VVCG_OK;
+  const uint64_t work = samples / (16 / sizeof(T)) + h;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, (uint64_t)ctx->num_sms * 8));
+  k_plane_metrics<T><<<grid, 256, 0, ctx->stream>>>(ref, ref_stride, dist, dist_stride, w, h,
+                                                    reinterpret_cast<unsigned long long*>(out));
+  CK(cudaGetLastError(), "metrics launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_plane_metrics_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint64_t ref_stride,
+                                                const uint8_t* dist, uint64_t dist_stride, uint32_t width,
+                                                uint32_t height, uint64_t* out) {
+  return plane_metrics(ctx, ref, ref_stride, dist, dist_stride, width, height, out);
+}
+
+extern "C" vvcg_status vvcg_plane_metrics_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint64_t ref_stride,
+                                                 const uint16_t* dist, uint64_t dist_stride, uint32_t width,
+                                                 uint32_t height, uint64_t* out) {
+  return plane_metrics(ctx, ref, ref_stride, dist, dist_stride, width, height, out);
+}
 
 // ---------------------------------------------------------------------------
 // Encoder (vvcg_encode_batch).
