@@ -255,7 +255,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
 
 // One warp per coding unit: the residuals of its coded TBs go to the scratch
 // planes at the TB's position. Grid: (ceil(max CUs per picture / 8), pictures).
-__global__ void __launch_bounds__(kWarpsPerCta * 32, 3)
+__global__ void __launch_bounds__(kWarpsPerCta * 32, 4)
 k_residual(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels,
            uint32_t* status) {
   __shared__ ResidWs ws[kWarpsPerCta];
