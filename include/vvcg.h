@@ -227,8 +227,19 @@ vvcg_status vvcg_mc_chroma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w
                                   uint32_t height, uint32_t stride, uint8_t bit_depth,
                                   uint8_t chroma_format, const vvcg_mc_block* blocks,
                                   uint32_t num_blocks, int32_t* out);
+/* 8-bit planes (the strict / multitool 8-bit encoders and decoders):
+ * interpolate_luma_block (inter.rs:896-1051) and interpolate_chroma_block_420
+ * (inter.rs:1056-1182, 4:2:0, MV in 1/16 luma = 1/32 chroma units). Flags and
+ * outputs as in the 16-bit functions; uni-prediction outputs are 0..255. */
+vvcg_status vvcg_mc_luma_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint32_t width, uint32_t height,
+                               uint32_t stride, const vvcg_mc_block* blocks, uint32_t num_blocks,
+                               int32_t* out);
+vvcg_status vvcg_mc_chroma_420_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint32_t width, uint32_t height,
+                                     uint32_t stride, const vvcg_mc_block* blocks, uint32_t num_blocks,
+                                     int32_t* out);
 /* BCW weighted bi-prediction average. Replaces: inter::weighted_average_bi_16
- * (inter.rs:2676). */
+ * (inter.rs:2676); with bit_depth 8 it is also weighted_average_bi
+ * (inter.rs:1189-1201). */
 vvcg_status vvcg_mc_bi_average_16_dev(vvcg_ctx* ctx, const int32_t* pred0, const int32_t* pred1,
                                       uint64_t count, uint8_t bcw_idx, uint8_t bit_depth,
                                       uint16_t* out);
@@ -349,6 +360,65 @@ vvcg_status vvcg_luma_tx_search_dev(vvcg_ctx* ctx, const vvcg_tx_search_req* req
                                     const int16_t* pred, const int16_t* src, uint64_t in_count,
                                     int16_t* levels, int16_t* samples, uint64_t out_count,
                                     vvcg_tx_search_res* res);
+
+/* ---- LMCS and joint chroma residuals (general decoding path) ------------- */
+
+/* LMCS APS (hls.rs:2723 VvcLmcsAps). */
+typedef struct vvcg_lmcs_aps {
+  int16_t bin_cw_delta[16];          /* LmcsDeltaCW[i] */
+  uint8_t min_bin_idx;               /* lmcs_min_bin_idx, 0..15 */
+  uint8_t max_bin_idx;               /* 15 - lmcs_delta_max_bin_idx */
+  int8_t chroma_res_scaling_offset;  /* LmcsDeltaCrs, -7..7 */
+  uint8_t reserved;
+} vvcg_lmcs_aps; /* 36 bytes */
+
+/* Reshaper tables of one APS at one bit depth (LmcsReshaper16, filter.rs:2604). */
+typedef struct vvcg_lmcs_tables {
+  uint8_t bit_depth, min_bin_idx, max_bin_idx, reserved;
+  int32_t reshape_pivot[17];
+  int32_t chroma_adj_lut[16];
+  uint16_t fwd_lut[4096]; /* 1 << bit_depth entries used */
+  uint16_t inv_lut[4096];
+} vvcg_lmcs_tables;
+
+/* Builds the reshaper tables on the host. Replaces: LmcsReshaper16::from_aps
+ * (crates/rustmpeg-video/src/vvc/filter.rs:2628-2705). */
+vvcg_status vvcg_lmcs_build(const vvcg_lmcs_aps* aps, uint8_t bit_depth, vvcg_lmcs_tables* out);
+/* Maps a 16-bit luma plane through the inverse (inverse != 0) or forward LUT in
+ * place (device plane). Replaces: apply_inverse_plane_16 / apply_forward_plane_16
+ * (filter.rs:2708-2722). */
+vvcg_status vvcg_lmcs_map_plane_16_dev(vvcg_ctx* ctx, const vvcg_lmcs_tables* tables, int inverse,
+                                       uint16_t* plane, uint32_t stride, uint32_t width, uint32_t height);
+/* Chroma residual scale factor (cScale) of the VPDU containing each luma
+ * position pos_xy[2i], pos_xy[2i+1] (device), from the average reconstructed
+ * luma left of and above the VPDU. Replaces: chroma_adj_luma
+ * (decode_general.rs:4803-4835) + chroma_scale_for_luma (filter.rs:2725). */
+vvcg_status vvcg_lmcs_chroma_scales_dev(vvcg_ctx* ctx, const vvcg_lmcs_tables* tables, const uint16_t* luma,
+                                        uint32_t stride, uint32_t pic_width, uint32_t pic_height,
+                                        uint32_t ctu_size, const uint32_t* pos_xy, uint32_t num,
+                                        int32_t* scale_out);
+
+enum {
+  VVCG_CRES_SCALE = 1u << 0, /* apply the LMCS chroma residual scaling with `scale` */
+  VVCG_CRES_SINGLE = 1u << 1 /* one component only (cb_off); no joint combination */
+};
+
+typedef struct vvcg_cres_rec {
+  uint8_t log2_w, log2_h; /* chroma TB size */
+  uint8_t bit_depth;      /* 8..12 */
+  int8_t joint;           /* JCCR mode with the picture's sign: -3..3, 0 = none */
+  uint32_t flags;         /* VVCG_CRES_* */
+  int32_t scale;          /* cScale (vvcg_lmcs_chroma_scales_dev) */
+  uint32_t cb_off, cr_off;/* int16 residual blocks (raster) in the buffer, in place */
+} vvcg_cres_rec; /* 20 bytes */
+
+/* Joint Cb-Cr residual derivation and LMCS chroma residual scaling of
+ * residual pairs in place. Replaces: the residual part of
+ * reconstruct_joint_cbcr (decode_general.rs:3932-3966) and of reconstruct_tu
+ * (:4075-4080) with LmcsReshaper16::scale_chroma_residual (filter.rs:2740).
+ * `recs` host memory, `res` device memory of `count` int16. */
+vvcg_status vvcg_chroma_residuals_dev(vvcg_ctx* ctx, const vvcg_cres_rec* recs, uint32_t num, int16_t* res,
+                                      uint64_t count);
 
 /* ---- plane metrics ---------------------------------------------------------- */
 

@@ -92,6 +92,18 @@ def _declare(L):
                                    C.POINTER(C.c_uint64), vp, vp, vp]
     L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     L.orc_tu_batch.argtypes = [i, vp, i, vp, vp]
+    L.orc_mc_luma_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_mc_luma_8.restype = None
+    L.orc_mc_chroma_420_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_mc_chroma_420_8.restype = None
+    L.orc_bi_average_8.argtypes = [vp, vp, i, i, vp]
+    L.orc_bi_average_8.restype = None
+    L.orc_lmcs_build.argtypes = [vp, i, vp]
+    L.orc_lmcs_map_plane.argtypes = [vp, i, vp, i]
+    L.orc_lmcs_map_plane.restype = None
+    L.orc_lmcs_chroma_scale.argtypes = [vp, vp, i, i, i, i, i, i]
+    L.orc_chroma_residuals.argtypes = [vp, vp]
+    L.orc_chroma_residuals.restype = None
     L.orc_luma_tx_search.argtypes = [i, vp, vp, i, i, i, i, vp, vp, C.POINTER(C.c_uint64)]
     L.orc_plane_metrics.argtypes = [vp, C.c_uint64, vp, C.c_uint64, C.c_uint32, C.c_uint32, i, vp]
 
@@ -304,6 +316,32 @@ def bi_average(p0, p1, bcw, bd):
     return out
 
 
+def mc_luma_8(ref, bx, by, w, h, mvx, mvy, bi=False, affine=False, alt_hpel=False):
+    """inter.rs:896-1051 interpolate_luma_block on an 8-bit plane."""
+    ref = np.ascontiguousarray(ref, dtype=np.uint8)
+    out = np.zeros((h, w), dtype=np.int32)
+    lib().orc_mc_luma_8(_p(ref), ref.shape[1], ref.shape[0], ref.shape[1], bx, by, w, h, mvx, mvy, int(bi),
+                        int(alt_hpel), int(affine), _p(out))
+    return out
+
+
+def mc_chroma_420_8(ref, cx, cy, cw, ch, mvx, mvy, bi=False):
+    """inter.rs:1056-1182 interpolate_chroma_block_420 on an 8-bit plane."""
+    ref = np.ascontiguousarray(ref, dtype=np.uint8)
+    out = np.zeros((ch, cw), dtype=np.int32)
+    lib().orc_mc_chroma_420_8(_p(ref), ref.shape[1], ref.shape[0], ref.shape[1], cx, cy, cw, ch, mvx, mvy,
+                              int(bi), _p(out))
+    return out
+
+
+def bi_average_8(p0, p1, bcw):
+    """inter.rs:1189-1201 weighted_average_bi."""
+    p0, p1 = _i32(p0), _i32(p1)
+    out = np.zeros(p0.shape, dtype=np.int32)
+    lib().orc_bi_average_8(_p(p0), _p(p1), p0.size, bcw, _p(out))
+    return out
+
+
 # ------------------------------------------------------------ frame path --
 
 # Record layouts of include/vvcg.h, as numpy structured dtypes.
@@ -429,3 +467,44 @@ def luma_tx_search(pred, src, qp, mode, use_ts=False, lfnst=False):
     r = lib().orc_luma_tx_search(n, _p(pred), _p(src), qp, mode, int(use_ts), int(lfnst), _p(lv), _p(sm),
                                  C.byref(sse))
     return (r >> 8) & 0xF, (r >> 4) & 0xF, (r >> 1) & 1, r & 1, sse.value, lv, sm
+
+
+# ------------------------------------------------------- LMCS / joint chroma --
+
+LMCS_APS_DTYPE = np.dtype([("bin_cw_delta", "<i2", (16,)), ("min_bin_idx", "u1"), ("max_bin_idx", "u1"),
+                           ("chroma_res_scaling_offset", "i1"), ("reserved", "u1")])
+LMCS_TABLES_DTYPE = np.dtype([("bit_depth", "u1"), ("min_bin_idx", "u1"), ("max_bin_idx", "u1"),
+                              ("reserved", "u1"), ("reshape_pivot", "<i4", (17,)), ("chroma_adj_lut", "<i4", (16,)),
+                              ("fwd_lut", "<u2", (4096,)), ("inv_lut", "<u2", (4096,))])
+CRES_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("joint", "i1"),
+                       ("flags", "<u4"), ("scale", "<i4"), ("cb_off", "<u4"), ("cr_off", "<u4")])
+
+
+def lmcs_build(aps, bd):
+    """LmcsReshaper16::from_aps (filter.rs:2628-2705) -> LMCS_TABLES_DTYPE record."""
+    a = np.asarray(aps, dtype=LMCS_APS_DTYPE).reshape(1).copy()
+    t = np.zeros(1, LMCS_TABLES_DTYPE)
+    lib().orc_lmcs_build(_p(a), bd, _p(t))
+    return t[0]
+
+
+def lmcs_map_plane(tables, plane, inverse=True):
+    t = np.asarray(tables, dtype=LMCS_TABLES_DTYPE).reshape(1).copy()
+    out = np.ascontiguousarray(plane, dtype=np.uint16).copy()
+    lib().orc_lmcs_map_plane(_p(t), int(inverse), _p(out), out.size)
+    return out
+
+
+def lmcs_chroma_scale(tables, luma, ctu, x, y):
+    t = np.asarray(tables, dtype=LMCS_TABLES_DTYPE).reshape(1).copy()
+    luma = np.ascontiguousarray(luma, dtype=np.uint16)
+    h, w = luma.shape
+    return lib().orc_lmcs_chroma_scale(_p(t), _p(luma), w, w, h, ctu, x, y)
+
+
+def chroma_residuals(recs, res):
+    recs = np.ascontiguousarray(recs, dtype=CRES_DTYPE)
+    out = np.ascontiguousarray(res, dtype=np.int16).copy()
+    for i in range(len(recs)):
+        lib().orc_chroma_residuals(_p(recs[i:i + 1].copy()), _p(out))
+    return out

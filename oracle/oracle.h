@@ -137,6 +137,12 @@ void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, in
                                         int32_t* out);
 void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int bd,
                             uint16_t* out);
+// ---- inter.rs (8-bit planes) ------------------------------------------------------
+void interpolate_luma_block_8(const uint8_t* ref, int pw, int ph, int stride, int bx, int by, int w, int h,
+                              int mv_x, int mv_y, bool bi, bool alt_hpel, bool affine, int32_t* out);
+void interpolate_chroma_block_420_8(const uint8_t* ref, int pw, int ph, int stride, int cx, int cy, int cw,
+                                    int ch, int mv_x, int mv_y, bool bi, int32_t* out);
+void weighted_average_bi_8(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int32_t* out);
 
 // ---- transform units (orc_tu.cpp) ------------------------------------------------
 // Same layout and flag values as vvcg_tu_rec / VVCG_TU_* of the C ABI.

@@ -166,3 +166,15 @@ extern "C" int orc_plane_metrics(const void* a, uint64_t sa, const void* b, uint
   out[2] = (uint64_t)w * h;
   return 0;
 }
+
+extern "C" void orc_mc_luma_8(const uint8_t* ref, int pw, int ph, int stride, int bx, int by, int w, int h,
+                              int mvx, int mvy, int bi, int alt_hpel, int affine, int32_t* out) {
+  orc::interpolate_luma_block_8(ref, pw, ph, stride, bx, by, w, h, mvx, mvy, bi, alt_hpel, affine, out);
+}
+extern "C" void orc_mc_chroma_420_8(const uint8_t* ref, int pw, int ph, int stride, int cx, int cy, int cw,
+                                    int ch, int mvx, int mvy, int bi, int32_t* out) {
+  orc::interpolate_chroma_block_420_8(ref, pw, ph, stride, cx, cy, cw, ch, mvx, mvy, bi, out);
+}
+extern "C" void orc_bi_average_8(const int32_t* p0, const int32_t* p1, int n, int bcw, int32_t* out) {
+  orc::weighted_average_bi_8(p0, p1, n, bcw, out);
+}

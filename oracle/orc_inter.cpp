@@ -169,6 +169,122 @@ void interpolate_chroma_block_format_16(const Plane16& ref, int bxc, int byc, in
     }
 }
 
+// inter.rs:896-1051 interpolate_luma_block (8-bit planes)
+void interpolate_luma_block_8(const uint8_t* ref, int pw, int ph, int stride, int bx, int by, int w, int h,
+                              int mv_x, int mv_y, bool bi, bool alt_hpel, bool affine, int32_t* out) {
+  const int int_x = bx + (mv_x >> 4), int_y = by + (mv_y >> 4);
+  const int fx = mv_x & 15, fy = mv_y & 15;
+  const int head = 14 - 8, offs = 1 << 13;  // IF_INTERNAL_PREC - 8, IF_INTERNAL_OFFS
+  auto g = [&](int x, int y) { return (int)ref[clampi(y, 0, ph - 1) * stride + clampi(x, 0, pw - 1)]; };
+  auto coeffs = [&](int frac, int* c) {
+    for (int k = 0; k < 8; k++)
+      c[k] = affine ? kAffineTaps8[frac * 8 + k] : (alt_hpel && frac == 8) ? kLumaAltHpel[k] : kLumaTaps8[frac * 8 + k];
+  };
+  // tap k at position p + tap_start + k (affine: tap_start -2 and one more -1)
+  const int tap0 = affine ? -2 - 1 : -3;
+  if (fx == 0 && fy == 0) {
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        int s = g(int_x + x, int_y + y);
+        out[y * w + x] = bi ? (s << head) - offs : s;
+      }
+    return;
+  }
+  if (fy == 0 || fx == 0) {
+    int c[8];
+    coeffs(fy == 0 ? fx : fy, c);
+    const int shift = bi ? 6 - head : 6;
+    const int offset = bi ? -offs << shift : 1 << (shift - 1);
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        int s = 0;
+        for (int k = 0; k < 8; k++)
+          s += (fy == 0 ? g(int_x + x + tap0 + k, int_y + y) : g(int_x + x, int_y + y + tap0 + k)) * c[k];
+        int v = (s + offset) >> shift;
+        out[y * w + x] = bi ? v : clampi(v, 0, 255);
+      }
+    return;
+  }
+  int cx[8], cy[8];
+  coeffs(fx, cx);
+  coeffs(fy, cy);
+  const int eh = h + 7, shift1 = 6 - head, offset1 = -offs << shift1;
+  std::vector<int> tmp((size_t)w * eh);
+  for (int y = 0; y < eh; y++)
+    for (int x = 0; x < w; x++) {
+      int s = 0;
+      for (int k = 0; k < 8; k++) s += g(int_x + x + tap0 + k, int_y - 3 + y) * cx[k];
+      tmp[y * w + x] = (s + offset1) >> shift1;
+    }
+  const int shift2 = bi ? 6 : 6 + head;
+  const int offset2 = bi ? 0 : (1 << (shift2 - 1)) + (offs << 6);
+  for (int y = 0; y < h; y++)
+    for (int x = 0; x < w; x++) {
+      int s = 0;
+      for (int k = 0; k < 8; k++) s += tmp[(y + k) * w + x] * cy[k];
+      int v = (s + offset2) >> shift2;
+      out[y * w + x] = bi ? v : clampi(v, 0, 255);
+    }
+}
+
+// inter.rs:1056-1182 interpolate_chroma_block_420 (8-bit planes; MV in 1/16
+// luma = 1/32 chroma units)
+void interpolate_chroma_block_420_8(const uint8_t* ref, int pw, int ph, int stride, int cx, int cy, int cw,
+                                    int ch, int mv_x, int mv_y, bool bi, int32_t* out) {
+  const int int_x = cx + (mv_x >> 5), int_y = cy + (mv_y >> 5);
+  const int fx = mv_x & 31, fy = mv_y & 31;
+  const int head = 6, offs = 1 << 13;
+  auto g = [&](int x, int y) { return (int)ref[clampi(y, 0, ph - 1) * stride + clampi(x, 0, pw - 1)]; };
+  if (fx == 0 && fy == 0) {
+    for (int y = 0; y < ch; y++)
+      for (int x = 0; x < cw; x++) {
+        int s = g(int_x + x, int_y + y);
+        out[y * cw + x] = bi ? (s << head) - offs : s;
+      }
+    return;
+  }
+  if (fy == 0 || fx == 0) {
+    const int8_t* c = &kChromaTaps4[(fy == 0 ? fx : fy) * 4];
+    const int shift = bi ? 6 - head : 6;
+    const int offset = bi ? -offs << shift : 1 << (shift - 1);
+    for (int y = 0; y < ch; y++)
+      for (int x = 0; x < cw; x++) {
+        int s = 0;
+        for (int k = 0; k < 4; k++)
+          s += (fy == 0 ? g(int_x + x - 1 + k, int_y + y) : g(int_x + x, int_y + y - 1 + k)) * c[k];
+        int v = (s + offset) >> shift;
+        out[y * cw + x] = bi ? v : clampi(v, 0, 255);
+      }
+    return;
+  }
+  const int8_t* cxf = &kChromaTaps4[fx * 4];
+  const int8_t* cyf = &kChromaTaps4[fy * 4];
+  const int eh = ch + 3, shift1 = 6 - head, offset1 = -offs << shift1;
+  std::vector<int> tmp((size_t)cw * eh);
+  for (int y = 0; y < eh; y++)
+    for (int x = 0; x < cw; x++) {
+      int s = 0;
+      for (int k = 0; k < 4; k++) s += g(int_x + x - 1 + k, int_y - 1 + y) * cxf[k];
+      tmp[y * cw + x] = (s + offset1) >> shift1;
+    }
+  const int shift2 = bi ? 6 : 6 + head;
+  const int offset2 = bi ? 0 : (1 << (shift2 - 1)) + (offs << 6);
+  for (int y = 0; y < ch; y++)
+    for (int x = 0; x < cw; x++) {
+      int s = 0;
+      for (int k = 0; k < 4; k++) s += tmp[(y + k) * cw + x] * cyf[k];
+      int v = (s + offset2) >> shift2;
+      out[y * cw + x] = bi ? v : clampi(v, 0, 255);
+    }
+}
+
+// inter.rs:1189-1201 weighted_average_bi (8-bit output range)
+void weighted_average_bi_8(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int32_t* out) {
+  const int w1 = kBcwWeights[std::min(bcw_idx, 4)], w0 = 8 - w1;
+  const int sn = 6 + 3, off = (1 << (sn - 1)) + ((1 << 13) << 3);
+  for (int i = 0; i < n; i++) out[i] = clampi((p0[i] * w0 + p1[i] * w1 + off) >> sn, 0, 255);
+}
+
 // inter.rs:2676-2698 weighted_average_bi_16
 void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int bd,
                             uint16_t* out) {

@@ -40,6 +40,14 @@ MC_BLOCK_DTYPE = np.dtype([("x", "<i4"), ("y", "<i4"), ("w", "<u2"), ("h", "<u2"
                            ("mv_x", "<i4"), ("mv_y", "<i4"), ("flags", "<u4"),
                            ("reserved", "<u4"), ("out_offset", "<u8")], align=True)
 
+LMCS_APS_DTYPE = np.dtype([("bin_cw_delta", "<i2", (16,)), ("min_bin_idx", "u1"), ("max_bin_idx", "u1"),
+                           ("chroma_res_scaling_offset", "i1"), ("reserved", "u1")])
+LMCS_TABLES_DTYPE = np.dtype([("bit_depth", "u1"), ("min_bin_idx", "u1"), ("max_bin_idx", "u1"),
+                              ("reserved", "u1"), ("reshape_pivot", "<i4", (17,)), ("chroma_adj_lut", "<i4", (16,)),
+                              ("fwd_lut", "<u2", (4096,)), ("inv_lut", "<u2", (4096,))])
+CRES_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("joint", "i1"),
+                       ("flags", "<u4"), ("scale", "<i4"), ("cb_off", "<u4"), ("cr_off", "<u4")])
+CRES_SCALE, CRES_SINGLE = 1, 2
 TXS_REQ_DTYPE = np.dtype([("log2_size", "u1"), ("qp", "u1"), ("mode", "u1"), ("flags", "u1"),
                           ("in_off", "<u4"), ("out_off", "<u4"), ("reserved", "<u4")])
 TXS_RES_DTYPE = np.dtype([("sse", "<u8"), ("mts_idx", "u1"), ("lfnst_idx", "u1"), ("transform_skip", "u1"),
@@ -116,6 +124,7 @@ class _Config(C.Structure):
 assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize == 32
 assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.itemsize == 16
 assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
+assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
 def build(force: bool = False) -> str:
@@ -159,6 +168,8 @@ def lib():
         L.vvcg_mc_luma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, vp, u32, vp]
         L.vvcg_mc_chroma_16_dev.argtypes = [vp, vp, u32, u32, u32, u8, u8, vp, u32, vp]
         L.vvcg_mc_bi_average_16_dev.argtypes = [vp, vp, vp, u64, u8, u8, vp]
+        L.vvcg_mc_luma_8_dev.argtypes = [vp, vp, u32, u32, u32, vp, u32, vp]
+        L.vvcg_mc_chroma_420_8_dev.argtypes = [vp, vp, u32, u32, u32, vp, u32, vp]
         for n in ("vvcg_tu_inverse_batch", "vvcg_tu_forward_batch"):
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
@@ -166,6 +177,10 @@ def lib():
         for n in ("vvcg_plane_metrics_8_dev", "vvcg_plane_metrics_16_dev"):
             getattr(L, n).argtypes = [vp, vp, u64, vp, u64, u32, u32, vp]
         L.vvcg_luma_tx_search_dev.argtypes = [vp, vp, u32, vp, vp, u64, vp, vp, u64, vp]
+        L.vvcg_lmcs_build.argtypes = [vp, u8, vp]
+        L.vvcg_lmcs_map_plane_16_dev.argtypes = [vp, vp, C.c_int, vp, u32, u32, u32]
+        L.vvcg_lmcs_chroma_scales_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, u32, vp]
+        L.vvcg_chroma_residuals_dev.argtypes = [vp, vp, u32, vp, u64]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -369,6 +384,26 @@ class Context:
         torch.cuda.synchronize(pred.device)
         return res.cpu().numpy().view(TXS_RES_DTYPE)
 
+    # -- LMCS / joint chroma residuals --
+    def lmcs_map_plane(self, tables, plane, inverse=True):
+        """Map a (H, W) int16 CUDA tensor of 16-bit luma samples in place."""
+        t = np.asarray(tables, dtype=LMCS_TABLES_DTYPE).reshape(1).copy()
+        h, w = plane.shape
+        self._check(self._L.vvcg_lmcs_map_plane_16_dev(self._h, _ptr(t), int(inverse), _ptr(plane),
+                                                       plane.stride(0), w, h))
+
+    def lmcs_chroma_scales(self, tables, luma, ctu, pos, out):
+        """cScale per luma position; pos: (N, 2) uint32-as-int32 CUDA tensor, out int32 CUDA tensor."""
+        t = np.asarray(tables, dtype=LMCS_TABLES_DTYPE).reshape(1).copy()
+        h, w = luma.shape
+        self._check(self._L.vvcg_lmcs_chroma_scales_dev(self._h, _ptr(t), _ptr(luma), luma.stride(0), w, h, ctu,
+                                                        _ptr(pos), pos.shape[0], _ptr(out)))
+
+    def chroma_residuals(self, recs, res):
+        recs = np.ascontiguousarray(recs, dtype=CRES_DTYPE)
+        self._keep = recs
+        self._check(self._L.vvcg_chroma_residuals_dev(self._h, _ptr(recs), len(recs), _ptr(res), res.numel()))
+
     # -- metrics --
     def plane_metrics(self, ref, dist):
         """(sse, sad, samples) of two equally shaped 2-D CUDA tensors (uint8, or
@@ -410,6 +445,18 @@ class Context:
         self._check(self._L.vvcg_tu_forward_batch(self._h, _ptr(recs), len(recs), _ptr(data),
                                                   data.numel(), _ptr(out), out.numel()))
 
+    def mc_luma_8(self, ref, blocks, out):
+        """ref: (H, W) uint8 CUDA tensor (the 8-bit functions of inter.rs)."""
+        h, w = ref.shape
+        n = blocks.numel() // MC_BLOCK_DTYPE.itemsize
+        self._check(self._L.vvcg_mc_luma_8_dev(self._h, _ptr(ref), w, h, ref.stride(0), _ptr(blocks), n, _ptr(out)))
+
+    def mc_chroma_420_8(self, ref, blocks, out):
+        h, w = ref.shape
+        n = blocks.numel() // MC_BLOCK_DTYPE.itemsize
+        self._check(self._L.vvcg_mc_chroma_420_8_dev(self._h, _ptr(ref), w, h, ref.stride(0), _ptr(blocks), n,
+                                                     _ptr(out)))
+
     def mc_bi_average(self, p0, p1, bcw_idx, bit_depth, out):
         self._check(self._L.vvcg_mc_bi_average_16_dev(self._h, _ptr(p0), _ptr(p1), p0.numel(),
                                                       bcw_idx, bit_depth, _ptr(out)))
@@ -437,3 +484,13 @@ def recon_picture_static(pic, cus, levels, planes, stream=None):
                                      C.c_void_p(raw) if raw else None, err, len(err))
     if st != OK:
         raise _ERRORS.get(st, Execution)(err.value.decode())
+
+
+def lmcs_build(aps, bit_depth):
+    """Reshaper tables (LMCS_TABLES_DTYPE) of an LMCS APS (host function of the library)."""
+    a = np.asarray(aps, dtype=LMCS_APS_DTYPE).reshape(1).copy()
+    t = np.zeros(1, LMCS_TABLES_DTYPE)
+    st = lib().vvcg_lmcs_build(_ptr(a), bit_depth, _ptr(t))
+    if st != OK:
+        raise _ERRORS.get(st, Execution)("invalid LMCS APS")
+    return t[0]

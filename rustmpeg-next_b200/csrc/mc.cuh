@@ -4,7 +4,10 @@
 // Follows interpolate_luma_block_16 (inter.rs:2010-2134),
 // interpolate_chroma_block_format_16 (:2543-2672) and weighted_average_bi_16
 // (:2676-2698) of the reference, including the uni-prediction second-stage
-// shift `12 - bd` for 2-D fractional positions (inter.rs:2051 / :2583).
+// shift `12 - bd` for 2-D fractional positions (inter.rs:2051 / :2583); and
+// the 8-bit functions interpolate_luma_block (inter.rs:896-1051) and
+// interpolate_chroma_block_420 (:1056-1182), which read 8-bit planes and use
+// the second stage (sum + 2^11) >> 12 for 2-D uni-prediction.
 //
 // Each CTA computes one block in 32x32 output tiles: the tile's reference
 // window (clamped to the plane, as the reference's get_p does) is staged in
@@ -20,6 +23,7 @@ constexpr int kMcT = 32;
 
 struct McParams {
   const uint16_t* ref;
+  const uint8_t* ref8;  // 8-bit plane of the 8-bit functions (then ref is unused and bd is 8)
   int32_t w, h, stride, bd;
   int32_t chroma;   // 0 = luma (8 taps), else chroma format (4 taps)
 };
@@ -84,7 +88,7 @@ __global__ void __launch_bounds__(256) k_mc(McParams Pm, const vvcg_mc_block* __
       for (int i = threadIdx.x; i < ww * wh; i += blockDim.x) {
         int yy = i / ww, xx = i % ww;
         int gx = clampi(wx0 + xx, 0, Pm.w - 1), gy = clampi(wy0 + yy, 0, Pm.h - 1);
-        win[yy][xx] = Pm.ref[(size_t)gy * Pm.stride + gx];
+        win[yy][xx] = Pm.ref8 ? (int)Pm.ref8[(size_t)gy * Pm.stride + gx] : (int)Pm.ref[(size_t)gy * Pm.stride + gx];
       }
       __syncthreads();
       if (fx == 0 && fy == 0) {
@@ -114,7 +118,12 @@ __global__ void __launch_bounds__(256) k_mc(McParams Pm, const vvcg_mc_block* __
           int x = i % tw, y = i / tw;
           int s = 0;
           for (int k = 0; k < ntap; k++) s += fv[k] * tmp[y + k][x];
-          o[(size_t)(ty0 + y) * bw + tx0 + x] = bi ? (s >> shift2) - offs : clampi((int)((unsigned)s + (unsigned)add2) >> shift2, 0, maxv);
+          // 8-bit functions: (sum of taps x (tmp - 2^13) + 2^11 + 2^13 x 64) >> 12,
+          // which is (s + 2^11) >> 12 because every filter's taps sum to 64
+          o[(size_t)(ty0 + y) * bw + tx0 + x] =
+              bi ? (s >> shift2) - offs
+                 : (Pm.ref8 ? clampi((s + 2048) >> 12, 0, 255)
+                            : clampi((int)((unsigned)s + (unsigned)add2) >> shift2, 0, maxv));
         }
       }
     }

@@ -14,6 +14,7 @@
 #include "../../include/vvcg.h"
 #include "enc.cuh"
 #include "filters.cuh"
+#include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
 #include "recon.cuh"
@@ -86,6 +87,7 @@ struct vvcg_ctx {
   // transform-unit batches
   std::vector<uint32_t> tu_idx;
   DevBuf d_tu_recs, d_tu_idx;
+  DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   uint64_t flags_count = 0;
 };
 
@@ -322,7 +324,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
-                    &ctx->d_tu_recs, &ctx->d_tu_idx})
+                    &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs})
     b->release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -697,11 +699,34 @@ static vvcg_status mc_common(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uin
   if (!ref || !out || (n && !blocks) || !w || !h || stride < w || bd < 8 || bd > 12)
     return fail(ctx, VVCG_INVALID_INPUT, "invalid MC arguments");
   if (n == 0) return VVCG_OK;
-  McParams pm{ref, (int32_t)w, (int32_t)h, (int32_t)stride, bd, chroma};
+  McParams pm{ref, nullptr, (int32_t)w, (int32_t)h, (int32_t)stride, bd, chroma};
   k_mc<<<n, 256, 0, ctx->stream>>>(pm, blocks, n, out, (uint32_t*)ctx->d_ctrl.p + 1);
   CK(cudaGetLastError(), "mc launch");
   ctx->launches++;
   return VVCG_OK;
+}
+
+static vvcg_status mc_common_8(vvcg_ctx* ctx, const uint8_t* ref, uint32_t w, uint32_t h, uint32_t stride,
+                               int chroma, const vvcg_mc_block* blocks, uint32_t n, int32_t* out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!ref || !out || (n && !blocks) || !w || !h || stride < w)
+    return fail(ctx, VVCG_INVALID_INPUT, "invalid MC arguments");
+  if (n == 0) return VVCG_OK;
+  McParams pm{nullptr, ref, (int32_t)w, (int32_t)h, (int32_t)stride, 8, chroma};
+  k_mc<<<n, 256, 0, ctx->stream>>>(pm, blocks, n, out, (uint32_t*)ctx->d_ctrl.p + 1);
+  CK(cudaGetLastError(), "mc launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+vvcg_status vvcg_mc_luma_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint32_t w, uint32_t h, uint32_t stride,
+                               const vvcg_mc_block* blocks, uint32_t n, int32_t* out) {
+  return mc_common_8(ctx, ref, w, h, stride, 0, blocks, n, out);
+}
+
+vvcg_status vvcg_mc_chroma_420_8_dev(vvcg_ctx* ctx, const uint8_t* ref, uint32_t w, uint32_t h, uint32_t stride,
+                                     const vvcg_mc_block* blocks, uint32_t n, int32_t* out) {
+  return mc_common_8(ctx, ref, w, h, stride, 1, blocks, n, out);
 }
 
 vvcg_status vvcg_mc_luma_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uint32_t h,
@@ -760,6 +785,107 @@ extern "C" vvcg_status vvcg_luma_tx_search_dev(vvcg_ctx* ctx, const vvcg_tx_sear
   k_luma_tx_search<<<num_reqs, kTxsWarps * 32, sizeof(TxsWs), ctx->stream>>>(
       (const vvcg_tx_search_req*)ctx->d_tu_recs.p, pred, src, levels, samples, res);
   CK(cudaGetLastError(), "transform search launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// LMCS and joint chroma residuals.
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_lmcs_build(const vvcg_lmcs_aps* aps, uint8_t bit_depth, vvcg_lmcs_tables* t) {
+  // LmcsReshaper16::from_aps (filter.rs:2628-2705)
+  if (!aps || !t) return VVCG_INVALID_INPUT;
+  memset(t, 0, sizeof(*t));
+  const int bd = std::min(12, std::max(8, (int)bit_depth));
+  const int max_val = (1 << bd) - 1, log2_cw = bd - 4, init_cw = 1 << log2_cw;
+  const int min_bin = std::min<int>(aps->min_bin_idx, 15);
+  const int max_bin = std::max(std::min<int>(aps->max_bin_idx, 15), min_bin);
+  int bin_cw[16] = {0}, in_piv[17] = {0}, re_piv[17] = {0}, fwd_sc[16], inv_sc[16], adj[16];
+  for (int i = min_bin; i <= max_bin; i++) bin_cw[i] = std::max(0, init_cw + aps->bin_cw_delta[i]);
+  for (int i = 0; i < 16; i++) {
+    re_piv[i + 1] = re_piv[i] + bin_cw[i];
+    in_piv[i + 1] = in_piv[i] + init_cw;
+    fwd_sc[i] = ((bin_cw[i] << kLmcsFpPrec) + (1 << (log2_cw - 1))) >> log2_cw;
+    inv_sc[i] = bin_cw[i] ? (init_cw << kLmcsFpPrec) / bin_cw[i] : 0;
+    adj[i] = bin_cw[i] ? (init_cw << kLmcsFpPrec) / std::max(1, bin_cw[i] + aps->chroma_res_scaling_offset)
+                       : 1 << kLmcsFpPrec;
+  }
+  const int half = 1 << (kLmcsFpPrec - 1);
+  for (int v = 0; v <= max_val; v++) {
+    const int iy = std::min(15, v >> log2_cw);
+    t->fwd_lut[v] = (uint16_t)std::min(max_val, std::max(0, re_piv[iy] + ((fwd_sc[iy] * (v - in_piv[iy]) + half) >> kLmcsFpPrec)));
+    int ii = min_bin;
+    while (ii <= max_bin && v >= re_piv[ii + 1]) ii++;
+    ii = std::min(ii, 15);
+    t->inv_lut[v] = (uint16_t)std::min(max_val, std::max(0, in_piv[ii] + ((inv_sc[ii] * (v - re_piv[ii]) + half) >> kLmcsFpPrec)));
+  }
+  t->bit_depth = (uint8_t)bd;
+  t->min_bin_idx = (uint8_t)min_bin;
+  t->max_bin_idx = (uint8_t)max_bin;
+  memcpy(t->reshape_pivot, re_piv, sizeof(re_piv));
+  memcpy(t->chroma_adj_lut, adj, sizeof(adj));
+  return VVCG_OK;
+}
+
+namespace {
+vvcg_status upload_lmcs(vvcg_ctx* ctx, const vvcg_lmcs_tables* t) {
+  if (!t || t->bit_depth < 8 || t->bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "LMCS tables");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_lmcs.reserve(sizeof(vvcg_lmcs_tables)), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_lmcs.p, t, sizeof(vvcg_lmcs_tables), cudaMemcpyHostToDevice, ctx->stream), "upload");
+  return VVCG_OK;
+}
+}  // namespace
+
+extern "C" vvcg_status vvcg_lmcs_map_plane_16_dev(vvcg_ctx* ctx, const vvcg_lmcs_tables* t, int inverse,
+                                                  uint16_t* plane, uint32_t stride, uint32_t w, uint32_t h) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (w && h && (!plane || stride < w)) return fail(ctx, VVCG_INVALID_INPUT, "plane");
+  vvcg_status st = upload_lmcs(ctx, t);
+  if (st != VVCG_OK || !w || !h) return st;
+  const vvcg_lmcs_tables* d = (const vvcg_lmcs_tables*)ctx->d_lmcs.p;
+  const uint64_t work = (uint64_t)((w + 3) / 4) * h;
+  const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>((work + 255) / 256, (uint64_t)ctx->num_sms * 8));
+  k_lut_plane<<<grid, 256, 0, ctx->stream>>>(inverse ? d->inv_lut : d->fwd_lut, t->bit_depth, plane, stride, w, h);
+  CK(cudaGetLastError(), "lmcs launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_lmcs_chroma_scales_dev(vvcg_ctx* ctx, const vvcg_lmcs_tables* t, const uint16_t* luma,
+                                                   uint32_t stride, uint32_t pw, uint32_t ph, uint32_t ctu,
+                                                   const uint32_t* pos, uint32_t num, int32_t* out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (num && (!luma || !pos || !out || !pw || !ph || stride < pw))
+    return fail(ctx, VVCG_INVALID_INPUT, "missing or invalid buffers");
+  if (ctu != 32 && ctu != 64 && ctu != 128) return fail(ctx, VVCG_INVALID_INPUT, "CTU size");
+  vvcg_status st = upload_lmcs(ctx, t);
+  if (st != VVCG_OK || !num) return st;
+  k_lmcs_chroma_scales<<<(num + 7) / 8, 256, 0, ctx->stream>>>((const vvcg_lmcs_tables*)ctx->d_lmcs.p, luma, stride,
+                                                              (int)pw, (int)ph, (int)ctu, pos, num, out);
+  CK(cudaGetLastError(), "lmcs launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_chroma_residuals_dev(vvcg_ctx* ctx, const vvcg_cres_rec* recs, uint32_t num,
+                                                 int16_t* res, uint64_t count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num) return VVCG_OK;
+  if (!recs || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing records or residuals");
+  for (uint32_t i = 0; i < num; i++) {
+    const vvcg_cres_rec& r = recs[i];
+    if (r.log2_w > 5 || r.log2_h > 5 || r.bit_depth < 8 || r.bit_depth > 12 || r.joint < -3 || r.joint > 3)
+      return fail(ctx, VVCG_INVALID_INPUT, "record %u: size, bit depth or joint mode", i);
+    const uint64_t n = 1ull << (r.log2_w + r.log2_h);
+    if (r.cb_off + n > count || (!(r.flags & VVCG_CRES_SINGLE) && r.cr_off + n > count))
+      return fail(ctx, VVCG_INVALID_INPUT, "record %u: residual range past the buffer", i);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_cres_rec) * num), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, recs, sizeof(vvcg_cres_rec) * num, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  k_chroma_residuals<<<(num + 7) / 8, 256, 0, ctx->stream>>>((const vvcg_cres_rec*)ctx->d_tu_recs.p, num, res);
+  CK(cudaGetLastError(), "chroma residual launch");
   ctx->launches++;
   return VVCG_OK;
 }

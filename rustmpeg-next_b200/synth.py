@@ -308,3 +308,17 @@ def source_planes(w, h, bd=10, cf=1, seed=0, vis=None):
         u = np.repeat(u, 2, axis=0)[:vh]
         v = np.repeat(v, 2, axis=0)[:vh]
     return pad_to(y, w, h), pad_to(u, cw, ch), pad_to(v, cw, ch)
+
+
+def random_lmcs_aps(rng):
+    """A seeded LMCS APS (LMCS_APS_DTYPE) with codeword deltas within the
+    range the syntax allows for the active bins."""
+    from . import LMCS_APS_DTYPE
+
+    a = np.zeros((), LMCS_APS_DTYPE)
+    lo = int(rng.integers(0, 4))
+    hi = int(rng.integers(12, 16))
+    a["min_bin_idx"], a["max_bin_idx"] = lo, hi
+    a["bin_cw_delta"] = rng.integers(-12, 13, 16)
+    a["chroma_res_scaling_offset"] = int(rng.integers(-7, 8))
+    return a
