@@ -187,6 +187,7 @@ def main():
     ap.add_argument("--frames-per-qp", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4, help="pictures in the CPU baseline sample")
+    ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -253,14 +254,15 @@ def main():
     ctx.run(pkg.STAGE_ALL)
     ctx.sync()
 
-    # warm-up, then the timed device-resident steps
+    # warm-up (the first graph run captures the stages), then the timed steps
+    use_graph = not args.no_graph
     for _ in range(args.warmup):
-        ctx.run(pkg.STAGE_ALL)
+        ctx.run(pkg.STAGE_ALL, graph=use_graph)
     ctx.sync()
     launches0 = ctx.kernel_launches
     sampler = ClockSampler(local)
     sampler.start()
-    ms_step = timed(lambda: ctx.run(pkg.STAGE_ALL), args.steps)
+    ms_step = timed(lambda: ctx.run(pkg.STAGE_ALL, graph=use_graph), args.steps)
     clocks = sampler.stop()
     launches = ctx.kernel_launches - launches0
     ctx.sync()
@@ -270,8 +272,8 @@ def main():
     for name, st in (("recon", pkg.STAGE_RECON), ("deblock", pkg.STAGE_DEBLOCK),
                      ("sao", pkg.STAGE_SAO), ("alf", pkg.STAGE_ALF)):
         for _ in range(2):
-            ctx.run(st)
-        stage_ms[name] = timed(lambda st=st: ctx.run(st), max(3, args.steps // 2))
+            ctx.run(st, graph=use_graph)
+        stage_ms[name] = timed(lambda st=st: ctx.run(st, graph=use_graph), max(3, args.steps // 2))
     ctx.run(pkg.STAGE_ALL)
     ctx.sync()
 
@@ -281,7 +283,7 @@ def main():
 
     def e2e_step():
         ctx.upload(batch)
-        ctx.run(pkg.STAGE_ALL)
+        ctx.run(pkg.STAGE_ALL, graph=use_graph)
         ctx.download(outs)  # synchronises the stream
 
     for _ in range(2):
@@ -341,6 +343,7 @@ def main():
             "config": {"workload": "1920x1080 10-bit 4:2:0, 32 frames x QP{22,27,32,37} = "
                                    f"{n_pics} pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)",
                        "pictures_per_step": n_pics, "parallelism": f"replicas x{world}",
+                       "launch": "direct launches" if args.no_graph else "CUDA graph replay",
                        "l2": "inputs larger than L2 (466 MB levels, 1.6 GB planes); no flush",
                        "records": "seeded synthetic decoder records"},
             "roofline": roofline,

@@ -191,6 +191,11 @@ vvcg_status vvcg_decode_batch(vvcg_ctx* ctx, const vvcg_batch* batch, const vvcg
 vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* batch);
 vvcg_status vvcg_batch_upload(vvcg_ctx* ctx, const vvcg_batch* batch);
 vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t stage_mask);
+/* vvcg_batch_run replayed from a CUDA graph: the first call for a prepared
+ * batch and stage mask captures the stages into a graph (the progress words
+ * of the wavefront are cleared inside it), later calls launch the graph.
+ * vvcg_batch_prepare drops the graph. Same results as vvcg_batch_run. */
+vvcg_status vvcg_batch_run_graph(vvcg_ctx* ctx, uint32_t stage_mask);
 vvcg_status vvcg_batch_sync(vvcg_ctx* ctx);
 vvcg_status vvcg_batch_download(vvcg_ctx* ctx, const vvcg_plane_out* out);
 /* Device address and stride (samples) of one reconstructed plane. */

@@ -162,6 +162,7 @@ def lib():
             getattr(L, n).argtypes = [vp, vp]
         L.vvcg_decode_batch.argtypes = [vp, vp, vp]
         L.vvcg_batch_run.argtypes = [vp, u32]
+        L.vvcg_batch_run_graph.argtypes = [vp, u32]
         L.vvcg_batch_sync.argtypes = [vp]
         L.vvcg_batch_download.argtypes = [vp, vp]
         L.vvcg_batch_plane.argtypes = [vp, u32, u32, C.POINTER(vp), C.POINTER(u32)]
@@ -294,8 +295,10 @@ class Context:
     def upload(self, batch: Batch):
         self._check(self._L.vvcg_batch_upload(self._h, C.byref(batch.as_struct())))
 
-    def run(self, stages: int = STAGE_ALL):
-        self._check(self._L.vvcg_batch_run(self._h, stages))
+    def run(self, stages: int = STAGE_ALL, graph: bool = False):
+        """Run the prepared batch's stages (graph=True: replay a captured CUDA graph)."""
+        fn = self._L.vvcg_batch_run_graph if graph else self._L.vvcg_batch_run
+        self._check(fn(self._h, stages))
 
     def sync(self):
         self._check(self._L.vvcg_batch_sync(self._h))

@@ -89,6 +89,12 @@ struct vvcg_ctx {
   DevBuf d_tu_recs, d_tu_idx;
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   uint64_t flags_count = 0;
+  int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
+  // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint32_t graph_mask = 0;
+  uint32_t graph_launches = 0;
 };
 
 namespace {
@@ -301,6 +307,12 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     delete ctx;
     return VVCG_UNAVAILABLE;
   }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->recon_per_sm, k_recon_rows, kWarpsPerCta * 32,
+                                                    kWarpsPerCta * sizeof(WaveWs)) != cudaSuccess) {
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return VVCG_UNAVAILABLE;
+  }
   if (upload_tables(ctx) != VVCG_OK) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -321,6 +333,8 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
@@ -343,6 +357,11 @@ uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx) { return ctx ? ctx->launches 
 vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   if (!ctx) return VVCG_INVALID_INPUT;
   ctx->prepared = false;
+  // a captured graph holds this batch's buffers and launch shapes
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->graph_exec = nullptr;
+  ctx->graph = nullptr;
   if (!b || !b->pics || b->num_pics == 0) return fail(ctx, VVCG_INVALID_INPUT, "empty batch");
   if (b->num_cus && !b->cus) return fail(ctx, VVCG_INVALID_INPUT, "missing CU records");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -563,13 +582,24 @@ vvcg_status vvcg_batch_upload(vvcg_ctx* ctx, const vvcg_batch* b) {
   return VVCG_OK;
 }
 
-vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
-  if (!ctx) return VVCG_INVALID_INPUT;
-  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+}  // extern "C"
+
+namespace {
+
+// Epoch of graph replays: the graph clears the progress words itself, and
+// direct runs never use this value.
+constexpr uint32_t kGraphEpoch = 0xFFFFFFFFu;
+
+// Enqueues the stages of `mask` for the prepared batch on the context's
+// stream. `epoch` tags the wavefront's progress words; with `clear_flags` the
+// words are zeroed first (graph replays). Counts the launches in *launches.
+vvcg_status enqueue_run(vvcg_ctx* ctx, uint32_t mask, uint32_t epoch, bool clear_flags, uint32_t* launches) {
   uint32_t* ctrl = (uint32_t*)ctx->d_ctrl.p;
   CK(cudaMemsetAsync(ctrl, 0, 2 * sizeof(uint32_t), ctx->stream), "memset");
+  if ((mask & VVCG_STAGE_RECON) && clear_flags)
+    CK(cudaMemsetAsync(ctx->flags.p, 0, ctx->flags_count * kRowFlagStride * sizeof(uint64_t), ctx->stream),
+       "memset flags");
   if (mask & VVCG_STAGE_RECON) {
-    ctx->epoch++;
     // residuals of every coded TB (no dependencies), into the scratch planes
     uint32_t max_cus = 0;
     for (auto& P : ctx->pics) max_cus = std::max<uint32_t>(max_cus, (uint32_t)(P.grid_w * P.grid_h));
@@ -577,21 +607,16 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
                  ctx->stream>>>((const DevPic*)ctx->d_pics.p, (const int16_t*)ctx->d_levels.p,
                                 ctx->num_levels, ctrl + 1);
     CK(cudaGetLastError(), "residual launch");
-    ctx->launches++;
+    (*launches)++;
     // prediction + reconstruction in CTU wavefront order
     const uint32_t n = (uint32_t)ctx->items.size();
-    int per_sm = 0;
     const size_t wave_smem = kWarpsPerCta * sizeof(WaveWs);
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recon_rows, kWarpsPerCta * 32,
-                                                     wave_smem),
-       "occupancy");
-    const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, per_sm) * kWarpsPerCta;
+    const uint32_t warps = (uint32_t)ctx->num_sms * std::max(1, ctx->recon_per_sm) * kWarpsPerCta;
     const uint32_t grid = (std::min<uint32_t>(n, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
     k_recon_rows<<<grid, kWarpsPerCta * 32, wave_smem, ctx->stream>>>(
-        (const DevPic*)ctx->d_pics.p, (const RowItem*)ctx->d_items.p, n, ctrl, ctx->epoch,
-        ctx->spin_limit, ctrl + 1);
+        (const DevPic*)ctx->d_pics.p, (const RowItem*)ctx->d_items.p, n, ctrl, epoch, ctx->spin_limit, ctrl + 1);
     CK(cudaGetLastError(), "recon launch");
-    ctx->launches++;
+    (*launches)++;
   }
   if (mask & VVCG_STAGE_DEBLOCK) {
     for (int k = 0; k < 4; k++) {
@@ -606,7 +631,7 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
       if (k == 2) k_deblock_chroma<true><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
       if (k == 3) k_deblock_chroma<false><<<grid, 128, 0, ctx->stream>>>(d, (int)v.size());
       CK(cudaGetLastError(), "deblock launch");
-      ctx->launches++;
+      (*launches)++;
     }
   }
   if ((mask & VVCG_STAGE_SAO) && !ctx->sao.empty()) {
@@ -620,7 +645,7 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     k_sao<<<dim3((unsigned)((items + 7) / 8), (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>(
         (const SaoPass*)ctx->d_sao.p, ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
-    ctx->launches++;
+    (*launches)++;
   }
   if ((mask & VVCG_STAGE_ALF) && !ctx->alf.empty()) {
     uint32_t gx = 0, gy = 0;
@@ -631,8 +656,61 @@ vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
     k_alf_luma<<<dim3(gx, gy, (unsigned)ctx->alf.size()), 256, 0, ctx->stream>>>(
         (const AlfPass*)ctx->d_alf.p, ctrl + 1);
     CK(cudaGetLastError(), "alf launch");
-    ctx->launches++;
+    (*launches)++;
   }
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vvcg_status vvcg_batch_run(vvcg_ctx* ctx, uint32_t mask) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+  bool clear = false;
+  if (mask & VVCG_STAGE_RECON) {
+    if (++ctx->epoch == kGraphEpoch) {  // never reuse the graph's tag
+      ctx->epoch = 1;
+      clear = true;
+    }
+  }
+  uint32_t n = 0;
+  vvcg_status st = enqueue_run(ctx, mask, ctx->epoch, clear, &n);
+  ctx->launches += n;
+  return st;
+}
+
+vvcg_status vvcg_batch_run_graph(vvcg_ctx* ctx, uint32_t mask) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
+  if (!ctx->graph_exec || ctx->graph_mask != mask) {
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    ctx->graph_exec = nullptr;
+    ctx->graph = nullptr;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    uint32_t n = 0;
+    vvcg_status st = enqueue_run(ctx, mask, kGraphEpoch, true, &n);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (st != VVCG_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "end capture");
+    e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return cuda_fail(ctx, e, "graph instantiate");
+    }
+    ctx->graph = g;
+    ctx->graph_mask = mask;
+    ctx->graph_launches = n;
+  }
+  CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream), "graph launch");
+  ctx->launches += ctx->graph_launches;
   return VVCG_OK;
 }
 

@@ -232,3 +232,27 @@ def test_fixed_filter_alf_abort_matches_the_reference(ctx, pkg, orc):
     assert ref[0][0] == -3
     with pytest.raises(pkg.InvalidInput):
         ctx.decode_batch(pkg.Batch(pics, cus, levels, ctus))
+
+
+def test_graph_replay_equals_direct_runs(ctx, pkg, orc):
+    """vvcg_batch_run_graph: captured once, replayed; interleaved with direct
+    runs, every run reconstructs and filters the same pictures."""
+    from rustmpeg_next_b200 import synth
+
+    pics, cus, levels, ctus, aps = synth.random_records(SPECS[:4], seed=21,
+                                                        tools=pkg.TOOL_DEBLOCK | pkg.TOOL_SAO | pkg.TOOL_ALF,
+                                                        alf_aps=True)
+    batch = pkg.Batch(pics, cus, levels, ctus, aps)
+    want = ctx.decode_batch(batch)
+    ctx.prepare(batch)
+    ctx.upload(batch)
+    for graph in (True, True, False, True, False):
+        n0 = ctx.kernel_launches
+        ctx.run(pkg.STAGE_ALL, graph=graph)
+        ctx.sync()
+        assert ctx.kernel_launches > n0
+        got = ctx.download(batch.output_planes())
+        for a, b in zip(want, got):
+            for c in range(3):
+                if a[c] is not None:
+                    assert (a[c] == b[c]).all(), f"graph={graph}"
