@@ -184,6 +184,26 @@ uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx);
  * (slice.rs:4834-4988 and :4990-5072). */
 vvcg_status vvcg_decode_batch(vvcg_ctx* ctx, const vvcg_batch* batch, const vvcg_plane_out* out);
 
+/* vvcg_decode_batch without the final wait: uploads, kernels and the copies
+ * into `out` are queued on the context's stream and the call returns;
+ * vvcg_batch_sync waits for them and reports the batch's status. The next
+ * call on the same context first waits for the previous batch, so a caller
+ * that streams batches alternates two contexts: one batch's download then
+ * overlaps the next batch's upload and kernels. Host buffers (records,
+ * levels, `out`) must be pinned for the copies to be asynchronous and must
+ * stay valid until vvcg_batch_sync returns. */
+vvcg_status vvcg_decode_batch_async(vvcg_ctx* ctx, const vvcg_batch* batch, const vvcg_plane_out* out);
+
+/* vvcg_decode_batch with the host copies overlapped: the batch is split into
+ * chunks of chunk_pictures pictures, processed round robin on num_lanes
+ * internal sub-contexts (own streams and device arenas; 0 = 3), so that one
+ * chunk's upload and another's download run while a third is reconstructed.
+ * Host buffers should be pinned for the copies to overlap. The caller's
+ * buffers must stay valid until the call returns; results equal
+ * vvcg_decode_batch's. chunk_pictures 0 or >= num_pics is vvcg_decode_batch. */
+vvcg_status vvcg_decode_batch_pipelined(vvcg_ctx* ctx, const vvcg_batch* batch, const vvcg_plane_out* out,
+                                        uint32_t chunk_pictures, uint32_t num_lanes);
+
 /* Split form of vvcg_decode_batch, for callers that keep pictures on the GPU:
  * prepare (validate, schedule, size the device arena), upload (records and
  * levels to the device), run (kernels only, asynchronous on the stream),

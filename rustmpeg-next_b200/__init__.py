@@ -161,6 +161,8 @@ def lib():
         for n in ("vvcg_batch_prepare", "vvcg_batch_upload"):
             getattr(L, n).argtypes = [vp, vp]
         L.vvcg_decode_batch.argtypes = [vp, vp, vp]
+        L.vvcg_decode_batch_pipelined.argtypes = [vp, vp, vp, u32, u32]
+        L.vvcg_decode_batch_async.argtypes = [vp, vp, vp]
         L.vvcg_batch_run.argtypes = [vp, u32]
         L.vvcg_batch_run_graph.argtypes = [vp, u32]
         L.vvcg_batch_sync.argtypes = [vp]
@@ -286,6 +288,23 @@ class Context:
         po = self._plane_outs(outs)
         self._keep = (batch, outs, po)
         self._check(self._L.vvcg_decode_batch(self._h, C.byref(batch.as_struct()), po))
+        return outs
+
+    def decode_batch_async(self, batch: Batch, outs):
+        """decode_batch without the wait: sync() waits and reports the status.
+        `batch` and `outs` (pinned host memory) must stay alive until then."""
+        po = self._plane_outs(outs)
+        self._keep_async = (batch, outs, po, batch.as_struct())
+        self._check(self._L.vvcg_decode_batch_async(self._h, C.byref(self._keep_async[3]), po))
+        return outs
+
+    def decode_batch_pipelined(self, batch: Batch, outs=None, chunk_pictures: int = 32, lanes: int = 3):
+        """decode_batch with host copies overlapped over picture chunks."""
+        outs = outs if outs is not None else batch.output_planes()
+        po = self._plane_outs(outs)
+        self._keep = (batch, outs, po)
+        self._check(self._L.vvcg_decode_batch_pipelined(self._h, C.byref(batch.as_struct()), po,
+                                                        chunk_pictures, lanes))
         return outs
 
     def prepare(self, batch: Batch):

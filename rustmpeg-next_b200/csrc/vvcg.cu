@@ -53,6 +53,29 @@ struct DevBuf {
   }
 };
 
+// Grow-only pinned host buffer (staging for asynchronous uploads). Grow it
+// only when no copy from it is in flight.
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t reserve(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(bytes, (size_t)4096);
+    want += want / 4;
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
 struct PicLayout {
   uint64_t plane_off[3], scratch_off[3];  // in samples within the plane arena
   int32_t stride[3], pw[3], ph[3];
@@ -95,6 +118,12 @@ struct vvcg_ctx {
   cudaGraphExec_t graph_exec = nullptr;
   uint32_t graph_mask = 0;
   uint32_t graph_launches = 0;
+  // sub-contexts (own streams and arenas) of vvcg_decode_batch_pipelined
+  std::vector<vvcg_ctx*> lanes;
+  // pinned staging of prepare's uploads (cursor in bytes), and of the
+  // rebased records of a pipelined chunk
+  PinnedBuf stage, stage_cus;
+  size_t stage_used = 0;
 };
 
 namespace {
@@ -238,14 +267,24 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
 }
 
 uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+bool encode_geometry(const vvcg_pic_desc& d, uint32_t* cus, uint64_t* levels);  // defined with the encoder
 int ilog2_host(int v) { return __builtin_ctz((unsigned)v); }
 
+// Copies v to the device through the pinned staging buffer when it has room
+// (an asynchronous copy that does not hold the host), else directly.
 template <typename T>
 vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
   if (v.empty()) return VVCG_OK;
-  CK(buf.reserve(sizeof(T) * v.size()), "cudaMalloc");
-  CK(cudaMemcpyAsync(buf.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, ctx->stream),
-     "upload");
+  const size_t bytes = sizeof(T) * v.size();
+  CK(buf.reserve(bytes), "cudaMalloc");
+  const void* src = v.data();
+  if (ctx->stage.p && ctx->stage_used + bytes <= ctx->stage.cap) {
+    void* dst = (char*)ctx->stage.p + ctx->stage_used;
+    memcpy(dst, v.data(), bytes);
+    ctx->stage_used += (bytes + 255) & ~(size_t)255;
+    src = dst;
+  }
+  CK(cudaMemcpyAsync(buf.p, src, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload");
   return VVCG_OK;
 }
 
@@ -335,6 +374,9 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  for (vvcg_ctx* l : ctx->lanes) vvcg_ctx_destroy(l);
+  ctx->stage.release();
+  ctx->stage_cus.release();
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
@@ -352,7 +394,12 @@ vvcg_status vvcg_set_stream(vvcg_ctx* ctx, void* stream) {
   return VVCG_OK;
 }
 
-uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+uint64_t vvcg_kernel_launches(const vvcg_ctx* ctx) {
+  if (!ctx) return 0;
+  uint64_t n = ctx->launches;
+  for (const vvcg_ctx* l : ctx->lanes) n += l->launches;
+  return n;
+}
 
 vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   if (!ctx) return VVCG_INVALID_INPUT;
@@ -365,6 +412,9 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   if (!b || !b->pics || b->num_pics == 0) return fail(ctx, VVCG_INVALID_INPUT, "empty batch");
   if (b->num_cus && !b->cus) return fail(ctx, VVCG_INVALID_INPUT, "missing CU records");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  // earlier work of this context may still read the staging buffer or the arena
+  CK(cudaStreamSynchronize(ctx->stream), "prepare");
+  ctx->stage_used = 0;
   const uint32_t np = b->num_pics;
   ctx->num_pics = np;
   ctx->layout.assign(np, PicLayout{});
@@ -552,6 +602,14 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
       }
     }
   }
+  // pinned staging for the uploads below (and one more picture table, which
+  // the encoder uploads again)
+  {
+    size_t need = 2 * (sizeof(DevPic) * ctx->pics.size() + 256) + sizeof(RowItem) * ctx->items.size() + 256 +
+                  sizeof(SaoPass) * ctx->sao.size() + 256 + sizeof(AlfPass) * ctx->alf.size() + 256;
+    for (int k = 0; k < 4; k++) need += sizeof(DbfPass) * ctx->dbf[k].size() + 256;
+    CK(ctx->stage.reserve(need), "cudaHostAlloc");
+  }
   vvcg_status st;
   if ((st = upload_vec(ctx, ctx->d_pics, ctx->pics)) != VVCG_OK) return st;
   if ((st = upload_vec(ctx, ctx->d_items, ctx->items)) != VVCG_OK) return st;
@@ -559,7 +617,9 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     if ((st = upload_vec(ctx, ctx->d_dbf[k], ctx->dbf[k])) != VVCG_OK) return st;
   if ((st = upload_vec(ctx, ctx->d_sao, ctx->sao)) != VVCG_OK) return st;
   if ((st = upload_vec(ctx, ctx->d_alf, ctx->alf)) != VVCG_OK) return st;
-  CK(cudaStreamSynchronize(ctx->stream), "prepare");
+  // no wait here: the copies read pinned staging (or pageable memory the
+  // driver has already staged), and the next prepare waits for the stream
+  // before it reuses the staging buffer
   ctx->prepared = true;
   return VVCG_OK;
 }
@@ -731,6 +791,32 @@ vvcg_status vvcg_batch_sync(vvcg_ctx* ctx) {
   return VVCG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The copies of vvcg_batch_download, without waiting for them.
+vvcg_status enqueue_download(vvcg_ctx* ctx, const vvcg_plane_out* out) {
+  for (uint32_t i = 0; i < ctx->num_pics; i++) {
+    const PicLayout& L = ctx->layout[i];
+    const DevPic& P = ctx->pics[i];
+    for (int c = 0; c < (P.cf ? 3 : 1); c++) {
+      const vvcg_plane_out& o = out[i * 3 + c];
+      if (!o.data) continue;
+      if (o.stride < (uint32_t)L.vis_w[c]) return fail(ctx, VVCG_INVALID_INPUT, "output stride too small");
+      const uint16_t* src = L.final_in_scratch[c] ? P.scratch[c] : P.plane[c];
+      CK(cudaMemcpy2DAsync(o.data, (size_t)o.stride * 2, src, (size_t)L.stride[c] * 2, (size_t)L.vis_w[c] * 2,
+                           L.vis_h[c], cudaMemcpyDeviceToHost, ctx->stream),
+         "download");
+    }
+  }
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 vvcg_status vvcg_batch_download(vvcg_ctx* ctx, const vvcg_plane_out* out) {
   if (!ctx || !out) return VVCG_INVALID_INPUT;
   if (!ctx->prepared) return fail(ctx, VVCG_INVALID_INPUT, "batch not prepared");
@@ -768,6 +854,115 @@ vvcg_status vvcg_decode_batch(vvcg_ctx* ctx, const vvcg_batch* b, const vvcg_pla
   if ((st = vvcg_batch_run(ctx, VVCG_STAGE_ALL)) != VVCG_OK) return st;
   if ((st = vvcg_batch_sync(ctx)) != VVCG_OK) return st;
   return vvcg_batch_download(ctx, out);
+}
+
+vvcg_status vvcg_decode_batch_async(vvcg_ctx* ctx, const vvcg_batch* b, const vvcg_plane_out* out) {
+  vvcg_status st;
+  if ((st = vvcg_batch_prepare(ctx, b)) != VVCG_OK) return st;  // waits for this context's previous work
+  if ((st = vvcg_batch_upload(ctx, b)) != VVCG_OK) return st;
+  if ((st = vvcg_batch_run(ctx, VVCG_STAGE_ALL)) != VVCG_OK) return st;
+  if (!out) return fail(ctx, VVCG_INVALID_INPUT, "missing output planes");
+  return enqueue_download(ctx, out);
+}
+
+vvcg_status vvcg_decode_batch_pipelined(vvcg_ctx* ctx, const vvcg_batch* b, const vvcg_plane_out* out,
+                                        uint32_t chunk_pictures, uint32_t num_lanes) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!b || !b->pics || !b->num_pics || !out) return fail(ctx, VVCG_INVALID_INPUT, "empty batch");
+  if (!chunk_pictures || chunk_pictures >= b->num_pics) return vvcg_decode_batch(ctx, b, out);
+  if (b->num_cus && !b->cus) return fail(ctx, VVCG_INVALID_INPUT, "missing CU records");
+  num_lanes = std::max<uint32_t>(1, std::min<uint32_t>(num_lanes ? num_lanes : 3, 8));
+  while (ctx->lanes.size() < num_lanes) {
+    vvcg_config cfg{ctx->device, 0, 0, ctx->spin_limit, 0};
+    vvcg_ctx* l = nullptr;
+    vvcg_status st = vvcg_ctx_create(&cfg, &l);
+    if (st != VVCG_OK) return fail(ctx, st, "lane context could not be created");
+    ctx->lanes.push_back(l);
+  }
+  // Each chunk is a batch of its own: its pictures' records, CTU records and
+  // the range of the level pool they index, with the offsets rebased.
+  const uint32_t nchunks = (b->num_pics + chunk_pictures - 1) / chunk_pictures;
+  std::vector<std::vector<vvcg_pic_desc>> cpics(nchunks);
+  std::vector<uint64_t> c_cu0(nchunks), c_lv0(nchunks);
+  std::vector<vvcg_batch> cb(nchunks);
+  for (uint32_t k = 0; k < nchunks; k++) {
+    const uint32_t p0 = k * chunk_pictures, p1 = std::min(b->num_pics, p0 + chunk_pictures);
+    uint64_t cu0 = UINT64_MAX, cu1 = 0, ct0 = UINT64_MAX, ct1 = 0, lv0 = UINT64_MAX, lv1 = 0;
+    for (uint32_t i = p0; i < p1; i++) {
+      const vvcg_pic_desc& d = b->pics[i];
+      uint32_t ncu;
+      uint64_t nl;
+      if (!encode_geometry(d, &ncu, &nl))
+        return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU size or coded size outside the frame path", i);
+      const uint32_t ctu = 1u << d.ctu_log2, tb = std::min<uint32_t>(ctu, 32);
+      const uint64_t nctu = (uint64_t)(d.width / ctu) * (d.height / ctu);
+      if ((uint64_t)d.cu_offset + ncu > b->num_cus)
+        return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CU records out of range", i);
+      cu0 = std::min<uint64_t>(cu0, d.cu_offset);
+      cu1 = std::max<uint64_t>(cu1, (uint64_t)d.cu_offset + ncu);
+      if (b->ctus) {
+        ct0 = std::min<uint64_t>(ct0, d.ctu_offset);
+        ct1 = std::max<uint64_t>(ct1, (uint64_t)d.ctu_offset + nctu);
+      }
+      const int cf = d.chroma_format, sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
+      const uint64_t nch = cf ? (uint64_t)std::max<int>(tb / sw, 2) * std::max<int>(tb / sh, 2) : 0;
+      const uint64_t nlc[3] = {(uint64_t)tb * tb, nch, nch};
+      for (uint32_t c = 0; c < ncu; c++) {
+        const vvcg_cu_rec& r = b->cus[d.cu_offset + c];
+        for (int q = 0; q < (cf ? 3 : 1); q++)
+          if (((r.cbf >> q) & 1) && r.level_off[q] >= 0) {
+            lv0 = std::min<uint64_t>(lv0, (uint64_t)r.level_off[q]);
+            lv1 = std::max<uint64_t>(lv1, (uint64_t)r.level_off[q] + nlc[q]);
+          }
+      }
+    }
+    if (lv0 == UINT64_MAX) lv0 = lv1 = 0;
+    if (ct0 == UINT64_MAX) ct0 = ct1 = 0;
+    if (lv1 > b->num_levels) return fail(ctx, VVCG_INVALID_INPUT, "chunk %u: level offsets out of range", k);
+    cpics[k].assign(b->pics + p0, b->pics + p1);
+    for (auto& d : cpics[k]) {
+      d.cu_offset -= (uint32_t)cu0;
+      d.ctu_offset -= (uint32_t)ct0;
+    }
+    c_cu0[k] = cu0;
+    c_lv0[k] = lv0;
+    cb[k] = vvcg_batch{cpics[k].data(), p1 - p0, (uint32_t)(cu1 - cu0), nullptr,
+                       b->levels ? b->levels + lv0 : nullptr, lv1 - lv0,
+                       b->ctus ? b->ctus + ct0 : nullptr, (uint32_t)(ct1 - ct0), b->num_aps, b->aps};
+  }
+  // round robin over the lanes: a lane takes its next chunk once its previous
+  // one has finished, while the other lanes' copies and kernels run
+  vvcg_status st = VVCG_OK;
+  for (uint32_t k = 0; k < nchunks && st == VVCG_OK; k++) {
+    vvcg_ctx* l = ctx->lanes[k % num_lanes];
+    // the lane's previous chunk must be done with the lane's pinned records
+    CK(cudaSetDevice(l->device), "cudaSetDevice");
+    CK(cudaStreamSynchronize(l->stream), "lane");
+    CK(l->stage_cus.reserve(std::max<size_t>(1, cb[k].num_cus) * sizeof(vvcg_cu_rec)), "cudaHostAlloc");
+    vvcg_cu_rec* rc = (vvcg_cu_rec*)l->stage_cus.p;
+    const uint64_t lv0 = c_lv0[k];
+    for (uint32_t i = 0; i < cb[k].num_cus; i++) {
+      vvcg_cu_rec r = b->cus[c_cu0[k] + i];
+      for (int q = 0; q < 3; q++)
+        if (r.level_off[q] >= 0 && (uint64_t)r.level_off[q] >= lv0) r.level_off[q] -= (int32_t)lv0;
+      rc[i] = r;
+    }
+    cb[k].cus = rc;
+    if ((st = vvcg_batch_prepare(l, &cb[k])) != VVCG_OK) break;
+    if ((st = vvcg_batch_upload(l, &cb[k])) != VVCG_OK) break;
+    if ((st = vvcg_batch_run(l, VVCG_STAGE_ALL)) != VVCG_OK) break;
+    st = enqueue_download(l, out + (size_t)k * chunk_pictures * 3);
+  }
+  for (uint32_t i = 0; i < num_lanes; i++) {
+    vvcg_status s2 = vvcg_batch_sync(ctx->lanes[i]);
+    if (st == VVCG_OK && s2 != VVCG_OK) st = s2;
+  }
+  if (st != VVCG_OK) {
+    for (vvcg_ctx* l : ctx->lanes)
+      if (!l->err.empty()) return fail(ctx, st, "%s", l->err.c_str());
+    return st;
+  }
+  return VVCG_OK;
 }
 
 static vvcg_status mc_common(vvcg_ctx* ctx, const uint16_t* ref, uint32_t w, uint32_t h,

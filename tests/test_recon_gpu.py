@@ -256,3 +256,68 @@ def test_graph_replay_equals_direct_runs(ctx, pkg, orc):
             for c in range(3):
                 if a[c] is not None:
                     assert (a[c] == b[c]).all(), f"graph={graph}"
+
+
+@pytest.mark.parametrize("chunk,lanes", [(1, 2), (2, 3), (3, 1)])
+def test_pipelined_decode_equals_whole_batch(ctx, pkg, orc, chunk, lanes):
+    """vvcg_decode_batch_pipelined: chunks of pictures on internal lanes give
+    the pictures vvcg_decode_batch gives, whatever the chunking, also when a
+    picture's levels are not in picture order in the pool."""
+    from rustmpeg_next_b200 import synth
+
+    pics, cus, levels, ctus, aps = synth.random_records(SPECS + SPECS[:2], seed=33,
+                                                        tools=pkg.TOOL_DEBLOCK | pkg.TOOL_SAO | pkg.TOOL_ALF,
+                                                        alf_aps=True)
+    # move picture 1's levels to the end of the pool
+    p1 = pics[1]
+    tb = min(1 << int(p1["ctu_log2"]), 32)
+    n1 = (int(p1["width"]) // tb) * (int(p1["height"]) // tb)
+    sel = cus[int(p1["cu_offset"]):int(p1["cu_offset"]) + n1].copy()
+    extra, at = [], len(levels)
+    for k in range(n1):
+        for c in range(3):
+            if sel["cbf"][k] >> c & 1 and sel["level_off"][k, c] >= 0:
+                o = int(sel["level_off"][k, c])
+                n = tb * tb if c == 0 else max(tb // 2, 2) ** 2
+                sel["level_off"][k, c] = at
+                extra.append(levels[o:o + n].copy())
+                at += n
+    cus[int(p1["cu_offset"]):int(p1["cu_offset"]) + n1] = sel
+    levels = np.concatenate([levels] + extra)
+    batch = pkg.Batch(pics, cus, levels, ctus, aps)
+    want = ctx.decode_batch(batch)
+    got = ctx.decode_batch_pipelined(batch, chunk_pictures=chunk, lanes=lanes)
+    for i, (a, b) in enumerate(zip(want, got)):
+        for c in range(3):
+            if a[c] is not None:
+                assert (a[c] == b[c]).all(), f"picture {i} plane {c}"
+
+
+def test_async_decode_on_two_contexts_equals_decode_batch(ctx, pkg, orc):
+    """vvcg_decode_batch_async + vvcg_batch_sync, alternating two contexts as a
+    streaming caller does, gives vvcg_decode_batch's pictures for every batch."""
+    import torch
+    from rustmpeg_next_b200 import synth
+
+    batches = []
+    for seed in (41, 42, 43):
+        pics, cus, levels, ctus, aps = synth.random_records(SPECS[:4], seed=seed,
+                                                            tools=pkg.TOOL_DEBLOCK | pkg.TOOL_SAO | pkg.TOOL_ALF,
+                                                            alf_aps=True)
+        pin = lambda a: torch.from_numpy(a.view(np.uint8)).pin_memory().numpy().view(a.dtype)  # noqa: E731
+        batches.append(pkg.Batch(pics, pin(cus), pin(levels), pin(ctus), pin(aps)))
+    want = [ctx.decode_batch(b) for b in batches]
+    with pkg.Context(0) as c1, pkg.Context(0) as c2:
+        lanes = [c1, c2]
+        outs = [b.output_planes() for b in batches]
+        for i, b in enumerate(batches):
+            if i >= 2:
+                lanes[i % 2].sync()
+            lanes[i % 2].decode_batch_async(b, outs[i])
+        c1.sync()
+        c2.sync()
+    for i in range(len(batches)):
+        for a, g in zip(want[i], outs[i]):
+            for c in range(3):
+                if a[c] is not None:
+                    assert (a[c] == g[c]).all(), f"batch {i}"
