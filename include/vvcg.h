@@ -445,6 +445,53 @@ typedef struct vvcg_cres_rec {
 vvcg_status vvcg_chroma_residuals_dev(vvcg_ctx* ctx, const vvcg_cres_rec* recs, uint32_t num, int16_t* res,
                                       uint64_t count);
 
+/* ---- matrix-based intra prediction (function level, batched) ------------- */
+
+#define VVCG_MIP_SEARCH 0xFFu /* vvcg_mip_req.mode: search every (transposed, mode) */
+
+typedef struct vvcg_mip_req {
+  uint8_t log2_w, log2_h; /* 2..6: blocks 4x4 .. 64x64 */
+  uint8_t bit_depth;      /* 8..12 */
+  uint8_t mode;           /* MIP mode (taken modulo the size class's mode count), or VVCG_MIP_SEARCH */
+  uint8_t transposed;     /* intra_mip_transposed_flag (ignored when searching) */
+  uint8_t reserved[3];
+  uint32_t ref_off;       /* first of the w above then h left reference samples (int16) in `refs` */
+  uint32_t out_off;       /* first of the w*h prediction samples (int16, raster) in `pred`; the
+                             source block of a search sits at the same offset in `src` */
+} vvcg_mip_req; /* 16 bytes */
+
+typedef struct vvcg_mip_res {
+  uint64_t sad;        /* SAD of the chosen candidate against the source */
+  uint8_t mode, transposed;
+  uint8_t reserved[6];
+} vvcg_mip_res; /* 16 bytes */
+
+/* MIP predictions of a batch of blocks from their reference samples; with
+ * VVCG_MIP_SEARCH, the (transposed, mode) of least SAD against `src` (a later
+ * candidate wins only when strictly lower; transposed 0 first), its SAD in
+ * `res` and its prediction in `pred`. Replaces: predict_mip_16 /
+ * predict_mip_bd (crates/rustmpeg-video/src/vvc/predict.rs:4109, :2461-2611)
+ * and choose_best_mip_mode_16 (predict.rs:4166-4199). `reqs` host memory;
+ * refs, src, pred (int16, counts ref_count / count) and res (device, one per
+ * request, needed only when searching) device memory. */
+vvcg_status vvcg_mip_predict_dev(vvcg_ctx* ctx, const vvcg_mip_req* reqs, uint32_t num_reqs, const int16_t* refs,
+                                 uint64_t ref_count, const int16_t* src, int16_t* pred, uint64_t count,
+                                 vvcg_mip_res* res);
+
+/* ---- general-decoder SAO -------------------------------------------------- */
+
+/* SAO of one plane as the general decoder applies it: every CTU region,
+ * cropped to the visible size, with its vvcg_sao (params: device memory, one
+ * per CTU, ctu_cols per row; ctu_size in this plane's samples). Edge class 3
+ * uses the (-1, 1) / (1, -1) pair and edge neighbours outside the visible
+ * picture leave a sample unchanged. Reads src, writes every sample of dst
+ * (device planes, same stride). Replaces: apply_sao (decode_general.rs:5189)
+ * over apply_sao_region_bounded_16 (filter.rs:1954-2033). */
+vvcg_status vvcg_sao_bounded_16_dev(vvcg_ctx* ctx, const uint16_t* src, uint16_t* dst, uint32_t stride,
+                                    uint32_t width, uint32_t height, uint32_t vis_width, uint32_t vis_height,
+                                    uint8_t bit_depth, uint32_t ctu_size, uint32_t ctu_cols,
+                                    const vvcg_sao* params);
+
 /* ---- plane metrics ---------------------------------------------------------- */
 
 /* Sum of squared errors, sum of absolute differences and sample count of one

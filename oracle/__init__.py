@@ -92,6 +92,11 @@ def _declare(L):
                                    C.POINTER(C.c_uint64), vp, vp, vp]
     L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     L.orc_tu_batch.argtypes = [i, vp, i, vp, vp]
+    L.orc_mip_predict.argtypes = [vp, vp, i, i, i, i, i, vp]
+    L.orc_mip_predict.restype = None
+    L.orc_mip_search.argtypes = [vp, vp, vp, i, i, i, vp, C.POINTER(C.c_uint64)]
+    L.orc_sao_bounded.argtypes = [vp, vp, i, i, i, i, i, i, i, vp, i]
+    L.orc_sao_bounded.restype = None
     L.orc_mc_luma_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, i, vp]
     L.orc_mc_luma_8.restype = None
     L.orc_mc_chroma_420_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, vp]
@@ -508,3 +513,31 @@ def chroma_residuals(recs, res):
     for i in range(len(recs)):
         lib().orc_chroma_residuals(_p(recs[i:i + 1].copy()), _p(out))
     return out
+
+
+def sao_bounded(plane, vis_w, vis_h, bd, ctu, ctu_cols, params):
+    """The general decoder's SAO of one plane (filter.rs:1954-2033 per CTU,
+    decode_general.rs:5189-5223); params: SAO_DTYPE-layout records per CTU."""
+    src = _u16(plane)
+    dst = np.zeros_like(src)
+    prm = np.ascontiguousarray(params).view(np.uint8)
+    lib().orc_sao_bounded(_p(src), _p(dst), src.shape[1], src.shape[0], vis_w, vis_h, bd, ctu, ctu_cols, _p(prm),
+                          prm.size // 6)
+    return dst
+
+
+def mip_predict(above, left, w, h, mode, transposed, bd):
+    """predict_mip_16 (predict.rs:4109 / predict_mip_bd :2461) of one block."""
+    a, l = _i32(above), _i32(left)
+    out = np.zeros(w * h, np.int32)
+    lib().orc_mip_predict(_p(a), _p(l), w, h, mode, int(transposed), bd, _p(out))
+    return out
+
+
+def mip_search(above, left, src, w, h, bd):
+    """choose_best_mip_mode_16 (predict.rs:4166): (mode, transposed, sad, pred)."""
+    a, l, s = _i32(above), _i32(left), _i32(src)
+    out = np.zeros(w * h, np.int32)
+    sad = C.c_uint64(0)
+    r = lib().orc_mip_search(_p(a), _p(l), _p(s), w, h, bd, _p(out), C.byref(sad))
+    return r & 0xFF, r >> 8, sad.value, out

@@ -117,6 +117,9 @@ struct Sao {
 // Returns -1 (without writing) where the reference aborts: see orc_filter.cpp.
 int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w, int h,
                         const Sao& sao);
+// filter.rs:1954-2033 / decode_general.rs:5189-5223: the general decoder's SAO of one plane.
+void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw, int ph, int vis_w, int vis_h,
+                          int bd, int ctu, int ctu_cols, const Sao* params);
 struct AlfAps {
   int num_luma_filters;  // 0 = fixed filters of the class
   bool luma_clip;

@@ -178,3 +178,15 @@ extern "C" void orc_mc_chroma_420_8(const uint8_t* ref, int pw, int ph, int stri
 extern "C" void orc_bi_average_8(const int32_t* p0, const int32_t* p1, int n, int bcw, int32_t* out) {
   orc::weighted_average_bi_8(p0, p1, n, bcw, out);
 }
+
+// params: 6 bytes per CTU (type, band_or_class, offsets[4]) as vvcg_sao
+extern "C" void orc_sao_bounded(const uint16_t* src, uint16_t* dst, int pw, int ph, int vis_w, int vis_h, int bd,
+                                int ctu, int ctu_cols, const uint8_t* params, int n_params) {
+  std::vector<orc::Sao> s(n_params);
+  for (int i = 0; i < n_params; i++) {
+    s[i].type = params[6 * i];
+    s[i].band_pos_or_class = params[6 * i + 1];
+    for (int k = 0; k < 4; k++) s[i].offsets[k] = (int8_t)params[6 * i + 2 + k];
+  }
+  orc::sao_plane_bounded_16(src, dst, pw, pw, ph, vis_w, vis_h, bd, ctu, ctu_cols, s.data());
+}

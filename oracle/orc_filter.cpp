@@ -536,3 +536,52 @@ void apply_alf_luma_plane_16(Plane16& p, const AlfAps& aps) {
 }
 
 }  // namespace orc
+
+namespace orc {
+
+// filter.rs:1954-2033 apply_sao_region_bounded_16, driven per CTU as
+// decode_general.rs:5189-5223 apply_sao does for one plane: CTU regions
+// cropped to the visible size; edge-offset neighbours outside the visible
+// picture leave the sample unchanged. `params` holds one Sao per CTU,
+// ctu_cols per row. Writes dst (a copy of src outside the changed samples).
+void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw, int ph, int vis_w, int vis_h,
+                          int bd, int ctu, int ctu_cols, const Sao* params) {
+  for (int y = 0; y < ph; y++)
+    for (int x = 0; x < pw; x++) dst[y * stride + x] = src[y * stride + x];
+  bd = std::min(12, std::max(8, bd));
+  const int max_val = (1 << bd) - 1, band_shift = bd - 5;
+  const int bw = std::min(vis_w, pw), bh = std::min(vis_h, ph);
+  for (int gy = 0; gy * ctu < vis_h; gy++)
+    for (int gx = 0; gx * ctu < vis_w; gx++) {
+      const Sao& s = params[gy * ctu_cols + gx];
+      const int x0 = gx * ctu, y0 = gy * ctu;
+      const int w_lim = std::min(x0 + std::min(ctu, vis_w - x0), pw), h_lim = std::min(y0 + std::min(ctu, vis_h - y0), ph);
+      if (s.type == 1) {
+        for (int y = y0; y < h_lim; y++)
+          for (int x = x0; x < w_lim; x++) {
+            const int c = src[y * stride + x];
+            const int band = (uint8_t)((uint8_t)(c >> band_shift) - (uint8_t)s.band_pos_or_class) & 31;
+            if (band < 4) dst[y * stride + x] = (uint16_t)std::min(max_val, std::max(0, c + s.offsets[band]));
+          }
+      } else if (s.type == 2) {
+        int dx, dy;
+        switch (s.band_pos_or_class & 3) {
+          case 0: dx = 1; dy = 0; break;
+          case 1: dx = 0; dy = 1; break;
+          case 2: dx = 1; dy = 1; break;
+          default: dx = -1; dy = 1; break;
+        }
+        for (int y = y0; y < h_lim; y++)
+          for (int x = x0; x < w_lim; x++) {
+            const int ax = x - dx, ay = y - dy, bxn = x + dx, byn = y + dy;
+            if (ax < 0 || ay < 0 || ax >= bw || ay >= bh || bxn < 0 || byn < 0 || bxn >= bw || byn >= bh) continue;
+            const int c = src[y * stride + x], a = src[ay * stride + ax], b = src[byn * stride + bxn];
+            const int ei = 2 + ((c > a) - (c < a)) + ((c > b) - (c < b));
+            const int off = ei == 0 ? s.offsets[0] : ei == 1 ? s.offsets[1] : ei == 3 ? s.offsets[2] : ei == 4 ? s.offsets[3] : 0;
+            dst[y * stride + x] = (uint16_t)std::min(max_val, std::max(0, c + off));
+          }
+      }
+    }
+}
+
+}  // namespace orc

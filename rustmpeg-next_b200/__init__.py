@@ -48,6 +48,10 @@ LMCS_TABLES_DTYPE = np.dtype([("bit_depth", "u1"), ("min_bin_idx", "u1"), ("max_
 CRES_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("joint", "i1"),
                        ("flags", "<u4"), ("scale", "<i4"), ("cb_off", "<u4"), ("cr_off", "<u4")])
 CRES_SCALE, CRES_SINGLE = 1, 2
+MIP_REQ_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("mode", "u1"),
+                          ("transposed", "u1"), ("reserved", "u1", (3,)), ("ref_off", "<u4"), ("out_off", "<u4")])
+MIP_RES_DTYPE = np.dtype([("sad", "<u8"), ("mode", "u1"), ("transposed", "u1"), ("reserved", "u1", (6,))])
+MIP_SEARCH = 0xFF
 TXS_REQ_DTYPE = np.dtype([("log2_size", "u1"), ("qp", "u1"), ("mode", "u1"), ("flags", "u1"),
                           ("in_off", "<u4"), ("out_off", "<u4"), ("reserved", "<u4")])
 TXS_RES_DTYPE = np.dtype([("sse", "<u8"), ("mts_idx", "u1"), ("lfnst_idx", "u1"), ("transform_skip", "u1"),
@@ -124,6 +128,7 @@ class _Config(C.Structure):
 assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize == 32
 assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.itemsize == 16
 assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
+assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
@@ -184,6 +189,8 @@ def lib():
         L.vvcg_lmcs_map_plane_16_dev.argtypes = [vp, vp, C.c_int, vp, u32, u32, u32]
         L.vvcg_lmcs_chroma_scales_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, vp, u32, vp]
         L.vvcg_chroma_residuals_dev.argtypes = [vp, vp, u32, vp, u64]
+        L.vvcg_sao_bounded_16_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u8, u32, u32, vp]
+        L.vvcg_mip_predict_dev.argtypes = [vp, vp, u32, vp, u64, vp, vp, u64, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -425,6 +432,28 @@ class Context:
         recs = np.ascontiguousarray(recs, dtype=CRES_DTYPE)
         self._keep = recs
         self._check(self._L.vvcg_chroma_residuals_dev(self._h, _ptr(recs), len(recs), _ptr(res), res.numel()))
+
+    # -- matrix-based intra prediction --
+    def mip_predict(self, reqs, refs, pred, src=None):
+        """MIP_REQ_DTYPE requests (host) over int16 CUDA tensors; returns the
+        MIP_RES_DTYPE results of searching requests (synchronises)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=MIP_REQ_DTYPE)
+        res = torch.zeros(len(reqs) * MIP_RES_DTYPE.itemsize, dtype=torch.uint8, device=refs.device)
+        self._keep = reqs
+        self._check(self._L.vvcg_mip_predict_dev(self._h, _ptr(reqs), len(reqs), _ptr(refs), refs.numel(),
+                                                 _ptr(src), _ptr(pred), pred.numel(), _ptr(res)))
+        torch.cuda.synchronize(refs.device)
+        return res.cpu().numpy().view(MIP_RES_DTYPE)
+
+    # -- general-decoder SAO --
+    def sao_bounded(self, src, dst, vis_w, vis_h, bit_depth, ctu, ctu_cols, params):
+        """src / dst: (H, W) int16 CUDA tensors of 16-bit samples; params: CUDA
+        uint8 tensor of SAO_DTYPE records (one per CTU)."""
+        h, w = src.shape
+        self._check(self._L.vvcg_sao_bounded_16_dev(self._h, _ptr(src), _ptr(dst), src.stride(0), w, h, vis_w, vis_h,
+                                                    bit_depth, ctu, ctu_cols, _ptr(params)))
 
     # -- metrics --
     def plane_metrics(self, ref, dist):

@@ -502,6 +502,52 @@ __global__ void __launch_bounds__(256) k_sao(const SaoPass* __restrict__ passes,
       make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
 }
 
+// SAO of one plane as the general decoder applies it:
+// apply_sao_region_bounded_16 (filter.rs:1954-2033) per CTU, driven by
+// apply_sao (decode_general.rs:5189-5223). CTU regions are cropped to the
+// visible size, edge class 3 pairs (-1, 1) with (1, -1), and a sample whose
+// edge-offset neighbour lies outside the visible picture is unchanged.
+// Thread per sample; dst receives every sample of the plane.
+struct SaoBoundedPass {
+  const uint16_t* src;
+  uint16_t* dst;
+  const vvcg_sao* params;  // one per CTU, ctu_cols per row
+  int32_t stride, w, h, vis_w, vis_h, bd, ctu, ctu_cols;
+};
+
+__global__ void __launch_bounds__(256) k_sao_bounded(SaoBoundedPass S) {
+  const int bd = clampi(S.bd, 8, 12), maxv = (1 << bd) - 1;
+  const int bw = min(S.vis_w, S.w), bh = min(S.vis_h, S.h);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (uint64_t)S.w * S.h;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const int y = (int)(i / S.w), x = (int)(i % S.w);
+    const int c = S.src[(size_t)y * S.stride + x];
+    int out = c;
+    if (x < S.vis_w && y < S.vis_h) {
+      const vvcg_sao sp = S.params[(y / S.ctu) * S.ctu_cols + x / S.ctu];
+      if (sp.type == 1) {
+        const int band = ((uint8_t)((uint8_t)(c >> (bd - 5)) - sp.band_or_class)) & 31;
+        if (band < 4) {
+          const int off = band == 0 ? sp.offsets[0] : band == 1 ? sp.offsets[1] : band == 2 ? sp.offsets[2] : sp.offsets[3];
+          out = clampi(c + off, 0, maxv);
+        }
+      } else if (sp.type == 2) {
+        const int cls = sp.band_or_class & 3;
+        const int dx = cls == 1 ? 0 : (cls == 3 ? -1 : 1), dy = cls == 0 ? 0 : 1;
+        const int ax = x - dx, ay = y - dy, bx = x + dx, by = y + dy;
+        if (!(ax < 0 || ay < 0 || ax >= bw || ay >= bh || bx < 0 || by < 0 || bx >= bw || by >= bh)) {
+          const int a = S.src[(size_t)ay * S.stride + ax], b = S.src[(size_t)by * S.stride + bx];
+          const int ei = 2 + ((c > a) - (c < a)) + ((c > b) - (c < b));
+          const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
+                          : ei == 4 ? sp.offsets[3] : 0;
+          out = clampi(c + off, 0, maxv);
+        }
+      }
+    }
+    S.dst[(size_t)y * S.stride + x] = (uint16_t)out;
+  }
+}
+
 // One luma ALF pass (whole plane, apply_alf_luma_plane_16 of filter.rs:2045-2124).
 struct AlfPass {
   const uint16_t* src;

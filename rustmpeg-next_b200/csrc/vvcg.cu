@@ -17,6 +17,7 @@
 #include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
+#include "mip.cuh"
 #include "recon.cuh"
 #include "tu.cuh"
 #include "txsearch.cuh"
@@ -261,6 +262,9 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
   CK(cudaMemcpyToSymbol(g_lfnst8, kLfnst8x8, sizeof(kLfnst8x8)), "tables");
   CK(cudaMemcpyToSymbol(g_lfnst4, kLfnst4x4, sizeof(kLfnst4x4)), "tables");
   CK(cudaMemcpyToSymbol(g_lfnst_lut, kLfnstLut, sizeof(kLfnstLut)), "tables");
+  CK(cudaMemcpyToSymbol(g_mip4, kMip4x4, sizeof(kMip4x4)), "tables");
+  CK(cudaMemcpyToSymbol(g_mip8, kMip8x8, sizeof(kMip8x8)), "tables");
+  CK(cudaMemcpyToSymbol(g_mip16, kMip16x16, sizeof(kMip16x16)), "tables");
   CK(cudaDeviceSynchronize(), "tables");
   if (ctx->device < 64) g_tables_ready[ctx->device] = true;
   return VVCG_OK;
@@ -1159,6 +1163,62 @@ extern "C" vvcg_status vvcg_chroma_residuals_dev(vvcg_ctx* ctx, const vvcg_cres_
   CK(cudaMemcpyAsync(ctx->d_tu_recs.p, recs, sizeof(vvcg_cres_rec) * num, cudaMemcpyHostToDevice, ctx->stream), "upload");
   k_chroma_residuals<<<(num + 7) / 8, 256, 0, ctx->stream>>>((const vvcg_cres_rec*)ctx->d_tu_recs.p, num, res);
   CK(cudaGetLastError(), "chroma residual launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Matrix-based intra prediction (vvcg_mip_predict_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_mip_predict_dev(vvcg_ctx* ctx, const vvcg_mip_req* reqs, uint32_t num_reqs,
+                                            const int16_t* refs, uint64_t ref_count, const int16_t* src,
+                                            int16_t* pred, uint64_t count, vvcg_mip_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !refs || !pred) return fail(ctx, VVCG_INVALID_INPUT, "missing requests or buffers");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_mip_req& q = reqs[i];
+    if (q.log2_w < 2 || q.log2_w > 6 || q.log2_h < 2 || q.log2_h > 6)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block size outside 4..64", i);
+    if (q.bit_depth < 8 || q.bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "request %u: bit depth", i);
+    const uint64_t w = 1u << q.log2_w, h = 1u << q.log2_h;
+    if (q.ref_off + w + h > ref_count || q.out_off + w * h > count)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: sample range past the buffers", i);
+    if (q.mode == VVCG_MIP_SEARCH && (!src || !res))
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: a search needs the source and results", i);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_mip_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(vvcg_mip_req) * num_reqs, cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  k_mip<<<(num_reqs + kMipWarps - 1) / kMipWarps, kMipWarps * 32, 0, ctx->stream>>>(
+      (const vvcg_mip_req*)ctx->d_tu_recs.p, num_reqs, refs, src, pred, res);
+  CK(cudaGetLastError(), "mip launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// General-decoder SAO of one plane (vvcg_sao_bounded_16_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_sao_bounded_16_dev(vvcg_ctx* ctx, const uint16_t* src, uint16_t* dst, uint32_t stride,
+                                               uint32_t width, uint32_t height, uint32_t vis_width,
+                                               uint32_t vis_height, uint8_t bit_depth, uint32_t ctu_size,
+                                               uint32_t ctu_cols, const vvcg_sao* params) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!width || !height) return VVCG_OK;
+  if (!src || !dst || !params || stride < width || !ctu_size || bit_depth < 8 || bit_depth > 12)
+    return fail(ctx, VVCG_INVALID_INPUT, "invalid SAO arguments");
+  if (vis_width > width || vis_height > height) return fail(ctx, VVCG_INVALID_INPUT, "visible size");
+  if (ctu_cols < (vis_width + ctu_size - 1) / ctu_size) return fail(ctx, VVCG_INVALID_INPUT, "CTU columns");
+  if (src == dst) return fail(ctx, VVCG_INVALID_INPUT, "SAO reads an unfiltered copy: src and dst must differ");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  SaoBoundedPass S{src, dst, params, (int32_t)stride, (int32_t)width, (int32_t)height, (int32_t)vis_width,
+                   (int32_t)vis_height, bit_depth, (int32_t)ctu_size, (int32_t)ctu_cols};
+  const uint64_t n = (uint64_t)width * height;
+  const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->num_sms * 16);
+  k_sao_bounded<<<grid, 256, 0, ctx->stream>>>(S);
+  CK(cudaGetLastError(), "sao launch");
   ctx->launches++;
   return VVCG_OK;
 }
