@@ -478,6 +478,51 @@ vvcg_status vvcg_mip_predict_dev(vvcg_ctx* ctx, const vvcg_mip_req* reqs, uint32
                                  uint64_t ref_count, const int16_t* src, int16_t* pred, uint64_t count,
                                  vvcg_mip_res* res);
 
+/* ---- general-decoder ALF (luma with virtual boundaries, chroma, CCALF) --- */
+
+enum { VVCG_ALF_OFF = 0, VVCG_ALF_FIXED = 1, VVCG_ALF_APS = 2 };
+
+/* One CTU's ALF switches (the general decoder's alf_luma / alf_cb / alf_cr /
+ * ccalf_cb / ccalf_cr per CTU). */
+typedef struct vvcg_alf_ctu {
+  uint8_t luma_mode;     /* VVCG_ALF_OFF / _FIXED / _APS */
+  uint8_t luma_set;      /* fixed filter set 0..15 (VVCG_ALF_FIXED) */
+  uint8_t cb_alt, cr_alt;/* chroma filter alternative, 0xFF = off */
+  uint8_t cc_cb, cc_cr;  /* CCALF filter index + 1, 0 = off */
+  uint8_t reserved[2];
+} vvcg_alf_ctu; /* 8 bytes */
+
+/* ALF parameters of a picture: the luma, chroma and CCALF parts of the APSs
+ * its slice refers to (hls.rs:2699 VvcAlfAps). */
+typedef struct vvcg_alf_params {
+  uint8_t num_luma_filters, luma_clip, num_chroma_filters, chroma_clip;
+  uint8_t num_cc_cb, num_cc_cr, reserved[2];
+  uint8_t coeff_delta_idx[25];
+  uint8_t reserved2[3];
+  int16_t luma_coeff[25][12];
+  uint8_t luma_clip_idx[25][12];
+  int16_t chroma_coeff[8][6];
+  uint8_t chroma_clip_idx[8][6];
+  int16_t cc_cb[4][7];
+  int16_t cc_cr[4][7];
+} vvcg_alf_params;
+
+/* ALF of a 4:2:0 picture as the general decoder applies it: per CTU, the luma
+ * 7x7 filter (fixed set or APS) with the CTU-row virtual boundary 4 rows above
+ * each CTU bottom, the chroma 5x5 filter (virtual boundary 2 rows above), and
+ * CCALF from the unfiltered luma added to the filtered chroma. src / dst are
+ * device planes (Y at width x height, Cb / Cr at half size, the given
+ * strides); CTUs without a switch copy src. ctus (one per CTU of the visible
+ * picture, ctu_cols per row) and params are host memory; a CTU in
+ * VVCG_ALF_APS mode needs num_luma_filters >= 1. Replaces:
+ * apply_alf (decode_general.rs:5225-5345) with alf_luma_block (:5411),
+ * alf_chroma_block (:5568), ccalf_block (:5348) and
+ * derive_alf_class_4x4_vb_16 (filter.rs:1558). */
+vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const src[3], uint16_t* const dst[3],
+                                 const uint32_t stride[3], uint32_t width, uint32_t height, uint32_t vis_width,
+                                 uint32_t vis_height, uint8_t bit_depth, uint32_t ctu_size, uint32_t ctu_cols,
+                                 const vvcg_alf_ctu* ctus, const vvcg_alf_params* params);
+
 /* ---- general-decoder SAO -------------------------------------------------- */
 
 /* SAO of one plane as the general decoder applies it: every CTU region,

@@ -92,6 +92,8 @@ def _declare(L):
                                    C.POINTER(C.c_uint64), vp, vp, vp]
     L.orc_recon_frame.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     L.orc_tu_batch.argtypes = [i, vp, i, vp, vp]
+    L.orc_alf_general.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, i, i, i, i, vp, vp]
+    L.orc_alf_general.restype = None
     L.orc_mip_predict.argtypes = [vp, vp, i, i, i, i, i, vp]
     L.orc_mip_predict.restype = None
     L.orc_mip_search.argtypes = [vp, vp, vp, i, i, i, vp, C.POINTER(C.c_uint64)]
@@ -541,3 +543,15 @@ def mip_search(above, left, src, w, h, bd):
     sad = C.c_uint64(0)
     r = lib().orc_mip_search(_p(a), _p(l), _p(s), w, h, bd, _p(out), C.byref(sad))
     return r & 0xFF, r >> 8, sad.value, out
+
+
+def alf_general(y, u, v, vis_w, vis_h, bd, ctu, ctu_cols, ctus, params):
+    """apply_alf of the general decoder (decode_general.rs:5225) on a 4:2:0
+    picture; ctus / params in the vvcg_alf_ctu / vvcg_alf_params layouts."""
+    y, u, v = _u16(y), _u16(u), _u16(v)
+    dy, du, dv = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
+    c = np.ascontiguousarray(ctus).view(np.uint8)
+    p = np.ascontiguousarray(params).view(np.uint8)
+    lib().orc_alf_general(_p(y), _p(u), _p(v), _p(dy), _p(du), _p(dv), y.shape[1], y.shape[0], vis_w, vis_h, bd,
+                          ctu, ctu_cols, _p(c), _p(p))
+    return dy, du, dv

@@ -48,6 +48,15 @@ LMCS_TABLES_DTYPE = np.dtype([("bit_depth", "u1"), ("min_bin_idx", "u1"), ("max_
 CRES_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("joint", "i1"),
                        ("flags", "<u4"), ("scale", "<i4"), ("cb_off", "<u4"), ("cr_off", "<u4")])
 CRES_SCALE, CRES_SINGLE = 1, 2
+ALF_CTU_DTYPE = np.dtype([("luma_mode", "u1"), ("luma_set", "u1"), ("cb_alt", "u1"), ("cr_alt", "u1"),
+                          ("cc_cb", "u1"), ("cc_cr", "u1"), ("reserved", "u1", (2,))])
+ALF_PARAMS_DTYPE = np.dtype([("num_luma_filters", "u1"), ("luma_clip", "u1"), ("num_chroma_filters", "u1"),
+                             ("chroma_clip", "u1"), ("num_cc_cb", "u1"), ("num_cc_cr", "u1"),
+                             ("reserved", "u1", (2,)), ("coeff_delta_idx", "u1", (25,)), ("reserved2", "u1", (3,)),
+                             ("luma_coeff", "<i2", (25, 12)), ("luma_clip_idx", "u1", (25, 12)),
+                             ("chroma_coeff", "<i2", (8, 6)), ("chroma_clip_idx", "u1", (8, 6)),
+                             ("cc_cb", "<i2", (4, 7)), ("cc_cr", "<i2", (4, 7))])
+ALF_OFF, ALF_FIXED, ALF_APS = 0, 1, 2
 MIP_REQ_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("mode", "u1"),
                           ("transposed", "u1"), ("reserved", "u1", (3,)), ("ref_off", "<u4"), ("out_off", "<u4")])
 MIP_RES_DTYPE = np.dtype([("sad", "<u8"), ("mode", "u1"), ("transposed", "u1"), ("reserved", "u1", (6,))])
@@ -129,6 +138,7 @@ assert C.sizeof(_Batch) == 64 and CU_DTYPE.itemsize == 16 and PIC_DTYPE.itemsize
 assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.itemsize == 16
 assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
 assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
+assert ALF_CTU_DTYPE.itemsize == 8 and ALF_PARAMS_DTYPE.itemsize == 1192
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
@@ -191,6 +201,7 @@ def lib():
         L.vvcg_chroma_residuals_dev.argtypes = [vp, vp, u32, vp, u64]
         L.vvcg_sao_bounded_16_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u8, u32, u32, vp]
         L.vvcg_mip_predict_dev.argtypes = [vp, vp, u32, vp, u64, vp, vp, u64, vp]
+        L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -446,6 +457,20 @@ class Context:
                                                  _ptr(src), _ptr(pred), pred.numel(), _ptr(res)))
         torch.cuda.synchronize(refs.device)
         return res.cpu().numpy().view(MIP_RES_DTYPE)
+
+    # -- general-decoder ALF --
+    def alf_general(self, src, dst, vis_w, vis_h, bit_depth, ctu, ctu_cols, ctus, params):
+        """src / dst: (Y, Cb, Cr) int16 CUDA tensors of a 4:2:0 picture; ctus
+        (ALF_CTU_DTYPE) and params (ALF_PARAMS_DTYPE) host arrays."""
+        ctus = np.ascontiguousarray(ctus, dtype=ALF_CTU_DTYPE)
+        params = np.ascontiguousarray(params, dtype=ALF_PARAMS_DTYPE).reshape(1)
+        sp = (C.c_void_p * 3)(*[t.data_ptr() for t in src])
+        dp = (C.c_void_p * 3)(*[t.data_ptr() for t in dst])
+        st = (C.c_uint32 * 3)(*[t.stride(0) for t in src])
+        h, w = src[0].shape
+        self._keep = (ctus, params)
+        self._check(self._L.vvcg_alf_general_dev(self._h, sp, dp, st, w, h, vis_w, vis_h, bit_depth, ctu, ctu_cols,
+                                                 _ptr(ctus), _ptr(params)))
 
     # -- general-decoder SAO --
     def sao_bounded(self, src, dst, vis_w, vis_h, bit_depth, ctu, ctu_cols, params):

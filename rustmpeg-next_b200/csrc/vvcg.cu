@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/vvcg.h"
+#include "alf_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
 #include "lmcs.cuh"
@@ -112,6 +113,7 @@ struct vvcg_ctx {
   std::vector<uint32_t> tu_idx;
   DevBuf d_tu_recs, d_tu_idx;
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
+  DevBuf d_alfp, d_alfc;  // general-decoder ALF parameters and CTU switches
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -384,7 +386,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
-                    &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs})
+                    &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs, &ctx->d_alfp, &ctx->d_alfc})
     b->release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -1195,6 +1197,80 @@ extern "C" vvcg_status vvcg_mip_predict_dev(vvcg_ctx* ctx, const vvcg_mip_req* r
       (const vvcg_mip_req*)ctx->d_tu_recs.p, num_reqs, refs, src, pred, res);
   CK(cudaGetLastError(), "mip launch");
   ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// General-decoder ALF (vvcg_alf_general_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const src[3], uint16_t* const dst[3],
+                                            const uint32_t stride[3], uint32_t width, uint32_t height,
+                                            uint32_t vis_width, uint32_t vis_height, uint8_t bit_depth,
+                                            uint32_t ctu_size, uint32_t ctu_cols, const vvcg_alf_ctu* ctus,
+                                            const vvcg_alf_params* a) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!src || !dst || !stride || !ctus || !a) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  if (!width || !height) return VVCG_OK;
+  for (int c = 0; c < 3; c++) {
+    const uint32_t pw = c ? (width + 1) / 2 : width;
+    if (!src[c] || !dst[c] || src[c] == dst[c] || stride[c] < pw)
+      return fail(ctx, VVCG_INVALID_INPUT, "plane %d: missing, in place, or stride too small", c);
+  }
+  if (bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "bit depth");
+  if (ctu_size < 16 || ctu_size > 128 || (ctu_size & (ctu_size - 1)))
+    return fail(ctx, VVCG_INVALID_INPUT, "CTU size must be a power of two in 16..128");
+  if (!vis_width || !vis_height || vis_width > width || vis_height > height)
+    return fail(ctx, VVCG_INVALID_INPUT, "visible size");
+  const uint32_t gw = (vis_width + ctu_size - 1) / ctu_size, gh = (vis_height + ctu_size - 1) / ctu_size;
+  if (ctu_cols < gw) return fail(ctx, VVCG_INVALID_INPUT, "CTU columns");
+  if (a->num_luma_filters > 25 || a->num_chroma_filters > 8 || a->num_cc_cb > 4 || a->num_cc_cr > 4)
+    return fail(ctx, VVCG_INVALID_INPUT, "ALF filter counts");
+  for (uint32_t gy = 0; gy < gh; gy++)
+    for (uint32_t gx = 0; gx < gw; gx++) {
+      const vvcg_alf_ctu& m = ctus[gy * ctu_cols + gx];
+      if (m.luma_mode > VVCG_ALF_APS) return fail(ctx, VVCG_INVALID_INPUT, "CTU %u,%u: luma mode", gx, gy);
+      if (m.luma_mode == VVCG_ALF_APS && a->num_luma_filters == 0)
+        return fail(ctx, VVCG_INVALID_INPUT, "CTU %u,%u: ALF APS mode without luma filters", gx, gy);
+    }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const size_t nctu = (size_t)gh * ctu_cols;
+  CK(ctx->d_alfp.reserve(sizeof(vvcg_alf_params)), "cudaMalloc");
+  CK(ctx->d_alfc.reserve(sizeof(vvcg_alf_ctu) * nctu), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_alfp.p, a, sizeof(vvcg_alf_params), cudaMemcpyHostToDevice, ctx->stream), "upload");
+  CK(cudaMemcpyAsync(ctx->d_alfc.p, ctus, sizeof(vvcg_alf_ctu) * nctu, cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  AlfGenPass P;
+  const int pw = (int)width, ph = (int)height, cw = (pw + 1) / 2, ch = (ph + 1) / 2;
+  const int cvw = ((int)vis_width + 1) / 2, cvh = ((int)vis_height + 1) / 2;
+  P.y = AlfGenView{src[0], (int32_t)stride[0], min((int)vis_width, pw), min((int)vis_height, ph)};
+  P.u = AlfGenView{src[1], (int32_t)stride[1], min(cvw, cw), min(cvh, ch)};
+  P.v = AlfGenView{src[2], (int32_t)stride[2], min(cvw, cw), min(cvh, ch)};
+  for (int c = 0; c < 3; c++) {
+    P.dst[c] = dst[c];
+    P.dstride[c] = (int32_t)stride[c];
+  }
+  P.pw = pw;
+  P.ph = ph;
+  P.cw = cw;
+  P.ch = ch;
+  P.vis_w = (int)vis_width;
+  P.vis_h = (int)vis_height;
+  P.cvis_w = cvw;
+  P.cvis_h = cvh;
+  P.bd = bit_depth;
+  P.ctu = (int)ctu_size;
+  P.ctu_cols = (int)ctu_cols;
+  P.ctus = (const vvcg_alf_ctu*)ctx->d_alfc.p;
+  P.a = (const vvcg_alf_params*)ctx->d_alfp.p;
+  const uint64_t nb = (uint64_t)((pw + 3) / 4) * ((ph + 3) / 4);
+  k_alf_general_luma<<<(uint32_t)std::min<uint64_t>((nb + 127) / 128, (uint64_t)ctx->num_sms * 16), 128, 0,
+                       ctx->stream>>>(P);
+  CK(cudaGetLastError(), "alf launch");
+  const uint64_t nc = 2ull * cw * ch;
+  k_alf_general_chroma<<<(uint32_t)std::min<uint64_t>((nc + 255) / 256, (uint64_t)ctx->num_sms * 16), 256, 0,
+                         ctx->stream>>>(P);
+  CK(cudaGetLastError(), "alf launch");
+  ctx->launches += 2;
   return VVCG_OK;
 }
 
