@@ -523,6 +523,62 @@ vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const src[3], ui
                                  uint32_t vis_height, uint8_t bit_depth, uint32_t ctu_size, uint32_t ctu_cols,
                                  const vvcg_alf_ctu* ctus, const vvcg_alf_params* params);
 
+/* ---- general-decoder deblocking ------------------------------------------- */
+
+enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };
+#define VVCG_DBK_NO_TU 0xFFFFFFFFu
+
+/* One 4x4 luma cell of the general decoder's deblocking state: the
+ * transform block marked there (mark_tu, decode_general.rs:4837-4907: id,
+ * width, height, luma cbf) and the coding-unit fields the boundary strength
+ * reads (LumaCell, decode_general.rs:114: valid, intra, ref_idx, mv). */
+typedef struct vvcg_dbk_cell {
+  uint32_t tu_id;      /* VVCG_DBK_NO_TU where no luma transform block is marked */
+  uint16_t tu_w, tu_h; /* luma samples */
+  int32_t mv[2][2];    /* [list][horizontal, vertical], 1/16 sample */
+  int8_t ref_idx[2];   /* -1 = list unused */
+  uint8_t flags;       /* VVCG_DBK_CODED | VVCG_DBK_INTRA | VVCG_DBK_CBF */
+  uint8_t reserved;
+} vvcg_dbk_cell; /* 28 bytes */
+
+/* One 2x2 chroma cell (4:2:0): the Cb and Cr transform blocks marked there
+ * and their size in chroma samples. */
+typedef struct vvcg_dbk_ccell {
+  uint32_t tu_cb, tu_cr; /* VVCG_DBK_NO_TU where none */
+  uint16_t tu_w, tu_h;
+} vvcg_dbk_ccell; /* 12 bytes */
+
+/* Slice-level deblocking parameters: QP and beta / tC offsets (div2) of Y,
+ * Cb, Cr, and the POC of each reference index of lists 0 and 1 (an index at
+ * or beyond num_ref reads POC 0, as the reference's unwrap_or(0) does). */
+typedef struct vvcg_dbk_params {
+  int32_t qp[3];
+  int32_t beta_offset_div2[3];
+  int32_t tc_offset_div2[3];
+  int32_t num_ref[2];
+  int32_t ref_poc[2][16];
+} vvcg_dbk_params;
+
+/* Deblocking of a 4:2:0 picture as the general decoder applies it, in place
+ * on device planes: luma transform-block edges on the 4-sample grid with the
+ * filter lengths of the transform sizes (1 / 3 / 7) and the intra / cbf /
+ * motion boundary strength; chroma transform-block edges on the 8-sample
+ * grid in 2-line groups with bS 2. Vertical edges, then horizontal edges.
+ * cells (cell_cols x cell_rows, raster, device memory) covers the picture
+ * padded to whole CTUs; ccells likewise covers its chroma at one cell per 2x2
+ * chroma samples. The maps must be what mark_tu leaves for a coding tree
+ * (transform blocks of 4 or more samples start on the 4-sample grid), which
+ * keeps the segments of one direction from touching each other's samples.
+ * Replaces: apply_deblock (decode_general.rs:4977-5187) with luma_lens
+ * (:4916), chroma_lens (:4929), deblock_bs (:4939), over
+ * deblock_luma_edge_normative_bd (filter.rs:718) and deblock_chroma_edge
+ * (filter.rs:935-1007). */
+vvcg_status vvcg_deblock_general_dev(vvcg_ctx* ctx, uint16_t* const planes[3], const uint32_t stride[3],
+                                     uint32_t vis_width, uint32_t vis_height, uint8_t bit_depth, uint32_t ctu_size,
+                                     const vvcg_dbk_cell* cells, uint32_t cell_cols, uint32_t cell_rows,
+                                     const vvcg_dbk_ccell* ccells, uint32_t ccell_cols, uint32_t ccell_rows,
+                                     const vvcg_dbk_params* params);
+
 /* ---- general-decoder SAO -------------------------------------------------- */
 
 /* SAO of one plane as the general decoder applies it: every CTU region,

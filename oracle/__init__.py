@@ -98,6 +98,11 @@ def _declare(L):
     L.orc_mip_predict.restype = None
     L.orc_mip_search.argtypes = [vp, vp, vp, i, i, i, vp, C.POINTER(C.c_uint64)]
     L.orc_sao_bounded.argtypes = [vp, vp, i, i, i, i, i, i, i, vp, i]
+    L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
+    L.orc_deblock_general.restype = None
+    L.orc_dbk_lens.argtypes = [i, i, i, i, vp]
+    L.orc_dbk_lens.restype = None
+    L.orc_dbk_bs.argtypes = [i] * 11
     L.orc_sao_bounded.restype = None
     L.orc_mc_luma_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, i, i, i, vp]
     L.orc_mc_luma_8.restype = None
@@ -543,6 +548,33 @@ def mip_search(above, left, src, w, h, bd):
     sad = C.c_uint64(0)
     r = lib().orc_mip_search(_p(a), _p(l), _p(s), w, h, bd, _p(out), C.byref(sad))
     return r & 0xFF, r >> 8, sad.value, out
+
+
+def deblock_general(planes, vis_w, vis_h, bd, ctu, cells, ccells, params):
+    """apply_deblock of the general decoder (decode_general.rs:4977) on a
+    4:2:0 picture; returns filtered copies of the (Y, Cb, Cr) planes. cells /
+    ccells / params in the vvcg_dbk_cell / vvcg_dbk_ccell / vvcg_dbk_params
+    layouts (2-D record arrays, rows x cols)."""
+    y, u, v = (_u16(p).copy() for p in planes)
+    c = np.ascontiguousarray(cells)
+    cc = np.ascontiguousarray(ccells)
+    prm = np.ascontiguousarray(params).reshape(1)
+    lib().orc_deblock_general(_p(y), _p(u), _p(v), y.shape[1], u.shape[1], vis_w, vis_h, bd, ctu, _p(c),
+                              c.shape[1], c.shape[0], _p(cc), cc.shape[1], cc.shape[0], _p(prm))
+    return y, u, v
+
+
+def dbk_lens(luma, size_p, size_q, ctb_boundary=False):
+    """luma_lens / chroma_lens (decode_general.rs:4916 / :4929)."""
+    out = np.zeros(2, np.int32)
+    lib().orc_dbk_lens(int(luma), size_p, size_q, int(ctb_boundary), _p(out))
+    return int(out[0]), int(out[1])
+
+
+def dbk_bs(p_intra, q_intra, p_cbf, q_cbf, tu_edge, pmv, qmv, pref, qref):
+    """derive_boundary_strength (filter.rs:202-226)."""
+    return lib().orc_dbk_bs(int(p_intra), int(q_intra), int(p_cbf), int(q_cbf), int(tu_edge), pmv[0], pmv[1],
+                            qmv[0], qmv[1], pref, qref)
 
 
 def alf_general(y, u, v, vis_w, vis_h, bd, ctu, ctu_cols, ctus, params):

@@ -18,6 +18,8 @@
 
 #include <vector>
 
+#include "../include/vvcg.h"
+
 namespace orc {
 
 enum TrType { kDct2 = 0, kDst7 = 1, kDct8 = 2 };
@@ -120,6 +122,15 @@ int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w,
 // filter.rs:1954-2033 / decode_general.rs:5189-5223: the general decoder's SAO of one plane.
 void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw, int ph, int vis_w, int vis_h,
                           int bd, int ctu, int ctu_cols, const Sao* params);
+// decode_general.rs:4916-4975 / filter.rs:202-226: general-decoder deblocking helpers.
+void dbk_luma_lens(int size_p, int size_q, int* lp, int* lq);
+void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq);
+int dbk_boundary_strength(bool p_intra, bool q_intra, bool p_cbf, bool q_cbf, bool tu_edge, int pmv_h,
+                          int pmv_v, int qmv_h, int qmv_v, int pref, int qref);
+// decode_general.rs:4977-5187 apply_deblock on a 4:2:0 picture, in place.
+void deblock_general(uint16_t* const planes[3], const int stride[3], int vis_w, int vis_h, int bd, int ctu,
+                     const vvcg_dbk_cell* cells, int cols, int rows, const vvcg_dbk_ccell* cc, int ccols,
+                     int crows, const vvcg_dbk_params& prm);
 struct AlfAps {
   int num_luma_filters;  // 0 = fixed filters of the class
   bool luma_clip;

@@ -179,6 +179,25 @@ extern "C" void orc_bi_average_8(const int32_t* p0, const int32_t* p1, int n, in
   orc::weighted_average_bi_8(p0, p1, n, bcw, out);
 }
 
+// planes row-major with strides (samples); cells / ccells / params in the
+// vvcg_dbk_cell / vvcg_dbk_ccell / vvcg_dbk_params layouts
+extern "C" void orc_deblock_general(uint16_t* y, uint16_t* u, uint16_t* v, int sy, int sc, int vis_w, int vis_h,
+                                    int bd, int ctu, const vvcg_dbk_cell* cells, int cols, int rows,
+                                    const vvcg_dbk_ccell* cc, int ccols, int crows, const vvcg_dbk_params* prm) {
+  uint16_t* const planes[3] = {y, u, v};
+  const int stride[3] = {sy, sc, sc};
+  orc::deblock_general(planes, stride, vis_w, vis_h, bd, ctu, cells, cols, rows, cc, ccols, crows, *prm);
+}
+extern "C" void orc_dbk_lens(int luma, int size_p, int size_q, int ctb_boundary, int* out) {
+  if (luma)
+    orc::dbk_luma_lens(size_p, size_q, &out[0], &out[1]);
+  else
+    orc::dbk_chroma_lens(size_p, size_q, ctb_boundary != 0, &out[0], &out[1]);
+}
+extern "C" int orc_dbk_bs(int p_intra, int q_intra, int p_cbf, int q_cbf, int tu_edge, int pmv_h, int pmv_v,
+                          int qmv_h, int qmv_v, int pref, int qref) {
+  return orc::dbk_boundary_strength(p_intra, q_intra, p_cbf, q_cbf, tu_edge, pmv_h, pmv_v, qmv_h, qmv_v, pref, qref);
+}
 // params: 6 bytes per CTU (type, band_or_class, offsets[4]) as vvcg_sao
 extern "C" void orc_sao_bounded(const uint16_t* src, uint16_t* dst, int pw, int ph, int vis_w, int vis_h, int bd,
                                 int ctu, int ctu_cols, const uint8_t* params, int n_params) {

@@ -366,6 +366,182 @@ void deblock_chroma_plane_16(Plane16& p, int cu_step, int ctb_height_c, int qp_c
   }
 }
 
+// ------------------------------------------------ general-decoder DBF ---
+
+// decode_general.rs:4916-4925 luma_lens
+void dbk_luma_lens(int size_p, int size_q, int* lp, int* lq) {
+  if (size_p <= 4 || size_q <= 4) {
+    *lp = *lq = 1;
+    return;
+  }
+  *lp = size_p >= 32 ? 7 : 3;
+  *lq = size_q >= 32 ? 7 : 3;
+}
+
+// decode_general.rs:4929-4935 chroma_lens
+void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq) {
+  if (size_p >= 8 && size_q >= 8) {
+    *lp = ctb_boundary ? 1 : 3;
+    *lq = 3;
+  } else {
+    *lp = *lq = 1;
+  }
+}
+
+// filter.rs:202-226 derive_boundary_strength
+int dbk_boundary_strength(bool p_intra, bool q_intra, bool p_cbf, bool q_cbf, bool tu_edge, int pmv_h,
+                          int pmv_v, int qmv_h, int qmv_v, int pref, int qref) {
+  if (p_intra || q_intra) return 2;
+  if (tu_edge && (p_cbf || q_cbf)) return 1;
+  if (pref != qref || std::abs(pmv_h - qmv_h) >= 8 || std::abs(pmv_v - qmv_v) >= 8) return 1;
+  return 0;
+}
+
+namespace {
+
+struct GenDbk {
+  const vvcg_dbk_cell* cells;
+  int cols, rows;
+  const vvcg_dbk_params* prm;
+  // Gen::lcell (decode_general.rs:463-469): None outside the grid or when invalid
+  const vvcg_dbk_cell* lcell(int x, int y) const {
+    if (x < 0 || y < 0 || x / 4 >= cols || y / 4 >= rows) return nullptr;
+    const vvcg_dbk_cell* c = &cells[(y / 4) * cols + x / 4];
+    return (c->flags & VVCG_DBK_CODED) ? c : nullptr;
+  }
+  // the `field` closure of deblock_bs: motion of the first list in use, POC via
+  // Gen::ref_poc (decode_general.rs:497-504) with unwrap_or(0)
+  void field(const vvcg_dbk_cell* c, int* mh, int* mv, int* poc) const {
+    *mh = *mv = *poc = 0;
+    if (!c) return;
+    for (int l = 0; l < 2; l++) {
+      if (c->ref_idx[l] >= 0) {
+        *mh = c->mv[l][0];
+        *mv = c->mv[l][1];
+        int idx = c->ref_idx[l];
+        *poc = idx < prm->num_ref[l] && idx < 16 ? prm->ref_poc[l][idx] : 0;
+        return;
+      }
+    }
+  }
+  bool cbf(int x, int y) const {
+    if (x / 4 < cols && y / 4 < rows) return (cells[(y / 4) * cols + x / 4].flags & VVCG_DBK_CBF) != 0;
+    return false;
+  }
+  // decode_general.rs:4939-4975 deblock_bs
+  int bs(int x, int y, bool vertical) const {
+    const vvcg_dbk_cell* p = vertical ? lcell(x - 1, y) : lcell(x, y - 1);
+    const vvcg_dbk_cell* q = lcell(x, y);
+    bool pi = p && (p->flags & VVCG_DBK_INTRA), qi = q && (q->flags & VVCG_DBK_INTRA);
+    if (pi || qi) return 2;
+    int ph, pv, pr, qh, qv, qr;
+    field(p, &ph, &pv, &pr);
+    field(q, &qh, &qv, &qr);
+    bool pc = vertical ? cbf(x - 1, y) : cbf(x, y - 1), qc = cbf(x, y);
+    return dbk_boundary_strength(pi, qi, pc, qc, true, ph, pv, qh, qv, pr, qr);
+  }
+};
+
+}  // namespace
+
+// decode_general.rs:4977-5187 apply_deblock: luma vertical then horizontal
+// edges on the 4-sample grid, then per chroma component vertical and
+// horizontal edges on the 8-sample grid in 2-line groups. Each segment is
+// gathered with clamped coordinates, filtered, and written back sample by
+// sample in gather order, as the reference does.
+void deblock_general(uint16_t* const planes[3], const int stride[3], int vis_w, int vis_h, int bd, int ctu,
+                     const vvcg_dbk_cell* cells, int cols, int rows, const vvcg_dbk_ccell* cc, int ccols,
+                     int crows, const vvcg_dbk_params& prm) {
+  const int max_val = (1 << bd) - 1;
+  const int qp_y = clampi(prm.qp[0], 0, 63);
+  GenDbk g{cells, cols, rows, &prm};
+  const int w = vis_w, h = vis_h;
+  uint16_t* Y = planes[0];
+  const int sy = stride[0];
+  auto id = [&](int cx, int cy) { return cells[cy * cols + cx].tu_id; };
+  int lines[4][16];
+  for (int x = 4; x < w; x += 4) {
+    for (int y = 0; y < h; y += 4) {
+      uint32_t a = id(x / 4 - 1, y / 4), b = id(x / 4, y / 4);
+      if (a == VVCG_DBK_NO_TU || b == VVCG_DBK_NO_TU || a == b) continue;
+      int lp, lq;
+      dbk_luma_lens(cells[(y / 4) * cols + x / 4 - 1].tu_w, cells[(y / 4) * cols + x / 4].tu_w, &lp, &lq);
+      for (int i = 0; i < 4; i++) {
+        int yy = std::min(y + i, h - 1);
+        for (int k = 0; k < 16; k++) lines[i][k] = Y[yy * sy + clampi(x - 8 + k, 0, w - 1)];
+      }
+      deblock_luma_edge_bd(lines, qp_y, qp_y, g.bs(x, y, true), prm.beta_offset_div2[0], prm.tc_offset_div2[0],
+                           bd, lp, lq, false);
+      for (int i = 0; i < 4; i++) {
+        int yy = std::min(y + i, h - 1);
+        for (int k = 0; k < 16; k++) Y[yy * sy + clampi(x - 8 + k, 0, w - 1)] = (uint16_t)clampi(lines[i][k], 0, max_val);
+      }
+    }
+  }
+  for (int y = 4; y < h; y += 4) {
+    for (int x = 0; x < w; x += 4) {
+      uint32_t a = id(x / 4, y / 4 - 1), b = id(x / 4, y / 4);
+      if (a == VVCG_DBK_NO_TU || b == VVCG_DBK_NO_TU || a == b) continue;
+      int lp, lq;
+      dbk_luma_lens(cells[(y / 4 - 1) * cols + x / 4].tu_h, cells[(y / 4) * cols + x / 4].tu_h, &lp, &lq);
+      for (int i = 0; i < 4; i++) {
+        int xx = std::min(x + i, w - 1);
+        for (int k = 0; k < 16; k++) lines[i][k] = Y[clampi(y - 8 + k, 0, h - 1) * sy + xx];
+      }
+      deblock_luma_edge_bd(lines, qp_y, qp_y, g.bs(x, y, false), prm.beta_offset_div2[0], prm.tc_offset_div2[0],
+                           bd, lp, lq, y % ctu == 0);
+      for (int i = 0; i < 4; i++) {
+        int xx = std::min(x + i, w - 1);
+        for (int k = 0; k < 16; k++) Y[clampi(y - 8 + k, 0, h - 1) * sy + xx] = (uint16_t)clampi(lines[i][k], 0, max_val);
+      }
+    }
+  }
+  const int cw = (vis_w + 1) / 2, ch = (vis_h + 1) / 2;
+  int cl[4][8];
+  for (int comp = 1; comp < 3; comp++) {
+    uint16_t* P = planes[comp];
+    const int sc = stride[comp];
+    const int qp = clampi(prm.qp[comp], 0, 63);
+    const int bo = prm.beta_offset_div2[comp], to = prm.tc_offset_div2[comp];
+    auto cid = [&](int cx, int cy) { return comp == 1 ? cc[cy * ccols + cx].tu_cb : cc[cy * ccols + cx].tu_cr; };
+    for (int x = 8; x < cw; x += 8) {
+      for (int y = 0; y + 2 <= ch; y += 2) {
+        uint32_t a = cid(x / 2 - 1, y / 2), b = cid(x / 2, y / 2);
+        if (a == VVCG_DBK_NO_TU || b == VVCG_DBK_NO_TU || a == b) continue;
+        int lp, lq;
+        dbk_chroma_lens(cc[(y / 2) * ccols + x / 2 - 1].tu_w, cc[(y / 2) * ccols + x / 2].tu_w, false, &lp, &lq);
+        for (int i = 0; i < 2; i++) {
+          int yy = std::min(y + i, ch - 1);
+          for (int k = 0; k < 8; k++) cl[i][k] = P[yy * sc + clampi(x - 4 + k, 0, cw - 1)];
+        }
+        deblock_chroma_edge(cl, 2, qp, 2, bo, to, lp, lq, bd);
+        for (int i = 0; i < 2; i++) {
+          int yy = std::min(y + i, ch - 1);
+          for (int k = 0; k < 8; k++) P[yy * sc + clampi(x - 4 + k, 0, cw - 1)] = (uint16_t)clampi(cl[i][k], 0, max_val);
+        }
+      }
+    }
+    for (int y = 8; y < ch; y += 8) {
+      for (int x = 0; x + 2 <= cw; x += 2) {
+        uint32_t a = cid(x / 2, y / 2 - 1), b = cid(x / 2, y / 2);
+        if (a == VVCG_DBK_NO_TU || b == VVCG_DBK_NO_TU || a == b) continue;
+        int lp, lq;
+        dbk_chroma_lens(cc[(y / 2 - 1) * ccols + x / 2].tu_h, cc[(y / 2) * ccols + x / 2].tu_h, y % (ctu / 2) == 0,
+                        &lp, &lq);
+        for (int i = 0; i < 2; i++) {
+          int xx = std::min(x + i, cw - 1);
+          for (int k = 0; k < 8; k++) cl[i][k] = P[clampi(y - 4 + k, 0, ch - 1) * sc + xx];
+        }
+        deblock_chroma_edge(cl, 2, qp, 2, bo, to, lp, lq, bd);
+        for (int i = 0; i < 2; i++) {
+          int xx = std::min(x + i, cw - 1);
+          for (int k = 0; k < 8; k++) P[clampi(y - 4 + k, 0, ch - 1) * sc + xx] = (uint16_t)clampi(cl[i][k], 0, max_val);
+        }
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------- SAO ---
 
 // filter.rs:1880-1947 apply_sao_region_16. For edge class 3 the reference uses

@@ -57,6 +57,13 @@ ALF_PARAMS_DTYPE = np.dtype([("num_luma_filters", "u1"), ("luma_clip", "u1"), ("
                              ("chroma_coeff", "<i2", (8, 6)), ("chroma_clip_idx", "u1", (8, 6)),
                              ("cc_cb", "<i2", (4, 7)), ("cc_cr", "<i2", (4, 7))])
 ALF_OFF, ALF_FIXED, ALF_APS = 0, 1, 2
+DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
+                           ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
+DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
+DBK_PARAMS_DTYPE = np.dtype([("qp", "<i4", (3,)), ("beta_offset_div2", "<i4", (3,)), ("tc_offset_div2", "<i4", (3,)),
+                             ("num_ref", "<i4", (2,)), ("ref_poc", "<i4", (2, 16))])
+DBK_CODED, DBK_INTRA, DBK_CBF = 1, 2, 4
+DBK_NO_TU = 0xFFFFFFFF
 MIP_REQ_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("mode", "u1"),
                           ("transposed", "u1"), ("reserved", "u1", (3,)), ("ref_off", "<u4"), ("out_off", "<u4")])
 MIP_RES_DTYPE = np.dtype([("sad", "<u8"), ("mode", "u1"), ("transposed", "u1"), ("reserved", "u1", (6,))])
@@ -139,6 +146,7 @@ assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.i
 assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
 assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
 assert ALF_CTU_DTYPE.itemsize == 8 and ALF_PARAMS_DTYPE.itemsize == 1192
+assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_PARAMS_DTYPE.itemsize == 172
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
@@ -202,6 +210,7 @@ def lib():
         L.vvcg_sao_bounded_16_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u8, u32, u32, vp]
         L.vvcg_mip_predict_dev.argtypes = [vp, vp, u32, vp, u64, vp, vp, u64, vp]
         L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
+        L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -471,6 +480,32 @@ class Context:
         self._keep = (ctus, params)
         self._check(self._L.vvcg_alf_general_dev(self._h, sp, dp, st, w, h, vis_w, vis_h, bit_depth, ctu, ctu_cols,
                                                  _ptr(ctus), _ptr(params)))
+
+    # -- general-decoder deblocking --
+    def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):
+        """In place on planes, (Y, Cb, Cr) int16 CUDA tensors of a 4:2:0
+        picture. cells / ccells: 2-D CUDA uint8 tensors or numpy arrays of
+        DBK_CELL_DTYPE / DBK_CCELL_DTYPE records (rows x cols, numpy arrays are
+        uploaded); params: one DBK_PARAMS_DTYPE record."""
+        import torch
+
+        def dev(a, dt):
+            if isinstance(a, np.ndarray):
+                a = np.ascontiguousarray(a, dtype=dt)
+                rows, cols = a.shape
+                t = torch.from_numpy(a.view(np.uint8).reshape(rows, cols * dt.itemsize).copy())
+                return t.to(planes[0].device), rows, cols
+            rows, nb = a.shape
+            return a, rows, nb // dt.itemsize
+
+        dc, rows, cols = dev(cells, DBK_CELL_DTYPE)
+        dcc, crows, ccols = dev(ccells, DBK_CCELL_DTYPE)
+        params = np.ascontiguousarray(params, dtype=DBK_PARAMS_DTYPE).reshape(1)
+        pp = (C.c_void_p * 3)(*[t.data_ptr() for t in planes])
+        st = (C.c_uint32 * 3)(*[t.stride(0) for t in planes])
+        self._keep = (dc, dcc, params)
+        self._check(self._L.vvcg_deblock_general_dev(self._h, pp, st, vis_w, vis_h, bit_depth, ctu, _ptr(dc), cols,
+                                                     rows, _ptr(dcc), ccols, crows, _ptr(params)))
 
     # -- general-decoder SAO --
     def sao_bounded(self, src, dst, vis_w, vis_h, bit_depth, ctu, ctu_cols, params):

@@ -278,6 +278,55 @@ __device__ __forceinline__ bool chroma_dec(int p0, int p3, int q0, int q3, int d
          abs(p0 - q0) < ((5 * tc + 1) >> 1);
 }
 
+// The decision and line filters of deblock_chroma_edge (filter.rs:960-1007)
+// on n lines of [p3 p2 p1 p0 q0 q1 q2 q3]; len_p / len_q are 1 or 3.
+__device__ __forceinline__ void chroma_edge_lines(int (*ln)[8], int n, int len_p, int len_q, int tc, int beta,
+                                                  int maxv) {
+  if (len_q == 3) {
+    int a[8], b[8];
+    for (int i = 0; i < 8; i++) {
+      a[i] = ln[0][i];
+      b[i] = ln[n - 1][i];
+    }
+    if (len_p == 1) {
+      a[0] = a[1] = a[2];
+      b[0] = b[1] = b[2];
+    }
+    int dp0 = abs(a[1] - 2 * a[2] + a[3]), dp1 = abs(b[1] - 2 * b[2] + b[3]);
+    int dq0 = abs(a[6] - 2 * a[5] + a[4]), dq1 = abs(b[6] - 2 * b[5] + b[4]);
+    int dpq0 = dp0 + dq0, dpq1 = dp1 + dq1;
+    bool strong = (dpq0 + dpq1) < beta && chroma_dec(a[3], a[0], a[4], a[7], 2 * dpq0, beta, tc) &&
+                  chroma_dec(b[3], b[0], b[4], b[7], 2 * dpq1, beta, tc);
+    if (!strong) {
+      len_p = 1;
+      len_q = 1;
+    }
+  }
+  for (int k = 0; k < n; k++) {
+    int* l = ln[k];
+    int m[8];
+    for (int i = 0; i < 8; i++) m[i] = l[i];
+    auto cl = [&](int o, int v) { return clampi(clampi(v, o - tc, o + tc), 0, maxv); };
+    if (len_p == 3 && len_q == 3) {
+      l[1] = cl(m[1], (3 * m[0] + 2 * m[1] + m[2] + m[3] + m[4] + 4) >> 3);
+      l[2] = cl(m[2], (2 * m[0] + m[1] + 2 * m[2] + m[3] + m[4] + m[5] + 4) >> 3);
+      l[3] = cl(m[3], (m[0] + m[1] + m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
+      l[4] = cl(m[4], (m[1] + m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
+      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
+      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
+    } else if (len_p == 1 && len_q == 3) {
+      l[3] = cl(m[3], (3 * m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
+      l[4] = cl(m[4], (2 * m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
+      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
+      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
+    } else {
+      int delta = clampi((4 * (m[4] - m[3]) + m[2] - m[5] + 4) >> 3, -tc, tc);
+      l[3] = clampi(m[3] + delta, 0, maxv);
+      l[4] = clampi(m[4] - delta, 0, maxv);
+    }
+  }
+}
+
 // deblock_chroma_edge (filter.rs:935-1007) + the strong / p1q3 / weak line
 // filters (:1010-1057), driven as in deblock_chroma_plane_16 (:2433-2527).
 // One thread per 2- or 4-line group.
@@ -332,49 +381,7 @@ __global__ void k_deblock_chroma(const DbfPass* __restrict__ passes, int n_pass)
       }
     }
   }
-  if (len_q == 3) {
-    int a[8], b[8];
-    for (int i = 0; i < 8; i++) {
-      a[i] = ln[0][i];
-      b[i] = ln[group - 1][i];
-    }
-    if (len_p == 1) {
-      a[0] = a[1] = a[2];
-      b[0] = b[1] = b[2];
-    }
-    int dp0 = abs(a[1] - 2 * a[2] + a[3]), dp1 = abs(b[1] - 2 * b[2] + b[3]);
-    int dq0 = abs(a[6] - 2 * a[5] + a[4]), dq1 = abs(b[6] - 2 * b[5] + b[4]);
-    int dpq0 = dp0 + dq0, dpq1 = dp1 + dq1;
-    bool strong = (dpq0 + dpq1) < beta && chroma_dec(a[3], a[0], a[4], a[7], 2 * dpq0, beta, tc) &&
-                  chroma_dec(b[3], b[0], b[4], b[7], 2 * dpq1, beta, tc);
-    if (!strong) {
-      len_p = 1;
-      len_q = 1;
-    }
-  }
-  for (int k = 0; k < group; k++) {
-    int* l = ln[k];
-    int m[8];
-    for (int i = 0; i < 8; i++) m[i] = l[i];
-    auto cl = [&](int o, int v) { return clampi(clampi(v, o - tc, o + tc), 0, maxv); };
-    if (len_p == 3 && len_q == 3) {
-      l[1] = cl(m[1], (3 * m[0] + 2 * m[1] + m[2] + m[3] + m[4] + 4) >> 3);
-      l[2] = cl(m[2], (2 * m[0] + m[1] + 2 * m[2] + m[3] + m[4] + m[5] + 4) >> 3);
-      l[3] = cl(m[3], (m[0] + m[1] + m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
-      l[4] = cl(m[4], (m[1] + m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
-      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
-      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
-    } else if (len_p == 1 && len_q == 3) {
-      l[3] = cl(m[3], (3 * m[2] + 2 * m[3] + m[4] + m[5] + m[6] + 4) >> 3);
-      l[4] = cl(m[4], (2 * m[2] + m[3] + 2 * m[4] + m[5] + m[6] + m[7] + 4) >> 3);
-      l[5] = cl(m[5], (m[2] + m[3] + m[4] + 2 * m[5] + m[6] + 2 * m[7] + 4) >> 3);
-      l[6] = cl(m[6], (m[3] + m[4] + m[5] + 2 * m[6] + 3 * m[7] + 4) >> 3);
-    } else {
-      int delta = clampi((4 * (m[4] - m[3]) + m[2] - m[5] + 4) >> 3, -tc, tc);
-      l[3] = clampi(m[3] + delta, 0, maxv);
-      l[4] = clampi(m[4] - delta, 0, maxv);
-    }
-  }
+  chroma_edge_lines(ln, group, len_p, len_q, tc, beta, maxv);
   // positions 0 and 7 are never modified; rewriting them is safe because
   // edges of one pass are at least 8 samples apart
   if (kVertical) {

@@ -13,6 +13,7 @@
 
 #include "../../include/vvcg.h"
 #include "alf_general.cuh"
+#include "dbk_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
 #include "lmcs.cuh"
@@ -1270,6 +1271,61 @@ extern "C" vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const
   k_alf_general_chroma<<<(uint32_t)std::min<uint64_t>((nc + 255) / 256, (uint64_t)ctx->num_sms * 16), 256, 0,
                          ctx->stream>>>(P);
   CK(cudaGetLastError(), "alf launch");
+  ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// General-decoder deblocking (vvcg_deblock_general_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_deblock_general_dev(vvcg_ctx* ctx, uint16_t* const planes[3], const uint32_t stride[3],
+                                                uint32_t vis_width, uint32_t vis_height, uint8_t bit_depth,
+                                                uint32_t ctu_size, const vvcg_dbk_cell* cells, uint32_t cell_cols,
+                                                uint32_t cell_rows, const vvcg_dbk_ccell* ccells,
+                                                uint32_t ccell_cols, uint32_t ccell_rows,
+                                                const vvcg_dbk_params* params) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!planes || !stride || !cells || !ccells || !params) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  if (!vis_width || !vis_height) return VVCG_OK;
+  if (vis_width > 32768 || vis_height > 32768) return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture larger than 32768");
+  const uint32_t cw = (vis_width + 1) / 2, ch = (vis_height + 1) / 2;
+  for (int c = 0; c < 3; c++)
+    if (!planes[c] || stride[c] < (c ? cw : vis_width))
+      return fail(ctx, VVCG_INVALID_INPUT, "plane %d: missing or stride too small", c);
+  if (bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "bit depth");
+  if (ctu_size < 16 || ctu_size > 128 || (ctu_size & (ctu_size - 1)))
+    return fail(ctx, VVCG_INVALID_INPUT, "CTU size must be a power of two in 16..128");
+  if (cell_cols < (vis_width + 3) / 4 || cell_rows < (vis_height + 3) / 4)
+    return fail(ctx, VVCG_INVALID_INPUT, "luma cell map smaller than the picture");
+  if (ccell_cols < (cw + 1) / 2 || ccell_rows < (ch + 1) / 2)
+    return fail(ctx, VVCG_INVALID_INPUT, "chroma cell map smaller than the picture");
+  if (params->num_ref[0] < 0 || params->num_ref[0] > 16 || params->num_ref[1] < 0 || params->num_ref[1] > 16)
+    return fail(ctx, VVCG_INVALID_INPUT, "reference list length must be 0..16");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  DbkGenArgs A;
+  for (int c = 0; c < 3; c++) {
+    A.plane[c] = planes[c];
+    A.stride[c] = (int32_t)stride[c];
+  }
+  A.vis_w = (int32_t)vis_width;
+  A.vis_h = (int32_t)vis_height;
+  A.cw = (int32_t)cw;
+  A.ch = (int32_t)ch;
+  A.bd = bit_depth;
+  A.ctu = (int32_t)ctu_size;
+  A.cells = cells;
+  A.cols = (int32_t)cell_cols;
+  A.rows = (int32_t)cell_rows;
+  A.cc = ccells;
+  A.ccols = (int32_t)ccell_cols;
+  A.crows = (int32_t)ccell_rows;
+  A.prm = *params;
+  const uint64_t n = (uint64_t)((vis_width + 3) / 4) * ((vis_height + 3) / 4);
+  const dim3 grid((uint32_t)std::min<uint64_t>((n + 127) / 128, (uint64_t)ctx->num_sms * 16), 3);
+  k_dbk_general<true><<<grid, 128, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "deblock launch");
+  k_dbk_general<false><<<grid, 128, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "deblock launch");
   ctx->launches += 2;
   return VVCG_OK;
 }

@@ -322,3 +322,178 @@ def random_lmcs_aps(rng):
     a["bin_cw_delta"] = rng.integers(-12, 13, 16)
     a["chroma_res_scaling_offset"] = int(rng.integers(-7, 8))
     return a
+
+
+def _split_tree(rng, x, y, w, h, pic_w, pic_h, min_size, out, leaf_bias, cout=None, chroma_done=False):
+    """Random QT / BT / TT coding tree over one node; nodes that cross the
+    picture's right or bottom edge split implicitly (halves), leaves go to out.
+    With cout, chroma stops splitting at the first node with a child narrower
+    or shorter than 8 luma samples (4:2:0 chroma blocks of 4x4 or more) and
+    its chroma leaves go to cout."""
+    cross_x, cross_y = x + w > pic_w, y + h > pic_h
+    if x >= pic_w or y >= pic_h:
+        return
+
+    def chroma_at(children_min):
+        # chroma of this node stays whole when a child would be below 8 luma
+        if cout is not None and not chroma_done and children_min < 8:
+            cout.append((x, y, w, h))
+            return True
+        return chroma_done
+
+    if cross_x or cross_y:
+        if cross_x and cross_y and w > min_size and h > min_size:
+            cd = chroma_at(min(w, h) // 2)
+            for dy in (0, h // 2):
+                for dx in (0, w // 2):
+                    _split_tree(rng, x + dx, y + dy, w // 2, h // 2, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+            return
+        if cross_x and w > min_size:
+            cd = chroma_at(min(w // 2, h))
+            _split_tree(rng, x, y, w // 2, h, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+            _split_tree(rng, x + w // 2, y, w // 2, h, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+            return
+        if cross_y and h > min_size:
+            cd = chroma_at(min(w, h // 2))
+            _split_tree(rng, x, y, w, h // 2, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+            _split_tree(rng, x, y + h // 2, w, h // 2, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+            return
+    opts = ["leaf"]
+    if w == h and w > min_size:
+        opts.append("qt")
+    if w > min_size:
+        opts.append("bv")
+    if h > min_size:
+        opts.append("bh")
+    if w >= 4 * min_size:
+        opts.append("tv")
+    if h >= 4 * min_size:
+        opts.append("th")
+    p_leaf = leaf_bias if w * h <= 256 else leaf_bias / 3
+    if w > 64 or h > 64:
+        p_leaf = 0.0
+    if len(opts) == 1 or rng.random() < p_leaf:
+        out.append((x, y, w, h))
+        if cout is not None and not chroma_done:
+            cout.append((x, y, w, h))
+        return
+    kind = opts[1 + int(rng.integers(0, len(opts) - 1))]
+    parts = {"qt": [(0, 0, w // 2, h // 2), (w // 2, 0, w // 2, h // 2), (0, h // 2, w // 2, h // 2),
+                    (w // 2, h // 2, w // 2, h // 2)],
+             "bv": [(0, 0, w // 2, h), (w // 2, 0, w // 2, h)],
+             "bh": [(0, 0, w, h // 2), (0, h // 2, w, h // 2)],
+             "tv": [(0, 0, w // 4, h), (w // 4, 0, w // 2, h), (3 * w // 4, 0, w // 4, h)],
+             "th": [(0, 0, w, h // 4), (0, h // 4, w, h // 2), (0, 3 * h // 4, w, h // 4)]}[kind]
+    cd = chroma_at(min(min(pw, ph) for _, _, pw, ph in parts))
+    for dx, dy, pw, ph in parts:
+        _split_tree(rng, x + dx, y + dy, pw, ph, pic_w, pic_h, min_size, out, leaf_bias, cout, cd)
+
+
+def random_deblock_picture(vis_w, vis_h, ctu=32, bd=10, seed=0, dual_tree=False, isp_prob=0.25,
+                           intra_prob=0.4, max_tb=64, leaf_bias=0.45):
+    """A 4:2:0 picture with a random coding tree for the general decoder's
+    deblocking: planes (Y, Cb, Cr) as uint16 arrays of the visible size with a
+    per-transform-block DC step on smooth noise (so that edges take every
+    filter decision), the luma cell map (DBK_CELL_DTYPE, one cell per 4x4 of
+    the picture padded to whole CTUs), the chroma cell map (DBK_CCELL_DTYPE,
+    one cell per 2x2 chroma samples) and slice parameters (DBK_PARAMS_DTYPE).
+    The maps are what mark_tu (decode_general.rs:4837-4907) leaves: luma
+    transform blocks tile each CU (max_tb, or ISP's 2 or 4 sub-partitions of
+    1..64 samples), chroma ones each chroma CU of the same tree, or of a
+    separate tree when dual_tree."""
+    from . import DBK_CCELL_DTYPE, DBK_CELL_DTYPE, DBK_CBF, DBK_CODED, DBK_INTRA, DBK_NO_TU, DBK_PARAMS_DTYPE
+
+    rng = np.random.default_rng(seed)
+    pic_w, pic_h = -(-vis_w // ctu) * ctu, -(-vis_h // ctu) * ctu
+    cols, rows = pic_w // 4, pic_h // 4
+    ccols, crows = -(-(pic_w // 2) // 2), -(-(pic_h // 2) // 2)
+    cells = np.zeros((rows, cols), DBK_CELL_DTYPE)
+    cells["tu_id"] = DBK_NO_TU
+    cells["ref_idx"] = -1
+    cc = np.zeros((crows, ccols), DBK_CCELL_DTYPE)
+    cc["tu_cb"] = DBK_NO_TU
+    cc["tu_cr"] = DBK_NO_TU
+    maxv = (1 << bd) - 1
+    amp = 1 << (bd - 8)
+    y_dc = np.zeros((pic_h, pic_w), np.int32)
+    c_dc = [np.zeros((pic_h // 2, pic_w // 2), np.int32) for _ in range(2)]
+    next_id = [0]
+
+    def mark(comp, x, y, w, h, cbf):
+        tid = next_id[0]
+        next_id[0] += 1
+        if comp == 0:
+            x1, y1 = min(x + w, cols * 4), min(y + h, rows * 4)
+            cx0, cx1, cy0, cy1 = x // 4, (x1 + 3) // 4, y // 4, (y1 + 3) // 4
+            sub = cells[cy0:cy1, cx0:cx1]
+            sub["tu_id"], sub["tu_w"], sub["tu_h"] = tid, w, h
+            sub["flags"] = (sub["flags"] & (0xFF ^ DBK_CBF)) | (DBK_CBF if cbf else 0)
+            y_dc[y:y + h, x:x + w] = int(rng.integers(-10, 11)) * amp
+        else:
+            cx, cy, cw_, ch_ = x // 2, y // 2, w // 2, h // 2
+            x1, y1 = min(cx + cw_, ccols * 2), min(cy + ch_, crows * 2)
+            sub = cc[cy // 2:(y1 + 1) // 2, cx // 2:(x1 + 1) // 2]
+            sub["tu_cb" if comp == 1 else "tu_cr"] = tid
+            sub["tu_w"], sub["tu_h"] = cw_, ch_
+            c_dc[comp - 1][cy:cy + ch_, cx:cx + cw_] = int(rng.integers(-8, 9)) * amp
+
+    cus, shared_ccus = [], []
+    for ty in range(0, pic_h, ctu):
+        for tx in range(0, pic_w, ctu):
+            _split_tree(rng, tx, ty, ctu, ctu, vis_w, vis_h, 4, cus, leaf_bias, shared_ccus)
+    for (x, y, w, h) in cus:
+        intra = rng.random() < intra_prob
+        sub = cells[y // 4:(y + h + 3) // 4, x // 4:(x + w + 3) // 4]
+        sub["flags"] = DBK_CODED | (DBK_INTRA if intra else 0)
+        if not intra:
+            d = int(rng.integers(1, 4))
+            for l in range(2):
+                if d & (1 << l):
+                    sub["ref_idx"][..., l] = int(rng.integers(0, 3))
+                    big = rng.random() < 0.5
+                    sub["mv"][..., l, :] = rng.integers(-40, 41, 2) if big else rng.integers(-3, 4, 2)
+        if intra and rng.random() < isp_prob and w * h > 16 and (w < 64 or h < 64):
+            vert = bool(rng.integers(0, 2)) if w > 1 and h > 1 else False
+            n = 2 if (w, h) in ((4, 8), (8, 4)) else 4
+            for i in range(n):
+                if vert:
+                    mark(0, x + i * (w // n), y, w // n, h, rng.random() < 0.6)
+                else:
+                    mark(0, x, y + i * (h // n), w, h // n, rng.random() < 0.6)
+        else:
+            tb = min(max_tb, 64)
+            for yy in range(y, y + h, min(h, tb)):
+                for xx in range(x, x + w, min(w, tb)):
+                    mark(0, xx, yy, min(w, tb), min(h, tb), rng.random() < 0.6)
+    ccus = []
+    if dual_tree:
+        for ty in range(0, pic_h, ctu):
+            for tx in range(0, pic_w, ctu):
+                _split_tree(rng, tx, ty, ctu, ctu, vis_w, vis_h, 8, ccus, leaf_bias)
+    else:
+        ccus = shared_ccus
+    for (x, y, w, h) in ccus:
+        tb = 64
+        for yy in range(y, y + h, min(h, tb)):
+            for xx in range(x, x + w, min(w, tb)):
+                for comp in (1, 2):
+                    mark(comp, xx, yy, min(w, tb), min(h, tb), True)
+    # smooth content plus the per-block steps
+    yn, un, vn = value_noise_frame(pic_w, pic_h, 10, frame=seed)
+
+    def scale(p):
+        return p.astype(np.int32) << (bd - 10) if bd >= 10 else p.astype(np.int32) >> (10 - bd)
+
+    ys = np.clip(scale(yn) // 4 + (maxv // 3) + y_dc + rng.integers(-amp, amp + 1, y_dc.shape), 0, maxv)
+    us = np.clip(scale(un) // 4 + (maxv // 3) + c_dc[0] + rng.integers(-amp, amp + 1, c_dc[0].shape), 0, maxv)
+    vs = np.clip(scale(vn) // 4 + (maxv // 3) + c_dc[1] + rng.integers(-amp, amp + 1, c_dc[1].shape), 0, maxv)
+    cw, ch = (vis_w + 1) // 2, (vis_h + 1) // 2
+    planes = (ys[:vis_h, :vis_w].astype(np.uint16), us[:ch, :cw].astype(np.uint16), vs[:ch, :cw].astype(np.uint16))
+    params = np.zeros((), DBK_PARAMS_DTYPE)
+    qp = int(rng.integers(22, 46))
+    params["qp"] = [qp, qp + int(rng.integers(-3, 2)), qp + int(rng.integers(-3, 2))]
+    params["beta_offset_div2"] = rng.integers(-4, 5, 3)
+    params["tc_offset_div2"] = rng.integers(-4, 5, 3)
+    params["num_ref"] = [3, 2]
+    params["ref_poc"] = rng.integers(-8, 9, (2, 16))
+    return planes, cells, cc, params
