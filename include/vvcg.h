@@ -523,6 +523,41 @@ vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const src[3], ui
                                  uint32_t vis_height, uint8_t bit_depth, uint32_t ctu_size, uint32_t ctu_cols,
                                  const vvcg_alf_ctu* ctus, const vvcg_alf_params* params);
 
+/* ---- 8-bit luma intra mode search ---------------------------------------- */
+
+enum { VVCG_ISR_MPM_ONLY = 1, VVCG_ISR_MRL = 2 };
+
+/* One luma block of an 8-bit picture to choose an intra mode for. */
+typedef struct vvcg_intra_search_req {
+  uint32_t x, y;           /* top-left sample; the block lies inside the plane */
+  uint8_t log2_w, log2_h;  /* 2..6 */
+  uint8_t flags;           /* VVCG_ISR_MPM_ONLY: the 6 MPMs instead of all 67 modes;
+                              VVCG_ISR_MRL: then reference lines 1 and 2 for mpm[1..5] */
+  uint8_t log2_ctu;        /* 4..7: CTU size (a block on a CTU's first row keeps line 0) */
+  uint8_t mpm[6];          /* most probable modes, 0..66 */
+  uint8_t reserved[2];
+} vvcg_intra_search_req; /* 20 bytes */
+
+typedef struct vvcg_intra_search_res {
+  uint64_t sad;            /* sum of |source - prediction| of the winner */
+  uint8_t mode, mrl_idx;   /* winning mode 0..66 and reference line */
+  uint8_t reserved[6];
+} vvcg_intra_search_res; /* 16 bytes */
+
+/* Luma intra mode decision of the 8-bit multi-tool encoder for a batch of
+ * blocks: Planar, DC and the 65 angular modes (or the MPMs) predicted from
+ * recon, compared with src by SAD, the first lowest winning (Planar on a
+ * tie); with VVCG_ISR_MRL the lines 1 and 2 predictions of mpm[1..5] then
+ * replace it when strictly lower. recon / src are device 8-bit planes of
+ * width x height with the given strides (in bytes), reqs host memory, res
+ * device memory (one per request). Replaces: choose_luma_intra_pred_mode
+ * (predict.rs:2737-2801) with predict_block_full (:2655-2699) and the MRL
+ * candidate loop of encode_picture_multitool (slice.rs:2698-2731). */
+vvcg_status vvcg_luma_intra_search_8_dev(vvcg_ctx* ctx, const uint8_t* recon, uint64_t recon_stride,
+                                         const uint8_t* src, uint64_t src_stride, uint32_t width, uint32_t height,
+                                         const vvcg_intra_search_req* reqs, uint32_t num_reqs,
+                                         vvcg_intra_search_res* res);
+
 /* ---- general-decoder deblocking ------------------------------------------- */
 
 enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };

@@ -98,6 +98,10 @@ def _declare(L):
     L.orc_mip_predict.restype = None
     L.orc_mip_search.argtypes = [vp, vp, vp, i, i, i, vp, C.POINTER(C.c_uint64)]
     L.orc_sao_bounded.argtypes = [vp, vp, i, i, i, i, i, i, i, vp, i]
+    L.orc_luma_intra_search_8.argtypes = [vp, vp, i, i, i, i, i, i, vp, i, i, i, vp]
+    L.orc_luma_intra_search_8.restype = None
+    L.orc_predict_luma_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, vp]
+    L.orc_predict_luma_8.restype = None
     L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
     L.orc_deblock_general.restype = None
     L.orc_dbk_lens.argtypes = [i, i, i, i, vp]
@@ -246,6 +250,28 @@ def predict_cclm(luma, chroma, bd, bxc, byc, cw, ch, mode, cf=CHROMA_420, ctu=32
     lib().orc_predict_cclm(_p(luma), luma.shape[1], luma.shape[0], _p(chroma), chroma.shape[1],
                            chroma.shape[0], bd, bxc, byc, cw, ch, mode, cf, ctu, _p(out))
     return out
+
+
+def predict_luma_8(recon, x, y, w, h, mode, mrl=0, ctu=32):
+    """predict_block_full (predict.rs:2655) of one luma Planar / DC / angular
+    mode on an 8-bit plane; int32 (h, w)."""
+    recon = np.ascontiguousarray(recon, dtype=np.uint8)
+    out = np.zeros((h, w), dtype=np.int32)
+    lib().orc_predict_luma_8(_p(recon), recon.shape[1], recon.shape[0], x, y, w, h, mode, mrl, ctu, _p(out))
+    return out
+
+
+def luma_intra_search_8(recon, src, x, y, w, h, mpm, mpm_only=False, mrl=False, ctu=32):
+    """choose_luma_intra_pred_mode (predict.rs:2737) on 8-bit planes, with the
+    multi-tool encoder's MRL candidates (slice.rs:2698-2731) when mrl;
+    returns (mode, mrl_idx, sad)."""
+    recon = np.ascontiguousarray(recon, dtype=np.uint8)
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    m = np.ascontiguousarray(mpm, dtype=np.uint8)
+    out = np.zeros(4, np.uint32)
+    lib().orc_luma_intra_search_8(_p(recon), _p(src), recon.shape[1], recon.shape[0], x, y, w, h, _p(m),
+                                  int(mpm_only), int(mrl), ctu, _p(out))
+    return int(out[0]), int(out[1]), int(out[2]) | (int(out[3]) << 32)
 
 
 def choose_intra_mode(recon, src, bd, bx, by, w, h):

@@ -62,6 +62,14 @@ struct Plane16 {
   }
 };
 
+// predict.rs:987-1030 Plane: row-major 8-bit samples, stride = width
+struct Plane8 {
+  const uint8_t* data;
+  int width;
+  int height;
+  int get(int x, int y) const { return data[(size_t)y * width + x]; }
+};
+
 struct Refs16 {
   int top_left;
   std::vector<int> above;  // 2 * width
@@ -101,6 +109,7 @@ struct AngularParams {
   bool interpolation_flag;
   bool apply_pdpc;
   int angular_scale;
+  int ref_w, ref_h;  // refW / refH (H.266 8.4.5.2.6)
 };
 AngularParams init_angular_params(int dir_mode, int pu_w, int pu_h, int cu_w, int cu_h,
                                   bool is_luma, int mrl_idx, bool use_isp);
@@ -122,6 +131,11 @@ int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w,
 // filter.rs:1954-2033 / decode_general.rs:5189-5223: the general decoder's SAO of one plane.
 void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw, int ph, int vis_w, int vis_h,
                           int bd, int ctu, int ctu_cols, const Sao* params);
+// predict.rs:2737-2801 choose_luma_intra_pred_mode (+ the multi-tool encoder's
+// MRL candidates, slice.rs:2698-2731) and predict_block_full (:2655) on 8-bit planes.
+void luma_intra_search_8(const Plane8& recon, const Plane8& src, int bx, int by, int w, int h, const uint8_t mpm[6],
+                         bool mpm_only, bool mrl, int ctu_size, int* best_mode, int* best_mrl, uint64_t* best_sad);
+void predict_luma_8(const Plane8& recon, int bx, int by, int w, int h, int mode, int mrl, int ctu_size, int32_t* out);
 // decode_general.rs:4916-4975 / filter.rs:202-226: general-decoder deblocking helpers.
 void dbk_luma_lens(int size_p, int size_q, int* lp, int* lq);
 void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq);

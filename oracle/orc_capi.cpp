@@ -179,6 +179,24 @@ extern "C" void orc_bi_average_8(const int32_t* p0, const int32_t* p1, int n, in
   orc::weighted_average_bi_8(p0, p1, n, bcw, out);
 }
 
+// out: mode, mrl index, SAD (low 32 bits), SAD (high 32 bits)
+extern "C" void orc_luma_intra_search_8(const uint8_t* recon, const uint8_t* src, int pw, int ph, int bx, int by,
+                                        int w, int h, const uint8_t* mpm, int mpm_only, int mrl, int ctu,
+                                        uint32_t* out) {
+  orc::Plane8 r{recon, pw, ph}, s{src, pw, ph};
+  int mode, mi;
+  uint64_t sad;
+  orc::luma_intra_search_8(r, s, bx, by, w, h, mpm, mpm_only != 0, mrl != 0, ctu, &mode, &mi, &sad);
+  out[0] = (uint32_t)mode;
+  out[1] = (uint32_t)mi;
+  out[2] = (uint32_t)sad;
+  out[3] = (uint32_t)(sad >> 32);
+}
+extern "C" void orc_predict_luma_8(const uint8_t* recon, int pw, int ph, int bx, int by, int w, int h, int mode,
+                                   int mrl, int ctu, int32_t* out) {
+  orc::Plane8 r{recon, pw, ph};
+  orc::predict_luma_8(r, bx, by, w, h, mode, mrl, ctu, out);
+}
 // planes row-major with strides (samples); cells / ccells / params in the
 // vvcg_dbk_cell / vvcg_dbk_ccell / vvcg_dbk_params layouts
 extern "C" void orc_deblock_general(uint16_t* y, uint16_t* u, uint16_t* v, int sy, int sc, int vis_w, int vis_h,

@@ -68,6 +68,8 @@ AngularParams init_angular_params(int dir_mode, int pu_w, int pu_h, int cu_w, in
       p.interpolation_flag = !int_slope;
     }
   }
+  p.ref_w = (use_isp && is_luma) ? cu_w + pu_w : 2 * pu_w;
+  p.ref_h = (use_isp && is_luma) ? cu_h + pu_h : 2 * pu_h;
   return p;
 }
 

@@ -57,6 +57,10 @@ ALF_PARAMS_DTYPE = np.dtype([("num_luma_filters", "u1"), ("luma_clip", "u1"), ("
                              ("chroma_coeff", "<i2", (8, 6)), ("chroma_clip_idx", "u1", (8, 6)),
                              ("cc_cb", "<i2", (4, 7)), ("cc_cr", "<i2", (4, 7))])
 ALF_OFF, ALF_FIXED, ALF_APS = 0, 1, 2
+ISR_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("log2_w", "u1"), ("log2_h", "u1"), ("flags", "u1"),
+                          ("log2_ctu", "u1"), ("mpm", "u1", (6,)), ("reserved", "u1", (2,))])
+ISR_RES_DTYPE = np.dtype([("sad", "<u8"), ("mode", "u1"), ("mrl_idx", "u1"), ("reserved", "u1", (6,))])
+ISR_MPM_ONLY, ISR_MRL = 1, 2
 DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
                            ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
 DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
@@ -146,6 +150,7 @@ assert CTU_DTYPE.itemsize == 20 and MC_BLOCK_DTYPE.itemsize == 40 and TU_DTYPE.i
 assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
 assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
 assert ALF_CTU_DTYPE.itemsize == 8 and ALF_PARAMS_DTYPE.itemsize == 1192
+assert ISR_REQ_DTYPE.itemsize == 20 and ISR_RES_DTYPE.itemsize == 16
 assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_PARAMS_DTYPE.itemsize == 172
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
@@ -210,6 +215,7 @@ def lib():
         L.vvcg_sao_bounded_16_dev.argtypes = [vp, vp, vp, u32, u32, u32, u32, u32, u8, u32, u32, vp]
         L.vvcg_mip_predict_dev.argtypes = [vp, vp, u32, vp, u64, vp, vp, u64, vp]
         L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
+        L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -480,6 +486,23 @@ class Context:
         self._keep = (ctus, params)
         self._check(self._L.vvcg_alf_general_dev(self._h, sp, dp, st, w, h, vis_w, vis_h, bit_depth, ctu, ctu_cols,
                                                  _ptr(ctus), _ptr(params)))
+
+    # -- 8-bit luma intra mode search --
+    def luma_intra_search_8(self, recon, src, reqs):
+        """recon / src: (H, W) uint8 CUDA tensors; reqs: ISR_REQ_DTYPE host
+        records. Returns the ISR_RES_DTYPE results (synchronises)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=ISR_REQ_DTYPE)
+        h, w = recon.shape
+        if tuple(src.shape) != (h, w):
+            raise InvalidInput("recon and source planes differ in size")
+        out = torch.empty(max(len(reqs), 1) * ISR_RES_DTYPE.itemsize, dtype=torch.uint8, device=recon.device)
+        self._keep = reqs
+        self._check(self._L.vvcg_luma_intra_search_8_dev(self._h, _ptr(recon), recon.stride(0), _ptr(src),
+                                                         src.stride(0), w, h, _ptr(reqs), len(reqs), _ptr(out)))
+        torch.cuda.synchronize(recon.device)
+        return out.cpu().numpy().view(ISR_RES_DTYPE)[:len(reqs)]
 
     # -- general-decoder deblocking --
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):

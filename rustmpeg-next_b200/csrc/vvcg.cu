@@ -16,6 +16,7 @@
 #include "dbk_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
+#include "intra8.cuh"
 #include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
@@ -1272,6 +1273,45 @@ extern "C" vvcg_status vvcg_alf_general_dev(vvcg_ctx* ctx, const uint16_t* const
                          ctx->stream>>>(P);
   CK(cudaGetLastError(), "alf launch");
   ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 8-bit luma intra mode search (vvcg_luma_intra_search_8_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_luma_intra_search_8_dev(vvcg_ctx* ctx, const uint8_t* recon, uint64_t recon_stride,
+                                                    const uint8_t* src, uint64_t src_stride, uint32_t width,
+                                                    uint32_t height, const vvcg_intra_search_req* reqs,
+                                                    uint32_t num_reqs, vvcg_intra_search_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!recon || !src || !reqs || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing planes, requests or results");
+  if (recon_stride < width || src_stride < width) return fail(ctx, VVCG_INVALID_INPUT, "stride smaller than width");
+  if (width > (1u << 20) || height > (1u << 20)) return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane larger than 2^20");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_intra_search_req& q = reqs[i];
+    if (q.log2_w < 2 || q.log2_w > 6 || q.log2_h < 2 || q.log2_h > 6)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block size outside 4..64", i);
+    if ((uint64_t)q.x + (1u << q.log2_w) > width || (uint64_t)q.y + (1u << q.log2_h) > height)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block outside the plane", i);
+    if (q.flags & ~(uint32_t)(VVCG_ISR_MPM_ONLY | VVCG_ISR_MRL))
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: unknown flags", i);
+    if ((q.flags & VVCG_ISR_MRL) && (q.log2_ctu < 4 || q.log2_ctu > 7))
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: CTU size outside 16..128", i);
+    for (int k = 0; k < 6; k++)
+      if (q.mpm[k] > 66) return fail(ctx, VVCG_INVALID_INPUT, "request %u: MPM %d is not a mode", i, k);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_intra_search_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(vvcg_intra_search_req) * num_reqs, cudaMemcpyHostToDevice,
+                     ctx->stream),
+     "upload");
+  IsrArgs A{recon, src, (int64_t)recon_stride, (int64_t)src_stride, (int32_t)width, (int32_t)height,
+            (int32_t)num_reqs, (const vvcg_intra_search_req*)ctx->d_tu_recs.p, res};
+  const uint32_t grid = std::min<uint32_t>(num_reqs, (uint32_t)ctx->num_sms * 8);
+  k_luma_intra_search_8<<<grid, kIsrWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "intra search launch");
+  ctx->launches++;
   return VVCG_OK;
 }
 
