@@ -558,6 +558,48 @@ vvcg_status vvcg_luma_intra_search_8_dev(vvcg_ctx* ctx, const uint8_t* recon, ui
                                          const vvcg_intra_search_req* reqs, uint32_t num_reqs,
                                          vvcg_intra_search_res* res);
 
+/* ---- CTU full search of the GPU encoder ------------------------------------ */
+
+/* Split types of a 32x32 CTU: none, quad (4 x 16x16), binary with a
+ * horizontal / vertical split line (2 x 32x16 / 2 x 16x32), ternary with
+ * horizontal / vertical lines (32x8 + 32x16 + 32x8 / 8x32 + 16x32 + 8x32). */
+enum {
+  VVCG_SPLIT_NONE = 0, VVCG_SPLIT_QT = 1, VVCG_SPLIT_BT_H = 2, VVCG_SPLIT_BT_V = 3,
+  VVCG_SPLIT_TT_H = 4, VVCG_SPLIT_TT_V = 5
+};
+
+typedef struct vvcg_ctu_search_req {
+  uint32_t x, y;       /* top-left luma sample of a 32x32 CTU inside the plane */
+  uint8_t split_mask;  /* bit s: evaluate split type s (0x3F: all six) */
+  uint8_t n_cand;      /* 0: all 67 modes for every block, else cand[0..n_cand) */
+  uint8_t cand[6];
+} vvcg_ctu_search_req; /* 16 bytes */
+
+typedef struct vvcg_ctu_search_res {
+  uint32_t cost;           /* cost of the chosen split */
+  uint32_t split_cost[6];  /* per split type, UINT32_MAX where not evaluated */
+  uint8_t split;           /* chosen split type */
+  uint8_t cu_mode;         /* best mode of the unsplit CU (0xFF when not evaluated) */
+  uint8_t modes[4];        /* modes of the chosen split's blocks, 0xFF past its count */
+  uint8_t reserved[2];
+} vvcg_ctu_search_res; /* 36 bytes */
+
+/* Mode and split decision of 32x32 CTUs of a luma plane (device, 8..12-bit
+ * samples in uint16, stride in samples) by full search: for every evaluated
+ * split type, each block takes the mode of lowest cost among all 67 (or the
+ * candidates) with predictions from the source plane's own samples (the
+ * predictors of predict_block_16, predict.rs:3079-3410); cost = sum over 8x8
+ * tiles of (sum |Hadamard(source - prediction)| + 2) >> 2 plus
+ * (lambda_q8 * bits) >> 8, with mode bits 2 + i for the i-th default MPM
+ * (Planar, DC, 50, 18, 46, 54) and 7 for any other mode, and split bits 1 /
+ * 2 / 3 / 3 / 4 / 4 added per split type. The first lowest cost wins, blocks
+ * and splits alike. reqs host memory, res device memory. This is the GPU
+ * encoder's candidate-cost stage; the reference's encoders evaluate a
+ * single 32x32 CU per CTU (slice.rs:2575-2800). */
+vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width, uint32_t height,
+                                uint8_t bit_depth, uint32_t lambda_q8, const vvcg_ctu_search_req* reqs,
+                                uint32_t num_reqs, vvcg_ctu_search_res* res);
+
 /* ---- general-decoder deblocking ------------------------------------------- */
 
 enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };

@@ -102,6 +102,8 @@ def _declare(L):
     L.orc_luma_intra_search_8.restype = None
     L.orc_predict_luma_8.argtypes = [vp, i, i, i, i, i, i, i, i, i, vp]
     L.orc_predict_luma_8.restype = None
+    L.orc_ctu_search.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint32, vp]
+    L.orc_ctu_search.restype = None
     L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
     L.orc_deblock_general.restype = None
     L.orc_dbk_lens.argtypes = [i, i, i, i, vp]
@@ -272,6 +274,25 @@ def luma_intra_search_8(recon, src, x, y, w, h, mpm, mpm_only=False, mrl=False, 
     lib().orc_luma_intra_search_8(_p(recon), _p(src), recon.shape[1], recon.shape[0], x, y, w, h, _p(m),
                                   int(mpm_only), int(mrl), ctu, _p(out))
     return int(out[0]), int(out[1]), int(out[2]) | (int(out[3]) << 32)
+
+
+def ctu_search(src, bd, x, y, lambda_q8, split_mask=0x3F, cand=()):
+    """The GPU encoder's CTU full search on a 16-bit luma plane (no reference
+    counterpart); returns a dict with the fields of vvcg_ctu_search_res."""
+    src = _u16(src)
+    c = np.zeros(6, np.uint8)
+    c[:len(cand)] = cand
+    out = np.zeros(10, np.uint32)
+    lib().orc_ctu_search(_p(src), src.shape[1], src.shape[0], bd, x, y, split_mask, len(cand), _p(c), lambda_q8,
+                         _p(out))
+    m = int(out[9])
+    return dict(cost=int(out[0]), split_cost=[int(v) for v in out[1:7]], split=int(out[7]), cu_mode=int(out[8]),
+                modes=[(m >> (8 * k)) & 0xFF for k in range(4)])
+
+
+def search_lambda_q8(qp):
+    """lambda of the CTU search in 1/256 units: sqrt(0.57 * 2^((qp - 12) / 3))."""
+    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0))))
 
 
 def choose_intra_mode(recon, src, bd, bx, by, w, h):

@@ -136,6 +136,9 @@ void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw
 void luma_intra_search_8(const Plane8& recon, const Plane8& src, int bx, int by, int w, int h, const uint8_t mpm[6],
                          bool mpm_only, bool mrl, int ctu_size, int* best_mode, int* best_mrl, uint64_t* best_sad);
 void predict_luma_8(const Plane8& recon, int bx, int by, int w, int h, int mode, int mrl, int ctu_size, int32_t* out);
+// The GPU encoder's CTU full search (orc_search.cpp; no reference counterpart).
+void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, const uint8_t* cand,
+                uint32_t lambda_q8, uint32_t* cost, uint32_t split_cost[6], int* split, int* cu_mode, int modes[4]);
 // decode_general.rs:4916-4975 / filter.rs:202-226: general-decoder deblocking helpers.
 void dbk_luma_lens(int size_p, int size_q, int* lp, int* lq);
 void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq);

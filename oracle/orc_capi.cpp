@@ -179,6 +179,16 @@ extern "C" void orc_bi_average_8(const int32_t* p0, const int32_t* p1, int n, in
   orc::weighted_average_bi_8(p0, p1, n, bcw, out);
 }
 
+// out[0..9]: cost, split_cost[6], split, cu_mode, modes packed 4 x 8 bits
+extern "C" void orc_ctu_search(const uint16_t* src, int pw, int ph, int bd, int cx, int cy, int split_mask,
+                               int n_cand, const uint8_t* cand, uint32_t lambda_q8, uint32_t* out) {
+  orc::Plane16 p{(uint16_t*)src, pw, ph, bd};
+  int split, cu_mode, modes[4];
+  orc::ctu_search(p, cx, cy, split_mask, n_cand, cand, lambda_q8, &out[0], &out[1], &split, &cu_mode, modes);
+  out[7] = (uint32_t)split;
+  out[8] = (uint32_t)cu_mode;
+  out[9] = (uint32_t)(modes[0] | (modes[1] << 8) | (modes[2] << 16) | ((uint32_t)modes[3] << 24));
+}
 // out: mode, mrl index, SAD (low 32 bits), SAD (high 32 bits)
 extern "C" void orc_luma_intra_search_8(const uint8_t* recon, const uint8_t* src, int pw, int ph, int bx, int by,
                                         int w, int h, const uint8_t* mpm, int mpm_only, int mrl, int ctu,

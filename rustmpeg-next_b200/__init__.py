@@ -61,6 +61,11 @@ ISR_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("log2_w", "u1"), ("log2_h
                           ("log2_ctu", "u1"), ("mpm", "u1", (6,)), ("reserved", "u1", (2,))])
 ISR_RES_DTYPE = np.dtype([("sad", "<u8"), ("mode", "u1"), ("mrl_idx", "u1"), ("reserved", "u1", (6,))])
 ISR_MPM_ONLY, ISR_MRL = 1, 2
+CTU_SEARCH_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("split_mask", "u1"), ("n_cand", "u1"),
+                                 ("cand", "u1", (6,))])
+CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), ("split", "u1"), ("cu_mode", "u1"),
+                                 ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
+SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
 DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
                            ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
 DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
@@ -151,6 +156,7 @@ assert TXS_REQ_DTYPE.itemsize == 16 and TXS_RES_DTYPE.itemsize == 16
 assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
 assert ALF_CTU_DTYPE.itemsize == 8 and ALF_PARAMS_DTYPE.itemsize == 1192
 assert ISR_REQ_DTYPE.itemsize == 20 and ISR_RES_DTYPE.itemsize == 16
+assert CTU_SEARCH_REQ_DTYPE.itemsize == 16 and CTU_SEARCH_RES_DTYPE.itemsize == 36
 assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_PARAMS_DTYPE.itemsize == 172
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
@@ -216,6 +222,7 @@ def lib():
         L.vvcg_mip_predict_dev.argtypes = [vp, vp, u32, vp, u64, vp, vp, u64, vp]
         L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
+        L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -503,6 +510,25 @@ class Context:
                                                          src.stride(0), w, h, _ptr(reqs), len(reqs), _ptr(out)))
         torch.cuda.synchronize(recon.device)
         return out.cpu().numpy().view(ISR_RES_DTYPE)[:len(reqs)]
+
+    # -- CTU full search of the GPU encoder --
+    def ctu_search(self, src, bit_depth, lambda_q8, reqs, out=None, sync=True):
+        """src: (H, W) int16 CUDA tensor of 16-bit luma samples; reqs:
+        CTU_SEARCH_REQ_DTYPE host records. Returns the CTU_SEARCH_RES_DTYPE
+        results (or fills the CUDA uint8 tensor out without synchronising)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=CTU_SEARCH_REQ_DTYPE)
+        h, w = src.shape
+        dst = out if out is not None else torch.empty(max(len(reqs), 1) * CTU_SEARCH_RES_DTYPE.itemsize,
+                                                      dtype=torch.uint8, device=src.device)
+        self._keep = reqs
+        self._check(self._L.vvcg_ctu_search_dev(self._h, _ptr(src), src.stride(0), w, h, bit_depth, lambda_q8,
+                                                _ptr(reqs), len(reqs), _ptr(dst)))
+        if out is not None and not sync:
+            return None
+        torch.cuda.synchronize(src.device)
+        return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:len(reqs)]
 
     # -- general-decoder deblocking --
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):

@@ -16,7 +16,7 @@
 #include "dbk_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
-#include "intra8.cuh"
+#include "intra_search.cuh"
 #include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
@@ -116,6 +116,7 @@ struct vvcg_ctx {
   DevBuf d_tu_recs, d_tu_idx;
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   DevBuf d_alfp, d_alfc;  // general-decoder ALF parameters and CTU switches
+  DevBuf d_search_reqs, d_search_cost, d_search_mode, d_search_ctus;  // CTU full search
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -1312,6 +1313,85 @@ extern "C" vvcg_status vvcg_luma_intra_search_8_dev(vvcg_ctx* ctx, const uint8_t
   k_luma_intra_search_8<<<grid, kIsrWarps * 32, 0, ctx->stream>>>(A);
   CK(cudaGetLastError(), "intra search launch");
   ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CTU full search of the GPU encoder (vvcg_ctu_search_dev).
+// ---------------------------------------------------------------------------
+// Blocks of a 32x32 CTU: (x, y, log2 w, log2 h) per slot; the slots of split
+// s are c_split_first[s] .. + c_split_count[s] - 1.
+static const uint8_t kSearchBlocks[15][4] = {
+    {0, 0, 5, 5},                                                   // none
+    {0, 0, 4, 4},  {16, 0, 4, 4}, {0, 16, 4, 4}, {16, 16, 4, 4},    // quad
+    {0, 0, 5, 4},  {0, 16, 5, 4},                                   // binary, horizontal split
+    {0, 0, 4, 5},  {16, 0, 4, 5},                                   // binary, vertical split
+    {0, 0, 5, 3},  {0, 8, 5, 4},  {0, 24, 5, 3},                    // ternary, horizontal split
+    {0, 0, 3, 5},  {8, 0, 4, 5},  {24, 0, 3, 5}};                   // ternary, vertical split
+static const uint8_t kSearchSplitFirst[6] = {0, 1, 5, 7, 9, 12};
+static const uint8_t kSearchSplitCount[6] = {1, 4, 2, 2, 3, 3};
+
+extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                           uint32_t height, uint8_t bit_depth, uint32_t lambda_q8,
+                                           const vvcg_ctu_search_req* reqs, uint32_t num_reqs,
+                                           vvcg_ctu_search_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!src || !reqs || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, requests or results");
+  if (stride < width) return fail(ctx, VVCG_INVALID_INPUT, "stride smaller than width");
+  if (bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "bit depth");
+  if (width > (1u << 20) || height > (1u << 20)) return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane larger than 2^20");
+  if (num_reqs > (1u << 24)) return fail(ctx, VVCG_LIMIT_EXCEEDED, "more than 2^24 CTUs");
+  std::vector<CostReq> blocks;
+  blocks.reserve((size_t)num_reqs * 15);
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_ctu_search_req& q = reqs[i];
+    if ((uint64_t)q.x + 32 > width || (uint64_t)q.y + 32 > height)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: CTU outside the plane", i);
+    if (!q.split_mask || q.split_mask > 0x3F) return fail(ctx, VVCG_INVALID_INPUT, "request %u: split mask", i);
+    if (q.n_cand > 6) return fail(ctx, VVCG_INVALID_INPUT, "request %u: more than 6 candidates", i);
+    for (int k = 0; k < q.n_cand; k++)
+      if (q.cand[k] > 66) return fail(ctx, VVCG_INVALID_INPUT, "request %u: candidate %d is not a mode", i, k);
+    for (int sp = 0; sp < 6; sp++) {
+      if (!(q.split_mask & (1u << sp))) continue;
+      for (int k = 0; k < kSearchSplitCount[sp]; k++) {
+        const int slot = kSearchSplitFirst[sp] + k;
+        CostReq b{};
+        b.x = q.x + kSearchBlocks[slot][0];
+        b.y = q.y + kSearchBlocks[slot][1];
+        b.log2_w = kSearchBlocks[slot][2];
+        b.log2_h = kSearchBlocks[slot][3];
+        b.n_cand = q.n_cand;
+        for (int c = 0; c < 6; c++) b.cand[c] = q.cand[c];
+        b.slot = (uint16_t)slot;
+        b.ctu = i;
+        blocks.push_back(b);
+      }
+    }
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_search_reqs.reserve(sizeof(CostReq) * blocks.size()), "cudaMalloc");
+  CK(ctx->d_search_ctus.reserve(sizeof(vvcg_ctu_search_req) * num_reqs), "cudaMalloc");
+  CK(ctx->d_search_cost.reserve(sizeof(uint32_t) * 15 * (size_t)num_reqs), "cudaMalloc");
+  CK(ctx->d_search_mode.reserve(15 * (size_t)num_reqs), "cudaMalloc");
+  // pageable sources: the copies have read them when cudaMemcpyAsync returns
+  CK(cudaMemcpyAsync(ctx->d_search_reqs.p, blocks.data(), sizeof(CostReq) * blocks.size(), cudaMemcpyHostToDevice,
+                     ctx->stream),
+     "upload");
+  CK(cudaMemcpyAsync(ctx->d_search_ctus.p, reqs, sizeof(vvcg_ctu_search_req) * num_reqs, cudaMemcpyHostToDevice,
+                     ctx->stream),
+     "upload");
+  CostArgs A{src, (int64_t)stride, (int32_t)width, (int32_t)height, bit_depth, (int32_t)blocks.size(), lambda_q8,
+             (const CostReq*)ctx->d_search_reqs.p, (uint32_t*)ctx->d_search_cost.p,
+             (uint8_t*)ctx->d_search_mode.p};
+  const uint32_t grid = (uint32_t)std::min<size_t>(blocks.size(), (size_t)ctx->num_sms * 8);
+  k_cost_search<<<grid, kIsrWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "search launch");
+  k_ctu_search_combine<<<(num_reqs + 127) / 128, 128, 0, ctx->stream>>>(
+      (const vvcg_ctu_search_req*)ctx->d_search_ctus.p, (int)num_reqs, lambda_q8,
+      (const uint32_t*)ctx->d_search_cost.p, (const uint8_t*)ctx->d_search_mode.p, res);
+  CK(cudaGetLastError(), "search launch");
+  ctx->launches += 2;
   return VVCG_OK;
 }
 
