@@ -600,6 +600,15 @@ vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t str
                                 uint8_t bit_depth, uint32_t lambda_q8, const vvcg_ctu_search_req* reqs,
                                 uint32_t num_reqs, vvcg_ctu_search_res* res);
 
+/* ---- tensor-core self-test ---------------------------------------------------- */
+
+/* One 128 x 32 x 16 bf16 tcgen05 MMA with fp32 accumulation in TMEM:
+ * d (128 x 32, row-major fp32) = a (128 x 16, row-major bf16 bits) times the
+ * transpose of b (32 x 16, row-major bf16 bits); device pointers. status
+ * (device, one word) becomes 1 if the completion wait gave up. Checks the
+ * descriptor, TMEM and completion plumbing that the CNN kernels share. */
+vvcg_status vvcg_tc_selftest_dev(vvcg_ctx* ctx, const uint16_t* a, const uint16_t* b, float* d, uint32_t* status);
+
 /* ---- general-decoder deblocking ------------------------------------------- */
 
 enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };

@@ -223,6 +223,7 @@ def lib():
         L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
+        L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -529,6 +530,22 @@ class Context:
             return None
         torch.cuda.synchronize(src.device)
         return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:len(reqs)]
+
+    # -- tensor-core self-test --
+    def tc_selftest(self, a, b):
+        """a: (128, 16), b: (32, 16) bfloat16 CUDA tensors; returns the fp32
+        (128, 32) product a @ b.T from one tcgen05 MMA, or raises Execution
+        when its completion wait gave up."""
+        import torch
+
+        d = torch.zeros((128, 32), dtype=torch.float32, device=a.device)
+        st = torch.zeros(1, dtype=torch.int32, device=a.device)
+        self._check(self._L.vvcg_tc_selftest_dev(self._h, _ptr(a.contiguous()), _ptr(b.contiguous()), _ptr(d),
+                                                 _ptr(st)))
+        torch.cuda.synchronize(a.device)
+        if int(st.item()):
+            raise Execution("tensor-core self-test: completion wait gave up")
+        return d
 
     # -- general-decoder deblocking --
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):

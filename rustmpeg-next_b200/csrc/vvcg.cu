@@ -24,6 +24,7 @@
 #include "recon.cuh"
 #include "tu.cuh"
 #include "txsearch.cuh"
+#include "umma.cuh"
 #include "vvc_tables.h"
 #include "vvcg_device.cuh"
 #include "vvcg_tables_dev.cuh"
@@ -1392,6 +1393,20 @@ extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, u
       (const uint32_t*)ctx->d_search_cost.p, (const uint8_t*)ctx->d_search_mode.p, res);
   CK(cudaGetLastError(), "search launch");
   ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tensor-core self-test (vvcg_tc_selftest_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_tc_selftest_dev(vvcg_ctx* ctx, const uint16_t* a, const uint16_t* b, float* d,
+                                            uint32_t* status) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!a || !b || !d || !status) return fail(ctx, VVCG_INVALID_INPUT, "missing buffers");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  k_umma_selftest<<<1, 128, 0, ctx->stream>>>(a, b, d, status);
+  CK(cudaGetLastError(), "self-test launch");
+  ctx->launches++;
   return VVCG_OK;
 }
 
