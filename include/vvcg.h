@@ -600,6 +600,31 @@ vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t str
                                 uint8_t bit_depth, uint32_t lambda_q8, const vvcg_ctu_search_req* reqs,
                                 uint32_t num_reqs, vvcg_ctu_search_res* res);
 
+/* ---- CNN pruner ------------------------------------------------------------- */
+
+/* Number of fp32 parameters of the CNN pruner and their layout: conv1 W
+ * [32 out][9 taps] and b[32]; conv2..4 W [32 out][32 in][9 taps] and b[32];
+ * intra head W [67][32] and b[67]; split head W [6][32] and b[6]. Taps are
+ * row-major over (dy, dx) in -1..1. */
+#define VVCG_CNN_PARAMS 30473
+#define VVCG_CNN_OUT 73 /* 67 intra-mode logits, then 6 split logits */
+
+/* Forward pass of the CNN pruner on 32x32 luma blocks of a device plane
+ * (8..12-bit samples in uint16, stride in samples) at the (x, y) positions
+ * ctu_xy (device, num_blocks pairs): input samples / (2^bit_depth - 1)
+ * rounded to bf16; conv 3x3 1->32 + ReLU (fp32, CUDA cores); 3 x conv 3x3
+ * 32->32 + ReLU on the tensor cores (bf16 operands, fp32 accumulation in
+ * TMEM, bf16 activations); global average; the two linear heads (fp32).
+ * logits: device, num_blocks x VVCG_CNN_OUT. gap (num_blocks x 32 fp32) and
+ * acts (num_blocks x 4 layers x 1024 pixels x 32 channels, bf16) are
+ * optional device outputs for training. status (device, one word) gets bit
+ * 0 when a completion wait gave up and bit 1 when a block lay outside the
+ * plane (its logits are NaN). This is the GPU encoder's pruning network;
+ * the reference has none. */
+vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                 uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy, uint32_t num_blocks,
+                                 const float* params, float* logits, float* gap, uint16_t* acts, uint32_t* status);
+
 /* ---- tensor-core self-test ---------------------------------------------------- */
 
 /* One 128 x 32 x 16 bf16 tcgen05 MMA with fp32 accumulation in TMEM:

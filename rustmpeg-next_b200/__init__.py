@@ -66,6 +66,7 @@ CTU_SEARCH_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("split_mask", "u1"
 CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), ("split", "u1"), ("cu_mode", "u1"),
                                  ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
 SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
+CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30473, 73, 67, 6
 DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
                            ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
 DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
@@ -224,6 +225,7 @@ def lib():
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
         L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
+        L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, u32, vp, vp, vp, vp, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -530,6 +532,33 @@ class Context:
             return None
         torch.cuda.synchronize(src.device)
         return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:len(reqs)]
+
+    # -- CNN pruner --
+    def cnn_forward(self, plane, bit_depth, xy, params, want_acts=False, sync=True):
+        """plane: (H, W) int16 CUDA tensor of 16-bit luma samples; xy: (n, 2)
+        int32 CUDA tensor of 32x32 block positions; params: CNN_PARAMS fp32
+        CUDA tensor. Returns (logits (n, 73), gap (n, 32), acts (n, 4, 1024,
+        32) bf16 or None) as CUDA tensors."""
+        import torch
+
+        n = int(xy.shape[0])
+        dev = plane.device
+        logits = torch.empty((n, CNN_OUT), dtype=torch.float32, device=dev)
+        gap = torch.empty((n, 32), dtype=torch.float32, device=dev)
+        acts = torch.empty((n, 4, 1024, 32), dtype=torch.bfloat16, device=dev) if want_acts else None
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        h, w = plane.shape
+        self._check(self._L.vvcg_cnn_forward_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth,
+                                                 _ptr(xy.contiguous()), n, _ptr(params), _ptr(logits), _ptr(gap),
+                                                 _ptr(acts), _ptr(st)))
+        if sync:
+            torch.cuda.synchronize(dev)
+            code = int(st.item())
+            if code & 1:
+                raise Execution("CNN forward: a tensor-core completion wait gave up")
+            if code & 2:
+                raise InvalidInput("CNN forward: a block lies outside the plane")
+        return logits, gap, acts
 
     # -- tensor-core self-test --
     def tc_selftest(self, a, b):

@@ -1,0 +1,78 @@
+"""Host side of the CNN pruner: parameter layout, initialisation, and a
+plain PyTorch fp32 restatement of the network used by the tests to check
+the tensor-core kernels (the library itself runs only its CUDA kernels).
+
+Parameter vector (fp32, CNN_PARAMS entries): conv1 W [32][9] and b[32];
+conv2..4 W [32 out][32 in][9] and b[32]; intra head W [67][32], b[67];
+split head W [6][32], b[6]. Taps are row-major over (dy, dx) in -1..1.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+CH, MODES, SPLITS = 32, 67, 6
+OFF_W1, OFF_B1 = 0, 288
+
+
+def off_w(layer):
+    return 320 + (layer - 2) * (CH * CH * 9 + CH)
+
+
+def off_b(layer):
+    return off_w(layer) + CH * CH * 9
+
+
+OFF_WI = off_w(5)
+OFF_BI = OFF_WI + MODES * CH
+OFF_WS = OFF_BI + MODES
+OFF_BS = OFF_WS + SPLITS * CH
+N_PARAMS = OFF_BS + SPLITS
+
+
+def init_params(seed=0):
+    """He-initialised weights, zero biases (fp32 numpy vector)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAMS, np.float32)
+    p[OFF_W1:OFF_W1 + 288] = rng.normal(0, np.sqrt(2 / 9), 288)
+    for layer in (2, 3, 4):
+        p[off_w(layer):off_w(layer) + CH * CH * 9] = rng.normal(0, np.sqrt(2 / (CH * 9)), CH * CH * 9)
+    p[OFF_WI:OFF_WI + MODES * CH] = rng.normal(0, np.sqrt(1 / CH), MODES * CH)
+    p[OFF_WS:OFF_WS + SPLITS * CH] = rng.normal(0, np.sqrt(1 / CH), SPLITS * CH)
+    return p
+
+
+def unpack(params):
+    """torch tensors (conv weights as [out, in, 3, 3]) from the vector."""
+    import torch
+
+    p = torch.as_tensor(params, dtype=torch.float32)
+    w1 = p[OFF_W1:OFF_W1 + 288].reshape(CH, 1, 3, 3)
+    b1 = p[OFF_B1:OFF_B1 + CH]
+    convs = [(p[off_w(layer):off_w(layer) + CH * CH * 9].reshape(CH, CH, 3, 3), p[off_b(layer):off_b(layer) + CH])
+             for layer in (2, 3, 4)]
+    wi, bi = p[OFF_WI:OFF_WI + MODES * CH].reshape(MODES, CH), p[OFF_BI:OFF_BI + MODES]
+    ws, bs = p[OFF_WS:OFF_WS + SPLITS * CH].reshape(SPLITS, CH), p[OFF_BS:OFF_BS + SPLITS]
+    return w1, b1, convs, wi, bi, ws, bs
+
+
+def reference_forward(blocks, bit_depth, params):
+    """fp32 restatement of the kernels' forward pass on (n, 32, 32) sample
+    blocks with the same bf16 roundings (input, activations of layers 1-3,
+    conv weights of layers 2-4); returns (logits (n, 73), gap (n, 32),
+    activations [a1..a4] as (n, 32, 32, 32) fp32)."""
+    import torch
+    import torch.nn.functional as F
+
+    bf = lambda t: t.to(torch.bfloat16).to(torch.float32)  # noqa: E731
+    w1, b1, convs, wi, bi, ws, bs = unpack(params)
+    x = bf(torch.as_tensor(blocks, dtype=torch.float32)[:, None] * (1.0 / ((1 << bit_depth) - 1)))
+    a = bf(F.relu(F.conv2d(x, w1, b1, padding=1)))
+    acts = [a]
+    for i, (w, b) in enumerate(convs):
+        a = F.relu(F.conv2d(a, bf(w), b, padding=1))
+        if i < 2:
+            a = bf(a)
+        acts.append(a)
+    gap = a.mean(dim=(2, 3))
+    logits = torch.cat([gap @ wi.T + bi, gap @ ws.T + bs], dim=1)
+    return logits, gap, acts

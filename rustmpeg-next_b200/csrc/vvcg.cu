@@ -13,6 +13,7 @@
 
 #include "../../include/vvcg.h"
 #include "alf_general.cuh"
+#include "cnn.cuh"
 #include "dbk_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
@@ -118,6 +119,7 @@ struct vvcg_ctx {
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   DevBuf d_alfp, d_alfc;  // general-decoder ALF parameters and CTU switches
   DevBuf d_search_reqs, d_search_cost, d_search_mode, d_search_ctus;  // CTU full search
+  DevBuf d_cnn_pack;  // packed bf16 convolution weights of the CNN
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -1392,6 +1394,39 @@ extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, u
       (const vvcg_ctu_search_req*)ctx->d_search_ctus.p, (int)num_reqs, lambda_q8,
       (const uint32_t*)ctx->d_search_cost.p, (const uint8_t*)ctx->d_search_mode.p, res);
   CK(cudaGetLastError(), "search launch");
+  ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CNN pruner forward pass (vvcg_cnn_forward_dev).
+// ---------------------------------------------------------------------------
+static_assert(kCnnParams == VVCG_CNN_PARAMS && kCnnOut == VVCG_CNN_OUT, "CNN layout");
+extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                            uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy,
+                                            uint32_t num_blocks, const float* params, float* logits, float* gap,
+                                            uint16_t* acts, uint32_t* status) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_blocks) return VVCG_OK;
+  if (!plane || !ctu_xy || !params || !logits || !status)
+    return fail(ctx, VVCG_INVALID_INPUT, "missing plane, positions, parameters, logits or status");
+  if (stride < width || bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
+  if (width > (1u << 20) || height > (1u << 20) || num_blocks > (1u << 24))
+    return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane or block count too large");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  static bool attr_set[64] = {};
+  if (ctx->device < 64 && !attr_set[ctx->device]) {
+    CK(cudaFuncSetAttribute(k_cnn_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, kCnnSmem), "smem attribute");
+    attr_set[ctx->device] = true;
+  }
+  CK(ctx->d_cnn_pack.reserve(3 * kPackL), "cudaMalloc");
+  k_cnn_pack<<<(3 * kCnnConvW + 255) / 256, 256, 0, ctx->stream>>>(params, (uint16_t*)ctx->d_cnn_pack.p, false);
+  CK(cudaGetLastError(), "cnn pack launch");
+  CnnFwdArgs A{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
+               ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, logits, gap, acts, status};
+  const uint32_t grid = std::min<uint32_t>(num_blocks, (uint32_t)ctx->num_sms);
+  k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "cnn launch");
   ctx->launches += 2;
   return VVCG_OK;
 }

@@ -15,3 +15,36 @@ def test_tensor_core_selftest_matches_fp32_matmul(ctx, pkg):
     d = ctx.tc_selftest(a.cuda().view(torch.int16), b.cuda().view(torch.int16)).cpu()
     want = a.float() @ b.float().T
     assert torch.allclose(d, want, rtol=1e-5, atol=1e-5), (d - want).abs().max()
+
+
+def _blocks(n, bd, seed):
+    import torch
+    from rustmpeg_next_b200 import synth
+
+    y, _, _ = synth.value_noise_frame(32 * 8, max(64, 32 * ((n + 7) // 8)), 10, frame=seed)
+    y = y.astype(np.int32)
+    y = y << (bd - 10) if bd >= 10 else y >> (10 - bd)
+    plane = np.ascontiguousarray(y.astype(np.uint16))
+    xy = np.array([[32 * (i % 8), 32 * (i // 8)] for i in range(n)], np.int32)
+    blocks = np.stack([plane[yy:yy + 32, xx:xx + 32] for xx, yy in xy]).astype(np.float32)
+    return torch.from_numpy(plane.view(np.int16)).cuda(), torch.from_numpy(xy).cuda(), blocks
+
+
+@pytest.mark.parametrize("n,bd,seed", [(1, 10, 1), (37, 10, 2), (300, 8, 3)])
+def test_cnn_forward_matches_fp32_reference(ctx, pkg, n, bd, seed):
+    import torch
+    from rustmpeg_next_b200 import cnn
+
+    plane, xy, blocks = _blocks(n, bd, seed)
+    params = cnn.init_params(seed)
+    logits, gap, acts = ctx.cnn_forward(plane, bd, xy, torch.from_numpy(params).cuda(), want_acts=True)
+    ref_logits, ref_gap, ref_acts = cnn.reference_forward(blocks, bd, params)
+    # layer 1 is fp32 on both sides: equal up to summation order and bf16 ties
+    a1 = acts[:, 0].float().cpu().reshape(n, 32, 32, 32).permute(0, 3, 1, 2)
+    assert (a1 - ref_acts[0]).abs().max() <= 1e-2 * max(1.0, float(ref_acts[0].abs().max()))
+    for l in (1, 2, 3):
+        got = acts[:, l].float().cpu().reshape(n, 32, 32, 32).permute(0, 3, 1, 2)
+        err = (got - ref_acts[l]).abs().max() / max(1e-6, float(ref_acts[l].abs().max()))
+        assert err < 2e-2, (l, float(err))
+    assert torch.allclose(gap.cpu(), ref_gap, rtol=2e-2, atol=2e-3), (gap.cpu() - ref_gap).abs().max()
+    assert torch.allclose(logits.cpu(), ref_logits, rtol=2e-2, atol=2e-2), (logits.cpu() - ref_logits).abs().max()
