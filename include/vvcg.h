@@ -625,6 +625,23 @@ vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t 
                                  uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy, uint32_t num_blocks,
                                  const float* params, float* logits, float* gap, uint16_t* acts, uint32_t* status);
 
+/* One training step of the CNN pruner on num_blocks 32x32 blocks (the batch)
+ * with labels (device, num_blocks x (intra mode 0..66, split type 0..5)):
+ * the forward pass, the mean softmax cross-entropy of both heads, the
+ * backward pass (input gradients of the 3x3 32->32 layers on the tensor
+ * cores, weight gradients on the CUDA cores), written to grads (device,
+ * VVCG_CNN_PARAMS fp32) and loss (device, one fp32); then, when lr > 0, an
+ * Adam update (beta 0.9 / 0.999, eps 1e-8, bias correction for `step`,
+ * counted from 1) of params with the moments adam_m / adam_v (device,
+ * VVCG_CNN_PARAMS fp32 each). status as for vvcg_cnn_forward_dev; blocks
+ * outside the plane or with a label out of range are skipped and flag bit
+ * 1. Asynchronous on the context's stream. */
+vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                    uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy,
+                                    const uint8_t* labels, uint32_t num_blocks, float* params, float* adam_m,
+                                    float* adam_v, uint32_t step, float lr, float* grads, float* loss,
+                                    uint32_t* status);
+
 /* ---- tensor-core self-test ---------------------------------------------------- */
 
 /* One 128 x 32 x 16 bf16 tcgen05 MMA with fp32 accumulation in TMEM:
@@ -633,6 +650,20 @@ vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t 
  * (device, one word) becomes 1 if the completion wait gave up. Checks the
  * descriptor, TMEM and completion plumbing that the CNN kernels share. */
 vvcg_status vvcg_tc_selftest_dev(vvcg_ctx* ctx, const uint16_t* a, const uint16_t* b, float* d, uint32_t* status);
+
+/* The CTU search of vvcg_ctu_search_dev with device-resident positions
+ * (ctu_xy: num_ctus (x, y) pairs) and, with logits (device, num_ctus x
+ * VVCG_CNN_OUT from vvcg_cnn_forward_dev), pruned by the CNN: the top_modes
+ * most probable intra modes are the candidates of every block and the
+ * top_splits most probable split types are evaluated; a head whose largest
+ * softmax probability is below threshold keeps its full set. logits = NULL
+ * is the full search. A CTU outside the plane gets cost UINT32_MAX and
+ * split 0xFF. All on the context's stream, no host round trip. */
+vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                       uint32_t height, uint8_t bit_depth, uint32_t lambda_q8,
+                                       const uint32_t* ctu_xy, uint32_t num_ctus, const float* logits,
+                                       uint32_t top_modes, uint32_t top_splits, float threshold,
+                                       vvcg_ctu_search_res* res);
 
 /* ---- general-decoder deblocking ------------------------------------------- */
 

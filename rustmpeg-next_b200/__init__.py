@@ -224,8 +224,11 @@ def lib():
         L.vvcg_alf_general_dev.argtypes = [vp, vp, vp, vp, u32, u32, u32, u32, u8, u32, u32, vp, vp]
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
+        L.vvcg_ctu_search_pruned_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, u32, u32, C.c_float, vp]
         L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
         L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, u32, vp, vp, vp, vp, vp]
+        L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
+                                              vp, vp, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -560,6 +563,32 @@ class Context:
                 raise InvalidInput("CNN forward: a block lies outside the plane")
         return logits, gap, acts
 
+    def cnn_train_step(self, plane, bit_depth, xy, labels, params, adam_m=None, adam_v=None, step=0, lr=0.0,
+                       sync=True):
+        """One training step on the blocks xy ((n, 2) int32 CUDA) with labels
+        ((n, 2) uint8 CUDA: intra mode, split type). Updates params (and the
+        Adam moments) in place when lr > 0. Returns (loss, grads) CUDA
+        tensors (one fp32; CNN_PARAMS fp32)."""
+        import torch
+
+        dev = plane.device
+        grads = torch.empty(CNN_PARAMS, dtype=torch.float32, device=dev)
+        loss = torch.empty(1, dtype=torch.float32, device=dev)
+        st = torch.zeros(1, dtype=torch.int32, device=dev)
+        h, w = plane.shape
+        self._check(self._L.vvcg_cnn_train_step_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth,
+                                                    _ptr(xy.contiguous()), _ptr(labels.contiguous()), int(xy.shape[0]),
+                                                    _ptr(params), _ptr(adam_m), _ptr(adam_v), step, lr, _ptr(grads),
+                                                    _ptr(loss), _ptr(st)))
+        if sync:
+            torch.cuda.synchronize(dev)
+            code = int(st.item())
+            if code & 1:
+                raise Execution("CNN training: a tensor-core completion wait gave up")
+            if code & 2:
+                raise InvalidInput("CNN training: a block outside the plane or a label out of range")
+        return loss, grads
+
     # -- tensor-core self-test --
     def tc_selftest(self, a, b):
         """a: (128, 16), b: (32, 16) bfloat16 CUDA tensors; returns the fp32
@@ -575,6 +604,26 @@ class Context:
         if int(st.item()):
             raise Execution("tensor-core self-test: completion wait gave up")
         return d
+
+    def ctu_search_xy(self, src, bit_depth, lambda_q8, xy, logits=None, top_modes=3, top_splits=2,
+                      threshold=0.4, out=None, sync=True):
+        """The CTU search over device positions xy ((n, 2) int32 CUDA), full
+        (logits None) or pruned by the CNN's logits ((n, 73) fp32 CUDA).
+        Returns CTU_SEARCH_RES_DTYPE results, or fills the CUDA uint8 tensor
+        out (n x 36 bytes) without synchronising when sync is False."""
+        import torch
+
+        n = int(xy.shape[0])
+        h, w = src.shape
+        dst = out if out is not None else torch.empty(max(n, 1) * CTU_SEARCH_RES_DTYPE.itemsize, dtype=torch.uint8,
+                                                      device=src.device)
+        self._check(self._L.vvcg_ctu_search_pruned_dev(self._h, _ptr(src), src.stride(0), w, h, bit_depth, lambda_q8,
+                                                       _ptr(xy.contiguous()), n, _ptr(logits), top_modes, top_splits,
+                                                       threshold, _ptr(dst)))
+        if not sync:
+            return None
+        torch.cuda.synchronize(src.device)
+        return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:n]
 
     # -- general-decoder deblocking --
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):

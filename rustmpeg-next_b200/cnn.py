@@ -45,7 +45,7 @@ def unpack(params):
     """torch tensors (conv weights as [out, in, 3, 3]) from the vector."""
     import torch
 
-    p = torch.as_tensor(params, dtype=torch.float32)
+    p = params if isinstance(params, torch.Tensor) else torch.as_tensor(params, dtype=torch.float32)
     w1 = p[OFF_W1:OFF_W1 + 288].reshape(CH, 1, 3, 3)
     b1 = p[OFF_B1:OFF_B1 + CH]
     convs = [(p[off_w(layer):off_w(layer) + CH * CH * 9].reshape(CH, CH, 3, 3), p[off_b(layer):off_b(layer) + CH])
@@ -69,10 +69,72 @@ def reference_forward(blocks, bit_depth, params):
     a = bf(F.relu(F.conv2d(x, w1, b1, padding=1)))
     acts = [a]
     for i, (w, b) in enumerate(convs):
-        a = F.relu(F.conv2d(a, bf(w), b, padding=1))
+        wq = w + (bf(w) - w).detach()  # bf16 values, fp32 weight gradients
+        a = F.relu(F.conv2d(a, wq, b, padding=1))
         if i < 2:
             a = bf(a)
         acts.append(a)
     gap = a.mean(dim=(2, 3))
     logits = torch.cat([gap @ wi.T + bi, gap @ ws.T + bs], dim=1)
     return logits, gap, acts
+
+
+def reference_loss_and_grads(blocks, labels, bit_depth, params):
+    """Mean cross-entropy of both heads and its gradient w.r.t. the
+    parameter vector, by autograd through reference_forward (fp32 with the
+    kernels' bf16 roundings)."""
+    import torch
+
+    p = torch.tensor(np.asarray(params, np.float32), requires_grad=True)
+    logits, _, _ = reference_forward(blocks, bit_depth, p)
+    lab = torch.as_tensor(np.asarray(labels), dtype=torch.long)
+    loss = torch.nn.functional.cross_entropy(logits[:, :MODES], lab[:, 0]) + \
+        torch.nn.functional.cross_entropy(logits[:, MODES:], lab[:, 1])
+    loss.backward()
+    return float(loss.detach()), p.grad.numpy()
+
+
+def search_lambda_q8(qp):
+    """lambda of the CTU search in 1/256 units: sqrt(0.57 * 2^((qp - 12) / 3))."""
+    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0))))
+
+
+def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37), seed=0):
+    """Labelled 32x32 luma blocks for the pruner: value-noise 10-bit frames
+    (the 1080p synthetic content), every CTU labelled by the full search at
+    each QP (intra mode of the unsplit CU, best split type). Returns a list
+    of (plane (H, W) int16 CUDA, xy (n, 2) int32 CUDA, labels (n, 2) uint8
+    CUDA, qp) per frame and QP."""
+    import torch
+
+    from . import synth
+
+    out = []
+    xs, ys = np.meshgrid(np.arange(0, width - 31, 32), np.arange(0, height - 31, 32))
+    xy = torch.from_numpy(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)).cuda()
+    for f in range(n_frames):
+        y, _, _ = synth.value_noise_frame(width, height, 10, frame=seed * 1000 + f)
+        plane = torch.from_numpy(np.ascontiguousarray(y.astype(np.uint16)).view(np.int16)).cuda()
+        for qp in qps:
+            r = ctx.ctu_search_xy(plane, 10, search_lambda_q8(qp), xy)
+            lab = torch.from_numpy(np.stack([r["cu_mode"], r["split"]], 1).astype(np.uint8)).cuda()
+            out.append((plane, xy, lab, qp))
+    return out
+
+
+def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None):
+    """Adam on the labelled blocks of training_set (batches drawn from one
+    frame at a time); returns (params CUDA tensor, losses)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    p = torch.from_numpy(init_params(seed) if params is None else params).cuda()
+    m, v = torch.zeros_like(p), torch.zeros_like(p)
+    losses = []
+    for step in range(1, steps + 1):
+        plane, xy, lab, _ = data[int(rng.integers(0, len(data)))]
+        idx = torch.from_numpy(rng.choice(xy.shape[0], min(batch, xy.shape[0]), replace=False)).cuda()
+        loss, _ = ctx.cnn_train_step(plane, 10, xy[idx], lab[idx], p, m, v, step, lr, sync=False)
+        losses.append(loss)
+    torch.cuda.synchronize()
+    return p, [float(x.item()) for x in losses]

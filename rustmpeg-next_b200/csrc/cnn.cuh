@@ -251,3 +251,283 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_con
 }
 
 }  // namespace vvcg
+
+namespace vvcg {
+
+// ---------------------------------------------------------------- backward --
+//
+// One CTA per block (persistent). From the forward's activations a1..a4,
+// gap and logits: the head gradients, then per layer l = 4, 3, 2 the
+// gradient dZ_l (w.r.t. the layer's pre-activation) held as a bf16 image:
+//  * its input gradient dA_{l-1} = conv(dZ_l, flipped W_l) is 144 tcgen05
+//    MMAs exactly as in the forward pass (the taps of the transposed
+//    convolution are the mirrored address offsets);
+//  * meanwhile the CUDA cores form the weight gradient
+//    dW_l[co][ci][tap] = sum_p dZ_l[p][co] a_{l-1}[p + tap][ci] (the 32
+//    channels of one tap are too few rows for a tensor-core operand) and
+//    the bias gradient;
+//  * the epilogue masks dA_{l-1} by a_{l-1} > 0 into dZ_{l-1}, in place of
+//    a_{l-1}.
+// Layer 1's weight gradient uses the bf16 input. Gradients and the loss
+// accumulate in the CTA's own slice of `partial` (no atomics); a second
+// kernel sums the slices.
+struct CnnBwdArgs {
+  const uint16_t* plane;
+  int64_t stride;
+  int32_t width, height, maxv, n;
+  const uint32_t* ctu_xy;
+  const uint8_t* labels;  // n x (mode, split)
+  const float* params;
+  const uint16_t* packT;  // flipped packed weights of layers 2..4
+  const float* logits;
+  const float* gap;
+  const uint16_t* acts;
+  float* partial;  // [gridDim.x][kCnnParams + 1]: gradients, then the loss sum
+  float inv_batch;
+  uint32_t* status;
+};
+constexpr int kCnnBwdMisc = (1024 + 32 + 32 * 8 + 96) * 4;
+constexpr int kCnnBwdSmem = 2 * kImg + kPackL + kCnnBwdMisc + 64;
+
+// Loads activation image `layer` (0..3) of block blk from global into an
+// image buffer (interior only; the halo stays zero).
+__device__ __forceinline__ void cnn_load_act(uint8_t* img, const uint16_t* acts, int blk, int layer) {
+  const uint4* src = (const uint4*)(acts + ((size_t)blk * 4 + layer) * 1024 * 32);
+  for (int i = threadIdx.x; i < 1024 * 4; i += kCnnThreads) {
+    const int p = i >> 2, g = i & 3;
+    *(uint4*)(img + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = src[i];
+  }
+}
+
+__global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_constant__ CnnBwdArgs A) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* P = smem;
+  uint8_t* Q = smem + kImg;
+  uint8_t* Wt = smem + 2 * kImg;
+  float* xin = (float*)(Wt + kPackL);  // bf16-rounded normalised input
+  float* dgap = xin + 1024;
+  float* dbp = dgap + 32;   // [8 warps][32] bias-gradient partials
+  float* dlog = dbp + 256;  // [73] logit gradients (+ pad)
+  uint64_t* mbar = (uint64_t*)(dlog + 96);
+  uint32_t* tslot = (uint32_t*)(mbar + 1);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  float* part = A.partial + (size_t)blockIdx.x * (kCnnParams + 1);
+  for (int i = t; i < kCnnParams + 1; i += kCnnThreads) part[i] = 0.0f;
+  for (int i = t; i < 2 * kImg / 16; i += kCnnThreads) ((uint4*)P)[i] = make_uint4(0, 0, 0, 0);
+  if (warp == 0) {
+    tmem_alloc(tslot, 256);
+    tmem_relinquish();
+  }
+  if (t == 0) {
+    mbar_init(mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  uint32_t phase = 0;
+  bool ok = true;
+  const int co4 = t >> 5, ci = t & 31;  // weight-gradient ownership: 4 output channels x 1 input channel
+
+  for (int blk = blockIdx.x; blk < A.n && ok; blk += gridDim.x) {
+    const uint32_t ux = A.ctu_xy[2 * blk], uy = A.ctu_xy[2 * blk + 1];
+    if (ux > (uint32_t)A.width - 32 || uy > (uint32_t)A.height - 32 || A.width < 32 || A.height < 32 ||
+        A.labels[2 * blk] >= kCnnModes || A.labels[2 * blk + 1] >= kCnnSplits) {
+      if (t == 0) atomicOr(A.status, 2u);  // skipped: outside the plane or a label out of range
+      continue;
+    }
+    // heads: softmax cross-entropy of both heads, mean over the batch
+    if (warp == 0 || warp == 1) {
+      const float* lg = A.logits + (size_t)blk * kCnnOut;
+      const int n_out = warp == 0 ? kCnnModes : kCnnSplits, base = warp == 0 ? 0 : kCnnModes;
+      const int label = A.labels[2 * blk + warp];
+      float mx = -INFINITY;
+      for (int j = lane; j < n_out; j += 32) mx = fmaxf(mx, lg[base + j]);
+      for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+      float se = 0.0f;
+      for (int j = lane; j < n_out; j += 32) se += __expf(lg[base + j] - mx);
+      for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xFFFFFFFFu, se, o);
+      for (int j = lane; j < n_out; j += 32) {
+        const float pj = __expf(lg[base + j] - mx) / se;
+        dlog[base + j] = (pj - (j == label ? 1.0f : 0.0f)) * A.inv_batch;
+      }
+      if (lane == 0) atomicAdd(&part[kCnnParams], (logf(se) + mx - lg[base + label]) * A.inv_batch);
+    }
+    const float inv = 1.0f / (float)A.maxv;
+    const int bx = (int)ux, by = (int)uy;
+    for (int i = t; i < 1024; i += kCnnThreads)
+      xin[i] = bf2f(f2bf((float)A.plane[(int64_t)(by + (i >> 5)) * A.stride + bx + (i & 31)] * inv));
+    __syncthreads();
+    const float* gp = A.gap + (size_t)blk * 32;
+    if (t < 32) {
+      float s = 0.0f;
+      for (int j = 0; j < kCnnModes; j++) s = fmaf(A.params[kOffWi + j * 32 + t], dlog[j], s);
+      for (int j = 0; j < kCnnSplits; j++) s = fmaf(A.params[kOffWs + j * 32 + t], dlog[kCnnModes + j], s);
+      dgap[t] = s;
+    }
+    for (int i = t; i < kCnnOut * 32; i += kCnnThreads) {
+      const int j = i >> 5, c = i & 31;
+      part[(j < kCnnModes ? kOffWi : kOffWs - kCnnModes * 32) + i] += dlog[j] * gp[c];
+    }
+    if (t < kCnnOut) part[t < kCnnModes ? kOffBi + t : kOffBs + t - kCnnModes] += dlog[t];
+    __syncthreads();
+    // dZ4 into P (a4 > 0 passes dgap / 1024), a3 into Q
+    {
+      const uint4* a4 = (const uint4*)(A.acts + ((size_t)blk * 4 + 3) * 1024 * 32);
+      float dbs[8];
+      for (int k = 0; k < 8; k++) dbs[k] = 0.0f;
+      for (int i = t; i < 1024 * 4; i += kCnnThreads) {
+        const int p = i >> 2, g = i & 3;  // g is fixed per thread (stride 256)
+        const uint4 av = a4[i];
+        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
+        uint32_t o[4];
+        for (int k = 0; k < 4; k++) {
+          const float d0 = (aw[k] & 0xFFFFu) && !(aw[k] & 0x8000u) ? dgap[g * 8 + 2 * k] * (1.0f / 1024.0f) : 0.0f;
+          const float d1 = (aw[k] >> 16) && !(aw[k] & 0x80000000u) ? dgap[g * 8 + 2 * k + 1] * (1.0f / 1024.0f) : 0.0f;
+          dbs[2 * k] += d0;
+          dbs[2 * k + 1] += d1;
+          o[k] = (uint32_t)f2bf(d0) | ((uint32_t)f2bf(d1) << 16);
+        }
+        *(uint4*)(P + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = make_uint4(o[0], o[1], o[2], o[3]);
+      }
+      // the 64 threads with the same g hold that plane's sums
+      for (int k = 0; k < 8; k++) atomicAdd(&part[cnn_off_b(4) + (t & 3) * 8 + k], dbs[k]);
+    }
+    cnn_load_act(Q, A.acts, blk, 2);
+    uint8_t* dz = P;  // dZ_l
+    uint8_t* act = Q; // a_{l-1}, becomes dZ_{l-1}
+    for (int layer = 4; layer >= 2 && ok; layer--) {
+      const int li = layer - 2;
+      for (int i = t; i < kPackL / 16; i += kCnnThreads)
+        ((uint4*)Wt)[i] = ((const uint4*)(A.packT + (size_t)li * (kPackL / 2)))[i];
+      fence_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      if (t == 0) cnn_issue_layer(tmem, smem_u32(dz), smem_u32(Wt), mbar);
+      // weight gradient on the CUDA cores while the tensor cores run
+      {
+        float acc[4][9];
+        for (int k = 0; k < 4; k++)
+          for (int tp = 0; tp < 9; tp++) acc[k][tp] = 0.0f;
+        const uint8_t* ap = act + (ci >> 3) * kPlane + (ci & 7) * 2;
+        const uint8_t* zp = dz + (co4 >> 1) * kPlane + (co4 & 1) * 8;
+        for (int iy = 0; iy < 32; iy++) {
+          float w[3][3];
+          for (int dy = 0; dy < 3; dy++)
+            for (int dx = 0; dx < 2; dx++) w[dy][dx + 1] = bf2f(*(const uint16_t*)(ap + ((iy + dy) * kImgW + dx) * 16));
+          for (int ix = 0; ix < 32; ix++) {
+            for (int dy = 0; dy < 3; dy++) {
+              w[dy][0] = w[dy][1];
+              w[dy][1] = w[dy][2];
+              w[dy][2] = bf2f(*(const uint16_t*)(ap + ((iy + dy) * kImgW + ix + 2) * 16));
+            }
+            const uint2 zv = *(const uint2*)(zp + ((iy + 1) * kImgW + ix + 1) * 16);
+            const float z[4] = {bf2f(zv.x & 0xFFFFu), bf2f(zv.x >> 16), bf2f(zv.y & 0xFFFFu), bf2f(zv.y >> 16)};
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+#pragma unroll
+              for (int tp = 0; tp < 9; tp++) acc[k][tp] = fmaf(z[k], w[tp / 3][tp % 3], acc[k][tp]);
+          }
+        }
+        float* gw = part + cnn_off_w(layer);
+        for (int k = 0; k < 4; k++)
+          for (int tp = 0; tp < 9; tp++) gw[((co4 * 4 + k) * kCnnCh + ci) * 9 + tp] += acc[k][tp];
+      }
+      ok = __syncthreads_and(mbar_wait(mbar, phase, 1u << 26));
+      phase ^= 1;
+      tc_fence_after();
+      if (!ok) break;
+      // epilogue: dZ_{l-1} = dA_{l-1} where a_{l-1} > 0, in place of a_{l-1}
+      float dbs[32];
+      for (int c = 0; c < 32; c++) dbs[c] = 0.0f;
+      const int q = warp & 3;
+      for (int k = 0; k < 4; k++) {
+        const int tile = (warp >> 2) + 2 * k;
+        const int m = 32 * q + lane, j = m >> 3, r = m & 7;
+        const int iy = 16 * (tile >> 2) + j, ix = 8 * (tile & 3) + r;
+        float v[32];
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + tile * 32, v);
+        tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + tile * 32 + 16, v + 16);
+        const int off = ((iy + 1) * kImgW + ix + 1) * 16;
+        for (int g = 0; g < 4; g++) {
+          uint4 av = *(const uint4*)(act + g * kPlane + off);
+          uint32_t aw[4] = {av.x, av.y, av.z, av.w}, o[4];
+          for (int k2 = 0; k2 < 4; k2++) {
+            const int c = g * 8 + 2 * k2;
+            const float d0 = ((aw[k2] & 0xFFFFu) && !(aw[k2] & 0x8000u)) ? v[c] : 0.0f;
+            const float d1 = ((aw[k2] >> 16) && !(aw[k2] & 0x80000000u)) ? v[c + 1] : 0.0f;
+            dbs[c] += d0;
+            dbs[c + 1] += d1;
+            o[k2] = (uint32_t)f2bf(d0) | ((uint32_t)f2bf(d1) << 16);
+          }
+          *(uint4*)(act + g * kPlane + off) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+      }
+      for (int c = 0; c < 32; c++) {
+        float s = dbs[c];
+        for (int o2 = 16; o2 > 0; o2 >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o2);
+        if (lane == 0) dbp[warp * 32 + c] = s;
+      }
+      tc_fence_before();
+      __syncthreads();
+      if (t < 32) {
+        float s = 0.0f;
+        for (int w2 = 0; w2 < 8; w2++) s += dbp[w2 * 32 + t];
+        part[layer == 2 ? kOffB1 + t : cnn_off_b(layer - 1) + t] += s;
+      }
+      // next layer: the old dZ_l buffer takes a_{l-2}
+      if (layer > 2) cnn_load_act(dz, A.acts, blk, layer - 3);
+      uint8_t* tmp = dz;
+      dz = act;
+      act = tmp;
+      __syncthreads();
+    }
+    if (!ok) break;
+    // layer 1: dW1[co][tap] = sum_p dZ1[p][co] x[p + tap] (dZ1 is in dz)
+    for (int o = t; o < 288; o += kCnnThreads) {
+      const int co = o / 9, tp = o % 9, dy = tp / 3 - 1, dx = tp % 3 - 1;
+      const uint8_t* zp = dz + (co >> 3) * kPlane + (co & 7) * 2;
+      float s = 0.0f;
+      for (int p = 0; p < 1024; p++) {
+        const int y = (p >> 5) + dy, x = (p & 31) + dx;
+        if (y < 0 || y >= 32 || x < 0 || x >= 32) continue;
+        s = fmaf(bf2f(*(const uint16_t*)(zp + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16)), xin[y * 32 + x], s);
+      }
+      part[kOffW1 + co * 9 + tp] += s;
+    }
+    __syncthreads();
+  }
+  if (!ok && t == 0) atomicOr(A.status, 1u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// grads[i] = sum over the CTA slices; loss[0] = sum of the loss slots.
+__global__ void k_cnn_reduce(const float* __restrict__ partial, int slices, float* __restrict__ grads,
+                             float* __restrict__ loss) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > kCnnParams) return;
+  float s = 0.0f;
+  for (int k = 0; k < slices; k++) s += partial[(size_t)k * (kCnnParams + 1) + i];
+  if (i < kCnnParams)
+    grads[i] = s;
+  else
+    loss[0] = s;
+}
+
+// Adam (bias-corrected) on the fp32 parameter vector.
+__global__ void k_cnn_adam(float* __restrict__ params, const float* __restrict__ grads, float* __restrict__ m,
+                           float* __restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kCnnParams) return;
+  const float g = grads[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * g, vi = b2 * v[i] + (1.0f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace vvcg

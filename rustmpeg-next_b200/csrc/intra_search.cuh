@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(kIsrWarps * 32) k_cost_search(const __grid_con
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   for (int q = blockIdx.x; q < A.n; q += gridDim.x) {
     const CostReq R = A.reqs[q];
+    if (R.log2_w == 0) continue;  // an unused slot (pruned search)
     const int w = 1 << R.log2_w, h = 1 << R.log2_h, bx = (int)R.x, by = (int)R.y;
     for (int i = t; i < w * h; i += blockDim.x) S.src[i] = A.src[(int64_t)(by + i / w) * A.stride + bx + (i % w)];
     isr_prepare(S, A.src, A.stride, A.width, A.height, bx, by, w, h, A.bd, false, true);

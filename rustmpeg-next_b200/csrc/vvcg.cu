@@ -18,6 +18,7 @@
 #include "enc.cuh"
 #include "filters.cuh"
 #include "intra_search.cuh"
+#include "prune.cuh"
 #include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
@@ -119,7 +120,8 @@ struct vvcg_ctx {
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   DevBuf d_alfp, d_alfc;  // general-decoder ALF parameters and CTU switches
   DevBuf d_search_reqs, d_search_cost, d_search_mode, d_search_ctus;  // CTU full search
-  DevBuf d_cnn_pack;  // packed bf16 convolution weights of the CNN
+  DevBuf d_cnn_pack, d_cnn_packT;  // packed bf16 convolution weights of the CNN (forward / transposed)
+  DevBuf d_cnn_acts, d_cnn_logits, d_cnn_gap, d_cnn_partial;  // CNN training workspace
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -1399,6 +1401,45 @@ extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, u
 }
 
 // ---------------------------------------------------------------------------
+// CTU search from device positions, full or CNN-pruned (vvcg_ctu_search_pruned_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride,
+                                                  uint32_t width, uint32_t height, uint8_t bit_depth,
+                                                  uint32_t lambda_q8, const uint32_t* ctu_xy, uint32_t num_ctus,
+                                                  const float* logits, uint32_t top_modes, uint32_t top_splits,
+                                                  float threshold, vvcg_ctu_search_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_ctus) return VVCG_OK;
+  if (!src || !ctu_xy || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, positions or results");
+  if (stride < width || bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
+  if (top_modes < 1 || top_modes > 6 || top_splits < 1 || top_splits > 6)
+    return fail(ctx, VVCG_INVALID_INPUT, "top_modes and top_splits must be 1..6");
+  if (width > (1u << 20) || height > (1u << 20) || num_ctus > (1u << 24))
+    return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane or CTU count too large");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const size_t nb = (size_t)num_ctus * 15;
+  CK(ctx->d_search_reqs.reserve(sizeof(CostReq) * nb), "cudaMalloc");
+  CK(ctx->d_search_ctus.reserve(sizeof(vvcg_ctu_search_req) * num_ctus), "cudaMalloc");
+  CK(ctx->d_search_cost.reserve(sizeof(uint32_t) * nb), "cudaMalloc");
+  CK(ctx->d_search_mode.reserve(nb), "cudaMalloc");
+  k_prune_requests<<<(num_ctus + 127) / 128, 128, 0, ctx->stream>>>(
+      logits, ctu_xy, (int)num_ctus, (int)width, (int)height, (int)top_modes, (int)top_splits, threshold,
+      (vvcg_ctu_search_req*)ctx->d_search_ctus.p, (CostReq*)ctx->d_search_reqs.p);
+  CK(cudaGetLastError(), "prune launch");
+  CostArgs A{src, (int64_t)stride, (int32_t)width, (int32_t)height, bit_depth, (int32_t)nb, lambda_q8,
+             (const CostReq*)ctx->d_search_reqs.p, (uint32_t*)ctx->d_search_cost.p,
+             (uint8_t*)ctx->d_search_mode.p};
+  k_cost_search<<<(uint32_t)std::min<size_t>(nb, (size_t)ctx->num_sms * 8), kIsrWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "search launch");
+  k_ctu_search_combine<<<(num_ctus + 127) / 128, 128, 0, ctx->stream>>>(
+      (const vvcg_ctu_search_req*)ctx->d_search_ctus.p, (int)num_ctus, lambda_q8,
+      (const uint32_t*)ctx->d_search_cost.p, (const uint8_t*)ctx->d_search_mode.p, res);
+  CK(cudaGetLastError(), "search launch");
+  ctx->launches += 3;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // CNN pruner forward pass (vvcg_cnn_forward_dev).
 // ---------------------------------------------------------------------------
 static_assert(kCnnParams == VVCG_CNN_PARAMS && kCnnOut == VVCG_CNN_OUT, "CNN layout");
@@ -1428,6 +1469,66 @@ extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane
   k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(A);
   CK(cudaGetLastError(), "cnn launch");
   ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CNN pruner training step (vvcg_cnn_train_step_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride,
+                                               uint32_t width, uint32_t height, uint8_t bit_depth,
+                                               const uint32_t* ctu_xy, const uint8_t* labels, uint32_t num_blocks,
+                                               float* params, float* adam_m, float* adam_v, uint32_t step, float lr,
+                                               float* grads, float* loss, uint32_t* status) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_blocks) return VVCG_OK;
+  if (!plane || !ctu_xy || !labels || !params || !grads || !loss || !status)
+    return fail(ctx, VVCG_INVALID_INPUT, "missing buffers");
+  if (lr > 0.0f && (!adam_m || !adam_v || step == 0))
+    return fail(ctx, VVCG_INVALID_INPUT, "an update needs the Adam moments and a step count from 1");
+  if (stride < width || bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
+  if (num_blocks > 65536) return fail(ctx, VVCG_LIMIT_EXCEEDED, "more than 65536 blocks in one step");
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  static bool attr_set[64] = {};
+  if (ctx->device < 64 && !attr_set[ctx->device]) {
+    CK(cudaFuncSetAttribute(k_cnn_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, kCnnSmem), "smem attribute");
+    CK(cudaFuncSetAttribute(k_cnn_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, kCnnBwdSmem),
+       "smem attribute");
+    attr_set[ctx->device] = true;
+  }
+  const uint32_t grid = std::min<uint32_t>(num_blocks, (uint32_t)ctx->num_sms);
+  CK(ctx->d_cnn_pack.reserve(3 * kPackL), "cudaMalloc");
+  CK(ctx->d_cnn_packT.reserve(3 * kPackL), "cudaMalloc");
+  CK(ctx->d_cnn_acts.reserve((size_t)num_blocks * 4 * 1024 * 32 * 2), "cudaMalloc");
+  CK(ctx->d_cnn_logits.reserve((size_t)num_blocks * kCnnOut * 4), "cudaMalloc");
+  CK(ctx->d_cnn_gap.reserve((size_t)num_blocks * 32 * 4), "cudaMalloc");
+  CK(ctx->d_cnn_partial.reserve((size_t)grid * (kCnnParams + 1) * 4), "cudaMalloc");
+  k_cnn_pack<<<(3 * kCnnConvW + 255) / 256, 256, 0, ctx->stream>>>(params, (uint16_t*)ctx->d_cnn_pack.p, false);
+  k_cnn_pack<<<(3 * kCnnConvW + 255) / 256, 256, 0, ctx->stream>>>(params, (uint16_t*)ctx->d_cnn_packT.p, true);
+  CK(cudaGetLastError(), "cnn pack launch");
+  CnnFwdArgs F{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
+               ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, (float*)ctx->d_cnn_logits.p,
+               (float*)ctx->d_cnn_gap.p, (uint16_t*)ctx->d_cnn_acts.p, status};
+  k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(F);
+  CK(cudaGetLastError(), "cnn forward launch");
+  CnnBwdArgs B{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
+               ctu_xy, labels, params, (const uint16_t*)ctx->d_cnn_packT.p, (const float*)ctx->d_cnn_logits.p,
+               (const float*)ctx->d_cnn_gap.p, (const uint16_t*)ctx->d_cnn_acts.p, (float*)ctx->d_cnn_partial.p,
+               1.0f / (float)num_blocks, status};
+  k_cnn_backward<<<grid, kCnnThreads, kCnnBwdSmem, ctx->stream>>>(B);
+  CK(cudaGetLastError(), "cnn backward launch");
+  k_cnn_reduce<<<(kCnnParams + 1 + 255) / 256, 256, 0, ctx->stream>>>((const float*)ctx->d_cnn_partial.p, (int)grid,
+                                                                      grads, loss);
+  CK(cudaGetLastError(), "cnn reduce launch");
+  ctx->launches += 5;
+  if (lr > 0.0f) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - powf(b1, (float)step), c2 = 1.0f - powf(b2, (float)step);
+    k_cnn_adam<<<(kCnnParams + 255) / 256, 256, 0, ctx->stream>>>(params, grads, adam_m, adam_v, lr, b1, b2, 1e-8f,
+                                                                   c1, c2);
+    CK(cudaGetLastError(), "adam launch");
+    ctx->launches++;
+  }
   return VVCG_OK;
 }
 

@@ -48,3 +48,49 @@ def test_cnn_forward_matches_fp32_reference(ctx, pkg, n, bd, seed):
         assert err < 2e-2, (l, float(err))
     assert torch.allclose(gap.cpu(), ref_gap, rtol=2e-2, atol=2e-3), (gap.cpu() - ref_gap).abs().max()
     assert torch.allclose(logits.cpu(), ref_logits, rtol=2e-2, atol=2e-2), (logits.cpu() - ref_logits).abs().max()
+
+
+@pytest.mark.parametrize("n,seed", [(3, 1), (150, 2)])
+def test_cnn_gradients_match_autograd(ctx, pkg, n, seed):
+    """Loss and the gradient of every parameter group against PyTorch
+    autograd through the fp32 restatement."""
+    import torch
+    from rustmpeg_next_b200 import cnn
+
+    plane, xy, blocks = _blocks(n, 10, seed)
+    rng = np.random.default_rng(seed)
+    labels = np.stack([rng.integers(0, 67, n), rng.integers(0, 6, n)], axis=1).astype(np.uint8)
+    params = cnn.init_params(seed)
+    p = torch.from_numpy(params).cuda()
+    loss, grads = ctx.cnn_train_step(plane, 10, xy, torch.from_numpy(labels).cuda(), p)
+    ref_loss, ref = cnn.reference_loss_and_grads(blocks, labels, 10, params)
+    assert abs(float(loss.item()) - ref_loss) <= 1e-3 * max(1.0, abs(ref_loss))
+    g = grads.cpu().numpy()
+    groups = [("w1", cnn.OFF_W1, 288), ("b1", cnn.OFF_B1, 32)] + \
+        [(f"w{l}", cnn.off_w(l), 9216) for l in (2, 3, 4)] + [(f"b{l}", cnn.off_b(l), 32) for l in (2, 3, 4)] + \
+        [("wi", cnn.OFF_WI, 67 * 32), ("bi", cnn.OFF_BI, 67), ("ws", cnn.OFF_WS, 192), ("bs", cnn.OFF_BS, 6)]
+    for name, off, cnt in groups:
+        a, b = g[off:off + cnt], ref[off:off + cnt]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert rel < 3e-2, (name, rel)
+    # params untouched without a learning rate
+    assert torch.equal(p.cpu(), torch.from_numpy(params))
+
+
+def test_cnn_adam_steps_reduce_the_loss(ctx, pkg):
+    import torch
+    from rustmpeg_next_b200 import cnn
+
+    plane, xy, blocks = _blocks(256, 10, 7)
+    # labels that the network can learn: classes of the block's brightness
+    mean = blocks.mean(axis=(1, 2)) / 1023.0
+    span = (mean - mean.min()) / max(1e-6, float(mean.max() - mean.min()))
+    labels = torch.from_numpy(np.stack([np.minimum((span * 8).astype(int), 7) * 8,
+                                        np.minimum((span * 6).astype(int), 5)], 1).astype(np.uint8))
+    p = torch.from_numpy(cnn.init_params(7)).cuda()
+    m, v = torch.zeros_like(p), torch.zeros_like(p)
+    losses = []
+    for step in range(1, 41):
+        loss, _ = ctx.cnn_train_step(plane, 10, xy, labels.cuda(), p, m, v, step, 3e-3)
+        losses.append(float(loss.item()))
+    assert losses[-1] < 0.7 * losses[0], losses
