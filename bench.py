@@ -191,6 +191,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4, help="pictures in the CPU baseline sample")
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
+    ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
+    ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
+    ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--eval-frames", type=int, default=8, help="held-out 1080p frames per QP for the encoder")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -369,6 +373,9 @@ def main():
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "clocks": clocks}
+    if rank == 0 and not args.no_encode:
+        with torch.cuda.stream(stream):
+            line["encode"] = bench_encoder(pkg, ctx, stream, dev, args, peaks)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
@@ -382,6 +389,115 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+CNN_FLOP_PER_BLOCK = 2 * 1024 * 32 * 9 * (2 + 3 * 32)  # conv1 (2 inputs) + 3 x conv 32->32 (57.8 MFLOP)
+
+
+def bench_encoder(pkg, ctx, stream, dev, args, peaks):
+    """The encoder's candidate-cost stage on 1080p 10-bit frames: full search
+    (6 split types x 67 modes per block) against the CNN-pruned search (top-3
+    modes, top-2 splits, full set when the largest softmax is below 0.4),
+    with the pruner trained here on full-search labels (Adam, lr 1e-3, batch
+    1024) from frames other than the evaluated ones."""
+    import torch
+
+    from rustmpeg_next_b200 import cnn
+
+    def ev_time(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    t0 = time.perf_counter()
+    data = cnn.training_set(ctx, n_frames=args.train_frames, qps=QPS, seed=11)
+    label_s = time.perf_counter() - t0
+    n_train = sum(int(d[1].shape[0]) for d in data)
+    cnn.train(ctx, data, steps=2, batch=1024, lr=1e-3, seed=11)  # warm-up (fresh parameters below)
+    t1 = time.perf_counter()
+    params, losses = cnn.train(ctx, data, steps=args.train_steps, batch=1024, lr=1e-3, seed=11)
+    train_s = time.perf_counter() - t1
+    del data
+    # held-out frames
+    xs, ys = np.meshgrid(np.arange(0, PIX_W - 31, 32), np.arange(0, PIX_H - 31, 32))
+    xy = torch.from_numpy(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)).to(dev)
+    n_ctu = int(xy.shape[0])
+    out_f = torch.empty(n_ctu * 36, dtype=torch.uint8, device=dev)
+    out_p = torch.empty(n_ctu * 36, dtype=torch.uint8, device=dev)
+    from rustmpeg_next_b200 import synth
+
+    frames = []
+    for f in range(args.eval_frames):
+        y, _, _ = synth.value_noise_frame(PIX_W, PIX_H, 10, frame=900000 + f)
+        frames.append(torch.from_numpy(np.ascontiguousarray(y.astype(np.uint16)).view(np.int16)).to(dev))
+    untrained = torch.from_numpy(cnn.init_params(12345)).to(dev)
+    full_ms = pruned_ms = cnn_ms = 0.0
+    cost_f = cost_p = cost_ft = cost_fu = 0.0
+    rec3 = rec2 = fb_mode = fb_split = total = 0
+    for qp in QPS:
+        lam = cnn.search_lambda_q8(qp)
+        for plane in frames:
+            ctx.ctu_search_xy(plane, 10, lam, xy, out=out_f, sync=False)  # warm
+            full_ms += ev_time(lambda: ctx.ctu_search_xy(plane, 10, lam, xy, out=out_f, sync=False))
+            box = {}
+
+            def pruned():
+                lg, _, _ = ctx.cnn_forward(plane, 10, xy, params, qp, sync=False)
+                box["lg"] = lg
+                ctx.ctu_search_xy(plane, 10, lam, xy, lg, 3, 2, 0.4, out=out_p, sync=False)
+
+            pruned()
+            pruned_ms += ev_time(pruned)
+            cnn_ms += ev_time(lambda: ctx.cnn_forward(plane, 10, xy, params, qp, sync=False))
+            rf = out_f.cpu().numpy().view(pkg.CTU_SEARCH_RES_DTYPE)
+            rp = out_p.cpu().numpy().view(pkg.CTU_SEARCH_RES_DTYPE)
+            lg = box["lg"].cpu().numpy()
+            # the same pruning without the fallback, trained vs untrained network
+            ft = ctx.ctu_search_xy(plane, 10, lam, xy, box["lg"], 3, 2, 0.0)
+            lg_u, _, _ = ctx.cnn_forward(plane, 10, xy, untrained, qp)
+            fu = ctx.ctu_search_xy(plane, 10, lam, xy, lg_u, 3, 2, 0.0)
+            cost_ft += float(ft["cost"].astype(np.float64).sum())
+            cost_fu += float(fu["cost"].astype(np.float64).sum())
+            cost_f += float(rf["cost"].astype(np.float64).sum())
+            cost_p += float(rp["cost"].astype(np.float64).sum())
+            top3 = np.argsort(-lg[:, :67], axis=1, kind="stable")[:, :3]
+            top2 = np.argsort(-lg[:, 67:], axis=1, kind="stable")[:, :2]
+            rec3 += int((top3 == rf["cu_mode"][:, None]).any(1).sum())
+            rec2 += int((top2 == rf["split"][:, None]).any(1).sum())
+            fb_mode += int(((np.exp(lg[:, :67] - lg[:, :67].max(1, keepdims=True)).sum(1)) ** -1 < 0.4).sum())
+            fb_split += int(((np.exp(lg[:, 67:] - lg[:, 67:].max(1, keepdims=True)).sum(1)) ** -1 < 0.4).sum())
+            total += n_ctu
+    n_runs = len(QPS) * len(frames)
+    # inference throughput on a 4096-block batch
+    xy4 = xy.repeat(3, 1)[:4096].contiguous()
+    ctx.cnn_forward(frames[0], 10, xy4, params, 32, sync=False)
+    ms4 = min(ev_time(lambda: ctx.cnn_forward(frames[0], 10, xy4, params, 32, sync=False)) for _ in range(5))
+    tflops = 4096 * CNN_FLOP_PER_BLOCK / (ms4 * 1e-3) / 1e12
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    full_fps = n_runs / (full_ms * 1e-3)
+    pruned_fps = n_runs / (pruned_ms * 1e-3)
+    return {"what": "candidate-cost stage of the GPU encoder (intra mode + split decision per 32x32 CTU, "
+                    "SATD + lambda*bits, open loop); no bitstream, so BD-rate is not measured",
+            "frames": f"{len(frames)} held-out 1920x1080 10-bit frames x QP{list(QPS)}",
+            "full_fps": round(full_fps, 1), "pruned_fps": round(pruned_fps, 1),
+            "speedup": round(pruned_fps / full_fps, 2),
+            "full_ms_per_frame": round(full_ms / n_runs, 4), "pruned_ms_per_frame": round(pruned_ms / n_runs, 4),
+            "cnn_ms_per_frame": round(cnn_ms / n_runs, 4),
+            "cost_increase_pct": round(100.0 * (cost_p / cost_f - 1.0), 3),
+            "no_fallback_cost_increase_pct": {"trained": round(100.0 * (cost_ft / cost_f - 1.0), 3),
+                                              "untrained": round(100.0 * (cost_fu / cost_f - 1.0), 3)},
+            "top3_mode_recall": round(rec3 / total, 4), "top2_split_recall": round(rec2 / total, 4),
+            "fallback_rate": {"modes": round(fb_mode / total, 4), "splits": round(fb_split / total, 4)},
+            "cnn_inference": {"blocks": 4096, "ms": round(ms4, 4), "tflops": round(tflops, 1),
+                              "peak": bf16_peak, "frac": round(tflops / bf16_peak, 4),
+                              "flop_per_block": CNN_FLOP_PER_BLOCK},
+            "training": {"ctus_labelled": n_train, "label_s": round(label_s, 2), "steps": args.train_steps,
+                         "batch": 1024, "s": round(train_s, 2), "first_loss": round(losses[0], 4),
+                         "final_loss": round(float(np.mean(losses[-20:])), 4)}}
 
 
 def _cpu_model():

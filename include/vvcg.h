@@ -590,9 +590,9 @@ typedef struct vvcg_ctu_search_res {
  * candidates) with predictions from the source plane's own samples (the
  * predictors of predict_block_16, predict.rs:3079-3410); cost = sum over 8x8
  * tiles of (sum |Hadamard(source - prediction)| + 2) >> 2 plus
- * (lambda_q8 * bits) >> 8, with mode bits 2 + i for the i-th default MPM
- * (Planar, DC, 50, 18, 46, 54) and 7 for any other mode, and split bits 1 /
- * 2 / 3 / 3 / 4 / 4 added per split type. The first lowest cost wins, blocks
+ * (lambda_q8 * bits) >> 8, with 8 header bits per block plus mode bits
+ * 2 + i for the i-th default MPM (Planar, DC, 50, 18, 46, 54) and 7 for any
+ * other mode, and split bits 1 / 2 / 3 / 3 / 4 / 4 added per split type. The first lowest cost wins, blocks
  * and splits alike. reqs host memory, res device memory. This is the GPU
  * encoder's candidate-cost stage; the reference's encoders evaluate a
  * single 32x32 CU per CTU (slice.rs:2575-2800). */
@@ -603,16 +603,17 @@ vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t str
 /* ---- CNN pruner ------------------------------------------------------------- */
 
 /* Number of fp32 parameters of the CNN pruner and their layout: conv1 W
- * [32 out][9 taps] and b[32]; conv2..4 W [32 out][32 in][9 taps] and b[32];
- * intra head W [67][32] and b[67]; split head W [6][32] and b[6]. Taps are
- * row-major over (dy, dx) in -1..1. */
-#define VVCG_CNN_PARAMS 30473
+ * [32 out][2 in][9 taps] and b[32]; conv2..4 W [32 out][32 in][9 taps] and
+ * b[32]; intra head W [67][32] and b[67]; split head W [6][32] and b[6].
+ * Taps are row-major over (dy, dx) in -1..1. */
+#define VVCG_CNN_PARAMS 30761
 #define VVCG_CNN_OUT 73 /* 67 intra-mode logits, then 6 split logits */
 
 /* Forward pass of the CNN pruner on 32x32 luma blocks of a device plane
  * (8..12-bit samples in uint16, stride in samples) at the (x, y) positions
- * ctu_xy (device, num_blocks pairs): input samples / (2^bit_depth - 1)
- * rounded to bf16; conv 3x3 1->32 + ReLU (fp32, CUDA cores); 3 x conv 3x3
+ * ctu_xy (device, num_blocks pairs), coded at qp (0..63): input samples /
+ * (2^bit_depth - 1) rounded to bf16, and a constant plane qp / 63 (bf16);
+ * conv 3x3 2->32 + ReLU (fp32, CUDA cores); 3 x conv 3x3
  * 32->32 + ReLU on the tensor cores (bf16 operands, fp32 accumulation in
  * TMEM, bf16 activations); global average; the two linear heads (fp32).
  * logits: device, num_blocks x VVCG_CNN_OUT. gap (num_blocks x 32 fp32) and
@@ -622,11 +623,12 @@ vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t str
  * plane (its logits are NaN). This is the GPU encoder's pruning network;
  * the reference has none. */
 vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
-                                 uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy, uint32_t num_blocks,
+                                 uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
+                                 uint32_t num_blocks,
                                  const float* params, float* logits, float* gap, uint16_t* acts, uint32_t* status);
 
-/* One training step of the CNN pruner on num_blocks 32x32 blocks (the batch)
- * with labels (device, num_blocks x (intra mode 0..66, split type 0..5)):
+/* One training step of the CNN pruner on num_blocks 32x32 blocks (the batch,
+ * all coded at qp) with labels (device, num_blocks x (intra mode 0..66, split type 0..5)):
  * the forward pass, the mean softmax cross-entropy of both heads, the
  * backward pass (input gradients of the 3x3 32->32 layers on the tensor
  * cores, weight gradients on the CUDA cores), written to grads (device,
@@ -637,7 +639,7 @@ vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t 
  * outside the plane or with a label out of range are skipped and flag bit
  * 1. Asynchronous on the context's stream. */
 vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
-                                    uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy,
+                                    uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
                                     const uint8_t* labels, uint32_t num_blocks, float* params, float* adam_m,
                                     float* adam_v, uint32_t step, float lr, float* grads, float* loss,
                                     uint32_t* status);

@@ -290,9 +290,10 @@ def ctu_search(src, bd, x, y, lambda_q8, split_mask=0x3F, cand=()):
                 modes=[(m >> (8 * k)) & 0xFF for k in range(4)])
 
 
-def search_lambda_q8(qp):
-    """lambda of the CTU search in 1/256 units: sqrt(0.57 * 2^((qp - 12) / 3))."""
-    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0))))
+def search_lambda_q8(qp, bit_depth=10):
+    """lambda of the CTU search (SATD domain) in 1/256 units:
+    sqrt(0.57 * 2^((qp - 12) / 3)) * 2^(bit_depth - 8)."""
+    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0)) * 2.0 ** (bit_depth - 8)))
 
 
 def choose_intra_mode(recon, src, bd, bx, by, w, h):

@@ -20,11 +20,12 @@ const int kBlocks[15][4] = {{0, 0, 32, 32}, {0, 0, 16, 16}, {16, 0, 16, 16}, {0,
                             {0, 8, 32, 16}, {0, 24, 32, 8}, {0, 0, 8, 32}, {8, 0, 16, 32}, {24, 0, 8, 32}};
 const int kFirst[6] = {0, 1, 5, 7, 9, 12}, kCount[6] = {1, 4, 2, 2, 3, 3}, kSplitBits[6] = {1, 2, 3, 3, 4, 4};
 
+// an 8-bit block header plus the mode: MPM i of the default list 2 + i bits, others 7
 int mode_bits(int m) {
   static const int mpm[6] = {0, 1, 50, 18, 46, 54};
   for (int i = 0; i < 6; i++)
-    if (mpm[i] == m) return 2 + i;
-  return 7;
+    if (mpm[i] == m) return 8 + 2 + i;
+  return 8 + 7;
 }
 
 // per 8x8 tile: (sum |H8 * D * H8^T| + 2) >> 2, H8 the unnormalised

@@ -66,7 +66,7 @@ CTU_SEARCH_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("split_mask", "u1"
 CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), ("split", "u1"), ("cu_mode", "u1"),
                                  ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
 SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
-CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30473, 73, 67, 6
+CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30761, 73, 67, 6
 DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
                            ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
 DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
@@ -226,8 +226,8 @@ def lib():
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
         L.vvcg_ctu_search_pruned_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, u32, u32, C.c_float, vp]
         L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
-        L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, u32, vp, vp, vp, vp, vp]
-        L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
+        L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, u32, vp, vp, vp, vp, vp]
+        L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
                                               vp, vp, vp]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
@@ -326,6 +326,17 @@ class Context:
         """Use a torch.cuda.Stream (or raw handle) for every launch; None = own stream."""
         raw = None if stream is None else getattr(stream, "cuda_stream", stream)
         self._check(self._L.vvcg_set_stream(self._h, C.c_void_p(raw) if raw else None))
+        self.torch_stream = stream if hasattr(stream, "cuda_stream") and raw else None
+
+    def torch_stream_scope(self):
+        """A `with` scope in which torch's current stream is this context's
+        stream (a new torch stream is bound to the context when it has none),
+        so that tensors made for a call are ordered with its kernels."""
+        import torch
+
+        if getattr(self, "torch_stream", None) is None:
+            self.set_stream(torch.cuda.Stream())
+        return torch.cuda.stream(self.torch_stream)
 
     # -- picture batches --
     def decode_batch(self, batch: Batch, outs=None):
@@ -537,10 +548,10 @@ class Context:
         return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:len(reqs)]
 
     # -- CNN pruner --
-    def cnn_forward(self, plane, bit_depth, xy, params, want_acts=False, sync=True):
+    def cnn_forward(self, plane, bit_depth, xy, params, qp, want_acts=False, sync=True):
         """plane: (H, W) int16 CUDA tensor of 16-bit luma samples; xy: (n, 2)
         int32 CUDA tensor of 32x32 block positions; params: CNN_PARAMS fp32
-        CUDA tensor. Returns (logits (n, 73), gap (n, 32), acts (n, 4, 1024,
+        CUDA tensor; qp: the QP the blocks are coded at. Returns (logits (n, 73), gap (n, 32), acts (n, 4, 1024,
         32) bf16 or None) as CUDA tensors."""
         import torch
 
@@ -551,7 +562,7 @@ class Context:
         acts = torch.empty((n, 4, 1024, 32), dtype=torch.bfloat16, device=dev) if want_acts else None
         st = torch.zeros(1, dtype=torch.int32, device=dev)
         h, w = plane.shape
-        self._check(self._L.vvcg_cnn_forward_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth,
+        self._check(self._L.vvcg_cnn_forward_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, qp,
                                                  _ptr(xy.contiguous()), n, _ptr(params), _ptr(logits), _ptr(gap),
                                                  _ptr(acts), _ptr(st)))
         if sync:
@@ -563,7 +574,7 @@ class Context:
                 raise InvalidInput("CNN forward: a block lies outside the plane")
         return logits, gap, acts
 
-    def cnn_train_step(self, plane, bit_depth, xy, labels, params, adam_m=None, adam_v=None, step=0, lr=0.0,
+    def cnn_train_step(self, plane, bit_depth, qp, xy, labels, params, adam_m=None, adam_v=None, step=0, lr=0.0,
                        sync=True):
         """One training step on the blocks xy ((n, 2) int32 CUDA) with labels
         ((n, 2) uint8 CUDA: intra mode, split type). Updates params (and the
@@ -576,7 +587,7 @@ class Context:
         loss = torch.empty(1, dtype=torch.float32, device=dev)
         st = torch.zeros(1, dtype=torch.int32, device=dev)
         h, w = plane.shape
-        self._check(self._L.vvcg_cnn_train_step_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth,
+        self._check(self._L.vvcg_cnn_train_step_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, qp,
                                                     _ptr(xy.contiguous()), _ptr(labels.contiguous()), int(xy.shape[0]),
                                                     _ptr(params), _ptr(adam_m), _ptr(adam_v), step, lr, _ptr(grads),
                                                     _ptr(loss), _ptr(st)))

@@ -2,7 +2,8 @@
 plain PyTorch fp32 restatement of the network used by the tests to check
 the tensor-core kernels (the library itself runs only its CUDA kernels).
 
-Parameter vector (fp32, CNN_PARAMS entries): conv1 W [32][9] and b[32];
+Parameter vector (fp32, CNN_PARAMS entries): conv1 W [32][2][9] and b[32]
+(input 0: the samples, input 1: a constant plane QP / 63);
 conv2..4 W [32 out][32 in][9] and b[32]; intra head W [67][32], b[67];
 split head W [6][32], b[6]. Taps are row-major over (dy, dx) in -1..1.
 """
@@ -11,11 +12,11 @@ from __future__ import annotations
 import numpy as np
 
 CH, MODES, SPLITS = 32, 67, 6
-OFF_W1, OFF_B1 = 0, 288
+OFF_W1, OFF_B1 = 0, 576
 
 
 def off_w(layer):
-    return 320 + (layer - 2) * (CH * CH * 9 + CH)
+    return 608 + (layer - 2) * (CH * CH * 9 + CH)
 
 
 def off_b(layer):
@@ -33,7 +34,7 @@ def init_params(seed=0):
     """He-initialised weights, zero biases (fp32 numpy vector)."""
     rng = np.random.default_rng(seed)
     p = np.zeros(N_PARAMS, np.float32)
-    p[OFF_W1:OFF_W1 + 288] = rng.normal(0, np.sqrt(2 / 9), 288)
+    p[OFF_W1:OFF_W1 + 576] = rng.normal(0, np.sqrt(2 / 18), 576)
     for layer in (2, 3, 4):
         p[off_w(layer):off_w(layer) + CH * CH * 9] = rng.normal(0, np.sqrt(2 / (CH * 9)), CH * CH * 9)
     p[OFF_WI:OFF_WI + MODES * CH] = rng.normal(0, np.sqrt(1 / CH), MODES * CH)
@@ -46,7 +47,7 @@ def unpack(params):
     import torch
 
     p = params if isinstance(params, torch.Tensor) else torch.as_tensor(params, dtype=torch.float32)
-    w1 = p[OFF_W1:OFF_W1 + 288].reshape(CH, 1, 3, 3)
+    w1 = p[OFF_W1:OFF_W1 + 576].reshape(CH, 2, 3, 3)
     b1 = p[OFF_B1:OFF_B1 + CH]
     convs = [(p[off_w(layer):off_w(layer) + CH * CH * 9].reshape(CH, CH, 3, 3), p[off_b(layer):off_b(layer) + CH])
              for layer in (2, 3, 4)]
@@ -55,7 +56,14 @@ def unpack(params):
     return w1, b1, convs, wi, bi, ws, bs
 
 
-def reference_forward(blocks, bit_depth, params):
+def qp_input(qp):
+    """The constant input plane's value: QP / 63 rounded to bf16."""
+    import torch
+
+    return float(torch.tensor(qp / 63.0, dtype=torch.float32).to(torch.bfloat16).float())
+
+
+def reference_forward(blocks, bit_depth, params, qp):
     """fp32 restatement of the kernels' forward pass on (n, 32, 32) sample
     blocks with the same bf16 roundings (input, activations of layers 1-3,
     conv weights of layers 2-4); returns (logits (n, 73), gap (n, 32),
@@ -66,6 +74,7 @@ def reference_forward(blocks, bit_depth, params):
     bf = lambda t: t.to(torch.bfloat16).to(torch.float32)  # noqa: E731
     w1, b1, convs, wi, bi, ws, bs = unpack(params)
     x = bf(torch.as_tensor(blocks, dtype=torch.float32)[:, None] * (1.0 / ((1 << bit_depth) - 1)))
+    x = torch.cat([x, torch.full_like(x, qp_input(qp))], dim=1)
     a = bf(F.relu(F.conv2d(x, w1, b1, padding=1)))
     acts = [a]
     for i, (w, b) in enumerate(convs):
@@ -79,14 +88,14 @@ def reference_forward(blocks, bit_depth, params):
     return logits, gap, acts
 
 
-def reference_loss_and_grads(blocks, labels, bit_depth, params):
+def reference_loss_and_grads(blocks, labels, bit_depth, params, qp):
     """Mean cross-entropy of both heads and its gradient w.r.t. the
     parameter vector, by autograd through reference_forward (fp32 with the
     kernels' bf16 roundings)."""
     import torch
 
     p = torch.tensor(np.asarray(params, np.float32), requires_grad=True)
-    logits, _, _ = reference_forward(blocks, bit_depth, p)
+    logits, _, _ = reference_forward(blocks, bit_depth, p, qp)
     lab = torch.as_tensor(np.asarray(labels), dtype=torch.long)
     loss = torch.nn.functional.cross_entropy(logits[:, :MODES], lab[:, 0]) + \
         torch.nn.functional.cross_entropy(logits[:, MODES:], lab[:, 1])
@@ -94,9 +103,10 @@ def reference_loss_and_grads(blocks, labels, bit_depth, params):
     return float(loss.detach()), p.grad.numpy()
 
 
-def search_lambda_q8(qp):
-    """lambda of the CTU search in 1/256 units: sqrt(0.57 * 2^((qp - 12) / 3))."""
-    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0))))
+def search_lambda_q8(qp, bit_depth=10):
+    """lambda of the CTU search (SATD domain) in 1/256 units:
+    sqrt(0.57 * 2^((qp - 12) / 3)) * 2^(bit_depth - 8)."""
+    return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0)) * 2.0 ** (bit_depth - 8)))
 
 
 def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37), seed=0):
@@ -110,8 +120,16 @@ def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37),
     from . import synth
 
     out = []
-    xs, ys = np.meshgrid(np.arange(0, width - 31, 32), np.arange(0, height - 31, 32))
-    xy = torch.from_numpy(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)).cuda()
+    with ctx.torch_stream_scope():
+        xs, ys = np.meshgrid(np.arange(0, width - 31, 32), np.arange(0, height - 31, 32))
+        xy = torch.from_numpy(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)).cuda()
+        _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed)
+    return out
+
+
+def _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed):
+    import torch
+
     for f in range(n_frames):
         y, _, _ = synth.value_noise_frame(width, height, 10, frame=seed * 1000 + f)
         plane = torch.from_numpy(np.ascontiguousarray(y.astype(np.uint16)).view(np.int16)).cuda()
@@ -119,7 +137,6 @@ def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37),
             r = ctx.ctu_search_xy(plane, 10, search_lambda_q8(qp), xy)
             lab = torch.from_numpy(np.stack([r["cu_mode"], r["split"]], 1).astype(np.uint8)).cuda()
             out.append((plane, xy, lab, qp))
-    return out
 
 
 def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None):
@@ -128,13 +145,14 @@ def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None):
     import torch
 
     rng = np.random.default_rng(seed)
-    p = torch.from_numpy(init_params(seed) if params is None else params).cuda()
-    m, v = torch.zeros_like(p), torch.zeros_like(p)
-    losses = []
-    for step in range(1, steps + 1):
-        plane, xy, lab, _ = data[int(rng.integers(0, len(data)))]
-        idx = torch.from_numpy(rng.choice(xy.shape[0], min(batch, xy.shape[0]), replace=False)).cuda()
-        loss, _ = ctx.cnn_train_step(plane, 10, xy[idx], lab[idx], p, m, v, step, lr, sync=False)
-        losses.append(loss)
-    torch.cuda.synchronize()
+    with ctx.torch_stream_scope():
+        p = torch.from_numpy(init_params(seed) if params is None else params).cuda()
+        m, v = torch.zeros_like(p), torch.zeros_like(p)
+        losses = []
+        for step in range(1, steps + 1):
+            plane, xy, lab, qp = data[int(rng.integers(0, len(data)))]
+            idx = torch.from_numpy(rng.choice(xy.shape[0], min(batch, xy.shape[0]), replace=False)).cuda()
+            loss, _ = ctx.cnn_train_step(plane, 10, qp, xy[idx], lab[idx], p, m, v, step, lr, sync=False)
+            losses.append(loss)
+        torch.cuda.synchronize()
     return p, [float(x.item()) for x in losses]

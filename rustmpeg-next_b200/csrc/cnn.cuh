@@ -1,6 +1,7 @@
 // The CNN pruner of the GPU encoder: 32x32 luma blocks (samples / max value,
-// rounded to bf16) -> conv 3x3 1->32 + ReLU -> 3 x (conv 3x3 32->32 + ReLU)
-// -> global average -> 67 intra-mode logits and 6 split logits.
+// rounded to bf16) with a second, constant input plane QP / 63 (the split
+// decision depends on lambda) -> conv 3x3 2->32 + ReLU -> 3 x (conv 3x3
+// 32->32 + ReLU) -> global average -> 67 intra-mode logits and 6 split logits.
 //
 // Forward: one CTA per block (persistent over blocks). The block's
 // activations stay in shared memory as two ping-pong images of 34 x 34
@@ -12,7 +13,7 @@
 // one image row, LBO one channel plane, and a tap is an address offset. The
 // 8 tiles of a layer accumulate in 256 TMEM columns; 8 warps read them back,
 // add the bias, apply ReLU and write the next image (or the average).
-// The first layer (one input channel) runs on the CUDA cores.
+// The first layer (two input channels) runs on the CUDA cores.
 #pragma once
 #include "umma.cuh"
 
@@ -20,14 +21,14 @@ namespace vvcg {
 
 constexpr int kCnnCh = 32, kCnnModes = 67, kCnnSplits = 6, kCnnOut = kCnnModes + kCnnSplits;
 constexpr int kCnnConvW = kCnnCh * kCnnCh * 9;  // 9216
-// fp32 parameter vector: W1 [co][tap], b1, then per layer 2..4 W [co][ci][tap]
-// and b, then the heads W [out][ch] and b.
-constexpr int kOffW1 = 0, kOffB1 = 288;
-__host__ __device__ constexpr int cnn_off_w(int layer) { return 320 + (layer - 2) * (kCnnConvW + kCnnCh); }
+// fp32 parameter vector: W1 [co][2 inputs][tap], b1, then per layer 2..4
+// W [co][ci][tap] and b, then the heads W [out][ch] and b.
+constexpr int kOffW1 = 0, kOffB1 = 576;
+__host__ __device__ constexpr int cnn_off_w(int layer) { return 608 + (layer - 2) * (kCnnConvW + kCnnCh); }
 __host__ __device__ constexpr int cnn_off_b(int layer) { return cnn_off_w(layer) + kCnnConvW; }
 constexpr int kOffWi = cnn_off_w(5), kOffBi = kOffWi + kCnnModes * kCnnCh;
 constexpr int kOffWs = kOffBi + kCnnModes, kOffBs = kOffWs + kCnnSplits * kCnnCh;
-constexpr int kCnnParams = kOffBs + kCnnSplits;  // 30473
+constexpr int kCnnParams = kOffBs + kCnnSplits;  // 30761
 
 constexpr int kImgW = 34;                 // 32 + halo
 constexpr int kPlane = kImgW * kImgW * 16;  // one plane of 8 channels, bytes
@@ -35,7 +36,7 @@ constexpr int kImg = 4 * kPlane;            // 73984
 constexpr int kPackL = 36 * 32 * 16;        // packed bf16 weights of one layer: [tap*4 + ci/8][co][ci%8]
 constexpr int kCnnThreads = 256;
 constexpr uint32_t kCnnIdesc = umma_idesc_bf16(128, 32);
-constexpr int kCnnMisc = (288 + 32 + 96 + 8 * 32 + 1024 + 32) * 4;
+constexpr int kCnnMisc = (576 + 32 + 96 + 8 * 32 + 1024 + 32) * 4;
 constexpr int kCnnSmem = 2 * kImg + 3 * kPackL + kCnnMisc + 64;
 
 __device__ __forceinline__ uint16_t f2bf(float f) {  // round to nearest even
@@ -66,6 +67,7 @@ struct CnnFwdArgs {
   const uint16_t* plane;
   int64_t stride;
   int32_t width, height, maxv, n;
+  float qp_in;             // the QP plane's value, QP / 63 rounded to bf16
   const uint32_t* ctu_xy;  // n (x, y) pairs
   const float* params;
   const uint16_t* pack;
@@ -99,7 +101,7 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_con
   uint8_t* X1 = smem + kImg;
   uint8_t* W = smem + 2 * kImg;
   float* w1 = (float*)(W + 3 * kPackL);
-  float* b1 = w1 + 288;
+  float* b1 = w1 + 576;
   float* bias = b1 + 32;   // [3][32]
   float* gpart = bias + 96;  // [8 warps][32]
   float* xin = gpart + 256;  // 32 x 32 input
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_con
   // weights, zero images (the halos stay zero), TMEM, barrier
   for (int i = t; i < 3 * kPackL / 16; i += kCnnThreads) ((uint4*)W)[i] = ((const uint4*)A.pack)[i];
   for (int i = t; i < 2 * kImg / 16; i += kCnnThreads) ((uint4*)X0)[i] = make_uint4(0, 0, 0, 0);
-  for (int i = t; i < 288; i += kCnnThreads) w1[i] = A.params[kOffW1 + i];
+  for (int i = t; i < 576; i += kCnnThreads) w1[i] = A.params[kOffW1 + i];
   if (t < 32) b1[t] = A.params[kOffB1 + t];
   if (t < 96) bias[t] = A.params[cnn_off_b(2 + t / 32) + t % 32];
   if (warp == 0) {
@@ -145,11 +147,13 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_con
     // layer 1 on the CUDA cores: 4 pixels per thread
     for (int p = t; p < 1024; p += kCnnThreads) {
       const int iy = p >> 5, ix = p & 31;
-      float in[9];
+      float in[9], iq[9];
 #pragma unroll
       for (int tap = 0; tap < 9; tap++) {
         const int y = iy + tap / 3 - 1, x = ix + tap % 3 - 1;
-        in[tap] = (y >= 0 && y < 32 && x >= 0 && x < 32) ? xin[y * 32 + x] : 0.0f;
+        const bool inside = y >= 0 && y < 32 && x >= 0 && x < 32;
+        in[tap] = inside ? xin[y * 32 + x] : 0.0f;
+        iq[tap] = inside ? A.qp_in : 0.0f;
       }
       uint32_t pk[16];
 #pragma unroll
@@ -157,8 +161,13 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_con
         float s0 = b1[c], s1 = b1[c + 1];
 #pragma unroll
         for (int tap = 0; tap < 9; tap++) {
-          s0 = fmaf(w1[c * 9 + tap], in[tap], s0);
-          s1 = fmaf(w1[(c + 1) * 9 + tap], in[tap], s1);
+          s0 = fmaf(w1[c * 18 + tap], in[tap], s0);
+          s1 = fmaf(w1[(c + 1) * 18 + tap], in[tap], s1);
+        }
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+          s0 = fmaf(w1[c * 18 + 9 + tap], iq[tap], s0);
+          s1 = fmaf(w1[(c + 1) * 18 + 9 + tap], iq[tap], s1);
         }
         pk[c / 2] = (uint32_t)f2bf(fmaxf(s0, 0.0f)) | ((uint32_t)f2bf(fmaxf(s1, 0.0f)) << 16);
       }
@@ -275,6 +284,7 @@ struct CnnBwdArgs {
   const uint16_t* plane;
   int64_t stride;
   int32_t width, height, maxv, n;
+  float qp_in;
   const uint32_t* ctu_xy;
   const uint8_t* labels;  // n x (mode, split)
   const float* params;
@@ -485,17 +495,20 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
       __syncthreads();
     }
     if (!ok) break;
-    // layer 1: dW1[co][tap] = sum_p dZ1[p][co] x[p + tap] (dZ1 is in dz)
+    // layer 1: dW1[co][input][tap] = sum_p dZ1[p][co] in[p + tap] (dZ1 is in dz)
     for (int o = t; o < 288; o += kCnnThreads) {
       const int co = o / 9, tp = o % 9, dy = tp / 3 - 1, dx = tp % 3 - 1;
       const uint8_t* zp = dz + (co >> 3) * kPlane + (co & 7) * 2;
-      float s = 0.0f;
+      float s = 0.0f, sq = 0.0f;
       for (int p = 0; p < 1024; p++) {
         const int y = (p >> 5) + dy, x = (p & 31) + dx;
         if (y < 0 || y >= 32 || x < 0 || x >= 32) continue;
-        s = fmaf(bf2f(*(const uint16_t*)(zp + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16)), xin[y * 32 + x], s);
+        const float z = bf2f(*(const uint16_t*)(zp + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16));
+        s = fmaf(z, xin[y * 32 + x], s);
+        sq += z;
       }
-      part[kOffW1 + co * 9 + tp] += s;
+      part[kOffW1 + co * 18 + tp] += s;
+      part[kOffW1 + co * 18 + 9 + tp] += sq * A.qp_in;
     }
     __syncthreads();
   }

@@ -381,11 +381,12 @@ __global__ void __launch_bounds__(kIsrWarps * 32) k_luma_intra_search_8(const __
 
 // ------------------------------------------------------- CTU full search ----
 
-// The default MPM list (derive_intra_mpms with no neighbours, predict.rs)
-// orders the mode bits of the search cost: MPM i costs 2 + i bits, any other
-// mode 7.
+// Bits a block is charged in the search cost: a header of 8 bits (split
+// flags, cbf and the like) plus its mode, ordered by the default MPM list
+// (derive_intra_mpms with no neighbours, predict.rs): MPM i costs 2 + i bits,
+// any other mode 7.
 __device__ __forceinline__ int search_mode_bits(int m) {
-  return m == 0 ? 2 : m == 1 ? 3 : m == 50 ? 4 : m == 18 ? 5 : m == 46 ? 6 : m == 54 ? 7 : 7;
+  return 8 + (m == 0 ? 2 : m == 1 ? 3 : m == 50 ? 4 : m == 18 ? 5 : m == 46 ? 6 : 7);
 }
 
 // One block of one split type of one CTU.

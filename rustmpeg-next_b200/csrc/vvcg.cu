@@ -1443,8 +1443,17 @@ extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t*
 // CNN pruner forward pass (vvcg_cnn_forward_dev).
 // ---------------------------------------------------------------------------
 static_assert(kCnnParams == VVCG_CNN_PARAMS && kCnnOut == VVCG_CNN_OUT, "CNN layout");
+static float cnn_qp_input(uint32_t qp) {  // QP / 63 rounded to bf16 (nearest even)
+  float f = (float)qp / 63.0f;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
 extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
-                                            uint32_t height, uint8_t bit_depth, const uint32_t* ctu_xy,
+                                            uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
                                             uint32_t num_blocks, const float* params, float* logits, float* gap,
                                             uint16_t* acts, uint32_t* status) {
   if (!ctx) return VVCG_INVALID_INPUT;
@@ -1463,8 +1472,9 @@ extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane
   CK(ctx->d_cnn_pack.reserve(3 * kPackL), "cudaMalloc");
   k_cnn_pack<<<(3 * kCnnConvW + 255) / 256, 256, 0, ctx->stream>>>(params, (uint16_t*)ctx->d_cnn_pack.p, false);
   CK(cudaGetLastError(), "cnn pack launch");
+  if (qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "QP above 63");
   CnnFwdArgs A{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
-               ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, logits, gap, acts, status};
+               cnn_qp_input(qp), ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, logits, gap, acts, status};
   const uint32_t grid = std::min<uint32_t>(num_blocks, (uint32_t)ctx->num_sms);
   k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(A);
   CK(cudaGetLastError(), "cnn launch");
@@ -1476,7 +1486,7 @@ extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane
 // CNN pruner training step (vvcg_cnn_train_step_dev).
 // ---------------------------------------------------------------------------
 extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride,
-                                               uint32_t width, uint32_t height, uint8_t bit_depth,
+                                               uint32_t width, uint32_t height, uint8_t bit_depth, uint8_t qp,
                                                const uint32_t* ctu_xy, const uint8_t* labels, uint32_t num_blocks,
                                                float* params, float* adam_m, float* adam_v, uint32_t step, float lr,
                                                float* grads, float* loss, uint32_t* status) {
@@ -1488,6 +1498,7 @@ extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* pl
     return fail(ctx, VVCG_INVALID_INPUT, "an update needs the Adam moments and a step count from 1");
   if (stride < width || bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
   if (num_blocks > 65536) return fail(ctx, VVCG_LIMIT_EXCEEDED, "more than 65536 blocks in one step");
+  if (qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "QP above 63");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   static bool attr_set[64] = {};
   if (ctx->device < 64 && !attr_set[ctx->device]) {
@@ -1507,12 +1518,12 @@ extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* pl
   k_cnn_pack<<<(3 * kCnnConvW + 255) / 256, 256, 0, ctx->stream>>>(params, (uint16_t*)ctx->d_cnn_packT.p, true);
   CK(cudaGetLastError(), "cnn pack launch");
   CnnFwdArgs F{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
-               ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, (float*)ctx->d_cnn_logits.p,
+               cnn_qp_input(qp), ctu_xy, params, (const uint16_t*)ctx->d_cnn_pack.p, (float*)ctx->d_cnn_logits.p,
                (float*)ctx->d_cnn_gap.p, (uint16_t*)ctx->d_cnn_acts.p, status};
   k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(F);
   CK(cudaGetLastError(), "cnn forward launch");
   CnnBwdArgs B{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
-               ctu_xy, labels, params, (const uint16_t*)ctx->d_cnn_packT.p, (const float*)ctx->d_cnn_logits.p,
+               cnn_qp_input(qp), ctu_xy, labels, params, (const uint16_t*)ctx->d_cnn_packT.p, (const float*)ctx->d_cnn_logits.p,
                (const float*)ctx->d_cnn_gap.p, (const uint16_t*)ctx->d_cnn_acts.p, (float*)ctx->d_cnn_partial.p,
                1.0f / (float)num_blocks, status};
   k_cnn_backward<<<grid, kCnnThreads, kCnnBwdSmem, ctx->stream>>>(B);

@@ -37,8 +37,9 @@ def test_cnn_forward_matches_fp32_reference(ctx, pkg, n, bd, seed):
 
     plane, xy, blocks = _blocks(n, bd, seed)
     params = cnn.init_params(seed)
-    logits, gap, acts = ctx.cnn_forward(plane, bd, xy, torch.from_numpy(params).cuda(), want_acts=True)
-    ref_logits, ref_gap, ref_acts = cnn.reference_forward(blocks, bd, params)
+    qp = 22 + 5 * seed
+    logits, gap, acts = ctx.cnn_forward(plane, bd, xy, torch.from_numpy(params).cuda(), qp, want_acts=True)
+    ref_logits, ref_gap, ref_acts = cnn.reference_forward(blocks, bd, params, qp)
     # layer 1 is fp32 on both sides: equal up to summation order and bf16 ties
     a1 = acts[:, 0].float().cpu().reshape(n, 32, 32, 32).permute(0, 3, 1, 2)
     assert (a1 - ref_acts[0]).abs().max() <= 1e-2 * max(1.0, float(ref_acts[0].abs().max()))
@@ -62,11 +63,11 @@ def test_cnn_gradients_match_autograd(ctx, pkg, n, seed):
     labels = np.stack([rng.integers(0, 67, n), rng.integers(0, 6, n)], axis=1).astype(np.uint8)
     params = cnn.init_params(seed)
     p = torch.from_numpy(params).cuda()
-    loss, grads = ctx.cnn_train_step(plane, 10, xy, torch.from_numpy(labels).cuda(), p)
-    ref_loss, ref = cnn.reference_loss_and_grads(blocks, labels, 10, params)
+    loss, grads = ctx.cnn_train_step(plane, 10, 27, xy, torch.from_numpy(labels).cuda(), p)
+    ref_loss, ref = cnn.reference_loss_and_grads(blocks, labels, 10, params, 27)
     assert abs(float(loss.item()) - ref_loss) <= 1e-3 * max(1.0, abs(ref_loss))
     g = grads.cpu().numpy()
-    groups = [("w1", cnn.OFF_W1, 288), ("b1", cnn.OFF_B1, 32)] + \
+    groups = [("w1", cnn.OFF_W1, 576), ("b1", cnn.OFF_B1, 32)] + \
         [(f"w{l}", cnn.off_w(l), 9216) for l in (2, 3, 4)] + [(f"b{l}", cnn.off_b(l), 32) for l in (2, 3, 4)] + \
         [("wi", cnn.OFF_WI, 67 * 32), ("bi", cnn.OFF_BI, 67), ("ws", cnn.OFF_WS, 192), ("bs", cnn.OFF_BS, 6)]
     for name, off, cnt in groups:
@@ -91,6 +92,6 @@ def test_cnn_adam_steps_reduce_the_loss(ctx, pkg):
     m, v = torch.zeros_like(p), torch.zeros_like(p)
     losses = []
     for step in range(1, 41):
-        loss, _ = ctx.cnn_train_step(plane, 10, xy, labels.cuda(), p, m, v, step, 3e-3)
+        loss, _ = ctx.cnn_train_step(plane, 10, 37, xy, labels.cuda(), p, m, v, step, 3e-3)
         losses.append(float(loss.item()))
     assert losses[-1] < 0.7 * losses[0], losses

@@ -10,9 +10,9 @@ def test_flat_picture_keeps_one_planar_cu(orc):
     lam = orc.search_lambda_q8(32)
     r = orc.ctu_search(src, 10, 32, 32, lam)
     assert (r["split"], r["cu_mode"], r["modes"][0]) == (0, 0, 0)
-    # SATD 0 everywhere: each cost is lambda * (split bits + 2 per Planar block)
+    # SATD 0 everywhere: each cost is lambda * (split bits + 8 + 2 per Planar block)
     counts, sbits = [1, 4, 2, 2, 3, 3], [1, 2, 3, 3, 4, 4]
-    want = [(lam * sbits[s]) // 256 + counts[s] * ((lam * 2) // 256) for s in range(6)]
+    want = [(lam * sbits[s]) // 256 + counts[s] * ((lam * 10) // 256) for s in range(6)]
     assert r["split_cost"] == want
 
 

@@ -79,7 +79,17 @@ def test_trained_pruner_stays_close_to_full_search(ctx, pkg):
     a, xy = _xy(1024, 512)
     lam = cnn.search_lambda_q8(32)
     full = ctx.ctu_search_xy(plane, 10, lam, xy)
-    logits, _, _ = ctx.cnn_forward(plane, 10, xy, params)
+    logits, _, _ = ctx.cnn_forward(plane, 10, xy, params, 32)
     pruned = ctx.ctu_search_xy(plane, 10, lam, xy, logits, 3, 2, 0.4)
-    inc = pruned["cost"].astype(np.float64).sum() / full["cost"].astype(np.float64).sum() - 1.0
+    total = full["cost"].astype(np.float64).sum()
+    inc = pruned["cost"].astype(np.float64).sum() / total - 1.0
     assert 0.0 <= inc < 0.05, inc
+    # what training buys: with the same pruning and no fallback, the trained
+    # network's candidates cost less than an untrained network's
+    untrained = torch.from_numpy(cnn.init_params(99)).cuda()
+    lg_u, _, _ = ctx.cnn_forward(plane, 10, xy, untrained, 32)
+    forced_t = ctx.ctu_search_xy(plane, 10, lam, xy, logits, 3, 2, 0.0)
+    forced_u = ctx.ctu_search_xy(plane, 10, lam, xy, lg_u, 3, 2, 0.0)
+    inc_t = forced_t["cost"].astype(np.float64).sum() / total - 1.0
+    inc_u = forced_u["cost"].astype(np.float64).sum() / total - 1.0
+    assert inc_t < 0.8 * inc_u, (inc_t, inc_u)
