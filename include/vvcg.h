@@ -667,6 +667,58 @@ vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint6
                                        uint32_t top_modes, uint32_t top_splits, float threshold,
                                        vvcg_ctu_search_res* res);
 
+/* ---- general-decoder intra prediction -------------------------------------- */
+
+enum { VVCG_ISP_NONE = 0, VVCG_ISP_HOR = 1, VVCG_ISP_VER = 2 };
+enum { VVCG_BDPCM_NONE = 0, VVCG_BDPCM_HOR = 1, VVCG_BDPCM_VER = 2 };
+
+/* One transform block to predict. Luma: Planar / DC / angular with reference
+ * line mrl, ISP sub-partitions (references over the CU width / height plus
+ * the block's, and the shared 4-wide prediction region of narrow vertical
+ * sub-partitions) or BDPCM. Chroma (4:2:0): Planar / DC / angular or CCLM
+ * (mode 81 LM, 82 LM-L, 83 LM-T). */
+typedef struct vvcg_gen_intra_req {
+  uint16_t x, y, w, h;          /* the block in its component's samples */
+  uint16_t cu_x, cu_y, cu_w, cu_h; /* its coding unit in luma samples (ISP) */
+  uint8_t comp;                 /* 0 Y, 1 Cb, 2 Cr */
+  uint8_t mode;                 /* 0..66 (larger luma values act as 66), or 81..83 for chroma */
+  uint8_t mrl;                  /* luma reference line 0..2 */
+  uint8_t isp;                  /* VVCG_ISP_* (luma) */
+  uint8_t bdpcm;                /* VVCG_BDPCM_* (luma) */
+  uint8_t reserved[3];
+  uint32_t out_off;             /* first of the w x h int16 predictions in the output */
+} vvcg_gen_intra_req; /* 28 bytes */
+
+/* The general decoder's state the predictions read: the Y / Cb / Cr planes
+ * (device, 16-bit samples, strides in samples, luma width x height = the
+ * picture padded to whole CTUs) and its decoded-sample maps (device): one
+ * byte per 4x4 luma cell (dec_y, width / 4 x height / 4) and one per chroma
+ * sample (dec_c, width / 2 x height / 2), nonzero where reconstructed. */
+typedef struct vvcg_gen_intra_state {
+  const uint16_t* plane[3];
+  uint32_t stride[3];
+  uint32_t width, height;
+  const uint8_t* dec_y;
+  const uint8_t* dec_c;
+  uint8_t bit_depth;            /* 8..12 */
+  uint8_t vert_collocated;      /* sps_chroma_vertical_collocated_flag */
+  uint8_t reserved[2];
+  uint32_t ctu_size;
+} vvcg_gen_intra_state;
+
+/* Intra prediction of independent transform blocks as the general decoder
+ * forms it (no residual, no reconstruction): reference samples with its
+ * availability and substitution (Gen::gather_len, decode_general.rs:
+ * 4260-4341; gather_mrl :4542-4632; isp_refs :4634-4648), predict_luma
+ * (:4650-4732) and predict_chroma (:4734-4793) with cclm_predict
+ * (:4372-4537), and the 4-wide ISP region of reconstruct_tu (:4001-4024).
+ * Blocks of one call must not read each other's samples (the caller orders
+ * calls along the decode order). reqs host memory, out device memory
+ * (int16). MIP coding units use vvcg_mip_predict_dev. */
+vvcg_status vvcg_gen_intra_predict_dev(vvcg_ctx* ctx, const vvcg_gen_intra_state* state,
+                                       const vvcg_gen_intra_req* reqs, uint32_t num_reqs, int16_t* out,
+                                       uint64_t out_count);
+
 /* ---- general-decoder deblocking ------------------------------------------- */
 
 enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };

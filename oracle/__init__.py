@@ -104,6 +104,8 @@ def _declare(L):
     L.orc_predict_luma_8.restype = None
     L.orc_ctu_search.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint32, vp]
     L.orc_ctu_search.restype = None
+    L.orc_gen_intra_predict.argtypes = [vp, vp, vp, i, i, i, i, vp, vp, i, i, i, vp, i, vp]
+    L.orc_gen_intra_predict.restype = None
     L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
     L.orc_deblock_general.restype = None
     L.orc_dbk_lens.argtypes = [i, i, i, i, vp]
@@ -294,6 +296,21 @@ def search_lambda_q8(qp, bit_depth=10):
     """lambda of the CTU search (SATD domain) in 1/256 units:
     sqrt(0.57 * 2^((qp - 12) / 3)) * 2^(bit_depth - 8)."""
     return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0)) * 2.0 ** (bit_depth - 8)))
+
+
+def gen_intra_predict(y, u, v, dec_y, dec_c, bd, ctu, reqs, out_count, vert_collocated=False):
+    """The general decoder's intra prediction (decode_general.rs:3983-4793)
+    of each request (vvcg_gen_intra_req layout) from the planes (Y at the
+    padded picture size, Cb / Cr at half) and the decoded maps (one byte per
+    4x4 luma cell, one per chroma sample). Returns the int16 output buffer."""
+    y, u, v = _u16(y), _u16(u), _u16(v)
+    dy = np.ascontiguousarray(dec_y, dtype=np.uint8)
+    dc = np.ascontiguousarray(dec_c, dtype=np.uint8)
+    r = np.ascontiguousarray(reqs)
+    out = np.zeros(out_count, np.int16)
+    lib().orc_gen_intra_predict(_p(y), _p(u), _p(v), y.shape[1], u.shape[1], y.shape[1], y.shape[0], _p(dy), _p(dc),
+                                bd, int(vert_collocated), ctu, _p(r), len(r), _p(out))
+    return out
 
 
 def choose_intra_mode(recon, src, bd, bx, by, w, h):

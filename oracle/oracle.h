@@ -131,6 +131,10 @@ int apply_sao_region_16(const Plane16& src, Plane16& dst, int bx, int by, int w,
 // filter.rs:1954-2033 / decode_general.rs:5189-5223: the general decoder's SAO of one plane.
 void sao_plane_bounded_16(const uint16_t* src, uint16_t* dst, int stride, int pw, int ph, int vis_w, int vis_h,
                           int bd, int ctu, int ctu_cols, const Sao* params);
+// predict.rs:2088-2177 derive_cclm_params_from_4_samples (sl / sc reordered in place).
+void cclm_params(int sl[4], int sc[4], int cnt, int bd, int* a_out, int* b_out, int* shift_out);
+// decode_general.rs:4001-4024 / :4260-4793: the general decoder's intra prediction of one block.
+void gen_intra_predict(const vvcg_gen_intra_state& st, const vvcg_gen_intra_req& r, int16_t* out);
 // predict.rs:2737-2801 choose_luma_intra_pred_mode (+ the multi-tool encoder's
 // MRL candidates, slice.rs:2698-2731) and predict_block_full (:2655) on 8-bit planes.
 void luma_intra_search_8(const Plane8& recon, const Plane8& src, int bx, int by, int w, int h, const uint8_t mpm[6],

@@ -189,6 +189,27 @@ extern "C" void orc_ctu_search(const uint16_t* src, int pw, int ph, int bd, int 
   out[8] = (uint32_t)cu_mode;
   out[9] = (uint32_t)(modes[0] | (modes[1] << 8) | (modes[2] << 16) | ((uint32_t)modes[3] << 24));
 }
+// planes Y / Cb / Cr row-major at the given strides; dec_y / dec_c byte maps;
+// reqs in the vvcg_gen_intra_req layout; out int16
+extern "C" void orc_gen_intra_predict(const uint16_t* y, const uint16_t* u, const uint16_t* v, int sy, int sc,
+                                      int width, int height, const uint8_t* dec_y, const uint8_t* dec_c, int bd,
+                                      int vert_collocated, int ctu, const vvcg_gen_intra_req* reqs, int n,
+                                      int16_t* out) {
+  vvcg_gen_intra_state st{};
+  st.plane[0] = y;
+  st.plane[1] = u;
+  st.plane[2] = v;
+  st.stride[0] = sy;
+  st.stride[1] = st.stride[2] = sc;
+  st.width = width;
+  st.height = height;
+  st.dec_y = dec_y;
+  st.dec_c = dec_c;
+  st.bit_depth = (uint8_t)bd;
+  st.vert_collocated = (uint8_t)vert_collocated;
+  st.ctu_size = ctu;
+  for (int i = 0; i < n; i++) orc::gen_intra_predict(st, reqs[i], out + reqs[i].out_off);
+}
 // out: mode, mrl index, SAD (low 32 bits), SAD (high 32 bits)
 extern "C" void orc_luma_intra_search_8(const uint8_t* recon, const uint8_t* src, int pw, int ph, int bx, int by,
                                         int w, int h, const uint8_t* mpm, int mpm_only, int mrl, int ctu,

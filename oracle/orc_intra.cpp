@@ -334,8 +334,7 @@ void predict_coded_block_16(const Plane16& p, int x, int y, int w, int h, bool i
 }
 
 // predict.rs:2088-2177 derive_cclm_params_from_4_samples
-static void cclm_params(int sl[4], int sc[4], int cnt, int bd, int* a_out, int* b_out,
-                        int* shift_out) {
+void cclm_params(int sl[4], int sc[4], int cnt, int bd, int* a_out, int* b_out, int* shift_out) {
   if (cnt == 0) {
     *a_out = 0;
     *b_out = 1 << (bd > 0 ? bd - 1 : 0);

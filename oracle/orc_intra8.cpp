@@ -318,7 +318,265 @@ uint64_t sad_of(const std::vector<int>& p, const Plane8& src, int bx, int by, in
   return s;
 }
 
+// ---- the general decoder (decode_general.rs) ----
+
+struct Gen {
+  const vvcg_gen_intra_state& S;
+  int plane_w(int c) const { return c ? (int)S.width / 2 : (int)S.width; }
+  int plane_h(int c) const { return c ? (int)S.height / 2 : (int)S.height; }
+  int get(int c, int x, int y) const { return S.plane[c][(size_t)y * S.stride[c] + x]; }
+  int dcv() const { return 1 << (clampi(S.bit_depth, 8, 12) - 1); }
+  // Gen::decoded_at (decode_general.rs:4239-4251)
+  bool decoded_at(bool luma, int x, int y) const {
+    if (x < 0 || y < 0) return false;
+    if (luma) {
+      if (x >= (int)S.width || y >= (int)S.height) return false;
+      return S.dec_y[(size_t)(y / 4) * (S.width / 4) + x / 4] != 0;
+    }
+    if (x >= (int)S.width / 2 || y >= (int)S.height / 2) return false;
+    return S.dec_c[(size_t)y * (S.width / 2) + x] != 0;
+  }
+  // Gen::gather_len (decode_general.rs:4260-4341) on component c
+  Refs8 gather_len(int c, bool luma, int x, int y, int top_len, int left_len) const {
+    const int pw = plane_w(c), ph = plane_h(c), d = dcv();
+    std::vector<char> aa(top_len, 0), la(left_len, 0);
+    bool any = false;
+    if (y > 0)
+      for (int k = 0; k < top_len; k++)
+        if (x + k < pw && decoded_at(luma, x + k, y - 1)) aa[k] = any = true;
+    if (x > 0)
+      for (int k = 0; k < left_len; k++)
+        if (y + k < ph && decoded_at(luma, x - 1, y + k)) la[k] = any = true;
+    const bool tl = x > 0 && y > 0 && decoded_at(luma, x - 1, y - 1);
+    if (tl) any = true;
+    int ft = -1, fl = -1;
+    for (int k = 0; k < top_len && ft < 0; k++)
+      if (aa[k]) ft = get(c, x + k, y - 1);
+    for (int k = 0; k < left_len && fl < 0; k++)
+      if (la[k]) fl = get(c, x - 1, y + k);
+    Refs8 r;
+    r.above.assign(top_len, d);
+    r.left.assign(left_len, d);
+    int prev = -1;
+    for (int k = 0; k < top_len; k++) {
+      if (aa[k]) {
+        r.above[k] = prev = get(c, x + k, y - 1);
+      } else {
+        r.above[k] = prev >= 0 ? prev : ft >= 0 ? ft : fl >= 0 ? fl : d;
+      }
+    }
+    prev = -1;
+    for (int k = 0; k < left_len; k++) {
+      if (la[k]) {
+        r.left[k] = prev = get(c, x - 1, y + k);
+      } else {
+        r.left[k] = prev >= 0 ? prev : fl >= 0 ? fl : ft >= 0 ? ft : d;
+      }
+    }
+    r.top_left = tl ? get(c, x - 1, y - 1) : (ft >= 0 ? ft : fl >= 0 ? fl : d);
+    if (!any) {
+      std::fill(r.above.begin(), r.above.end(), d);
+      std::fill(r.left.begin(), r.left.end(), d);
+    }
+    return r;
+  }
+  // Gen::gather_mrl (decode_general.rs:4542-4632)
+  MrlRefs gather_mrl(int x, int y, int w, int h, int mrl) const {
+    const int d = dcv(), off = 1 + mrl, al = 2 * w, ll = 2 * h;
+    MrlRefs m;
+    m.mrl_idx = mrl;
+    m.row_above.assign(al + off + 4, d);
+    m.row_left.assign(ll + off + 4, d);
+    const bool tl = x >= off && y >= off && decoded_at(true, x - off, y - off);
+    if (tl) {
+      m.row_above[0] = m.row_left[0] = get(0, x - off, y - off);
+      for (int i = 1; i < off; i++) {
+        m.row_above[i] = get(0, x - off + i, y - off);
+        m.row_left[i] = get(0, x - off, y - off + i);
+      }
+    }
+    std::vector<char> ta(al, 0), la(ll, 0);
+    if (y >= off)
+      for (int k = 0; k < al; k++)
+        if (x + k < (int)S.width && decoded_at(true, x + k, y - off)) ta[k] = 1;
+    if (x >= off)
+      for (int k = 0; k < ll; k++)
+        if (y + k < (int)S.height && decoded_at(true, x - off, y + k)) la[k] = 1;
+    int ft = -1, fl = -1;
+    for (int k = 0; k < al && ft < 0; k++)
+      if (ta[k]) ft = get(0, x + k, y - off);
+    for (int k = 0; k < ll && fl < 0; k++)
+      if (la[k]) fl = get(0, x - off, y + k);
+    int prev = -1;
+    for (int k = 0; k < al; k++) {
+      if (ta[k])
+        m.row_above[off + k] = prev = get(0, x + k, y - off);
+      else
+        m.row_above[off + k] = prev >= 0 ? prev : ft >= 0 ? ft : fl >= 0 ? fl : d;
+    }
+    for (size_t k = off + al; k < m.row_above.size(); k++) m.row_above[k] = m.row_above[off + al - 1];
+    prev = -1;
+    for (int k = 0; k < ll; k++) {
+      if (la[k])
+        m.row_left[off + k] = prev = get(0, x - off, y + k);
+      else
+        m.row_left[off + k] = prev >= 0 ? prev : fl >= 0 ? fl : ft >= 0 ? ft : d;
+    }
+    for (size_t k = off + ll; k < m.row_left.size(); k++) m.row_left[k] = m.row_left[off + ll - 1];
+    if (!tl) {
+      const int fb = ft >= 0 ? ft : fl >= 0 ? fl : d;
+      for (int i = 0; i < off; i++) m.row_above[i] = m.row_left[i] = fb;
+    }
+    return m;
+  }
+  // Gen::cclm_predict (decode_general.rs:4372-4537); mode 0 LM, 1 LM-L, 2 LM-T
+  std::vector<int> cclm(int comp, int mode, int xc, int yc, int w, int h) const {
+    const int mid = dcv(), maxv = (1 << clampi(S.bit_depth, 8, 12)) - 1;
+    const int xtb = xc * 2, ytb = yc * 2;
+    const bool al = xc > 0 && decoded_at(false, xc - 1, yc);
+    const bool at = yc > 0 && decoded_at(false, xc, yc - 1);
+    const bool ctb = S.ctu_size > 0 && (ytb & (S.ctu_size - 1)) == 0;
+    const bool vc = S.vert_collocated != 0;
+    auto py = [&](int x, int y) {
+      if (y < 0 && !at) y = 0;
+      if (x < 0 && !al) x = 0;
+      return get(0, xtb + x, ytb + y);
+    };
+    int ntr = 0, nlb = 0;
+    if (mode == 2 && at)
+      for (int x = w; x < 2 * w && decoded_at(false, xc + x, yc - 1); x++) ntr++;
+    if (mode == 1 && al)
+      for (int y = h; y < 2 * h && decoded_at(false, xc - 1, yc + y); y++) nlb++;
+    int nt, nl;
+    if (mode == 0) {
+      nt = at ? w : 0;
+      nl = al ? h : 0;
+    } else if (mode == 2) {
+      nt = at ? w + std::min(ntr, h) : 0;
+      nl = 0;
+    } else {
+      nt = 0;
+      nl = al ? h + std::min(nlb, w) : 0;
+    }
+    const int is4n = !(at && al && mode == 0);
+    int sl[4] = {mid, mid, mid, mid}, sc[4] = {mid, mid, mid, mid};
+    int count = 0;
+    auto top_ds = [&](int x) {
+      const int lx = 2 * x;
+      if (ctb) return (py(lx - 1, -1) + 2 * py(lx, -1) + py(lx + 1, -1) + 2) >> 2;
+      if (vc) return (py(lx, -3) + py(lx - 1, -2) + 4 * py(lx, -2) + py(lx + 1, -2) + py(lx, -1) + 4) >> 3;
+      return (py(lx - 1, -1) + py(lx - 1, -2) + 2 * py(lx, -1) + 2 * py(lx, -2) + py(lx + 1, -1) + py(lx + 1, -2) +
+              4) >> 3;
+    };
+    auto left_ds = [&](int y) {
+      const int ly = 2 * y;
+      if (vc) return (py(-2, ly - 1) + py(-3, ly) + 4 * py(-2, ly) + py(-1, ly) + py(-2, ly + 1) + 4) >> 3;
+      return (py(-3, ly) + py(-3, ly + 1) + 2 * py(-2, ly) + 2 * py(-2, ly + 1) + py(-1, ly) + py(-1, ly + 1) +
+              4) >> 3;
+    };
+    if (nt > 0) {
+      const int start = nt >> (2 + is4n), step = std::max(1, nt >> (1 + is4n)), cnt = std::min(nt, (1 + is4n) << 1);
+      for (int pos = 0; pos < cnt; pos++) {
+        const int x = start + pos * step;
+        if (x >= nt) break;
+        sl[count] = top_ds(x);
+        sc[count] = get(comp, xc + x, yc - 1);
+        count++;
+      }
+    }
+    if (nl > 0) {
+      const int start = nl >> (2 + is4n), step = std::max(1, nl >> (1 + is4n)), cnt = std::min(nl, (1 + is4n) << 1);
+      for (int pos = 0; pos < cnt; pos++) {
+        const int y = start + pos * step;
+        if (y >= nl) break;
+        sl[count] = left_ds(y);
+        sc[count] = get(comp, xc - 1, yc + y);
+        count++;
+      }
+    }
+    if (count == 0) return std::vector<int>(w * h, mid);
+    int a, b, shift;
+    cclm_params(sl, sc, count, S.bit_depth, &a, &b, &shift);
+    std::vector<int> out(w * h);
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) {
+        const int lx = 2 * x, ly = 2 * y;
+        const int ds = vc ? (py(lx, ly - 1) + py(lx - 1, ly) + 4 * py(lx, ly) + py(lx + 1, ly) + py(lx, ly + 1) + 4) >> 3
+                          : (py(lx - 1, ly) + py(lx - 1, ly + 1) + 2 * py(lx, ly) + 2 * py(lx, ly + 1) +
+                             py(lx + 1, ly) + py(lx + 1, ly + 1) + 4) >> 3;
+        out[y * w + x] = clampi(((ds * a) >> shift) + b, 0, maxv);
+      }
+    return out;
+  }
+  // predict_luma (decode_general.rs:4650-4732) for an intra CU
+  std::vector<int> luma(const vvcg_gen_intra_req& r, int x, int y, int w, int h) const {
+    const int mode = r.mode;
+    if (r.bdpcm) {  // predict_bdpcm (predict.rs:1993-2010) on gather_avail
+      Refs8 refs = gather_len(0, true, x, y, 2 * w, 2 * h);
+      std::vector<int> p(w * h);
+      for (int yy = 0; yy < h; yy++)
+        for (int xx = 0; xx < w; xx++) p[yy * w + xx] = r.bdpcm == VVCG_BDPCM_VER ? refs.above[xx] : refs.left[yy];
+      return p;
+    }
+    const bool isp = r.isp != VVCG_ISP_NONE;
+    const int mrl = std::min<int>(r.mrl, 2);
+    MrlRefs m = isp ? from_refs(gather_len(0, true, x, y, r.cu_w + w, r.cu_h + h))
+                    : mrl == 0 ? from_refs(gather_len(0, true, x, y, 2 * w, 2 * h)) : gather_mrl(x, y, w, h, mrl);
+    const int off = m.mrl_idx;
+    Refs8 base;
+    base.above.assign(m.row_above.begin() + off + 1, m.row_above.begin() + off + 1 + 2 * w);
+    base.left.assign(m.row_left.begin() + off + 1, m.row_left.begin() + off + 1 + 2 * h);
+    base.top_left = m.row_above[off];
+    if (mode == PLANAR || mode == DC) {
+      const Refs8 used = (mode == PLANAR && mrl == 0 && !isp && w * h > 32) ? filtered(base) : base;
+      std::vector<int> p = mode == PLANAR ? planar(used, w, h) : dc(used, w, h);
+      if (mrl == 0 && w >= 4 && h >= 4) pdpc(p, used, w, h);
+      return p;
+    }
+    const int dir = std::min(mode, 66);
+    AngularParams P = init_angular_params(dir, w, h, r.cu_w, r.cu_h, true, mrl, isp);
+    if (mrl == 0 && !isp)
+      return angular(from_refs(P.ref_filter_flag ? filtered(base) : base), w, h, true, P, S.bit_depth);
+    return angular(m, w, h, true, P, S.bit_depth);
+  }
+  // predict_chroma (decode_general.rs:4734-4793) for an intra CU
+  std::vector<int> chroma(const vvcg_gen_intra_req& r) const {
+    const int c = r.comp, x = r.x, y = r.y, w = r.w, h = r.h, mode = r.mode;
+    if (mode >= 81 && mode <= 83) return cclm(c, mode == 81 ? 0 : mode == 82 ? 1 : 2, x, y, w, h);
+    Refs8 refs = gather_len(c, false, x, y, 2 * w, 2 * h);
+    if (mode == PLANAR || mode == DC) {
+      std::vector<int> p = mode == PLANAR ? planar(refs, w, h) : dc(refs, w, h);
+      if (w >= 4 && h >= 4) pdpc(p, refs, w, h);
+      return p;
+    }
+    AngularParams P = init_angular_params(std::min(mode, 66), w, h, w, h, false, 0, false);  // predict_angular_bd
+    return angular(from_refs(refs), w, h, false, P, S.bit_depth);
+  }
+};
+
 }  // namespace
+
+// reconstruct_tu's prediction (decode_general.rs:3983-4024): the block's
+// prediction into out (w * h); a narrow vertical ISP sub-partition takes its
+// columns of the 4-wide region it shares.
+void gen_intra_predict(const vvcg_gen_intra_state& st, const vvcg_gen_intra_req& r, int16_t* out) {
+  Gen g{st};
+  std::vector<int> p;
+  if (r.comp == 0) {
+    if (r.isp == VVCG_ISP_VER && (r.cu_w == 4 || (r.cu_w == 8 && r.cu_h > 4))) {
+      const int rx = r.cu_x + ((r.x - r.cu_x) / 4) * 4;
+      std::vector<int> full = g.luma(r, rx, r.y, 4, r.h);
+      p.resize(r.w * r.h);
+      for (int yy = 0; yy < r.h; yy++)
+        for (int xx = 0; xx < r.w; xx++) p[yy * r.w + xx] = full[yy * 4 + (r.x - rx) + xx];
+    } else {
+      p = g.luma(r, r.x, r.y, r.w, r.h);
+    }
+  } else {
+    p = g.chroma(r);
+  }
+  for (int i = 0; i < r.w * r.h; i++) out[i] = (int16_t)p[i];
+}
 
 // predict.rs:2737-2801 choose_luma_intra_pred_mode (Planar wins ties: the
 // first candidate with the lowest SAD), then, with mrl, the MRL loop of

@@ -67,6 +67,20 @@ CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), (
                                  ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
 SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
 CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30761, 73, 67, 6
+GEN_INTRA_REQ_DTYPE = np.dtype([("x", "<u2"), ("y", "<u2"), ("w", "<u2"), ("h", "<u2"), ("cu_x", "<u2"),
+                                ("cu_y", "<u2"), ("cu_w", "<u2"), ("cu_h", "<u2"), ("comp", "u1"), ("mode", "u1"),
+                                ("mrl", "u1"), ("isp", "u1"), ("bdpcm", "u1"), ("reserved", "u1", (3,)),
+                                ("out_off", "<u4")])
+ISP_NONE, ISP_HOR, ISP_VER = 0, 1, 2
+BDPCM_NONE, BDPCM_HOR, BDPCM_VER = 0, 1, 2
+
+
+class _GenIntraState(C.Structure):
+    _fields_ = [("plane", C.c_void_p * 3), ("stride", C.c_uint32 * 3), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("dec_y", C.c_void_p), ("dec_c", C.c_void_p), ("bit_depth", C.c_uint8),
+                ("vert_collocated", C.c_uint8), ("reserved", C.c_uint8 * 2), ("ctu_size", C.c_uint32)]
+
+
 DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
                            ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
 DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
@@ -158,6 +172,7 @@ assert MIP_REQ_DTYPE.itemsize == 16 and MIP_RES_DTYPE.itemsize == 16
 assert ALF_CTU_DTYPE.itemsize == 8 and ALF_PARAMS_DTYPE.itemsize == 1192
 assert ISR_REQ_DTYPE.itemsize == 20 and ISR_RES_DTYPE.itemsize == 16
 assert CTU_SEARCH_REQ_DTYPE.itemsize == 16 and CTU_SEARCH_RES_DTYPE.itemsize == 36
+assert GEN_INTRA_REQ_DTYPE.itemsize == 28
 assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_PARAMS_DTYPE.itemsize == 172
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
@@ -229,6 +244,7 @@ def lib():
         L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, u32, vp, vp, vp, vp, vp]
         L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
                                               vp, vp, vp]
+        L.vvcg_gen_intra_predict_dev.argtypes = [vp, vp, vp, u32, vp, u64]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
@@ -635,6 +651,29 @@ class Context:
             return None
         torch.cuda.synchronize(src.device)
         return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:n]
+
+    # -- general-decoder intra prediction --
+    def gen_intra_predict(self, planes, dec_y, dec_c, bit_depth, ctu, reqs, out_count, vert_collocated=False):
+        """planes: (Y, Cb, Cr) int16 CUDA tensors (Y at the padded picture
+        size); dec_y / dec_c: uint8 CUDA tensors (one byte per 4x4 luma cell /
+        per chroma sample); reqs: GEN_INTRA_REQ_DTYPE host records. Returns
+        the int16 CUDA output of out_count samples (synchronises)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=GEN_INTRA_REQ_DTYPE)
+        st = _GenIntraState()
+        for c in range(3):
+            st.plane[c] = planes[c].data_ptr()
+            st.stride[c] = planes[c].stride(0)
+        st.height, st.width = planes[0].shape
+        st.dec_y, st.dec_c = dec_y.data_ptr(), dec_c.data_ptr()
+        st.bit_depth, st.vert_collocated, st.ctu_size = bit_depth, int(vert_collocated), ctu
+        out = torch.zeros(max(out_count, 1), dtype=torch.int16, device=planes[0].device)
+        self._keep = (reqs, st)
+        self._check(self._L.vvcg_gen_intra_predict_dev(self._h, C.byref(st), _ptr(reqs), len(reqs), _ptr(out),
+                                                       out_count))
+        torch.cuda.synchronize(planes[0].device)
+        return out
 
     # -- general-decoder deblocking --
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):

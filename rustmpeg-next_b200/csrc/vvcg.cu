@@ -17,6 +17,7 @@
 #include "dbk_general.cuh"
 #include "enc.cuh"
 #include "filters.cuh"
+#include "gen_intra.cuh"
 #include "intra_search.cuh"
 #include "prune.cuh"
 #include "lmcs.cuh"
@@ -1553,6 +1554,65 @@ extern "C" vvcg_status vvcg_tc_selftest_dev(vvcg_ctx* ctx, const uint16_t* a, co
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   k_umma_selftest<<<1, 128, 0, ctx->stream>>>(a, b, d, status);
   CK(cudaGetLastError(), "self-test launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// General-decoder intra prediction (vvcg_gen_intra_predict_dev).
+// ---------------------------------------------------------------------------
+static bool pow2_in(uint32_t v, uint32_t lo, uint32_t hi) { return v >= lo && v <= hi && (v & (v - 1)) == 0; }
+
+extern "C" vvcg_status vvcg_gen_intra_predict_dev(vvcg_ctx* ctx, const vvcg_gen_intra_state* st,
+                                                  const vvcg_gen_intra_req* reqs, uint32_t num_reqs, int16_t* out,
+                                                  uint64_t out_count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!st || !reqs || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing state, requests or output");
+  if (!st->plane[0] || !st->plane[1] || !st->plane[2] || !st->dec_y || !st->dec_c)
+    return fail(ctx, VVCG_INVALID_INPUT, "missing planes or decoded maps");
+  if (!st->width || !st->height || (st->width & 7) || (st->height & 7))
+    return fail(ctx, VVCG_INVALID_INPUT, "picture size must be a multiple of 8");
+  if (st->width > 16384 || st->height > 16384) return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture larger than 16384");
+  if (st->stride[0] < st->width || st->stride[1] < st->width / 2 || st->stride[2] < st->width / 2)
+    return fail(ctx, VVCG_INVALID_INPUT, "stride smaller than the plane width");
+  if (st->bit_depth < 8 || st->bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "bit depth");
+  if (st->ctu_size && !pow2_in(st->ctu_size, 16, 128)) return fail(ctx, VVCG_INVALID_INPUT, "CTU size");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_gen_intra_req& r = reqs[i];
+    if (r.comp > 2) return fail(ctx, VVCG_INVALID_INPUT, "request %u: component", i);
+    if ((uint64_t)r.out_off + (uint64_t)r.w * r.h > out_count)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: output past the buffer", i);
+    if (r.comp == 0) {
+      if (!pow2_in(r.w, 1, 64) || !pow2_in(r.h, 1, 64) || r.x + r.w > st->width || r.y + r.h > st->height)
+        return fail(ctx, VVCG_INVALID_INPUT, "request %u: luma block", i);
+      if (r.mrl > 2 || r.isp > VVCG_ISP_VER || r.bdpcm > VVCG_BDPCM_VER)
+        return fail(ctx, VVCG_INVALID_INPUT, "request %u: mrl / isp / bdpcm", i);
+      if (r.isp != VVCG_ISP_NONE) {
+        if (!pow2_in(r.cu_w, 4, 64) || !pow2_in(r.cu_h, 4, 64) || r.x < r.cu_x || r.y < r.cu_y ||
+            r.x + r.w > r.cu_x + r.cu_w || r.y + r.h > r.cu_y + r.cu_h)
+          return fail(ctx, VVCG_INVALID_INPUT, "request %u: ISP sub-partition outside its CU", i);
+        if (r.isp == VVCG_ISP_VER && (r.cu_w == 4 || (r.cu_w == 8 && r.cu_h > 4)) && (r.cu_x & 3))
+          return fail(ctx, VVCG_INVALID_INPUT, "request %u: ISP region off the 4-sample grid", i);
+      } else if (r.mrl && (r.w < 4 || r.h < 4)) {
+        return fail(ctx, VVCG_INVALID_INPUT, "request %u: MRL on a block below 4x4", i);
+      }
+    } else {
+      if (!pow2_in(r.w, 2, 32) || !pow2_in(r.h, 2, 32) || r.x + r.w > st->width / 2 || r.y + r.h > st->height / 2)
+        return fail(ctx, VVCG_INVALID_INPUT, "request %u: chroma block", i);
+      if (r.mode > 66 && (r.mode < 81 || r.mode > 83)) return fail(ctx, VVCG_INVALID_INPUT, "request %u: mode", i);
+      if (r.mode >= 81 && ((r.x | r.y) & 1)) return fail(ctx, VVCG_INVALID_INPUT, "request %u: CCLM position", i);
+    }
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_gen_intra_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(vvcg_gen_intra_req) * num_reqs, cudaMemcpyHostToDevice,
+                     ctx->stream),
+     "upload");
+  GenIntraArgs A{*st, (const vvcg_gen_intra_req*)ctx->d_tu_recs.p, (int32_t)num_reqs, out};
+  const uint32_t grid = std::min<uint32_t>((num_reqs + kGiWarps - 1) / kGiWarps, (uint32_t)ctx->num_sms * 8);
+  k_gen_intra<<<grid, kGiWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "intra launch");
   ctx->launches++;
   return VVCG_OK;
 }

@@ -497,3 +497,79 @@ def random_deblock_picture(vis_w, vis_h, ctu=32, bd=10, seed=0, dual_tree=False,
     params["num_ref"] = [3, 2]
     params["ref_poc"] = rng.integers(-8, 9, (2, 16))
     return planes, cells, cc, params
+
+
+def random_gen_intra_state(width, height, bd=10, seed=0, hole_prob=0.15):
+    """Planes and decoded maps for the general decoder's intra prediction:
+    smooth content with noise (Y at width x height, Cb / Cr at half), and
+    decoded maps that are the raster-order decode of a random position
+    (everything above it and left of it on its CTU row band) with random
+    holes; one byte per 4x4 luma cell, one per chroma sample."""
+    rng = np.random.default_rng(seed)
+    maxv = (1 << bd) - 1
+    y, u, v = value_noise_frame(max(width, 128), max(height, 128), 10, frame=seed)
+    sc = (lambda p: (p.astype(np.int32) << (bd - 10)) if bd >= 10 else (p.astype(np.int32) >> (10 - bd)))
+    Y = np.clip(sc(y[:height, :width]) + rng.integers(-3, 4, (height, width)), 0, maxv).astype(np.uint16)
+    U = np.clip(sc(u[:height // 2, :width // 2]) + rng.integers(-3, 4, (height // 2, width // 2)), 0, maxv).astype(np.uint16)
+    V = np.clip(sc(v[:height // 2, :width // 2]) + rng.integers(-3, 4, (height // 2, width // 2)), 0, maxv).astype(np.uint16)
+    cy, cx = rng.integers(0, height), rng.integers(0, width)
+    yy, xx = np.mgrid[0:height // 4, 0:width // 4]
+    dec_y = ((yy * 4 < cy - 32) | ((yy * 4 < cy + 32) & (xx * 4 < cx))).astype(np.uint8)
+    dec_y &= (rng.random(dec_y.shape) >= hole_prob).astype(np.uint8)
+    yc, xc = np.mgrid[0:height // 2, 0:width // 2]
+    dec_c = ((yc * 2 < cy - 32) | ((yc * 2 < cy + 32) & (xc * 2 < cx))).astype(np.uint8)
+    dec_c &= (rng.random(dec_c.shape) >= hole_prob / 4).astype(np.uint8)
+    return (Y, U, V), dec_y, dec_c
+
+
+def random_gen_intra_reqs(width, height, n, seed=0):
+    """Random requests of every kind (GEN_INTRA_REQ_DTYPE) inside a width x
+    height picture: luma blocks 4..64 with Planar / DC / angular (MRL 0..2),
+    BDPCM, ISP sub-partitions of 4..64-sample CUs (1..64 samples, including
+    the narrow vertical ones that share a 4-wide region), and chroma blocks
+    2..32 with Planar / DC / angular / CCLM."""
+    from . import GEN_INTRA_REQ_DTYPE
+
+    rng = np.random.default_rng(seed)
+    r = np.zeros(n, GEN_INTRA_REQ_DTYPE)
+    off = 0
+    for i in range(n):
+        q = r[i]
+        kind = int(rng.integers(0, 6))
+        if kind <= 2:  # luma regular / MRL / BDPCM
+            w, h = 1 << int(rng.integers(2, 7)), 1 << int(rng.integers(2, 7))
+            x = int(rng.integers(0, (width - w) // 4 + 1)) * 4
+            y = int(rng.integers(0, (height - h) // 4 + 1)) * 4
+            q["comp"], q["x"], q["y"], q["w"], q["h"] = 0, x, y, w, h
+            q["cu_x"], q["cu_y"], q["cu_w"], q["cu_h"] = x, y, w, h
+            q["mode"] = int(rng.integers(0, 67))
+            if kind == 1:
+                q["mrl"] = int(rng.integers(1, 3))
+            if kind == 2:
+                q["bdpcm"] = int(rng.integers(1, 3))
+        elif kind == 3:  # ISP sub-partition
+            cw, ch = 1 << int(rng.integers(2, 7)), 1 << int(rng.integers(2, 7))
+            cx = int(rng.integers(0, (width - cw) // 4 + 1)) * 4
+            cy = int(rng.integers(0, (height - ch) // 4 + 1)) * 4
+            ver = bool(rng.integers(0, 2))
+            nparts = 2 if (cw, ch) in ((4, 8), (8, 4)) else 4
+            k = int(rng.integers(0, nparts))
+            if ver:
+                w, h = max(1, cw // nparts), ch
+                x, y = cx + k * w, cy
+            else:
+                w, h = cw, max(1, ch // nparts)
+                x, y = cx, cy + k * h
+            q["comp"], q["x"], q["y"], q["w"], q["h"] = 0, x, y, w, h
+            q["cu_x"], q["cu_y"], q["cu_w"], q["cu_h"] = cx, cy, cw, ch
+            q["isp"] = 2 if ver else 1
+            q["mode"] = int(rng.integers(0, 67))
+        else:  # chroma
+            w, h = 1 << int(rng.integers(1, 6)), 1 << int(rng.integers(1, 6))
+            x = int(rng.integers(0, (width // 2 - w) // 2 + 1)) * 2
+            y = int(rng.integers(0, (height // 2 - h) // 2 + 1)) * 2
+            q["comp"], q["x"], q["y"], q["w"], q["h"] = int(rng.integers(1, 3)), x, y, w, h
+            q["mode"] = int(rng.choice([0, 1, int(rng.integers(2, 67)), 81, 82, 83]))
+        q["out_off"] = off
+        off += int(q["w"]) * int(q["h"])
+    return r, off
