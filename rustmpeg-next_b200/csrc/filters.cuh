@@ -416,6 +416,7 @@ struct SaoPass {
   int32_t stride, w, h, bd, comp;
   int32_t ctu_w_log2, ctu_h_log2;  // CTU size in this plane's samples (powers of 2)
   int32_t ctu_cols;                // CTUs per row
+  uint32_t cols_magic;             // ceil(2^32 / ctu_cols): ctu / ctu_cols = umulhi(ctu, magic)
 };
 
 // apply_sao_region_16 (filter.rs:1880-1947), every sample of the plane; the
@@ -442,18 +443,21 @@ __device__ __forceinline__ void unpack4(uint2 v, int* o) {
 __global__ void __launch_bounds__(256) k_sao(const SaoPass* __restrict__ passes, uint32_t* status) {
   const SaoPass& S = passes[blockIdx.y];
   const int lane = threadIdx.x & 31;
-  const int tpr = max(1, (1 << S.ctu_w_log2) >> 2);   // lanes per CTU row
-  const int rpw = 32 / tpr;                            // CTU rows per warp
+  // CTU sizes are powers of two: shifts and masks only (a CTU row is at
+  // least 4 and at most 32 lanes), and one multiply-high for the CTU row
+  const int tpr_log2 = max(0, S.ctu_w_log2 - 2);       // lanes per CTU row (log2)
+  const int rpw_log2 = 5 - tpr_log2;                   // CTU rows per warp (log2)
   const int ctu_h = 1 << S.ctu_h_log2;
-  const int groups = (ctu_h + rpw - 1) / rpw;
+  const int groups_log2 = max(0, S.ctu_h_log2 - rpw_log2);
   const int n_ctu = S.ctu_cols * ((S.h + ctu_h - 1) >> S.ctu_h_log2);
   const int item = blockIdx.x * 8 + (threadIdx.x >> 5);
-  if (item >= n_ctu * groups) return;
-  const int ctu = item / groups, grp = item - ctu * groups;
-  const int cxs = (ctu % S.ctu_cols) << S.ctu_w_log2, cys = (ctu / S.ctu_cols) << S.ctu_h_log2;
-  const int x = cxs + (lane % tpr) * 4;
-  const int y = cys + grp * rpw + lane / tpr;
-  if (lane >= tpr * rpw || x >= S.w || y >= S.h || y >= cys + ctu_h) return;
+  if (item >= (n_ctu << groups_log2)) return;
+  const int ctu = item >> groups_log2, grp = item & ((1 << groups_log2) - 1);
+  const int cyi = (int)__umulhi((uint32_t)ctu, S.cols_magic), cxi = ctu - cyi * S.ctu_cols;
+  const int cxs = cxi << S.ctu_w_log2, cys = cyi << S.ctu_h_log2;
+  const int x = cxs + ((lane & ((1 << tpr_log2) - 1)) << 2);
+  const int y = cys + (grp << rpw_log2) + (lane >> tpr_log2);
+  if (x >= S.w || y >= S.h || y >= cys + ctu_h) return;
   const int st = S.stride, w = S.w, h = S.h;
   const uint16_t* src = S.src;
   int c[4];

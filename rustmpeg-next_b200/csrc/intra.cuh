@@ -199,12 +199,14 @@ __device__ __forceinline__ bool in_phase(int phase, int x, int y, int w, int h, 
 }
 
 // Reconstruction of the pairs of one w x h block that belong to `phase`:
-// `pred(x, y, v0, v1)` gives the prediction of the pair (x, x+1) of row y; the
+// `pred(x, y)` gives the prediction of sample (x, y), called for the two
+// samples of a pair in a loop kept rolled (instruction-cache misses, not
+// arithmetic, limit the wavefront kernels); the
 // lane's residual pairs (int16 in a plane-strided buffer, nullable) are all
 // fetched before the first is used, then clip(pred + res) is stored with
 // 32-bit stores (into the plane when `store`). `keep` (nullable) receives the
 // samples (int16 raster, width w).
-constexpr int kPairChunk = 4;  // pairs per lane fetched and emitted together
+constexpr int kPairChunk = 1;  // pairs per lane fetched and emitted together
 template <class F>
 __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, int y0, int w, int h,
                                            const int16_t* res, int16_t* keep, bool store, int phase,
@@ -231,10 +233,11 @@ __device__ __forceinline__ void emit_block(const DevPic& P, int comp, int x0, in
       const int q = lane + 32 * (k0 + k);
       const int y = (2 * q) >> lw, x = (2 * q) & (w - 1);
       if (q < npair && in_phase(phase, x, y, w, h, rows, cols)) {
-        int v0, v1;
-        pred(x, y, v0, v1);
-        v0 = clampi(v0 + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
-        v1 = clampi(v1 + (int)(int16_t)(rv[k] >> 16), 0, maxv);
+        int pv[2];
+#pragma unroll 1
+        for (int t = 0; t < 2; t++) pv[t] = pred(x + t, y);
+        const int v0 = clampi(pv[0] + (int)(int16_t)(rv[k] & 0xFFFFu), 0, maxv);
+        const int v1 = clampi(pv[1] + (int)(int16_t)(rv[k] >> 16), 0, maxv);
         const uint32_t pk = (uint32_t)v0 | ((uint32_t)v1 << 16);
         if (store) *reinterpret_cast<uint32_t*>(base + (size_t)y * st + x) = pk;
         if (keep) *reinterpret_cast<uint32_t*>(&keep[y * w + x]) = pk;
@@ -337,41 +340,30 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     const int shift = lw + lh + 1;
     const int tr = A[w], bl = L[h];
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx, int ry) -> int {
       const int left = L[ry];
       const int wt = 32 >> min(31, (ry * 2) >> sc);
-      int v[2];
-#pragma unroll
-      for (int t = 0; t < 2; t++) {
-        const int rx = rx0 + t;
-        // exact in int32 for bd <= 12 and w, h <= 64
-        int ver = (h - 1 - ry) * A[rx] + (ry + 1) * bl;
-        int hor = (w - 1 - rx) * left + (rx + 1) * tr;
-        int val = clampi(((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift, 0, maxv);
-        int wl = 32 >> min(31, (rx * 2) >> sc);
-        v[t] = clampi(val + ((wl * (left - val) + wt * (A[rx] - val) + 32) >> 6), 0, maxv);
-      }
-      v0 = v[0];
-      v1 = v[1];
+      // exact in int32 for bd <= 12 and w, h <= 64
+      int ver = (h - 1 - ry) * A[rx] + (ry + 1) * bl;
+      int hor = (w - 1 - rx) * left + (rx + 1) * tr;
+      int val = clampi(((ver << lw) + (hor << lh) + (1 << (shift - 1))) >> shift, 0, maxv);
+      int wl = 32 >> min(31, (rx * 2) >> sc);
+      return clampi(val + ((wl * (left - val) + wt * (A[rx] - val) + 32) >> 6), 0, maxv);
     });
     return;
   }
   if (mode == 1) {
     const int dc = S.dc;
     const int sc = (lw + lh >= 2 ? lw + lh - 2 : 0) >> 2;
-    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx0, int ry, int& v0, int& v1) {
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int rx, int ry) -> int {
       const int wt = 32 >> min(31, (ry * 2) >> sc);
-      int wl0 = 32 >> min(31, (rx0 * 2) >> sc), wl1 = 32 >> min(31, ((rx0 + 1) * 2) >> sc);
-      v0 = clampi(dc + ((wl0 * (S.left[ry] - dc) + wt * (S.above[rx0] - dc) + 32) >> 6), 0, maxv);
-      v1 = clampi(dc + ((wl1 * (S.left[ry] - dc) + wt * (S.above[rx0 + 1] - dc) + 32) >> 6), 0, maxv);
+      const int wl = 32 >> min(31, (rx * 2) >> sc);
+      return clampi(dc + ((wl * (S.left[ry] - dc) + wt * (S.above[rx] - dc) + 32) >> 6), 0, maxv);
     });
     return;
   }
   if (mode < 2 || mode > 66) {
-    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int, int, int& v0, int& v1) {
-      v0 = 0;
-      v1 = 0;
-    });
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int, int) -> int { return 0; });
     return;
   }
   const AngP p = angular_params(mode, w, h, is_luma);
@@ -392,14 +384,8 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
       }
       return val;
     };
-    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
-      if (p.is_ver) {
-        v0 = sample(ox0, oy);
-        v1 = sample(ox0 + 1, oy);
-      } else {
-        v0 = sample(oy, ox0);
-        v1 = sample(oy, ox0 + 1);
-      }
+    emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox, int oy) -> int {
+      return p.is_ver ? sample(ox, oy) : sample(oy, ox);
     });
     return;
   }
@@ -437,15 +423,9 @@ __device__ __noinline__ void emit_intra(const DevPic& P, int comp, int x0, int y
     }
     return val;
   };
-  emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox0, int oy, int& v0, int& v1) {
-    if (p.is_ver) {
-      v0 = sample(ox0, oy);
-      v1 = sample(ox0 + 1, oy);
-    } else {
-      v0 = sample(oy, ox0);
-      v1 = sample(oy, ox0 + 1);
-    }
-  });
+  emit_block(P, comp, x0, y0, w, h, res, keep, store, phase, rows, cols, [&](int ox, int oy) -> int {
+      return p.is_ver ? sample(ox, oy) : sample(oy, ox);
+    });
 }
 
 // CCLM templates and linear models for both chroma components of the chroma
@@ -648,9 +628,8 @@ __device__ __noinline__ void emit_cclm(const DevPic& P, int comp, int bxc, int b
     }
     return T(bx + x, by + y);
   };
-  emit_block(P, comp, bxc, byc, cw, ch, res, keep, store, phase, 1, 1, [&](int x, int y, int& v0, int& v1) {
-    v0 = clampi(((ds(x, y) * a) >> shift) + b, 0, maxv);
-    v1 = clampi(((ds(x + 1, y) * a) >> shift) + b, 0, maxv);
+  emit_block(P, comp, bxc, byc, cw, ch, res, keep, store, phase, 1, 1, [&](int x, int y) -> int {
+    return clampi(((ds(x, y) * a) >> shift) + b, 0, maxv);
   });
 }
 

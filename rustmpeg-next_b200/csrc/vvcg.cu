@@ -600,7 +600,8 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
       sao_ran = true;
       for (int c = 0; c < ncomp; c++) {
         SaoPass s{P.plane[c], P.scratch[c], P.ctus, P.stride[c], P.pw[c], P.ph[c], P.bd, c,
-                  ilog2_host(c ? P.ctu / P.sub_w : P.ctu), ilog2_host(c ? P.ctu / P.sub_h : P.ctu), P.ctu_w};
+                  ilog2_host(c ? P.ctu / P.sub_w : P.ctu), ilog2_host(c ? P.ctu / P.sub_h : P.ctu), P.ctu_w,
+                  (uint32_t)(((1ull << 32) + (uint64_t)P.ctu_w - 1) / (uint64_t)P.ctu_w)};
         ctx->sao.push_back(s);
         L.final_in_scratch[c] = 1;
       }
