@@ -12,8 +12,8 @@ value : device-resident throughput (records already in HBM; the 466 MB level
 e2e   : the same through the C ABI with host buffers, streamed: every step
         copies the records from pinned host memory, runs, and copies the
         visible planes back to pinned host memory (vvcg_decode_batch_async,
-        vvcg_batch_sync); steps alternate two contexts so that one step's
-        download overlaps the next step's upload and kernels. Wall-clock time
+        vvcg_batch_sync); steps rotate over three contexts so that one step's
+        download overlaps the next steps' uploads and kernels. Wall-clock time
         over the steps, fill and drain included.
 Multi-GPU: replicas (each rank reconstructs its own batch; no collective on the
 data path); time is the max over ranks.
@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG_DIR = os.path.join(ROOT, "rustmpeg-next_b200")
 PIX_W, PIX_H, CODED_H = 1920, 1080, 1088
 QPS = (22, 27, 32, 37)
+E2E_LANES = 3  # contexts the end-to-end stream rotates over
 METRIC = "VVC recon+filter Mpx/s bit-exact"
 
 
@@ -288,35 +289,38 @@ def main():
     h2d = cus.nbytes + levels.nbytes + ctus.nbytes + aps.nbytes
     d2h = n_pics * PIX_W * PIX_H * 2 * 3 // 2
 
-    # Streaming through the host-buffer call: steps alternate two contexts
-    # (vvcg_decode_batch_async + vvcg_batch_sync), each with its own pinned
-    # output planes, so one step's download overlaps the next step's upload
-    # and kernels. Every step still copies its records in and its planes out.
-    ctx_b = pkg.Context(local)
-    outs_b = [tuple(torch.empty(a.shape, dtype=torch.int16).pin_memory().numpy().view(np.uint16) for a in o)
-              for o in outs]
-    lanes = [(ctx, outs), (ctx_b, outs_b)]
-    busy = [False, False]
+    # Streaming through the host-buffer call: steps rotate over E2E_LANES
+    # contexts (vvcg_decode_batch_async + vvcg_batch_sync), each with its own
+    # pinned output planes, so one step's download (the longest copy) overlaps
+    # the following steps' uploads and kernels. Every step still copies its
+    # records in and its planes out.
+    lanes = [(ctx, outs)]
+    for _ in range(E2E_LANES - 1):
+        lanes.append((pkg.Context(local),
+                      [tuple(torch.empty(a.shape, dtype=torch.int16).pin_memory().numpy().view(np.uint16) for a in o)
+                       for o in outs]))
+    busy = [False] * len(lanes)
 
     def e2e_step(i):
-        c, o = lanes[i % 2]
-        if busy[i % 2]:
+        j = i % len(lanes)
+        c, o = lanes[j]
+        if busy[j]:
             c.sync()
         c.decode_batch_async(batch, o)
-        busy[i % 2] = True
+        busy[j] = True
 
     def e2e_drain():
-        for j in range(2):
+        for j in range(len(lanes)):
             if busy[j]:
                 lanes[j][0].sync()
                 busy[j] = False
 
-    for i in range(2):
+    for i in range(len(lanes)):
         e2e_step(i)
     e2e_drain()
     sync_all()
     t0 = time.perf_counter()
-    k_e2e = max(6, args.steps // 2)
+    k_e2e = max(3 * E2E_LANES, args.steps // 2)
     for i in range(k_e2e):
         e2e_step(i)
     e2e_drain()
@@ -394,12 +398,19 @@ def main():
 CNN_FLOP_PER_BLOCK = 2 * 1024 * 32 * 9 * (2 + 3 * 32)  # conv1 (2 inputs) + 3 x conv 32->32 (57.8 MFLOP)
 
 
+# CNN pruning policies (top modes, top splits, probability-mass threshold);
+# the first is the headline, the others show the speed / cost trade-off.
+PRUNE_POLICIES = ((6, 2, 0.7), (3, 2, 0.0), (6, 3, 0.7), (6, 2, 0.8), (3, 3, 0.8))
+
+
 def bench_encoder(pkg, ctx, stream, dev, args, peaks):
     """The encoder's candidate-cost stage on 1080p 10-bit frames: full search
-    (6 split types x 67 modes per block) against the CNN-pruned search (top-3
-    modes, top-2 splits, full set when the largest softmax is below 0.4),
+    (6 split types x 67 modes per block) against the CNN-pruned search (the
+    top modes and split types of the pruner's softmax; a head keeps its full
+    set when those hold less than the threshold of its probability mass),
     with the pruner trained here on full-search labels (Adam, lr 1e-3, batch
-    1024) from frames other than the evaluated ones."""
+    1024) from frames other than the evaluated ones. Pruned times include the
+    CNN forward pass."""
     import torch
 
     from rustmpeg_next_b200 import cnn
@@ -435,41 +446,48 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
         y, _, _ = synth.value_noise_frame(PIX_W, PIX_H, 10, frame=900000 + f)
         frames.append(torch.from_numpy(np.ascontiguousarray(y.astype(np.uint16)).view(np.int16)).to(dev))
     untrained = torch.from_numpy(cnn.init_params(12345)).to(dev)
-    full_ms = pruned_ms = cnn_ms = 0.0
-    cost_f = cost_p = cost_ft = cost_fu = 0.0
-    rec3 = rec2 = fb_mode = fb_split = total = 0
+
+    def mass_fallback(lg, k):  # rows whose top-k softmax mass is below each policy's threshold
+        e = np.exp(lg.astype(np.float64) - lg.max(1, keepdims=True))
+        top = -np.sort(-e, axis=1)[:, :k].sum(1)
+        return top / e.sum(1)
+
+    full_ms = cnn_ms = 0.0
+    cost_f = cost_ft = cost_fu = 0.0
+    rec3 = rec2 = total = 0
+    pol = [{"ms": 0.0, "cost": 0.0, "fb_mode": 0, "fb_split": 0} for _ in PRUNE_POLICIES]
     for qp in QPS:
         lam = cnn.search_lambda_q8(qp)
         for plane in frames:
             ctx.ctu_search_xy(plane, 10, lam, xy, out=out_f, sync=False)  # warm
             full_ms += ev_time(lambda: ctx.ctu_search_xy(plane, 10, lam, xy, out=out_f, sync=False))
-            box = {}
-
-            def pruned():
-                lg, _, _ = ctx.cnn_forward(plane, 10, xy, params, qp, sync=False)
-                box["lg"] = lg
-                ctx.ctu_search_xy(plane, 10, lam, xy, lg, 3, 2, 0.4, out=out_p, sync=False)
-
-            pruned()
-            pruned_ms += ev_time(pruned)
-            cnn_ms += ev_time(lambda: ctx.cnn_forward(plane, 10, xy, params, qp, sync=False))
             rf = out_f.cpu().numpy().view(pkg.CTU_SEARCH_RES_DTYPE)
-            rp = out_p.cpu().numpy().view(pkg.CTU_SEARCH_RES_DTYPE)
-            lg = box["lg"].cpu().numpy()
-            # the same pruning without the fallback, trained vs untrained network
-            ft = ctx.ctu_search_xy(plane, 10, lam, xy, box["lg"], 3, 2, 0.0)
+            cost_f += float(rf["cost"].astype(np.float64).sum())
+            lg_t, _, _ = ctx.cnn_forward(plane, 10, xy, params, qp)
+            cnn_ms += ev_time(lambda: ctx.cnn_forward(plane, 10, xy, params, qp, sync=False))
+            lg = lg_t.cpu().numpy()
+            for pi, (tm, ts, thr) in enumerate(PRUNE_POLICIES):
+                def pruned():
+                    lgd, _, _ = ctx.cnn_forward(plane, 10, xy, params, qp, sync=False)
+                    ctx.ctu_search_xy(plane, 10, lam, xy, lgd, tm, ts, thr, out=out_p, sync=False)
+
+                pruned()
+                pol[pi]["ms"] += ev_time(pruned)
+                rp = out_p.cpu().numpy().view(pkg.CTU_SEARCH_RES_DTYPE)
+                pol[pi]["cost"] += float(rp["cost"].astype(np.float64).sum())
+                pol[pi]["fb_mode"] += int((mass_fallback(lg[:, :67], tm) < thr).sum())
+                pol[pi]["fb_split"] += int((mass_fallback(lg[:, 67:], ts) < thr).sum())
+            # the headline pruning without the fallback, trained vs untrained network
+            tm, ts, _ = PRUNE_POLICIES[0]
+            ft = ctx.ctu_search_xy(plane, 10, lam, xy, lg_t, tm, ts, 0.0)
             lg_u, _, _ = ctx.cnn_forward(plane, 10, xy, untrained, qp)
-            fu = ctx.ctu_search_xy(plane, 10, lam, xy, lg_u, 3, 2, 0.0)
+            fu = ctx.ctu_search_xy(plane, 10, lam, xy, lg_u, tm, ts, 0.0)
             cost_ft += float(ft["cost"].astype(np.float64).sum())
             cost_fu += float(fu["cost"].astype(np.float64).sum())
-            cost_f += float(rf["cost"].astype(np.float64).sum())
-            cost_p += float(rp["cost"].astype(np.float64).sum())
             top3 = np.argsort(-lg[:, :67], axis=1, kind="stable")[:, :3]
             top2 = np.argsort(-lg[:, 67:], axis=1, kind="stable")[:, :2]
             rec3 += int((top3 == rf["cu_mode"][:, None]).any(1).sum())
             rec2 += int((top2 == rf["split"][:, None]).any(1).sum())
-            fb_mode += int(((np.exp(lg[:, :67] - lg[:, :67].max(1, keepdims=True)).sum(1)) ** -1 < 0.4).sum())
-            fb_split += int(((np.exp(lg[:, 67:] - lg[:, 67:].max(1, keepdims=True)).sum(1)) ** -1 < 0.4).sum())
             total += n_ctu
     n_runs = len(QPS) * len(frames)
     # inference throughput on a 4096-block batch
@@ -479,19 +497,27 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
     tflops = 4096 * CNN_FLOP_PER_BLOCK / (ms4 * 1e-3) / 1e12
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
     full_fps = n_runs / (full_ms * 1e-3)
-    pruned_fps = n_runs / (pruned_ms * 1e-3)
+    policies = []
+    for (tm, ts, thr), p in zip(PRUNE_POLICIES, pol):
+        policies.append({"top_modes": tm, "top_splits": ts, "threshold": thr,
+                         "fps": round(n_runs / (p["ms"] * 1e-3), 1), "speedup": round(full_ms / p["ms"], 2),
+                         "cost_increase_pct": round(100.0 * (p["cost"] / cost_f - 1.0), 3),
+                         "fallback_rate": {"modes": round(p["fb_mode"] / total, 4),
+                                           "splits": round(p["fb_split"] / total, 4)}})
+    head = policies[0]
     return {"what": "candidate-cost stage of the GPU encoder (intra mode + split decision per 32x32 CTU, "
                     "SATD + lambda*bits, open loop); no bitstream, so BD-rate is not measured",
             "frames": f"{len(frames)} held-out 1920x1080 10-bit frames x QP{list(QPS)}",
-            "full_fps": round(full_fps, 1), "pruned_fps": round(pruned_fps, 1),
-            "speedup": round(pruned_fps / full_fps, 2),
-            "full_ms_per_frame": round(full_ms / n_runs, 4), "pruned_ms_per_frame": round(pruned_ms / n_runs, 4),
+            "full_fps": round(full_fps, 1), "pruned_fps": head["fps"], "speedup": head["speedup"],
+            "policy": {k: head[k] for k in ("top_modes", "top_splits", "threshold")},
+            "full_ms_per_frame": round(full_ms / n_runs, 4),
+            "pruned_ms_per_frame": round(pol[0]["ms"] / n_runs, 4),
             "cnn_ms_per_frame": round(cnn_ms / n_runs, 4),
-            "cost_increase_pct": round(100.0 * (cost_p / cost_f - 1.0), 3),
+            "cost_increase_pct": head["cost_increase_pct"],
             "no_fallback_cost_increase_pct": {"trained": round(100.0 * (cost_ft / cost_f - 1.0), 3),
                                               "untrained": round(100.0 * (cost_fu / cost_f - 1.0), 3)},
             "top3_mode_recall": round(rec3 / total, 4), "top2_split_recall": round(rec2 / total, 4),
-            "fallback_rate": {"modes": round(fb_mode / total, 4), "splits": round(fb_split / total, 4)},
+            "fallback_rate": head["fallback_rate"], "policies": policies,
             "cnn_inference": {"blocks": 4096, "ms": round(ms4, 4), "tflops": round(tflops, 1),
                               "peak": bf16_peak, "frac": round(tflops / bf16_peak, 4),
                               "flop_per_block": CNN_FLOP_PER_BLOCK},

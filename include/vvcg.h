@@ -657,8 +657,9 @@ vvcg_status vvcg_tc_selftest_dev(vvcg_ctx* ctx, const uint16_t* a, const uint16_
  * (ctu_xy: num_ctus (x, y) pairs) and, with logits (device, num_ctus x
  * VVCG_CNN_OUT from vvcg_cnn_forward_dev), pruned by the CNN: the top_modes
  * most probable intra modes are the candidates of every block and the
- * top_splits most probable split types are evaluated; a head whose largest
- * softmax probability is below threshold keeps its full set. logits = NULL
+ * top_splits most probable split types are evaluated; a head whose chosen
+ * entries hold less than threshold of its softmax probability mass keeps its
+ * full set (threshold 0: never). logits = NULL
  * is the full search. A CTU outside the plane gets cost UINT32_MAX and
  * split 0xFF. All on the context's stream, no host round trip. */
 vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,

@@ -632,10 +632,12 @@ class Context:
             raise Execution("tensor-core self-test: completion wait gave up")
         return d
 
-    def ctu_search_xy(self, src, bit_depth, lambda_q8, xy, logits=None, top_modes=3, top_splits=2,
-                      threshold=0.4, out=None, sync=True):
+    def ctu_search_xy(self, src, bit_depth, lambda_q8, xy, logits=None, top_modes=6, top_splits=2,
+                      threshold=0.7, out=None, sync=True):
         """The CTU search over device positions xy ((n, 2) int32 CUDA), full
-        (logits None) or pruned by the CNN's logits ((n, 73) fp32 CUDA).
+        (logits None) or pruned by the CNN's logits ((n, 73) fp32 CUDA): the
+        top_modes / top_splits most probable entries of each head, or its full
+        set when they hold less than threshold of its softmax mass.
         Returns CTU_SEARCH_RES_DTYPE results, or fills the CUDA uint8 tensor
         out (n x 36 bytes) without synchronising when sync is False."""
         import torch

@@ -1,8 +1,10 @@
 // CNN-pruned CTU search: the pruner's logits choose, per CTU, the intra
 // candidates (the top_modes most probable modes) and the split types (the
 // top_splits most probable) that the full search of intra_search.cuh then
-// evaluates; a head whose largest softmax probability is below the
-// threshold keeps its full set (all 67 modes / all 6 splits). Everything
+// evaluates; a head whose chosen candidates hold less than the threshold of
+// its softmax probability mass (for a calibrated network: the chance that
+// the full search's choice is among them) keeps its full set (all 67 modes /
+// all 6 splits). Everything
 // stays on the device: requests are built from the logits by one thread per
 // CTU and expanded into the 15 block slots of the search.
 #pragma once
@@ -30,13 +32,14 @@ __device__ __forceinline__ void top_k(const float* v, int n, int k, uint8_t* out
   }
 }
 
-// the largest softmax probability of v[0..n)
-__device__ __forceinline__ float max_prob(const float* v, int n) {
-  float mx = v[0];
-  for (int j = 1; j < n; j++) mx = fmaxf(mx, v[j]);
-  float s = 0.0f;
+// softmax probability mass of the k entries idx[0..k) of v[0..n); idx[0] is
+// the largest entry
+__device__ __forceinline__ float top_mass(const float* v, int n, const uint8_t* idx, int k) {
+  const float mx = v[idx[0]];
+  float s = 0.0f, t = 0.0f;
   for (int j = 0; j < n; j++) s += __expf(v[j] - mx);
-  return 1.0f / s;
+  for (int r = 0; r < k; r++) t += __expf(v[idx[r]] - mx);
+  return t / s;
 }
 
 __global__ void k_prune_requests(const float* __restrict__ logits, const uint32_t* __restrict__ xy, int n, int width,
@@ -52,13 +55,15 @@ __global__ void k_prune_requests(const float* __restrict__ logits, const uint32_
   r.n_cand = 0;
   if (inside && logits) {
     const float* lg = logits + (size_t)i * kCnnOut;
-    if (max_prob(lg, kCnnModes) >= thr) {
+    uint8_t cand[6];
+    top_k(lg, kCnnModes, top_modes, cand);
+    if (top_mass(lg, kCnnModes, cand, top_modes) >= thr) {
       r.n_cand = (uint8_t)top_modes;
-      top_k(lg, kCnnModes, top_modes, r.cand);
+      for (int k = 0; k < top_modes; k++) r.cand[k] = cand[k];
     }
-    if (max_prob(lg + kCnnModes, kCnnSplits) >= thr) {
-      uint8_t sp[6];
-      top_k(lg + kCnnModes, kCnnSplits, top_splits, sp);
+    uint8_t sp[6];
+    top_k(lg + kCnnModes, kCnnSplits, top_splits, sp);
+    if (top_mass(lg + kCnnModes, kCnnSplits, sp, top_splits) >= thr) {
       r.split_mask = 0;
       for (int k = 0; k < top_splits; k++) r.split_mask |= (uint8_t)(1u << sp[k]);
     }

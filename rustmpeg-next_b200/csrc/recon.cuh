@@ -127,11 +127,15 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
 #pragma unroll
     for (int v = 0; v < 4; v++)
       if (v < nvec) {
-        const uint32_t wv[4] = {buf[v].x, buf[v].y, buf[v].z, buf[v].w};
-#pragma unroll
+        uint32_t x0 = buf[v].x, x1 = buf[v].y, x2 = buf[v].z, x3 = buf[v].w;
+#pragma unroll 1
         for (int e = 0; e < 8; e++) {
-          int L = (int)(int16_t)(wv[e >> 1] >> (16 * (e & 1)));
+          int L = (int)(int16_t)(x0 & 0xFFFFu);
           if (L != 0) put(8 * (lane + 32 * v) + e, L);
+          x0 = __funnelshift_r(x0, x1, 16);
+          x1 = __funnelshift_r(x1, x2, 16);
+          x2 = __funnelshift_r(x2, x3, 16);
+          x3 >>= 16;
         }
       }
   } else {
