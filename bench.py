@@ -87,6 +87,13 @@ class ClockSampler:
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: timing begins once it has sampled
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 3.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -115,26 +122,31 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
-def cpu_baseline_oracle(pics, cus, levels, ctus, aps, n_pics, processes=1):
-    """Time the oracle (C++ restatement of the reference CPU path) on a bounded
-    sample of the same pictures; returns (Mpx/s, seconds, pictures)."""
+def workload_name(frames_per_qp):
+    return (f"1920x1080 10-bit 4:2:0, {frames_per_qp} frames x QP{{22,27,32,37}} = {4 * frames_per_qp} "
+            "pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)")
+
+
+def sample_indices(n_total, n):
+    """n picture indices spread evenly over a batch of n_total (all QPs)."""
+    n = max(1, min(n, n_total))
+    return [i * n_total // n for i in range(n)]
+
+
+def cpu_baseline_oracle(pics, cus, levels, ctus, aps, n_pics):
+    """Time the oracle (C++ restatement of the reference CPU path) on one
+    thread over a bounded sample of the same pictures, spread over the batch;
+    returns (Mpx/s, seconds, pictures)."""
     sys.path.insert(0, ROOT)
     import oracle
 
     oracle.build()
-    sample = list(range(n_pics))
+    sample = sample_indices(len(pics), n_pics)
     t0 = time.perf_counter()
-    if processes <= 1:
-        for i in sample:
-            _oracle_one(pics[i], cus, levels, ctus, aps)
-    else:
-        import multiprocessing as mp
-
-        ctxm = mp.get_context("spawn")
-        with ctxm.Pool(processes) as pool:
-            pool.starmap(_oracle_one, [(pics[i], cus, levels, ctus, aps) for i in sample])
+    for i in sample:
+        _oracle_one(pics[i], cus, levels, ctus, aps)
     dt = time.perf_counter() - t0
-    return n_pics * PIX_W * PIX_H / dt / 1e6, dt, n_pics
+    return len(sample) * PIX_W * PIX_H / dt / 1e6, dt, len(sample)
 
 
 def _oracle_one(p, cus, levels, ctus, aps):
@@ -150,33 +162,61 @@ def _oracle_one(p, cus, levels, ctus, aps):
     assert rc == 0
 
 
+# Worker state of the reference arm's process pool: the batch's records are
+# handed to each worker once, when the pool starts; a task is a picture index.
+_WORKER = {}
+
+
+def _worker_init(pics, cus, levels, ctus, aps):
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    oracle.build()
+    _WORKER.update(pics=pics, cus=cus, levels=levels, ctus=ctus, aps=aps)
+
+
+def _worker_picture(i):
+    w = _WORKER
+    _oracle_one(w["pics"][i], w["cus"], w["levels"], w["ctus"], w["aps"])
+    return i
+
+
 def run_reference(args, rank):
-    """--impl reference: the oracle on all host cores (replaces the unbuildable
-    Rust reference; bounded sample per step)."""
+    """--impl reference: the oracle on all host cores, one process per core
+    (the Rust reference cannot be built here). Each step reconstructs a
+    bounded sample of the workload's pictures, one per core, spread over the
+    four QPs; the pool and its copies of the records exist before the timed
+    steps, so a step times decoding only."""
     if rank != 0:
         return
+    import multiprocessing as mp
+
     pkg = load_pkg()
     cores = os.cpu_count() or 1
-    n_sample = max(2, min(cores, 16))
-    pics, cus, levels, ctus, aps = build_records(pkg, 1, seed=0x5EED0000)
-    for _ in range(args.warmup):
-        cpu_baseline_oracle(pics, cus, levels, ctus, aps, min(n_sample, len(pics)), processes=cores)
-    times = []
-    for _ in range(args.steps):
-        v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, min(n_sample, len(pics)), processes=cores)
-        times.append(dt)
+    pics, cus, levels, ctus, aps = build_records(pkg, max(1, (cores + 3) // 4), seed=0x5EED0000)
+    sample = sample_indices(len(pics), cores)
+    n = len(sample)
+    with mp.get_context("spawn").Pool(cores, initializer=_worker_init,
+                                      initargs=(pics, cus, levels, ctus, aps)) as pool:
+        for _ in range(args.warmup):
+            pool.map(_worker_picture, sample, chunksize=1)
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            pool.map(_worker_picture, sample, chunksize=1)
+            times.append(time.perf_counter() - t0)
     mean = sum(times) / len(times)
-    n = min(n_sample, len(pics))
     value = n * PIX_W * PIX_H / mean / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpx/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-            "config": {"workload": "1920x1080 10-bit 4:2:0 recon+deblock+SAO+ALF (CTU 32)",
-                       "sample_pictures_per_step": n},
+            "config": {"workload": workload_name(args.frames_per_qp), "pictures_per_step": 4 * args.frames_per_qp,
+                       "sample_pictures_per_step": n,
+                       "sample": "pictures of the same generator and QPs as the workload"},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
-                             "sample": f"{n} pictures of 1920x1080 per step, one process per core "
-                                       "(C++ restatement of the reference CPU path, g++ -O2)"},
+                             "sample": f"{n} pictures of 1920x1080 per step (QP 22-37), one process per "
+                                       "core (C++ restatement of the reference CPU path, g++ -O2)"},
             "e2e": {"value": round(value, 3), "unit": "Mpx/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -185,12 +225,13 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames-per-qp", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=4, help="pictures in the CPU baseline sample")
+    ap.add_argument("--cpu-sample", type=int, default=64,
+                    help="pictures in the CPU baseline sample (about 0.15 s each on one core)")
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -366,8 +407,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic",
-            "config": {"workload": "1920x1080 10-bit 4:2:0, 32 frames x QP{22,27,32,37} = "
-                                   f"{n_pics} pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)",
+            "config": {"workload": workload_name(args.frames_per_qp),
                        "pictures_per_step": n_pics, "parallelism": f"replicas x{world}",
                        "launch": "direct launches" if args.no_graph else "CUDA graph replay",
                        "l2": "inputs larger than L2 (466 MB levels, 1.6 GB planes); no flush",
@@ -383,7 +423,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
-                                "sample": f"{n} pictures of 1920x1080 from the same batch, "
+                                "sample": f"{n} pictures of 1920x1080 spread over the batch (all QPs), "
                                           f"{dt:.1f} s, one thread (C++ restatement of the "
                                           "reference CPU path, g++ -O2)",
                                 "host_cpu": _cpu_model(), "nproc": os.cpu_count()}
