@@ -572,23 +572,36 @@ constexpr int kAlfBlocks = (kAlfTw / 4) * (kAlfTh / 4);
 
 // Tile of 64x16 outputs: the tile plus a 4-sample halo (coordinates clamped
 // to the plane, as the reference's get_p does, so reads inside the staged
-// tile need no further clamping) is staged in shared memory. Each 4x4 block is
+// tile need no further clamping) is staged in shared memory; a tile whose halo
+// lies inside the plane needs no clamping and is staged with 8-byte loads. Each 4x4 block is
 // classified (classify_alf_4x4_16, filter.rs:2126-2182) and its transposed
 // coefficients and clip values are formed once; then each thread filters one
 // 4-sample row of a block with the 7x7 diamond.
 __global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
   const AlfPass& A = passes[blockIdx.z];
   constexpr int W = kAlfTw + 2 * kAlfHalo, H = kAlfTh + 2 * kAlfHalo;
-  __shared__ uint16_t t[H][W];
+  __shared__ __align__(16) uint16_t t[H][W];
   __shared__ int16_t s_fc[kAlfBlocks][12];
   __shared__ int16_t s_fcl[kAlfBlocks][12];
   __shared__ uint8_t s_abort[kAlfBlocks];
   const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
   if (x0 >= A.w || y0 >= A.h) return;
-  for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
-    int ty = i / W, tx = i % W;
-    int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
-    t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
+  static_assert(W % 4 == 0 && kAlfHalo % 4 == 0 && kAlfTw % 4 == 0, "8-byte staging");
+  const bool inner = x0 >= kAlfHalo && y0 >= kAlfHalo && x0 + kAlfTw + kAlfHalo <= A.w &&
+                     y0 + kAlfTh + kAlfHalo <= A.h && (A.stride & 3) == 0 &&
+                     (reinterpret_cast<uintptr_t>(A.src) & 7) == 0;
+  if (inner) {  // no clamping: 4 samples per 8-byte load
+    const uint16_t* base = A.src + (size_t)(y0 - kAlfHalo) * A.stride + (x0 - kAlfHalo);
+    for (int i = threadIdx.x; i < (W / 4) * H; i += blockDim.x) {
+      const int ty = i / (W / 4), q = i - ty * (W / 4);
+      *reinterpret_cast<uint2*>(&t[ty][4 * q]) = *reinterpret_cast<const uint2*>(base + (size_t)ty * A.stride + 4 * q);
+    }
+  } else {
+    for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
+      int ty = i / W, tx = i % W;
+      int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
+      t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
+    }
   }
   __syncthreads();
   // tile coordinates of plane position (x, y) inside the staged region
