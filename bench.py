@@ -122,6 +122,29 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def rank_seed(rank):
+    """Seed of a rank's synthetic records: each replica decodes its own batch."""
+    return 0x5EED0000 + 1000 * rank
+
+
+def max_over_ranks(value, dist, device):
+    """The largest of every rank's value (a time), the same on all ranks;
+    value itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mpx_per_s(world, px_per_rank_step, ms_per_step):
+    """Whole-job throughput: every rank reconstructs its own batch of
+    px_per_rank_step pixels per step; ms_per_step is the slowest rank's."""
+    return world * px_per_rank_step / (ms_per_step * 1e-3) / 1e6
+
+
 def workload_name(frames_per_qp):
     return (f"1920x1080 10-bit 4:2:0, {frames_per_qp} frames x QP{{22,27,32,37}} = {4 * frames_per_qp} "
             "pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)")
@@ -193,7 +216,7 @@ def run_reference(args, rank):
 
     pkg = load_pkg()
     cores = os.cpu_count() or 1
-    pics, cus, levels, ctus, aps = build_records(pkg, max(1, (cores + 3) // 4), seed=0x5EED0000)
+    pics, cus, levels, ctus, aps = build_records(pkg, max(1, (cores + 3) // 4), seed=rank_seed(0))
     sample = sample_indices(len(pics), cores)
     n = len(sample)
     with mp.get_context("spawn").Pool(cores, initializer=_worker_init,
@@ -260,7 +283,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
 
-    pics, cus, levels, ctus, aps = build_records(pkg, args.frames_per_qp, seed=0x5EED0000 + 1000 * rank)
+    pics, cus, levels, ctus, aps = build_records(pkg, args.frames_per_qp, seed=rank_seed(rank))
     n_pics = len(pics)
     # pinned host copies for the end-to-end leg
     pin = lambda a: torch.from_numpy(a.view(np.uint8)).pin_memory().numpy().view(a.dtype)  # noqa: E731
@@ -293,11 +316,7 @@ def main():
         ev1.synchronize()
         ms = ev0.elapsed_time(ev1) / k
         sync_all()
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ms, dist, dev)
 
     # correctness of the configuration before timing (no reference aborts)
     ctx.run(pkg.STAGE_ALL)
@@ -365,15 +384,11 @@ def main():
     for i in range(k_e2e):
         e2e_step(i)
     e2e_drain()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / k_e2e
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / k_e2e, dist, dev)
 
     px_step = n_pics * PIX_W * PIX_H
-    value = world * px_step / (ms_step * 1e-3) / 1e6
-    e2e_value = world * px_step / (e2e_ms * 1e-3) / 1e6
+    value = job_mpx_per_s(world, px_step, ms_step)
+    e2e_value = job_mpx_per_s(world, px_step, e2e_ms)
 
     # roofline of the dominant stage
     peaks = {}
