@@ -345,6 +345,19 @@ vvcg_status vvcg_tu_inverse_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32
 vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
                                   const int16_t* in, uint64_t in_count, int16_t* out,
                                   uint64_t out_count);
+/* Block-size-binning autotuner of the two functions above (no counterpart in
+ * the reference, which transforms one unit at a time). The units are grouped
+ * by size (at most 256, 1024 and 4096 coefficients); for each non-empty group
+ * every CTA width the library has for it (2, 4 or 8 warps; 1, 2 or 4 for the
+ * largest group; one unit per warp) is timed on this batch, and the fastest
+ * stays in the context for later vvcg_tu_inverse_batch (forward = 0) or
+ * vvcg_tu_forward_batch (forward = 1) calls. warps[g] receives the chosen
+ * width of group g, 0 for an empty group (whose choice is kept). Arguments
+ * and checks as in those functions; out receives the batch's results, which
+ * never depend on the width. Synchronous: returns after the timings. */
+vvcg_status vvcg_tu_autotune(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs, const int16_t* in,
+                             uint64_t in_count, int16_t* out, uint64_t out_count, uint32_t forward,
+                             uint32_t warps[3]);
 
 /* ---- encoder candidate cost: luma transform search ----------------------- */
 

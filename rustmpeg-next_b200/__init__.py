@@ -225,6 +225,7 @@ def lib():
         L.vvcg_mc_chroma_420_8_dev.argtypes = [vp, vp, u32, u32, u32, vp, u32, vp]
         for n in ("vvcg_tu_inverse_batch", "vvcg_tu_forward_batch"):
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
+        L.vvcg_tu_autotune.argtypes = [vp, vp, u32, vp, u64, vp, u64, u32, vp]
         L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
         L.vvcg_encode_batch.argtypes = [vp, vp, u32, vp, vp, u32, vp, u64]
         for n in ("vvcg_plane_metrics_8_dev", "vvcg_plane_metrics_16_dev"):
@@ -751,6 +752,17 @@ class Context:
         self._keep = recs
         self._check(self._L.vvcg_tu_forward_batch(self._h, _ptr(recs), len(recs), _ptr(data),
                                                   data.numel(), _ptr(out), out.numel()))
+
+    def tu_autotune(self, recs, data, out, forward):
+        """Times each CTA width of every size group of this batch and keeps the
+        fastest for later tu_inverse (forward False) / tu_forward (True) calls;
+        returns the chosen warps per CTA of the 256 / 1024 / 4096-coefficient
+        groups (0: no unit of that size). out receives the batch's results."""
+        recs = np.ascontiguousarray(recs, dtype=TU_DTYPE)
+        warps = np.zeros(3, np.uint32)
+        self._check(self._L.vvcg_tu_autotune(self._h, _ptr(recs), len(recs), _ptr(data), data.numel(), _ptr(out),
+                                             out.numel(), int(bool(forward)), _ptr(warps)))
+        return tuple(int(w) for w in warps)
 
     def mc_luma_8(self, ref, blocks, out):
         """ref: (H, W) uint8 CUDA tensor (the 8-bit functions of inter.rs)."""

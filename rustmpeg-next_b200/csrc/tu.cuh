@@ -25,7 +25,6 @@ __device__ int8_t g_lfnst8[4 * 2 * 16 * 48];
 __device__ int8_t g_lfnst4[4 * 2 * 16 * 16];
 __device__ uint8_t g_lfnst_lut[95];
 
-constexpr int kTuWarps = 4;  // warps per CTA (2 for the 64x64 bin)
 constexpr int kTuPad = 64;   // tiles are padded by one sample per row or column
 
 // Transform types and zero-out of a unit (decode_general.rs:4165-4198 with

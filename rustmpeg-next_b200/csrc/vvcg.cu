@@ -115,9 +115,11 @@ struct vvcg_ctx {
   // device memory
   DevBuf planes, flags, d_pics, d_items, d_dbf[4], d_sao, d_alf, d_cus, d_levels, d_ctus, d_aps,
       d_ctrl;  // d_ctrl: [0] queue counter, [1] status word
-  // transform-unit batches
+  // transform-unit batches; tu_pick[forward][size bin] indexes the bin's CTA
+  // widths (kTuTable), chosen by vvcg_tu_autotune (default: the middle one)
   std::vector<uint32_t> tu_idx;
   DevBuf d_tu_recs, d_tu_idx;
+  uint8_t tu_pick[2][3] = {{1, 1, 1}, {1, 1, 1}};
   DevBuf d_lmcs;  // a device copy of the LMCS tables of the last call
   DevBuf d_alfp, d_alfc;  // general-decoder ALF parameters and CTU switches
   DevBuf d_search_reqs, d_search_cost, d_search_mode, d_search_ctus;  // CTU full search
@@ -303,6 +305,8 @@ vvcg_status upload_vec(vvcg_ctx* ctx, DevBuf& buf, const std::vector<T>& v) {
   return VVCG_OK;
 }
 
+bool tu_set_smem_limits();  // every transform-unit kernel variant may use its shared memory
+
 }  // namespace
 
 extern "C" {
@@ -353,10 +357,7 @@ vvcg_status vvcg_ctx_create(const vvcg_config* cfg, vvcg_ctx** out) {
     delete ctx;
     return VVCG_UNAVAILABLE;
   }
-  if (cudaFuncSetAttribute(k_tu<4096, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tu_smem_bytes<4096, 2>()) != cudaSuccess ||
-      cudaFuncSetAttribute(k_tu<4096, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tu_smem_bytes<4096, 2>()) != cudaSuccess) {
+  if (!tu_set_smem_limits()) {
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return VVCG_UNAVAILABLE;
@@ -1872,6 +1873,45 @@ extern "C" vvcg_status vvcg_encode_batch(vvcg_ctx* ctx, const vvcg_pic_desc* pic
 // ---------------------------------------------------------------------------
 namespace {
 
+// Size bins of the transform-unit batches (at most 256, 1024 and 4096
+// coefficients) and the CTA widths each can launch with: one unit per warp,
+// kTuTable[bin][variant] warps per CTA. Wider CTAs share fewer, larger
+// launches; narrower ones spread a small bin over more SMs. The results do
+// not depend on the width (every warp transforms its own unit), so
+// vvcg_tu_autotune can pick the fastest per bin by timing alone.
+using TuKernel = void (*)(const vvcg_tu_rec*, const uint32_t*, uint32_t, const int16_t*, int16_t*);
+struct TuVariant {
+  TuKernel inv, fwd;
+  int warps;
+  size_t smem;
+};
+constexpr int kTuBins = 3, kTuVariants = 3;
+template <int kEl, int kW>
+TuVariant tu_variant() {
+  return TuVariant{k_tu<kEl, kW, false>, k_tu<kEl, kW, true>, kW, tu_smem_bytes<kEl, kW>()};
+}
+const TuVariant kTuTable[kTuBins][kTuVariants] = {
+    {tu_variant<256, 2>(), tu_variant<256, 4>(), tu_variant<256, 8>()},
+    {tu_variant<1024, 2>(), tu_variant<1024, 4>(), tu_variant<1024, 8>()},
+    {tu_variant<4096, 1>(), tu_variant<4096, 2>(), tu_variant<4096, 4>()}};
+static_assert(sizeof(((vvcg_ctx*)nullptr)->tu_pick[0]) == kTuBins, "one choice per bin");
+
+bool tu_set_smem_limits() {
+  for (int b = 0; b < kTuBins; b++)
+    for (int v = 0; v < kTuVariants; v++) {
+      const TuVariant& V = kTuTable[b][v];
+      if (cudaFuncSetAttribute(V.inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)V.smem) != cudaSuccess ||
+          cudaFuncSetAttribute(V.fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)V.smem) != cudaSuccess)
+        return false;
+    }
+  return true;
+}
+
+int tu_bin(const vvcg_tu_rec& r) {
+  const uint32_t el = 1u << (r.log2_w + r.log2_h);
+  return el <= 256 ? 0 : (el <= 1024 ? 1 : 2);
+}
+
 // Why the reference would reject a unit (dct.rs matrix_for_any / zero-out
 // checks, lfnst.rs parameters_rect, slice.rs:701 MTS with LFNST), or nullptr.
 const char* tu_reject(const vvcg_tu_rec& r, bool forward, uint64_t in_count, uint64_t out_count) {
@@ -1896,55 +1936,53 @@ const char* tu_reject(const vvcg_tu_rec& r, bool forward, uint64_t in_count, uin
   return nullptr;
 }
 
-vvcg_status tu_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t n, const int16_t* in,
-                     uint64_t in_count, int16_t* out, uint64_t out_count, bool forward) {
-  if (!ctx) return VVCG_INVALID_INPUT;
-  if (n == 0) return VVCG_OK;
-  if (!recs || !in || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing records or buffers");
-  uint32_t count[3] = {0, 0, 0};
+// Validates the units, groups them by size bin (count[b] units of bin b, in
+// that order in d_tu_idx) and uploads records and order to the device.
+vvcg_status tu_stage(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t n, uint64_t in_count, uint64_t out_count,
+                     bool forward, uint32_t count[kTuBins]) {
+  for (int b = 0; b < kTuBins; b++) count[b] = 0;
   for (uint32_t i = 0; i < n; i++) {
     if (const char* why = tu_reject(recs[i], forward, in_count, out_count))
       return fail(ctx, VVCG_INVALID_INPUT, "transform unit %u: %s", i, why);
-    const uint32_t el = 1u << (recs[i].log2_w + recs[i].log2_h);
-    count[el <= 256 ? 0 : (el <= 1024 ? 1 : 2)]++;
+    count[tu_bin(recs[i])]++;
   }
   // units grouped by size bin
   ctx->tu_idx.resize(n);
-  uint32_t at[3] = {0, count[0], count[0] + count[1]};
-  for (uint32_t i = 0; i < n; i++) {
-    const uint32_t el = 1u << (recs[i].log2_w + recs[i].log2_h);
-    ctx->tu_idx[at[el <= 256 ? 0 : (el <= 1024 ? 1 : 2)]++] = i;
-  }
+  uint32_t at[kTuBins] = {0, count[0], count[0] + count[1]};
+  for (uint32_t i = 0; i < n; i++) ctx->tu_idx[at[tu_bin(recs[i])]++] = i;
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   CK(ctx->d_tu_recs.reserve(sizeof(vvcg_tu_rec) * n), "cudaMalloc");
   CK(ctx->d_tu_idx.reserve(sizeof(uint32_t) * n), "cudaMalloc");
   CK(cudaMemcpyAsync(ctx->d_tu_recs.p, recs, sizeof(vvcg_tu_rec) * n, cudaMemcpyHostToDevice, ctx->stream), "upload");
   CK(cudaMemcpyAsync(ctx->d_tu_idx.p, ctx->tu_idx.data(), sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->stream),
      "upload");
-  const vvcg_tu_rec* d_recs = (const vvcg_tu_rec*)ctx->d_tu_recs.p;
-  const uint32_t* d_idx = (const uint32_t*)ctx->d_tu_idx.p;
-  if (count[0]) {
-    auto k = forward ? k_tu<256, kTuWarps, true> : k_tu<256, kTuWarps, false>;
-    k<<<(count[0] + kTuWarps - 1) / kTuWarps, kTuWarps * 32, tu_smem_bytes<256, kTuWarps>(), ctx->stream>>>(
-        d_recs, d_idx, count[0], in, out);
-    CK(cudaGetLastError(), "transform-unit launch");
-    ctx->launches++;
-  }
-  if (count[1]) {
-    auto k = forward ? k_tu<1024, kTuWarps, true> : k_tu<1024, kTuWarps, false>;
-    k<<<(count[1] + kTuWarps - 1) / kTuWarps, kTuWarps * 32, tu_smem_bytes<1024, kTuWarps>(), ctx->stream>>>(
-        d_recs, d_idx + count[0], count[1], in, out);
-    CK(cudaGetLastError(), "transform-unit launch");
-    ctx->launches++;
-  }
-  if (count[2]) {
-    auto k = forward ? k_tu<4096, 2, true> : k_tu<4096, 2, false>;
-    k<<<(count[2] + 1) / 2, 64, tu_smem_bytes<4096, 2>(), ctx->stream>>>(d_recs, d_idx + count[0] + count[1],
-                                                                         count[2], in, out);
-    CK(cudaGetLastError(), "transform-unit launch");
-    ctx->launches++;
-  }
   return VVCG_OK;
+}
+
+// Launches the staged units of size bin b with CTA width variant v.
+vvcg_status tu_launch(vvcg_ctx* ctx, const uint32_t count[kTuBins], int b, int v, bool forward, const int16_t* in,
+                      int16_t* out) {
+  const TuVariant& V = kTuTable[b][v];
+  uint32_t first = 0;
+  for (int k = 0; k < b; k++) first += count[k];
+  const TuKernel k = forward ? V.fwd : V.inv;
+  k<<<(count[b] + V.warps - 1) / V.warps, V.warps * 32, V.smem, ctx->stream>>>(
+      (const vvcg_tu_rec*)ctx->d_tu_recs.p, (const uint32_t*)ctx->d_tu_idx.p + first, count[b], in, out);
+  CK(cudaGetLastError(), "transform-unit launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+vvcg_status tu_batch(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t n, const int16_t* in,
+                     uint64_t in_count, int16_t* out, uint64_t out_count, bool forward) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (n == 0) return VVCG_OK;
+  if (!recs || !in || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing records or buffers");
+  uint32_t count[kTuBins];
+  vvcg_status st = tu_stage(ctx, recs, n, in_count, out_count, forward, count);
+  for (int b = 0; b < kTuBins && st == VVCG_OK; b++)
+    if (count[b]) st = tu_launch(ctx, count, b, ctx->tu_pick[forward ? 1 : 0][b], forward, in, out);
+  return st;
 }
 
 }  // namespace
@@ -1959,6 +1997,57 @@ extern "C" vvcg_status vvcg_tu_forward_batch(vvcg_ctx* ctx, const vvcg_tu_rec* r
                                              const int16_t* in, uint64_t in_count, int16_t* out,
                                              uint64_t out_count) {
   return tu_batch(ctx, recs, num_recs, in, in_count, out, out_count, true);
+}
+
+// Times every CTA width of each non-empty size bin on the caller's batch
+// (one warm-up launch, then kTuTuneReps launches between two events on the
+// context's stream) and keeps the fastest in the context.
+extern "C" vvcg_status vvcg_tu_autotune(vvcg_ctx* ctx, const vvcg_tu_rec* recs, uint32_t num_recs,
+                                        const int16_t* in, uint64_t in_count, int16_t* out, uint64_t out_count,
+                                        uint32_t forward, uint32_t warps[3]) {
+  constexpr int kTuTuneReps = 3;
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!warps) return fail(ctx, VVCG_INVALID_INPUT, "missing result array");
+  for (int b = 0; b < kTuBins; b++) warps[b] = 0;
+  if (num_recs == 0) return VVCG_OK;
+  if (!recs || !in || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing records or buffers");
+  const bool fwd = forward != 0;
+  uint32_t count[kTuBins];
+  vvcg_status st = tu_stage(ctx, recs, num_recs, in_count, out_count, fwd, count);
+  if (st != VVCG_OK) return st;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct Events {
+    cudaEvent_t* e;
+    ~Events() {
+      for (int i = 0; i < 2; i++)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } guard{ev};
+  CK(cudaEventCreate(&ev[0]), "cudaEventCreate");
+  CK(cudaEventCreate(&ev[1]), "cudaEventCreate");
+  for (int b = 0; b < kTuBins; b++) {
+    if (!count[b]) continue;
+    int best = ctx->tu_pick[fwd ? 1 : 0][b];
+    float best_ms = 0.0f;
+    for (int v = 0; v < kTuVariants; v++) {
+      if ((st = tu_launch(ctx, count, b, v, fwd, in, out)) != VVCG_OK) return st;
+      CK(cudaEventRecord(ev[0], ctx->stream), "cudaEventRecord");
+      for (int r = 0; r < kTuTuneReps; r++)
+        if ((st = tu_launch(ctx, count, b, v, fwd, in, out)) != VVCG_OK) return st;
+      CK(cudaEventRecord(ev[1], ctx->stream), "cudaEventRecord");
+      CK(cudaEventSynchronize(ev[1]), "transform-unit timing");
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, ev[0], ev[1]), "cudaEventElapsedTime");
+      if (v == 0 || ms < best_ms) {
+        best_ms = ms;
+        best = v;
+      }
+    }
+    ctx->tu_pick[fwd ? 1 : 0][b] = (uint8_t)best;
+    warps[b] = (uint32_t)kTuTable[b][best].warps;
+  }
+  CK(cudaStreamSynchronize(ctx->stream), "transform-unit timing");
+  return VVCG_OK;
 }
 
 // ---------------------------------------------------------------------------
