@@ -581,6 +581,30 @@ enum {
   VVCG_SPLIT_TT_H = 4, VVCG_SPLIT_TT_V = 5
 };
 
+/* ---- partition hook of the reference encoders -------------------------------- */
+
+typedef struct vvcg_split_req {
+  uint32_t x, y;    /* top-left luma sample of the region (it may reach past the plane) */
+  uint16_t w, h;    /* region size, 1..4096 each */
+  uint16_t min_cb;  /* minimum coding-block size: w or h <= max(min_cb, 8) means no split */
+  uint8_t qp;       /* slice QP, 0..63 */
+  uint8_t reserved;
+} vvcg_split_req;   /* 16 bytes */
+
+/* Quadrant-mean split decision of each region: res[i] (device) becomes
+ * VVCG_SPLIT_NONE, _QT, _BT_H or _BT_V. Replaces choose_qt_mtt_partition_rdo_16
+ * and choose_qt_mtt_partition_rdo (crates/rustmpeg-video/src/vvc/slice.rs:
+ * 4111-4167), hooks that no encoder of the reference calls: samples are
+ * rounded to 8 bits as Plane16::to_plane_8bit does (predict.rs:2914-2926); a
+ * quadrant's mean is the sum of its samples inside the plane over the full
+ * quadrant area; mean differences across the two midlines against
+ * max(qp, 4) / 2 + 8 decide. plane: device luma, bit_depth 8..12 in uint16
+ * (8-bit samples as they are); reqs: host. Asynchronous on the context's
+ * stream. */
+vvcg_status vvcg_qt_mtt_split_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                  uint32_t height, uint8_t bit_depth, const vvcg_split_req* reqs,
+                                  uint32_t num_reqs, uint8_t* res);
+
 typedef struct vvcg_ctu_search_req {
   uint32_t x, y;       /* top-left luma sample of a 32x32 CTU inside the plane */
   uint8_t split_mask;  /* bit s: evaluate split type s (0x3F: all six) */

@@ -104,6 +104,8 @@ def _declare(L):
     L.orc_predict_luma_8.restype = None
     L.orc_ctu_search.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint32, vp]
     L.orc_ctu_search.restype = None
+    L.orc_qt_mtt_split.argtypes = [vp, i, i, i, vp, i, vp]
+    L.orc_qt_mtt_split.restype = None
     L.orc_gen_intra_predict.argtypes = [vp, vp, vp, i, i, i, i, vp, vp, i, i, i, vp, i, vp]
     L.orc_gen_intra_predict.restype = None
     L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
@@ -290,6 +292,17 @@ def ctu_search(src, bd, x, y, lambda_q8, split_mask=0x3F, cand=()):
     m = int(out[9])
     return dict(cost=int(out[0]), split_cost=[int(v) for v in out[1:7]], split=int(out[7]), cu_mode=int(out[8]),
                 modes=[(m >> (8 * k)) & 0xFF for k in range(4)])
+
+
+def qt_mtt_split(src, bd, regions):
+    """choose_qt_mtt_partition_rdo_16 (slice.rs:4111-4167) of each region
+    (x, y, w, h, qp, min_cb) of a 16-bit luma plane of bit depth bd; returns
+    uint8 splits: 0 none, 1 quad, 2 binary horizontal, 3 binary vertical."""
+    src = _u16(src)
+    r = np.ascontiguousarray(np.asarray(regions, dtype=np.int64).reshape(-1, 6))
+    out = np.zeros(len(r), np.uint8)
+    lib().orc_qt_mtt_split(_p(src), src.shape[1], src.shape[0], bd, _p(r), len(r), _p(out))
+    return out
 
 
 def search_lambda_q8(qp, bit_depth=10):

@@ -143,6 +143,8 @@ void predict_luma_8(const Plane8& recon, int bx, int by, int w, int h, int mode,
 // The GPU encoder's CTU full search (orc_search.cpp; no reference counterpart).
 void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, const uint8_t* cand,
                 uint32_t lambda_q8, uint32_t* cost, uint32_t split_cost[6], int* split, int* cu_mode, int modes[4]);
+// slice.rs:4111-4167: the quadrant-mean partition hook (orc_search.cpp).
+int qt_mtt_split(const Plane16& src, int64_t bx, int64_t by, int64_t w, int64_t h, int qp, int64_t min_cb);
 // decode_general.rs:4916-4975 / filter.rs:202-226: general-decoder deblocking helpers.
 void dbk_luma_lens(int size_p, int size_q, int* lp, int* lq);
 void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq);

@@ -189,6 +189,15 @@ extern "C" void orc_ctu_search(const uint16_t* src, int pw, int ph, int bd, int 
   out[8] = (uint32_t)cu_mode;
   out[9] = (uint32_t)(modes[0] | (modes[1] << 8) | (modes[2] << 16) | ((uint32_t)modes[3] << 24));
 }
+// regions as (x, y, w, h, qp, min_cb) int64 sextuples; out one split per region
+extern "C" void orc_qt_mtt_split(const uint16_t* src, int pw, int ph, int bd, const int64_t* regions, int n,
+                                 uint8_t* out) {
+  orc::Plane16 p{(uint16_t*)src, pw, ph, bd};
+  for (int i = 0; i < n; i++) {
+    const int64_t* r = regions + 6 * i;
+    out[i] = (uint8_t)orc::qt_mtt_split(p, r[0], r[1], r[2], r[3], (int)r[4], r[5]);
+  }
+}
 // planes Y / Cb / Cr row-major at the given strides; dec_y / dec_c byte maps;
 // reqs in the vvcg_gen_intra_req layout; out int16
 extern "C" void orc_gen_intra_predict(const uint16_t* y, const uint16_t* u, const uint16_t* v, int sy, int sc,

@@ -102,4 +102,44 @@ void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, 
   }
 }
 
+// choose_qt_mtt_partition_rdo_16 (slice.rs:4111-4121) over
+// choose_qt_mtt_partition_rdo (slice.rs:4126-4167): the region's samples are
+// first rounded to 8 bits as Plane16::to_plane_8bit does (predict.rs:2914-2926:
+// (v saturating+ 2^(bd-9)) >> (bd-8), at most 255); each quadrant's mean is
+// its sum over the samples inside the plane divided by the full quadrant area;
+// the mean differences across the horizontal and vertical midlines, against
+// max(qp, 4) / 2 + 8, choose quad, horizontal binary, vertical binary or no
+// split. Returns 0 none, 1 quad, 2 binary horizontal, 3 binary vertical.
+int qt_mtt_split(const Plane16& src, int64_t bx, int64_t by, int64_t w, int64_t h, int qp, int64_t min_cb) {
+  const int64_t lim = min_cb > 8 ? min_cb : 8;
+  if (w <= lim || h <= lim) return 0;
+  const int shift = src.bd > 8 ? src.bd - 8 : 0;
+  const uint32_t add = shift > 0 ? 1u << (shift - 1) : 0u;
+  auto to8 = [&](uint16_t v) -> int64_t {
+    uint32_t t = (uint32_t)v + add;
+    if (t > 65535u) t = 65535u;
+    t >>= shift;
+    return t > 255u ? 255 : (int64_t)t;
+  };
+  const int64_t hw = w / 2, hh = h / 2;
+  auto quad_mean = [&](int64_t qx, int64_t qy, int64_t qw, int64_t qh) -> int64_t {
+    int64_t sum = 0;
+    const int64_t ye = qy + qh < src.height ? qy + qh : src.height;
+    const int64_t xe = qx + qw < src.width ? qx + qw : src.width;
+    for (int64_t y = qy; y < ye; y++)
+      for (int64_t x = qx; x < xe; x++) sum += to8(src.get((int)x, (int)y));
+    const int64_t area = qw * qh > 1 ? qw * qh : 1;
+    return sum / area;
+  };
+  const int64_t m00 = quad_mean(bx, by, hw, hh), m10 = quad_mean(bx + hw, by, hw, hh);
+  const int64_t m01 = quad_mean(bx, by + hh, hw, hh), m11 = quad_mean(bx + hw, by + hh, hw, hh);
+  const int64_t hor = llabs(m00 - m01) + llabs(m10 - m11);
+  const int64_t ver = llabs(m00 - m10) + llabs(m01 - m11);
+  const int64_t thr = (qp > 4 ? qp : 4) / 2 + 8;
+  if (w == h && hor > thr && ver > thr) return 1;
+  if (hor > ver && hor > thr) return 2;
+  if (ver > thr) return 3;
+  return 0;
+}
+
 }  // namespace orc

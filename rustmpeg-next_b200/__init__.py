@@ -66,6 +66,8 @@ CTU_SEARCH_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("split_mask", "u1"
 CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), ("split", "u1"), ("cu_mode", "u1"),
                                  ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
 SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
+SPLIT_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("w", "<u2"), ("h", "<u2"), ("min_cb", "<u2"), ("qp", "u1"),
+                            ("reserved", "u1")])
 CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30761, 73, 67, 6
 GEN_INTRA_REQ_DTYPE = np.dtype([("x", "<u2"), ("y", "<u2"), ("w", "<u2"), ("h", "<u2"), ("cu_x", "<u2"),
                                 ("cu_y", "<u2"), ("cu_w", "<u2"), ("cu_h", "<u2"), ("comp", "u1"), ("mode", "u1"),
@@ -226,6 +228,7 @@ def lib():
         for n in ("vvcg_tu_inverse_batch", "vvcg_tu_forward_batch"):
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.vvcg_tu_autotune.argtypes = [vp, vp, u32, vp, u64, vp, u64, u32, vp]
+        L.vvcg_qt_mtt_split_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, u32, vp]
         L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
         L.vvcg_encode_batch.argtypes = [vp, vp, u32, vp, vp, u32, vp, u64]
         for n in ("vvcg_plane_metrics_8_dev", "vvcg_plane_metrics_16_dev"):
@@ -752,6 +755,20 @@ class Context:
         self._keep = recs
         self._check(self._L.vvcg_tu_forward_batch(self._h, _ptr(recs), len(recs), _ptr(data),
                                                   data.numel(), _ptr(out), out.numel()))
+
+    def qt_mtt_split(self, plane, bit_depth, reqs):
+        """Quadrant-mean split decision (choose_qt_mtt_partition_rdo_16) of each
+        SPLIT_REQ_DTYPE region of a (H, W) 16-bit CUDA luma plane; returns uint8
+        SPLIT_NONE / SPLIT_QT / SPLIT_BT_H / SPLIT_BT_V per region."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=SPLIT_REQ_DTYPE)
+        h, w = plane.shape
+        out = torch.empty(max(len(reqs), 1), dtype=torch.uint8, device=plane.device)
+        self._check(self._L.vvcg_qt_mtt_split_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, _ptr(reqs),
+                                                  len(reqs), _ptr(out)))
+        torch.cuda.synchronize(plane.device)
+        return out.cpu().numpy()[:len(reqs)]
 
     def tu_autotune(self, recs, data, out, forward):
         """Times each CTA width of every size group of this batch and keeps the

@@ -20,6 +20,7 @@
 #include "gen_intra.cuh"
 #include "intra_search.cuh"
 #include "prune.cuh"
+#include "split.cuh"
 #include "lmcs.cuh"
 #include "mc.cuh"
 #include "metrics.cuh"
@@ -1322,6 +1323,38 @@ extern "C" vvcg_status vvcg_luma_intra_search_8_dev(vvcg_ctx* ctx, const uint8_t
 }
 
 // ---------------------------------------------------------------------------
+// Partition hook of the reference encoders (vvcg_qt_mtt_split_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_qt_mtt_split_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                             uint32_t height, uint8_t bit_depth, const vvcg_split_req* reqs,
+                                             uint32_t num_reqs, uint8_t* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!plane || !reqs || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, requests or results");
+  if (stride < width || bit_depth < 8 || bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
+  if (width > (1u << 20) || height > (1u << 20) || num_reqs > (1u << 24))
+    return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane or request count too large");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_split_req& q = reqs[i];
+    if (q.w < 1 || q.h < 1 || q.w > 4096 || q.h > 4096)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: region size outside 1..4096", i);
+    if (q.qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "request %u: QP above 63", i);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(vvcg_split_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(vvcg_split_req) * num_reqs, cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  SplitArgs A{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (int32_t)bit_depth, (int32_t)num_reqs,
+              (const vvcg_split_req*)ctx->d_tu_recs.p, res};
+  const uint32_t grid =
+      std::min<uint32_t>((num_reqs + kSplitWarps - 1) / kSplitWarps, (uint32_t)ctx->num_sms * 8);
+  k_qt_mtt_split<<<grid, kSplitWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "split launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // CTU full search of the GPU encoder (vvcg_ctu_search_dev).
 // ---------------------------------------------------------------------------
 // Blocks of a 32x32 CTU: (x, y, log2 w, log2 h) per slot; the slots of split
@@ -1443,6 +1476,7 @@ extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t*
 // CNN pruner forward pass (vvcg_cnn_forward_dev).
 // ---------------------------------------------------------------------------
 static_assert(kCnnParams == VVCG_CNN_PARAMS && kCnnOut == VVCG_CNN_OUT, "CNN layout");
+static_assert(sizeof(vvcg_split_req) == 16, "split request layout");
 static float cnn_qp_input(uint32_t qp) {  // QP / 63 rounded to bf16 (nearest even)
   float f = (float)qp / 63.0f;
   uint32_t u;
