@@ -605,6 +605,51 @@ vvcg_status vvcg_qt_mtt_split_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t
                                   uint32_t height, uint8_t bit_depth, const vvcg_split_req* reqs,
                                   uint32_t num_reqs, uint8_t* res);
 
+/* ---- motion-estimation hook of the reference encoders ------------------------ */
+
+typedef struct vvcg_mv_cand {  /* InterMergeCand (crates/rustmpeg-video/src/vvc/inter.rs:274) */
+  int32_t mv[2][2];            /* per list L0 / L1: (horizontal, vertical) in 1/16 luma samples */
+  int8_t ref_idx[2];           /* per list: reference index, < 0 = list unused */
+  uint8_t inter_dir;           /* bit 0: L0, bit 1: L1 */
+  uint8_t bcw_idx;             /* BCW weight index (values above 4 act as 4; 2 = equal weights) */
+  uint8_t alt_hpel;            /* alternative half-sample luma filter */
+  uint8_t reserved[3];
+} vvcg_mv_cand;                /* 24 bytes */
+
+typedef struct vvcg_me_req {
+  uint32_t x, y;               /* top-left luma sample; the block lies inside the plane */
+  uint16_t w, h;               /* block size, 1..128 each */
+  uint32_t cand_off;           /* first merge candidate of this block in the candidate array */
+  uint16_t num_cands;          /* merge list length (may be 0) */
+  uint16_t search_range;       /* diamond iterations at most (0 acts as 1) */
+  int32_t amvp[2];             /* the L0 AMVP predictor, 1/16 luma samples */
+} vvcg_me_req;                 /* 28 bytes */
+
+typedef struct vvcg_me_res {
+  uint64_t sad;                /* luma SAD of the choice; UINT64_MAX when nothing was evaluated */
+  vvcg_mv_cand cand;           /* the chosen merge candidate, or L0 uni-prediction at the searched MV */
+  uint16_t merge_idx;          /* merge list index when is_merge */
+  uint8_t is_merge;
+  uint8_t reserved[5];
+} vvcg_me_res;                 /* 40 bytes */
+
+/* Motion estimation of each block on 8-bit luma planes. Replaces
+ * estimate_inter_block (crates/rustmpeg-video/src/vvc/inter.rs:1866-2003), a
+ * hook that no encoder of the reference calls: the SAD of every merge
+ * candidate's luma prediction (predict_inter_pu, inter.rs:1733-1847, with BDOF
+ * and DMVR off: 8-tap interpolation, BCW average for bi-prediction, 128 without
+ * a usable list), then, when L0 has a reference, an integer diamond search on
+ * L0 reference 0 from the AMVP predictor and a quarter-sample refinement; the
+ * lowest SAD wins, the merge candidate on a tie. src and the references are
+ * device planes of one size and stride; ref_l0 / ref_l1 are host arrays of at
+ * most 16 device pointers each; cands and reqs are host arrays; res is device
+ * memory. Asynchronous on the context's stream. */
+vvcg_status vvcg_inter_search_8_dev(vvcg_ctx* ctx, const uint8_t* src, uint64_t stride, uint32_t width,
+                                    uint32_t height, const uint8_t* const* ref_l0, uint32_t num_l0,
+                                    const uint8_t* const* ref_l1, uint32_t num_l1, const vvcg_mv_cand* cands,
+                                    uint32_t num_cands, const vvcg_me_req* reqs, uint32_t num_reqs,
+                                    vvcg_me_res* res);
+
 typedef struct vvcg_ctu_search_req {
   uint32_t x, y;       /* top-left luma sample of a 32x32 CTU inside the plane */
   uint8_t split_mask;  /* bit s: evaluate split type s (0x3F: all six) */

@@ -104,6 +104,8 @@ def _declare(L):
     L.orc_predict_luma_8.restype = None
     L.orc_ctu_search.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint32, vp]
     L.orc_ctu_search.restype = None
+    L.orc_inter_search_8.argtypes = [vp, i, i, vp, i, i, vp, vp, i, vp]
+    L.orc_inter_search_8.restype = None
     L.orc_qt_mtt_split.argtypes = [vp, i, i, i, vp, i, vp]
     L.orc_qt_mtt_split.restype = None
     L.orc_gen_intra_predict.argtypes = [vp, vp, vp, i, i, i, i, vp, vp, i, i, i, vp, i, vp]
@@ -292,6 +294,21 @@ def ctu_search(src, bd, x, y, lambda_q8, split_mask=0x3F, cand=()):
     m = int(out[9])
     return dict(cost=int(out[0]), split_cost=[int(v) for v in out[1:7]], split=int(out[7]), cu_mode=int(out[8]),
                 modes=[(m >> (8 * k)) & 0xFF for k in range(4)])
+
+
+def inter_search_8(src, refs_l0, refs_l1, cands, reqs, res_dtype):
+    """estimate_inter_block (inter.rs:1866-2003) of each request on 8-bit
+    planes of one size: cands / reqs are structured arrays in the
+    vvcg_mv_cand / vvcg_me_req layouts; returns res_dtype (vvcg_me_res) results."""
+    src = np.ascontiguousarray(src, dtype=np.uint8)
+    planes = [np.ascontiguousarray(r, dtype=np.uint8) for r in list(refs_l0) + list(refs_l1)]
+    refs = np.ascontiguousarray(np.stack(planes)) if planes else np.zeros(1, np.uint8)
+    cands = np.ascontiguousarray(cands)
+    reqs = np.ascontiguousarray(reqs)
+    out = np.zeros(len(reqs), res_dtype)
+    lib().orc_inter_search_8(_p(src), src.shape[1], src.shape[0], _p(refs), len(refs_l0), len(refs_l1),
+                             _p(cands) if len(cands) else None, _p(reqs), len(reqs), _p(out))
+    return out
 
 
 def qt_mtt_split(src, bd, regions):

@@ -180,6 +180,10 @@ void interpolate_luma_block_8(const uint8_t* ref, int pw, int ph, int stride, in
 void interpolate_chroma_block_420_8(const uint8_t* ref, int pw, int ph, int stride, int cx, int cy, int cw,
                                     int ch, int mv_x, int mv_y, bool bi, int32_t* out);
 void weighted_average_bi_8(const int32_t* p0, const int32_t* p1, int n, int bcw_idx, int32_t* out);
+// inter.rs:1866-2003 estimate_inter_block on 8-bit planes of one size and stride.
+void estimate_inter_block_8(const uint8_t* src, const uint8_t* const* l0, int n0, const uint8_t* const* l1, int n1,
+                            int pw, int ph, int stride, const vvcg_mv_cand* cands, int ncand, int amvp_x, int amvp_y,
+                            int bx, int by, int w, int h, int range, vvcg_me_res* res);
 
 // ---- transform units (orc_tu.cpp) ------------------------------------------------
 // Same layout and flag values as vvcg_tu_rec / VVCG_TU_* of the C ABI.

@@ -189,6 +189,20 @@ extern "C" void orc_ctu_search(const uint16_t* src, int pw, int ph, int bd, int 
   out[8] = (uint32_t)cu_mode;
   out[9] = (uint32_t)(modes[0] | (modes[1] << 8) | (modes[2] << 16) | ((uint32_t)modes[3] << 24));
 }
+// 8-bit planes of pw x ph (row-major): src, then n0 + n1 references back to
+// back (L0 first); cands / reqs / out in the vvcg_mv_cand / vvcg_me_req /
+// vvcg_me_res layouts
+extern "C" void orc_inter_search_8(const uint8_t* src, int pw, int ph, const uint8_t* refs, int n0, int n1,
+                                   const vvcg_mv_cand* cands, const vvcg_me_req* reqs, int n, vvcg_me_res* out) {
+  std::vector<const uint8_t*> l0, l1;
+  for (int i = 0; i < n0; i++) l0.push_back(refs + (size_t)i * pw * ph);
+  for (int i = 0; i < n1; i++) l1.push_back(refs + (size_t)(n0 + i) * pw * ph);
+  for (int i = 0; i < n; i++) {
+    const vvcg_me_req& q = reqs[i];
+    orc::estimate_inter_block_8(src, l0.data(), n0, l1.data(), n1, pw, ph, pw, cands + q.cand_off, q.num_cands,
+                                q.amvp[0], q.amvp[1], (int)q.x, (int)q.y, q.w, q.h, q.search_range, &out[i]);
+  }
+}
 // regions as (x, y, w, h, qp, min_cb) int64 sextuples; out one split per region
 extern "C" void orc_qt_mtt_split(const uint16_t* src, int pw, int ph, int bd, const int64_t* regions, int n,
                                  uint8_t* out) {

@@ -299,4 +299,114 @@ void weighted_average_bi_16(const int32_t* p0, const int32_t* p1, int n, int bcw
   for (int i = 0; i < n; i++) out[i] = (uint16_t)clampi((p0[i] * w0 + p1[i] * w1 + off) >> sn, 0, mx);
 }
 
+// predict_inter_pu (inter.rs:1733-1847) luma part with BDOF and DMVR off, as
+// estimate_inter_block calls it: bi-prediction = two 14-bit interpolations and
+// weighted_average_bi; uni-prediction from the one usable list; 128 without.
+static void predict_pu_luma_8(const uint8_t* const* l0, int n0, const uint8_t* const* l1, int n1, int pw, int ph,
+                              int stride, const vvcg_mv_cand& c, int bx, int by, int w, int h, int32_t* out) {
+  const bool has0 = (c.inter_dir & 1) && c.ref_idx[0] >= 0 && n0 > 0;
+  const bool has1 = (c.inter_dir & 2) && c.ref_idx[1] >= 0 && n1 > 0;
+  const bool alt = c.alt_hpel != 0;
+  if (has0 && has1) {
+    const uint8_t* r0 = l0[std::min((int)c.ref_idx[0], n0 - 1)];
+    const uint8_t* r1 = l1[std::min((int)c.ref_idx[1], n1 - 1)];
+    std::vector<int32_t> p0((size_t)w * h), p1((size_t)w * h);
+    interpolate_luma_block_8(r0, pw, ph, stride, bx, by, w, h, c.mv[0][0], c.mv[0][1], true, alt, false, p0.data());
+    interpolate_luma_block_8(r1, pw, ph, stride, bx, by, w, h, c.mv[1][0], c.mv[1][1], true, alt, false, p1.data());
+    weighted_average_bi_8(p0.data(), p1.data(), w * h, c.bcw_idx, out);
+  } else if (has0 || has1) {
+    const int l = has0 ? 0 : 1;
+    const uint8_t* r = has0 ? l0[std::min((int)c.ref_idx[0], n0 - 1)] : l1[std::min((int)c.ref_idx[1], n1 - 1)];
+    interpolate_luma_block_8(r, pw, ph, stride, bx, by, w, h, c.mv[l][0], c.mv[l][1], false, alt, false, out);
+  } else {
+    for (int i = 0; i < w * h; i++) out[i] = 128;
+  }
+}
+
+// estimate_inter_block (inter.rs:1866-2003): merge candidates by luma SAD
+// (first lowest wins), then, with an L0 reference, the integer diamond search
+// on L0 reference 0 from the AMVP predictor (at most max(range, 1) rounds of
+// the four neighbours of the round's centre, stopping after a round without
+// improvement) and the quarter-sample refinement around its result; the merge
+// candidate wins ties with the searched vector.
+void estimate_inter_block_8(const uint8_t* src, const uint8_t* const* l0, int n0, const uint8_t* const* l1, int n1,
+                            int pw, int ph, int stride, const vvcg_mv_cand* cands, int ncand, int amvp_x, int amvp_y,
+                            int bx, int by, int w, int h, int range, vvcg_me_res* res) {
+  std::vector<int32_t> pred((size_t)w * h);
+  auto sad_of = [&]() {
+    uint64_t t = 0;
+    for (int y = 0; y < h; y++)
+      for (int x = 0; x < w; x++) t += (uint64_t)abs((int)src[(size_t)(by + y) * stride + bx + x] - pred[y * w + x]);
+    return t;
+  };
+  vvcg_mv_cand best_merge{};
+  best_merge.inter_dir = 1;  // InterMergeCand::default (inter.rs:297-306)
+  best_merge.ref_idx[0] = 0;
+  best_merge.ref_idx[1] = -1;
+  best_merge.bcw_idx = 2;
+  if (ncand > 0) best_merge = cands[0];
+  uint64_t best_merge_sad = UINT64_MAX;
+  int best_merge_idx = 0;
+  for (int i = 0; i < ncand; i++) {
+    predict_pu_luma_8(l0, n0, l1, n1, pw, ph, stride, cands[i], bx, by, w, h, pred.data());
+    const uint64_t s = sad_of();
+    if (s < best_merge_sad) {
+      best_merge_sad = s;
+      best_merge_idx = i;
+      best_merge = cands[i];
+    }
+  }
+  *res = vvcg_me_res{};
+  res->cand = best_merge;
+  res->is_merge = 1;
+  res->merge_idx = (uint16_t)best_merge_idx;
+  res->sad = best_merge_sad;
+  if (n0 == 0) return;
+  const uint8_t* r0 = l0[0];
+  auto sad_at = [&](int mx, int my) {
+    interpolate_luma_block_8(r0, pw, ph, stride, bx, by, w, h, mx, my, false, false, false, pred.data());
+    return sad_of();
+  };
+  int bmx = (amvp_x >> 4) << 4, bmy = (amvp_y >> 4) << 4;
+  uint64_t best = sad_at(bmx, bmy);
+  static const int kDiamond[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};
+  for (int it = 0; it < std::max(range, 1); it++) {
+    bool improved = false;
+    const int cx = bmx >> 4, cy = bmy >> 4;
+    for (int k = 0; k < 4; k++) {
+      const int tx = (cx + kDiamond[k][0]) << 4, ty = (cy + kDiamond[k][1]) << 4;
+      const uint64_t s = sad_at(tx, ty);
+      if (s < best) {
+        best = s;
+        bmx = tx;
+        bmy = ty;
+        improved = true;
+      }
+    }
+    if (!improved) break;
+  }
+  const int ix = bmx, iy = bmy;
+  static const int kQuarter[4][2] = {{4, 0}, {-4, 0}, {0, 4}, {0, -4}};
+  for (int k = 0; k < 4; k++) {
+    const uint64_t s = sad_at(ix + kQuarter[k][0], iy + kQuarter[k][1]);
+    if (s < best) {
+      best = s;
+      bmx = ix + kQuarter[k][0];
+      bmy = iy + kQuarter[k][1];
+    }
+  }
+  if (best_merge_sad <= best) return;
+  vvcg_mv_cand c{};
+  c.inter_dir = 1;
+  c.mv[0][0] = bmx;
+  c.mv[0][1] = bmy;
+  c.ref_idx[0] = 0;
+  c.ref_idx[1] = -1;
+  c.bcw_idx = 2;
+  res->cand = c;
+  res->is_merge = 0;
+  res->merge_idx = 0;
+  res->sad = best;
+}
+
 }  // namespace orc

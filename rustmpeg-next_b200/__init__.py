@@ -66,6 +66,12 @@ CTU_SEARCH_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("split_mask", "u1"
 CTU_SEARCH_RES_DTYPE = np.dtype([("cost", "<u4"), ("split_cost", "<u4", (6,)), ("split", "u1"), ("cu_mode", "u1"),
                                  ("modes", "u1", (4,)), ("reserved", "u1", (2,))])
 SPLIT_NONE, SPLIT_QT, SPLIT_BT_H, SPLIT_BT_V, SPLIT_TT_H, SPLIT_TT_V = range(6)
+MV_CAND_DTYPE = np.dtype([("mv", "<i4", (2, 2)), ("ref_idx", "i1", (2,)), ("inter_dir", "u1"), ("bcw_idx", "u1"),
+                          ("alt_hpel", "u1"), ("reserved", "u1", (3,))])
+ME_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("w", "<u2"), ("h", "<u2"), ("cand_off", "<u4"),
+                         ("num_cands", "<u2"), ("search_range", "<u2"), ("amvp", "<i4", (2,))])
+ME_RES_DTYPE = np.dtype([("sad", "<u8"), ("cand", MV_CAND_DTYPE), ("merge_idx", "<u2"), ("is_merge", "u1"),
+                         ("reserved", "u1", (5,))])
 SPLIT_REQ_DTYPE = np.dtype([("x", "<u4"), ("y", "<u4"), ("w", "<u2"), ("h", "<u2"), ("min_cb", "<u2"), ("qp", "u1"),
                             ("reserved", "u1")])
 CNN_PARAMS, CNN_OUT, CNN_MODES, CNN_SPLITS = 30761, 73, 67, 6
@@ -229,6 +235,7 @@ def lib():
             getattr(L, n).argtypes = [vp, vp, u32, vp, u64, vp, u64]
         L.vvcg_tu_autotune.argtypes = [vp, vp, u32, vp, u64, vp, u64, u32, vp]
         L.vvcg_qt_mtt_split_dev.argtypes = [vp, vp, u64, u32, u32, u8, vp, u32, vp]
+        L.vvcg_inter_search_8_dev.argtypes = [vp, vp, u64, u32, u32, vp, u32, vp, u32, vp, u32, vp, u32, vp]
         L.vvcg_encode_sizes.argtypes = [vp, u32, C.POINTER(u32), C.POINTER(u64)]
         L.vvcg_encode_batch.argtypes = [vp, vp, u32, vp, vp, u32, vp, u64]
         for n in ("vvcg_plane_metrics_8_dev", "vvcg_plane_metrics_16_dev"):
@@ -755,6 +762,27 @@ class Context:
         self._keep = recs
         self._check(self._L.vvcg_tu_forward_batch(self._h, _ptr(recs), len(recs), _ptr(data),
                                                   data.numel(), _ptr(out), out.numel()))
+
+    def inter_search_8(self, src, refs_l0, refs_l1, cands, reqs):
+        """Motion estimation (estimate_inter_block) of each ME_REQ_DTYPE block on
+        a (H, W) uint8 CUDA plane against lists of same-size uint8 CUDA
+        references, with MV_CAND_DTYPE merge candidates; returns ME_RES_DTYPE."""
+        import torch
+
+        cands = np.ascontiguousarray(cands, dtype=MV_CAND_DTYPE)
+        reqs = np.ascontiguousarray(reqs, dtype=ME_REQ_DTYPE)
+        h, w = src.shape
+        for r in list(refs_l0) + list(refs_l1):
+            if tuple(r.shape) != (h, w) or r.stride(0) != src.stride(0):
+                raise InvalidInput("references must have the source plane's size and stride")
+        l0 = (C.c_void_p * max(len(refs_l0), 1))(*[r.data_ptr() for r in refs_l0])
+        l1 = (C.c_void_p * max(len(refs_l1), 1))(*[r.data_ptr() for r in refs_l1])
+        out = torch.empty(max(len(reqs), 1) * ME_RES_DTYPE.itemsize, dtype=torch.uint8, device=src.device)
+        self._check(self._L.vvcg_inter_search_8_dev(self._h, _ptr(src), src.stride(0), w, h, l0, len(refs_l0), l1,
+                                                    len(refs_l1), _ptr(cands) if len(cands) else None, len(cands),
+                                                    _ptr(reqs), len(reqs), _ptr(out)))
+        torch.cuda.synchronize(src.device)
+        return out.cpu().numpy().view(ME_RES_DTYPE)[:len(reqs)]
 
     def qt_mtt_split(self, plane, bit_depth, reqs):
         """Quadrant-mean split decision (choose_qt_mtt_partition_rdo_16) of each

@@ -19,6 +19,7 @@
 #include "filters.cuh"
 #include "gen_intra.cuh"
 #include "intra_search.cuh"
+#include "inter_search.cuh"
 #include "prune.cuh"
 #include "split.cuh"
 #include "lmcs.cuh"
@@ -126,6 +127,7 @@ struct vvcg_ctx {
   DevBuf d_search_reqs, d_search_cost, d_search_mode, d_search_ctus;  // CTU full search
   DevBuf d_cnn_pack, d_cnn_packT;  // packed bf16 convolution weights of the CNN (forward / transposed)
   DevBuf d_cnn_acts, d_cnn_logits, d_cnn_gap, d_cnn_partial;  // CNN training workspace
+  DevBuf d_me_reqs, d_me_cands;  // motion-estimation requests and merge candidates
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -397,7 +399,10 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
                     &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
-                    &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs, &ctx->d_alfp, &ctx->d_alfc})
+                    &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs, &ctx->d_alfp, &ctx->d_alfc,
+                    &ctx->d_search_reqs, &ctx->d_search_cost, &ctx->d_search_mode, &ctx->d_search_ctus,
+                    &ctx->d_cnn_pack, &ctx->d_cnn_packT, &ctx->d_cnn_acts, &ctx->d_cnn_logits, &ctx->d_cnn_gap,
+                    &ctx->d_cnn_partial, &ctx->d_me_reqs, &ctx->d_me_cands})
     b->release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -1355,6 +1360,65 @@ extern "C" vvcg_status vvcg_qt_mtt_split_dev(vvcg_ctx* ctx, const uint16_t* plan
 }
 
 // ---------------------------------------------------------------------------
+// Motion-estimation hook of the reference encoders (vvcg_inter_search_8_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_inter_search_8_dev(vvcg_ctx* ctx, const uint8_t* src, uint64_t stride, uint32_t width,
+                                               uint32_t height, const uint8_t* const* ref_l0, uint32_t num_l0,
+                                               const uint8_t* const* ref_l1, uint32_t num_l1,
+                                               const vvcg_mv_cand* cands, uint32_t num_cands,
+                                               const vvcg_me_req* reqs, uint32_t num_reqs, vvcg_me_res* res) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!src || !reqs || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, requests or results");
+  if (!width || !height || stride < width) return fail(ctx, VVCG_INVALID_INPUT, "plane geometry");
+  if (width > (1u << 20) || height > (1u << 20) || num_reqs > (1u << 24))
+    return fail(ctx, VVCG_LIMIT_EXCEEDED, "plane or request count too large");
+  if (num_l0 > (uint32_t)kMeMaxRefs || num_l1 > (uint32_t)kMeMaxRefs)
+    return fail(ctx, VVCG_LIMIT_EXCEEDED, "more than %d references in a list", kMeMaxRefs);
+  if ((num_l0 && !ref_l0) || (num_l1 && !ref_l1) || (num_cands && !cands))
+    return fail(ctx, VVCG_INVALID_INPUT, "missing reference list or candidates");
+  MeArgs A{};
+  for (uint32_t i = 0; i < num_l0; i++)
+    if (!(A.l0[i] = ref_l0[i])) return fail(ctx, VVCG_INVALID_INPUT, "L0 reference %u is null", i);
+  for (uint32_t i = 0; i < num_l1; i++)
+    if (!(A.l1[i] = ref_l1[i])) return fail(ctx, VVCG_INVALID_INPUT, "L1 reference %u is null", i);
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_me_req& q = reqs[i];
+    if (q.w < 1 || q.h < 1 || q.w > 128 || q.h > 128)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block size outside 1..128", i);
+    if ((uint64_t)q.x + q.w > width || (uint64_t)q.y + q.h > height)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block outside the plane", i);
+    if ((uint64_t)q.cand_off + q.num_cands > num_cands)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: merge candidates past the array", i);
+  }
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_me_reqs.reserve(sizeof(vvcg_me_req) * num_reqs), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_me_reqs.p, reqs, sizeof(vvcg_me_req) * num_reqs, cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  if (num_cands) {
+    CK(ctx->d_me_cands.reserve(sizeof(vvcg_mv_cand) * num_cands), "cudaMalloc");
+    CK(cudaMemcpyAsync(ctx->d_me_cands.p, cands, sizeof(vvcg_mv_cand) * num_cands, cudaMemcpyHostToDevice,
+                       ctx->stream),
+       "upload");
+  }
+  A.src = src;
+  A.stride = (int64_t)stride;
+  A.width = (int32_t)width;
+  A.height = (int32_t)height;
+  A.n0 = (int32_t)num_l0;
+  A.n1 = (int32_t)num_l1;
+  A.cands = num_cands ? (const vvcg_mv_cand*)ctx->d_me_cands.p : nullptr;
+  A.reqs = (const vvcg_me_req*)ctx->d_me_reqs.p;
+  A.n = (int32_t)num_reqs;
+  A.res = res;
+  const uint32_t grid = std::min<uint32_t>(num_reqs, (uint32_t)ctx->num_sms * 8);
+  k_inter_search_8<<<grid, kMeThreads, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "motion search launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
 // CTU full search of the GPU encoder (vvcg_ctu_search_dev).
 // ---------------------------------------------------------------------------
 // Blocks of a 32x32 CTU: (x, y, log2 w, log2 h) per slot; the slots of split
@@ -1477,6 +1541,8 @@ extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t*
 // ---------------------------------------------------------------------------
 static_assert(kCnnParams == VVCG_CNN_PARAMS && kCnnOut == VVCG_CNN_OUT, "CNN layout");
 static_assert(sizeof(vvcg_split_req) == 16, "split request layout");
+static_assert(sizeof(vvcg_mv_cand) == 24 && sizeof(vvcg_me_req) == 28 && sizeof(vvcg_me_res) == 40,
+              "motion-estimation layouts");
 static float cnn_qp_input(uint32_t qp) {  // QP / 63 rounded to bf16 (nearest even)
   float f = (float)qp / 63.0f;
   uint32_t u;
