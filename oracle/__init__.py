@@ -104,6 +104,8 @@ def _declare(L):
     L.orc_predict_luma_8.restype = None
     L.orc_ctu_search.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint32, vp]
     L.orc_ctu_search.restype = None
+    L.orc_lfnst.argtypes = [i, vp, i, i, i, i]
+    L.orc_lfnst.restype = i
     L.orc_inter_search_8.argtypes = [vp, i, i, vp, i, i, vp, vp, i, vp]
     L.orc_inter_search_8.restype = None
     L.orc_qt_mtt_split.argtypes = [vp, i, i, i, vp, i, vp]
@@ -294,6 +296,14 @@ def ctu_search(src, bd, x, y, lambda_q8, split_mask=0x3F, cand=()):
     m = int(out[9])
     return dict(cost=int(out[0]), split_cost=[int(v) for v in out[1:7]], split=int(out[7]), cu_mode=int(out[8]),
                 modes=[(m >> (8 * k)) & 0xFF for k in range(4)])
+
+
+def lfnst(coeffs, w, h, idx, mode, forward):
+    """forward_lfnst_rect / inverse_lfnst_rect (lfnst.rs) on a copy of the
+    w x h raster coefficients; returns (status, coefficients), status 0 = ok."""
+    c = np.ascontiguousarray(np.asarray(coeffs, dtype=np.int32).reshape(-1)).copy()
+    rc = lib().orc_lfnst(int(bool(forward)), _p(c), w, h, idx, mode)
+    return rc, c
 
 
 def inter_search_8(src, refs_l0, refs_l1, cands, reqs, res_dtype):

@@ -189,6 +189,11 @@ extern "C" void orc_ctu_search(const uint16_t* src, int pw, int ph, int bd, int 
   out[8] = (uint32_t)cu_mode;
   out[9] = (uint32_t)(modes[0] | (modes[1] << 8) | (modes[2] << 16) | ((uint32_t)modes[3] << 24));
 }
+// lfnst.rs forward_lfnst_rect / inverse_lfnst_rect on a w x h raster block in
+// place; returns 0, or non-zero where the reference returns an error
+extern "C" int orc_lfnst(int forward, int32_t* coeffs, int w, int h, int idx, int mode) {
+  return forward ? orc::forward_lfnst_rect(coeffs, w, h, idx, mode) : orc::inverse_lfnst_rect(coeffs, w, h, idx, mode);
+}
 // 8-bit planes of pw x ph (row-major): src, then n0 + n1 references back to
 // back (L0 first); cands / reqs / out in the vvcg_mv_cand / vvcg_me_req /
 // vvcg_me_res layouts
