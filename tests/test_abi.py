@@ -107,3 +107,40 @@ def test_value_noise_content_shape_and_range(pkg):
     assert y.max() <= 1023 and u.min() >= 384 and u.max() <= 640
     y2, _, _ = synth.value_noise_frame(256, 144, 10, frame=2)
     assert (y == y2).all()
+
+
+# every record dtype of the package and the header struct it mirrors
+RECORDS = {
+    "CU_DTYPE": "vvcg_cu_rec", "SAO_DTYPE": "vvcg_sao", "CTU_DTYPE": "vvcg_ctu_filter",
+    "PIC_DTYPE": "vvcg_pic_desc", "APS_DTYPE": "vvcg_alf_aps", "MC_BLOCK_DTYPE": "vvcg_mc_block",
+    "LMCS_APS_DTYPE": "vvcg_lmcs_aps", "LMCS_TABLES_DTYPE": "vvcg_lmcs_tables", "CRES_DTYPE": "vvcg_cres_rec",
+    "ALF_CTU_DTYPE": "vvcg_alf_ctu", "ALF_PARAMS_DTYPE": "vvcg_alf_params",
+    "ISR_REQ_DTYPE": "vvcg_intra_search_req", "ISR_RES_DTYPE": "vvcg_intra_search_res",
+    "CTU_SEARCH_REQ_DTYPE": "vvcg_ctu_search_req", "CTU_SEARCH_RES_DTYPE": "vvcg_ctu_search_res",
+    "MV_CAND_DTYPE": "vvcg_mv_cand", "ME_REQ_DTYPE": "vvcg_me_req", "ME_RES_DTYPE": "vvcg_me_res",
+    "SPLIT_REQ_DTYPE": "vvcg_split_req", "GEN_INTRA_REQ_DTYPE": "vvcg_gen_intra_req",
+    "DBK_CELL_DTYPE": "vvcg_dbk_cell", "DBK_CCELL_DTYPE": "vvcg_dbk_ccell", "DBK_PARAMS_DTYPE": "vvcg_dbk_params",
+    "MIP_REQ_DTYPE": "vvcg_mip_req", "MIP_RES_DTYPE": "vvcg_mip_res", "TXS_REQ_DTYPE": "vvcg_tx_search_req",
+    "TXS_RES_DTYPE": "vvcg_tx_search_res", "TU_DTYPE": "vvcg_tu_rec",
+}
+
+
+def test_every_record_dtype_matches_its_struct_field_by_field(pkg):
+    missing = sorted(n for n in dir(pkg) if n.endswith("_DTYPE") and n not in RECORDS)
+    assert not missing, f"record dtypes without a layout check: {missing}"
+    lines, expect = [], []
+    for name, struct in RECORDS.items():
+        dt = getattr(pkg, name)
+        lines.append(f'  printf("%zu\\n", sizeof({struct}));')
+        expect.append(dt.itemsize)
+        for field, (_, off) in dt.fields.items():
+            lines.append(f'  printf("%zu\\n", offsetof({struct}, {field}));')
+            expect.append(off)
+    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"vvcg.h\"\nint main(void) {\n" + "\n".join(lines) + \
+        "\n  return 0;\n}\n"
+    with tempfile.TemporaryDirectory() as d:
+        src, exe = os.path.join(d, "t.c"), os.path.join(d, "t")
+        open(src, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", exe, src], check=True)
+        got = list(map(int, subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()))
+    assert got == expect
