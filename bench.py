@@ -77,16 +77,20 @@ class ClockSampler:
     def __init__(self, device_index):
         self.dev = device_index
         self.proc = None
-        self.path = tempfile.mktemp(suffix=".csv")
+        self.path = None
 
     def start(self):
         try:
-            self.f = open(self.path, "w")
+            self.f = tempfile.NamedTemporaryFile("w", suffix=".csv", delete=False)
+            self.path = self.f.name
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            if self.path:
+                self.f.close()
+                os.unlink(self.path)
             return
         # nvidia-smi takes a moment to start: timing begins once it has sampled
         t0 = time.perf_counter()
