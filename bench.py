@@ -457,9 +457,23 @@ def main():
 CNN_FLOP_PER_BLOCK = 2 * 1024 * 32 * 9 * (2 + 3 * 32)  # conv1 (2 inputs) + 3 x conv 32->32 (57.8 MFLOP)
 
 
-# CNN pruning policies (top modes, top splits, probability-mass threshold);
-# the first is the headline, the others show the speed / cost trade-off.
-PRUNE_POLICIES = ((6, 2, 0.7), (3, 2, 0.0), (6, 3, 0.7), (6, 2, 0.8), (3, 3, 0.8))
+# CNN pruning policies (top modes, top splits, probability-mass threshold).
+# The headline is the fastest whose total cost stays within COST_BOUND_PCT of
+# the full search (the stand-in for the metric's 1% BD-rate bound, which
+# needs a bitstream); all are reported. The first also gives the
+# no-fallback comparison of the trained and an untrained network.
+PRUNE_POLICIES = ((6, 2, 0.7), (3, 2, 0.0), (6, 3, 0.7), (6, 2, 0.75), (6, 3, 0.75), (6, 2, 0.8), (6, 3, 0.8),
+                  (3, 3, 0.8), (6, 3, 0.85))
+COST_BOUND_PCT = 1.0
+
+
+def pick_headline(policies, bound_pct=COST_BOUND_PCT):
+    """The fastest policy whose total cost is within bound_pct of the full
+    search (the first of equals); the cheapest one when none is."""
+    within = [q for q in policies if q["cost_increase_pct"] <= bound_pct]
+    if within:
+        return max(within, key=lambda q: q["speedup"])
+    return min(policies, key=lambda q: q["cost_increase_pct"])
 
 
 def bench_encoder(pkg, ctx, stream, dev, args, peaks):
@@ -560,17 +574,19 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
     for (tm, ts, thr), p in zip(PRUNE_POLICIES, pol):
         policies.append({"top_modes": tm, "top_splits": ts, "threshold": thr,
                          "fps": round(n_runs / (p["ms"] * 1e-3), 1), "speedup": round(full_ms / p["ms"], 2),
+                         "ms_per_frame": round(p["ms"] / n_runs, 4),
                          "cost_increase_pct": round(100.0 * (p["cost"] / cost_f - 1.0), 3),
                          "fallback_rate": {"modes": round(p["fb_mode"] / total, 4),
                                            "splits": round(p["fb_split"] / total, 4)}})
-    head = policies[0]
+    head = pick_headline(policies)
     return {"what": "candidate-cost stage of the GPU encoder (intra mode + split decision per 32x32 CTU, "
                     "SATD + lambda*bits, open loop); no bitstream, so BD-rate is not measured",
             "frames": f"{len(frames)} held-out 1920x1080 10-bit frames x QP{list(QPS)}",
             "full_fps": round(full_fps, 1), "pruned_fps": head["fps"], "speedup": head["speedup"],
             "policy": {k: head[k] for k in ("top_modes", "top_splits", "threshold")},
+            "headline_rule": f"fastest policy with total cost within {COST_BOUND_PCT}% of the full search",
             "full_ms_per_frame": round(full_ms / n_runs, 4),
-            "pruned_ms_per_frame": round(pol[0]["ms"] / n_runs, 4),
+            "pruned_ms_per_frame": head["ms_per_frame"],
             "cnn_ms_per_frame": round(cnn_ms / n_runs, 4),
             "cost_increase_pct": head["cost_increase_pct"],
             "no_fallback_cost_increase_pct": {"trained": round(100.0 * (cost_ft / cost_f - 1.0), 3),
