@@ -28,3 +28,20 @@ def test_cpu_sample_spreads_over_the_batch():
     assert len(idx) == 64 and len(set(idx)) == 64
     assert {i // 32 for i in idx} == {0, 1, 2, 3}  # every QP group of 32 pictures
     assert bench.sample_indices(4, 16) == [0, 1, 2, 3]
+
+
+def test_reference_arm_prints_the_contract_line():
+    import json
+    import subprocess
+
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, timeout=600, check=True).stdout
+    lines = [l for l in out.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == "Mpx/s"
+    assert d["higher_is_better"] is True and d["steps"] == 1 and d["value"] > 0
+    assert d["config"]["workload"] == bench.workload_name(32)
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["kind"] == "port"
+    assert d["e2e"] == {"value": d["value"], "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
