@@ -835,11 +835,42 @@ def recon_picture_static(pic, cus, levels, planes, stream=None):
     the current device and `stream` (a torch.cuda.Stream, a raw handle, or
     None for the legacy default stream) and returns when it has finished.
     """
+    import torch
+
     L = lib()
     desc = np.asarray(pic, dtype=PIC_DTYPE).reshape(1).copy()
+    # The C side sees raw pointers only: every size, type and layout the
+    # kernels rely on is checked here, before anything is launched.
+    dev = torch.cuda.current_device()
+
+    def on_device(t, what):
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.device.index != dev:
+            raise InvalidInput(f"{what} must be a CUDA tensor on the current device (cuda:{dev})")
+
+    on_device(cus, "cus")
+    on_device(levels, "levels")
+    if cus.dtype != torch.uint8 or not cus.is_contiguous():
+        raise InvalidInput("cus must be a contiguous uint8 tensor of CU_DTYPE records")
+    if cus.numel() % CU_DTYPE.itemsize:
+        raise InvalidInput(f"cus holds {cus.numel()} bytes, not a whole number of {CU_DTYPE.itemsize}-byte records")
+    if levels.dtype != torch.int16 or not levels.is_contiguous():
+        raise InvalidInput("levels must be a contiguous int16 tensor")
+    w, h, cf = int(desc[0]["width"]), int(desc[0]["height"]), int(desc[0]["chroma_format"])
+    cw, ch = chroma_dims(w, h, cf)
+    dims = [(h, w), (ch, cw), (ch, cw)]
     arr = (_PlaneOut * 3)()
     for c in range(3):
         a = planes[c] if c < len(planes) else None
+        if c > 0 and cf == CHROMA_400:
+            a = None
+        elif a is None:
+            raise InvalidInput(f"plane {c} is missing")
+        if a is not None:
+            on_device(a, f"plane {c}")
+            if a.dtype not in (torch.int16, torch.uint16) or a.dim() != 2 or a.stride(1) != 1:
+                raise InvalidInput(f"plane {c} must be a 2-D 16-bit tensor with unit column stride")
+            if a.shape[0] < dims[c][0] or a.shape[1] < dims[c][1]:
+                raise InvalidInput(f"plane {c} is {tuple(a.shape)}; the coded size needs {dims[c]}")
         arr[c] = _PlaneOut(None, 0, 0) if a is None else _PlaneOut(_ptr(a), a.stride(0), 0)
     raw = None if stream is None else getattr(stream, "cuda_stream", stream)
     err = C.create_string_buffer(512)
