@@ -2,24 +2,30 @@
 
 Workload (one step): a batch of 128 pictures of 1920x1080 (coded 1920x1088)
 10-bit 4:2:0 = 32 frames at each of QP 22, 27, 32, 37, CTU 32, reconstructed
-(dequantisation, inverse DCT-II, intra prediction as a CTU wavefront, add/clip)
-and filtered (deblocking, SAO, ALF with an APS). Decoder records are seeded
-synthetic records with coded-picture statistics (rustmpeg-next_b200/synth.py).
-The metric counts visible luma pixels (1920x1080) per second.
+(dequantisation incl. dependent quantisation, inverse DCT-II, intra
+prediction as a CTU wavefront, add/clip) and filtered (deblocking, SAO, ALF
+with an APS). The records are what the repo's GPU encoder (vvcg_encode_batch,
+bit-exact with the oracle's restatement of the reference encoder) makes of
+the full-frame content (value noise translated per frame plus 8 moving
+textured rectangles, rustmpeg-next_b200/synth.py); SAO and ALF parameters
+are seeded per CTU. The metric counts visible luma pixels (1920x1080) per
+second. Before timing, every picture of the batch is compared with the
+oracle (the `parity` object of the line).
 
-value : device-resident throughput (records already in HBM; the 466 MB level
-        pool and 1.6 GB of planes exceed the 126 MB L2, so no flush is needed).
+value : device-resident throughput (records already in HBM; the level pool
+        and the 1.6 GB of planes exceed the 126 MB L2, so no flush is needed).
 e2e   : the same through the C ABI with host buffers, streamed: every step
         copies the records from pinned host memory, runs, and copies the
         visible planes back to pinned host memory (vvcg_decode_batch_async,
         vvcg_batch_sync); steps rotate over three contexts so that one step's
         download overlaps the next steps' uploads and kernels. Wall-clock time
         over the steps, fill and drain included.
-Multi-GPU: replicas (each rank reconstructs its own batch; no collective on the
-data path); time is the max over ranks.
+Multi-GPU: replicas (each rank reconstructs its own batch, from its own
+content stream; no collective on the data path); time is the max over ranks.
 
 `--impl reference` times the CPU oracle (the C++ restatement of the reference's
-single-threaded CPU decoder path) on the host cores instead.
+single-threaded CPU decoder path) on the host cores instead, one process per
+core, each decoding its own picture of the same workload per step.
 """
 from __future__ import annotations
 
@@ -55,16 +61,98 @@ def load_pkg():
     return mod
 
 
-def workload_specs(frames_per_qp):
-    return [dict(width=PIX_W, height=CODED_H, visible_width=PIX_W, visible_height=PIX_H, bit_depth=10,
-                 chroma_format=1, ctu_log2=5, qp=q) for q in QPS for _ in range(frames_per_qp)]
-
-
-def build_records(pkg, frames_per_qp, seed):
+def _frame_sources(frame, stream):
+    """Coded-size source planes of one frame of the workload's content
+    (a task of the spawned generator pool)."""
+    load_pkg()
     from rustmpeg_next_b200 import synth
 
-    tools = pkg.TOOL_DEBLOCK | pkg.TOOL_SAO | pkg.TOOL_ALF
-    return synth.random_records(workload_specs(frames_per_qp), seed=seed, tools=tools, alf_aps=True)
+    _, _, p = synth.workload_picture(frame, 1, QPS[:1])
+    return synth.workload_sources(frame, p, stream)
+
+
+def make_sources(frames, stream, procs):
+    """The frames' source planes, generated in a pool of spawned processes."""
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(max(1, min(procs, frames))) as pool:
+        planes = pool.starmap(_frame_sources, [(f, stream) for f in range(frames)])
+    return dict(enumerate(planes))
+
+
+def build_workload(pkg, ctx, frames_per_qp, rank):
+    """The step's decoder records: frames_per_qp frames of the rank's content
+    stream at each QP, encoded on the GPU by `ctx`."""
+    from rustmpeg_next_b200 import synth
+
+    sources = make_sources(frames_per_qp, rank, os.cpu_count() or 1)
+    return synth.encoded_workload(ctx, frames_per_qp, QPS, rank_seed(rank), sources=sources, stream=rank)
+
+
+def picture_records(pics, cus, levels, ctus, i):
+    """Picture i's own records, with its level range cut out and rebased."""
+    p = pics[i].copy()
+    tb = min(1 << int(p["ctu_log2"]), 32)
+    n = (int(p["width"]) // tb) * (int(p["height"]) // tb)
+    nc = (int(p["width"]) >> int(p["ctu_log2"])) * (int(p["height"]) >> int(p["ctu_log2"]))
+    c = cus[int(p["cu_offset"]):][:n].copy()
+    t = ctus[int(p["ctu_offset"]):][:nc].copy()
+    lo = c["level_off"]
+    used = lo[lo >= 0]
+    start = int(used.min()) if used.size else 0
+    end = min(len(levels), int(used.max()) + tb * tb) if used.size else 0
+    c["level_off"] = np.where(lo >= 0, lo - start, -1)
+    p["cu_offset"], p["ctu_offset"] = 0, 0
+    return p, c, levels[start:end].copy(), t
+
+
+def _parity_task(task):
+    """Oracle reconstruction of one picture against the GPU's visible planes;
+    returns (oracle status, differing samples)."""
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    p, c, lv, t, a, planes = task
+    rc, ref = oracle.recon_frame(p, c, lv, t, a)
+    bad = 0
+    for g, r in zip(planes, ref):
+        if g is not None:
+            bad += int((g != r[:g.shape[0], :g.shape[1]]).sum())
+    return rc, bad
+
+
+def parity_check(pics, cus, levels, ctus, aps, outs, procs):
+    """Every picture of the batch against the oracle (outside the timed
+    region), in a pool of spawned processes."""
+    import multiprocessing as mp
+
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    oracle.build()
+    tasks = []
+    for i in range(len(pics)):
+        p, c, lv, t = picture_records(pics, cus, levels, ctus, i)
+        a = None if aps is None or int(p["alf_aps"]) < 0 else aps[int(p["alf_aps"])]
+        tasks.append((p, c, lv, t, a, outs[i]))
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(max(1, min(procs, len(tasks)))) as pool:
+        res = pool.map(_parity_task, tasks, chunksize=1)
+    return {"checked": len(res), "mismatches": sum(1 for rc, bad in res if rc != 0 or bad),
+            "samples_differing": sum(bad for _, bad in res),
+            "against": "oracle (C++ restatement of the reference decoder), every picture of the batch, "
+                       "all planes, before timing",
+            "s": round(time.perf_counter() - t0, 1)}
+
+
+def workload_name(frames_per_qp):
+    return (f"1920x1080 10-bit 4:2:0, {frames_per_qp} frames x QP{{22,27,32,37}} = {4 * frames_per_qp} "
+            "pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)")
+
+
+RECORDS = ("value-noise content of the full-frame configuration encoded all-intra by the repo's GPU encoder "
+           "(7-mode intra, CCLM, dependent quantisation, deblocking; bit-exact with the oracle's encoder); "
+           "SAO and ALF parameters seeded per CTU; coded TBs' levels only")
 
 
 class ClockSampler:
@@ -189,49 +277,68 @@ def _oracle_one(p, cus, levels, ctus, aps):
     assert rc == 0
 
 
-# Worker state of the reference arm's process pool: the batch's records are
-# handed to each worker once, when the pool starts; a task is a picture index.
-_WORKER = {}
-
-
-def _worker_init(pics, cus, levels, ctus, aps):
+def _ref_worker(conn, index, frames_per_qp, seed):
+    """One core of the reference arm: builds its own picture of the workload
+    (the oracle's encoder on the same content), then decodes it once per
+    "go" until told to stop."""
     sys.path.insert(0, ROOT)
     import oracle
 
     oracle.build()
-    _WORKER.update(pics=pics, cus=cus, levels=levels, ctus=ctus, aps=aps)
+    load_pkg()
+    from rustmpeg_next_b200 import synth
 
-
-def _worker_picture(i):
-    w = _WORKER
-    _oracle_one(w["pics"][i], w["cus"], w["levels"], w["ctus"], w["aps"])
-    return i
+    p, cus, levels, ctus = synth.oracle_workload_picture(oracle, index, frames_per_qp, QPS, seed)
+    aps = synth.workload_aps(seed)
+    conn.send("ready")
+    while conn.recv() is not None:
+        rc, _ = oracle.recon_frame(p, cus, levels, ctus, aps[0])
+        conn.send(rc)
 
 
 def run_reference(args, rank):
     """--impl reference: the oracle on all host cores, one process per core
-    (the Rust reference cannot be built here). Each step reconstructs a
-    bounded sample of the workload's pictures, one per core, spread over the
-    four QPs; the pool and its copies of the records exist before the timed
+    (the Rust reference cannot be built here). Each process holds one picture
+    of the workload (sampled over the batch, all four QPs) and decodes it
+    once per step; the processes and their records exist before the timed
     steps, so a step times decoding only."""
     if rank != 0:
         return
     import multiprocessing as mp
 
-    pkg = load_pkg()
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    oracle.build()  # once, before the workers load it
     cores = os.cpu_count() or 1
-    pics, cus, levels, ctus, aps = build_records(pkg, max(1, (cores + 3) // 4), seed=rank_seed(0))
-    sample = sample_indices(len(pics), cores)
+    sample = sample_indices(4 * args.frames_per_qp, cores)
+    ctx = mp.get_context("spawn")
+    workers = []
+    for i in sample:
+        here, there = ctx.Pipe()
+        proc = ctx.Process(target=_ref_worker, args=(there, i, args.frames_per_qp, rank_seed(0)), daemon=True)
+        proc.start()
+        workers.append((proc, here))
+    for _, c in workers:
+        assert c.recv() == "ready"
+
+    def step():
+        for _, c in workers:
+            c.send(True)
+        for _, c in workers:
+            assert c.recv() == 0
+
+    for _ in range(args.warmup):
+        step()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    for proc, c in workers:
+        c.send(None)
+        proc.join(timeout=30)
     n = len(sample)
-    with mp.get_context("spawn").Pool(cores, initializer=_worker_init,
-                                      initargs=(pics, cus, levels, ctus, aps)) as pool:
-        for _ in range(args.warmup):
-            pool.map(_worker_picture, sample, chunksize=1)
-        times = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            pool.map(_worker_picture, sample, chunksize=1)
-            times.append(time.perf_counter() - t0)
     mean = sum(times) / len(times)
     value = n * PIX_W * PIX_H / mean / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mpx/s",
@@ -239,8 +346,9 @@ def run_reference(args, rank):
             "ms_per_step": round(mean * 1e3, 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": workload_name(args.frames_per_qp), "pictures_per_step": 4 * args.frames_per_qp,
-                       "sample_pictures_per_step": n,
-                       "sample": "pictures of the same generator and QPs as the workload"},
+                       "sample_pictures_per_step": n, "records": RECORDS,
+                       "sample": "pictures of the same workload (same content, QPs, encoder and seeds), "
+                                 "spread over the batch"},
             "cpu_baseline": {"value": round(value, 3), "unit": "Mpx/s", "cores": cores, "kind": "port",
                              "sample": f"{n} pictures of 1920x1080 per step (QP 22-37), one process per "
                                        "core (C++ restatement of the reference CPU path, g++ -O2)"},
@@ -257,8 +365,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames-per-qp", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=64,
-                    help="pictures in the CPU baseline sample (about 0.15 s each on one core)")
+    ap.add_argument("--cpu-sample", type=int, default=48,
+                    help="pictures in the CPU baseline sample (about 0.25 s each on one core)")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the batch before timing")
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -287,7 +396,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
 
-    pics, cus, levels, ctus, aps = build_records(pkg, args.frames_per_qp, seed=rank_seed(rank))
+    ctx = pkg.Context(local)
+    t_wl = time.perf_counter()
+    pics, cus, levels, ctus, aps = build_workload(pkg, ctx, args.frames_per_qp, rank)
+    workload_s = time.perf_counter() - t_wl
     n_pics = len(pics)
     # pinned host copies for the end-to-end leg
     pin = lambda a: torch.from_numpy(a.view(np.uint8)).pin_memory().numpy().view(a.dtype)  # noqa: E731
@@ -298,7 +410,6 @@ def main():
              torch.empty((PIX_H // 2, PIX_W // 2), dtype=torch.int16).pin_memory().numpy().view(np.uint16))
             for _ in range(n_pics)]
 
-    ctx = pkg.Context(local)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream)
     ctx.prepare(batch)
@@ -322,9 +433,14 @@ def main():
         sync_all()
         return max_over_ranks(ms, dist, dev)
 
-    # correctness of the configuration before timing (no reference aborts)
+    # correctness of the configuration before timing: every picture of the
+    # batch against the oracle (rank 0; the other replicas run the same code)
     ctx.run(pkg.STAGE_ALL)
     ctx.sync()
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = parity_check(pics, cus, levels, ctus, aps, ctx.download(batch.output_planes()),
+                              os.cpu_count() or 1)
 
     # warm-up (the first graph run captures the stages), then the timed steps
     use_graph = not args.no_graph
@@ -413,12 +529,16 @@ def main():
                 "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
                 "stages_frac": {k: round(alg[k] / (stage_ms[k] * 1e-3) / 1e9 / hbm_peak, 4)
                                 for k in stage_ms}}
+    # DRAM traffic of the dominant stage per step: not measured in this run
+    # (bench numbers are never taken under a profiler) but read from the
+    # committed ncu capture of the same workload, with that capture's note
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         try:
             tr = json.load(open(traffic_file))
-            if dom in tr:
-                roofline["traffic"] = tr[dom]
+            if tr.get("workload") == workload_name(args.frames_per_qp) and dom in tr.get("per_step", {}):
+                roofline["traffic"] = tr["per_step"][dom]
+                roofline["traffic_source"] = tr.get("_note")
         except Exception:
             pass
 
@@ -430,7 +550,8 @@ def main():
                        "pictures_per_step": n_pics, "parallelism": f"replicas x{world}",
                        "launch": "direct launches" if args.no_graph else "CUDA graph replay",
                        "l2": "inputs larger than L2 (466 MB levels, 1.6 GB planes); no flush",
-                       "records": "seeded synthetic decoder records"},
+                       "records": RECORDS, "workload_build_s": round(workload_s, 1)},
+            "parity": parity,
             "roofline": roofline,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mpx/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import (APS_DTYPE, CTU_DTYPE, CU_DTYPE, PIC_DTYPE, TOOL_ALF, TOOL_DEBLOCK, TOOL_DEP_QUANT,
-               TOOL_SAO, chroma_dims)
+               TOOL_ENC_CCLM, TOOL_ENC_FULL_INTRA, TOOL_SAO, chroma_dims)
 
 
 def seed_for(stream: int, frame: int) -> int:
@@ -154,27 +154,7 @@ def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=
             cbf |= (coded.astype(np.uint8) << c)
         cus["level_off"] = lo
         cus["cbf"] = cbf
-        nctu = (h // ctu) * (w // ctu)
-        ctus = np.zeros(nctu, CTU_DTYPE)
-        omax = (1 << (min(bd, 10) - 5)) - 1
-        row = np.arange(nctu) // (w // ctu)
-        edge_row = (row == 0) | (row == h // ctu - 1)
-        for c in range(3 if cf else 1):
-            r = rng.random(nctu)
-            band = r < sao_prob / 2
-            edge = (r >= sao_prob / 2) & (r <= sao_prob)
-            eo = rng.integers(0, 4, nctu)
-            if not sao_class3_on_edges:
-                eo = np.where((eo == 3) & edge_row, 2, eo)
-            o = rng.integers(0, omax + 1, (nctu, 4))
-            ob = rng.integers(-omax, omax + 1, (nctu, 4))
-            s = ctus["sao"][:, c]
-            s["type"] = np.where(band, 1, np.where(edge, 2, 0))
-            s["band_or_class"] = np.where(band, rng.integers(0, 32, nctu), np.where(edge, eo, 0))
-            s["offsets"] = np.where(band[:, None], ob,
-                                    np.where(edge[:, None], o * np.array([1, 1, -1, -1]), 0))
-            ctus["sao"][:, c] = s
-        ctus["alf_luma"] = rng.random(nctu) < 0.7
+        ctus = random_ctu_params(rng, w, h, ctu, bd, cf, sao_prob, sao_class3_on_edges)
         pics.append(p)
         cu_chunks.append(cus)
         ctu_chunks.append(ctus)
@@ -186,6 +166,36 @@ def random_records(pics_spec, seed=0, tools=TOOL_DEBLOCK, sao_prob=0.6, alf_aps=
     levels = np.concatenate(lv_chunks) if lv_chunks else np.zeros(0, np.int16)
     return (np.array(pics, PIC_DTYPE), np.concatenate(cu_chunks), levels,
             np.concatenate(ctu_chunks), aps)
+
+
+def random_ctu_params(rng, w, h, ctu, bd, cf, sao_prob=0.6, sao_class3_on_edges=False, alf_prob=0.7):
+    """Per-CTU SAO parameters (band offset or one of the 4 edge classes per
+    component, offsets within the ranges the syntax allows at this bit depth)
+    and ALF luma switches for one w x h picture, CTU_DTYPE records in raster
+    order. SAO edge class 3 is kept off the first and last CTU rows unless
+    sao_class3_on_edges (the reference aborts on it there)."""
+    nctu = (h // ctu) * (w // ctu)
+    ctus = np.zeros(nctu, CTU_DTYPE)
+    omax = (1 << (min(bd, 10) - 5)) - 1
+    row = np.arange(nctu) // (w // ctu)
+    edge_row = (row == 0) | (row == h // ctu - 1)
+    for c in range(3 if cf else 1):
+        r = rng.random(nctu)
+        band = r < sao_prob / 2
+        edge = (r >= sao_prob / 2) & (r <= sao_prob)
+        eo = rng.integers(0, 4, nctu)
+        if not sao_class3_on_edges:
+            eo = np.where((eo == 3) & edge_row, 2, eo)
+        o = rng.integers(0, omax + 1, (nctu, 4))
+        ob = rng.integers(-omax, omax + 1, (nctu, 4))
+        s = ctus["sao"][:, c]
+        s["type"] = np.where(band, 1, np.where(edge, 2, 0))
+        s["band_or_class"] = np.where(band, rng.integers(0, 32, nctu), np.where(edge, eo, 0))
+        s["offsets"] = np.where(band[:, None], ob,
+                                np.where(edge[:, None], o * np.array([1, 1, -1, -1]), 0))
+        ctus["sao"][:, c] = s
+    ctus["alf_luma"] = rng.random(nctu) < alf_prob
+    return ctus
 
 
 def synthetic_aps(rng, n_filters=25, luma_clip=True):
@@ -573,3 +583,159 @@ def random_gen_intra_reqs(width, height, n, seed=0):
         q["out_off"] = off
         off += int(q["w"]) * int(q["h"])
     return r, off
+
+
+# ------------------------------------------------------------------ encoded content --
+# The full-frame configuration decodes what the repo's own encoder makes of
+# its content: value-noise frames encoded all-intra (the reference encodes
+# every 10-bit frame as an IDR, mod.rs:1727-1802) with the frame path's
+# tools, then decoded with deblocking, SAO and ALF (SAO / ALF parameters
+# are seeded per CTU: the reference encoders never switch them on,
+# slice.rs:2611-2630).
+
+ENC_TOOLS = TOOL_ENC_FULL_INTRA | TOOL_ENC_CCLM | TOOL_DEP_QUANT | TOOL_DEBLOCK
+DEC_TOOLS = TOOL_DEP_QUANT | TOOL_DEBLOCK | TOOL_SAO | TOOL_ALF
+
+
+def chroma_qp_scaled(qp, bd):
+    """Qp'C of derived_chroma_qp_bd (hls.rs:796-802) with a zero chroma QP offset."""
+    off = 6 * (bd - 8)
+    qpi = min(63, max(-off, qp))
+    mapped = qpi if qpi <= 26 else qpi - 1
+    return min(63 + off, max(0, min(63, max(-off, mapped)) + off))
+
+
+def workload_picture(index, frames_per_qp, qps, width=1920, height=1080, bd=10, ctu_log2=5):
+    """(frame, qp, PIC_DTYPE encoder descriptor) of picture `index` of a
+    workload of frames_per_qp frames at each QP, QP-major; the coded height
+    is the CTU multiple above the visible one (mod.rs:300-324)."""
+    ctu = 1 << ctu_log2
+    frame, qp = index % frames_per_qp, qps[index // frames_per_qp]
+    p = np.zeros((), PIC_DTYPE)
+    p["width"], p["height"] = -(-width // ctu) * ctu, -(-height // ctu) * ctu
+    p["visible_width"], p["visible_height"] = width, height
+    p["bit_depth"], p["chroma_format"], p["ctu_log2"] = bd, 1, ctu_log2
+    p["slice_qp"], p["chroma_qp_scaled"] = qp, chroma_qp_scaled(qp, bd)
+    p["tools"] = ENC_TOOLS
+    p["alf_aps"] = -1
+    return frame, qp, p
+
+
+def workload_sources(frame, p, stream=0):
+    """Coded-size source planes of frame `frame` of content stream `stream`
+    (4:2:0, the picture's bit depth; edge padding below the visible rows)."""
+    w, h, vw, vh = int(p["width"]), int(p["height"]), int(p["visible_width"]), int(p["visible_height"])
+    bd = int(p["bit_depth"])
+    y, u, v = value_noise_frame(vw, vh, 10, frame=frame, stream=stream)
+    if bd != 10:
+        y, u, v = ((a.astype(np.int32) << bd >> 10).astype(np.uint16) if bd > 10 else (a >> (10 - bd))
+                   for a in (y, u, v))
+    cw, ch = chroma_dims(w, h, 1)
+    return pad_to(y, w, h), pad_to(u, cw, ch), pad_to(v, cw, ch)
+
+
+def compact_levels(p, cus, levels):
+    """The picture's coded TBs' levels in CU order (luma, Cb, Cr of each CU),
+    as a parser emits them; returns (cus with new offsets, levels)."""
+    cf = int(p["chroma_format"])
+    tb = min(1 << int(p["ctu_log2"]), 32)
+    cw, ch = chroma_dims(tb, tb, cf)
+    sizes = np.array([tb * tb, max(cw, 2) * max(ch, 2) if cf else 0, max(cw, 2) * max(ch, 2) if cf else 0])
+    cus = cus.copy()
+    lo = cus["level_off"].astype(np.int64)
+    coded = ((cus["cbf"][:, None] >> np.arange(3)) & 1).astype(bool) & (lo >= 0)
+    if not cf:
+        coded[:, 1:] = False
+    n = coded * sizes[None, :]
+    new = (np.cumsum(n.ravel()) - n.ravel()).reshape(n.shape)
+    out = np.zeros(int(n.sum()), np.int16)
+    for c in range(3):
+        k = np.nonzero(coded[:, c])[0]
+        if len(k):
+            ar = np.arange(sizes[c])[None, :]
+            out[new[k, c][:, None] + ar] = levels[lo[k, c][:, None] + ar]
+    cus["level_off"] = np.where(coded, new, -1).astype(np.int32)
+    return cus, out
+
+
+def decoder_picture(index, p_enc, cus, levels, seed):
+    """Decoder records of one encoded picture: the encoder's CUs with a
+    compact level pool, DEC_TOOLS, and per-CTU SAO / ALF parameters seeded
+    by (seed, index). Returns (pic, cus, levels, ctus)."""
+    p = np.asarray(p_enc, PIC_DTYPE).copy()
+    cus, levels = compact_levels(p, cus, levels)
+    p["tools"] = DEC_TOOLS
+    p["alf_aps"] = 0
+    ctu = 1 << int(p["ctu_log2"])
+    rng = np.random.default_rng([seed, index])
+    ctus = random_ctu_params(rng, int(p["width"]), int(p["height"]), ctu, int(p["bit_depth"]),
+                             int(p["chroma_format"]))
+    return p, cus, levels, ctus
+
+
+def workload_aps(seed):
+    """The workload's ALF APS (fixed-filter coefficient sets, seeded)."""
+    return synthetic_aps(np.random.default_rng([seed, 1 << 30]))
+
+
+def assemble(parts, aps):
+    """One batch from per-picture (pic, cus, levels, ctus) parts: offsets
+    rebased into shared record and level arrays. Returns (pics, cus, levels,
+    ctus, aps)."""
+    pics, cu_l, lv_l, ctu_l = [], [], [], []
+    n_cu = n_lv = n_ctu = 0
+    for p, cus, levels, ctus in parts:
+        p = np.asarray(p, PIC_DTYPE).copy()
+        p["cu_offset"], p["ctu_offset"] = n_cu, n_ctu
+        cus = cus.copy()
+        cus["level_off"] = np.where(cus["level_off"] >= 0, cus["level_off"] + n_lv, -1)
+        pics.append(p)
+        cu_l.append(cus)
+        lv_l.append(levels)
+        ctu_l.append(ctus)
+        n_cu += len(cus)
+        n_lv += len(levels)
+        n_ctu += len(ctus)
+    return (np.array(pics, PIC_DTYPE), np.concatenate(cu_l), np.concatenate(lv_l), np.concatenate(ctu_l),
+            aps)
+
+
+def encoded_workload(ctx, frames_per_qp, qps, seed, sources=None, width=1920, height=1080, bd=10,
+                     encode_chunk=32, stream=0):
+    """The decoder records of frames_per_qp value-noise frames at each QP,
+    encoded on the GPU by `ctx` (vvcg_encode_batch, the frame-path encoder;
+    bit-exact with the oracle's encoder). `sources` maps a frame index to its
+    coded-size planes (generated here when absent). Returns (pics, cus,
+    levels, ctus, aps) ready for Batch."""
+    n = frames_per_qp * len(qps)
+    descs = [workload_picture(i, frames_per_qp, qps, width, height, bd) for i in range(n)]
+    src = dict(sources or {})
+    for f, _, p in descs:
+        if f not in src:
+            src[f] = workload_sources(f, p, stream)
+    parts = []
+    for a in range(0, n, encode_chunk):
+        chunk = descs[a:a + encode_chunk]
+        pics = np.array([p for _, _, p in chunk], PIC_DTYPE)
+        cus, levels = ctx.encode_batch(pics, [src[f] for f, _, _ in chunk])
+        # the encoder's pictures are consecutive in its records
+        tb = min(1 << int(pics[0]["ctu_log2"]), 32)
+        at = 0
+        for j, (_, _, p) in enumerate(chunk):
+            ncu = (int(p["width"]) // tb) * (int(p["height"]) // tb)
+            parts.append(decoder_picture(a + j, p, cus[at:at + ncu], levels, seed))
+            at += ncu
+    return assemble(parts, workload_aps(seed))
+
+
+def oracle_workload_picture(oracle, index, frames_per_qp, qps, seed, width=1920, height=1080, bd=10, stream=0):
+    """The same decoder records for one picture, encoded by the oracle's
+    encoder on the CPU (for the CPU baseline, which runs without a GPU)."""
+    f, _, p = workload_picture(index, frames_per_qp, qps, width, height, bd)
+    y, u, v = workload_sources(f, p, stream)
+    t = int(p["tools"])
+    opts = ((oracle.OPT_FULL_INTRA if t & TOOL_ENC_FULL_INTRA else 0) | (oracle.OPT_CCLM if t & TOOL_ENC_CCLM else 0)
+            | (oracle.OPT_DEP_QUANT if t & TOOL_DEP_QUANT else 0) | (oracle.OPT_DEBLOCK if t & TOOL_DEBLOCK else 0))
+    cus, levels, _ = oracle.encode_frame(y, u, v, int(p["bit_depth"]), int(p["slice_qp"]), int(p["ctu_log2"]),
+                                         opts, int(p["chroma_format"]))
+    return decoder_picture(index, p, cus, levels, seed)

@@ -79,17 +79,18 @@ def test_job_throughput_counts_every_replica():
 
 
 def test_replicas_decode_different_records(pkg):
+    """Each rank encodes its own content stream (same generator, different
+    seed), so the replicas' batches differ."""
     sys.path.insert(0, ROOT)
     import bench
     import numpy as np
     from rustmpeg_next_b200 import synth
 
-    specs = [dict(width=128, height=128, bit_depth=10, chroma_format=1, ctu_log2=5, qp=27)]
-    tools = pkg.TOOL_DEBLOCK | pkg.TOOL_SAO
-    a = synth.random_records(specs, seed=bench.rank_seed(0), tools=tools)
-    b = synth.random_records(specs, seed=bench.rank_seed(1), tools=tools)
+    _, _, p = synth.workload_picture(0, 1, (27,), width=128, height=64)
+    a = synth.workload_sources(0, p, stream=0)
+    b = synth.workload_sources(0, p, stream=1)
+    assert a[0].shape == (64, 128) and not np.array_equal(a[0], b[0])
     assert bench.rank_seed(0) != bench.rank_seed(1)
-    assert not np.array_equal(a[2], b[2])
 
 
 def test_reference_arm_prints_on_rank_zero_only(capsys):
