@@ -458,7 +458,7 @@ def main():
     # per-stage times (each stage alone, same data) for the roofline
     stage_ms = {}
     for name, st in (("recon", pkg.STAGE_RECON), ("deblock", pkg.STAGE_DEBLOCK),
-                     ("sao", pkg.STAGE_SAO), ("alf", pkg.STAGE_ALF)):
+                     ("sao_alf", pkg.STAGE_SAO | pkg.STAGE_ALF)):
         for _ in range(2):
             ctx.run(st, graph=use_graph)
         stage_ms[name] = timed(lambda st=st: ctx.run(st, graph=use_graph), max(3, args.steps // 2))
@@ -518,9 +518,10 @@ def main():
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     coded = n_pics * PIX_W * CODED_H * 3 // 2
-    luma = n_pics * PIX_W * CODED_H
-    alg = {"recon": levels.nbytes + cus.nbytes + 2 * coded, "deblock": 4 * coded,
-           "sao": 4 * coded, "alf": 4 * luma}
+    # algorithmic bytes per stage: recon reads the coded TBs' levels and the
+    # records and writes every sample; deblocking reads and writes every
+    # sample; SAO (chroma) and SAO + ALF (luma, one pass) likewise
+    alg = {"recon": levels.nbytes + cus.nbytes + 2 * coded, "deblock": 4 * coded, "sao_alf": 4 * coded}
     dom = max(stage_ms, key=stage_ms.get)
     achieved = alg[dom] / (stage_ms[dom] * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak,

@@ -157,8 +157,9 @@ typedef struct vvcg_plane_out {
 enum {
   VVCG_STAGE_RECON = 1u << 0,   /* dequant + inverse transform + intra + add/clip */
   VVCG_STAGE_DEBLOCK = 1u << 1, /* pictures with VVCG_TOOL_DEBLOCK */
-  VVCG_STAGE_SAO = 1u << 2,     /* pictures with VVCG_TOOL_SAO */
-  VVCG_STAGE_ALF = 1u << 3,     /* pictures with VVCG_TOOL_ALF and an enabled CTU */
+  VVCG_STAGE_SAO = 1u << 2,     /* pictures with VVCG_TOOL_SAO; where luma ALF also applies, the
+                                   luma plane's SAO and ALF run fused in this stage */
+  VVCG_STAGE_ALF = 1u << 3,     /* luma ALF of pictures with VVCG_TOOL_ALF, an enabled CTU and no SAO */
   VVCG_STAGE_ALL = 0xFu
 };
 

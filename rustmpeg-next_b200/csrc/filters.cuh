@@ -6,6 +6,7 @@
 // apart and a segment writes at most 7 samples on each side, reading 8), so
 // each direction runs fully parallel and matches the reference's serial scan.
 #pragma once
+#include "tma.cuh"
 #include "vvcg_device.cuh"
 #include "vvcg_tables_dev.cuh"
 
@@ -569,111 +570,100 @@ struct AlfPass {
 
 constexpr int kAlfTw = 64, kAlfTh = 16, kAlfHalo = 4;
 constexpr int kAlfBlocks = (kAlfTw / 4) * (kAlfTh / 4);
+constexpr int kAlfW = kAlfTw + 2 * kAlfHalo, kAlfH = kAlfTh + 2 * kAlfHalo;  // staged tile with its halo
 
-// Tile of 64x16 outputs: the tile plus a 4-sample halo (coordinates clamped
-// to the plane, as the reference's get_p does, so reads inside the staged
-// tile need no further clamping) is staged in shared memory; a tile whose halo
-// lies inside the plane needs no clamping and is staged with 8-byte loads. Each 4x4 block is
-// classified (classify_alf_4x4_16, filter.rs:2126-2182) and its transposed
-// coefficients and clip values are formed once; then each thread filters one
-// 4-sample row of a block with the 7x7 diamond.
-__global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
-  const AlfPass& A = passes[blockIdx.z];
-  constexpr int W = kAlfTw + 2 * kAlfHalo, H = kAlfTh + 2 * kAlfHalo;
-  __shared__ __align__(16) uint16_t t[H][W];
-  __shared__ int16_t s_fc[kAlfBlocks][12];
-  __shared__ int16_t s_fcl[kAlfBlocks][12];
-  __shared__ uint8_t s_abort[kAlfBlocks];
-  const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
-  if (x0 >= A.w || y0 >= A.h) return;
-  static_assert(W % 4 == 0 && kAlfHalo % 4 == 0 && kAlfTw % 4 == 0, "8-byte staging");
-  const bool inner = x0 >= kAlfHalo && y0 >= kAlfHalo && x0 + kAlfTw + kAlfHalo <= A.w &&
-                     y0 + kAlfTh + kAlfHalo <= A.h && (A.stride & 3) == 0 &&
-                     (reinterpret_cast<uintptr_t>(A.src) & 7) == 0;
-  if (inner) {  // no clamping: 4 samples per 8-byte load
-    const uint16_t* base = A.src + (size_t)(y0 - kAlfHalo) * A.stride + (x0 - kAlfHalo);
-    for (int i = threadIdx.x; i < (W / 4) * H; i += blockDim.x) {
-      const int ty = i / (W / 4), q = i - ty * (W / 4);
-      *reinterpret_cast<uint2*>(&t[ty][4 * q]) = *reinterpret_cast<const uint2*>(base + (size_t)ty * A.stride + 4 * q);
+// Per-tile filter state of the luma ALF: each 4x4 block's transposed
+// coefficients and clip values, and whether the reference aborts on it.
+struct AlfTileWs {
+  int16_t fc[kAlfBlocks][12];
+  int16_t fcl[kAlfBlocks][12];
+  uint8_t abort[kAlfBlocks];
+};
+
+// classify_alf_4x4_16 (filter.rs:2126-2182) of the tile's 4x4 blocks and the
+// filter each block uses, for a 256-thread CTA: four threads per block, each
+// summing one of the four gradient directions over the block's 3x3
+// subsampled positions; the group then shares the sums and every thread
+// forms three of the block's twelve coefficient / clip pairs. `t` is the
+// staged tile (kAlfH x kAlfW, output (x0, y0) at (kAlfHalo, kAlfHalo),
+// positions outside the plane holding the clamped samples). Not inlined:
+// inlined, it raised the filtering kernels from 40 to 73 registers.
+__device__ __noinline__ void alf_classify_tile(const uint16_t (&t)[kAlfH][kAlfW], int x0, int y0, int w, int h, int bd,
+                                                  const vvcg_alf_aps* aps_p, AlfTileWs& ws) {
+  const int b = threadIdx.x >> 2, q = threadIdx.x & 3;
+  const int bxi = b % (kAlfTw / 4), byi = b / (kAlfTw / 4);
+  const int bx = x0 + bxi * 4, by = y0 + byi * 4;
+  // direction q: 0 horizontal, 1 vertical, 2 the 135-degree diagonal, 3 the 45-degree one
+  const int ax = q == 1 ? 0 : (q == 3 ? 1 : -1), ay = q == 0 ? 0 : -1;
+  int sum = 0;
+  for (int dy = 0; dy <= 4; dy += 2)
+    for (int dx = 0; dx <= 4; dx += 2) {
+      const int tx = bxi * 4 + dx + kAlfHalo, ty = byi * 4 + dy + kAlfHalo;
+      sum += abs(((int)t[ty][tx] << 1) - (int)t[ty + ay][tx + ax] - (int)t[ty - ay][tx - ax]);
     }
-  } else {
-    for (int i = threadIdx.x; i < W * H; i += blockDim.x) {
-      int ty = i / W, tx = i % W;
-      int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
-      t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
-    }
+  const int base = threadIdx.x & ~3 & 31;
+  const int sh = __shfl_sync(0xffffffffu, sum, base), sv = __shfl_sync(0xffffffffu, sum, base + 1);
+  const int d0 = __shfl_sync(0xffffffffu, sum, base + 2), d1 = __shfl_sync(0xffffffffu, sum, base + 3);
+  int cls = 0, tr = 0;
+  if (bx < w && by < h) {
+    long long act = ((long long)(sh + sv) * 64) >> (bd + 4);
+    // activity quantiser {0, 1, 2 x5, 3 x8, 4} of filter.rs:2163
+    const int ac = (int)(act < 0 ? 0 : (act > 15 ? 15 : act));
+    const int q_act = ac == 0 ? 0 : ac == 1 ? 1 : ac <= 6 ? 2 : ac <= 14 ? 3 : 4;
+    int hv1, hv0, dhv, dd1, dd0, ddd;
+    if (sv > sh) { hv1 = sv; hv0 = sh; dhv = 1; } else { hv1 = sh; hv0 = sv; dhv = 3; }
+    if (d0 > d1) { dd1 = d0; dd0 = d1; ddd = 0; } else { dd1 = d1; dd0 = d0; ddd = 2; }
+    int h1, h0, mdir, sdir;
+    if ((long long)dd1 * hv0 > (long long)hv1 * dd0) { h1 = dd1; h0 = dd0; mdir = ddd; sdir = dhv; }
+    else { h1 = hv1; h0 = hv0; mdir = dhv; sdir = ddd; }
+    int ds = 0;
+    if (h1 > 2 * h0) ds = (h1 * 2 > 9 * h0) ? 2 : 1;
+    // transpose index {0, 1, 0, 2, 2, 3, 1, 3}[mdir * 2 + sdir / 2], 2 bits each
+    tr = (0xDE84 >> (2 * (mdir * 2 + (sdir >> 1)))) & 3;
+    cls = q_act;
+    if (ds) cls += (((mdir & 1) << 1) + ds - 1 + 1) * 5;
+    cls = min(cls, 24);
   }
-  __syncthreads();
-  // tile coordinates of plane position (x, y) inside the staged region
+  // filter of the class: APS filter (coeff_delta_idx) or the fixed filter
+  // (the reference indexes a [16][25] table by class and aborts for >= 16)
+  const int* ct = bd >= 12 ? c_alf_clip[2] : (bd >= 10 ? c_alf_clip[1] : c_alf_clip[0]);
+  const bool aps = aps_p && aps_p->num_luma_filters > 0;
+  const int filt = aps ? min((int)aps_p->coeff_delta_idx[cls], (int)aps_p->num_luma_filters - 1) : 0;
+  const bool abort = !aps && cls >= 16;
+  const bool use_clip = aps_p && aps_p->luma_clip && filt < (int)aps_p->num_luma_filters;
+  const int fixed = abort ? 0 : c_alf_class_to_filter[cls * 25];
+#pragma unroll
+  for (int k = 3 * q; k < 3 * q + 3; k++) {
+    const int p = c_alf_transpose_perm[(tr & 3) * 12 + k];
+    ws.fc[b][k] = (int16_t)(aps ? aps_p->coeff[filt][p] : (abort ? 0 : c_alf_fixed[fixed * 13 + p]));
+    ws.fcl[b][k] = (int16_t)ct[(use_clip ? aps_p->clip_idx[filt][p] : 0) & 3];
+  }
+  if (q == 0) ws.abort[b] = abort ? 1 : 0;
+}
+
+// The 7x7 diamond (apply_alf_luma_plane_16, filter.rs:2045-2124) on the
+// staged tile after alf_classify_tile: each of the 256 threads filters one
+// 4-sample row of a block and stores it to dst.
+__device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW], int x0, int y0, int w, int h, int bd,
+                                                const AlfTileWs& ws, uint16_t* dst, int stride, uint32_t* status) {
   auto g = [&](int tx, int ty) -> int { return t[ty][tx]; };
-  const int* ct = A.bd >= 12 ? c_alf_clip[2] : (A.bd >= 10 ? c_alf_clip[1] : c_alf_clip[0]);
-  if (threadIdx.x < kAlfBlocks) {
-    const int bxi = threadIdx.x % (kAlfTw / 4), byi = threadIdx.x / (kAlfTw / 4);
-    const int bx = x0 + bxi * 4, by = y0 + byi * 4;
-    int cls = 0, tr = 0;
-    if (bx < A.w && by < A.h) {
-      int sh = 0, sv = 0, d0 = 0, d1 = 0;
-      for (int dy = 0; dy <= 4; dy += 2)
-        for (int dx = 0; dx <= 4; dx += 2) {
-          // plane positions bx + dx, by + dy and their +-1 neighbours, clamped as
-          // the staged halo is (the tile covers -4 .. +4 around the outputs)
-          const int tx = bxi * 4 + dx + kAlfHalo, ty = byi * 4 + dy + kAlfHalo;
-          const int c2 = g(tx, ty) << 1;
-          sh += abs(c2 - g(tx - 1, ty) - g(tx + 1, ty));
-          sv += abs(c2 - g(tx, ty - 1) - g(tx, ty + 1));
-          d0 += abs(c2 - g(tx - 1, ty - 1) - g(tx + 1, ty + 1));
-          d1 += abs(c2 - g(tx + 1, ty - 1) - g(tx - 1, ty + 1));
-        }
-      long long act = ((long long)(sh + sv) * 64) >> (A.bd + 4);
-      // activity quantiser {0, 1, 2 x5, 3 x8, 4} of filter.rs:2163
-      const int ac = (int)(act < 0 ? 0 : (act > 15 ? 15 : act));
-      int q_act = ac == 0 ? 0 : ac == 1 ? 1 : ac <= 6 ? 2 : ac <= 14 ? 3 : 4;
-      int hv1, hv0, dhv, dd1, dd0, ddd;
-      if (sv > sh) { hv1 = sv; hv0 = sh; dhv = 1; } else { hv1 = sh; hv0 = sv; dhv = 3; }
-      if (d0 > d1) { dd1 = d0; dd0 = d1; ddd = 0; } else { dd1 = d1; dd0 = d0; ddd = 2; }
-      int h1, h0, mdir, sdir;
-      if ((long long)dd1 * hv0 > (long long)hv1 * dd0) { h1 = dd1; h0 = dd0; mdir = ddd; sdir = dhv; }
-      else { h1 = hv1; h0 = hv0; mdir = dhv; sdir = ddd; }
-      int ds = 0;
-      if (h1 > 2 * h0) ds = (h1 * 2 > 9 * h0) ? 2 : 1;
-      // transpose index {0, 1, 0, 2, 2, 3, 1, 3}[mdir * 2 + sdir / 2], 2 bits each
-      tr = (0xDE84 >> (2 * (mdir * 2 + (sdir >> 1)))) & 3;
-      cls = q_act;
-      if (ds) cls += (((mdir & 1) << 1) + ds - 1 + 1) * 5;
-      cls = min(cls, 24);
-    }
-    // filter of the class: APS filter (coeff_delta_idx) or the fixed filter
-    // (the reference indexes a [16][25] table by class and aborts for >= 16)
-    const bool aps = A.aps && A.aps->num_luma_filters > 0;
-    const int filt = aps ? min((int)A.aps->coeff_delta_idx[cls], (int)A.aps->num_luma_filters - 1) : 0;
-    const bool abort = !aps && cls >= 16;
-    const bool use_clip = A.aps && A.aps->luma_clip && filt < (int)A.aps->num_luma_filters;
-    const int fixed = abort ? 0 : c_alf_class_to_filter[cls * 25];
-    for (int k = 0; k < 12; k++) {
-      const int p = c_alf_transpose_perm[(tr & 3) * 12 + k];
-      s_fc[threadIdx.x][k] = (int16_t)(aps ? A.aps->coeff[filt][p] : (abort ? 0 : c_alf_fixed[fixed * 13 + p]));
-      s_fcl[threadIdx.x][k] = (int16_t)ct[(use_clip ? A.aps->clip_idx[filt][p] : 0) & 3];
-    }
-    s_abort[threadIdx.x] = abort ? 1 : 0;
-  }
-  __syncthreads();
   const int b = threadIdx.x >> 2, r = threadIdx.x & 3;
   const int bxi = b % (kAlfTw / 4), byi = b / (kAlfTw / 4);
   const int x = x0 + bxi * 4, y = y0 + byi * 4 + r;
-  if (x >= A.w || y >= A.h) return;
+  if (x >= w || y >= h) return;
   const int tx0 = bxi * 4 + kAlfHalo, ty = byi * 4 + r + kAlfHalo;
   int out[4];
-  if (s_abort[b]) {
+  if (ws.abort[b]) {
     atomicOr(status, kStatusAlfAbort);
     for (int i = 0; i < 4; i++) out[i] = g(tx0 + i, ty);
   } else {
     int fc[12], fcl[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) {
-      fc[k] = s_fc[b][k];
-      fcl[k] = s_fcl[b][k];
+      fc[k] = ws.fc[b][k];
+      fcl[k] = ws.fcl[b][k];
     }
-    const int maxv = (1 << A.bd) - 1;
+    const int maxv = (1 << bd) - 1;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int tx = tx0 + i;
@@ -695,8 +685,149 @@ __global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ pa
       out[i] = clampi(c + ((s + 64) >> 7), 0, maxv);
     }
   }
-  *reinterpret_cast<uint2*>(A.dst + (size_t)y * A.stride + x) =
+  *reinterpret_cast<uint2*>(dst + (size_t)y * stride + x) =
       make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
+}
+
+// Tile of 64x16 outputs: the tile plus a 4-sample halo (coordinates clamped
+// to the plane, as the reference's get_p does, so reads inside the staged
+// tile need no further clamping) is staged in shared memory; a tile whose
+// halo lies inside the plane needs no clamping and is staged with 8-byte
+// loads. Then the blocks are classified and filtered (alf_classify_tile,
+// alf_filter_tile).
+__global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
+  const AlfPass& A = passes[blockIdx.z];
+  __shared__ __align__(16) uint16_t t[kAlfH][kAlfW];
+  __shared__ AlfTileWs ws;
+  const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
+  if (x0 >= A.w || y0 >= A.h) return;
+  static_assert(kAlfW % 4 == 0 && kAlfHalo % 4 == 0 && kAlfTw % 4 == 0, "8-byte staging");
+  const bool inner = x0 >= kAlfHalo && y0 >= kAlfHalo && x0 + kAlfTw + kAlfHalo <= A.w &&
+                     y0 + kAlfTh + kAlfHalo <= A.h && (A.stride & 3) == 0 &&
+                     (reinterpret_cast<uintptr_t>(A.src) & 7) == 0;
+  if (inner) {  // no clamping: 4 samples per 8-byte load
+    const uint16_t* base = A.src + (size_t)(y0 - kAlfHalo) * A.stride + (x0 - kAlfHalo);
+    for (int i = threadIdx.x; i < (kAlfW / 4) * kAlfH; i += blockDim.x) {
+      const int ty = i / (kAlfW / 4), q = i - ty * (kAlfW / 4);
+      *reinterpret_cast<uint2*>(&t[ty][4 * q]) = *reinterpret_cast<const uint2*>(base + (size_t)ty * A.stride + 4 * q);
+    }
+  } else {
+    for (int i = threadIdx.x; i < kAlfW * kAlfH; i += blockDim.x) {
+      int ty = i / kAlfW, tx = i % kAlfW;
+      int gx = clampi(x0 + tx - kAlfHalo, 0, A.w - 1), gy = clampi(y0 + ty - kAlfHalo, 0, A.h - 1);
+      t[ty][tx] = A.src[(size_t)gy * A.stride + gx];
+    }
+  }
+  __syncthreads();
+  alf_classify_tile(t, x0, y0, A.w, A.h, A.bd, A.aps, ws);
+  __syncthreads();
+  alf_filter_tile(t, x0, y0, A.w, A.h, A.bd, ws, A.dst, A.stride, status);
+}
+
+// ---------------------------------------------------------------------------
+// SAO then ALF of a luma plane in one pass per 64x16 tile (the frame path's
+// order, slice.rs:5022-5069: apply_sao_region_16 per CTU into a copy, then
+// apply_alf_luma_plane_16 over the whole SAO output). The deblocked samples
+// of the tile and a halo of 5 (SAO's neighbour plus ALF's 4) are staged in
+// shared memory, by one TMA box load for tiles whose staged region lies
+// inside the plane, else by clamped plain loads; SAO is evaluated for the
+// tile and ALF's 4-sample halo into a second shared tile (positions outside
+// the plane take the SAO output of the clamped position, which is what the
+// reference's clamped ALF reads see), and ALF filters from there. The SAO
+// output never goes to memory: luma moves 2 B in and 2 B out per sample
+// instead of 4 B each way for SAO and ALF separately.
+// ---------------------------------------------------------------------------
+struct SaoAlfPass {
+  const uint16_t* src;         // deblocked luma
+  uint16_t* dst;               // SAO + ALF output
+  const vvcg_ctu_filter* ctus;  // per-CTU SAO parameters (component 0)
+  const vvcg_alf_aps* aps;      // NULL = fixed filter of each class
+  const CUtensorMap* tmap;      // src as a tensor map with a kSaStW x kSaStH box; NULL = plain loads
+  int32_t stride, w, h, bd, ctu_log2, ctu_cols;
+};
+
+constexpr int kSaStX = 8, kSaStY = 5;                       // staged origin: (x0 - 8, y0 - 5)
+constexpr int kSaStW = kAlfTw + 16, kSaStH = kAlfTh + 10;   // 80 x 26 samples (x 16-byte aligned)
+constexpr uint32_t kSaStBytes = kSaStW * kSaStH * 2;
+
+// SAO output of the deblocked sample at plane position (gx, gy), from the
+// staged tile `d` whose element [0][0] is plane position (ox, oy); same
+// rules as k_sao (apply_sao_region_16, filter.rs:1880-1947).
+__device__ __forceinline__ int sao_at(const uint16_t (*d)[kSaStW], int ox, int oy, int gx, int gy,
+                                      const SaoAlfPass& S, bool& abort) {
+  const int c = d[gy - oy][gx - ox];
+  const vvcg_sao sp = S.ctus[(gy >> S.ctu_log2) * S.ctu_cols + (gx >> S.ctu_log2)].sao[0];
+  if (sp.type == 1) {
+    const int band = ((uint8_t)((uint8_t)(c >> (S.bd - 5)) - sp.band_or_class)) & 31;
+    if (band < 4) {
+      const int off = band == 0 ? sp.offsets[0] : band == 1 ? sp.offsets[1] : band == 2 ? sp.offsets[2] : sp.offsets[3];
+      return clampi(c + off, 0, (1 << S.bd) - 1);
+    }
+  } else if (sp.type == 2) {
+    const int cls = sp.band_or_class & 3;
+    const int dx = cls == 1 ? 0 : 1, dy = cls == 0 ? 0 : (cls == 3 ? -1 : 1);
+    const bool xin = !(gx - dx < 0 || gx + dx >= S.w);
+    const int ya = gy - dy, yb = gy + dy;
+    if (dy == -1 && xin && (gy == 0 || gy == S.h - 1)) {
+      abort = true;
+    } else if (xin && ya >= 0 && ya < S.h && yb >= 0 && yb < S.h) {
+      const int av = d[ya - oy][gx - dx - ox], bv = d[yb - oy][gx + dx - ox];
+      const int ei = 2 + ((c > av) - (c < av)) + ((c > bv) - (c < bv));
+      const int off = ei == 0 ? sp.offsets[0] : ei == 1 ? sp.offsets[1] : ei == 3 ? sp.offsets[2]
+                      : ei == 4 ? sp.offsets[3] : 0;
+      return clampi(c + off, 0, (1 << S.bd) - 1);
+    }
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(256) k_sao_alf_luma(const SaoAlfPass* __restrict__ passes, uint32_t spin_limit,
+                                                      uint32_t* status) {
+  const SaoAlfPass& S = passes[blockIdx.z];
+  __shared__ __align__(128) uint16_t d[kSaStH][kSaStW];
+  __shared__ __align__(16) uint16_t t[kAlfH][kAlfW];
+  __shared__ AlfTileWs ws;
+  __shared__ __align__(8) uint64_t mbar;
+  const int x0 = blockIdx.x * kAlfTw, y0 = blockIdx.y * kAlfTh;
+  if (x0 >= S.w || y0 >= S.h) return;
+  const int ox = x0 - kSaStX, oy = y0 - kSaStY;
+  const bool boxed = S.tmap && ox >= 0 && oy >= 0 && ox + kSaStW <= S.w && oy + kSaStH <= S.h;
+  if (boxed) {
+    if (threadIdx.x == 0) {
+      mbar_init(&mbar, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tma_acquire_map(S.tmap);
+      mbar_expect_tx(&mbar, kSaStBytes);
+      tma_load_2d(&d[0][0], S.tmap, ox, oy, &mbar);
+    }
+    // bounded wait; a copy that never lands voids the batch (status) and the
+    // wait goes on, again bounded, so the CTA does not leave with it in flight
+    if (!mbar_wait(&mbar, 0, spin_limit)) {
+      atomicOr(status, kStatusTimeout);
+      mbar_wait(&mbar, 0, spin_limit);
+    }
+  } else {
+    for (int i = threadIdx.x; i < kSaStW * kSaStH; i += blockDim.x) {
+      const int ty = i / kSaStW, tx = i - ty * kSaStW;
+      d[ty][tx] = S.src[(size_t)clampi(oy + ty, 0, S.h - 1) * S.stride + clampi(ox + tx, 0, S.w - 1)];
+    }
+    __syncthreads();
+  }
+  // SAO of the tile and ALF's halo, at clamped plane positions
+  bool abort = false;
+  for (int i = threadIdx.x; i < kAlfW * kAlfH; i += blockDim.x) {
+    const int ty = i / kAlfW, tx = i - ty * kAlfW;
+    const int gx = clampi(x0 - kAlfHalo + tx, 0, S.w - 1), gy = clampi(y0 - kAlfHalo + ty, 0, S.h - 1);
+    t[ty][tx] = (uint16_t)sao_at(d, ox, oy, gx, gy, S, abort);
+  }
+  if (abort) atomicOr(status, kStatusSaoAbort);
+  __syncthreads();
+  alf_classify_tile(t, x0, y0, S.w, S.h, S.bd, S.aps, ws);
+  __syncthreads();
+  alf_filter_tile(t, x0, y0, S.w, S.h, S.bd, ws, S.dst, S.stride, status);
 }
 
 #undef LP

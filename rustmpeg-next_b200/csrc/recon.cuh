@@ -4,12 +4,14 @@
 // transformed by one warp, with no dependencies between TBs; the int16
 // residual goes to the picture's scratch planes (free until SAO runs).
 //
-// k_recon_wavefront: a persistent kernel in which every warp works on its own
-// CTU. Work items are CTUs handed out by an atomic counter in wavefront order
-// (diagonal t = cx + 2*cy, across all pictures of the batch), so a warp only
-// ever waits on items that running warps already hold and the schedule cannot
-// deadlock. For each coding unit the warp waits (bounded) for the left and
-// top-right CTUs, then predicts, adds the residual, clips and stores.
+// k_recon_rows: a persistent kernel in which every warp walks one CTU row at a
+// time. Rows are handed out by an atomic counter, row-major across the
+// pictures of the batch, so a warp only ever waits on the row above, which a
+// running warp took earlier, and the schedule cannot deadlock. Before each CTU
+// the warp waits (bounded) until the row above has finished the CTU
+// above-right of it; the left neighbour is its own previous CTU. It then
+// predicts every coding unit, adds the residual, clips, stores, and publishes
+// the row's progress word.
 //
 // Follows slice::decode_vvc_frame_picture_with_chroma_qp (slice.rs:4834-4988):
 // predict_coded_block_16 / predict_cclm_with_format_16 prediction (intra.cuh),

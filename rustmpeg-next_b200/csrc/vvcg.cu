@@ -113,10 +113,12 @@ struct vvcg_ctx {
   std::vector<DbfPass> dbf[4];  // luma V, luma H, chroma V, chroma H
   std::vector<SaoPass> sao;
   std::vector<AlfPass> alf;
+  std::vector<SaoAlfPass> sao_alf;  // luma SAO + ALF in one pass (pictures with both)
+  std::vector<CUtensorMap> tmaps;   // one per sao_alf pass: its deblocked luma plane
   uint64_t num_cus = 0, num_levels = 0, num_ctus = 0, num_aps = 0;
   // device memory
-  DevBuf planes, flags, d_pics, d_items, d_dbf[4], d_sao, d_alf, d_cus, d_levels, d_ctus, d_aps,
-      d_ctrl;  // d_ctrl: [0] queue counter, [1] status word
+  DevBuf planes, flags, d_pics, d_items, d_dbf[4], d_sao, d_alf, d_sao_alf, d_tmaps, d_cus, d_levels, d_ctus,
+      d_aps, d_ctrl;  // d_ctrl: [0] queue counter, [1] status word
   // transform-unit batches; tu_pick[forward][size bin] indexes the bin's CTA
   // widths (kTuTable), chosen by vvcg_tu_autotune (default: the middle one)
   std::vector<uint32_t> tu_idx;
@@ -147,6 +149,39 @@ namespace {
 
 std::mutex g_tables_mu;
 bool g_tables_ready[64] = {false};
+
+// cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
+// link-time dependency on libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return (EncodeTiledFn)p;
+  }();
+  return fn;
+}
+
+// Tensor map of a w x h plane of 16-bit samples (row pitch `stride` samples,
+// a multiple of 8) whose loads copy box_w x box_h samples; false when the
+// driver has no encoder or rejects the plane.
+bool plane_tensor_map(CUtensorMap* m, void* base, int w, int h, int stride, int box_w, int box_h) {
+  EncodeTiledFn enc = encode_tiled_fn();
+  if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) || (stride & 7)) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)w, (cuuint64_t)h};
+  const cuuint64_t strides[1] = {(cuuint64_t)stride * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)box_h};
+  const cuuint32_t elem[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
 
 vvcg_status fail(vvcg_ctx* ctx, vvcg_status st, const char* fmt, ...) {
   if (ctx) {
@@ -397,7 +432,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   ctx->stage.release();
   ctx->stage_cus.release();
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
-                    &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf,
+                    &ctx->d_dbf[1], &ctx->d_dbf[2], &ctx->d_dbf[3], &ctx->d_sao, &ctx->d_alf, &ctx->d_sao_alf, &ctx->d_tmaps,
                     &ctx->d_cus, &ctx->d_levels, &ctx->d_ctus, &ctx->d_aps, &ctx->d_ctrl,
                     &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs, &ctx->d_alfp, &ctx->d_alfc,
                     &ctx->d_search_reqs, &ctx->d_search_cost, &ctx->d_search_mode, &ctx->d_search_ctus,
@@ -445,6 +480,8 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   for (auto& v : ctx->dbf) v.clear();
   ctx->sao.clear();
   ctx->alf.clear();
+  ctx->sao_alf.clear();
+  ctx->tmaps.clear();
   ctx->num_cus = b->num_cus;
   ctx->num_levels = b->num_levels;
   ctx->num_ctus = b->num_ctus;
@@ -602,34 +639,49 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
         }
       }
     }
-    bool sao_ran = false;
-    if (d.tools & VVCG_TOOL_SAO) {
-      sao_ran = true;
-      for (int c = 0; c < ncomp; c++) {
+    bool alf_any = false;
+    if (d.tools & VVCG_TOOL_ALF)
+      for (uint64_t k = 0; k < (uint64_t)P.ctu_w * P.ctu_h; k++) alf_any |= b->ctus[d.ctu_offset + k].alf_luma != 0;
+    const bool sao = (d.tools & VVCG_TOOL_SAO) != 0;
+    const vvcg_alf_aps* aps_dev = d.alf_aps >= 0 ? (const vvcg_alf_aps*)ctx->d_aps.p + d.alf_aps : nullptr;
+    if (sao && alf_any) {
+      // luma: SAO and ALF in one pass (slice.rs:5022-5069 order), deblocked
+      // plane -> scratch; the tensor map is fixed up once the maps' device
+      // copy exists (a null map means plain loads)
+      CUtensorMap m;
+      const bool ok = plane_tensor_map(&m, P.plane[0], P.pw[0], P.ph[0], P.stride[0], kSaStW, kSaStH);
+      if (!ok) memset(&m, 0, sizeof(m));
+      SaoAlfPass f{P.plane[0], P.scratch[0], P.ctus, aps_dev, ok ? reinterpret_cast<const CUtensorMap*>(1) : nullptr,
+                   P.stride[0], P.pw[0], P.ph[0], P.bd, ilog2_host(P.ctu), P.ctu_w};
+      ctx->sao_alf.push_back(f);
+      ctx->tmaps.push_back(m);
+      L.final_in_scratch[0] = 1;
+    }
+    if (sao) {
+      for (int c = (alf_any ? 1 : 0); c < ncomp; c++) {
         SaoPass s{P.plane[c], P.scratch[c], P.ctus, P.stride[c], P.pw[c], P.ph[c], P.bd, c,
                   ilog2_host(c ? P.ctu / P.sub_w : P.ctu), ilog2_host(c ? P.ctu / P.sub_h : P.ctu), P.ctu_w,
                   (uint32_t)(((1ull << 32) + (uint64_t)P.ctu_w - 1) / (uint64_t)P.ctu_w)};
         ctx->sao.push_back(s);
         L.final_in_scratch[c] = 1;
       }
+    } else if (alf_any) {
+      AlfPass a{P.plane[0], P.scratch[0], aps_dev, P.stride[0], P.pw[0], P.ph[0], P.bd};
+      ctx->alf.push_back(a);
+      L.final_in_scratch[0] = 1;
     }
-    if (d.tools & VVCG_TOOL_ALF) {
-      bool any = false;
-      for (uint64_t k = 0; k < (uint64_t)P.ctu_w * P.ctu_h; k++) any |= b->ctus[d.ctu_offset + k].alf_luma != 0;
-      if (any) {
-        AlfPass a{sao_ran ? P.scratch[0] : P.plane[0], sao_ran ? P.plane[0] : P.scratch[0],
-                  d.alf_aps >= 0 ? (const vvcg_alf_aps*)ctx->d_aps.p + d.alf_aps : nullptr,
-                  P.stride[0], P.pw[0], P.ph[0], P.bd};
-        ctx->alf.push_back(a);
-        L.final_in_scratch[0] = sao_ran ? 0 : 1;
-      }
-    }
+  }
+  if (!ctx->tmaps.empty()) {
+    CK(ctx->d_tmaps.reserve(sizeof(CUtensorMap) * ctx->tmaps.size()), "cudaMalloc");
+    for (size_t i = 0; i < ctx->sao_alf.size(); i++)
+      if (ctx->sao_alf[i].tmap) ctx->sao_alf[i].tmap = (const CUtensorMap*)ctx->d_tmaps.p + i;
   }
   // pinned staging for the uploads below (and one more picture table, which
   // the encoder uploads again)
   {
     size_t need = 2 * (sizeof(DevPic) * ctx->pics.size() + 256) + sizeof(RowItem) * ctx->items.size() + 256 +
-                  sizeof(SaoPass) * ctx->sao.size() + 256 + sizeof(AlfPass) * ctx->alf.size() + 256;
+                  sizeof(SaoPass) * ctx->sao.size() + 256 + sizeof(AlfPass) * ctx->alf.size() + 256 +
+                  sizeof(SaoAlfPass) * ctx->sao_alf.size() + 256 + sizeof(CUtensorMap) * ctx->tmaps.size() + 256;
     for (int k = 0; k < 4; k++) need += sizeof(DbfPass) * ctx->dbf[k].size() + 256;
     CK(ctx->stage.reserve(need), "cudaHostAlloc");
   }
@@ -640,6 +692,8 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     if ((st = upload_vec(ctx, ctx->d_dbf[k], ctx->dbf[k])) != VVCG_OK) return st;
   if ((st = upload_vec(ctx, ctx->d_sao, ctx->sao)) != VVCG_OK) return st;
   if ((st = upload_vec(ctx, ctx->d_alf, ctx->alf)) != VVCG_OK) return st;
+  if ((st = upload_vec(ctx, ctx->d_tmaps, ctx->tmaps)) != VVCG_OK) return st;
+  if ((st = upload_vec(ctx, ctx->d_sao_alf, ctx->sao_alf)) != VVCG_OK) return st;
   // no wait here: the copies read pinned staging (or pageable memory the
   // driver has already staged), and the next prepare waits for the stream
   // before it reuses the staging buffer
@@ -728,6 +782,18 @@ vvcg_status enqueue_run(vvcg_ctx* ctx, uint32_t mask, uint32_t epoch, bool clear
     k_sao<<<dim3((unsigned)((items + 7) / 8), (unsigned)ctx->sao.size()), 256, 0, ctx->stream>>>(
         (const SaoPass*)ctx->d_sao.p, ctrl + 1);
     CK(cudaGetLastError(), "sao launch");
+    (*launches)++;
+  }
+  if ((mask & VVCG_STAGE_SAO) && !ctx->sao_alf.empty()) {
+    // luma SAO + ALF of the pictures that use both (part of the SAO stage)
+    uint32_t gx = 0, gy = 0;
+    for (auto& a : ctx->sao_alf) {
+      gx = std::max<uint32_t>(gx, (a.w + kAlfTw - 1) / kAlfTw);
+      gy = std::max<uint32_t>(gy, (a.h + kAlfTh - 1) / kAlfTh);
+    }
+    k_sao_alf_luma<<<dim3(gx, gy, (unsigned)ctx->sao_alf.size()), 256, 0, ctx->stream>>>(
+        (const SaoAlfPass*)ctx->d_sao_alf.p, ctx->spin_limit, ctrl + 1);
+    CK(cudaGetLastError(), "sao+alf launch");
     (*launches)++;
   }
   if ((mask & VVCG_STAGE_ALF) && !ctx->alf.empty()) {
