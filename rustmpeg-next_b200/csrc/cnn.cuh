@@ -362,8 +362,11 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
         const float pj = __expf(lg[base + j] - mx) / se;
         dlog[base + j] = (pj - (j == label ? 1.0f : 0.0f)) * A.inv_batch;
       }
-      if (lane == 0) atomicAdd(&part[kCnnParams], (logf(se) + mx - lg[base + label]) * A.inv_batch);
+      if (lane == 0) dlog[kCnnOut + warp] = (logf(se) + mx - lg[base + label]) * A.inv_batch;
     }
+    __syncthreads();
+    // the two heads' losses, added in a fixed order (training is deterministic)
+    if (t == 0) part[kCnnParams] += dlog[kCnnOut] + dlog[kCnnOut + 1];
     const float inv = 1.0f / (float)A.maxv;
     const int bx = (int)ux, by = (int)uy;
     for (int i = t; i < 1024; i += kCnnThreads)
@@ -401,8 +404,19 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
         }
         *(uint4*)(P + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = make_uint4(o[0], o[1], o[2], o[3]);
       }
-      // the 64 threads with the same g hold that plane's sums
-      for (int k = 0; k < 8; k++) atomicAdd(&part[cnn_off_b(4) + (t & 3) * 8 + k], dbs[k]);
+      // the 64 threads with the same g hold that plane's sums: reduced over
+      // the warp's lanes of equal g, then over the warps in a fixed order
+      for (int k = 0; k < 8; k++) {
+        float s2 = dbs[k];
+        for (int o2 = 4; o2 < 32; o2 <<= 1) s2 += __shfl_xor_sync(0xFFFFFFFFu, s2, o2);
+        if (lane < 4) dbp[warp * 32 + lane * 8 + k] = s2;
+      }
+      __syncthreads();
+      if (t < 32) {
+        float s2 = 0.0f;
+        for (int w2 = 0; w2 < 8; w2++) s2 += dbp[w2 * 32 + t];
+        part[cnn_off_b(4) + t] += s2;
+      }
     }
     cnn_load_act(Q, A.acts, blk, 2);
     uint8_t* dz = P;  // dZ_l

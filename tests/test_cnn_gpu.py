@@ -95,3 +95,27 @@ def test_cnn_adam_steps_reduce_the_loss(ctx, pkg):
         loss, _ = ctx.cnn_train_step(plane, 10, 37, xy, labels.cuda(), p, m, v, step, 3e-3)
         losses.append(float(loss.item()))
     assert losses[-1] < 0.7 * losses[0], losses
+
+
+def test_cnn_training_is_deterministic(ctx, pkg):
+    """Two runs of the same training steps give bit-identical losses and
+    parameters: every gradient and the loss are summed in a fixed order (no
+    floating-point atomics)."""
+    import torch
+    from rustmpeg_next_b200 import cnn
+
+    plane, xy, blocks = _blocks(512, 10, 9)
+    mean = blocks.mean(axis=(1, 2)) / 1023.0
+    labels = torch.from_numpy(np.stack([(mean * 60).astype(int) % 67, (mean * 50).astype(int) % 6],
+                                       1).astype(np.uint8)).cuda()
+    runs = []
+    for _ in range(2):
+        p = torch.from_numpy(cnn.init_params(9)).cuda()
+        m, v = torch.zeros_like(p), torch.zeros_like(p)
+        losses = []
+        for step in range(1, 11):
+            loss, _ = ctx.cnn_train_step(plane, 10, 32, xy, labels, p, m, v, step, 1e-3)
+            losses.append(float(loss.item()))
+        runs.append((losses, p.cpu().numpy()))
+    assert runs[0][0] == runs[1][0]
+    assert np.array_equal(runs[0][1], runs[1][1])
