@@ -67,7 +67,7 @@ def _frame_sources(frame, stream):
     load_pkg()
     from rustmpeg_next_b200 import synth
 
-    _, _, p = synth.workload_picture(frame, 1, QPS[:1])
+    _, _, p = synth.workload_picture(0, 1, QPS[:1])  # the workload's picture geometry
     return synth.workload_sources(frame, p, stream)
 
 

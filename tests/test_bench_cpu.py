@@ -45,3 +45,18 @@ def test_reference_arm_prints_the_contract_line():
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["cpu_baseline"]["kind"] == "port"
     assert d["e2e"] == {"value": d["value"], "unit": "Mpx/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_frame_sources_task_makes_the_workload_frame():
+    """The generator pool's task returns frame f of the rank's content stream
+    at the workload's coded size (what encoded_workload encodes)."""
+    import numpy as np
+
+    bench.load_pkg()
+    from rustmpeg_next_b200 import synth
+
+    got = bench._frame_sources(5, 1)
+    _, _, p = synth.workload_picture(5, 32, bench.QPS)
+    want = synth.workload_sources(5, p, 1)
+    assert got[0].shape == (bench.CODED_H, bench.PIX_W)
+    assert all(np.array_equal(a, b) for a, b in zip(got, want))
