@@ -816,12 +816,51 @@ __global__ void __launch_bounds__(256) k_sao_alf_luma(const SaoAlfPass* __restri
     }
     __syncthreads();
   }
-  // SAO of the tile and ALF's halo, at clamped plane positions
+  // SAO of the tile and ALF's halo
   bool abort = false;
-  for (int i = threadIdx.x; i < kAlfW * kAlfH; i += blockDim.x) {
-    const int ty = i / kAlfW, tx = i - ty * kAlfW;
-    const int gx = clampi(x0 - kAlfHalo + tx, 0, S.w - 1), gy = clampi(y0 - kAlfHalo + ty, 0, S.h - 1);
-    t[ty][tx] = (uint16_t)sao_at(d, ox, oy, gx, gy, S, abort);
+  if (boxed) {
+    // The staged region lies inside the plane with a margin, so every
+    // position and its edge-offset neighbours are in the picture and none is
+    // on the first or last row: 4 samples per thread, one CTU's parameters
+    // each (CTU widths are multiples of 4).
+    const int maxv = (1 << S.bd) - 1;
+    for (int i = threadIdx.x; i < (kAlfW / 4) * kAlfH; i += blockDim.x) {
+      const int ty = i / (kAlfW / 4), q = i - ty * (kAlfW / 4);
+      const int gx = x0 - kAlfHalo + 4 * q, gy = y0 - kAlfHalo + ty;
+      const int dx0 = gx - ox, dy0 = gy - oy;
+      int c[4];
+      unpack4(*reinterpret_cast<const uint2*>(&d[dy0][dx0]), c);
+      int out[4] = {c[0], c[1], c[2], c[3]};
+      const vvcg_sao sp = S.ctus[(gy >> S.ctu_log2) * S.ctu_cols + (gx >> S.ctu_log2)].sao[0];
+      const int o0 = sp.offsets[0], o1 = sp.offsets[1], o2 = sp.offsets[2], o3 = sp.offsets[3];
+      if (sp.type == 1) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int band = ((uint8_t)((uint8_t)(c[k] >> (S.bd - 5)) - sp.band_or_class)) & 31;
+          const int off = band == 0 ? o0 : band == 1 ? o1 : band == 2 ? o2 : o3;
+          if (band < 4) out[k] = clampi(c[k] + off, 0, maxv);
+        }
+      } else if (sp.type == 2) {
+        const int cls = sp.band_or_class & 3;
+        const int dx = cls == 1 ? 0 : 1, dy = cls == 0 ? 0 : (cls == 3 ? -1 : 1);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int av = d[dy0 - dy][dx0 + k - dx], bv = d[dy0 + dy][dx0 + k + dx];
+          const int ei = 2 + ((c[k] > av) - (c[k] < av)) + ((c[k] > bv) - (c[k] < bv));
+          const int off = ei == 0 ? o0 : ei == 1 ? o1 : ei == 3 ? o2 : ei == 4 ? o3 : 0;
+          out[k] = clampi(c[k] + off, 0, maxv);
+        }
+      }
+      *reinterpret_cast<uint2*>(&t[ty][4 * q]) =
+          make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
+    }
+  } else {
+    // at clamped plane positions, with the picture-edge rules
+    for (int i = threadIdx.x; i < kAlfW * kAlfH; i += blockDim.x) {
+      const int ty = i / kAlfW, tx = i - ty * kAlfW;
+      const int gx = clampi(x0 - kAlfHalo + tx, 0, S.w - 1), gy = clampi(y0 - kAlfHalo + ty, 0, S.h - 1);
+      t[ty][tx] = (uint16_t)sao_at(d, ox, oy, gx, gy, S, abort);
+    }
   }
   if (abort) atomicOr(status, kStatusSaoAbort);
   __syncthreads();

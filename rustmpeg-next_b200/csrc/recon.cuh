@@ -97,6 +97,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   const bool s2 = ((lw + lh) & 1) != 0;
   const int tr_shift = 15 - bd - ((lw + lh) >> 1) - (s2 ? 1 : 0);
   int maxr = -1, maxc = -1;
+  int lastpos = -1;  // dependent quantisation: largest scan position of a nonzero level
   // All of the TB's levels are fetched up front (streaming 16-byte loads, one
   // round trip), while the coefficient tile is cleared.
   uint4 buf[4];
@@ -114,10 +115,12 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   const int qp = max(4, qp_scaled);
   const int rs = 6 - (tr_shift + qp / 6);
   const int scale = c_inv_quant_scale[s2 ? 1 : 0][qp % 6];
+  const int scan_off = g_scan_off[(lw - 1) * 6 + (lh - 1)];
   auto put = [&](int i, int L) {
     int r = i >> lw, c = i & (w - 1);
     maxr = max(maxr, r);
     maxc = max(maxc, c);
+    if (dq) lastpos = max(lastpos, (int)g_scan_pos[scan_off + i]);
     int v = L;
     if (!dq) {
       long long val = (long long)L * scale;
@@ -130,6 +133,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     for (int v = 0; v < 4; v++)
       if (v < nvec) {
         uint32_t x0 = buf[v].x, x1 = buf[v].y, x2 = buf[v].z, x3 = buf[v].w;
+        if ((x0 | x1 | x2 | x3) == 0) continue;  // 8 zero levels (most of a TB)
 #pragma unroll 1
         for (int e = 0; e < 8; e++) {
           int L = (int)(int16_t)(x0 & 0xFFFFu);
@@ -152,28 +156,23 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     // split into 32 chunks; each lane composes its chunk's state transitions,
     // a warp scan of the compositions gives each chunk's entry state, then
     // every lane replays its chunk.
+    // The transitions (32040 >> ((st << 2) + ((L & 1) << 1))) & 3 are: for
+    // an even level, swap the two bits of the state (0 1 2 3 -> 0 2 1 3);
+    // for an odd one, swap and flip the high bit (-> 2 0 3 1). A chunk's
+    // composition of all 4 entry states, packed 2 bits each, therefore
+    // updates with a few bit operations per position, in one pass.
     __syncwarp();
-    const int16_t* scan = g_scan + g_scan_off[(lw - 1) * 6 + (lh - 1)];
-    const int ns = min(w, 32) * min(h, 32);
-    int last = -1;
-    for (int s = lane; s < ns; s += 32) {
-      int r = scan[s];
-      if (W.ct[(r & (w - 1)) * kTS + (r >> lw)] != 0) last = max(last, s);
-    }
-    last = __reduce_max_sync(0xffffffffu, last);
+    const int16_t* scan = g_scan + scan_off;
+    const int last = __reduce_max_sync(0xffffffffu, lastpos);
     if (last >= 0) {
       const int cs = (last + 32) >> 5;
       const int hi = last - lane * cs;
       const int lo = max(hi - cs + 1, 0);
-      uint32_t map = 0;
-      for (int st0 = 0; st0 < 4; st0++) {
-        int st = st0;
-        for (int s = hi; s >= lo; s--) {
-          int r = scan[s];
-          int L = W.ct[(r & (w - 1)) * kTS + (r >> lw)];
-          st = (32040 >> ((st << 2) + ((L & 1) << 1))) & 3;
-        }
-        map |= (uint32_t)st << (2 * st0);
+      uint32_t map = 0xE4u;  // entry state s -> field s holds s
+      for (int s = hi; s >= lo; s--) {
+        int r = scan[s];
+        int L = W.ct[(r & (w - 1)) * kTS + (r >> lw)];
+        map = (((map & 0x55u) << 1) | ((map >> 1) & 0x55u)) ^ ((L & 1) ? 0xAAu : 0u);
       }
       uint32_t pre = map;
       for (int o = 1; o < 32; o <<= 1) {
@@ -202,7 +201,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
           long long q = (long long)(2 * L + (L > 0 ? -(st >> 1) : (st >> 1)));
           *p = (int16_t)clip16((q * inv_q + add) >> rsh);
         }
-        st = (32040 >> ((st << 2) + ((L & 1) << 1))) & 3;
+        st = (((st & 1) << 1) | (st >> 1)) ^ ((L & 1) << 1);
       }
     }
   }

@@ -298,6 +298,13 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
     }
   CK(cudaMemcpyToSymbol(g_scan, scans.data(), sizeof(int16_t) * pos), "tables");
   CK(cudaMemcpyToSymbol(g_scan_off, offs, sizeof(offs)), "tables");
+  std::vector<int16_t> scan_pos(36 * 1024, 0);
+  for (int a = 1; a <= 5; a++)
+    for (int b = 1; b <= 5; b++) {
+      const int o = offs[(a - 1) * 6 + (b - 1)], n = (1 << a) * (1 << b);
+      for (int k = 0; k < n; k++) scan_pos[o + scans[o + k]] = (int16_t)k;
+    }
+  CK(cudaMemcpyToSymbol(g_scan_pos, scan_pos.data(), sizeof(int16_t) * scan_pos.size()), "tables");
   // every (log2 w, log2 h) in 0..6 for the transform-unit kernels
   std::vector<int16_t> tu_scans(kTuScanTotal, 0);
   int32_t tu_offs[49];

@@ -33,5 +33,8 @@ __device__ int8_t g_dct8_m[4][32 * 32];
 // (log2 w, log2 h) in 1..6 x 1..6, and their offsets into g_scan.
 __device__ int16_t g_scan[36 * 1024];
 __device__ int32_t g_scan_off[36];
+// Inverse of g_scan for TBs of at most 32x32: scan position of each raster
+// index (same offsets as g_scan).
+__device__ int16_t g_scan_pos[36 * 1024];
 
 }  // namespace vvcg
