@@ -803,6 +803,27 @@ vvcg_status vvcg_gen_intra_predict_dev(vvcg_ctx* ctx, const vvcg_gen_intra_state
                                        const vvcg_gen_intra_req* reqs, uint32_t num_reqs, int16_t* out,
                                        uint64_t out_count);
 
+
+/* Reconstruction of transform blocks in decode order, for blocks that read
+ * each other's samples, such as the ISP sub-partitions of a coding unit:
+ * reqs are split into groups (group_start: num_groups + 1 indices into reqs,
+ * host memory); the blocks of a group are reconstructed one after the other
+ * by one warp, different groups in parallel (groups of one call must not read
+ * each other's samples). Each block is predicted as vvcg_gen_intra_predict_dev
+ * predicts it (into pred, device, at out_off), residual (device, int16, w x h
+ * at out_off, the inverse-transformed and BDPCM-accumulated residual of
+ * vvcg_tu_inverse_batch; NULL for none) is added, the sum clipped to the bit
+ * depth and stored into the block's plane of the state, and the block marked
+ * decoded in the state's maps (luma: every 4x4 cell it touches; chroma: every
+ * sample), which the next block's reference gathering reads. The state's
+ * planes and maps are written (device memory).
+ * Replaces: reconstruct_tu (decode_general.rs:3985-4096) for each transform
+ * unit of a coding unit, in order, with mark_tu's decoded maps (:4891-4906);
+ * for ISP the loop over sub-partitions of :4009-4024. */
+vvcg_status vvcg_gen_intra_recon_dev(vvcg_ctx* ctx, const vvcg_gen_intra_state* state,
+                                     const vvcg_gen_intra_req* reqs, uint32_t num_reqs,
+                                     const uint32_t* group_start, uint32_t num_groups,
+                                     const int16_t* residual, int16_t* pred, uint64_t out_count);
 /* ---- general-decoder deblocking ------------------------------------------- */
 
 enum { VVCG_DBK_CODED = 1, VVCG_DBK_INTRA = 2, VVCG_DBK_CBF = 4 };
@@ -858,6 +879,124 @@ vvcg_status vvcg_deblock_general_dev(vvcg_ctx* ctx, uint16_t* const planes[3], c
                                      const vvcg_dbk_cell* cells, uint32_t cell_cols, uint32_t cell_rows,
                                      const vvcg_dbk_ccell* ccells, uint32_t ccell_cols, uint32_t ccell_rows,
                                      const vvcg_dbk_params* params);
+
+/* ---- inter-prediction tools (BDOF, DMVR, affine / PROF, CIIP, GPM) -------- */
+
+/* A block of the batched inter tools: w x h samples at `off` of the tool's
+ * int32 input and output arrays (row-major). */
+typedef struct vvcg_bdof_req {
+  uint16_t w, h;  /* multiples of 4 */
+  uint32_t off;
+} vvcg_bdof_req;
+
+/* BDOF of bi-predicted luma blocks: pred0 / pred1 are the two 14-bit
+ * intermediate predictions, out the 8-bit result (device, int32).
+ * Replaces: apply_bdof_luma (inter.rs:1218-1339). */
+vvcg_status vvcg_bdof_dev(vvcg_ctx* ctx, const vvcg_bdof_req* reqs, uint32_t num_reqs, const int32_t* pred0,
+                          const int32_t* pred1, int32_t* out, uint64_t count);
+
+/* A DMVR subblock: position and size (luma samples) and the bi-prediction's
+ * motion vectors [list][horizontal, vertical] (1/16 sample). */
+typedef struct vvcg_dmvr_req {
+  int32_t bx, by;
+  uint16_t dx, dy; /* at most 16 x 16 */
+  int32_t mv[2][2];
+} vvcg_dmvr_req;
+
+/* DMVR refinement of each subblock against 8-bit reference planes ref0 /
+ * ref1 (device, width x height, stride; samples outside read the nearest
+ * edge): the refined pair goes to mv_out (device, 4 int32 per request).
+ * Replaces: refine_dmvr_subblock (inter.rs:1371-1471). */
+vvcg_status vvcg_dmvr_dev(vvcg_ctx* ctx, const uint8_t* ref0, const uint8_t* ref1, uint32_t width, uint32_t height,
+                          uint32_t stride, const vvcg_dmvr_req* reqs, uint32_t num_reqs, int32_t* mv_out);
+
+/* An affine coding unit: control-point MVs [top-left, top-right,
+ * bottom-left][horizontal, vertical], size, model and prediction type. */
+typedef struct vvcg_affine_req {
+  int32_t cp[3][2];
+  uint16_t w, h;      /* multiples of 4, 8..128 */
+  uint8_t six_param;  /* 1: 6-parameter model, 0: 4-parameter */
+  uint8_t inter_dir;  /* 1 / 2 uni-prediction, 3 bi-prediction */
+  uint8_t reserved[2];
+  uint32_t sub_off;   /* first subblock MV of this CU in sub_mv (pairs) */
+} vvcg_affine_req;
+
+/* Affine subblock motion: the (w/4) x (h/4) 4x4-subblock MVs of each CU
+ * (sub_mv, device, int32 pairs from sub_off), and its PROF deltas (prof,
+ * device, 33 int32 per request: 16 horizontal, 16 vertical, 1 when PROF
+ * applies). Replaces: derive_affine_subblock_mvs (inter.rs:1502-1579). */
+vvcg_status vvcg_affine_mvs_dev(vvcg_ctx* ctx, const vvcg_affine_req* reqs, uint32_t num_reqs, int32_t* sub_mv,
+                                uint64_t sub_count, int32_t* prof);
+
+/* A PROF subblock: its 6x6 14-bit intermediate window (36 int32 at src_off),
+ * deltas (16 horizontal then 16 vertical at dmv_off), 16 outputs at out_off. */
+typedef struct vvcg_prof_req {
+  uint32_t src_off, dmv_off, out_off;
+  uint8_t bi; /* 1: keep the refined intermediate, 0: round to 8 bits */
+  uint8_t reserved[3];
+} vvcg_prof_req;
+
+/* PROF of 4x4 subblocks (device arrays). Replaces: apply_prof_4x4
+ * (inter.rs:1581-1609). */
+vvcg_status vvcg_prof_dev(vvcg_ctx* ctx, const vvcg_prof_req* reqs, uint32_t num_reqs, const int32_t* src,
+                          uint64_t src_count, const int32_t* dmv, uint64_t dmv_count, int32_t* out, uint64_t out_count);
+
+/* A CIIP block: n samples at off; whether the left / above neighbours are intra. */
+typedef struct vvcg_ciip_req {
+  uint32_t n, off;
+  uint8_t left_intra, above_intra, reserved[2];
+} vvcg_ciip_req;
+
+/* CIIP blending of inter and Planar intra predictions (device int32).
+ * Replaces: apply_ciip_blend (inter.rs:1615-1630). */
+vvcg_status vvcg_ciip_blend_dev(vvcg_ctx* ctx, const vvcg_ciip_req* reqs, uint32_t num_reqs, const int32_t* inter,
+                                const int32_t* intra, int32_t* out, uint64_t count);
+
+/* A GPM block: size in its component's samples, split direction 0..63 and
+ * the component's subsampling (0 luma, 1 for 4:2:0 chroma). */
+typedef struct vvcg_gpm_req {
+  uint16_t w, h;
+  uint8_t split_dir, scale_x, scale_y, reserved;
+  uint32_t off;
+} vvcg_gpm_req;
+
+/* GPM blending of two uni-predictions (device int32).
+ * Replaces: derive_gpm_params_table + predict_gpm_block (inter.rs:1641-1731). */
+vvcg_status vvcg_gpm_blend_dev(vvcg_ctx* ctx, const vvcg_gpm_req* reqs, uint32_t num_reqs, const int32_t* pred0,
+                               const int32_t* pred1, int32_t* out, uint64_t count);
+
+/* ---- CTU-boundary deblocking of inter pictures ---------------------------- */
+
+/* One CTU of an inter picture of the 8-bit multi-tool path as its CTU-boundary
+ * deblocking reads it (slice.rs:2319-2326, :2438-2444): mv_field[0] of the
+ * prediction unit at the CTU's top-left, top-right and bottom-left luma
+ * samples (what get_at_luma returns on the Q side of an edge, the P side of
+ * a vertical edge and the P side of a horizontal edge), and the CTU's
+ * coded-residual flags (the cbf grids). */
+typedef struct vvcg_ctu_motion {
+  int32_t mv[3][2]; /* [top-left, top-right, bottom-left][horizontal, vertical], 1/16 sample */
+  int32_t ref[3];   /* ref_idx of the same three */
+  uint8_t cbf;      /* bit0 Y, bit1 Cb, bit2 Cr */
+  uint8_t reserved[3];
+} vvcg_ctu_motion; /* 40 bytes */
+
+/* Deblocking of an 8-bit 4:2:0 inter picture in place on device planes, on
+ * CTU boundaries only: every vertical CTU boundary, then every horizontal
+ * one, each CTU-long edge with its own boundary strength
+ * (derive_boundary_strength, filter.rs:202-226, of the two CTUs' cbf of the
+ * plane and motion; not intra), SliceQpY `qp` for luma and derived_chroma_qp
+ * for chroma, maximum filter lengths of min(ctu, 32)-sample luma and
+ * ctu/2-sample chroma transforms, the P side of a horizontal chroma edge
+ * limited to 1 (CTB-row boundary). Samples are 8-bit values in 16-bit
+ * planes (the reference's u8 planes); width and height are multiples of ctu
+ * (32, 64 or 128); cells: (width/ctu) x (height/ctu) records in raster order,
+ * device memory.
+ * Replaces: the deblocking part of apply_inter_loop_filters
+ * (slice.rs:2291-2554), over deblock_luma_edge_normative (filter.rs:689) and
+ * deblock_chroma_edge_region (filter.rs:1069). */
+vvcg_status vvcg_deblock_ctu_edges_dev(vvcg_ctx* ctx, uint16_t* const planes[3], const uint32_t stride[3],
+                                       uint32_t width, uint32_t height, uint32_t ctu, uint8_t qp,
+                                       const vvcg_ctu_motion* cells);
 
 /* ---- general-decoder SAO -------------------------------------------------- */
 

@@ -114,6 +114,20 @@ def _declare(L):
     L.orc_gen_intra_predict.restype = None
     L.orc_deblock_general.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp, i, i, vp, i, i, vp]
     L.orc_deblock_general.restype = None
+    L.orc_inter_ctu_deblock.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
+    L.orc_inter_ctu_deblock.restype = None
+    L.orc_bdof.argtypes = [vp, vp, i, i, vp]
+    L.orc_bdof.restype = None
+    L.orc_dmvr.argtypes = [vp, vp, i, i, i, i, i, i, i, vp]
+    L.orc_dmvr.restype = None
+    L.orc_affine_mvs.argtypes = [vp, i, i, i, i, vp, vp, vp]
+    L.orc_affine_mvs.restype = i
+    L.orc_prof.argtypes = [vp, vp, vp, i, vp]
+    L.orc_prof.restype = None
+    L.orc_ciip.argtypes = [vp, vp, i, i, i, vp]
+    L.orc_ciip.restype = None
+    L.orc_gpm.argtypes = [vp, vp, i, i, i, i, i, vp]
+    L.orc_gpm.restype = None
     L.orc_dbk_lens.argtypes = [i, i, i, i, vp]
     L.orc_dbk_lens.restype = None
     L.orc_dbk_bs.argtypes = [i] * 11
@@ -351,6 +365,45 @@ def gen_intra_predict(y, u, v, dec_y, dec_c, bd, ctu, reqs, out_count, vert_coll
     lib().orc_gen_intra_predict(_p(y), _p(u), _p(v), y.shape[1], u.shape[1], y.shape[1], y.shape[0], _p(dy), _p(dc),
                                 bd, int(vert_collocated), ctu, _p(r), len(r), _p(out))
     return out
+
+
+def gen_intra_recon(y, u, v, dec_y, dec_c, bd, ctu, reqs, group_start, residual, out_count, vert_collocated=False):
+    """Transform blocks reconstructed in decode order, as reconstruct_tu
+    (decode_general.rs:3985-4096) does for each transform unit of a coding
+    unit (for ISP, its sub-partitions, :4009-4024): the prediction of the
+    block from the current planes and decoded maps (gen_intra_predict), plus
+    the residual (int16, w x h at out_off; None = zero), clipped to the bit
+    depth (:4087-4093) and stored, then the block marked decoded as mark_tu
+    does (:4891-4906: every 4x4 luma cell it touches, every chroma sample).
+    Groups are processed one after another. Returns the new (y, u, v, dec_y,
+    dec_c) and the predictions."""
+    planes = [_u16(p).copy() for p in (y, u, v)]
+    dy = np.ascontiguousarray(dec_y, dtype=np.uint8).copy()
+    dc = np.ascontiguousarray(dec_c, dtype=np.uint8).copy()
+    reqs = np.ascontiguousarray(reqs)
+    pred = np.zeros(out_count, np.int16)
+    maxv = (1 << bd) - 1
+    h_pic, w_pic = planes[0].shape
+    for g in range(len(group_start) - 1):
+        for q in range(int(group_start[g]), int(group_start[g + 1])):
+            r = reqs[q:q + 1]
+            w, h, x0, y0, comp = int(r["w"][0]), int(r["h"][0]), int(r["x"][0]), int(r["y"][0]), int(r["comp"][0])
+            off = int(r["out_off"][0])
+            one = r.copy()
+            one["out_off"] = 0
+            p = gen_intra_predict(planes[0], planes[1], planes[2], dy, dc, bd, ctu, one, w * h,
+                                  vert_collocated)[:w * h].astype(np.int32)
+            pred[off:off + w * h] = p
+            res = np.zeros(w * h, np.int32) if residual is None else residual[off:off + w * h].astype(np.int32)
+            planes[comp][y0:y0 + h, x0:x0 + w] = np.clip(p + res, 0, maxv).reshape(h, w).astype(np.uint16)
+            if comp == 0:
+                cw = w_pic // 4
+                rows = slice(y0 // 4, min((y0 + h + 3) // 4, h_pic // 4))
+                cols = slice(x0 // 4, min((x0 + w + 3) // 4, cw))
+                dy.reshape(-1, cw)[rows, cols] = 1
+            else:
+                dc.reshape(-1, w_pic // 2)[y0:y0 + h, x0:x0 + w] = 1
+    return planes[0], planes[1], planes[2], dy, dc, pred
 
 
 def choose_intra_mode(recon, src, bd, bx, by, w, h):
@@ -667,6 +720,77 @@ def deblock_general(planes, vis_w, vis_h, bd, ctu, cells, ccells, params):
     lib().orc_deblock_general(_p(y), _p(u), _p(v), y.shape[1], u.shape[1], vis_w, vis_h, bd, ctu, _p(c),
                               c.shape[1], c.shape[0], _p(cc), cc.shape[1], cc.shape[0], _p(prm))
     return y, u, v
+
+
+CTU_MOTION_DTYPE = np.dtype([("mv", "<i4", (3, 2)), ("ref", "<i4", (3,)), ("cbf", "u1"), ("reserved", "u1", (3,))])
+assert CTU_MOTION_DTYPE.itemsize == 40
+
+
+def inter_ctu_deblock(planes, ctu, qp, cells):
+    """The deblocking part of apply_inter_loop_filters (slice.rs:2291-2554)
+    on an 8-bit 4:2:0 picture: returns filtered copies of the (Y, Cb, Cr)
+    planes. cells: (height/ctu, width/ctu) CTU_MOTION_DTYPE records."""
+    y, u, v = (_u16(p).copy() for p in planes)
+    c = np.ascontiguousarray(cells, dtype=CTU_MOTION_DTYPE)
+    h, w = y.shape
+    assert c.shape == (h // ctu, w // ctu)
+    lib().orc_inter_ctu_deblock(_p(y), _p(u), _p(v), y.shape[1], u.shape[1], w, h, ctu, qp, _p(c))
+    return y, u, v
+
+
+def _i32c(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def bdof(pred0, pred1, w, h):
+    """apply_bdof_luma (inter.rs:1218-1339): w x h 14-bit predictions -> 8-bit samples."""
+    a, b = _i32c(pred0), _i32c(pred1)
+    out = np.zeros(w * h, np.int32)
+    lib().orc_bdof(_p(a), _p(b), w, h, _p(out))
+    return out
+
+
+def dmvr(ref0, ref1, bx, by, dx, dy, mv):
+    """refine_dmvr_subblock (inter.rs:1371-1471) on 8-bit planes; mv =
+    (mv0 hor, mv0 ver, mv1 hor, mv1 ver); returns the refined four."""
+    r0, r1 = np.ascontiguousarray(ref0, dtype=np.uint8), np.ascontiguousarray(ref1, dtype=np.uint8)
+    m = _i32c(mv).copy()
+    lib().orc_dmvr(_p(r0), _p(r1), r0.shape[1], r0.shape[0], r0.shape[1], bx, by, dx, dy, _p(m))
+    return m
+
+
+def affine_mvs(cp, six_param, w, h, inter_dir):
+    """derive_affine_subblock_mvs (inter.rs:1502-1579): (subblock MVs
+    (n, 2), PROF horizontal deltas (16,), vertical (16,), PROF enabled)."""
+    c = _i32c(cp).reshape(6)
+    sub = np.zeros(2 * (w // 4) * (h // 4), np.int32)
+    ph, pv = np.zeros(16, np.int32), np.zeros(16, np.int32)
+    en = lib().orc_affine_mvs(_p(c), int(six_param), w, h, inter_dir, _p(sub), _p(ph), _p(pv))
+    return sub.reshape(-1, 2), ph, pv, bool(en)
+
+
+def prof(src6x6, dmv_x, dmv_y, bi):
+    """apply_prof_4x4 (inter.rs:1581-1609)."""
+    s, x, y = _i32c(src6x6), _i32c(dmv_x), _i32c(dmv_y)
+    out = np.zeros(16, np.int32)
+    lib().orc_prof(_p(s), _p(x), _p(y), int(bi), _p(out))
+    return out
+
+
+def ciip(inter, intra, left_intra, above_intra):
+    """apply_ciip_blend (inter.rs:1615-1630)."""
+    a, b = _i32c(inter), _i32c(intra)
+    out = np.zeros(a.size, np.int32)
+    lib().orc_ciip(_p(a), _p(b), a.size, int(left_intra), int(above_intra), _p(out))
+    return out
+
+
+def gpm(pred0, pred1, w, h, split_dir, scale_x=0, scale_y=0):
+    """predict_gpm_block (inter.rs:1673-1731)."""
+    a, b = _i32c(pred0), _i32c(pred1)
+    out = np.zeros(w * h, np.int32)
+    lib().orc_gpm(_p(a), _p(b), w, h, split_dir, scale_x, scale_y, _p(out))
+    return out
 
 
 def dbk_lens(luma, size_p, size_q, ctb_boundary=False):

@@ -151,6 +151,8 @@ void dbk_chroma_lens(int size_p, int size_q, bool ctb_boundary, int* lp, int* lq
 int dbk_boundary_strength(bool p_intra, bool q_intra, bool p_cbf, bool q_cbf, bool tu_edge, int pmv_h,
                           int pmv_v, int qmv_h, int qmv_v, int pref, int qref);
 // decode_general.rs:4977-5187 apply_deblock on a 4:2:0 picture, in place.
+void inter_ctu_deblock(uint16_t* const planes[3], const int stride[3], int w, int h, int ctu, int qp,
+                       const vvcg_ctu_motion* cells);
 void deblock_general(uint16_t* const planes[3], const int stride[3], int vis_w, int vis_h, int bd, int ctu,
                      const vvcg_dbk_cell* cells, int cols, int rows, const vvcg_dbk_ccell* cc, int ccols,
                      int crows, const vvcg_dbk_params& prm);

@@ -258,6 +258,13 @@ extern "C" void orc_predict_luma_8(const uint8_t* recon, int pw, int ph, int bx,
 }
 // planes row-major with strides (samples); cells / ccells / params in the
 // vvcg_dbk_cell / vvcg_dbk_ccell / vvcg_dbk_params layouts
+extern "C" void orc_inter_ctu_deblock(uint16_t* y, uint16_t* u, uint16_t* v, int sy, int sc, int w, int h, int ctu,
+                                      int qp, const vvcg_ctu_motion* cells) {
+  uint16_t* const planes[3] = {y, u, v};
+  const int stride[3] = {sy, sc, sc};
+  orc::inter_ctu_deblock(planes, stride, w, h, ctu, qp, cells);
+}
+
 extern "C" void orc_deblock_general(uint16_t* y, uint16_t* u, uint16_t* v, int sy, int sc, int vis_w, int vis_h,
                                     int bd, int ctu, const vvcg_dbk_cell* cells, int cols, int rows,
                                     const vvcg_dbk_ccell* cc, int ccols, int crows, const vvcg_dbk_params* prm) {

@@ -397,6 +397,97 @@ int dbk_boundary_strength(bool p_intra, bool q_intra, bool p_cbf, bool q_cbf, bo
   return 0;
 }
 
+// slice.rs:2291-2554 apply_inter_loop_filters, its deblocking part: CTU
+// boundaries of an 8-bit 4:2:0 inter picture, vertical then horizontal, with
+// a per-edge bS from the two CTUs' cbf and motion (8-bit samples in 16-bit
+// planes; the reference clamps to 0..255).
+void inter_ctu_deblock(uint16_t* const planes[3], const int stride[3], int w, int h, int ctu, int qp,
+                       const vvcg_ctu_motion* cells) {
+  const int grid_w = w / ctu, grid_h = h / ctu;
+  const int cw = ctu / 2;
+  const int cwid = (w + 1) / 2, chei = (h + 1) / 2;
+  const int chroma_qp = clampi(derived_chroma_qp(qp), 0, 63);
+  const int luma_max_len = luma_filter_length(std::min(ctu, 32));
+  const int chroma_len = chroma_filter_length(cw);
+  auto Y = [&](int x, int y) -> uint16_t& { return planes[0][(size_t)y * stride[0] + x]; };
+  auto bs_of = [&](const vvcg_ctu_motion& p, int pk, const vvcg_ctu_motion& q, int qk, int comp) {
+    return dbk_boundary_strength(false, false, (p.cbf >> comp) & 1, (q.cbf >> comp) & 1, true, p.mv[pk][0],
+                                 p.mv[pk][1], q.mv[qk][0], q.mv[qk][1], p.ref[pk], q.ref[qk]);
+  };
+  // filter.rs:1069-1112 deblock_chroma_edge_region at bit depth 8
+  auto chroma_region = [&](int comp, bool vertical, int edge, int start, int end, int bs, int lp, int lq) {
+    uint16_t* pl = planes[comp];
+    const int st = stride[comp];
+    const int limit = vertical ? cwid : chei;
+    if (edge < 4 || edge + 4 > limit) return;
+    for (int pos = start; pos + 2 <= end; pos += 2) {
+      int lines[4][8];
+      for (int k = 0; k < 2; k++)
+        for (int i = 0; i < 8; i++) {
+          const int d = edge - 4 + i;
+          lines[k][i] = vertical ? pl[(size_t)(pos + k) * st + d] : pl[(size_t)d * st + pos + k];
+        }
+      deblock_chroma_edge(lines, 2, chroma_qp, bs, 0, 0, lp, lq, 8);
+      for (int k = 0; k < 2; k++)
+        for (int i = 0; i < 8; i++) {
+          const int d = edge - 4 + i;
+          const uint16_t v = (uint16_t)clampi(lines[k][i], 0, 255);
+          if (vertical)
+            pl[(size_t)(pos + k) * st + d] = v;
+          else
+            pl[(size_t)d * st + pos + k] = v;
+        }
+    }
+  };
+  int lines[4][16];
+  // 1. vertical CTU boundaries
+  for (int gx = 1; gx < grid_w; gx++) {
+    const int x = gx * ctu, cx = gx * cw;
+    for (int gy = 0; gy < grid_h; gy++) {
+      const vvcg_ctu_motion& P = cells[gy * grid_w + gx - 1];
+      const vvcg_ctu_motion& Q = cells[gy * grid_w + gx];
+      const int bs_y = bs_of(P, 1, Q, 0, 0);
+      if (bs_y > 0 && x >= 8 && x + 8 <= w) {
+        const int y_end = std::min((gy + 1) * ctu, h);
+        for (int y = gy * ctu; y + 4 <= y_end; y += 4) {
+          for (int dy = 0; dy < 4; dy++)
+            for (int k = 0; k < 16; k++) lines[dy][k] = Y(x - 8 + k, y + dy);
+          deblock_luma_edge_bd(lines, qp, qp, bs_y, 0, 0, 8, luma_max_len, luma_max_len, false);
+          for (int dy = 0; dy < 4; dy++)
+            for (int k = 0; k < 16; k++) Y(x - 8 + k, y + dy) = (uint16_t)clampi(lines[dy][k], 0, 255);
+        }
+      }
+      for (int c = 1; c <= 2; c++) {
+        const int bs = bs_of(P, 1, Q, 0, c);
+        if (bs > 0) chroma_region(c, true, cx, gy * cw, std::min((gy + 1) * cw, chei), bs, chroma_len, chroma_len);
+      }
+    }
+  }
+  // 2. horizontal CTU boundaries
+  for (int gy = 1; gy < grid_h; gy++) {
+    const int y = gy * ctu, cy = gy * cw;
+    for (int gx = 0; gx < grid_w; gx++) {
+      const vvcg_ctu_motion& P = cells[(gy - 1) * grid_w + gx];
+      const vvcg_ctu_motion& Q = cells[gy * grid_w + gx];
+      const int bs_y = bs_of(P, 2, Q, 0, 0);
+      if (bs_y > 0 && y >= 8 && y + 8 <= h) {
+        const int x_end = std::min((gx + 1) * ctu, w);
+        for (int bx = gx * ctu; bx + 4 <= x_end; bx += 4) {
+          for (int dx = 0; dx < 4; dx++)
+            for (int k = 0; k < 16; k++) lines[dx][k] = Y(bx + dx, y - 8 + k);
+          deblock_luma_edge_bd(lines, qp, qp, bs_y, 0, 0, 8, luma_max_len, luma_max_len, true);
+          for (int dx = 0; dx < 4; dx++)
+            for (int k = 0; k < 16; k++) Y(bx + dx, y - 8 + k) = (uint16_t)clampi(lines[dx][k], 0, 255);
+        }
+      }
+      for (int c = 1; c <= 2; c++) {
+        const int bs = bs_of(P, 2, Q, 0, c);
+        if (bs > 0) chroma_region(c, false, cy, gx * cw, std::min((gx + 1) * cw, cwid), bs, 1, chroma_len);
+      }
+    }
+  }
+}
+
 namespace {
 
 struct GenDbk {

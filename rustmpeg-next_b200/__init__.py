@@ -95,6 +95,17 @@ DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"),
 DBK_PARAMS_DTYPE = np.dtype([("qp", "<i4", (3,)), ("beta_offset_div2", "<i4", (3,)), ("tc_offset_div2", "<i4", (3,)),
                              ("num_ref", "<i4", (2,)), ("ref_poc", "<i4", (2, 16))])
 DBK_CODED, DBK_INTRA, DBK_CBF = 1, 2, 4
+CTU_MOTION_DTYPE = np.dtype([("mv", "<i4", (3, 2)), ("ref", "<i4", (3,)), ("cbf", "u1"), ("reserved", "u1", (3,))])
+BDOF_REQ_DTYPE = np.dtype([("w", "<u2"), ("h", "<u2"), ("off", "<u4")])
+DMVR_REQ_DTYPE = np.dtype([("bx", "<i4"), ("by", "<i4"), ("dx", "<u2"), ("dy", "<u2"), ("mv", "<i4", (2, 2))])
+AFFINE_REQ_DTYPE = np.dtype([("cp", "<i4", (3, 2)), ("w", "<u2"), ("h", "<u2"), ("six_param", "u1"),
+                             ("inter_dir", "u1"), ("reserved", "u1", (2,)), ("sub_off", "<u4")])
+PROF_REQ_DTYPE = np.dtype([("src_off", "<u4"), ("dmv_off", "<u4"), ("out_off", "<u4"), ("bi", "u1"),
+                           ("reserved", "u1", (3,))])
+CIIP_REQ_DTYPE = np.dtype([("n", "<u4"), ("off", "<u4"), ("left_intra", "u1"), ("above_intra", "u1"),
+                           ("reserved", "u1", (2,))])
+GPM_REQ_DTYPE = np.dtype([("w", "<u2"), ("h", "<u2"), ("split_dir", "u1"), ("scale_x", "u1"), ("scale_y", "u1"),
+                          ("reserved", "u1"), ("off", "<u4")])
 DBK_NO_TU = 0xFFFFFFFF
 MIP_REQ_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("mode", "u1"),
                           ("transposed", "u1"), ("reserved", "u1", (3,)), ("ref_off", "<u4"), ("out_off", "<u4")])
@@ -182,6 +193,9 @@ assert ISR_REQ_DTYPE.itemsize == 20 and ISR_RES_DTYPE.itemsize == 16
 assert CTU_SEARCH_REQ_DTYPE.itemsize == 16 and CTU_SEARCH_RES_DTYPE.itemsize == 36
 assert GEN_INTRA_REQ_DTYPE.itemsize == 28
 assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_PARAMS_DTYPE.itemsize == 172
+assert CTU_MOTION_DTYPE.itemsize == 40 and BDOF_REQ_DTYPE.itemsize == 8 and DMVR_REQ_DTYPE.itemsize == 28
+assert AFFINE_REQ_DTYPE.itemsize == 36 and PROF_REQ_DTYPE.itemsize == 16 and CIIP_REQ_DTYPE.itemsize == 12
+assert GPM_REQ_DTYPE.itemsize == 12
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
@@ -256,7 +270,15 @@ def lib():
         L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
                                               vp, vp, vp]
         L.vvcg_gen_intra_predict_dev.argtypes = [vp, vp, vp, u32, vp, u64]
+        L.vvcg_gen_intra_recon_dev.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, u64]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
+        L.vvcg_deblock_ctu_edges_dev.argtypes = [vp, vp, vp, u32, u32, u32, u8, vp]
+        L.vvcg_bdof_dev.argtypes = [vp, vp, u32, vp, vp, vp, u64]
+        L.vvcg_dmvr_dev.argtypes = [vp, vp, vp, u32, u32, u32, vp, u32, vp]
+        L.vvcg_affine_mvs_dev.argtypes = [vp, vp, u32, vp, u64, vp]
+        L.vvcg_prof_dev.argtypes = [vp, vp, u32, vp, u64, vp, u64, vp, u64]
+        L.vvcg_ciip_blend_dev.argtypes = [vp, vp, u32, vp, vp, vp, u64]
+        L.vvcg_gpm_blend_dev.argtypes = [vp, vp, u32, vp, vp, vp, u64]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
@@ -688,7 +710,82 @@ class Context:
         torch.cuda.synchronize(planes[0].device)
         return out
 
+    def gen_intra_recon(self, planes, dec_y, dec_c, bit_depth, ctu, reqs, group_start, residual, out_count,
+                        vert_collocated=False):
+        """Sequential reconstruction (vvcg_gen_intra_recon_dev), in place on
+        planes and the decoded maps (CUDA tensors as for gen_intra_predict).
+        group_start: num_groups + 1 request indices; residual: int16 CUDA
+        tensor of out_count samples or None. Returns the predictions
+        (synchronises)."""
+        import torch
+
+        reqs = np.ascontiguousarray(reqs, dtype=GEN_INTRA_REQ_DTYPE)
+        groups = np.ascontiguousarray(group_start, dtype=np.uint32)
+        st = _GenIntraState()
+        for c in range(3):
+            st.plane[c] = planes[c].data_ptr()
+            st.stride[c] = planes[c].stride(0)
+        st.height, st.width = planes[0].shape
+        st.dec_y, st.dec_c = dec_y.data_ptr(), dec_c.data_ptr()
+        st.bit_depth, st.vert_collocated, st.ctu_size = bit_depth, int(vert_collocated), ctu
+        pred = torch.zeros(max(out_count, 1), dtype=torch.int16, device=planes[0].device)
+        self._keep = (reqs, groups, st)
+        self._check(self._L.vvcg_gen_intra_recon_dev(self._h, C.byref(st), _ptr(reqs), len(reqs), _ptr(groups),
+                                                     len(groups) - 1, _ptr(residual), _ptr(pred), out_count))
+        torch.cuda.synchronize(planes[0].device)
+        return pred
+
+    # -- inter-prediction tools (device int32 arrays; requests are host records) --
+    def _inter_tool(self, fn, reqs, dtype, *args):
+        reqs = np.ascontiguousarray(reqs, dtype=dtype)
+        self._keep = reqs
+        self._check(fn(self._h, _ptr(reqs), len(reqs), *args))
+
+    def bdof(self, reqs, pred0, pred1, out):
+        """BDOF_REQ_DTYPE requests over int32 CUDA tensors (14-bit intermediates in, 8-bit out)."""
+        self._inter_tool(self._L.vvcg_bdof_dev, reqs, BDOF_REQ_DTYPE, _ptr(pred0), _ptr(pred1), _ptr(out), out.numel())
+
+    def dmvr(self, ref0, ref1, reqs, mv_out):
+        """ref0 / ref1: (H, W) uint8 CUDA tensors; mv_out: int32 CUDA tensor of 4 per request."""
+        h, w = ref0.shape
+        reqs = np.ascontiguousarray(reqs, dtype=DMVR_REQ_DTYPE)
+        self._keep = reqs
+        self._check(self._L.vvcg_dmvr_dev(self._h, _ptr(ref0), _ptr(ref1), w, h, ref0.stride(0), _ptr(reqs),
+                                          len(reqs), _ptr(mv_out)))
+
+    def affine_mvs(self, reqs, sub_mv, prof):
+        self._inter_tool(self._L.vvcg_affine_mvs_dev, reqs, AFFINE_REQ_DTYPE, _ptr(sub_mv), sub_mv.numel() // 2,
+                         _ptr(prof))
+
+    def prof(self, reqs, src, dmv, out):
+        self._inter_tool(self._L.vvcg_prof_dev, reqs, PROF_REQ_DTYPE, _ptr(src), src.numel(), _ptr(dmv), dmv.numel(),
+                         _ptr(out), out.numel())
+
+    def ciip_blend(self, reqs, inter, intra, out):
+        self._inter_tool(self._L.vvcg_ciip_blend_dev, reqs, CIIP_REQ_DTYPE, _ptr(inter), _ptr(intra), _ptr(out),
+                         out.numel())
+
+    def gpm_blend(self, reqs, pred0, pred1, out):
+        self._inter_tool(self._L.vvcg_gpm_blend_dev, reqs, GPM_REQ_DTYPE, _ptr(pred0), _ptr(pred1), _ptr(out),
+                         out.numel())
+
     # -- general-decoder deblocking --
+    def deblock_ctu_edges(self, planes, ctu, qp, cells):
+        """CTU-boundary deblocking of an 8-bit 4:2:0 inter picture, in place on
+        planes, (Y, Cb, Cr) int16 CUDA tensors (8-bit sample values); cells:
+        (rows, cols) CTU_MOTION_DTYPE records (numpy, uploaded here)."""
+        import torch
+
+        cells = np.ascontiguousarray(cells, dtype=CTU_MOTION_DTYPE)
+        h, w = planes[0].shape
+        if cells.shape != (h // ctu, w // ctu):
+            raise InvalidInput(f"cells are {cells.shape}; the picture needs {(h // ctu, w // ctu)}")
+        dc = torch.from_numpy(cells.view(np.uint8).reshape(-1).copy()).to(planes[0].device)
+        pp = (C.c_void_p * 3)(*[t.data_ptr() for t in planes])
+        st = (C.c_uint32 * 3)(*[t.stride(0) for t in planes])
+        self._keep = dc
+        self._check(self._L.vvcg_deblock_ctu_edges_dev(self._h, pp, st, w, h, ctu, qp, _ptr(dc)))
+
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):
         """In place on planes, (Y, Cb, Cr) int16 CUDA tensors of a 4:2:0
         picture. cells / ccells: 2-D CUDA uint8 tensors or numpy arrays of

@@ -192,7 +192,38 @@ struct DbfPass {
   int32_t len_p, len_q;  // luma: max filter length; chroma: lengths from the lattice
   int32_t sub;           // chroma: SubHeightC (vertical pass) / SubWidthC (horizontal pass)
   int32_t n_edges, n_segs;
+  // Per-edge boundary strength on a CTU lattice (step = the CTU size in this
+  // plane) instead of `bs`: cells of the CTUs (cell_cols per row), the cbf
+  // bit of this plane, and this plane's samples per CTU along an edge.
+  const vvcg_ctu_motion* cells;
+  int32_t cell_cols, comp, span;
 };
+
+// derive_boundary_strength (filter.rs:202-226) of a CTU edge of an inter
+// picture (not intra, a transform edge) between CTU cells p and q, reading
+// motion entry pk of p and qk of q (0 top-left, 1 top-right, 2 bottom-left).
+__device__ __forceinline__ int ctu_edge_bs(const vvcg_ctu_motion& p, int pk, const vvcg_ctu_motion& q, int qk,
+                                           int comp) {
+  if (((p.cbf | q.cbf) >> comp) & 1) return 1;
+  if (p.ref[pk] != q.ref[qk] || abs(p.mv[pk][0] - q.mv[qk][0]) >= 8 || abs(p.mv[pk][1] - q.mv[qk][1]) >= 8)
+    return 1;
+  return 0;
+}
+
+// Boundary strength of segment position `seg` on edge e of pass D: the
+// pass's constant, or from the CTU cells either side of a CTU-lattice edge
+// (slice.rs:2319-2334 for vertical, :2438-2452 for horizontal edges).
+template <bool kVertical>
+__device__ __forceinline__ int pass_bs(const DbfPass& D, int e, int seg) {
+  if (!D.cells) return D.bs;
+  const int along = seg / D.span;
+  if (kVertical) {
+    const vvcg_ctu_motion* row = D.cells + (size_t)along * D.cell_cols;
+    return ctu_edge_bs(row[e], 1, row[e + 1], 0, D.comp);
+  }
+  return ctu_edge_bs(D.cells[(size_t)e * D.cell_cols + along], 2, D.cells[(size_t)(e + 1) * D.cell_cols + along], 0,
+                     D.comp);
+}
 
 // deblock_luma_edge_bd (filter.rs:638-679) on the segment's 4 lines;
 // vertical edges (filter.rs:2360-2390) or horizontal edges (:2392-2425) of
@@ -207,11 +238,12 @@ __global__ void k_deblock_luma(const DbfPass* __restrict__ passes, int n_pass) {
   int seg = s * 4;
   int bd = D.bd, maxv = (1 << bd) - 1;
   int qp = D.qp;
-  int idx_tc = clampi(qp + 2 * (D.bs - 1) + 2 * D.tc_off, 0, 65);
+  const int bs = pass_bs<kVertical>(D, e, seg);
+  int idx_tc = clampi(qp + 2 * (bs - 1) + 2 * D.tc_off, 0, 65);
   int idx_b = clampi(qp + 2 * D.beta_off, 0, 63);
   int tc = tc_for(idx_tc, bd);
   int beta = c_dbf_beta[idx_b] << (bd - 8);
-  if (D.bs == 0 || beta == 0 || tc == 0) return;
+  if (bs == 0 || beta == 0 || tc == 0) return;
   int ln[4][16];
   uint16_t* pl = D.plane;
   const int st = D.stride;
@@ -341,11 +373,12 @@ __global__ void k_deblock_chroma(const DbfPass* __restrict__ passes, int n_pass)
   const int group = D.sub == 1 ? 4 : 2;
   const int seg = s * group;
   const int bd = D.bd, maxv = (1 << bd) - 1;
-  if (D.bs == 0) return;
+  const int bs = pass_bs<kVertical>(D, e, seg);
+  if (bs == 0) return;
   int len_p = min(D.len_p, 3), len_q = min(D.len_q, 3);
   if (!kVertical && (pos % D.ctb) == 0) len_p = 1;  // upper chroma CTB boundary
-  if (len_p == 1 && len_q == 1 && D.bs != 2) return;
-  int idx_tc = clampi(D.qp + 2 * (D.bs - 1) + 2 * D.tc_off, 0, 65);
+  if (len_p == 1 && len_q == 1 && bs != 2) return;
+  int idx_tc = clampi(D.qp + 2 * (bs - 1) + 2 * D.tc_off, 0, 65);
   int idx_b = clampi(D.qp + 2 * D.beta_off, 0, 63);
   int tc = tc_for(idx_tc, bd);
   int beta = c_dbf_beta[idx_b] << (bd - 8);

@@ -499,87 +499,145 @@ __device__ void gi_cclm(const vvcg_gen_intra_state& S, int comp, int mode, int x
   __syncwarp();
 }
 
+// The prediction of one request into out (w x h int16, row-major), by the
+// calling warp.
+__device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R, int16_t* out, GiWs& W) {
+  const int lane = threadIdx.x & 31;
+  const int bd = S.bit_depth;
+  if (R.comp == 0) {
+    // the 4-wide region of narrow vertical ISP sub-partitions
+    const bool region = R.isp == VVCG_ISP_VER && (R.cu_w == 4 || (R.cu_w == 8 && R.cu_h > 4));
+    const int px = region ? R.cu_x + ((R.x - R.cu_x) / 4) * 4 : R.x;
+    const int pw = region ? 4 : R.w, ph = R.h, col0 = R.x - px;
+    auto put = [&](int i, int v) {
+      const int yy = i / pw, xx = i - yy * pw - col0;
+      if (xx >= 0 && xx < R.w) out[yy * R.w + xx] = (int16_t)v;
+    };
+    if (R.bdpcm) {
+      gi_gather_len(S, 0, true, px, R.y, 2 * pw, 2 * ph, W);
+      for (int i = lane; i < pw * ph; i += 32) {
+        const int yy = i / pw, xx = i - yy * pw;
+        put(i, R.bdpcm == VVCG_BDPCM_VER ? W.above[xx] : W.left[yy]);
+      }
+      __syncwarp();
+      return;
+    }
+    const bool isp = R.isp != VVCG_ISP_NONE;
+    const int mrl = min((int)R.mrl, 2);
+    if (isp) {
+      gi_gather_len(S, 0, true, px, R.y, R.cu_w + pw, R.cu_h + ph, W);
+      gi_rows_from_refs(R.cu_w + pw, R.cu_h + ph, W);
+    } else if (mrl == 0) {
+      gi_gather_len(S, 0, true, px, R.y, 2 * pw, 2 * ph, W);
+      gi_rows_from_refs(2 * pw, 2 * ph, W);
+    } else {
+      gi_gather_mrl(S, px, R.y, pw, ph, mrl, W);
+    }
+    const int off = W.off;
+    const int mode = R.mode;
+    if (mode <= 1) {
+      const bool filt = mode == 0 && mrl == 0 && !isp && pw * ph > 32;
+      if (filt) {
+        gi_filter_into_base(W.rowa + off + 1, W.rowl + off + 1, W.rowa[off], 2 * pw, 2 * ph, W);
+      } else {
+        for (int i = lane; i < 2 * pw; i += 32) W.ba[i] = W.rowa[off + 1 + i];
+        for (int i = lane; i < 2 * ph; i += 32) W.bl[i] = W.rowl[off + 1 + i];
+        __syncwarp();
+      }
+      gi_planar_dc(mode == 0, pw, ph, mrl == 0 && pw >= 4 && ph >= 4, W, put);
+      return;
+    }
+    const GiAng P = gi_ang_params(min(mode, 66), pw, ph, R.cu_w, R.cu_h, true, mrl, isp);
+    if (mrl == 0 && !isp && P.ref_filter) {
+      // rows from the filtered base refs
+      gi_filter_into_base(W.rowa + 1, W.rowl + 1, W.rowa[0], 2 * pw, 2 * ph, W);
+      for (int i = lane; i < 2 * pw + 5; i += 32) W.rowa[i] = i == 0 ? (int16_t)W.btl : W.ba[min(i - 1, 2 * pw - 1)];
+      for (int i = lane; i < 2 * ph + 5; i += 32) W.rowl[i] = i == 0 ? (int16_t)W.btl : W.bl[min(i - 1, 2 * ph - 1)];
+      __syncwarp();
+    }
+    gi_angular(P, pw, ph, true, W.off, bd, W, put);  // the rows' reference line
+    return;
+  }
+  // chroma
+  auto put = [&](int i, int v) { out[i] = (int16_t)v; };
+  const int w = R.w, h = R.h;
+  if (R.mode >= 81 && R.mode <= 83) {
+    gi_cclm(S, R.comp, R.mode - 81, R.x, R.y, w, h, put);
+    return;
+  }
+  gi_gather_len(S, R.comp, false, R.x, R.y, 2 * w, 2 * h, W);
+  if (R.mode <= 1) {
+    for (int i = lane; i < 2 * w; i += 32) W.ba[i] = W.above[i];
+    for (int i = lane; i < 2 * h; i += 32) W.bl[i] = W.left[i];
+    __syncwarp();
+    gi_planar_dc(R.mode == 0, w, h, w >= 4 && h >= 4, W, put);
+    return;
+  }
+  gi_rows_from_refs(2 * w, 2 * h, W);
+  const GiAng P = gi_ang_params(min((int)R.mode, 66), w, h, w, h, false, 0, false);
+  gi_angular(P, w, h, false, 0, bd, W, put);
+}
+
 __global__ void __launch_bounds__(kGiWarps * 32) k_gen_intra(const __grid_constant__ GenIntraArgs A) {
   __shared__ GiWs ws[kGiWarps];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  GiWs& W = ws[warp];
-  const vvcg_gen_intra_state& S = A.st;
+  const int warp = threadIdx.x >> 5;
   for (int q = blockIdx.x * kGiWarps + warp; q < A.n; q += gridDim.x * kGiWarps) {
     const vvcg_gen_intra_req R = A.reqs[q];
-    int16_t* out = A.out + R.out_off;
-    const int bd = S.bit_depth;
-    if (R.comp == 0) {
-      // the 4-wide region of narrow vertical ISP sub-partitions
-      const bool region = R.isp == VVCG_ISP_VER && (R.cu_w == 4 || (R.cu_w == 8 && R.cu_h > 4));
-      const int px = region ? R.cu_x + ((R.x - R.cu_x) / 4) * 4 : R.x;
-      const int pw = region ? 4 : R.w, ph = R.h, col0 = R.x - px;
-      auto put = [&](int i, int v) {
-        const int yy = i / pw, xx = i - yy * pw - col0;
-        if (xx >= 0 && xx < R.w) out[yy * R.w + xx] = (int16_t)v;
-      };
-      if (R.bdpcm) {
-        gi_gather_len(S, 0, true, px, R.y, 2 * pw, 2 * ph, W);
-        for (int i = lane; i < pw * ph; i += 32) {
-          const int yy = i / pw, xx = i - yy * pw;
-          put(i, R.bdpcm == VVCG_BDPCM_VER ? W.above[xx] : W.left[yy]);
-        }
-        __syncwarp();
-        continue;
-      }
-      const bool isp = R.isp != VVCG_ISP_NONE;
-      const int mrl = min((int)R.mrl, 2);
-      if (isp) {
-        gi_gather_len(S, 0, true, px, R.y, R.cu_w + pw, R.cu_h + ph, W);
-        gi_rows_from_refs(R.cu_w + pw, R.cu_h + ph, W);
-      } else if (mrl == 0) {
-        gi_gather_len(S, 0, true, px, R.y, 2 * pw, 2 * ph, W);
-        gi_rows_from_refs(2 * pw, 2 * ph, W);
-      } else {
-        gi_gather_mrl(S, px, R.y, pw, ph, mrl, W);
-      }
-      const int off = W.off;
-      const int mode = R.mode;
-      if (mode <= 1) {
-        const bool filt = mode == 0 && mrl == 0 && !isp && pw * ph > 32;
-        if (filt) {
-          gi_filter_into_base(W.rowa + off + 1, W.rowl + off + 1, W.rowa[off], 2 * pw, 2 * ph, W);
-        } else {
-          for (int i = lane; i < 2 * pw; i += 32) W.ba[i] = W.rowa[off + 1 + i];
-          for (int i = lane; i < 2 * ph; i += 32) W.bl[i] = W.rowl[off + 1 + i];
-          __syncwarp();
-        }
-        gi_planar_dc(mode == 0, pw, ph, mrl == 0 && pw >= 4 && ph >= 4, W, put);
-        continue;
-      }
-      const GiAng P = gi_ang_params(min(mode, 66), pw, ph, R.cu_w, R.cu_h, true, mrl, isp);
-      if (mrl == 0 && !isp && P.ref_filter) {
-        // rows from the filtered base refs
-        gi_filter_into_base(W.rowa + 1, W.rowl + 1, W.rowa[0], 2 * pw, 2 * ph, W);
-        for (int i = lane; i < 2 * pw + 5; i += 32) W.rowa[i] = i == 0 ? (int16_t)W.btl : W.ba[min(i - 1, 2 * pw - 1)];
-        for (int i = lane; i < 2 * ph + 5; i += 32) W.rowl[i] = i == 0 ? (int16_t)W.btl : W.bl[min(i - 1, 2 * ph - 1)];
-        __syncwarp();
-      }
-      gi_angular(P, pw, ph, true, W.off, bd, W, put);  // the rows' reference line
-      continue;
-    }
-    // chroma
-    auto put = [&](int i, int v) { out[i] = (int16_t)v; };
-    const int w = R.w, h = R.h;
-    if (R.mode >= 81 && R.mode <= 83) {
-      gi_cclm(S, R.comp, R.mode - 81, R.x, R.y, w, h, put);
-      continue;
-    }
-    gi_gather_len(S, R.comp, false, R.x, R.y, 2 * w, 2 * h, W);
-    if (R.mode <= 1) {
-      for (int i = lane; i < 2 * w; i += 32) W.ba[i] = W.above[i];
-      for (int i = lane; i < 2 * h; i += 32) W.bl[i] = W.left[i];
+    gi_predict(A.st, R, A.out + R.out_off, ws[warp]);
+  }
+}
+
+// Sequential reconstruction of groups of transform blocks (one group per
+// warp, its blocks in order; groups are independent): each block is
+// predicted (gi_predict), its residual added, clipped to the bit depth and
+// stored into its plane, and its samples marked decoded, so the next block of
+// the group (the next ISP sub-partition) predicts from them. Follows
+// reconstruct_tu (decode_general.rs:3985-4096; the add / clip / set loop
+// :4087-4093) and the decoded maps of mark_tu (:4891-4906).
+struct GenReconArgs {
+  vvcg_gen_intra_state st;
+  const vvcg_gen_intra_req* reqs;
+  const uint32_t* group_start;  // num_groups + 1 entries
+  int32_t num_groups;
+  const int16_t* res;           // per request w x h at out_off; null = no residual
+  int16_t* pred;                // receives the predictions (w x h at out_off)
+};
+
+__global__ void __launch_bounds__(kGiWarps * 32) k_gen_intra_recon(const __grid_constant__ GenReconArgs A) {
+  __shared__ GiWs ws[kGiWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const vvcg_gen_intra_state& S = A.st;
+  const int maxv = (1 << S.bit_depth) - 1;
+  for (int g = blockIdx.x * kGiWarps + warp; g < A.num_groups; g += gridDim.x * kGiWarps) {
+    for (uint32_t q = A.group_start[g]; q < A.group_start[g + 1]; q++) {
+      const vvcg_gen_intra_req R = A.reqs[q];
+      int16_t* pred = A.pred + R.out_off;
+      gi_predict(S, R, pred, ws[warp]);
       __syncwarp();
-      gi_planar_dc(R.mode == 0, w, h, w >= 4 && h >= 4, W, put);
-      continue;
+      const int16_t* res = A.res ? A.res + R.out_off : nullptr;
+      uint16_t* pl = const_cast<uint16_t*>(S.plane[R.comp]);
+      const int st = (int)S.stride[R.comp];
+      for (int i = lane; i < R.w * R.h; i += 32) {
+        const int yy = i / R.w, xx = i - yy * R.w;
+        const int v = (int)pred[i] + (res ? (int)res[i] : 0);
+        pl[(size_t)(R.y + yy) * st + R.x + xx] = (uint16_t)clampi(v, 0, maxv);
+      }
+      // mark_tu's decoded maps: luma per 4x4 cell touched, chroma per sample
+      if (R.comp == 0) {
+        uint8_t* dm = const_cast<uint8_t*>(S.dec_y);
+        const int cw = (int)S.width >> 2;
+        const int x0 = R.x >> 2, x1 = min((R.x + R.w + 3) >> 2, cw), y0 = R.y >> 2;
+        const int y1 = min((R.y + R.h + 3) >> 2, (int)S.height >> 2);
+        for (int i = lane; i < (x1 - x0) * (y1 - y0); i += 32)
+          dm[(size_t)(y0 + i / (x1 - x0)) * cw + x0 + i % (x1 - x0)] = 1;
+      } else {
+        uint8_t* dm = const_cast<uint8_t*>(S.dec_c);
+        const int cw = (int)S.width >> 1;
+        for (int i = lane; i < R.w * R.h; i += 32) dm[(size_t)(R.y + i / R.w) * cw + R.x + i % R.w] = 1;
+      }
+      __threadfence_block();
+      __syncwarp();
     }
-    gi_rows_from_refs(2 * w, 2 * h, W);
-    const GiAng P = gi_ang_params(min((int)R.mode, 66), w, h, w, h, false, 0, false);
-    gi_angular(P, w, h, false, 0, bd, W, put);
   }
 }
 

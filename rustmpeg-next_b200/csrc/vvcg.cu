@@ -20,6 +20,7 @@
 #include "gen_intra.cuh"
 #include "intra_search.cuh"
 #include "inter_search.cuh"
+#include "inter_tools.cuh"
 #include "prune.cuh"
 #include "split.cuh"
 #include "lmcs.cuh"
@@ -130,6 +131,8 @@ struct vvcg_ctx {
   DevBuf d_cnn_pack, d_cnn_packT;  // packed bf16 convolution weights of the CNN (forward / transposed)
   DevBuf d_cnn_acts, d_cnn_logits, d_cnn_gap, d_cnn_partial;  // CNN training workspace
   DevBuf d_me_reqs, d_me_cands;  // motion-estimation requests and merge candidates
+  std::vector<DbfPass> dbf_ctu;  // CTU-boundary deblocking passes of inter pictures
+  DevBuf d_dbf_ctu;
   uint64_t flags_count = 0;
   int recon_per_sm = 0;  // resident k_recon_rows CTAs per SM
   // CUDA graph of vvcg_batch_run_graph for the prepared batch and one stage mask
@@ -272,6 +275,9 @@ vvcg_status upload_tables(vvcg_ctx* ctx) {
   CK(cudaMemcpyToSymbol(c_affine_taps8, kAffineTaps8, sizeof(kAffineTaps8)), "tables");
   CK(cudaMemcpyToSymbol(c_luma_alt_hpel, kLumaAltHpel, sizeof(kLumaAltHpel)), "tables");
   CK(cudaMemcpyToSymbol(c_bcw_weights, kBcwWeights, sizeof(kBcwWeights)), "tables");
+  CK(cudaMemcpyToSymbol(c_geo_dis, kGeoDis, sizeof(kGeoDis)), "tables");
+  CK(cudaMemcpyToSymbol(c_geo_angle_to_mask, kGeoAngleToMask, sizeof(kGeoAngleToMask)), "tables");
+  CK(cudaMemcpyToSymbol(c_bilinear4, kBilinear4, sizeof(kBilinear4)), "tables");
   CK(cudaMemcpyToSymbol(c_alf_clip, kAlfClip, sizeof(kAlfClip)), "tables");
   CK(cudaMemcpyToSymbol(c_alf_fixed, kAlfFixedCoeff, sizeof(kAlfFixedCoeff)), "tables");
   CK(cudaMemcpyToSymbol(c_alf_class_to_filter, kAlfClassToFilter, sizeof(kAlfClassToFilter)), "tables");
@@ -444,7 +450,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
                     &ctx->d_tu_recs, &ctx->d_tu_idx, &ctx->d_lmcs, &ctx->d_alfp, &ctx->d_alfc,
                     &ctx->d_search_reqs, &ctx->d_search_cost, &ctx->d_search_mode, &ctx->d_search_ctus,
                     &ctx->d_cnn_pack, &ctx->d_cnn_packT, &ctx->d_cnn_acts, &ctx->d_cnn_logits, &ctx->d_cnn_gap,
-                    &ctx->d_cnn_partial, &ctx->d_me_reqs, &ctx->d_me_cands})
+                    &ctx->d_cnn_partial, &ctx->d_me_reqs, &ctx->d_me_cands, &ctx->d_dbf_ctu})
     b->release();
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -1789,6 +1795,74 @@ extern "C" vvcg_status vvcg_gen_intra_predict_dev(vvcg_ctx* ctx, const vvcg_gen_
   return VVCG_OK;
 }
 
+// Checks one general intra request against the picture (shared by the
+// prediction and the reconstruction entry points); null when valid.
+static const char* gen_intra_req_error(const vvcg_gen_intra_state* st, const vvcg_gen_intra_req& r,
+                                       uint64_t out_count) {
+  if (r.comp > 2) return "component";
+  if ((uint64_t)r.out_off + (uint64_t)r.w * r.h > out_count) return "output past the buffer";
+  if (r.comp == 0) {
+    if (!pow2_in(r.w, 1, 64) || !pow2_in(r.h, 1, 64) || r.x + r.w > st->width || r.y + r.h > st->height)
+      return "luma block";
+    if (r.mrl > 2 || r.isp > VVCG_ISP_VER || r.bdpcm > VVCG_BDPCM_VER) return "mrl / isp / bdpcm";
+    if (r.isp != VVCG_ISP_NONE) {
+      if (!pow2_in(r.cu_w, 4, 64) || !pow2_in(r.cu_h, 4, 64) || r.x < r.cu_x || r.y < r.cu_y ||
+          r.x + r.w > r.cu_x + r.cu_w || r.y + r.h > r.cu_y + r.cu_h)
+        return "ISP sub-partition outside its CU";
+      if (r.isp == VVCG_ISP_VER && (r.cu_w == 4 || (r.cu_w == 8 && r.cu_h > 4)) && (r.cu_x & 3))
+        return "ISP region off the 4-sample grid";
+    } else if (r.mrl && (r.w < 4 || r.h < 4)) {
+      return "MRL on a block below 4x4";
+    }
+  } else {
+    if (!pow2_in(r.w, 2, 32) || !pow2_in(r.h, 2, 32) || r.x + r.w > st->width / 2 || r.y + r.h > st->height / 2)
+      return "chroma block";
+    if (r.mode > 66 && (r.mode < 81 || r.mode > 83)) return "mode";
+    if (r.mode >= 81 && ((r.x | r.y) & 1)) return "CCLM position";
+  }
+  return nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// General-decoder sequential reconstruction (vvcg_gen_intra_recon_dev).
+// ---------------------------------------------------------------------------
+extern "C" vvcg_status vvcg_gen_intra_recon_dev(vvcg_ctx* ctx, const vvcg_gen_intra_state* st,
+                                                const vvcg_gen_intra_req* reqs, uint32_t num_reqs,
+                                                const uint32_t* group_start, uint32_t num_groups,
+                                                const int16_t* residual, int16_t* pred, uint64_t out_count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_groups) return VVCG_OK;
+  if (!st || !reqs || !group_start || !pred) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  if (!st->plane[0] || !st->plane[1] || !st->plane[2] || !st->dec_y || !st->dec_c)
+    return fail(ctx, VVCG_INVALID_INPUT, "missing planes or decoded maps");
+  if (!st->width || !st->height || (st->width & 7) || (st->height & 7))
+    return fail(ctx, VVCG_INVALID_INPUT, "picture size must be a multiple of 8");
+  if (st->width > 16384 || st->height > 16384) return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture larger than 16384");
+  if (st->stride[0] < st->width || st->stride[1] < st->width / 2 || st->stride[2] < st->width / 2)
+    return fail(ctx, VVCG_INVALID_INPUT, "stride smaller than the plane width");
+  if (st->bit_depth < 8 || st->bit_depth > 12) return fail(ctx, VVCG_INVALID_INPUT, "bit depth");
+  if (st->ctu_size && !pow2_in(st->ctu_size, 16, 128)) return fail(ctx, VVCG_INVALID_INPUT, "CTU size");
+  if (group_start[0] != 0 || group_start[num_groups] != num_reqs)
+    return fail(ctx, VVCG_INVALID_INPUT, "groups must cover the requests from 0 to num_reqs");
+  for (uint32_t g = 0; g < num_groups; g++)
+    if (group_start[g + 1] < group_start[g]) return fail(ctx, VVCG_INVALID_INPUT, "group %u: decreasing start", g);
+  for (uint32_t i = 0; i < num_reqs; i++)
+    if (const char* e = gen_intra_req_error(st, reqs[i], out_count))
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: %s", i, e);
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  const size_t rb = sizeof(vvcg_gen_intra_req) * num_reqs, gb = sizeof(uint32_t) * (num_groups + 1);
+  CK(ctx->d_tu_recs.reserve(rb + 256 + gb), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, rb, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  uint32_t* d_groups = (uint32_t*)((char*)ctx->d_tu_recs.p + ((rb + 255) & ~(size_t)255));
+  CK(cudaMemcpyAsync(d_groups, group_start, gb, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  GenReconArgs A{*st, (const vvcg_gen_intra_req*)ctx->d_tu_recs.p, d_groups, (int32_t)num_groups, residual, pred};
+  const uint32_t grid = std::min<uint32_t>((num_groups + kGiWarps - 1) / kGiWarps, (uint32_t)ctx->num_sms * 8);
+  k_gen_intra_recon<<<grid, kGiWarps * 32, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "intra reconstruction launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
 // ---------------------------------------------------------------------------
 // General-decoder deblocking (vvcg_deblock_general_dev).
 // ---------------------------------------------------------------------------
@@ -1841,6 +1915,203 @@ extern "C" vvcg_status vvcg_deblock_general_dev(vvcg_ctx* ctx, uint16_t* const p
   k_dbk_general<false><<<grid, 128, 0, ctx->stream>>>(A);
   CK(cudaGetLastError(), "deblock launch");
   ctx->launches += 2;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Inter-prediction tools (BDOF, DMVR, affine / PROF, CIIP, GPM).
+// ---------------------------------------------------------------------------
+static_assert(sizeof(vvcg_bdof_req) == 8 && sizeof(vvcg_dmvr_req) == 28 && sizeof(vvcg_affine_req) == 36 &&
+                  sizeof(vvcg_prof_req) == 16 && sizeof(vvcg_ciip_req) == 12 && sizeof(vvcg_gpm_req) == 12,
+              "inter tool request layouts");
+
+namespace {
+
+// Copies n host requests into the context's request buffer; the device copy.
+template <class T>
+vvcg_status upload_reqs(vvcg_ctx* ctx, const T* reqs, uint32_t n, const T** dev) {
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  CK(ctx->d_tu_recs.reserve(sizeof(T) * n), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_tu_recs.p, reqs, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  *dev = (const T*)ctx->d_tu_recs.p;
+  return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_bdof_dev(vvcg_ctx* ctx, const vvcg_bdof_req* reqs, uint32_t num_reqs, const int32_t* pred0,
+                                     const int32_t* pred1, int32_t* out, uint64_t count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !pred0 || !pred1 || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_bdof_req& r = reqs[i];
+    if (r.w < 4 || r.h < 4 || (r.w & 3) || (r.h & 3) || r.w > 128 || r.h > 128)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: block must be 4..128 and a multiple of 4", i);
+    if ((uint64_t)r.off + (uint64_t)r.w * r.h > count) return fail(ctx, VVCG_INVALID_INPUT, "request %u: past the arrays", i);
+  }
+  const vvcg_bdof_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  k_bdof<<<num_reqs, 128, 0, ctx->stream>>>(d, pred0, pred1, out);
+  CK(cudaGetLastError(), "bdof launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_dmvr_dev(vvcg_ctx* ctx, const uint8_t* ref0, const uint8_t* ref1, uint32_t width,
+                                     uint32_t height, uint32_t stride, const vvcg_dmvr_req* reqs, uint32_t num_reqs,
+                                     int32_t* mv_out) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!ref0 || !ref1 || !reqs || !mv_out) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  if (!width || !height || stride < width || width > 16384 || height > 16384)
+    return fail(ctx, VVCG_INVALID_INPUT, "reference plane geometry");
+  for (uint32_t i = 0; i < num_reqs; i++)
+    if (!reqs[i].dx || !reqs[i].dy || reqs[i].dx > 16 || reqs[i].dy > 16)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: subblock must be 1..16 x 1..16", i);
+  const vvcg_dmvr_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  DmvrArgs A{ref0, ref1, (int32_t)width, (int32_t)height, (int32_t)stride, (int32_t)num_reqs, d, mv_out};
+  k_dmvr<<<(num_reqs + 3) / 4, 128, 0, ctx->stream>>>(A);
+  CK(cudaGetLastError(), "dmvr launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_affine_mvs_dev(vvcg_ctx* ctx, const vvcg_affine_req* reqs, uint32_t num_reqs,
+                                           int32_t* sub_mv, uint64_t sub_count, int32_t* prof) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !sub_mv || !prof) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_affine_req& r = reqs[i];
+    if (!pow2_in(r.w, 8, 128) || !pow2_in(r.h, 8, 128) || r.inter_dir < 1 || r.inter_dir > 3)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: size or prediction type", i);
+    if ((uint64_t)r.sub_off + (uint64_t)(r.w / 4) * (r.h / 4) > sub_count)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: subblock MVs past the array", i);
+  }
+  const vvcg_affine_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  k_affine_mvs<<<(num_reqs + 127) / 128, 128, 0, ctx->stream>>>(d, (int)num_reqs, sub_mv, prof);
+  CK(cudaGetLastError(), "affine launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_prof_dev(vvcg_ctx* ctx, const vvcg_prof_req* reqs, uint32_t num_reqs, const int32_t* src,
+                                     uint64_t src_count, const int32_t* dmv, uint64_t dmv_count, int32_t* out,
+                                     uint64_t out_count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !src || !dmv || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  for (uint32_t i = 0; i < num_reqs; i++)
+    if ((uint64_t)reqs[i].src_off + 36 > src_count || (uint64_t)reqs[i].dmv_off + 32 > dmv_count ||
+        (uint64_t)reqs[i].out_off + 16 > out_count)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: past the arrays", i);
+  const vvcg_prof_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  k_prof<<<(16 * num_reqs + 127) / 128, 128, 0, ctx->stream>>>(d, (int)num_reqs, src, dmv, out);
+  CK(cudaGetLastError(), "prof launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_ciip_blend_dev(vvcg_ctx* ctx, const vvcg_ciip_req* reqs, uint32_t num_reqs,
+                                           const int32_t* inter, const int32_t* intra, int32_t* out, uint64_t count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !inter || !intra || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  for (uint32_t i = 0; i < num_reqs; i++)
+    if ((uint64_t)reqs[i].off + reqs[i].n > count) return fail(ctx, VVCG_INVALID_INPUT, "request %u: past the arrays", i);
+  const vvcg_ciip_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  k_ciip<<<num_reqs, 128, 0, ctx->stream>>>(d, inter, intra, out);
+  CK(cudaGetLastError(), "ciip launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_gpm_blend_dev(vvcg_ctx* ctx, const vvcg_gpm_req* reqs, uint32_t num_reqs,
+                                          const int32_t* pred0, const int32_t* pred1, int32_t* out, uint64_t count) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!num_reqs) return VVCG_OK;
+  if (!reqs || !pred0 || !pred1 || !out) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  for (uint32_t i = 0; i < num_reqs; i++) {
+    const vvcg_gpm_req& r = reqs[i];
+    if (!r.w || !r.h || r.w > 128 || r.h > 128 || r.split_dir > 63 || r.scale_x > 1 || r.scale_y > 1)
+      return fail(ctx, VVCG_INVALID_INPUT, "request %u: size, split direction or subsampling", i);
+    if ((uint64_t)r.off + (uint64_t)r.w * r.h > count) return fail(ctx, VVCG_INVALID_INPUT, "request %u: past the arrays", i);
+  }
+  const vvcg_gpm_req* d;
+  vvcg_status st = upload_reqs(ctx, reqs, num_reqs, &d);
+  if (st != VVCG_OK) return st;
+  k_gpm<<<num_reqs, 128, 0, ctx->stream>>>(d, pred0, pred1, out);
+  CK(cudaGetLastError(), "gpm launch");
+  ctx->launches++;
+  return VVCG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CTU-boundary deblocking of inter pictures (vvcg_deblock_ctu_edges_dev).
+// ---------------------------------------------------------------------------
+static_assert(sizeof(vvcg_ctu_motion) == 40, "CTU motion layout");
+
+extern "C" vvcg_status vvcg_deblock_ctu_edges_dev(vvcg_ctx* ctx, uint16_t* const planes[3], const uint32_t stride[3],
+                                                  uint32_t width, uint32_t height, uint32_t ctu, uint8_t qp,
+                                                  const vvcg_ctu_motion* cells) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (!planes || !stride || !cells) return fail(ctx, VVCG_INVALID_INPUT, "missing arguments");
+  if (ctu != 32 && ctu != 64 && ctu != 128) return fail(ctx, VVCG_INVALID_INPUT, "CTU size must be 32, 64 or 128");
+  if (!width || !height || width % ctu || height % ctu)
+    return fail(ctx, VVCG_INVALID_INPUT, "picture size must be a nonzero multiple of the CTU size");
+  if ((uint64_t)width * height > kMaxLumaSamples) return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture too large");
+  if (qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "QP above 63");
+  const int w = (int)width, h = (int)height, cw = w / 2, ch = h / 2, c = (int)ctu, cc = c / 2;
+  for (int k = 0; k < 3; k++)
+    if (!planes[k] || stride[k] < (uint32_t)(k ? cw : w) || (stride[k] & 7) ||
+        (reinterpret_cast<uintptr_t>(planes[k]) & 15))
+      return fail(ctx, VVCG_INVALID_INPUT,
+                  "plane %d: needs a 16-byte aligned pointer and a stride >= the width that is a multiple of 8", k);
+  CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+  // slice.rs:2305-2311: SliceQpY, derived_chroma_qp, lengths of min(ctu, 32)
+  // luma and ctu/2 chroma transform sides
+  const int cqp = std::min(63, std::max(0, (int)qp <= 26 ? (int)qp : (int)qp - 1));
+  const int lml = std::min(c, 32) >= 32 ? 7 : 3;
+  const int cols = w / c, rows = h / c;
+  auto& v = ctx->dbf_ctu;
+  v.clear();
+  // luma V, Cb V, Cr V, luma H, Cb H, Cr H
+  v.push_back(DbfPass{planes[0], (int32_t)stride[0], w, h, 8, c, c, (int)qp, 0, 0, 0, lml, lml, 1, cols - 1, h / 4,
+                      cells, cols, 0, c});
+  for (int k = 1; k <= 2; k++)
+    v.push_back(DbfPass{planes[k], (int32_t)stride[k], cw, ch, 8, cc, cc, cqp, 0, 0, 0, 3, 3, 2, cols - 1, ch / 2,
+                        cells, cols, k, cc});
+  v.push_back(DbfPass{planes[0], (int32_t)stride[0], w, h, 8, c, c, (int)qp, 0, 0, 0, lml, lml, 1, rows - 1, w / 4,
+                      cells, cols, 0, c});
+  for (int k = 1; k <= 2; k++)
+    v.push_back(DbfPass{planes[k], (int32_t)stride[k], cw, ch, 8, cc, cc, cqp, 0, 0, 0, 3, 3, 2, rows - 1, cw / 2,
+                        cells, cols, k, cc});
+  CK(ctx->d_dbf_ctu.reserve(sizeof(DbfPass) * v.size()), "cudaMalloc");
+  CK(cudaMemcpyAsync(ctx->d_dbf_ctu.p, v.data(), sizeof(DbfPass) * v.size(), cudaMemcpyHostToDevice, ctx->stream),
+     "upload");
+  const DbfPass* d = (const DbfPass*)ctx->d_dbf_ctu.p;
+  auto blocks = [](const DbfPass& p) { return (unsigned)((std::max(0, p.n_edges * p.n_segs) + 127) / 128); };
+  if (cols > 1) {
+    k_deblock_luma<true><<<dim3(blocks(v[0]), 1), 128, 0, ctx->stream>>>(d, 1);
+    k_deblock_chroma<true><<<dim3(blocks(v[1]), 2), 128, 0, ctx->stream>>>(d + 1, 2);
+    ctx->launches += 2;
+  }
+  if (rows > 1) {
+    k_deblock_luma<false><<<dim3(blocks(v[3]), 1), 128, 0, ctx->stream>>>(d + 3, 1);
+    k_deblock_chroma<false><<<dim3(blocks(v[4]), 2), 128, 0, ctx->stream>>>(d + 4, 2);
+    ctx->launches += 2;
+  }
+  CK(cudaGetLastError(), "deblock launch");
   return VVCG_OK;
 }
 

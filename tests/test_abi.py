@@ -121,7 +121,9 @@ RECORDS = {
     "SPLIT_REQ_DTYPE": "vvcg_split_req", "GEN_INTRA_REQ_DTYPE": "vvcg_gen_intra_req",
     "DBK_CELL_DTYPE": "vvcg_dbk_cell", "DBK_CCELL_DTYPE": "vvcg_dbk_ccell", "DBK_PARAMS_DTYPE": "vvcg_dbk_params",
     "MIP_REQ_DTYPE": "vvcg_mip_req", "MIP_RES_DTYPE": "vvcg_mip_res", "TXS_REQ_DTYPE": "vvcg_tx_search_req",
-    "TXS_RES_DTYPE": "vvcg_tx_search_res", "TU_DTYPE": "vvcg_tu_rec",
+    "TXS_RES_DTYPE": "vvcg_tx_search_res", "TU_DTYPE": "vvcg_tu_rec", "CTU_MOTION_DTYPE": "vvcg_ctu_motion",
+    "BDOF_REQ_DTYPE": "vvcg_bdof_req", "DMVR_REQ_DTYPE": "vvcg_dmvr_req", "AFFINE_REQ_DTYPE": "vvcg_affine_req",
+    "PROF_REQ_DTYPE": "vvcg_prof_req", "CIIP_REQ_DTYPE": "vvcg_ciip_req", "GPM_REQ_DTYPE": "vvcg_gpm_req",
 }
 
 
