@@ -37,6 +37,7 @@ TABLES = [
     ("filter.rs", "ALF_CLIP_VALS_12BIT"), ("filter.rs", "ALF_TRANSPOSE_PERM"),
     ("inter.rs", "LUMA_FILTER_8TAP"), ("inter.rs", "LUMA_ALT_HPEL_FILTER_8TAP"),
     ("inter.rs", "AFFINE_LUMA_FILTER_8TAP"), ("inter.rs", "BCW_WEIGHTS"),
+    ("inter.rs", "GEO_DIS"), ("inter.rs", "GEO_ANGLE_TO_MASK"), ("inter.rs", "BILINEAR_FILTER_PREC4"),
     ("predict.rs", "ANG_TABLE"), ("predict.rs", "INV_ANG_TABLE"), ("predict.rs", "INTRA_FILTER_THRESHOLD"),
     ("predict.rs", "CHROMA_FILTER_4TAP"), ("predict.rs", "CCLM_DIV_SIG_TABLE"),
     ("predict.rs", "MIP_MATRIX_4X4"), ("predict.rs", "MIP_MATRIX_8X8"), ("predict.rs", "MIP_MATRIX_16X16"),

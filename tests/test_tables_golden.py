@@ -34,6 +34,7 @@ PAIRS = {
     "kAlfTransposePerm": ["ALF_TRANSPOSE_PERM"],
     "kLumaTaps8": ["LUMA_FILTER_8TAP"], "kLumaAltHpel": ["LUMA_ALT_HPEL_FILTER_8TAP"],
     "kAffineTaps8": ["AFFINE_LUMA_FILTER_8TAP"], "kBcwWeights": ["BCW_WEIGHTS"],
+    "kGeoDis": ["GEO_DIS"], "kGeoAngleToMask": ["GEO_ANGLE_TO_MASK"], "kBilinear4": ["BILINEAR_FILTER_PREC4"],
     "kAngTable": ["ANG_TABLE"], "kInvAngTable": ["INV_ANG_TABLE"],
     "kIntraFilterThreshold": ["INTRA_FILTER_THRESHOLD"], "kChromaTaps4": ["CHROMA_FILTER_4TAP"],
     "kCclmDivSig": ["CCLM_DIV_SIG_TABLE"],
