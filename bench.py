@@ -368,6 +368,9 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=48,
                     help="pictures in the CPU baseline sample (about 0.25 s each on one core)")
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle check of the batch before timing")
+    ap.add_argument("--no-batching", action="store_true", help="skip the batching (mixed streams) section")
+    ap.add_argument("--batch-streams", type=int, default=64)
+    ap.add_argument("--batch-frames", type=int, default=8)
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -558,9 +561,13 @@ def main():
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "clocks": clocks}
-    if rank == 0 and not args.no_encode:
+    # the encoder and batching sections run at N = 1 only: under torchrun the
+    # other ranks would wait at the closing barrier meanwhile
+    if world == 1 and not args.no_encode:
         with torch.cuda.stream(stream):
             line["encode"] = bench_encoder(pkg, ctx, stream, dev, args, peaks)
+    if world == 1 and not args.no_batching:
+        line["batching"] = bench_batching(pkg, dev, stream, args, timed)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
@@ -721,6 +728,86 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
             "training": {"ctus_labelled": n_train, "label_s": round(label_s, 2), "steps": args.train_steps,
                          "batch": 1024, "s": round(train_s, 2), "first_loss": round(losses[0], 4),
                          "final_loss": round(float(np.mean(losses[-20:])), 4)}}
+
+
+def _stream_sources(w, h, bd, stream, frames):
+    """Coded-size source planes of a batching stream's frames (a task of the
+    spawned generator pool)."""
+    load_pkg()
+    from rustmpeg_next_b200 import synth
+
+    _, _, p = synth.workload_picture(0, 1, QPS[:1], width=w, height=h, bd=bd)
+    return [synth.workload_sources(f, p, stream) for f in range(frames)]
+
+
+def bench_batching(pkg, dev, stream, args, timed):
+    """The batching configuration: independent streams (resolutions drawn
+    from 416x240 .. 3840x2160, 8 or 10 bits, QP 22..37), each its frames of
+    the full-frame content encoded by the GPU encoder, reconstructed and
+    filtered in one batched pass (one prepared batch, one graph replay) and,
+    for comparison, one context and graph replay per stream on the same
+    stream; every picture of the batch is checked against the oracle."""
+    import multiprocessing as mp
+
+    from rustmpeg_next_b200 import synth
+
+    seed = 0x5EED0000 + 777
+    specs = synth.batching_streams(args.batch_streams, seed)
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(max(1, min(os.cpu_count() or 1, len(specs)))) as pool:
+        srcs = pool.starmap(_stream_sources, [(w, h, bd, 1000 + k, args.batch_frames)
+                                              for k, (w, h, bd, _) in enumerate(specs)])
+    enc = pkg.Context(dev.index)
+    streams = []
+    for k, ((w, h, bd, qp), frames) in enumerate(zip(specs, srcs)):
+        streams.append(synth.encoded_parts(enc, args.batch_frames, (qp,), seed + k, sources=dict(enumerate(frames)),
+                                           width=w, height=h, bd=bd, stream=1000 + k))
+    enc.close()
+    del srcs
+    build_s = time.perf_counter() - t0
+    aps = synth.workload_aps(seed)
+    every = synth.assemble([p for parts in streams for p in parts], aps)
+    batch = pkg.Batch(*every)
+    px = int(sum(int(p["visible_width"]) * int(p["visible_height"]) for p in every[0]))
+    ctx = pkg.Context(dev.index)
+    ctx.set_stream(stream)
+    ctx.prepare(batch)
+    ctx.upload(batch)
+    ctx.run(pkg.STAGE_ALL)
+    ctx.sync()
+    parity = parity_check(*every, ctx.download(batch.output_planes()), os.cpu_count() or 1)
+    singles = []
+    for parts in streams:
+        b = pkg.Batch(*synth.assemble(parts, aps))
+        c = pkg.Context(dev.index)
+        c.set_stream(stream)
+        c.prepare(b)
+        c.upload(b)
+        singles.append((c, b))
+    k = max(3, args.steps // 5)
+    for _ in range(2):
+        ctx.run(pkg.STAGE_ALL, graph=True)
+        for c, _ in singles:
+            c.run(pkg.STAGE_ALL, graph=True)
+    batched_ms = timed(lambda: ctx.run(pkg.STAGE_ALL, graph=True), k)
+    per_stream_ms = timed(lambda: [c.run(pkg.STAGE_ALL, graph=True) for c, _ in singles], k)
+    ctx.close()
+    for c, _ in singles:
+        c.close()
+    res = sorted({(w, h) for w, h, _, _ in specs})
+    return {"what": "independent streams of uneven resolution and bit depth, each frame of the full-frame content "
+                    "encoded by the GPU encoder; recon + deblock + SAO + ALF (APS); one batched pass (a graph "
+                    "replay over all pictures) against one context and graph replay per stream",
+            "streams": len(specs), "frames_per_stream": args.batch_frames, "pictures": len(every[0]),
+            "resolutions": [f"{w}x{h}" for w, h in res],
+            "bit_depths": {str(b): sum(1 for s in specs if s[2] == b) for b in (8, 10)},
+            "mpx_per_step": round(px / 1e6, 2),
+            "batched_ms": round(batched_ms, 3), "per_stream_ms": round(per_stream_ms, 3),
+            "batched_mpx_s": round(px / (batched_ms * 1e-3) / 1e6, 1),
+            "per_stream_mpx_s": round(px / (per_stream_ms * 1e-3) / 1e6, 1),
+            "speedup": round(per_stream_ms / batched_ms, 2), "parity": parity, "build_s": round(build_s, 1),
+            "block_sizes": "32x32 coding units of the frame path (the 4x4..128x128 tree of the general decoder "
+                           "has no picture-level pass)"}
 
 
 def _cpu_model():

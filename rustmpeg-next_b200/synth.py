@@ -707,6 +707,13 @@ def encoded_workload(ctx, frames_per_qp, qps, seed, sources=None, width=1920, he
     bit-exact with the oracle's encoder). `sources` maps a frame index to its
     coded-size planes (generated here when absent). Returns (pics, cus,
     levels, ctus, aps) ready for Batch."""
+    parts = encoded_parts(ctx, frames_per_qp, qps, seed, sources, width, height, bd, encode_chunk, stream)
+    return assemble(parts, workload_aps(seed))
+
+
+def encoded_parts(ctx, frames_per_qp, qps, seed, sources=None, width=1920, height=1080, bd=10, encode_chunk=32,
+                  stream=0):
+    """encoded_workload's per-picture (pic, cus, levels, ctus) parts."""
     n = frames_per_qp * len(qps)
     descs = [workload_picture(i, frames_per_qp, qps, width, height, bd) for i in range(n)]
     src = dict(sources or {})
@@ -725,7 +732,7 @@ def encoded_workload(ctx, frames_per_qp, qps, seed, sources=None, width=1920, he
             ncu = (int(p["width"]) // tb) * (int(p["height"]) // tb)
             parts.append(decoder_picture(a + j, p, cus[at:at + ncu], levels, seed))
             at += ncu
-    return assemble(parts, workload_aps(seed))
+    return parts
 
 
 def oracle_workload_picture(oracle, index, frames_per_qp, qps, seed, width=1920, height=1080, bd=10, stream=0):
@@ -739,3 +746,21 @@ def oracle_workload_picture(oracle, index, frames_per_qp, qps, seed, width=1920,
     cus, levels, _ = oracle.encode_frame(y, u, v, int(p["bit_depth"]), int(p["slice_qp"]), int(p["ctu_log2"]),
                                          opts, int(p["chroma_format"]))
     return decoder_picture(index, p, cus, levels, seed)
+
+
+# ------------------------------------------------------------------ batching --
+# The batching configuration: independent streams of uneven resolution and
+# bit depth decoded in one pass.
+BATCH_RESOLUTIONS = ((416, 240), (832, 480), (1280, 720), (1920, 1080), (3840, 2160))
+BATCH_WEIGHTS = (0.3, 0.3, 0.2, 0.15, 0.05)
+
+
+def batching_streams(n_streams, seed):
+    """(width, height, bit depth, QP) of each stream: resolution drawn with
+    BATCH_WEIGHTS, bit depth uniform over {8, 10}, QP uniform in 22..37."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_streams):
+        w, h = BATCH_RESOLUTIONS[int(rng.choice(len(BATCH_RESOLUTIONS), p=BATCH_WEIGHTS))]
+        out.append((w, h, int(rng.choice((8, 10))), int(rng.integers(22, 38))))
+    return out
