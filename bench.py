@@ -152,7 +152,8 @@ def workload_name(frames_per_qp):
 
 RECORDS = ("value-noise content of the full-frame configuration encoded all-intra by the repo's GPU encoder "
            "(7-mode intra, CCLM, dependent quantisation, deblocking; bit-exact with the oracle's encoder); "
-           "SAO and ALF parameters seeded per CTU; coded TBs' levels only")
+           "SAO and ALF parameters seeded per CTU; coded TBs' levels only, in the sparse form for the timed "
+           "legs (level_forms)")
 
 
 class ClockSampler:
@@ -235,11 +236,6 @@ def job_mpx_per_s(world, px_per_rank_step, ms_per_step):
     """Whole-job throughput: every rank reconstructs its own batch of
     px_per_rank_step pixels per step; ms_per_step is the slowest rank's."""
     return world * px_per_rank_step / (ms_per_step * 1e-3) / 1e6
-
-
-def workload_name(frames_per_qp):
-    return (f"1920x1080 10-bit 4:2:0, {frames_per_qp} frames x QP{{22,27,32,37}} = {4 * frames_per_qp} "
-            "pictures/step, CTU 32, recon+deblock+SAO+ALF(APS)")
 
 
 def sample_indices(n_total, n):
@@ -389,6 +385,8 @@ def main():
 
     pkg = load_pkg()
     pkg.build()
+    from rustmpeg_next_b200 import synth
+
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -401,7 +399,10 @@ def main():
 
     ctx = pkg.Context(local)
     t_wl = time.perf_counter()
-    pics, cus, levels, ctus, aps = build_workload(pkg, ctx, args.frames_per_qp, rank)
+    # dense raster levels (what the oracle and the CPU baseline read) and the
+    # same TBs in the sparse form the timed batch carries
+    pics_d, cus_d, levels_d, ctus, aps = build_workload(pkg, ctx, args.frames_per_qp, rank)
+    pics, cus, levels = synth.sparsify(pics_d, cus_d, levels_d)
     workload_s = time.perf_counter() - t_wl
     n_pics = len(pics)
     # pinned host copies for the end-to-end leg
@@ -442,7 +443,7 @@ def main():
     ctx.sync()
     parity = None
     if rank == 0 and not args.no_parity:
-        parity = parity_check(pics, cus, levels, ctus, aps, ctx.download(batch.output_planes()),
+        parity = parity_check(pics_d, cus_d, levels_d, ctus, aps, ctx.download(batch.output_planes()),
                               os.cpu_count() or 1)
 
     # warm-up (the first graph run captures the stages), then the timed steps
@@ -468,8 +469,23 @@ def main():
     ctx.run(pkg.STAGE_ALL)
     ctx.sync()
 
+    # the same batch with dense raster levels, device-resident, on a context
+    # of its own (for the comparison of the two level forms)
+    batch_d = pkg.Batch(pics_d, pin(cus_d), pin(levels_d), ctus_p, aps_p)
+    with pkg.Context(local) as ctx_d:
+        ctx_d.set_stream(stream)
+        ctx_d.prepare(batch_d)
+        ctx_d.upload(batch_d)
+        for _ in range(args.warmup):
+            ctx_d.run(pkg.STAGE_ALL, graph=use_graph)
+        dense_ms = timed(lambda: ctx_d.run(pkg.STAGE_ALL, graph=use_graph), max(3, args.steps // 2))
+        ctx_d.run(pkg.STAGE_RECON, graph=use_graph)
+        dense_recon_ms = timed(lambda: ctx_d.run(pkg.STAGE_RECON, graph=use_graph), max(3, args.steps // 2))
+        ctx_d.sync()
+
     # end to end through the C ABI with pinned host buffers
     h2d = cus.nbytes + levels.nbytes + ctus.nbytes + aps.nbytes
+    h2d_dense = cus_d.nbytes + levels_d.nbytes + ctus.nbytes + aps.nbytes
     d2h = n_pics * PIX_W * PIX_H * 2 * 3 // 2
 
     # Streaming through the host-buffer call: steps rotate over E2E_LANES
@@ -484,12 +500,12 @@ def main():
                        for o in outs]))
     busy = [False] * len(lanes)
 
-    def e2e_step(i):
+    def e2e_step(b, i):
         j = i % len(lanes)
         c, o = lanes[j]
         if busy[j]:
             c.sync()
-        c.decode_batch_async(batch, o)
+        c.decode_batch_async(b, o)
         busy[j] = True
 
     def e2e_drain():
@@ -498,20 +514,32 @@ def main():
                 lanes[j][0].sync()
                 busy[j] = False
 
-    for i in range(len(lanes)):
-        e2e_step(i)
-    e2e_drain()
-    sync_all()
-    t0 = time.perf_counter()
-    k_e2e = max(3 * E2E_LANES, args.steps // 2)
-    for i in range(k_e2e):
-        e2e_step(i)
-    e2e_drain()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / k_e2e, dist, dev)
+    def e2e_run(b):
+        for i in range(len(lanes)):
+            e2e_step(b, i)
+        e2e_drain()
+        sync_all()
+        t0 = time.perf_counter()
+        k_e2e = max(3 * E2E_LANES, args.steps // 2)
+        for i in range(k_e2e):
+            e2e_step(b, i)
+        e2e_drain()
+        return max_over_ranks((time.perf_counter() - t0) * 1e3 / k_e2e, dist, dev)
+
+    e2e_dense_ms = e2e_run(batch_d)
+    e2e_ms = e2e_run(batch)
 
     px_step = n_pics * PIX_W * PIX_H
     value = job_mpx_per_s(world, px_step, ms_step)
     e2e_value = job_mpx_per_s(world, px_step, e2e_ms)
+    level_forms = {
+        "timed": "sparse: per coded TB its nonzero-level count and (raster index, level) int16 pairs "
+                 "(VVCG_TOOL_SPARSE_LEVELS); parity is checked against the oracle on the dense records",
+        "sparse_level_bytes": int(levels.nbytes), "dense_level_bytes": int(levels_d.nbytes),
+        "dense": {"value": round(job_mpx_per_s(world, px_step, dense_ms), 2),
+                  "ms_per_step": round(dense_ms, 4), "recon_ms": round(dense_recon_ms, 4),
+                  "e2e": round(job_mpx_per_s(world, px_step, e2e_dense_ms), 2),
+                  "h2d_bytes_per_step": int(h2d_dense)}}
 
     # roofline of the dominant stage
     peaks = {}
@@ -553,8 +581,10 @@ def main():
             "config": {"workload": workload_name(args.frames_per_qp),
                        "pictures_per_step": n_pics, "parallelism": f"replicas x{world}",
                        "launch": "direct launches" if args.no_graph else "CUDA graph replay",
-                       "l2": "inputs larger than L2 (466 MB levels, 1.6 GB planes); no flush",
+                       "l2": f"inputs larger than L2 ({levels.nbytes / 1e6:.0f} MB sparse levels, "
+                             f"{2 * coded / 1e9:.1f} GB planes read and written per stage); no flush",
                        "records": RECORDS, "workload_build_s": round(workload_s, 1)},
+            "level_forms": level_forms,
             "parity": parity,
             "roofline": roofline,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mpx/s", "h2d_bytes_per_step": int(h2d),
@@ -569,7 +599,7 @@ def main():
     if world == 1 and not args.no_batching:
         line["batching"] = bench_batching(pkg, dev, stream, args, timed)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt, n = cpu_baseline_oracle(pics, cus, levels, ctus, aps, args.cpu_sample)
+        v, dt, n = cpu_baseline_oracle(pics_d, cus_d, levels_d, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
                                 "sample": f"{n} pictures of 1920x1080 spread over the batch (all QPs), "
                                           f"{dt:.1f} s, one thread (C++ restatement of the "

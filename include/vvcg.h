@@ -73,7 +73,9 @@ enum {
   VVCG_TOOL_ALF = 1u << 3,       /* enable_alf */
   /* encoder only (vvcg_encode_batch): */
   VVCG_TOOL_ENC_FULL_INTRA = 1u << 4, /* all 7 searched luma modes, not only Planar / DC */
-  VVCG_TOOL_ENC_CCLM = 1u << 5        /* chroma mode by SAD among DM and the 3 CCLM modes */
+  VVCG_TOOL_ENC_CCLM = 1u << 5,       /* chroma mode by SAD among DM and the 3 CCLM modes */
+  /* decoder: the picture's level_off values index sparse TBs (see vvcg_cu_rec) */
+  VVCG_TOOL_SPARSE_LEVELS = 1u << 6
 };
 
 /* One picture of the 8..12-bit frame path: the inputs of
@@ -105,7 +107,13 @@ typedef struct vvcg_cu_rec {
   uint8_t cbf;          /* bit0 Y, bit1 Cb, bit2 Cr */
   uint8_t reserved;
   int32_t level_off[3]; /* start of each TB's raster-order levels in the level
-                           pool (int16), -1 when the TB has no levels */
+                           pool (int16), -1 when the TB has no levels. With
+                           VVCG_TOOL_SPARSE_LEVELS the TB is sparse: at
+                           level_off (even) the count n of its coded levels,
+                           one unused int16, then n pairs (raster index,
+                           level) with strictly rising indices; an index
+                           outside the TB or out of order fails the batch
+                           with VVCG_INVALID_INPUT */
 } vvcg_cu_rec;
 
 /* SAO parameters of one colour component of one CTU (filter.rs:1229 SaoType). */

@@ -121,7 +121,7 @@ TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("
                      ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
 
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
-TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM = 16, 32
+TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM, TOOL_SPARSE_LEVELS = 16, 32, 64
 TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
 MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4
@@ -736,38 +736,50 @@ class Context:
         return pred
 
     # -- inter-prediction tools (device int32 arrays; requests are host records) --
-    def _inter_tool(self, fn, reqs, dtype, *args):
+    # The context's stream does not wait for torch's: each call synchronises
+    # the device before (tensors just made or filled by torch) and after
+    # (results read through torch).
+    def _inter_tool(self, fn, reqs, dtype, dev, *args):
+        import torch
+
         reqs = np.ascontiguousarray(reqs, dtype=dtype)
         self._keep = reqs
+        torch.cuda.synchronize(dev)
         self._check(fn(self._h, _ptr(reqs), len(reqs), *args))
+        torch.cuda.synchronize(dev)
 
     def bdof(self, reqs, pred0, pred1, out):
         """BDOF_REQ_DTYPE requests over int32 CUDA tensors (14-bit intermediates in, 8-bit out)."""
-        self._inter_tool(self._L.vvcg_bdof_dev, reqs, BDOF_REQ_DTYPE, _ptr(pred0), _ptr(pred1), _ptr(out), out.numel())
+        self._inter_tool(self._L.vvcg_bdof_dev, reqs, BDOF_REQ_DTYPE, out.device, _ptr(pred0), _ptr(pred1), _ptr(out),
+                         out.numel())
 
     def dmvr(self, ref0, ref1, reqs, mv_out):
         """ref0 / ref1: (H, W) uint8 CUDA tensors; mv_out: int32 CUDA tensor of 4 per request."""
+        import torch
+
         h, w = ref0.shape
         reqs = np.ascontiguousarray(reqs, dtype=DMVR_REQ_DTYPE)
         self._keep = reqs
+        torch.cuda.synchronize(mv_out.device)
         self._check(self._L.vvcg_dmvr_dev(self._h, _ptr(ref0), _ptr(ref1), w, h, ref0.stride(0), _ptr(reqs),
                                           len(reqs), _ptr(mv_out)))
+        torch.cuda.synchronize(mv_out.device)
 
     def affine_mvs(self, reqs, sub_mv, prof):
-        self._inter_tool(self._L.vvcg_affine_mvs_dev, reqs, AFFINE_REQ_DTYPE, _ptr(sub_mv), sub_mv.numel() // 2,
-                         _ptr(prof))
+        self._inter_tool(self._L.vvcg_affine_mvs_dev, reqs, AFFINE_REQ_DTYPE, sub_mv.device, _ptr(sub_mv),
+                         sub_mv.numel() // 2, _ptr(prof))
 
     def prof(self, reqs, src, dmv, out):
-        self._inter_tool(self._L.vvcg_prof_dev, reqs, PROF_REQ_DTYPE, _ptr(src), src.numel(), _ptr(dmv), dmv.numel(),
-                         _ptr(out), out.numel())
+        self._inter_tool(self._L.vvcg_prof_dev, reqs, PROF_REQ_DTYPE, out.device, _ptr(src), src.numel(), _ptr(dmv),
+                         dmv.numel(), _ptr(out), out.numel())
 
     def ciip_blend(self, reqs, inter, intra, out):
-        self._inter_tool(self._L.vvcg_ciip_blend_dev, reqs, CIIP_REQ_DTYPE, _ptr(inter), _ptr(intra), _ptr(out),
-                         out.numel())
+        self._inter_tool(self._L.vvcg_ciip_blend_dev, reqs, CIIP_REQ_DTYPE, out.device, _ptr(inter), _ptr(intra),
+                         _ptr(out), out.numel())
 
     def gpm_blend(self, reqs, pred0, pred1, out):
-        self._inter_tool(self._L.vvcg_gpm_blend_dev, reqs, GPM_REQ_DTYPE, _ptr(pred0), _ptr(pred1), _ptr(out),
-                         out.numel())
+        self._inter_tool(self._L.vvcg_gpm_blend_dev, reqs, GPM_REQ_DTYPE, out.device, _ptr(pred0), _ptr(pred1),
+                         _ptr(out), out.numel())
 
     # -- general-decoder deblocking --
     def deblock_ctu_edges(self, planes, ctu, qp, cells):
@@ -784,7 +796,9 @@ class Context:
         pp = (C.c_void_p * 3)(*[t.data_ptr() for t in planes])
         st = (C.c_uint32 * 3)(*[t.stride(0) for t in planes])
         self._keep = dc
+        torch.cuda.synchronize(planes[0].device)
         self._check(self._L.vvcg_deblock_ctu_edges_dev(self._h, pp, st, w, h, ctu, qp, _ptr(dc)))
+        torch.cuda.synchronize(planes[0].device)
 
     def deblock_general(self, planes, vis_w, vis_h, bit_depth, ctu, cells, ccells, params):
         """In place on planes, (Y, Cb, Cr) int16 CUDA tensors of a 4:2:0

@@ -87,11 +87,16 @@ __device__ __forceinline__ int dot_col(const MatRegs& R, const int16_t* row, int
 }
 
 // Dequantisation (regular or dependent) and 2-D inverse DCT-II of a w x h TB
-// (w, h in {16, 32}) whose int16 raster levels start at `lv`; the residual is
-// stored to `out` (int16, row stride `ostride`). Rows/columns past the last
-// nonzero level hold zeros and are skipped without changing any sum.
-__device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int qp_scaled, int bd,
-                              bool dq, const MatRegs& R, ResidWs& W, int16_t* out, int ostride) {
+// (w, h in {16, 32}) whose levels start at `lv`: int16 raster levels, or with
+// kSparse the sparse form (lv[2..] holds nsparse (raster index, level) int16
+// pairs, 4-byte aligned). The residual is stored to `out` (int16, row
+// stride `ostride`). Rows/columns past the last nonzero level hold zeros and
+// are skipped without changing any sum. Returns false when a sparse entry's
+// index lies outside the TB or does not rise above the entry before it (the
+// entry is skipped).
+template <bool kSparse>
+__device__ bool warp_residual(const int16_t* __restrict__ lv, int w, int h, int qp_scaled, int bd,
+                              bool dq, const MatRegs& R, ResidWs& W, int16_t* out, int ostride, int nsparse) {
   const int lane = threadIdx.x & 31;
   const int n = w * h, lw = ilog2(w), lh = ilog2(h);
   const bool s2 = ((lw + lh) & 1) != 0;
@@ -102,7 +107,8 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
   // round trip), while the coefficient tile is cleared.
   uint4 buf[4];
   const int nvec = n >> 8;  // uint4 per lane: 4 (1024 levels), 2 (512), 1 (256)
-  const bool vec_ok = ((reinterpret_cast<uintptr_t>(lv) & 15) == 0) && (n & 255) == 0;
+  const bool vec_ok = !kSparse && ((reinterpret_cast<uintptr_t>(lv) & 15) == 0) && (n & 255) == 0;
+  bool ok = true;
   if (vec_ok) {
     const uint4* lv4 = reinterpret_cast<const uint4*>(lv);
 #pragma unroll
@@ -128,7 +134,29 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     }
     W.ct[c * kTS + r] = (int16_t)v;
   };
-  if (vec_ok) {
+  if (kSparse) {
+    // (raster index, level) pairs, little-endian int16 pairs read as one
+    // word; the indices must rise strictly (each checked against the entry
+    // before it, so that no two entries land on one coefficient)
+    const uint32_t* pr = reinterpret_cast<const uint32_t*>(lv + 2);
+    int prev_last = -1;
+    for (int base = 0; base < nsparse; base += 32) {
+      const int i = base + lane;
+      const bool have = i < nsparse;
+      const uint32_t e = have ? __ldcs(pr + i) : (uint32_t)n;
+      const int pos = (int)(e & 0xFFFFu), L = (int)(int16_t)(e >> 16);
+      int prev = __shfl_up_sync(0xffffffffu, pos, 1);
+      if (lane == 0) prev = prev_last;
+      if (have) {
+        if (pos >= n || pos <= prev)
+          ok = false;
+        else if (L != 0)
+          put(pos, L);
+      }
+      prev_last = __shfl_sync(0xffffffffu, pos, 31);
+    }
+    ok = __all_sync(0xffffffffu, ok);
+  } else if (vec_ok) {
 #pragma unroll
     for (int v = 0; v < 4; v++)
       if (v < nvec) {
@@ -213,7 +241,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
       int y = (2 * i) >> lw, x = (2 * i) & (w - 1);
       *reinterpret_cast<uint32_t*>(&out[(size_t)y * ostride + x]) = 0;
     }
-    return;
+    return ok;
   }
   // Stage 1, columns (dct.rs:1075-1087): tt[j][i] = clip16((sum_k Mv[k][j] ct[i][k] + 64) >> 7)
   const int ngr = (maxr + 4) >> 2;
@@ -256,6 +284,7 @@ __device__ void warp_residual(const int16_t* __restrict__ lv, int w, int h, int 
     }
   }
   __syncwarp();
+  return ok;
 }
 
 // One warp per coding unit: the residuals of its coded TBs go to the scratch
@@ -273,18 +302,30 @@ k_residual(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, 
   const vvcg_cu_rec rec = P.cus[cu];
   const int gx = cu % P.grid_w, gy = cu / P.grid_w;
   const bool dq = (P.tools & VVCG_TOOL_DEP_QUANT) != 0;
+  const bool sparse = (P.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
   for (int c = 0; c < (P.cf ? 3 : 1); c++) {
     if (!((rec.cbf >> c) & 1)) continue;
     const int off = rec.level_off[c];
     if (off < 0) continue;
     const int w = c ? P.tb_cw : P.tb, h = c ? P.tb_ch : P.tb;
-    if ((uint64_t)off + (uint64_t)(w * h) > n_levels) {
+    int nsp = -1;
+    if (sparse) {  // count at levels[off], pairs from off + 2 (off even)
+      nsp = (off & 1) || (uint64_t)off + 2 > n_levels ? -2 : levels[off];
+      if (nsp < 0 || nsp > w * h || (uint64_t)off + 2 + 2 * (uint64_t)nsp > n_levels) {
+        if (lane == 0) atomicOr(status, kStatusBadRecord);
+        continue;
+      }
+    } else if ((uint64_t)off + (uint64_t)(w * h) > n_levels) {
       if (lane == 0) atomicOr(status, kStatusBadRecord);
       continue;
     }
     const int x0 = c ? gx * P.tb / P.sub_w : gx * P.tb, y0 = c ? gy * P.tb / P.sub_h : gy * P.tb;
     int16_t* out = reinterpret_cast<int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0;
-    warp_residual(levels + off, w, h, c ? P.cqp : P.lqp, P.bd, dq, R, ws[wid], out, P.stride[c]);
+    const bool ok = sparse ? warp_residual<true>(levels + off, w, h, c ? P.cqp : P.lqp, P.bd, dq, R, ws[wid], out,
+                                                 P.stride[c], nsp)
+                           : warp_residual<false>(levels + off, w, h, c ? P.cqp : P.lqp, P.bd, dq, R, ws[wid], out,
+                                                  P.stride[c], 0);
+    if (!ok && lane == 0) atomicOr(status, kStatusBadRecord);
   }
 }
 

@@ -153,6 +153,19 @@ namespace {
 std::mutex g_tables_mu;
 bool g_tables_ready[64] = {false};
 
+// The int16 words a TB's levels take at off: its n coefficients when dense;
+// when sparse the count word, one unused word and count (index, level)
+// pairs. Zero for a malformed record: past the array, an odd sparse offset
+// or a count outside 0..n. The index range of each pair is checked on the
+// device, where the pairs are read.
+uint64_t tb_level_extent(const int16_t* levels, uint64_t num_levels, uint64_t off, uint64_t n, bool sparse) {
+  if (!sparse) return off + n <= num_levels ? n : 0;
+  if ((off & 1) || off + 2 > num_levels) return 0;
+  const int cnt = levels[off];
+  if (cnt < 0 || (uint64_t)cnt > n || off + 2 + 2 * (uint64_t)cnt > num_levels) return 0;
+  return 2 + 2 * (uint64_t)cnt;
+}
+
 // cuTensorMapEncodeTiled, fetched from the driver through the runtime (no
 // link-time dependency on libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -528,12 +541,13 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     if (filt && (!b->ctus || (uint64_t)d.ctu_offset + (uint64_t)cw_ * ch_ > b->num_ctus))
       return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU filter records out of range", i);
     // level offsets
+    const bool sparse = (d.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
     for (uint32_t k = 0; k < gw * gh; k++) {
       const vvcg_cu_rec& r = b->cus[d.cu_offset + k];
       for (int c = 0; c < (cf ? 3 : 1); c++) {
         if (!((r.cbf >> c) & 1) || r.level_off[c] < 0) continue;
         uint64_t n = c ? (uint64_t)tcw * tch : (uint64_t)tb * tb;
-        if (!b->levels || (uint64_t)r.level_off[c] + n > b->num_levels)
+        if (!b->levels || !tb_level_extent(b->levels, b->num_levels, (uint64_t)r.level_off[c], n, sparse))
           return fail(ctx, VVCG_INVALID_INPUT, "picture %u CU %u: level offset out of range", i, k);
       }
     }
@@ -883,7 +897,7 @@ vvcg_status vvcg_batch_sync(vvcg_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream), "synchronize");
   if (status & kStatusTimeout)
     return fail(ctx, VVCG_TIMEOUT, "a wavefront wait gave up after %u polls", ctx->spin_limit);
-  if (status & kStatusBadRecord) return fail(ctx, VVCG_INVALID_INPUT, "a level offset was out of range");
+  if (status & kStatusBadRecord) return fail(ctx, VVCG_INVALID_INPUT, "a level offset or sparse level entry was out of range");
   if (status & kStatusAlfAbort)
     return fail(ctx, VVCG_INVALID_INPUT,
                 "fixed-filter ALF reached a class >= 16, where the reference aborts");
@@ -1006,16 +1020,21 @@ vvcg_status vvcg_decode_batch_pipelined(vvcg_ctx* ctx, const vvcg_batch* b, cons
       const int cf = d.chroma_format, sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
       const uint64_t nch = cf ? (uint64_t)std::max<int>(tb / sw, 2) * std::max<int>(tb / sh, 2) : 0;
       const uint64_t nlc[3] = {(uint64_t)tb * tb, nch, nch};
+      const bool sparse = (d.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
       for (uint32_t c = 0; c < ncu; c++) {
         const vvcg_cu_rec& r = b->cus[d.cu_offset + c];
         for (int q = 0; q < (cf ? 3 : 1); q++)
           if (((r.cbf >> q) & 1) && r.level_off[q] >= 0) {
-            lv0 = std::min<uint64_t>(lv0, (uint64_t)r.level_off[q]);
-            lv1 = std::max<uint64_t>(lv1, (uint64_t)r.level_off[q] + nlc[q]);
+            const uint64_t off = (uint64_t)r.level_off[q];
+            const uint64_t ext = b->levels ? tb_level_extent(b->levels, b->num_levels, off, nlc[q], sparse) : 0;
+            if (!ext) return fail(ctx, VVCG_INVALID_INPUT, "picture %u CU %u: level offset out of range", i, c);
+            lv0 = std::min<uint64_t>(lv0, off);
+            lv1 = std::max<uint64_t>(lv1, off + ext);
           }
       }
     }
     if (lv0 == UINT64_MAX) lv0 = lv1 = 0;
+    lv0 &= ~1ull;  // sparse TBs start at even offsets, also after rebasing
     if (ct0 == UINT64_MAX) ct0 = ct1 = 0;
     if (lv1 > b->num_levels) return fail(ctx, VVCG_INVALID_INPUT, "chunk %u: level offsets out of range", k);
     cpics[k].assign(b->pics + p0, b->pics + p1);
@@ -2249,6 +2268,8 @@ extern "C" vvcg_status vvcg_encode_batch(vvcg_ctx* ctx, const vvcg_pic_desc* pic
   for (uint32_t i = 0; i < num_pics; i++) {
     if (d[i].tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF))
       return fail(ctx, VVCG_INVALID_INPUT, "picture %u: the encoder does not apply SAO or ALF", i);
+    if (d[i].tools & VVCG_TOOL_SPARSE_LEVELS)
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: the encoder writes dense levels", i);
     if (d[i].slice_qp > 63) return fail(ctx, VVCG_INVALID_INPUT, "picture %u: slice QP above 63", i);
     for (int c = 0; c < (d[i].chroma_format ? 3 : 1); c++)
       if (!src[i * 3 + c].data) return fail(ctx, VVCG_INVALID_INPUT, "picture %u: missing source plane %d", i, c);
@@ -2744,6 +2765,6 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
   SCK(cudaStreamSynchronize(s), "synchronize");
   if (status & kStatusTimeout)
     return static_fail(err, err_cap, VVCG_TIMEOUT, "a wavefront wait gave up after %u polls", kDefaultSpinLimit);
-  if (status & kStatusBadRecord) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "a level offset was out of range");
+  if (status & kStatusBadRecord) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "a level offset or sparse level entry was out of range");
   return VVCG_OK;
 }

@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import (APS_DTYPE, CTU_DTYPE, CU_DTYPE, PIC_DTYPE, TOOL_ALF, TOOL_DEBLOCK, TOOL_DEP_QUANT,
-               TOOL_ENC_CCLM, TOOL_ENC_FULL_INTRA, TOOL_SAO, chroma_dims)
+               TOOL_ENC_CCLM, TOOL_ENC_FULL_INTRA, TOOL_SAO, TOOL_SPARSE_LEVELS, chroma_dims)
 
 
 def seed_for(stream: int, frame: int) -> int:
@@ -656,6 +656,90 @@ def compact_levels(p, cus, levels):
             out[new[k, c][:, None] + ar] = levels[lo[k, c][:, None] + ar]
     cus["level_off"] = np.where(coded, new, -1).astype(np.int32)
     return cus, out
+
+
+def _tb_sizes(p):
+    """Levels per TB of a frame-path picture: (luma, Cb, Cr)."""
+    cf = int(p["chroma_format"])
+    tb = min(1 << int(p["ctu_log2"]), 32)
+    cw, ch = chroma_dims(tb, tb, cf)
+    nc = max(cw, 2) * max(ch, 2) if cf else 0
+    return tb, (tb * tb, nc, nc)
+
+
+def sparsify(pics, cus, levels):
+    """The batch with every picture's TBs in the sparse level form
+    (TOOL_SPARSE_LEVELS): per coded TB, at an even offset, the count of its
+    nonzero levels, one unused word, then (raster index, level) int16 pairs
+    with rising indices. Returns (pics, cus, levels); the inputs are not
+    changed."""
+    pics = np.array(pics, PIC_DTYPE, copy=True)
+    cus = np.array(cus, CU_DTYPE, copy=True)
+    levels = np.asarray(levels, np.int16)
+    lo = cus["level_off"].astype(np.int64)
+    new_off = np.full(lo.shape, -1, np.int64)
+    blocks, at = [], 0
+    for i in range(len(pics)):
+        p = pics[i]
+        tb, sizes = _tb_sizes(p)
+        c0 = int(p["cu_offset"])
+        ncu = (int(p["width"]) // tb) * (int(p["height"]) // tb)
+        cbf = cus["cbf"][c0:c0 + ncu]
+        for c in range(3 if int(p["chroma_format"]) else 1):
+            coded = ((cbf >> c) & 1).astype(bool) & (lo[c0:c0 + ncu, c] >= 0)
+            k = np.nonzero(coded)[0]
+            if not len(k):
+                continue
+            g = levels[lo[c0 + k, c][:, None] + np.arange(sizes[c])[None, :]]
+            nz = g != 0
+            cnt = nz.sum(1)
+            words = 2 + 2 * cnt
+            start = np.cumsum(words) - words
+            blk = np.zeros(int(words.sum()), np.int16)
+            blk[start] = cnt
+            r, col = np.nonzero(nz)
+            rank = np.arange(len(r)) - (np.cumsum(cnt) - cnt)[r]
+            at_e = start[r] + 2 + 2 * rank
+            blk[at_e] = col
+            blk[at_e + 1] = g[r, col]
+            new_off[c0 + k, c] = at + start
+            blocks.append(blk)
+            at += len(blk)
+        pics["tools"][i] = int(p["tools"]) | TOOL_SPARSE_LEVELS
+    if at >= 1 << 31:
+        raise ValueError("sparse level pool exceeds int32 offsets")
+    cus["level_off"] = new_off.astype(np.int32)
+    return pics, cus, np.concatenate(blocks) if blocks else np.zeros(0, np.int16)
+
+
+def densify(pics, cus, levels):
+    """The inverse of sparsify: raster-order TBs, TOOL_SPARSE_LEVELS cleared."""
+    pics = np.array(pics, PIC_DTYPE, copy=True)
+    cus = np.array(cus, CU_DTYPE, copy=True)
+    levels = np.asarray(levels, np.int16)
+    lo = cus["level_off"].astype(np.int64)
+    new_off = np.full(lo.shape, -1, np.int64)
+    out, at = [], 0
+    for i in range(len(pics)):
+        p = pics[i]
+        tb, sizes = _tb_sizes(p)
+        c0 = int(p["cu_offset"])
+        ncu = (int(p["width"]) // tb) * (int(p["height"]) // tb)
+        for k in range(ncu):
+            for c in range(3 if int(p["chroma_format"]) else 1):
+                o = int(lo[c0 + k, c])
+                if o < 0 or not (int(cus["cbf"][c0 + k]) >> c) & 1:
+                    continue
+                tbl = np.zeros(sizes[c], np.int16)
+                n = int(levels[o])
+                pairs = levels[o + 2:o + 2 + 2 * n].reshape(-1, 2)
+                tbl[pairs[:, 0].astype(np.int64)] = pairs[:, 1]
+                new_off[c0 + k, c] = at
+                out.append(tbl)
+                at += sizes[c]
+        pics["tools"][i] = int(p["tools"]) & ~TOOL_SPARSE_LEVELS
+    cus["level_off"] = new_off.astype(np.int32)
+    return pics, cus, np.concatenate(out) if out else np.zeros(0, np.int16)
 
 
 def decoder_picture(index, p_enc, cus, levels, seed):
