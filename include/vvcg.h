@@ -75,7 +75,24 @@ enum {
   VVCG_TOOL_ENC_FULL_INTRA = 1u << 4, /* all 7 searched luma modes, not only Planar / DC */
   VVCG_TOOL_ENC_CCLM = 1u << 5,       /* chroma mode by SAD among DM and the 3 CCLM modes */
   /* decoder: the picture's level_off values index sparse TBs (see vvcg_cu_rec) */
-  VVCG_TOOL_SPARSE_LEVELS = 1u << 6
+  VVCG_TOOL_SPARSE_LEVELS = 1u << 6,
+  /* decoder: the CU records carry per-TB transform choices in tu_tools (the
+   * strict 8-bit decoder's transform skip, mts_idx and lfnst_idx,
+   * slice.rs:458-627); not with VVCG_TOOL_SPARSE_LEVELS */
+  VVCG_TOOL_TU_TOOLS = 1u << 7
+};
+
+/* vvcg_cu_rec.tu_tools of a picture with VVCG_TOOL_TU_TOOLS (ignored
+ * otherwise): transform skip per component, and the luma TB's explicit MTS
+ * index (mts_types, slice.rs:647-656) or LFNST index (LFNST set from the
+ * CU's luma mode). mts_idx and lfnst_idx are not both nonzero, and neither
+ * is with luma transform skip. */
+enum {
+  VVCG_CU_TS_Y = 1u << 0,
+  VVCG_CU_TS_CB = 1u << 1,
+  VVCG_CU_TS_CR = 1u << 2,
+  VVCG_CU_MTS_SHIFT = 3,   /* bits 3..5: mts_idx 0..4 */
+  VVCG_CU_LFNST_SHIFT = 6  /* bits 6..7: lfnst_idx 0..2 */
 };
 
 /* One picture of the 8..12-bit frame path: the inputs of
@@ -105,7 +122,7 @@ typedef struct vvcg_cu_rec {
   uint8_t luma_mode;    /* IntraPredModeY, 0..66 */
   uint8_t chroma_mode;  /* 0..66, or 81 / 82 / 83 for CCLM LM / LM-L / LM-T */
   uint8_t cbf;          /* bit0 Y, bit1 Cb, bit2 Cr */
-  uint8_t reserved;
+  uint8_t tu_tools;     /* VVCG_TU_* with VVCG_TOOL_TU_TOOLS, else 0 */
   int32_t level_off[3]; /* start of each TB's raster-order levels in the level
                            pool (int16), -1 when the TB has no levels. With
                            VVCG_TOOL_SPARSE_LEVELS the TB is sparse: at

@@ -116,6 +116,8 @@ def _declare(L):
     L.orc_deblock_general.restype = None
     L.orc_inter_ctu_deblock.argtypes = [vp, vp, vp, i, i, i, i, i, i, vp]
     L.orc_inter_ctu_deblock.restype = None
+    L.orc_strict_encode.argtypes = [vp, vp, vp, i, i, i, i, vp, vp, vp, vp, vp, vp]
+    L.orc_strict_decode.argtypes = [vp, vp, C.c_uint64, i, i, i, i, vp, vp, vp]
     L.orc_bdof.argtypes = [vp, vp, i, i, vp]
     L.orc_bdof.restype = None
     L.orc_dmvr.argtypes = [vp, vp, i, i, i, i, i, i, i, vp]
@@ -516,7 +518,7 @@ def bi_average_8(p0, p1, bcw):
 
 # Record layouts of include/vvcg.h, as numpy structured dtypes.
 CU_DTYPE = np.dtype([("luma_mode", "u1"), ("chroma_mode", "u1"), ("cbf", "u1"),
-                     ("reserved", "u1"), ("level_off", "<i4", (3,))])
+                     ("tu_tools", "u1"), ("level_off", "<i4", (3,))])
 SAO_DTYPE = np.dtype([("type", "u1"), ("band_or_class", "u1"), ("offsets", "i1", (4,))])
 CTU_DTYPE = np.dtype([("sao", SAO_DTYPE, (3,)), ("alf_luma", "u1"), ("reserved", "u1")])
 PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("visible_width", "<u4"),
@@ -563,6 +565,41 @@ def encode_frame(y, u, v, bd, qp, ctu_log2=5, opts=OPT_FULL_INTRA | OPT_DEBLOCK,
     if rc:
         raise ValueError(f"encode_frame rejected ({rc})")
     return cus, levels[: used.value].copy(), (ry, ru, rv)
+
+
+def strict_encode(y, u, v, qp, ctu_log2=5):
+    """slice::encode_picture's decisions and reconstruction (slice.rs:325-455,
+    without the CABAC writes) on an 8-bit 4:2:0 picture of coded size.
+
+    Returns (cus, levels, (rec_y, rec_u, rec_v)): CU_DTYPE records in
+    tb-grid raster order with the syntax decode_picture parses (modes, cbf,
+    tu_tools: transform skip per coded TB, mts_idx, lfnst_idx), dense levels.
+    """
+    y, u, v = (np.ascontiguousarray(a, dtype=np.uint8) for a in (y, u, v))
+    h, w = y.shape
+    cus = np.zeros((h // 32) * (w // 32), dtype=CU_DTYPE)
+    levels = np.zeros(w * h * 3 // 2 + 64, np.int16)
+    used = C.c_uint64(0)
+    ry, ru, rv = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
+    rc = lib().orc_strict_encode(_p(y), _p(u), _p(v), w, h, qp, ctu_log2, _p(cus), _p(levels), C.byref(used),
+                                 _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"strict_encode rejected ({rc})")
+    return cus, levels[:used.value].copy(), (ry, ru, rv)
+
+
+def strict_decode(cus, levels, w, h, qp, ctu_log2=5):
+    """slice::decode_picture's reconstruction (slice.rs:458-627) from parsed
+    records (as strict_encode returns them); returns (y, u, v) uint8."""
+    cus = np.ascontiguousarray(cus, dtype=CU_DTYPE)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    ry = np.zeros((h, w), np.uint8)
+    ru = np.zeros((h // 2, w // 2), np.uint8)
+    rv = np.zeros((h // 2, w // 2), np.uint8)
+    rc = lib().orc_strict_decode(_p(cus), _p(levels), levels.size, w, h, qp, ctu_log2, _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"strict_decode rejected ({rc})")
+    return ry, ru, rv
 
 
 def recon_frame(pic, cus, levels, ctus, aps=None):

@@ -140,6 +140,16 @@ void gen_intra_predict(const vvcg_gen_intra_state& st, const vvcg_gen_intra_req&
 void luma_intra_search_8(const Plane8& recon, const Plane8& src, int bx, int by, int w, int h, const uint8_t mpm[6],
                          bool mpm_only, bool mrl, int ctu_size, int* best_mode, int* best_mrl, uint64_t* best_sad);
 void predict_luma_8(const Plane8& recon, int bx, int by, int w, int h, int mode, int mrl, int ctu_size, int32_t* out);
+// predict.rs:2619 predict_block: Planar / DC / angular of one component block on an 8-bit plane.
+void predict_block_8(const Plane8& recon, int bx, int by, int w, int h, bool is_luma, int mode, int32_t* out);
+// slice.rs:325-455 encode_picture (decisions and reconstruction; no CABAC) and
+// slice.rs:458-627 decode_picture (reconstruction from parsed syntax) of the
+// strict 8-bit 4:2:0 intra profile (orc_strict.cpp). Records as vvcg_cu_rec
+// documents for VVCG_TOOL_TU_TOOLS pictures; planes row-major, stride = width.
+int strict_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp, int ctu_log2,
+                  vvcg_cu_rec* cus, int16_t* levels, uint64_t* num_levels, uint8_t* ry, uint8_t* ru, uint8_t* rv);
+int strict_decode(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                  int ctu_log2, uint8_t* ry, uint8_t* ru, uint8_t* rv);
 // The GPU encoder's CTU full search (orc_search.cpp; no reference counterpart).
 void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, const uint8_t* cand,
                 uint32_t lambda_q8, uint32_t* cost, uint32_t split_cost[6], int* split, int* cu_mode, int modes[4]);

@@ -293,3 +293,14 @@ extern "C" void orc_sao_bounded(const uint16_t* src, uint16_t* dst, int pw, int 
   }
   orc::sao_plane_bounded_16(src, dst, pw, pw, ph, vis_w, vis_h, bd, ctu, ctu_cols, s.data());
 }
+
+// slice.rs:325-455 / :458-627: the strict 8-bit profile's encoder decisions and decoder.
+extern "C" int orc_strict_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp,
+                                 int ctu_log2, void* cus, int16_t* levels, uint64_t* num_levels, uint8_t* ry,
+                                 uint8_t* ru, uint8_t* rv) {
+  return orc::strict_encode(y, u, v, w, h, qp, ctu_log2, (vvcg_cu_rec*)cus, levels, num_levels, ry, ru, rv);
+}
+extern "C" int orc_strict_decode(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                                 int ctu_log2, uint8_t* ry, uint8_t* ru, uint8_t* rv) {
+  return orc::strict_decode((const vvcg_cu_rec*)cus, levels, num_levels, w, h, qp, ctu_log2, ry, ru, rv);
+}

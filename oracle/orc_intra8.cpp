@@ -8,7 +8,8 @@
 //   predict_planar / predict_dc         predict.rs:1688-1736
 //   apply_pdpc                          predict.rs:1739-1754
 //   predict_angular_with_params_bd      predict.rs:1776-1958
-//   predict_block / predict_block_full  predict.rs:2619-2699 (luma modes)
+//   predict_block / predict_block_full  predict.rs:2619-2699 (predict_block for
+//                                       both components, the full form for luma)
 //   choose_luma_intra_pred_mode         predict.rs:2737-2801
 // and the MRL candidate loop of encode_picture_multitool (slice.rs:2698-2731).
 #include <stdlib.h>
@@ -309,6 +310,22 @@ std::vector<int> predict_full(const Plane8& r, int bx, int by, int w, int h, int
   MrlRefs m = gather_mrl(r, bx, by, w, h, mrl, ctu);
   AngularParams P = init_angular_params(mode, w, h, w, h, true, m.mrl_idx, false);
   return angular(m, w, h, true, P, 8);
+}
+
+// predict.rs:2619-2650 predict_block for either component: Planar / DC with
+// the [1 2 1] filter on luma only (uses_reference_filter, :1287-1293) and
+// PDPC, angular through predict_angular (:1962-1987) with is_luma selecting
+// the interpolation and reference-filter rules.
+std::vector<int> predict_block8(const Plane8& r, int bx, int by, int w, int h, bool is_luma, int mode) {
+  Refs8 refs = gather(r, bx, by, w, h);
+  if (mode == PLANAR || mode == DC) {
+    const Refs8 used = (mode == PLANAR && is_luma && w * h > 32) ? filtered(refs) : refs;
+    std::vector<int> p = mode == PLANAR ? planar(used, w, h) : dc(used, w, h);
+    pdpc(p, used, w, h);
+    return p;
+  }
+  AngularParams P = init_angular_params(mode, w, h, w, h, is_luma, 0, false);
+  return angular(from_refs(P.ref_filter_flag ? filtered(refs) : refs), w, h, is_luma, P, 8);
 }
 
 uint64_t sad_of(const std::vector<int>& p, const Plane8& src, int bx, int by, int w, int h) {
@@ -624,6 +641,12 @@ void luma_intra_search_8(const Plane8& recon, const Plane8& src, int bx, int by,
   *best_mode = bm;
   *best_mrl = bmrl;
   *best_sad = bc;
+}
+
+// predict_block (predict.rs:2619) of one component block into out (w * h).
+void predict_block_8(const Plane8& recon, int bx, int by, int w, int h, bool is_luma, int mode, int32_t* out) {
+  std::vector<int> p = predict_block8(recon, bx, by, w, h, is_luma, mode);
+  std::copy(p.begin(), p.end(), out);
 }
 
 // predict_block_full (predict.rs:2655) of one luma mode into out (w * h).

@@ -25,7 +25,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
 
 # ------------------------------------------------------------------ records --
 CU_DTYPE = np.dtype([("luma_mode", "u1"), ("chroma_mode", "u1"), ("cbf", "u1"),
-                     ("reserved", "u1"), ("level_off", "<i4", (3,))])
+                     ("tu_tools", "u1"), ("level_off", "<i4", (3,))])
 SAO_DTYPE = np.dtype([("type", "u1"), ("band_or_class", "u1"), ("offsets", "i1", (4,))])
 CTU_DTYPE = np.dtype([("sao", SAO_DTYPE, (3,)), ("alf_luma", "u1"), ("reserved", "u1")])
 PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("visible_width", "<u4"),
@@ -121,7 +121,8 @@ TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("
                      ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
 
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
-TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM, TOOL_SPARSE_LEVELS = 16, 32, 64
+TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM, TOOL_SPARSE_LEVELS, TOOL_TU_TOOLS = 16, 32, 64, 128
+CU_TS_Y, CU_TS_CB, CU_TS_CR, CU_MTS_SHIFT, CU_LFNST_SHIFT = 1, 2, 4, 3, 6
 TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
 MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4

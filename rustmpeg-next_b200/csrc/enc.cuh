@@ -198,7 +198,7 @@ __device__ void encode_cu(const DevPic& P, int gx, int gy, EncWs& W) {
     r.luma_mode = (uint8_t)luma_mode;
     r.chroma_mode = (uint8_t)chroma_mode;
     r.cbf = (uint8_t)((cbf_y ? 1 : 0) | (cbf_c[0] ? 2 : 0) | (cbf_c[1] ? 4 : 0));
-    r.reserved = 0;
+    r.tu_tools = 0;
     r.level_off[0] = cbf_y ? off0 : -1;
     r.level_off[1] = cbf_c[0] ? off0 + tb * tb : -1;
     r.level_off[2] = cbf_c[1] ? off0 + tb * tb + cw * ch : -1;

@@ -303,8 +303,11 @@ k_residual(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, 
   const int gx = cu % P.grid_w, gy = cu / P.grid_w;
   const bool dq = (P.tools & VVCG_TOOL_DEP_QUANT) != 0;
   const bool sparse = (P.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
+  // TBs with transform skip, MTS or LFNST belong to k_residual_tools
+  const uint32_t tu_tools = (P.tools & VVCG_TOOL_TU_TOOLS) ? rec.tu_tools : 0;
   for (int c = 0; c < (P.cf ? 3 : 1); c++) {
     if (!((rec.cbf >> c) & 1)) continue;
+    if (((tu_tools >> c) & 1) || (c == 0 && (tu_tools >> VVCG_CU_MTS_SHIFT))) continue;
     const int off = rec.level_off[c];
     if (off < 0) continue;
     const int w = c ? P.tb_cw : P.tb, h = c ? P.tb_ch : P.tb;

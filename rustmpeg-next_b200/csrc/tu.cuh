@@ -427,9 +427,10 @@ __device__ void tu_forward_transform(int32_t* A, int32_t* B, const TuShape& S, i
 }
 
 // One warp: levels -> residual of one unit (decode_general.rs:4100-4199 and
-// the BDPCM of :4055-4060).
+// the BDPCM of :4055-4060). The residual goes to `out` with row stride
+// `ostride` (0: the unit's width).
 __device__ void warp_tu_inverse(const vvcg_tu_rec& r, const int16_t* __restrict__ in,
-                                int16_t* __restrict__ out, int32_t* A, int32_t* B, int lane) {
+                                int16_t* __restrict__ out, int32_t* A, int32_t* B, int lane, int ostride = 0) {
   TuShape S;
   tu_shape(r, S);
   const int bd = r.bit_depth, qp = r.qp;
@@ -472,7 +473,11 @@ __device__ void warp_tu_inverse(const vvcg_tu_rec& r, const int16_t* __restrict_
     }
     __syncwarp();
   }
-  for (int i = lane; i < S.n; i += 32) out[i] = (int16_t)A[i];
+  if (ostride == 0)
+    for (int i = lane; i < S.n; i += 32) out[i] = (int16_t)A[i];
+  else
+    for (int i = lane; i < S.n; i += 32) out[(size_t)(i >> S.lw) * ostride + (i & (S.w - 1))] = (int16_t)A[i];
+  __syncwarp();
 }
 
 // One warp: residual -> levels of one unit (slice.rs:690-760, level side).
@@ -529,6 +534,66 @@ k_tu(const vvcg_tu_rec* __restrict__ recs, const uint32_t* __restrict__ idx, uin
 template <int kMax, int kWarps>
 constexpr size_t tu_smem_bytes() {
   return (size_t)kWarps * 2 * (kMax + kTuPad) * sizeof(int32_t);
+}
+
+// True when TB c of a coding unit with tu_tools `t` leaves the frame path's
+// DCT-2 residual kernel: transform skip, or (luma) explicit MTS / LFNST.
+__host__ __device__ __forceinline__ bool tb_uses_tu_tools(uint32_t t, int c) {
+  return ((t >> c) & 1) || (c == 0 && (t >> VVCG_CU_MTS_SHIFT) != 0);
+}
+
+constexpr int kResToolWarps = 4;
+
+// The frame path's TBs with per-TB transform choices (pictures with
+// VVCG_TOOL_TU_TOOLS; slice.rs:1050-1097 reconstruct_block, residual part):
+// one warp per coding unit runs each such coded TB through the TU path above
+// (transform-skip dequantisation, or dequantisation, inverse LFNST with the
+// CU's luma mode, inverse DCT-2 / DST-7 / DCT-8 with the zero-out) into the
+// scratch planes, where the reconstruction adds it to the prediction.
+// Records outside the ranges of vvcg_cu_rec.tu_tools, or with levels past the
+// pool, set the bad-record status and are skipped.
+// Grid: (ceil(max CUs per picture / kResToolWarps), pictures).
+__global__ void __launch_bounds__(kResToolWarps * 32)
+k_residual_tools(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels,
+                 uint32_t* status) {
+  __shared__ __align__(16) int32_t ws[kResToolWarps][2][1024 + kTuPad];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const DevPic& P = pics[blockIdx.y];
+  if (!(P.tools & VVCG_TOOL_TU_TOOLS)) return;
+  const int cu = blockIdx.x * kResToolWarps + wid;
+  if (cu >= P.grid_w * P.grid_h) return;
+  const vvcg_cu_rec rec = P.cus[cu];
+  const uint32_t t = rec.tu_tools;
+  if (!t) return;
+  const int mts = (t >> VVCG_CU_MTS_SHIFT) & 7, lfnst = t >> VVCG_CU_LFNST_SHIFT;
+  const bool bad_tools = mts > 4 || lfnst > 2 || (mts && lfnst) || ((t & VVCG_CU_TS_Y) && (mts || lfnst)) ||
+                         (P.tools & VVCG_TOOL_SPARSE_LEVELS);
+  const int gx = cu % P.grid_w, gy = cu / P.grid_w;
+  for (int c = 0; c < (P.cf ? 3 : 1); c++) {
+    if (!tb_uses_tu_tools(t, c) || !((rec.cbf >> c) & 1)) continue;
+    const int off = rec.level_off[c];
+    if (off < 0) continue;
+    const int w = c ? P.tb_cw : P.tb, h = c ? P.tb_ch : P.tb;
+    if (bad_tools || (uint64_t)off + (uint64_t)(w * h) > n_levels) {
+      if (lane == 0) atomicOr(status, kStatusBadRecord);
+      continue;
+    }
+    const bool ts = (t >> c) & 1;
+    const int q = c ? P.cqp : P.lqp;
+    vvcg_tu_rec r;
+    r.log2_w = (uint8_t)ilog2(w);
+    r.log2_h = (uint8_t)ilog2(h);
+    r.bit_depth = (uint8_t)P.bd;
+    r.qp = (uint8_t)(ts ? max(4, q) : q);
+    r.flags = ts ? VVCG_TU_TRANSFORM_SKIP : ((P.tools & VVCG_TOOL_DEP_QUANT) ? VVCG_TU_DEP_QUANT : 0);
+    r.mts_idx = (uint8_t)(c ? 0 : mts);
+    r.lfnst_idx = (uint8_t)(c ? 0 : lfnst);
+    r.lfnst_mode = rec.luma_mode;
+    r.in_off = r.out_off = 0;
+    const int x0 = c ? gx * P.tb / P.sub_w : gx * P.tb, y0 = c ? gy * P.tb / P.sub_h : gy * P.tb;
+    int16_t* out = reinterpret_cast<int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0;
+    warp_tu_inverse(r, levels + off, out, ws[wid][0], ws[wid][1], lane, P.stride[c]);
+  }
 }
 
 }  // namespace vvcg

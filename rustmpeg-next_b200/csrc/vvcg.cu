@@ -107,6 +107,7 @@ struct vvcg_ctx {
   int num_sms = 0;
   // batch state
   bool prepared = false;
+  bool any_tu_tools = false;  // a prepared picture carries VVCG_TOOL_TU_TOOLS
   uint32_t num_pics = 0;
   std::vector<PicLayout> layout;
   std::vector<DevPic> pics;
@@ -158,6 +159,16 @@ bool g_tables_ready[64] = {false};
 // pairs. Zero for a malformed record: past the array, an odd sparse offset
 // or a count outside 0..n. The index range of each pair is checked on the
 // device, where the pairs are read.
+// Why a CU's tu_tools byte is outside vvcg_cu_rec's ranges, or null.
+const char* cu_tu_tools_error(uint32_t t) {
+  const uint32_t mts = (t >> VVCG_CU_MTS_SHIFT) & 7, lfnst = t >> VVCG_CU_LFNST_SHIFT;
+  if (mts > 4) return "mts_idx above 4";
+  if (lfnst > 2) return "lfnst_idx above 2";
+  if (mts && lfnst) return "MTS combined with LFNST";
+  if ((t & VVCG_CU_TS_Y) && (mts || lfnst)) return "luma transform skip with MTS or LFNST";
+  return nullptr;
+}
+
 uint64_t tb_level_extent(const int16_t* levels, uint64_t num_levels, uint64_t off, uint64_t n, bool sparse) {
   if (!sparse) return off + n <= num_levels ? n : 0;
   if ((off & 1) || off + 2 > num_levels) return 0;
@@ -513,6 +524,7 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   ctx->num_ctus = b->num_ctus;
   ctx->num_aps = b->num_aps;
   uint64_t plane_samples = 0;
+  bool any_tools = false;
   for (uint32_t i = 0; i < np; i++) {
     const vvcg_pic_desc& d = b->pics[i];
     if (d.ctu_log2 < 5 || d.ctu_log2 > 7)
@@ -540,6 +552,15 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     const bool filt = d.tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF);
     if (filt && (!b->ctus || (uint64_t)d.ctu_offset + (uint64_t)cw_ * ch_ > b->num_ctus))
       return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU filter records out of range", i);
+    const bool tu_tools = (d.tools & VVCG_TOOL_TU_TOOLS) != 0;
+    if (tu_tools && (d.tools & VVCG_TOOL_SPARSE_LEVELS))
+      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: per-TB transform tools need dense levels", i);
+    if (tu_tools)
+      for (uint32_t k = 0; k < gw * gh; k++) {
+        const char* why = cu_tu_tools_error(b->cus[d.cu_offset + k].tu_tools);
+        if (why) return fail(ctx, VVCG_INVALID_INPUT, "picture %u CU %u: %s", i, k, why);
+      }
+    any_tools |= tu_tools;
     // level offsets
     const bool sparse = (d.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
     for (uint32_t k = 0; k < gw * gh; k++) {
@@ -724,6 +745,7 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
   // no wait here: the copies read pinned staging (or pageable memory the
   // driver has already staged), and the next prepare waits for the stream
   // before it reuses the staging buffer
+  ctx->any_tu_tools = any_tools;
   ctx->prepared = true;
   return VVCG_OK;
 }
@@ -772,6 +794,13 @@ vvcg_status enqueue_run(vvcg_ctx* ctx, uint32_t mask, uint32_t epoch, bool clear
                                 ctx->num_levels, ctrl + 1);
     CK(cudaGetLastError(), "residual launch");
     (*launches)++;
+    if (ctx->any_tu_tools) {  // TBs with transform skip, MTS or LFNST
+      k_residual_tools<<<dim3((max_cus + kResToolWarps - 1) / kResToolWarps, ctx->num_pics), kResToolWarps * 32, 0,
+                         ctx->stream>>>((const DevPic*)ctx->d_pics.p, (const int16_t*)ctx->d_levels.p,
+                                        ctx->num_levels, ctrl + 1);
+      CK(cudaGetLastError(), "residual (TU tools) launch");
+      (*launches)++;
+    }
     // prediction + reconstruction in CTU wavefront order
     const uint32_t n = (uint32_t)ctx->items.size();
     const size_t wave_smem = kWarpsPerCta * sizeof(WaveWs);
@@ -2633,6 +2662,8 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
   if (d.tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF))
     return static_fail(err, err_cap, VVCG_INVALID_INPUT,
                        "SAO and ALF need a second set of planes (use vvcg_decode_batch)");
+  if ((d.tools & VVCG_TOOL_TU_TOOLS) && (d.tools & VVCG_TOOL_SPARSE_LEVELS))
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "per-TB transform tools need dense levels");
   const int tb = std::min<int>(ctu, 32);
   const int cf = d.chroma_format;
   const int sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;
@@ -2741,6 +2772,11 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
   k_residual<<<dim3((ncus + kWarpsPerCta - 1) / kWarpsPerCta, 1), kWarpsPerCta * 32, 0, s>>>(
       d_pic, levels, num_levels, ctrl + 1);
   SCK(cudaGetLastError(), "residual launch");
+  if (d.tools & VVCG_TOOL_TU_TOOLS) {
+    k_residual_tools<<<dim3((ncus + kResToolWarps - 1) / kResToolWarps, 1), kResToolWarps * 32, 0, s>>>(
+        d_pic, levels, num_levels, ctrl + 1);
+    SCK(cudaGetLastError(), "residual (TU tools) launch");
+  }
   const uint32_t warps = (uint32_t)S->num_sms * std::max(1, S->recon_ctas_per_sm) * kWarpsPerCta;
   const uint32_t grid = (std::min<uint32_t>((uint32_t)P.ctu_h, warps) + kWarpsPerCta - 1) / kWarpsPerCta;
   const uint32_t epoch = 1;  // progress lines were cleared above

@@ -17,7 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 from . import (APS_DTYPE, CTU_DTYPE, CU_DTYPE, PIC_DTYPE, TOOL_ALF, TOOL_DEBLOCK, TOOL_DEP_QUANT,
-               TOOL_ENC_CCLM, TOOL_ENC_FULL_INTRA, TOOL_SAO, TOOL_SPARSE_LEVELS, chroma_dims)
+               TOOL_ENC_CCLM, TOOL_ENC_FULL_INTRA, TOOL_SAO, TOOL_SPARSE_LEVELS, TOOL_TU_TOOLS, chroma_dims)
 
 
 def seed_for(stream: int, frame: int) -> int:
@@ -75,6 +75,39 @@ def value_noise_frame(w=1920, h=1080, bd=10, frame=0, stream=0):
     v = lo + _noise(ch, cw, base + 2, ox / 2, oy / 2) * (hi - lo)
     return (np.clip(np.rint(y), 0, mx).astype(np.uint16), np.clip(np.rint(u), 0, mx).astype(np.uint16),
             np.clip(np.rint(v), 0, mx).astype(np.uint16))
+
+
+def config1_frame(frame, stream=0, size=64):
+    """One frame of the 8-bit 4:2:0 small-picture configuration: luma a
+    horizontal ramp 16 -> 235 plus integer noise U[-8, 8] and a 16x16 square
+    of value 200 that moves +2 px per frame (from x = 8, y = 24); chroma
+    128 + U[-4, 4]. Returns (y, u, v) uint8."""
+    rng = np.random.default_rng(seed_for(stream, frame))
+    x = np.arange(size)
+    ramp = np.rint(16 + 219 * x / (size - 1)).astype(np.int32)
+    y = ramp[None, :] + rng.integers(-8, 9, (size, size))
+    x0 = 8 + 2 * frame
+    y[24:40, x0:x0 + 16] = 200
+    y = y.clip(0, 255).astype(np.uint8)
+    u = (128 + rng.integers(-4, 5, (size // 2, size // 2))).astype(np.uint8)
+    v = (128 + rng.integers(-4, 5, (size // 2, size // 2))).astype(np.uint8)
+    return y, u, v
+
+
+def strict_picture(width, height, qp, cu_offset=0):
+    """A PIC_DTYPE record for a strict 8-bit 4:2:0 picture (slice.rs:458
+    decode_picture) on the frame path: CTU 32, per-TB transform tools, no
+    loop filters."""
+    p = np.zeros((), PIC_DTYPE)
+    p["width"], p["height"] = width, height
+    p["visible_width"], p["visible_height"] = width, height
+    p["bit_depth"], p["chroma_format"], p["ctu_log2"] = 8, 1, 5
+    p["slice_qp"] = qp
+    p["chroma_qp_scaled"] = chroma_qp_scaled(qp, 8)  # derived_chroma_qp (hls.rs:778), 8-bit
+    p["tools"] = TOOL_TU_TOOLS
+    p["alf_aps"] = -1
+    p["cu_offset"] = cu_offset
+    return p
 
 
 def pad_to(plane, w, h):
