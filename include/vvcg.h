@@ -905,6 +905,82 @@ vvcg_status vvcg_deblock_general_dev(vvcg_ctx* ctx, uint16_t* const planes[3], c
                                      const vvcg_dbk_ccell* ccells, uint32_t ccell_cols, uint32_t ccell_rows,
                                      const vvcg_dbk_params* params);
 
+/* ---- general-decoder intra pictures, batched ------------------------------ */
+
+/* One transform block of a general-decoder intra picture, in decode order:
+ * its prediction (vvcg_gen_intra_req: block, coding unit, component, mode,
+ * MRL, ISP, BDPCM; out_off indexes the batch's residual / prediction slots)
+ * and, when coded, its residual (vvcg_tu_rec with the block's log2 sizes,
+ * the picture's bit depth, levels at in_off of the level pool and
+ * out_off = pred.out_off; the rules of vvcg_tu_inverse_batch). */
+typedef struct vvcg_gen_tb {
+  vvcg_gen_intra_req pred;
+  vvcg_tu_rec tu;
+  uint32_t coded; /* 0: no residual, the block is its prediction */
+} vvcg_gen_tb;    /* 48 bytes */
+
+/* One 4:2:0 picture of the general decoder (decode_general.rs), coded as a
+ * tree of intra coding units. Its transform blocks form groups in decode
+ * order (vvcg_gen_batch.group_first): a group is reconstructed block after
+ * block (a coding unit's luma blocks or ISP sub-partitions, then its chroma
+ * blocks; or the chroma blocks of a node whose luma was split below 8x8),
+ * and groups that do not read each other's samples run in parallel. */
+typedef struct vvcg_gen_pic {
+  uint32_t width, height;            /* coded size: whole CTUs, multiples of 8 */
+  uint32_t vis_width, vis_height;    /* cropped size (<= coded) */
+  uint8_t bit_depth;                 /* 8..12 */
+  uint8_t ctu_log2;                  /* 4..7 */
+  uint8_t vert_collocated;           /* sps_chroma_vertical_collocated_flag */
+  uint8_t tools;                     /* VVCG_TOOL_DEBLOCK | VVCG_TOOL_SAO | VVCG_TOOL_ALF */
+  uint32_t group_offset, num_groups; /* its groups: group_first[group_offset .. + num_groups] */
+  uint32_t sao_offset;               /* with SAO: 3 x CTUs vvcg_sao at sao[sao_offset] (Y, Cb, Cr per CTU,
+                                        CTUs of the visible picture in raster order) */
+  uint32_t alf_offset;               /* with ALF: CTUs vvcg_alf_ctu at alf_ctus[alf_offset] */
+  int32_t alf_params;                /* with ALF: index into vvcg_gen_batch.alf_params */
+  vvcg_dbk_params dbk;               /* with deblocking: QPs and offsets (reference lists unused) */
+} vvcg_gen_pic;
+
+typedef struct vvcg_gen_batch {
+  const vvcg_gen_pic* pics;
+  uint32_t num_pics;
+  uint32_t num_groups;               /* all pictures' groups */
+  const vvcg_gen_tb* tbs;            /* all pictures' blocks, each picture's in decode order */
+  const uint32_t* group_first;       /* num_groups + 1 block indices, nondecreasing */
+  uint64_t num_tbs;
+  const int16_t* levels;             /* level pool of the coded blocks */
+  uint64_t num_levels;
+  uint64_t slot_count;               /* residual / prediction slots (int16) the blocks' out_off index */
+  const vvcg_sao* sao;
+  uint64_t num_sao;
+  const vvcg_alf_ctu* alf_ctus;
+  uint64_t num_alf_ctus;
+  const vvcg_alf_params* alf_params;
+  uint32_t num_alf_params;
+  uint32_t reserved;
+} vvcg_gen_batch;
+
+/* The general decoder's picture pass over a batch of intra pictures, the
+ * reconstruction and loop filters of decode_general_picture
+ * (decode_general.rs:1134-1150 after the parse): residuals of every coded
+ * block (the size-binned TU kernels), intra reconstruction in decode order
+ * (reconstruct_tus :3885 / reconstruct_tu :3985 with mark_tu's decoded maps),
+ * deblocking with the transform-block maps mark_tu leaves (apply_deblock
+ * :4977), SAO (apply_sao :5189) and ALF (apply_alf :5225). The groups of all
+ * pictures are put in dependency levels on the host: a group runs after
+ * every earlier group whose samples it may read and every earlier group that
+ * may read its samples, so each block sees the decoded maps of the
+ * picture's sequential decode. prepare validates and uploads the batch (host
+ * memory) and derives the levels and deblocking maps; run enqueues the pass
+ * (graph != 0: as one CUDA graph, captured on the first run of the prepared
+ * batch); download synchronises and copies the visible planes to out (3 per
+ * picture, host, 16-bit samples). vvcg_decode_general_batch does all three. */
+vvcg_status vvcg_gen_prepare(vvcg_ctx* ctx, const vvcg_gen_batch* b);
+vvcg_status vvcg_gen_run(vvcg_ctx* ctx, uint32_t graph);
+vvcg_status vvcg_gen_download(vvcg_ctx* ctx, const vvcg_plane_out* out);
+vvcg_status vvcg_decode_general_batch(vvcg_ctx* ctx, const vvcg_gen_batch* b, const vvcg_plane_out* out);
+/* Dependency levels of the prepared batch (the intra kernel's launches per run). */
+uint32_t vvcg_gen_levels(const vvcg_ctx* ctx);
+
 /* ---- inter-prediction tools (BDOF, DMVR, affine / PROF, CIIP, GPM) -------- */
 
 /* A block of the batched inter tools: w x h samples at `off` of the tool's

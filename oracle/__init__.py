@@ -853,3 +853,84 @@ def alf_general(y, u, v, vis_w, vis_h, bd, ctu, ctu_cols, ctus, params):
     lib().orc_alf_general(_p(y), _p(u), _p(v), _p(dy), _p(du), _p(dv), y.shape[1], y.shape[0], vis_w, vis_h, bd,
                           ctu, ctu_cols, _p(c), _p(p))
     return dy, du, dv
+
+
+# ------------------------------------------------- general-decoder pictures --
+
+DBK_CELL_DTYPE = np.dtype([("tu_id", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2"), ("mv", "<i4", (2, 2)),
+                           ("ref_idx", "i1", (2,)), ("flags", "u1"), ("reserved", "u1")])
+DBK_CCELL_DTYPE = np.dtype([("tu_cb", "<u4"), ("tu_cr", "<u4"), ("tu_w", "<u2"), ("tu_h", "<u2")])
+_DBK_CODED, _DBK_INTRA, _DBK_CBF, _DBK_NO_TU = 1, 2, 4, 0xFFFFFFFF
+
+
+def mark_tu_maps(width, height, tbs):
+    """The deblocking maps mark_tu (decode_general.rs:4837-4907) leaves after
+    the picture's transform blocks, visited in decode order (tbs: records
+    with a "pred" block (x, y, w, h in component samples, cu_*, comp) and a
+    "coded" flag): per 4x4 luma cell the last luma block's id (its index),
+    size and cbf, and the coded / intra flags of its coding unit; per 2x2
+    chroma cell the last Cb / Cr block ids and size."""
+    cols, rows = width // 4, height // 4
+    cells = np.zeros((rows, cols), DBK_CELL_DTYPE)
+    cells["tu_id"] = _DBK_NO_TU
+    cells["ref_idx"] = -1
+    cc = np.zeros((rows, cols), DBK_CCELL_DTYPE)
+    cc["tu_cb"] = _DBK_NO_TU
+    cc["tu_cr"] = _DBK_NO_TU
+    for i, t in enumerate(tbs):
+        r = t["pred"]
+        x, y, w, h = int(r["x"]), int(r["y"]), int(r["w"]), int(r["h"])
+        if int(r["comp"]) == 0:
+            x1, y1 = min(x + w, cols * 4), min(y + h, rows * 4)
+            sub = cells[y // 4:(y1 + 3) // 4, x // 4:(x1 + 3) // 4]
+            sub["tu_id"], sub["tu_w"], sub["tu_h"] = i, w, h
+            sub["flags"] = (sub["flags"] & (0xFF ^ _DBK_CBF)) | (_DBK_CBF if int(t["coded"]) else 0)
+            cx, cy, cw_, ch_ = int(r["cu_x"]), int(r["cu_y"]), int(r["cu_w"]), int(r["cu_h"])
+            cx1, cy1 = min(cx + cw_, cols * 4), min(cy + ch_, rows * 4)
+            cu = cells[cy // 4:(cy1 + 3) // 4, cx // 4:(cx1 + 3) // 4]
+            cu["flags"] |= _DBK_CODED | _DBK_INTRA
+        else:
+            x1, y1 = min(x + w, cols * 2), min(y + h, rows * 2)
+            sub = cc[y // 2:(y1 + 1) // 2, x // 2:(x1 + 1) // 2]
+            sub["tu_cb" if int(r["comp"]) == 1 else "tu_cr"] = i
+            sub["tu_w"], sub["tu_h"] = w, h
+    return cells, cc
+
+
+def general_picture(pic, tbs, group_sizes, levels, slot_count, sao, alf_ctus, alf_params):
+    """decode_general_picture's reconstruction and loop filters for one intra
+    picture, composed from the restatements above in the reference's order
+    (decode_general.rs:1134-1150): residuals of the coded blocks (tu_batch),
+    reconstruction of every block in decode order (gen_intra_recon, one group
+    after another), deblocking over mark_tu's maps (deblock_general), SAO per
+    component (sao_bounded; chroma CTUs of half size) and ALF (alf_general),
+    as the picture's tools select. Records as the GEN_* layouts of the
+    package; offsets local to the picture. Returns the visible (Y, Cb, Cr)."""
+    w, h = int(pic["width"]), int(pic["height"])
+    vw, vh = int(pic["vis_width"]), int(pic["vis_height"])
+    cvw, cvh = (vw + 1) // 2, (vh + 1) // 2
+    bd, ctu, tools = int(pic["bit_depth"]), 1 << int(pic["ctu_log2"]), int(pic["tools"])
+    coded = tbs[tbs["coded"] != 0]["tu"]
+    rc, res = tu_batch(coded.view(TU_DTYPE) if coded.dtype != TU_DTYPE else coded, levels, slot_count)
+    if rc:
+        raise ValueError(f"tu_batch rejected record {-rc - 1}")
+    Y = np.zeros((h, w), np.uint16)
+    U = np.zeros((h // 2, w // 2), np.uint16)
+    V = np.zeros((h // 2, w // 2), np.uint16)
+    dy = np.zeros((h // 4, w // 4), np.uint8)
+    dc = np.zeros((h // 2, w // 2), np.uint8)
+    starts = np.concatenate([[0], np.cumsum(group_sizes)]).astype(np.uint32)
+    Y, U, V, _, _, _ = gen_intra_recon(Y, U, V, dy, dc, bd, ctu, np.ascontiguousarray(tbs["pred"]), starts, res,
+                                       slot_count, bool(int(pic["vert_collocated"])))
+    cols, rows = -(-vw // ctu), -(-vh // ctu)
+    nctu = cols * rows
+    if tools & 2:  # deblocking
+        cells, cc = mark_tu_maps(w, h, tbs)
+        Y, U, V = deblock_general((Y, U, V), vw, vh, bd, ctu, cells, cc, pic["dbk"])
+    if tools & 4:  # SAO
+        Y = sao_bounded(Y, vw, vh, bd, ctu, cols, sao[:nctu])
+        U = sao_bounded(U, cvw, cvh, bd, ctu // 2, cols, sao[nctu:2 * nctu])
+        V = sao_bounded(V, cvw, cvh, bd, ctu // 2, cols, sao[2 * nctu:3 * nctu])
+    if tools & 8:  # ALF
+        Y, U, V = alf_general(Y, U, V, vw, vh, bd, ctu, cols, alf_ctus, alf_params)
+    return Y[:vh, :vw], U[:cvh, :cvw], V[:cvh, :cvw]

@@ -120,6 +120,12 @@ TU_DTYPE = np.dtype([("log2_w", "u1"), ("log2_h", "u1"), ("bit_depth", "u1"), ("
                      ("flags", "u1"), ("mts_idx", "u1"), ("lfnst_idx", "u1"),
                      ("lfnst_mode", "u1"), ("in_off", "<u4"), ("out_off", "<u4")])
 
+GEN_TB_DTYPE = np.dtype([("pred", GEN_INTRA_REQ_DTYPE), ("tu", TU_DTYPE), ("coded", "<u4")])
+GEN_PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("vis_width", "<u4"), ("vis_height", "<u4"),
+                          ("bit_depth", "u1"), ("ctu_log2", "u1"), ("vert_collocated", "u1"), ("tools", "u1"),
+                          ("group_offset", "<u4"), ("num_groups", "<u4"), ("sao_offset", "<u4"),
+                          ("alf_offset", "<u4"), ("alf_params", "<i4"), ("dbk", DBK_PARAMS_DTYPE)])
+
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
 TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM, TOOL_SPARSE_LEVELS, TOOL_TU_TOOLS = 16, 32, 64, 128
 CU_TS_Y, CU_TS_CB, CU_TS_CR, CU_MTS_SHIFT, CU_LFNST_SHIFT = 1, 2, 4, 3, 6
@@ -172,6 +178,15 @@ class _Batch(C.Structure):
                 ("aps", C.c_void_p)]
 
 
+class _GenBatch(C.Structure):
+    _fields_ = [("pics", C.c_void_p), ("num_pics", C.c_uint32), ("num_groups", C.c_uint32),
+                ("tbs", C.c_void_p), ("group_first", C.c_void_p), ("num_tbs", C.c_uint64),
+                ("levels", C.c_void_p), ("num_levels", C.c_uint64), ("slot_count", C.c_uint64),
+                ("sao", C.c_void_p), ("num_sao", C.c_uint64), ("alf_ctus", C.c_void_p),
+                ("num_alf_ctus", C.c_uint64), ("alf_params", C.c_void_p), ("num_alf_params", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
 class _PlaneOut(C.Structure):
     _fields_ = [("data", C.c_void_p), ("stride", C.c_uint32), ("reserved", C.c_uint32)]
 
@@ -197,6 +212,7 @@ assert DBK_CELL_DTYPE.itemsize == 28 and DBK_CCELL_DTYPE.itemsize == 12 and DBK_
 assert CTU_MOTION_DTYPE.itemsize == 40 and BDOF_REQ_DTYPE.itemsize == 8 and DMVR_REQ_DTYPE.itemsize == 28
 assert AFFINE_REQ_DTYPE.itemsize == 36 and PROF_REQ_DTYPE.itemsize == 16 and CIIP_REQ_DTYPE.itemsize == 12
 assert GPM_REQ_DTYPE.itemsize == 12
+assert GEN_TB_DTYPE.itemsize == 48 and GEN_PIC_DTYPE.itemsize == 212
 assert LMCS_APS_DTYPE.itemsize == 36 and LMCS_TABLES_DTYPE.itemsize == 16520 and CRES_DTYPE.itemsize == 20
 
 
@@ -281,6 +297,12 @@ def lib():
         L.vvcg_ciip_blend_dev.argtypes = [vp, vp, u32, vp, vp, vp, u64]
         L.vvcg_gpm_blend_dev.argtypes = [vp, vp, u32, vp, vp, vp, u64]
         L.vvcg_recon_picture_static.argtypes = [vp, vp, u32, vp, u64, vp, vp, C.c_char_p, C.c_size_t]
+        L.vvcg_gen_prepare.argtypes = [vp, vp]
+        L.vvcg_gen_run.argtypes = [vp, u32]
+        L.vvcg_gen_download.argtypes = [vp, vp]
+        L.vvcg_decode_general_batch.argtypes = [vp, vp, vp]
+        L.vvcg_gen_levels.argtypes = [vp]
+        L.vvcg_gen_levels.restype = u32
         _lib = L
     return _lib
 
@@ -329,6 +351,39 @@ class Batch:
             outs.append((np.zeros((h, w), np.uint16),
                          np.zeros((ch, cw), np.uint16) if cf else None,
                          np.zeros((ch, cw), np.uint16) if cf else None))
+        return outs
+
+
+class GenBatch:
+    """Host-side records of a batch of general-decoder intra pictures (the
+    inputs of vvcg_gen_batch): GEN_PIC_DTYPE pictures, GEN_TB_DTYPE blocks in
+    decode order, group_first (num_groups + 1 block indices), the int16 level
+    pool, the residual / prediction slot count, and the SAO (SAO_DTYPE, 3 per
+    CTU), ALF CTU (ALF_CTU_DTYPE) and ALF parameter (ALF_PARAMS_DTYPE) arrays."""
+
+    def __init__(self, pics, tbs, group_first, levels, slot_count, sao=None, alf_ctus=None, alf_params=None):
+        self.pics = np.ascontiguousarray(pics, dtype=GEN_PIC_DTYPE)
+        self.tbs = np.ascontiguousarray(tbs, dtype=GEN_TB_DTYPE)
+        self.group_first = np.ascontiguousarray(group_first, dtype=np.uint32)
+        self.levels = np.ascontiguousarray(levels, dtype=np.int16)
+        self.slot_count = int(slot_count)
+        self.sao = None if sao is None else np.ascontiguousarray(sao, dtype=SAO_DTYPE)
+        self.alf_ctus = None if alf_ctus is None else np.ascontiguousarray(alf_ctus, dtype=ALF_CTU_DTYPE)
+        self.alf_params = None if alf_params is None else np.ascontiguousarray(alf_params, dtype=ALF_PARAMS_DTYPE)
+
+    def as_struct(self):
+        n = lambda a: 0 if a is None else len(a)  # noqa: E731
+        return _GenBatch(_ptr(self.pics), len(self.pics), len(self.group_first) - 1, _ptr(self.tbs),
+                         _ptr(self.group_first), len(self.tbs), _ptr(self.levels), self.levels.size,
+                         self.slot_count, _ptr(self.sao), n(self.sao), _ptr(self.alf_ctus), n(self.alf_ctus),
+                         _ptr(self.alf_params), n(self.alf_params), 0)
+
+    def output_planes(self):
+        outs = []
+        for p in self.pics:
+            w, h = int(p["vis_width"]), int(p["vis_height"])
+            outs.append((np.zeros((h, w), np.uint16), np.zeros(((h + 1) // 2, (w + 1) // 2), np.uint16),
+                         np.zeros(((h + 1) // 2, (w + 1) // 2), np.uint16)))
         return outs
 
 
@@ -395,6 +450,32 @@ class Context:
         po = self._plane_outs(outs)
         self._keep = (batch, outs, po)
         self._check(self._L.vvcg_decode_batch(self._h, C.byref(batch.as_struct()), po))
+        return outs
+
+    # -- general-decoder intra pictures --
+    def gen_prepare(self, batch: GenBatch):
+        self._gen_keep = (batch, batch.as_struct())
+        self._check(self._L.vvcg_gen_prepare(self._h, C.byref(self._gen_keep[1])))
+
+    def gen_run(self, graph=False):
+        self._check(self._L.vvcg_gen_run(self._h, 1 if graph else 0))
+
+    def gen_download(self, outs):
+        po = self._plane_outs(outs)
+        self._check(self._L.vvcg_gen_download(self._h, po))
+        return outs
+
+    @property
+    def gen_levels(self) -> int:
+        return int(self._L.vvcg_gen_levels(self._h))
+
+    def decode_general(self, batch: GenBatch, outs=None):
+        """Whole call with host buffers; returns [(y, u, v)] visible planes."""
+        outs = outs if outs is not None else batch.output_planes()
+        po = self._plane_outs(outs)
+        st = batch.as_struct()
+        self._keep = (batch, outs, po, st)
+        self._check(self._L.vvcg_decode_general_batch(self._h, C.byref(st), po))
         return outs
 
     def decode_batch_async(self, batch: Batch, outs):

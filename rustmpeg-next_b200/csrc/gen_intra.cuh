@@ -603,40 +603,74 @@ struct GenReconArgs {
   int16_t* pred;                // receives the predictions (w x h at out_off)
 };
 
+// One block of a sequential reconstruction: predicted (gi_predict), its
+// residual added, clipped to the bit depth and stored into its plane, and its
+// samples marked decoded for the blocks after it.
+__device__ void gi_recon_block(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R, int16_t* pred,
+                               const int16_t* res, GiWs& ws, int lane) {
+  const int maxv = (1 << S.bit_depth) - 1;
+  gi_predict(S, R, pred, ws);
+  __syncwarp();
+  uint16_t* pl = const_cast<uint16_t*>(S.plane[R.comp]);
+  const int st = (int)S.stride[R.comp];
+  for (int i = lane; i < R.w * R.h; i += 32) {
+    const int yy = i / R.w, xx = i - yy * R.w;
+    const int v = (int)pred[i] + (res ? (int)res[i] : 0);
+    pl[(size_t)(R.y + yy) * st + R.x + xx] = (uint16_t)clampi(v, 0, maxv);
+  }
+  // mark_tu's decoded maps: luma per 4x4 cell touched, chroma per sample
+  if (R.comp == 0) {
+    uint8_t* dm = const_cast<uint8_t*>(S.dec_y);
+    const int cw = (int)S.width >> 2;
+    const int x0 = R.x >> 2, x1 = min((R.x + R.w + 3) >> 2, cw), y0 = R.y >> 2;
+    const int y1 = min((R.y + R.h + 3) >> 2, (int)S.height >> 2);
+    for (int i = lane; i < (x1 - x0) * (y1 - y0); i += 32)
+      dm[(size_t)(y0 + i / (x1 - x0)) * cw + x0 + i % (x1 - x0)] = 1;
+  } else {
+    uint8_t* dm = const_cast<uint8_t*>(S.dec_c);
+    const int cw = (int)S.width >> 1;
+    for (int i = lane; i < R.w * R.h; i += 32) dm[(size_t)(R.y + i / R.w) * cw + R.x + i % R.w] = 1;
+  }
+  __threadfence_block();
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(kGiWarps * 32) k_gen_intra_recon(const __grid_constant__ GenReconArgs A) {
   __shared__ GiWs ws[kGiWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const vvcg_gen_intra_state& S = A.st;
-  const int maxv = (1 << S.bit_depth) - 1;
-  for (int g = blockIdx.x * kGiWarps + warp; g < A.num_groups; g += gridDim.x * kGiWarps) {
+  for (int g = blockIdx.x * kGiWarps + warp; g < A.num_groups; g += gridDim.x * kGiWarps)
     for (uint32_t q = A.group_start[g]; q < A.group_start[g + 1]; q++) {
       const vvcg_gen_intra_req R = A.reqs[q];
-      int16_t* pred = A.pred + R.out_off;
-      gi_predict(S, R, pred, ws[warp]);
-      __syncwarp();
-      const int16_t* res = A.res ? A.res + R.out_off : nullptr;
-      uint16_t* pl = const_cast<uint16_t*>(S.plane[R.comp]);
-      const int st = (int)S.stride[R.comp];
-      for (int i = lane; i < R.w * R.h; i += 32) {
-        const int yy = i / R.w, xx = i - yy * R.w;
-        const int v = (int)pred[i] + (res ? (int)res[i] : 0);
-        pl[(size_t)(R.y + yy) * st + R.x + xx] = (uint16_t)clampi(v, 0, maxv);
-      }
-      // mark_tu's decoded maps: luma per 4x4 cell touched, chroma per sample
-      if (R.comp == 0) {
-        uint8_t* dm = const_cast<uint8_t*>(S.dec_y);
-        const int cw = (int)S.width >> 2;
-        const int x0 = R.x >> 2, x1 = min((R.x + R.w + 3) >> 2, cw), y0 = R.y >> 2;
-        const int y1 = min((R.y + R.h + 3) >> 2, (int)S.height >> 2);
-        for (int i = lane; i < (x1 - x0) * (y1 - y0); i += 32)
-          dm[(size_t)(y0 + i / (x1 - x0)) * cw + x0 + i % (x1 - x0)] = 1;
-      } else {
-        uint8_t* dm = const_cast<uint8_t*>(S.dec_c);
-        const int cw = (int)S.width >> 1;
-        for (int i = lane; i < R.w * R.h; i += 32) dm[(size_t)(R.y + i / R.w) * cw + R.x + i % R.w] = 1;
-      }
-      __threadfence_block();
-      __syncwarp();
+      gi_recon_block(A.st, R, A.pred + R.out_off, A.res ? A.res + R.out_off : nullptr, ws[warp], lane);
+    }
+}
+
+// One dependency level of the general picture pass: each warp takes coding
+// units (groups of blocks in decode order) of the level, from any picture of
+// the batch, and reconstructs their blocks in order. The host puts a group
+// in a later level than every earlier group whose samples it may read and
+// every earlier group that may read its samples, so the decoded maps each
+// block sees are those of the picture's sequential decode.
+struct GenLevelArgs {
+  const vvcg_gen_intra_state* states;  // per picture
+  const vvcg_gen_intra_req* reqs;      // all blocks of the batch
+  const uint32_t* group_first;         // per group: first block; group_first[g + 1] ends it
+  const uint32_t* group_pic;           // per group: picture
+  const uint32_t* level_groups;        // the groups of this level
+  uint32_t n;
+  const int16_t* res;                  // residuals at out_off (zero where uncoded)
+  int16_t* pred;                       // predictions at out_off
+};
+
+__global__ void __launch_bounds__(kGiWarps * 32) k_gen_recon_level(const __grid_constant__ GenLevelArgs A) {
+  __shared__ GiWs ws[kGiWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint32_t i = blockIdx.x * kGiWarps + warp; i < A.n; i += gridDim.x * kGiWarps) {
+    const uint32_t g = A.level_groups[i];
+    const vvcg_gen_intra_state& S = A.states[A.group_pic[g]];
+    for (uint32_t q = A.group_first[g]; q < A.group_first[g + 1]; q++) {
+      const vvcg_gen_intra_req R = A.reqs[q];
+      gi_recon_block(S, R, A.pred + R.out_off, A.res + R.out_off, ws[warp], lane);
     }
   }
 }

@@ -96,6 +96,9 @@ struct PicLayout {
 
 }  // namespace
 
+struct GenPass;  // the general decoder's picture pass (gen_picture.cuh)
+void gen_pass_free(GenPass* g);
+
 struct vvcg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -147,6 +150,7 @@ struct vvcg_ctx {
   // rebased records of a pipelined chunk
   PinnedBuf stage, stage_cus;
   size_t stage_used = 0;
+  GenPass* gen = nullptr;  // state of vvcg_gen_prepare / vvcg_gen_run
 };
 
 namespace {
@@ -466,6 +470,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   for (vvcg_ctx* l : ctx->lanes) vvcg_ctx_destroy(l);
+  gen_pass_free(ctx->gen);
   ctx->stage.release();
   ctx->stage_cus.release();
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
@@ -2804,3 +2809,5 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
   if (status & kStatusBadRecord) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "a level offset or sparse level entry was out of range");
   return VVCG_OK;
 }
+
+#include "gen_picture.cuh"

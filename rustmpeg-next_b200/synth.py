@@ -881,3 +881,254 @@ def batching_streams(n_streams, seed):
         w, h = BATCH_RESOLUTIONS[int(rng.choice(len(BATCH_RESOLUTIONS), p=BATCH_WEIGHTS))]
         out.append((w, h, int(rng.choice((8, 10))), int(rng.integers(22, 38))))
     return out
+
+
+# ---------------------------------------------------------------------------
+# General-decoder intra pictures (coding trees of 4x4..128x128 blocks)
+# ---------------------------------------------------------------------------
+
+def random_alf_general_params(rng):
+    """An ALF_PARAMS_DTYPE record with random luma, chroma and CCALF filters."""
+    from . import ALF_PARAMS_DTYPE
+
+    a = np.zeros((), ALF_PARAMS_DTYPE)
+    a["num_luma_filters"] = int(rng.integers(1, 26))
+    a["luma_clip"] = int(rng.integers(0, 2))
+    a["coeff_delta_idx"] = rng.integers(0, int(a["num_luma_filters"]), 25)
+    a["luma_coeff"] = rng.integers(-40, 41, (25, 12))
+    a["luma_clip_idx"] = rng.integers(0, 4, (25, 12))
+    a["num_chroma_filters"] = int(rng.integers(1, 9))
+    a["chroma_clip"] = int(rng.integers(0, 2))
+    a["chroma_coeff"] = rng.integers(-40, 41, (8, 6))
+    a["chroma_clip_idx"] = rng.integers(0, 4, (8, 6))
+    a["num_cc_cb"], a["num_cc_cr"] = int(rng.integers(1, 5)), int(rng.integers(0, 5))
+    a["cc_cb"] = rng.integers(-64, 65, (4, 7))
+    a["cc_cr"] = rng.integers(-64, 65, (4, 7))
+    return a
+
+
+def _general_groups(rng, tx, ty, ctu, vis_w, vis_h, leaf_bias, out):
+    """The coding units of one CTU in decode order as groups: ("cu", x, y, w,
+    h, with_chroma) for a coding unit (with its chroma when its node is at
+    least 8x8 luma) and ("chroma", x, y, w, h) for the chroma of a node whose
+    luma children are narrower or shorter than 8, after its last child.
+    The same splitting rules as _split_tree (implicit halving across the
+    picture edge, no leaf above 64)."""
+
+    def walk(x, y, w, h, chroma_done):
+        if x >= vis_w or y >= vis_h:
+            return
+        cross_x, cross_y = x + w > vis_w, y + h > vis_h
+        parts = None
+        if cross_x or cross_y:
+            if cross_x and cross_y and w > 4 and h > 4:
+                parts = [(0, 0, w // 2, h // 2), (w // 2, 0, w // 2, h // 2), (0, h // 2, w // 2, h // 2),
+                         (w // 2, h // 2, w // 2, h // 2)]
+            elif cross_x and w > 4:
+                parts = [(0, 0, w // 2, h), (w // 2, 0, w // 2, h)]
+            elif cross_y and h > 4:
+                parts = [(0, 0, w, h // 2), (0, h // 2, w, h // 2)]
+        if parts is None:
+            opts = ["leaf"]
+            if w == h and w > 4:
+                opts.append("qt")
+            if w > 4:
+                opts.append("bv")
+            if h > 4:
+                opts.append("bh")
+            if w >= 16:
+                opts.append("tv")
+            if h >= 16:
+                opts.append("th")
+            p_leaf = leaf_bias if w * h <= 256 else leaf_bias / 3
+            if w > 64 or h > 64:
+                p_leaf = 0.0
+            if len(opts) == 1 or rng.random() < p_leaf:
+                out.append(("cu", x, y, w, h, not chroma_done))
+                return
+            kind = opts[1 + int(rng.integers(0, len(opts) - 1))]
+            parts = {"qt": [(0, 0, w // 2, h // 2), (w // 2, 0, w // 2, h // 2), (0, h // 2, w // 2, h // 2),
+                            (w // 2, h // 2, w // 2, h // 2)],
+                     "bv": [(0, 0, w // 2, h), (w // 2, 0, w // 2, h)],
+                     "bh": [(0, 0, w, h // 2), (0, h // 2, w, h // 2)],
+                     "tv": [(0, 0, w // 4, h), (w // 4, 0, w // 2, h), (3 * w // 4, 0, w // 4, h)],
+                     "th": [(0, 0, w, h // 4), (0, h // 4, w, h // 2), (0, 3 * h // 4, w, h // 4)]}[kind]
+        here = not chroma_done and min(min(pw, ph) for _, _, pw, ph in parts) < 8
+        for dx, dy, pw, ph in parts:
+            walk(x + dx, y + dy, pw, ph, chroma_done or here)
+        if here:
+            out.append(("chroma", x, y, w, h))
+
+    walk(tx, ty, ctu, ctu, False)
+
+
+def random_general_picture(vis_w, vis_h, ctu=64, bd=10, qp=32, seed=0, tools=TOOL_DEBLOCK | TOOL_SAO | TOOL_ALF,
+                           dep_quant=False, isp_prob=0.2, mrl_prob=0.2, bdpcm_prob=0.08, lfnst_prob=0.15,
+                           mts_prob=0.2, ts_prob=0.08, coded_prob=0.75, leaf_bias=0.45, implicit_mts=True):
+    """One general-decoder intra picture as GenBatch parts: (pic, tbs,
+    group_sizes, levels, slot_count, sao, alf_ctus, alf_params). Blocks are
+    in decode order with slots and level offsets local to the picture."""
+    from . import (GEN_PIC_DTYPE, GEN_TB_DTYPE, SAO_DTYPE, ALF_CTU_DTYPE, ISP_HOR, ISP_VER, TU_DEP_QUANT,
+                   TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS)
+
+    rng = np.random.default_rng(seed)
+    pic_w, pic_h = -(-vis_w // ctu) * ctu, -(-vis_h // ctu) * ctu
+    groups = []
+    for ty in range(0, pic_h, ctu):
+        for tx in range(0, pic_w, ctu):
+            _general_groups(rng, tx, ty, ctu, vis_w, vis_h, leaf_bias, groups)
+    lqp = min(63 + 6 * (bd - 8), qp + 6 * (bd - 8))
+    cqp = chroma_qp_scaled(qp, bd)
+    tbs, sizes, lv_chunks = [], [], []
+    slot = lvl = 0
+
+    def add(x, y, w, h, cu, comp, mode, mrl=0, isp=0, bdpcm=0, ts=False, mts=0, lfnst=0, coded=True):
+        nonlocal slot, lvl
+        t = np.zeros((), GEN_TB_DTYPE)
+        t["pred"]["x"], t["pred"]["y"], t["pred"]["w"], t["pred"]["h"] = x, y, w, h
+        t["pred"]["cu_x"], t["pred"]["cu_y"], t["pred"]["cu_w"], t["pred"]["cu_h"] = cu
+        t["pred"]["comp"], t["pred"]["mode"], t["pred"]["mrl"] = comp, mode, mrl
+        t["pred"]["isp"], t["pred"]["bdpcm"] = isp, bdpcm
+        t["pred"]["out_off"] = slot
+        tu = t["tu"]
+        tu["log2_w"], tu["log2_h"] = int(w).bit_length() - 1, int(h).bit_length() - 1
+        tu["bit_depth"], tu["qp"] = bd, lqp if comp == 0 else cqp
+        flags = 0
+        if ts:
+            flags |= TU_TRANSFORM_SKIP
+            if bdpcm:
+                flags |= TU_BDPCM_HOR if bdpcm == 1 else TU_BDPCM_VER
+        elif dep_quant:
+            flags |= TU_DEP_QUANT
+        if comp == 0 and implicit_mts and not isp and not ts and mts == 0 and lfnst == 0:
+            flags |= TU_IMPLICIT_MTS
+        tu["flags"], tu["mts_idx"], tu["lfnst_idx"], tu["lfnst_mode"] = flags, mts, lfnst, mode if lfnst else 0
+        tu["out_off"] = slot
+        if coded:
+            tu["in_off"] = lvl
+            lv = _tb_levels(rng, 1, w, h, int(tu["qp"]))[0]
+            if lfnst:  # LFNST codes only its top-left coefficients
+                keep = np.zeros_like(lv)
+                keep[:4, :4] = lv[:4, :4]
+                lv = keep if keep.any() else np.pad(np.ones((1, 1), np.int16), ((0, h - 1), (0, w - 1)))
+            if mts and (w == 32 or h == 32):
+                lv[16:, :] = 0
+                lv[:, 16:] = 0
+            lv_chunks.append(lv.reshape(-1))
+            lvl += w * h
+        t["coded"] = 1 if coded else 0
+        tbs.append(t)
+        slot += w * h
+
+    for g in groups:
+        n0 = len(tbs)
+        if g[0] == "cu":
+            _, x, y, w, h, with_chroma = g
+            mode = int(rng.integers(0, 67))
+            isp = mrl = bdpcm = 0
+            if w * h > 16 and w <= 64 and h <= 64 and rng.random() < isp_prob:
+                isp = ISP_HOR if rng.random() < 0.5 else ISP_VER
+            elif w <= 32 and h <= 32 and rng.random() < bdpcm_prob:
+                bdpcm = 1 + int(rng.integers(0, 2))
+                mode = 18 if bdpcm == 1 else 50
+            elif y % ctu and w >= 4 and h >= 4 and rng.random() < mrl_prob:
+                mrl = 1 + int(rng.integers(0, 2))
+            cu = (x, y, w, h)
+            if isp:
+                n = 2 if (w, h) in ((4, 8), (8, 4)) else 4
+                for k in range(n):
+                    sx, sy, sw, sh = (x, y + k * h // n, w, h // n) if isp == ISP_HOR else (x + k * w // n, y, w // n, h)
+                    add(sx, sy, sw, sh, cu, 0, mode, isp=isp, coded=rng.random() < coded_prob)
+            else:
+                tb = 64
+                for yy in range(y, y + h, min(h, tb)):
+                    for xx in range(x, x + w, min(w, tb)):
+                        tw, th = min(w, tb), min(h, tb)
+                        ts = bool(bdpcm) or (tw <= 32 and th <= 32 and rng.random() < ts_prob)
+                        lfnst = 0
+                        mts = 0
+                        if not ts and tw == th and tw >= 4 and rng.random() < lfnst_prob:
+                            lfnst = 1 + int(rng.integers(0, 2))
+                        elif not ts and tw <= 32 and th <= 32 and tw >= 4 and th >= 4 and rng.random() < mts_prob:
+                            mts = 1 + int(rng.integers(0, 4))
+                        add(xx, yy, tw, th, cu, 0, mode, mrl=mrl, bdpcm=bdpcm, ts=ts, mts=mts, lfnst=lfnst,
+                            coded=bdpcm or rng.random() < coded_prob)
+            if with_chroma:
+                groups_chroma = [(x, y, w, h)]
+            else:
+                groups_chroma = []
+        else:
+            _, x, y, w, h = g
+            groups_chroma = [(x, y, w, h)]
+        for (x, y, w, h) in groups_chroma:
+            cm = int(rng.choice([0, 1, 18, 50, 66, 81, 82, 83]))
+            cw_, ch_ = w // 2, h // 2
+            for yy in range(0, ch_, min(ch_, 32)):
+                for xx in range(0, cw_, min(cw_, 32)):
+                    tw, th = min(cw_, 32), min(ch_, 32)
+                    for comp in (1, 2):
+                        add(x // 2 + xx, y // 2 + yy, tw, th, (x, y, w, h), comp, cm,
+                            ts=tw <= 32 and rng.random() < ts_prob, coded=rng.random() < coded_prob)
+        sizes.append(len(tbs) - n0)
+    cols, rows = -(-vis_w // ctu), -(-vis_h // ctu)
+    nctu = cols * rows
+    sao = np.zeros(3 * nctu, SAO_DTYPE)
+    kind = rng.integers(0, 3, 3 * nctu)
+    omax = (1 << (min(bd, 10) - 5)) - 1
+    sao["type"] = kind
+    sao["band_or_class"] = np.where(kind == 1, rng.integers(0, 32, 3 * nctu), rng.integers(0, 4, 3 * nctu))
+    sao["offsets"] = np.where((kind == 2)[:, None],
+                              rng.integers(0, omax + 1, (3 * nctu, 4)) * np.array([1, 1, -1, -1]),
+                              rng.integers(-omax, omax + 1, (3 * nctu, 4)))
+    alf = np.zeros(nctu, ALF_CTU_DTYPE)
+    alf["luma_mode"] = rng.integers(0, 3, nctu)
+    alf["luma_set"] = rng.integers(0, 16, nctu)
+    alf["cb_alt"] = np.where(rng.random(nctu) < 0.7, rng.integers(0, 8, nctu), 0xFF)
+    alf["cr_alt"] = np.where(rng.random(nctu) < 0.7, rng.integers(0, 8, nctu), 0xFF)
+    alf["cc_cb"] = rng.integers(0, 5, nctu)
+    alf["cc_cr"] = rng.integers(0, 5, nctu)
+    p = np.zeros((), GEN_PIC_DTYPE)
+    p["width"], p["height"], p["vis_width"], p["vis_height"] = pic_w, pic_h, vis_w, vis_h
+    p["bit_depth"], p["ctu_log2"], p["vert_collocated"], p["tools"] = bd, int(ctu).bit_length() - 1, 0, tools
+    p["alf_params"] = 0
+    d = p["dbk"]
+    d["qp"] = [qp, min(63, max(0, qp + int(rng.integers(-3, 2)))), min(63, max(0, qp + int(rng.integers(-3, 2))))]
+    d["beta_offset_div2"] = rng.integers(-4, 5, 3)
+    d["tc_offset_div2"] = rng.integers(-4, 5, 3)
+    levels = np.concatenate(lv_chunks) if lv_chunks else np.zeros(0, np.int16)
+    return (p, np.array(tbs, GEN_TB_DTYPE), np.array(sizes, np.uint32), levels, slot, sao, alf,
+            random_alf_general_params(rng))
+
+
+def general_batch(parts):
+    """GenBatch inputs from random_general_picture parts: pictures, blocks,
+    group_first, levels and slots rebased into shared arrays. Returns a dict
+    of the GenBatch constructor's arguments."""
+    from . import GEN_PIC_DTYPE
+
+    pics, tbs, firsts, levels, saos, alfs, prms = [], [], [0], [], [], [], []
+    n_tb = n_grp = n_lv = n_slot = n_sao = n_alf = 0
+    for k, (p, t, sizes, lv, slots, sao, alf, prm) in enumerate(parts):
+        p = np.asarray(p, GEN_PIC_DTYPE).copy()
+        p["group_offset"], p["num_groups"] = n_grp, len(sizes)
+        p["sao_offset"], p["alf_offset"], p["alf_params"] = n_sao, n_alf, k
+        t = t.copy()
+        t["pred"]["out_off"] += n_slot
+        t["tu"]["out_off"] += n_slot
+        t["tu"]["in_off"] = np.where(t["coded"] != 0, t["tu"]["in_off"] + n_lv, 0)
+        pics.append(p)
+        tbs.append(t)
+        firsts.extend((n_tb + np.cumsum(sizes)).tolist())
+        levels.append(lv)
+        saos.append(sao)
+        alfs.append(alf)
+        prms.append(prm)
+        n_tb += len(t)
+        n_grp += len(sizes)
+        n_lv += len(lv)
+        n_slot += slots
+        n_sao += len(sao)
+        n_alf += len(alf)
+    return dict(pics=np.array(pics, GEN_PIC_DTYPE), tbs=np.concatenate(tbs), group_first=np.array(firsts, np.uint32),
+                levels=np.concatenate(levels), slot_count=n_slot, sao=np.concatenate(saos),
+                alf_ctus=np.concatenate(alfs), alf_params=np.array(prms))

@@ -124,6 +124,7 @@ RECORDS = {
     "TXS_RES_DTYPE": "vvcg_tx_search_res", "TU_DTYPE": "vvcg_tu_rec", "CTU_MOTION_DTYPE": "vvcg_ctu_motion",
     "BDOF_REQ_DTYPE": "vvcg_bdof_req", "DMVR_REQ_DTYPE": "vvcg_dmvr_req", "AFFINE_REQ_DTYPE": "vvcg_affine_req",
     "PROF_REQ_DTYPE": "vvcg_prof_req", "CIIP_REQ_DTYPE": "vvcg_ciip_req", "GPM_REQ_DTYPE": "vvcg_gpm_req",
+    "GEN_TB_DTYPE": "vvcg_gen_tb", "GEN_PIC_DTYPE": "vvcg_gen_pic",
 }
 
 
