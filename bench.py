@@ -367,6 +367,8 @@ def main():
     ap.add_argument("--no-batching", action="store_true", help="skip the batching (mixed streams) section")
     ap.add_argument("--batch-streams", type=int, default=64)
     ap.add_argument("--batch-frames", type=int, default=8)
+    ap.add_argument("--no-general", action="store_true", help="skip the coding-tree (general decoder) section")
+    ap.add_argument("--general-streams", type=int, default=64)
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -598,6 +600,8 @@ def main():
             line["encode"] = bench_encoder(pkg, ctx, stream, dev, args, peaks)
     if world == 1 and not args.no_batching:
         line["batching"] = bench_batching(pkg, dev, stream, args, timed)
+    if world == 1 and not args.no_general:
+        line["general"] = bench_general(pkg, dev, stream, args, timed)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics_d, cus_d, levels_d, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
@@ -838,6 +842,100 @@ def bench_batching(pkg, dev, stream, args, timed):
             "speedup": round(per_stream_ms / batched_ms, 2), "parity": parity, "build_s": round(build_s, 1),
             "block_sizes": "32x32 coding units of the frame path (the 4x4..128x128 tree of the general decoder "
                            "has no picture-level pass)"}
+
+
+def _general_part(spec):
+    """One synthetic general-decoder picture (a task of the spawned pool)."""
+    load_pkg()
+    from rustmpeg_next_b200 import synth
+
+    return synth.random_general_picture(**spec)
+
+
+def _general_parity(task):
+    """The oracle's composition of one general picture against the GPU's
+    visible planes; returns the differing samples."""
+    sys.path.insert(0, ROOT)
+    import oracle
+
+    part, planes = task
+    want = oracle.general_picture(*part)
+    return sum(int((g != w).sum()) for g, w in zip(planes, want))
+
+
+def bench_general(pkg, dev, stream, args, timed):
+    """The batching configuration with coding trees of 4x4..128x128 blocks:
+    one intra picture per stream (resolutions drawn from 416x240 ..
+    3840x2160 with the configuration's weights, 8 or 10 bits, QP 22..37,
+    CTU 128), synthetic coding trees (QT / BT / TT splits, 67 intra modes,
+    ISP, MRL, BDPCM, CCLM, DCT-2 / MTS / LFNST / transform skip residuals),
+    deblocking, SAO and ALF, decoded by the general picture pass as one
+    batch (one graph replay) against one context and graph replay per
+    stream; every picture checked against the oracle."""
+    import multiprocessing as mp
+
+    from rustmpeg_next_b200 import synth
+
+    rng = np.random.default_rng(0x5EED0000 + 888)
+    specs = []
+    for k in range(args.general_streams):
+        w, h = synth.BATCH_RESOLUTIONS[int(rng.choice(len(synth.BATCH_RESOLUTIONS), p=synth.BATCH_WEIGHTS))]
+        specs.append(dict(vis_w=w, vis_h=h, ctu=128, bd=int(rng.choice([8, 10])), qp=int(rng.integers(22, 38)),
+                          seed=0x5EED0000 + 2000 + k))
+    t0 = time.perf_counter()
+    procs = max(1, min(os.cpu_count() or 1, len(specs)))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        parts = pool.map(_general_part, specs, chunksize=1)
+    build_s = time.perf_counter() - t0
+    batch = pkg.GenBatch(**synth.general_batch(parts))
+    px = int(sum(s["vis_w"] * s["vis_h"] for s in specs))
+    ctx = pkg.Context(dev.index)
+    ctx.set_stream(stream)
+    ctx.gen_prepare(batch)
+    levels = ctx.gen_levels
+    ctx.gen_run(graph=True)
+    outs = ctx.gen_download(batch.output_planes())
+    t1 = time.perf_counter()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        bad = pool.map(_general_parity, list(zip(parts, outs)), chunksize=1)
+    parity = {"checked": len(bad), "mismatches": sum(1 for b in bad if b), "samples_differing": int(sum(bad)),
+              "against": "oracle (its restatements composed in the reference's decode order), every picture, "
+                         "all planes", "s": round(time.perf_counter() - t1, 1)}
+    singles, single_levels = [], 0
+    for part in parts:
+        c = pkg.Context(dev.index)
+        c.set_stream(stream)
+        b = pkg.GenBatch(**synth.general_batch([part]))
+        c.gen_prepare(b)
+        single_levels += c.gen_levels
+        singles.append((c, b))
+    k = max(3, args.steps // 20)
+    for _ in range(2):
+        ctx.gen_run(graph=True)
+        for c, _ in singles:
+            c.gen_run(graph=True)
+    batched_ms = timed(lambda: ctx.gen_run(graph=True), k)
+    per_stream_ms = timed(lambda: [c.gen_run(graph=True) for c, _ in singles], k)
+    ctx.close()
+    for c, _ in singles:
+        c.close()
+    tbs = batch.tbs
+    res = sorted({(s["vis_w"], s["vis_h"]) for s in specs})
+    return {"what": "general-decoder intra pictures of independent streams (synthetic coding trees of 4x4..128x128 "
+                    "blocks: QT/BT/TT splits, 67 modes, ISP, MRL, BDPCM, CCLM, DCT-2/MTS/LFNST/transform-skip "
+                    "residuals, dependent quantisation off; deblocking, SAO, ALF) in one batched pass (one graph "
+                    "replay) against one context and graph replay per stream",
+            "streams": len(specs), "pictures": len(specs), "resolutions": [f"{w}x{h}" for w, h in res],
+            "bit_depths": {str(b): sum(1 for s in specs if s["bd"] == b) for b in (8, 10)},
+            "blocks": int(len(tbs)), "groups": int(len(batch.group_first) - 1),
+            "luma_block_sizes": sorted({f"{int(t['w'])}x{int(t['h'])}" for t in tbs["pred"][tbs["pred"]["comp"] == 0]},
+                                       key=lambda s: tuple(map(int, s.split("x")))),
+            "levels_batched": levels, "levels_per_stream_sum": single_levels,
+            "mpx_per_step": round(px / 1e6, 2),
+            "batched_ms": round(batched_ms, 3), "per_stream_ms": round(per_stream_ms, 3),
+            "batched_mpx_s": round(px / (batched_ms * 1e-3) / 1e6, 1),
+            "per_stream_mpx_s": round(px / (per_stream_ms * 1e-3) / 1e6, 1),
+            "speedup": round(per_stream_ms / batched_ms, 2), "parity": parity, "build_s": round(build_s, 1)}
 
 
 def _cpu_model():

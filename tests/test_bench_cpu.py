@@ -60,3 +60,19 @@ def test_frame_sources_task_makes_the_workload_frame():
     want = synth.workload_sources(5, p, 1)
     assert got[0].shape == (bench.CODED_H, bench.PIX_W)
     assert all(np.array_equal(a, b) for a, b in zip(got, want))
+
+
+def test_general_section_tasks():
+    """The coding-tree section's pool tasks: one synthetic picture, and its
+    parity count (zero against the oracle's own planes, nonzero when one
+    sample is off)."""
+    import numpy as np
+    import oracle
+
+    oracle.build()
+    part = bench._general_part(dict(vis_w=96, vis_h=64, ctu=32, bd=8, qp=30, seed=5))
+    planes = [p.copy() for p in oracle.general_picture(*part)]
+    assert bench._general_parity((part, planes)) == 0
+    planes[1][3, 4] ^= 1
+    assert bench._general_parity((part, planes)) == 1
+    assert planes[0].shape == (64, 96) and planes[1].dtype == np.uint16
