@@ -110,15 +110,17 @@ __device__ void gi_fill_side(const vvcg_gen_intra_state& S, int c, int len, int1
   const int lane = threadIdx.x & 31;
   int carry = -1;  // value of the last available position of earlier chunks
   int first = -1;
+  const int pw = c ? (int)S.width >> 1 : (int)S.width, ph = c ? (int)S.height >> 1 : (int)S.height;
   for (int k0 = 0; k0 < len; k0 += 32) {
     const int k = k0 + lane;
+    // the sample is loaded with the availability lookup, not after it (one
+    // memory round trip instead of two); unavailable ones are dropped
+    int px = 0, py = 0;
+    if (k < len) pos(k, &px, &py);
+    const bool inplane = k < len && px >= 0 && py >= 0 && px < pw && py < ph;
+    int v = inplane ? gi_get(S, c, px, py) : -1;
     const bool a = k < len && av(k);
-    int v = -1;
-    if (a) {
-      int px, py;
-      pos(k, &px, &py);
-      v = gi_get(S, c, px, py);
-    }
+    if (!a) v = -1;
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, a);
     if (first < 0 && m) first = __shfl_sync(0xFFFFFFFFu, v, __ffs(m) - 1);
     const uint32_t below = m & ((1u << lane) - 1u);
@@ -499,9 +501,10 @@ __device__ void gi_cclm(const vvcg_gen_intra_state& S, int comp, int mode, int x
   __syncwarp();
 }
 
-// The prediction of one request into out (w x h int16, row-major), by the
-// calling warp.
-__device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R, int16_t* out, GiWs& W) {
+// The prediction of one request, by the calling warp: emit(i, v) per sample
+// (i: raster index in the w x h block), once every reference is in W.
+template <class Emit>
+__device__ void gi_predict_emit(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R, GiWs& W, Emit emit) {
   const int lane = threadIdx.x & 31;
   const int bd = S.bit_depth;
   if (R.comp == 0) {
@@ -511,7 +514,7 @@ __device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_r
     const int pw = region ? 4 : R.w, ph = R.h, col0 = R.x - px;
     auto put = [&](int i, int v) {
       const int yy = i / pw, xx = i - yy * pw - col0;
-      if (xx >= 0 && xx < R.w) out[yy * R.w + xx] = (int16_t)v;
+      if (xx >= 0 && xx < R.w) emit(yy * R.w + xx, v);
     };
     if (R.bdpcm) {
       gi_gather_len(S, 0, true, px, R.y, 2 * pw, 2 * ph, W);
@@ -559,7 +562,7 @@ __device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_r
     return;
   }
   // chroma
-  auto put = [&](int i, int v) { out[i] = (int16_t)v; };
+  auto put = [&](int i, int v) { emit(i, v); };
   const int w = R.w, h = R.h;
   if (R.mode >= 81 && R.mode <= 83) {
     gi_cclm(S, R.comp, R.mode - 81, R.x, R.y, w, h, put);
@@ -576,6 +579,11 @@ __device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_r
   gi_rows_from_refs(2 * w, 2 * h, W);
   const GiAng P = gi_ang_params(min((int)R.mode, 66), w, h, w, h, false, 0, false);
   gi_angular(P, w, h, false, 0, bd, W, put);
+}
+
+// The prediction of one request into out (w x h int16, row-major).
+__device__ void gi_predict(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R, int16_t* out, GiWs& W) {
+  gi_predict_emit(S, R, W, [&](int i, int v) { out[i] = (int16_t)v; });
 }
 
 __global__ void __launch_bounds__(kGiWarps * 32) k_gen_intra(const __grid_constant__ GenIntraArgs A) {
@@ -635,6 +643,34 @@ __device__ void gi_recon_block(const vvcg_gen_intra_state& S, const vvcg_gen_int
   __syncwarp();
 }
 
+// gi_recon_block without the prediction buffer: each predicted sample goes
+// straight into the plane with its residual added and clipped.
+__device__ void gi_recon_block_fused(const vvcg_gen_intra_state& S, const vvcg_gen_intra_req& R,
+                                     const int16_t* __restrict__ res, GiWs& ws, int lane) {
+  const int maxv = (1 << S.bit_depth) - 1;
+  uint16_t* pl = const_cast<uint16_t*>(S.plane[R.comp]);
+  const int st = (int)S.stride[R.comp];
+  gi_predict_emit(S, R, ws, [&](int i, int v) {
+    const int yy = i / R.w, xx = i - yy * R.w;
+    pl[(size_t)(R.y + yy) * st + R.x + xx] = (uint16_t)clampi(v + (int)res[i], 0, maxv);
+  });
+  __syncwarp();
+  if (R.comp == 0) {
+    uint8_t* dm = const_cast<uint8_t*>(S.dec_y);
+    const int cw = (int)S.width >> 2;
+    const int x0 = R.x >> 2, x1 = min((R.x + R.w + 3) >> 2, cw), y0 = R.y >> 2;
+    const int y1 = min((R.y + R.h + 3) >> 2, (int)S.height >> 2);
+    for (int i = lane; i < (x1 - x0) * (y1 - y0); i += 32)
+      dm[(size_t)(y0 + i / (x1 - x0)) * cw + x0 + i % (x1 - x0)] = 1;
+  } else {
+    uint8_t* dm = const_cast<uint8_t*>(S.dec_c);
+    const int cw = (int)S.width >> 1;
+    for (int i = lane; i < R.w * R.h; i += 32) dm[(size_t)(R.y + i / R.w) * cw + R.x + i % R.w] = 1;
+  }
+  __threadfence_block();
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(kGiWarps * 32) k_gen_intra_recon(const __grid_constant__ GenReconArgs A) {
   __shared__ GiWs ws[kGiWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -670,7 +706,7 @@ __global__ void __launch_bounds__(kGiWarps * 32) k_gen_recon_level(const __grid_
     const vvcg_gen_intra_state& S = A.states[A.group_pic[g]];
     for (uint32_t q = A.group_first[g]; q < A.group_first[g + 1]; q++) {
       const vvcg_gen_intra_req R = A.reqs[q];
-      gi_recon_block(S, R, A.pred + R.out_off, A.res + R.out_off, ws[warp], lane);
+      gi_recon_block_fused(S, R, A.res + R.out_off, ws[warp], lane);
     }
   }
 }
