@@ -981,6 +981,48 @@ vvcg_status vvcg_decode_general_batch(vvcg_ctx* ctx, const vvcg_gen_batch* b, co
 /* Dependency levels of the prepared batch (the intra kernel's launches per run). */
 uint32_t vvcg_gen_levels(const vvcg_ctx* ctx);
 
+/* ---- CABAC parse of strict-profile pictures (host) ------------------------ */
+
+/* One IDR picture of the strict 8-bit 4:2:0 intra profile: its slice data
+ * (the CABAC substream the reference's encode_picture writes, slice.rs:325),
+ * coded size (multiples of 32, CTU 32) and slice QP, and where its records
+ * and levels go. */
+typedef struct vvcg_strict_substream {
+  const uint8_t* data;
+  uint64_t size;
+  uint32_t width, height;
+  uint8_t qp;
+  uint8_t reserved[3];
+  uint32_t cu_offset;     /* first of its (width / 32) * (height / 32) records in cus */
+  uint64_t level_offset;  /* first level it writes (even with sparse) */
+  uint64_t level_cap;     /* levels it may write */
+} vvcg_strict_substream;
+
+/* Parses each picture's slice data on the host as decode_picture does
+ * (slice.rs:458-575: luma and chroma modes, cbfs, transform_skip_flag,
+ * residual_coding / residual_ts_coding, lfnst_idx and mts_idx where present,
+ * end_of_slice_one_bit) into frame-path CU records (VVCG_TOOL_TU_TOOLS
+ * tu_tools; level_off absolute in `levels`) and levels, dense or, with
+ * sparse != 0, in the VVCG_TOOL_SPARSE_LEVELS form. Pictures are parsed in
+ * parallel on `threads` host threads (0: one). levels_used[i] receives the
+ * levels picture i wrote. VVCG_LIMIT_EXCEEDED when a picture's level_cap is
+ * too small, VVCG_INVALID_INPUT for a malformed substream; err (optional)
+ * receives the reason. No device work. */
+vvcg_status vvcg_parse_strict(const vvcg_strict_substream* pics, uint32_t num_pics, uint32_t sparse,
+                              uint32_t threads, vvcg_cu_rec* cus, uint64_t num_cus, int16_t* levels,
+                              uint64_t num_levels, uint64_t* levels_used, char* err, size_t err_cap);
+
+enum { VVCG_PARSE_LUMA = 1, VVCG_PARSE_DEP_QUANT = 2, VVCG_PARSE_SIGN_HIDING = 4, VVCG_PARSE_TRANSFORM_SKIP = 8 };
+
+/* One block's CABAC substream (its residual_coding, or with
+ * VVCG_PARSE_TRANSFORM_SKIP its residual_ts_coding, on fresh I-slice
+ * contexts at qp, then end_of_slice_one_bit and the byte alignment) into w x
+ * h raster levels (out, host int32): the parser's residual decoding alone
+ * (residual.rs:534-881 decode_residual_with_options, slice.rs:1323-1435
+ * decode_ts_block). VVCG_INVALID_INPUT for a malformed substream. */
+vvcg_status vvcg_parse_residual_block(const uint8_t* data, uint64_t size, uint32_t w, uint32_t h, uint32_t flags,
+                                      uint32_t qp, int32_t* out);
+
 /* ---- inter-prediction tools (BDOF, DMVR, affine / PROF, CIIP, GPM) -------- */
 
 /* A block of the batched inter tools: w x h samples at `off` of the tool's

@@ -118,6 +118,8 @@ def _declare(L):
     L.orc_inter_ctu_deblock.restype = None
     L.orc_strict_encode.argtypes = [vp, vp, vp, i, i, i, i, vp, vp, vp, vp, vp, vp]
     L.orc_strict_decode.argtypes = [vp, vp, C.c_uint64, i, i, i, i, vp, vp, vp]
+    L.orc_strict_write.argtypes = [vp, vp, C.c_uint64, i, i, i, vp, C.c_uint64, vp]
+    L.orc_block_write.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint64, vp]
     L.orc_bdof.argtypes = [vp, vp, i, i, vp]
     L.orc_bdof.restype = None
     L.orc_dmvr.argtypes = [vp, vp, i, i, i, i, i, i, i, vp]
@@ -600,6 +602,37 @@ def strict_decode(cus, levels, w, h, qp, ctu_log2=5):
     if rc:
         raise ValueError(f"strict_decode rejected ({rc})")
     return ry, ru, rv
+
+
+def strict_write(cus, levels, w, h, qp):
+    """The slice data encode_picture writes (slice.rs:407-455, with
+    cabac.rs BinEncoder and residual.rs / slice.rs residual coding) for
+    records as strict_encode returns them; bytes."""
+    cus = np.ascontiguousarray(cus, dtype=CU_DTYPE)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    cap = 64 + 4 * levels.size + 16 * len(cus)
+    out = np.zeros(cap, np.uint8)
+    n = C.c_uint64(0)
+    rc = lib().orc_strict_write(_p(cus), _p(levels), levels.size, w, h, qp, _p(out), cap, C.byref(n))
+    if rc:
+        raise ValueError(f"strict_write rejected the records ({rc})")
+    return out[:n.value].tobytes()
+
+
+def block_write(levels, luma=True, dep_quant=False, sign_hiding=False, ts=False, qp=26):
+    """One block's residual_coding (residual.rs encode_residual_with_options)
+    or residual_ts_coding (slice.rs encode_ts_block) on fresh I-slice
+    contexts, then the terminating bin and byte alignment; bytes."""
+    lv = np.ascontiguousarray(levels, dtype=np.int32)
+    h, w = lv.shape
+    cap = 64 + 8 * lv.size
+    out = np.zeros(cap, np.uint8)
+    n = C.c_uint64(0)
+    rc = lib().orc_block_write(_p(lv), w, h, int(luma), int(dep_quant), int(sign_hiding), int(ts), qp, _p(out), cap,
+                               C.byref(n))
+    if rc:
+        raise ValueError(f"block_write rejected the block ({rc})")
+    return out[:n.value].tobytes()
 
 
 def recon_frame(pic, cus, levels, ctus, aps=None):

@@ -150,6 +150,13 @@ int strict_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, i
                   vvcg_cu_rec* cus, int16_t* levels, uint64_t* num_levels, uint8_t* ry, uint8_t* ru, uint8_t* rv);
 int strict_decode(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
                   int ctu_log2, uint8_t* ry, uint8_t* ru, uint8_t* rv);
+// orc_cabac.cpp: the encoder side of CABAC (cabac.rs BinEncoder, residual.rs
+// encode_residual_with_options, slice.rs encode_ts_block and encode_picture's
+// syntax writes) for records as strict_encode returns them, and for one block.
+int strict_write(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                 std::vector<uint8_t>* out);
+int block_write(const int32_t* c, int w, int h, bool luma, bool dq, bool sdh, bool ts, int qp,
+                std::vector<uint8_t>* out);
 // The GPU encoder's CTU full search (orc_search.cpp; no reference counterpart).
 void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, const uint8_t* cand,
                 uint32_t lambda_q8, uint32_t* cost, uint32_t split_cost[6], int* split, int* cu_mode, int modes[4]);

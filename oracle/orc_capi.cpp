@@ -304,3 +304,28 @@ extern "C" int orc_strict_decode(const void* cus, const int16_t* levels, uint64_
                                  int ctu_log2, uint8_t* ry, uint8_t* ru, uint8_t* rv) {
   return orc::strict_decode((const vvcg_cu_rec*)cus, levels, num_levels, w, h, qp, ctu_log2, ry, ru, rv);
 }
+
+// cabac.rs / residual.rs / slice.rs encoder side (orc_cabac.cpp): a strict
+// picture's slice data, or one residual block's substream. Returns 0 and the
+// byte count in *size, -1000 when `cap` is too small, or the writer's code.
+extern "C" int orc_strict_write(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                                uint8_t* out, uint64_t cap, uint64_t* size) {
+  std::vector<uint8_t> b;
+  const int rc = orc::strict_write((const vvcg_cu_rec*)cus, levels, num_levels, w, h, qp, &b);
+  if (rc) return rc;
+  if (b.size() > cap) return -1000;
+  memcpy(out, b.data(), b.size());
+  *size = b.size();
+  return 0;
+}
+extern "C" int orc_block_write(const int32_t* c, int w, int h, int luma, int dq, int sdh, int ts, int qp, uint8_t* out,
+                               uint64_t cap, uint64_t* size) {
+  std::vector<uint8_t> b;
+  const int rc = orc::block_write(c, w, h, luma != 0, dq != 0, sdh != 0, ts != 0, qp, &b);
+  if (rc) return rc;
+  if (b.size() > cap) return -1000;
+  memcpy(out, b.data(), b.size());
+  *size = b.size();
+  return 0;
+}
+

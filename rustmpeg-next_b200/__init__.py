@@ -187,6 +187,12 @@ class _GenBatch(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class _StrictSubstream(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("qp", C.c_uint8), ("reserved", C.c_uint8 * 3), ("cu_offset", C.c_uint32),
+                ("level_offset", C.c_uint64), ("level_cap", C.c_uint64)]
+
+
 class _PlaneOut(C.Structure):
     _fields_ = [("data", C.c_void_p), ("stride", C.c_uint32), ("reserved", C.c_uint32)]
 
@@ -303,6 +309,8 @@ def lib():
         L.vvcg_decode_general_batch.argtypes = [vp, vp, vp]
         L.vvcg_gen_levels.argtypes = [vp]
         L.vvcg_gen_levels.restype = u32
+        L.vvcg_parse_strict.argtypes = [vp, u32, u32, u32, vp, u64, vp, u64, vp, C.c_char_p, C.c_size_t]
+        L.vvcg_parse_residual_block.argtypes = [vp, u64, u32, u32, u32, u32, vp]
         _lib = L
     return _lib
 
@@ -1082,3 +1090,58 @@ def lmcs_build(aps, bit_depth):
     if st != OK:
         raise _ERRORS.get(st, Execution)("invalid LMCS APS")
     return t[0]
+
+
+PARSE_LUMA, PARSE_DEP_QUANT, PARSE_SIGN_HIDING, PARSE_TRANSFORM_SKIP = 1, 2, 4, 8
+
+
+def parse_strict(streams, sparse=False, threads=0):
+    """Parse strict-profile slice data on the host (vvcg_parse_strict).
+
+    streams: [(bytes, width, height, qp)]. Returns (pics, cus, levels): a
+    PIC_DTYPE batch (8-bit 4:2:0, CTU 32, VVCG_TOOL_TU_TOOLS, plus
+    VVCG_TOOL_SPARSE_LEVELS when sparse), the CU records and the level pool,
+    ready for Batch / decode_batch."""
+    L = lib()
+    n = len(streams)
+    subs = (_StrictSubstream * max(1, n))()
+    bufs, cu_at, lv_at = [], 0, 0
+    for i, (data, w, h, qp) in enumerate(streams):
+        buf = np.frombuffer(bytes(data), np.uint8)
+        bufs.append(buf)
+        ncu = (w // 32) * (h // 32)
+        cap = (w * h * 3) // 2 * (2 if sparse else 1) + 8 * ncu
+        subs[i] = _StrictSubstream(_ptr(buf) if buf.size else None, buf.size, w, h, qp, (C.c_uint8 * 3)(), cu_at,
+                                   lv_at, cap)
+        cu_at += ncu
+        lv_at += cap + (cap & 1)
+    cus = np.zeros(cu_at, CU_DTYPE)
+    levels = np.zeros(max(1, lv_at), np.int16)
+    used = np.zeros(max(1, n), np.uint64)
+    err = C.create_string_buffer(256)
+    st = L.vvcg_parse_strict(subs, n, int(sparse), threads, _ptr(cus), len(cus), _ptr(levels), levels.size,
+                             _ptr(used), err, 256)
+    if st != OK:
+        raise _ERRORS.get(st, Execution)(err.value.decode())
+    pics = np.zeros(n, PIC_DTYPE)
+    for i, (_, w, h, qp) in enumerate(streams):
+        p = pics[i:i + 1]
+        p["width"], p["height"], p["visible_width"], p["visible_height"] = w, h, w, h
+        p["bit_depth"], p["chroma_format"], p["ctu_log2"], p["slice_qp"] = 8, CHROMA_420, 5, qp
+        qpc = min(63, max(0, qp if qp <= 26 else qp - 1))  # derived_chroma_qp (hls.rs:778) at 8 bits
+        p["chroma_qp_scaled"] = qpc
+        p["tools"] = TOOL_TU_TOOLS | (TOOL_SPARSE_LEVELS if sparse else 0)
+        p["alf_aps"] = -1
+        p["cu_offset"] = subs[i].cu_offset
+    return pics, cus, levels, used[:n].copy()
+
+
+def parse_residual_block(data, w, h, flags, qp):
+    """One block's substream into (h, w) int32 levels (vvcg_parse_residual_block)."""
+    buf = np.frombuffer(bytes(data), np.uint8)
+    out = np.zeros((h, w), np.int32)
+    st = lib().vvcg_parse_residual_block(_ptr(buf) if buf.size else None, buf.size, w, h, flags, qp, _ptr(out))
+    if st != OK:
+        raise _ERRORS.get(st, Execution)("malformed residual substream")
+    return out
+

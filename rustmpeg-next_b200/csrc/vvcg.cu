@@ -2811,3 +2811,77 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
 }
 
 #include "gen_picture.cuh"
+
+// ---------------------------------------------------------------------------
+// CABAC parse of strict-profile pictures on the host (vvcg_parse_strict).
+// ---------------------------------------------------------------------------
+#include <atomic>
+#include <thread>
+
+#include "cabac_parse.h"
+
+extern "C" vvcg_status vvcg_parse_strict(const vvcg_strict_substream* pics, uint32_t num_pics, uint32_t sparse,
+                                         uint32_t threads, vvcg_cu_rec* cus, uint64_t num_cus, int16_t* levels,
+                                         uint64_t num_levels, uint64_t* levels_used, char* err, size_t err_cap) {
+  if (err && err_cap) err[0] = 0;
+  if (!num_pics) return VVCG_OK;
+  if (!pics || !cus || !levels || !levels_used)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "missing pictures, records, levels or counts");
+  for (uint32_t i = 0; i < num_pics; i++) {
+    const vvcg_strict_substream& p = pics[i];
+    if (!p.data && p.size) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: missing data", i);
+    if (!p.width || !p.height || p.width % 32 || p.height % 32 || p.width > 16384 || p.height > 16384)
+      return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: coded size not a multiple of 32", i);
+    if (p.qp > 63) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: slice QP above 63", i);
+    if ((uint64_t)p.cu_offset + (uint64_t)(p.width / 32) * (p.height / 32) > num_cus)
+      return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: records past the array", i);
+    if (p.level_offset + p.level_cap > num_levels || (sparse && (p.level_offset & 1)))
+      return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: level range", i);
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<int> code(num_pics, 0);
+  auto work = [&]() {
+    for (uint32_t i; (i = next.fetch_add(1)) < num_pics;) {
+      const vvcg_strict_substream& p = pics[i];
+      vvcg_parse::LevelSink sink{levels + p.level_offset, p.level_cap, 0, sparse != 0};
+      code[i] = vvcg_parse::parse_strict_picture(p.data, p.size, p.qp, (int)p.width, (int)p.height,
+                                                 cus + p.cu_offset, sink, (int64_t)p.level_offset);
+      levels_used[i] = sink.at;
+    }
+  };
+  const uint32_t n = std::max<uint32_t>(1, std::min<uint32_t>(threads ? threads : 1, num_pics));
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < n; t++) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  static const char* kWhy[] = {"", "last position outside the block", "level outside 16 bits", "syntax",
+                               "level capacity exceeded", "no end of slice or alignment"};
+  for (uint32_t i = 0; i < num_pics; i++)
+    if (code[i])
+      return static_fail(err, err_cap, code[i] == 4 ? VVCG_LIMIT_EXCEEDED : VVCG_INVALID_INPUT,
+                         "picture %u: %s", i, kWhy[std::min(code[i], 5)]);
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_parse_residual_block(const uint8_t* data, uint64_t size, uint32_t w, uint32_t h,
+                                                 uint32_t flags, uint32_t qp, int32_t* out) {
+  if (!out || (!data && size)) return VVCG_INVALID_INPUT;
+  if (w < 1 || h < 1 || w > 64 || h > 64 || (w & (w - 1)) || (h & (h - 1)) || w * h < 2 || qp > 63)
+    return VVCG_INVALID_INPUT;
+  if ((flags & VVCG_PARSE_TRANSFORM_SKIP) && (w > 32 || h > 32)) return VVCG_INVALID_INPUT;
+  const vvcg_parse::Scan s = vvcg_parse::make_scan((int)w, (int)h);
+  vvcg_parse::Reader r;
+  r.start(data, size);
+  vvcg_parse::Models m;
+  m.init_i_slice((int)qp);
+  if (flags & VVCG_PARSE_TRANSFORM_SKIP) {
+    vvcg_parse::decode_ts_residual(r, m, s, out);
+  } else if (vvcg_parse::decode_residual(r, m, s, out, (flags & VVCG_PARSE_LUMA) != 0,
+                                         (flags & VVCG_PARSE_DEP_QUANT) != 0,
+                                         (flags & VVCG_PARSE_SIGN_HIDING) != 0) != vvcg_parse::kOk) {
+    return VVCG_INVALID_INPUT;
+  }
+  if (!r.terminate() || !r.aligned_end()) return VVCG_INVALID_INPUT;
+  return VVCG_OK;
+}
+
