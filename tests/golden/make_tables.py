@@ -4,7 +4,7 @@ Reads the Rust sources of the reference's VVC module (the path below; run it
 where the reference tree is mounted) and writes, for every table the
 kernels and the oracle use, the flat list of its values in row-major order
 together with the file:line of its declaration. tests/test_tables_golden.py
-compares rustmpeg-next_b200/csrc/vvc_tables.h with that file entry by entry,
+compares rustmpeg-next_b200/csrc/vvc_tables.h and vvc_cabac.h with that file entry by entry,
 so a transcription error in the shared header cannot pass the GPU parity
 tests unnoticed.
 
@@ -41,6 +41,9 @@ TABLES = [
     ("predict.rs", "ANG_TABLE"), ("predict.rs", "INV_ANG_TABLE"), ("predict.rs", "INTRA_FILTER_THRESHOLD"),
     ("predict.rs", "CHROMA_FILTER_4TAP"), ("predict.rs", "CCLM_DIV_SIG_TABLE"),
     ("predict.rs", "MIP_MATRIX_4X4"), ("predict.rs", "MIP_MATRIX_8X8"), ("predict.rs", "MIP_MATRIX_16X16"),
+    ("cabac.rs", "CTX_INIT_I"), ("cabac.rs", "RENORM_LPS"),
+    ("residual.rs", "PREFIX_CTX"), ("residual.rs", "MIN_IN_GROUP"), ("residual.rs", "GROUP_IDX"),
+    ("residual.rs", "GO_RICE_PARS_COEFF"),
 ]
 
 
@@ -58,7 +61,11 @@ def extract(src: str, name: str):
     m = re.search(r"\bconst\s+" + re.escape(name) + r"\s*:\s*(.*?)=\s*\[", clean, re.S)
     if not m:
         raise KeyError(name)
-    dims = [int(d) for d in re.findall(r";\s*(\d+)\s*\]", m.group(1))][::-1]
+    names = {k: int(v) for k, v in re.findall(r"\bconst\s+(\w+)\s*:\s*usize\s*=\s*(\d+)\s*;", clean)}
+    dims = [int(d) if d.isdigit() else names[d] for d in re.findall(r";\s*(\w+)\s*\]", m.group(1))][::-1]
+    tup = re.search(r"\(([^)]*)\)", m.group(1))
+    if tup:  # an array of tuples: one more dimension, the tuple's arity
+        dims.append(len(tup.group(1).split(",")))
     start = m.end() - 1
     depth = 0
     for i in range(start, len(clean)):
@@ -81,6 +88,22 @@ def extract(src: str, name: str):
     return vals, dims, line
 
 
+def context_offsets(src: str):
+    """The first context of every syntax element's set: the constants of
+    cabac.rs's `pub mod ctx`, name -> value, and the line of the module."""
+    clean = _strip_comments(src)
+    start = clean.index("pub mod ctx")
+    depth, i = 0, clean.index("{", start)
+    for j in range(i, len(clean)):
+        depth += clean[j] == "{"
+        depth -= clean[j] == "}"
+        if depth == 0:
+            break
+    body = clean[i:j]
+    vals = {k: int(v) for k, v in re.findall(r"pub\s+const\s+(\w+)\s*:\s*usize\s*=\s*(\d+)\s*;", body)}
+    return vals, src.count("\n", 0, start) + 1
+
+
 def main(root: str = DEFAULT_ROOT) -> str:
     out = {"_source": "table literals of crates/rustmpeg-video/src/vvc/*.rs of the reference, "
                       "extracted by tests/golden/make_tables.py"}
@@ -90,6 +113,8 @@ def main(root: str = DEFAULT_ROOT) -> str:
             cache[fname] = open(os.path.join(root, VVC, fname)).read()
         vals, dims, line = extract(cache[fname], name)
         out[name] = {"at": f"V/{fname}:{line}", "dims": dims, "values": vals}
+    offs, line = context_offsets(cache["cabac.rs"])
+    out["_ctx_offsets"] = {"at": f"V/cabac.rs:{line}", "values": offs}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tables.json")
     with open(dst, "w") as f:
         json.dump(out, f, separators=(",", ":"))

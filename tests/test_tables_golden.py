@@ -39,15 +39,20 @@ PAIRS = {
     "kIntraFilterThreshold": ["INTRA_FILTER_THRESHOLD"], "kChromaTaps4": ["CHROMA_FILTER_4TAP"],
     "kCclmDivSig": ["CCLM_DIV_SIG_TABLE"],
     "kMip4x4": ["MIP_MATRIX_4X4"], "kMip8x8": ["MIP_MATRIX_8X8"], "kMip16x16": ["MIP_MATRIX_16X16"],
+    # vvc_cabac.h
+    "kCtxInitI": ["CTX_INIT_I"], "kRenormLps": ["RENORM_LPS"], "kPrefixCtx": ["PREFIX_CTX"],
+    "kMinInGroup": ["MIN_IN_GROUP"], "kGroupIdx": ["GROUP_IDX"], "kGoRicePars": ["GO_RICE_PARS_COEFF"],
 }
+CABAC_HDR = os.path.join(ROOT, "rustmpeg-next_b200", "csrc", "vvc_cabac.h")
 
 
 def header_tables():
-    """Every `static const <type> kName[..]...[..] = { ... };` of the header,
-    flattened row-major, keyed by name."""
-    src = re.sub(r"//[^\n]*", "", open(HDR).read())
+    """Every `static const <type> kName[..]...[..] = { ... };` (or constexpr)
+    of the two headers, flattened row-major, keyed by name."""
+    src = re.sub(r"//[^\n]*", "", open(HDR).read() + open(CABAC_HDR).read())
+    src = src.replace("[kNumContexts]", "[379]")
     out = {}
-    for m in re.finditer(r"static\s+const\s+\w+\s+(k\w+)\s*((?:\[\s*\d+\s*\])+)\s*=\s*\{", src):
+    for m in re.finditer(r"(?:static\s+const|constexpr)\s+\w+\s+(k\w+)\s*((?:\[\s*\d+\s*\])+)\s*=\s*\{", src):
         depth, i = 0, m.end() - 1
         while True:
             if src[i] == "{":
@@ -89,6 +94,16 @@ def test_header_table_equals_reference_literal(name, gold, hdr):
 def test_every_golden_table_is_checked(gold):
     used = {r for refs in PAIRS.values() for r in refs}
     assert used == {k for k in gold if not k.startswith("_")}
+
+
+def test_context_offsets_equal_the_reference(gold):
+    """The first context of each syntax element's set (vvc_cabac.h kCtx*)
+    against cabac.rs's ctx module, every constant."""
+    src = open(CABAC_HDR).read()
+    got = {m.group(1): int(m.group(2)) for m in re.finditer(r"constexpr\s+int\s+kCtx(\w+)\s*=\s*(\d+)\s*;", src)}
+    ref = gold["_ctx_offsets"]["values"]
+    camel = {"".join(w.capitalize() for w in k.lower().split("_")): v for k, v in ref.items()}
+    assert got == camel, sorted(set(got.items()) ^ set(camel.items()))[:5]
 
 
 def test_dct2_matrices_nest(hdr):
