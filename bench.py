@@ -369,6 +369,8 @@ def main():
     ap.add_argument("--batch-frames", type=int, default=8)
     ap.add_argument("--no-general", action="store_true", help="skip the coding-tree (general decoder) section")
     ap.add_argument("--general-streams", type=int, default=64)
+    ap.add_argument("--no-streams", action="store_true", help="skip the slice-data (CABAC parse) section")
+    ap.add_argument("--stream-pictures", type=int, default=64)
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -602,6 +604,8 @@ def main():
         line["batching"] = bench_batching(pkg, dev, stream, args, timed)
     if world == 1 and not args.no_general:
         line["general"] = bench_general(pkg, dev, stream, args, timed)
+    if world == 1 and not args.no_streams:
+        line["streams"] = bench_streams(pkg, dev, stream, args, timed)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics_d, cus_d, levels_d, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
@@ -936,6 +940,86 @@ def bench_general(pkg, dev, stream, args, timed):
             "batched_mpx_s": round(px / (batched_ms * 1e-3) / 1e6, 1),
             "per_stream_mpx_s": round(px / (per_stream_ms * 1e-3) / 1e6, 1),
             "speedup": round(per_stream_ms / batched_ms, 2), "parity": parity, "build_s": round(build_s, 1)}
+
+
+STRICT_STREAMS = os.path.join(ROOT, "tests", "golden", "strict_streams_1080p.npz")
+
+
+def bench_streams(pkg, dev, stream, args, timed):
+    """Slice data to pixels for the strict 8-bit intra profile: the committed
+    CABAC slice data of 16 pictures of 1920x1088 (the full-frame content at 8
+    bits, QP 22..37; tests/golden/strict_streams_1080p.npz), repeated to a
+    batch, parsed on the host (vvcg_parse_strict, sparse levels) and decoded
+    on the GPU (frame path with per-TB transform skip / MTS / LFNST). Every
+    decoded picture is hashed against the encoder's reconstruction the
+    fixture holds."""
+    import hashlib
+
+    z = np.load(STRICT_STREAMS)
+    data, offs = z["data"], z["offsets"]
+    w, h = int(z["width"]), int(z["height"])
+    base = [(data[offs[i]:offs[i + 1]].tobytes(), w, h, int(z["qp"][i])) for i in range(len(offs) - 1)]
+    hashes = [str(x) for x in z["sha256"]]
+    reps = max(1, args.stream_pictures // len(base))
+    streams = base * reps
+    threads = os.cpu_count() or 1
+    px = len(streams) * w * h
+    nbytes = sum(len(b) for b, _, _, _ in streams)
+
+    def parse_ms(nthreads, k):
+        best = None
+        for _ in range(k):
+            t0 = time.perf_counter()
+            out = pkg.parse_strict(streams, sparse=True, threads=nthreads)
+            dt = (time.perf_counter() - t0) * 1e3
+            best = dt if best is None else min(best, dt)
+        return best, out
+
+    one_ms, _ = parse_ms(1, 2)
+    all_ms, (pics, cus, levels, used) = parse_ms(threads, 5)
+    batch = pkg.Batch(pics, cus, levels)
+    ctx = pkg.Context(dev.index)
+    ctx.set_stream(stream)
+    ctx.prepare(batch)
+    ctx.upload(batch)
+    ctx.run(pkg.STAGE_ALL)
+    ctx.sync()
+    outs = ctx.download(batch.output_planes())
+    bad = 0
+    for i, o in enumerate(outs):
+        hh = hashlib.sha256()
+        for p in o:
+            hh.update(p.astype(np.uint8).tobytes())
+        bad += hh.hexdigest() != hashes[i % len(hashes)]
+    for _ in range(3):
+        ctx.run(pkg.STAGE_ALL, graph=True)
+    dev_ms = timed(lambda: ctx.run(pkg.STAGE_ALL, graph=True), max(3, args.steps // 5))
+    # slice data to host pixels: parse on every host thread, then the whole
+    # host-buffer call (upload, decode, download), step after step
+    import torch
+
+    outs2 = [tuple(torch.empty(a.shape, dtype=torch.int16).pin_memory().numpy().view(np.uint16) for a in o)
+             for o in outs]
+    k = max(3, args.steps // 20)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        p2, c2, l2, _ = pkg.parse_strict(streams, sparse=True, threads=threads)
+        ctx.decode_batch(pkg.Batch(p2, c2, l2), outs2)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / k
+    ctx.close()
+    return {"what": "strict 8-bit intra slice data (CABAC) of 1920x1088 pictures at QP 22..37 parsed on the host "
+                    "into sparse frame-path records, decoded on the GPU (transform skip, MTS, LFNST per TB); every "
+                    "picture's SHA-256 checked against the encoder reconstruction in the fixture",
+            "pictures": len(streams), "slice_data_bytes": int(nbytes), "mpx_per_step": round(px / 1e6, 2),
+            "parse_ms_1_thread": round(one_ms, 2), "parse_ms": round(all_ms, 2), "parse_threads": threads,
+            "parse_mpx_s": round(px / (all_ms * 1e-3) / 1e6, 1),
+            "parse_mpx_s_1_thread": round(px / (one_ms * 1e-3) / 1e6, 1),
+            "parse_mbit_s": round(nbytes * 8 / (all_ms * 1e-3) / 1e6, 1),
+            "device_ms": round(dev_ms, 3), "device_mpx_s": round(px / (dev_ms * 1e-3) / 1e6, 1),
+            "slice_data_to_pixels_ms": round(e2e_ms, 2),
+            "slice_data_to_pixels_mpx_s": round(px / (e2e_ms * 1e-3) / 1e6, 1),
+            "parity": {"checked": len(outs), "mismatches": int(bad),
+                       "against": "SHA-256 of the encoder reconstruction of each picture (fixture)"}}
 
 
 def _cpu_model():

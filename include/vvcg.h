@@ -78,7 +78,7 @@ enum {
   VVCG_TOOL_SPARSE_LEVELS = 1u << 6,
   /* decoder: the CU records carry per-TB transform choices in tu_tools (the
    * strict 8-bit decoder's transform skip, mts_idx and lfnst_idx,
-   * slice.rs:458-627); not with VVCG_TOOL_SPARSE_LEVELS */
+   * slice.rs:458-627) */
   VVCG_TOOL_TU_TOOLS = 1u << 7
 };
 

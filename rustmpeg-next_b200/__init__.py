@@ -1101,7 +1101,7 @@ def parse_strict(streams, sparse=False, threads=0):
     streams: [(bytes, width, height, qp)]. Returns (pics, cus, levels): a
     PIC_DTYPE batch (8-bit 4:2:0, CTU 32, VVCG_TOOL_TU_TOOLS, plus
     VVCG_TOOL_SPARSE_LEVELS when sparse), the CU records and the level pool,
-    ready for Batch / decode_batch."""
+    ready for Batch / decode_batch, and the levels each picture used."""
     L = lib()
     n = len(streams)
     subs = (_StrictSubstream * max(1, n))()
@@ -1123,6 +1123,22 @@ def parse_strict(streams, sparse=False, threads=0):
                              _ptr(used), err, 256)
     if st != OK:
         raise _ERRORS.get(st, Execution)(err.value.decode())
+    # one compact pool: each picture's levels moved next to the previous
+    # picture's (even offsets for the sparse form), its records rebased
+    pool_n, starts = 0, []
+    for i in range(n):
+        pool_n += pool_n & 1
+        starts.append(pool_n)
+        pool_n += int(used[i])
+    pool = np.zeros(max(1, pool_n), np.int16)
+    for i in range(n):
+        a, m = int(subs[i].level_offset), int(used[i])
+        pool[starts[i]:starts[i] + m] = levels[a:a + m]
+        c0, w, h = int(subs[i].cu_offset), streams[i][1], streams[i][2]
+        rec = cus[c0:c0 + (w // 32) * (h // 32)]
+        lo = rec["level_off"].astype(np.int64)
+        rec["level_off"] = np.where(lo >= 0, lo - a + starts[i], -1).astype(np.int32)
+    levels = pool
     pics = np.zeros(n, PIC_DTYPE)
     for i, (_, w, h, qp) in enumerate(streams):
         p = pics[i:i + 1]

@@ -553,10 +553,38 @@ constexpr int kResToolWarps = 4;
 // Records outside the ranges of vvcg_cu_rec.tu_tools, or with levels past the
 // pool, set the bad-record status and are skipped.
 // Grid: (ceil(max CUs per picture / kResToolWarps), pictures).
+// A sparse TB's (raster index, level) pairs expanded into n dense levels;
+// false when an index is outside the TB or not above the one before it.
+__device__ bool expand_sparse(const int16_t* __restrict__ lv, int count, int n, int16_t* dense, int lane) {
+  for (int i = lane; i < n; i += 32) dense[i] = 0;
+  __syncwarp();
+  const uint32_t* pr = reinterpret_cast<const uint32_t*>(lv + 2);
+  bool ok = true;
+  int prev_last = -1;
+  for (int base = 0; base < count; base += 32) {
+    const int i = base + lane;
+    const bool have = i < count;
+    const uint32_t e = have ? pr[i] : (uint32_t)n;
+    const int pos = (int)(e & 0xFFFFu);
+    int prev = __shfl_up_sync(0xffffffffu, pos, 1);
+    if (lane == 0) prev = prev_last;
+    if (have) {
+      if (pos >= n || pos <= prev)
+        ok = false;
+      else
+        dense[pos] = (int16_t)(e >> 16);
+    }
+    prev_last = __shfl_sync(0xffffffffu, pos, 31);
+  }
+  __syncwarp();
+  return __all_sync(0xffffffffu, ok);
+}
+
 __global__ void __launch_bounds__(kResToolWarps * 32)
 k_residual_tools(const DevPic* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels,
                  uint32_t* status) {
   __shared__ __align__(16) int32_t ws[kResToolWarps][2][1024 + kTuPad];
+  __shared__ __align__(16) int16_t dense[kResToolWarps][1024];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const DevPic& P = pics[blockIdx.y];
   if (!(P.tools & VVCG_TOOL_TU_TOOLS)) return;
@@ -566,15 +594,24 @@ k_residual_tools(const DevPic* __restrict__ pics, const int16_t* __restrict__ le
   const uint32_t t = rec.tu_tools;
   if (!t) return;
   const int mts = (t >> VVCG_CU_MTS_SHIFT) & 7, lfnst = t >> VVCG_CU_LFNST_SHIFT;
-  const bool bad_tools = mts > 4 || lfnst > 2 || (mts && lfnst) || ((t & VVCG_CU_TS_Y) && (mts || lfnst)) ||
-                         (P.tools & VVCG_TOOL_SPARSE_LEVELS);
+  const bool bad_tools = mts > 4 || lfnst > 2 || (mts && lfnst) || ((t & VVCG_CU_TS_Y) && (mts || lfnst));
+  const bool sparse = (P.tools & VVCG_TOOL_SPARSE_LEVELS) != 0;
   const int gx = cu % P.grid_w, gy = cu / P.grid_w;
   for (int c = 0; c < (P.cf ? 3 : 1); c++) {
     if (!tb_uses_tu_tools(t, c) || !((rec.cbf >> c) & 1)) continue;
     const int off = rec.level_off[c];
     if (off < 0) continue;
     const int w = c ? P.tb_cw : P.tb, h = c ? P.tb_ch : P.tb;
-    if (bad_tools || (uint64_t)off + (uint64_t)(w * h) > n_levels) {
+    const int16_t* src = levels + off;
+    if (sparse) {  // count at levels[off], pairs from off + 2 (off even)
+      const int cnt = (off & 1) || (uint64_t)off + 2 > n_levels ? -1 : levels[off];
+      if (bad_tools || cnt < 0 || cnt > w * h || (uint64_t)off + 2 + 2 * (uint64_t)cnt > n_levels ||
+          !expand_sparse(levels + off, cnt, w * h, dense[wid], lane)) {
+        if (lane == 0) atomicOr(status, kStatusBadRecord);
+        continue;
+      }
+      src = dense[wid];
+    } else if (bad_tools || (uint64_t)off + (uint64_t)(w * h) > n_levels) {
       if (lane == 0) atomicOr(status, kStatusBadRecord);
       continue;
     }
@@ -592,7 +629,7 @@ k_residual_tools(const DevPic* __restrict__ pics, const int16_t* __restrict__ le
     r.in_off = r.out_off = 0;
     const int x0 = c ? gx * P.tb / P.sub_w : gx * P.tb, y0 = c ? gy * P.tb / P.sub_h : gy * P.tb;
     int16_t* out = reinterpret_cast<int16_t*>(P.scratch[c]) + (size_t)y0 * P.stride[c] + x0;
-    warp_tu_inverse(r, levels + off, out, ws[wid][0], ws[wid][1], lane, P.stride[c]);
+    warp_tu_inverse(r, src, out, ws[wid][0], ws[wid][1], lane, P.stride[c]);
   }
 }
 

@@ -558,8 +558,6 @@ vvcg_status vvcg_batch_prepare(vvcg_ctx* ctx, const vvcg_batch* b) {
     if (filt && (!b->ctus || (uint64_t)d.ctu_offset + (uint64_t)cw_ * ch_ > b->num_ctus))
       return fail(ctx, VVCG_INVALID_INPUT, "picture %u: CTU filter records out of range", i);
     const bool tu_tools = (d.tools & VVCG_TOOL_TU_TOOLS) != 0;
-    if (tu_tools && (d.tools & VVCG_TOOL_SPARSE_LEVELS))
-      return fail(ctx, VVCG_INVALID_INPUT, "picture %u: per-TB transform tools need dense levels", i);
     if (tu_tools)
       for (uint32_t k = 0; k < gw * gh; k++) {
         const char* why = cu_tu_tools_error(b->cus[d.cu_offset + k].tu_tools);
@@ -2667,8 +2665,6 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
   if (d.tools & (VVCG_TOOL_SAO | VVCG_TOOL_ALF))
     return static_fail(err, err_cap, VVCG_INVALID_INPUT,
                        "SAO and ALF need a second set of planes (use vvcg_decode_batch)");
-  if ((d.tools & VVCG_TOOL_TU_TOOLS) && (d.tools & VVCG_TOOL_SPARSE_LEVELS))
-    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "per-TB transform tools need dense levels");
   const int tb = std::min<int>(ctu, 32);
   const int cf = d.chroma_format;
   const int sw = (cf == 1 || cf == 2) ? 2 : 1, sh = cf == 1 ? 2 : 1;

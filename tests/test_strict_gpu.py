@@ -127,9 +127,28 @@ def test_bad_transform_tools_are_rejected(ctx, pkg, orc):
         bad["tu_tools"][1] = t
         with pytest.raises(pkg.InvalidInput):
             ctx.decode_batch(_batch(pkg, [(p, bad, levels, rec)]))
-    sparse = p.copy()
-    sparse["tools"] = int(p["tools"]) | pkg.TOOL_SPARSE_LEVELS
-    with pytest.raises(pkg.InvalidInput):
-        ctx.decode_batch(_batch(pkg, [(sparse, cus, levels, rec)]))
     got = ctx.decode_batch(_batch(pkg, [(p, cus, levels, rec)]))  # the context still works
     _assert_planes(got[0], rec, "after rejections")
+
+
+@pytest.mark.parametrize("sparse", [False, True])
+def test_strict_bitstreams_decode_on_the_gpu(ctx, pkg, orc, sparse):
+    """From slice data to pixels: the small-picture sequence at QP 26 (and
+    the QP 4 / 50 pictures) written as CABAC slice data by the oracle's
+    encoder side, parsed by the library's host parser (dense or sparse
+    levels) and decoded on the GPU, equal to the encoder's reconstruction."""
+    from rustmpeg_next_b200 import synth
+
+    streams, recs = [], []
+    for qp in (26, 26, 26, 4, 50):
+        y, u, v = synth.config1_frame(len(streams) % 3)
+        cus, levels, rec = orc.strict_encode(y, u, v, qp)
+        streams.append((orc.strict_write(cus, levels, 64, 64, qp), 64, 64, qp))
+        recs.append(rec)
+    pics, cus, levels, _ = pkg.parse_strict(streams, sparse=sparse, threads=4)
+    ctus = np.zeros(4 * len(pics), pkg.CTU_DTYPE)
+    for i in range(len(pics)):
+        pics["ctu_offset"][i] = 4 * i
+    got = ctx.decode_batch(pkg.Batch(pics, cus, levels, ctus))
+    for k, (g, rec) in enumerate(zip(got, recs)):
+        _assert_planes(g, rec, f"stream {k}")
