@@ -1023,6 +1023,130 @@ enum { VVCG_PARSE_LUMA = 1, VVCG_PARSE_DEP_QUANT = 2, VVCG_PARSE_SIGN_HIDING = 4
 vvcg_status vvcg_parse_residual_block(const uint8_t* data, uint64_t size, uint32_t w, uint32_t h, uint32_t flags,
                                       uint32_t qp, int32_t* out);
 
+/* ---- the multi-tool stream: IDR and P pictures, picture buffer ------------ */
+
+/* Slice coding options of the multi-tool stream (SliceCodingOptions,
+ * slice.rs:1471-1507) this library's multi-tool entries take; the other
+ * tools (CCLM, MIP, MRL, ISP, BDPCM, joint Cb-Cr, SAO, ALF, LMCS, palette,
+ * IBC, ACT) are not supported by them and rejected. */
+enum {
+  VVCG_SLICE_DEP_QUANT = 1u << 0,        /* dep_quant */
+  VVCG_SLICE_SIGN_HIDING = 1u << 1,      /* sign_data_hiding (syntax only) */
+  VVCG_SLICE_DEBLOCK = 1u << 2,          /* enable_deblock (IDR: the frame path's deblocking; P: CTU boundaries) */
+  VVCG_SLICE_FULL_INTRA_MODES = 1u << 3  /* full_intra_modes (an encoder decision; no syntax change) */
+};
+
+/* One slice-data substream of the multi-tool stream: an IDR picture
+ * (encode_picture_multitool, slice.rs:2575) or a P picture
+ * (encode_inter_picture, slice.rs:3307), coded size (multiples of the CTU
+ * size), slice QP, CTU size, options, and where its records and levels go. */
+typedef struct vvcg_slice_substream {
+  const uint8_t* data;
+  uint64_t size;
+  uint32_t width, height;
+  uint8_t qp;
+  uint8_t ctu_log2;       /* 5: CTU 32, one coding unit per CTU */
+  uint8_t options;        /* VVCG_SLICE_* */
+  uint8_t reserved;
+  uint32_t cu_offset;     /* first record of the picture in the output array */
+  uint64_t level_offset;  /* first level it writes (even with sparse) */
+  uint64_t level_cap;     /* levels it may write */
+} vvcg_slice_substream;
+
+/* Parses IDR pictures of the multi-tool stream on the host as
+ * decode_picture_multitool does (slice.rs:3012-3190: per coding unit the luma
+ * mode against the MPM list of the left neighbour, the chroma mode, the cbfs,
+ * transform_skip_flag and the residuals; end_of_slice_one_bit) into
+ * frame-path records (VVCG_TOOL_TU_TOOLS with transform-skip flags only;
+ * (width / 32) * (height / 32) records, raster order), dense or sparse
+ * levels, pictures on `threads` host threads. The pictures decode on the
+ * frame path (vvcg_decode_batch) with tools TU_TOOLS, plus DEP_QUANT and
+ * DEBLOCK as the substream's options ask, at SliceQpY max(qp, 4) (the QP
+ * decode_picture_multitool reconstructs and deblocks with). Errors as
+ * vvcg_parse_strict. */
+vvcg_status vvcg_parse_multitool_idr(const vvcg_slice_substream* pics, uint32_t num_pics, uint32_t sparse,
+                                     uint32_t threads, vvcg_cu_rec* cus, uint64_t num_cus, int16_t* levels,
+                                     uint64_t num_levels, uint64_t* levels_used, char* err, size_t err_cap);
+
+enum {
+  VVCG_INTER_CU_MERGE = 1,   /* merge (or skip) coding unit: motion of merge candidate 0 */
+  VVCG_INTER_CU_SKIP = 2,    /* cu_skip_flag */
+  VVCG_INTER_CU_ALT_HPEL = 4 /* the alternative half-sample luma filter */
+};
+
+/* One coding unit (a whole CTU) of a P picture: its motion as
+ * decode_inter_picture derives it (merge candidate 0, or the AMVP predictor
+ * plus the coded difference), the cbfs, transform-skip flags and levels
+ * (level_off as in vvcg_cu_rec). mvd and mvp_idx are the parsed AMVP syntax;
+ * the GPU reads only the motion. */
+typedef struct vvcg_inter_cu {
+  int32_t mv[2][2];  /* [L0, L1][horizontal, vertical], 1/16 luma sample */
+  int32_t mvd[2];    /* AMVP: coded motion vector difference */
+  int8_t ref_idx[2]; /* per list; -1 = list unused */
+  uint8_t inter_dir; /* 1 = L0 (P pictures take L0 only) */
+  uint8_t bcw_idx;   /* 2 = equal weights */
+  uint8_t flags;     /* VVCG_INTER_CU_* */
+  uint8_t mvp_idx;   /* AMVP: predictor index */
+  uint8_t cbf;       /* bit0 Y, bit1 Cb, bit2 Cr */
+  uint8_t tu_tools;  /* bit c: transform skip of component c */
+  int32_t level_off[3];
+  uint32_t reserved;
+} vvcg_inter_cu; /* 48 bytes */
+
+/* Parses P pictures of the multi-tool stream on the host as
+ * decode_inter_picture does (slice.rs:3552-3677: cu_skip_flag with its
+ * neighbour context, pred_mode_flag, general_merge_flag, mvd_coding and
+ * mvp_l0_flag, rqt_root_cbf, the cbfs with tu_y_coded_flag inferred,
+ * transform_skip_flag and the residuals on P-slice contexts) and derives
+ * each coding unit's motion (derive_merge_candidates candidate 0 or
+ * derive_amvp_candidates plus the difference, the HMVP table reset per CTU
+ * row). One record per CTU, raster order. Intra coding units in a P picture
+ * are rejected as the reference rejects them. Errors as vvcg_parse_strict. */
+vvcg_status vvcg_parse_multitool_p(const vvcg_slice_substream* pics, uint32_t num_pics, uint32_t sparse,
+                                   uint32_t threads, vvcg_inter_cu* cus, uint64_t num_cus, int16_t* levels,
+                                   uint64_t num_levels, uint64_t* levels_used, char* err, size_t err_cap);
+
+/* The context's picture buffer: device pictures of 8-bit 4:2:0 samples in
+ * 16-bit planes (stride a multiple of 64 samples), the reference pictures of
+ * P pictures (the reference decoder's DecodedPictureBuffer, inter.rs:446,
+ * kept on the device). vvcg_dpb_reserve makes `slots` slots of width x
+ * height (contents undefined; earlier slots are released). */
+vvcg_status vvcg_dpb_reserve(vvcg_ctx* ctx, uint32_t slots, uint32_t width, uint32_t height);
+/* Copies picture `pic` of the last frame-path batch (vvcg_decode_batch or
+ * vvcg_batch_run; same coded size, 8-bit 4:2:0) into a slot, on the device. */
+vvcg_status vvcg_dpb_store(vvcg_ctx* ctx, uint32_t pic, uint32_t slot);
+/* Host or device planes (copy direction inferred) into / out of a slot. */
+vvcg_status vvcg_dpb_upload(vvcg_ctx* ctx, uint32_t slot, const vvcg_plane_in planes[3]);
+vvcg_status vvcg_dpb_download(vvcg_ctx* ctx, uint32_t slot, const vvcg_plane_out planes[3]);
+/* Device pointer and stride (samples) of one plane of a slot. */
+vvcg_status vvcg_dpb_plane(vvcg_ctx* ctx, uint32_t slot, uint32_t comp, void** dev_ptr, uint32_t* stride);
+
+/* One P picture of the multi-tool stream for vvcg_decode_p_batch: 8-bit
+ * 4:2:0, CTU 32 (one coding unit per CTU). */
+typedef struct vvcg_p_pic {
+  uint32_t width, height; /* the picture buffer's size */
+  uint8_t qp;             /* SliceQpY */
+  uint8_t options;        /* VVCG_SLICE_DEP_QUANT, VVCG_SLICE_DEBLOCK */
+  uint8_t num_refs;       /* L0 entries, 1..4 */
+  uint8_t sparse;         /* levels in the VVCG_TOOL_SPARSE_LEVELS form */
+  int32_t ref_slot[4];    /* picture-buffer slot of L0 reference index i */
+  int32_t out_slot;       /* slot of the reconstruction; not one of its references */
+  uint32_t cu_offset;     /* first of its (width / 32) * (height / 32) records */
+} vvcg_p_pic; /* 36 bytes */
+
+/* Decodes P pictures in the given order into their picture-buffer slots:
+ * per coding unit the luma 8-tap and chroma 4-tap motion compensation from
+ * the reference slot (8-bit uni-prediction, clamped reference reads), the
+ * dequantised and inverse DCT-2 (or transform-skip) residual, add and clip,
+ * then with VVCG_SLICE_DEBLOCK the CTU-boundary deblocking. Pictures whose
+ * slots do not depend on each other run in the same launches. Records and
+ * levels are host memory. Replaces: decode_inter_picture's reconstruction
+ * (slice.rs:3677-3834) over predict_inter_pu (inter.rs:1734),
+ * reconstruct_component_full (slice.rs:1920) and apply_inter_loop_filters
+ * (slice.rs:2291). Synchronous; VVCG_INVALID_INPUT for bad records. */
+vvcg_status vvcg_decode_p_batch(vvcg_ctx* ctx, const vvcg_p_pic* pics, uint32_t num_pics, const vvcg_inter_cu* cus,
+                                uint32_t num_cus, const int16_t* levels, uint64_t num_levels);
+
 /* ---- inter-prediction tools (BDOF, DMVR, affine / PROF, CIIP, GPM) -------- */
 
 /* A block of the batched inter tools: w x h samples at `off` of the tool's

@@ -120,6 +120,16 @@ def _declare(L):
     L.orc_strict_decode.argtypes = [vp, vp, C.c_uint64, i, i, i, i, vp, vp, vp]
     L.orc_strict_write.argtypes = [vp, vp, C.c_uint64, i, i, i, vp, C.c_uint64, vp]
     L.orc_block_write.argtypes = [vp, i, i, i, i, i, i, i, vp, C.c_uint64, vp]
+    u32 = C.c_uint32
+    L.orc_mt_encode.argtypes = [vp, vp, vp, i, i, i, i, u32, vp, vp, vp, vp, vp, vp]
+    L.orc_mt_decode.argtypes = [vp, vp, C.c_uint64, i, i, i, i, u32, vp, vp, vp]
+    L.orc_inter_encode.argtypes = [vp, vp, vp, i, i, i, i, u32, vp, i, vp, vp, vp, vp, vp, vp]
+    L.orc_inter_resolve_motion.argtypes = [vp, i, i, i]
+    L.orc_inter_decode.argtypes = [vp, vp, C.c_uint64, i, i, i, i, u32, vp, i, vp, vp, vp]
+    L.orc_derive_intra_mpms.argtypes = [i, i, vp]
+    L.orc_derive_intra_mpms.restype = None
+    L.orc_mt_write.argtypes = [vp, vp, C.c_uint64, i, i, i, u32, vp, C.c_uint64, vp]
+    L.orc_p_write.argtypes = [vp, vp, C.c_uint64, i, i, i, u32, vp, C.c_uint64, vp]
     L.orc_bdof.argtypes = [vp, vp, i, i, vp]
     L.orc_bdof.restype = None
     L.orc_dmvr.argtypes = [vp, vp, i, i, i, i, i, i, i, vp]
@@ -967,3 +977,143 @@ def general_picture(pic, tbs, group_sizes, levels, slot_count, sao, alf_ctus, al
     if tools & 8:  # ALF
         Y, U, V = alf_general(Y, U, V, vw, vh, bd, ctu, cols, alf_ctus, alf_params)
     return Y[:vh, :vw], U[:cvh, :cvw], V[:cvh, :cvw]
+
+
+# ---- the multi-tool stream (VvcMultiToolEncoder: IDR + P pictures) ----------
+SLICE_DEP_QUANT, SLICE_SIGN_HIDING, SLICE_DEBLOCK, SLICE_FULL_INTRA_MODES = 1, 2, 4, 8
+INTER_CU_MERGE, INTER_CU_SKIP, INTER_CU_ALT_HPEL = 1, 2, 4
+INTER_CU_DTYPE = np.dtype([("mv", "<i4", (2, 2)), ("mvd", "<i4", (2,)), ("ref_idx", "i1", (2,)), ("inter_dir", "u1"),
+                           ("bcw_idx", "u1"), ("flags", "u1"), ("mvp_idx", "u1"), ("cbf", "u1"), ("tu_tools", "u1"),
+                           ("level_off", "<i4", (3,)), ("reserved", "<u4")])
+assert INTER_CU_DTYPE.itemsize == 48
+
+
+def derive_intra_mpms(left=None, above=None):
+    """predict.rs:1455-1506: the 6 MPM candidates from the left / above modes."""
+    out = np.zeros(6, np.uint8)
+    lib().orc_derive_intra_mpms(-1 if left is None else int(left), -1 if above is None else int(above), _p(out))
+    return out
+
+
+def _planes8(y, u, v):
+    return tuple(np.ascontiguousarray(a, dtype=np.uint8) for a in (y, u, v))
+
+
+def _ref_ptrs(refs):
+    refs = [_planes8(*r) for r in refs]
+    arr = (C.c_void_p * (3 * len(refs)))(*[a.ctypes.data for r in refs for a in r])
+    return refs, arr
+
+
+def mt_encode(y, u, v, qp, opts=0, ctu_log2=5):
+    """encode_picture_multitool's decisions and reconstruction (slice.rs:2575-2970)
+    of one 8-bit 4:2:0 IDR picture; returns (cus, levels, (y, u, v))."""
+    y, u, v = _planes8(y, u, v)
+    h, w = y.shape
+    tb = min(1 << ctu_log2, 32)
+    cus = np.zeros((h // tb) * (w // tb), dtype=CU_DTYPE)
+    levels = np.zeros(w * h * 3 // 2 + 64, np.int16)
+    used = C.c_uint64(0)
+    ry, ru, rv = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
+    rc = lib().orc_mt_encode(_p(y), _p(u), _p(v), w, h, qp, ctu_log2, opts, _p(cus), _p(levels), C.byref(used),
+                             _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"mt_encode rejected ({rc})")
+    return cus, levels[:used.value].copy(), (ry, ru, rv)
+
+
+def mt_decode(cus, levels, w, h, qp, opts=0, ctu_log2=5):
+    """decode_picture_multitool's reconstruction (slice.rs:3012-3300)."""
+    cus = np.ascontiguousarray(cus, dtype=CU_DTYPE)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    ry = np.zeros((h, w), np.uint8)
+    ru, rv = np.zeros((h // 2, w // 2), np.uint8), np.zeros((h // 2, w // 2), np.uint8)
+    rc = lib().orc_mt_decode(_p(cus), _p(levels), levels.size, w, h, qp, ctu_log2, opts, _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"mt_decode rejected ({rc})")
+    return ry, ru, rv
+
+
+def _write(fn, cus, dtype, levels, w, h, qp, opts):
+    cus = np.ascontiguousarray(cus, dtype=dtype)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    cap = 64 + 4 * levels.size + 32 * len(cus)
+    out = np.zeros(cap, np.uint8)
+    n = C.c_uint64(0)
+    rc = fn(_p(cus), _p(levels), levels.size, w, h, qp, opts, _p(out), cap, C.byref(n))
+    if rc:
+        raise ValueError(f"the writer rejected the records ({rc})")
+    return out[:n.value].tobytes()
+
+
+def mt_write(cus, levels, w, h, qp, opts=0):
+    """The slice data encode_picture_multitool writes (slice.rs:2867-2960); bytes."""
+    return _write(lib().orc_mt_write, cus, CU_DTYPE, levels, w, h, qp, opts)
+
+
+def p_write(cus, levels, w, h, qp, opts=0):
+    """The slice data encode_inter_picture writes (slice.rs:3451-3536); bytes."""
+    return _write(lib().orc_p_write, cus, INTER_CU_DTYPE, levels, w, h, qp, opts)
+
+
+def inter_encode(y, u, v, qp, refs, opts=0):
+    """encode_inter_picture (slice.rs:3307-3549) of one P picture against the
+    L0 reference pictures `refs` ((y, u, v) each); returns (cus, levels, (y, u, v))."""
+    y, u, v = _planes8(y, u, v)
+    h, w = y.shape
+    keep, arr = _ref_ptrs(refs)
+    cus = np.zeros((h // 32) * (w // 32), dtype=INTER_CU_DTYPE)
+    levels = np.zeros(w * h * 3 // 2 + 64, np.int16)
+    used = C.c_uint64(0)
+    ry, ru, rv = np.zeros_like(y), np.zeros_like(u), np.zeros_like(v)
+    rc = lib().orc_inter_encode(_p(y), _p(u), _p(v), w, h, qp, 5, opts, arr, len(keep), _p(cus), _p(levels),
+                                C.byref(used), _p(ry), _p(ru), _p(rv))
+    if rc:
+        raise ValueError(f"inter_encode rejected ({rc})")
+    return cus, levels[:used.value].copy(), (ry, ru, rv)
+
+
+def inter_resolve_motion(cus, w, h):
+    """decode_inter_picture's motion derivation (slice.rs:3617-3677): fills
+    the motion of merge / skip records (candidate 0) and AMVP records
+    (predictor mvp_idx + mvd) in place order; returns a new array."""
+    cus = np.array(cus, dtype=INTER_CU_DTYPE, copy=True)
+    rc = lib().orc_inter_resolve_motion(_p(cus), w, h, 5)
+    if rc:
+        raise ValueError(f"inter_resolve_motion rejected ({rc})")
+    return cus
+
+
+def inter_decode(cus, levels, w, h, qp, refs, opts=0):
+    """decode_inter_picture's reconstruction (slice.rs:3677-3834) from records with motion."""
+    cus = np.ascontiguousarray(cus, dtype=INTER_CU_DTYPE)
+    levels = np.ascontiguousarray(levels, dtype=np.int16)
+    keep, arr = _ref_ptrs(refs)
+    ry = np.zeros((h, w), np.uint8)
+    ru, rv = np.zeros((h // 2, w // 2), np.uint8), np.zeros((h // 2, w // 2), np.uint8)
+    rc = lib().orc_inter_decode(_p(cus), _p(levels), levels.size, w, h, qp, 5, opts, arr, len(keep), _p(ry), _p(ru),
+                                _p(rv))
+    if rc:
+        raise ValueError(f"inter_decode rejected ({rc})")
+    return ry, ru, rv
+
+
+def multitool_stream(frames, qp, keyint=3, opts=0):
+    """VvcMultiToolEncoder::encode_i420 (mod.rs:1512-1720) over 8-bit 4:2:0
+    frames of coded size: an IDR picture whenever poc = index % keyint is 0,
+    else a P picture predicting from the most recent picture (the DPB's
+    build_ref_lists, inter.rs:481). Returns one dict per picture: kind ("I" /
+    "P"), data (slice data), cus, levels, recon (y, u, v)."""
+    out, last = [], None
+    for i, (y, u, v) in enumerate(frames):
+        h, w = np.asarray(y).shape
+        if i % max(keyint, 1) == 0 or last is None:
+            cus, levels, rec = mt_encode(y, u, v, qp, opts)
+            data = mt_write(cus, levels, w, h, qp, opts)
+            out.append(dict(kind="I", data=data, cus=cus, levels=levels, recon=rec))
+        else:
+            cus, levels, rec = inter_encode(y, u, v, qp, [last], opts)
+            data = p_write(cus, levels, w, h, qp, opts)
+            out.append(dict(kind="P", data=data, cus=cus, levels=levels, recon=rec))
+        last = rec
+    return out

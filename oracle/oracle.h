@@ -157,6 +157,31 @@ int strict_write(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_lev
                  std::vector<uint8_t>* out);
 int block_write(const int32_t* c, int w, int h, bool luma, bool dq, bool sdh, bool ts, int qp,
                 std::vector<uint8_t>* out);
+// orc_multitool.cpp: the multi-tool stream (VvcMultiToolEncoder): IDR
+// pictures (encode_picture_multitool slice.rs:2575 / decode_picture_multitool
+// :3012) as vvcg_cu_rec records, P pictures (encode_inter_picture :3307 /
+// decode_inter_picture :3552) as vvcg_inter_cu records; opts VVCG_SLICE_*;
+// refs: num_refs L0 pictures of three 8-bit planes each.
+void derive_intra_mpms(int left_dir, int above_dir, uint8_t mpm[6]);
+int mt_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp, int ctu_log2,
+              uint32_t opts, vvcg_cu_rec* cus, int16_t* levels, uint64_t* num_levels, uint8_t* ry, uint8_t* ru,
+              uint8_t* rv);
+int mt_decode(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp, int ctu_log2,
+              uint32_t opts, uint8_t* ry, uint8_t* ru, uint8_t* rv);
+int inter_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp, int ctu_log2,
+                 uint32_t opts, const uint8_t* const* refs, int num_refs, vvcg_inter_cu* cus, int16_t* levels,
+                 uint64_t* num_levels, uint8_t* ry, uint8_t* ru, uint8_t* rv);
+int inter_resolve_motion(vvcg_inter_cu* cus, int w, int h, int ctu_log2);
+int inter_decode(const vvcg_inter_cu* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                 int ctu_log2, uint32_t opts, const uint8_t* const* refs, int num_refs, uint8_t* ry, uint8_t* ru,
+                 uint8_t* rv);
+void inter_ctu_cells(const vvcg_inter_cu* cus, int w, int h, int ctu, vvcg_ctu_motion* cells);
+// orc_cabac.cpp: the slice data encode_picture_multitool and
+// encode_inter_picture write for such records.
+int mt_write(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+             uint32_t opts, std::vector<uint8_t>* out);
+int p_write(const vvcg_inter_cu* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+            uint32_t opts, std::vector<uint8_t>* out);
 // The GPU encoder's CTU full search (orc_search.cpp; no reference counterpart).
 void ctu_search(const Plane16& src, int cx, int cy, int split_mask, int n_cand, const uint8_t* cand,
                 uint32_t lambda_q8, uint32_t* cost, uint32_t split_cost[6], int* split, int* cu_mode, int modes[4]);

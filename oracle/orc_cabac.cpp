@@ -13,6 +13,10 @@
 //                                      :1106-1115 / encode_full_luma_intra_mode
 //                                      :1658-1689, lfnst / mts idx :994-1029,
 //                                      classify_luma_mode_mpm predict.rs:1527
+//   encode_picture_multitool's writes  slice.rs:2867-2960 with
+//                                      encode_chroma_intra_mode :1718-1754
+//   encode_inter_picture's writes      slice.rs:3451-3536 with encode_mvd
+//                                      :1782-1806, CtxStore::new_p_slice
 // The context tables come from rustmpeg-next_b200/csrc/vvc_cabac.h, which a
 // CPU test checks against the reference's literals.
 #include <stdlib.h>
@@ -63,11 +67,12 @@ struct Ctx {
   }
 };
 
+// cabac.rs:267-308 CtxStore::from_table (I, P or B initialisation)
 struct CtxStore {
   Ctx models[kNumContexts];
-  explicit CtxStore(int qp) {
+  explicit CtxStore(int qp, const uint8_t (*table)[2] = kCtxInitI) {
     qp = std::min(63, std::max(0, qp));
-    for (int i = 0; i < kNumContexts; i++) models[i].init(qp, kCtxInitI[i][0], kCtxInitI[i][1]);
+    for (int i = 0; i < kNumContexts; i++) models[i].init(qp, table[i][0], table[i][1]);
   }
 };
 
@@ -620,7 +625,177 @@ void write_luma_mode(Encoder& e, CtxStore& m, int mode) {
   e.trunc_bin((uint32_t)rem, 61);
 }
 
+// slice.rs:1658-1689 encode_full_luma_intra_mode (intra_luma_ref_idx 0, no
+// ISP) against an MPM list
+void write_full_luma_mode(Encoder& e, CtxStore& m, int mode, const uint8_t mpm[6]) {
+  for (int i = 0; i < 6; i++)
+    if (mpm[i] == mode) {
+      e.bin(true, m.models[kCtxIntraLumaMpmFlag]);
+      e.bin(i != 0, m.models[kCtxIntraLumaPlanarFlag + 1]);
+      if (i) e.unary_max((uint32_t)(i - 1), 4);
+      return;
+    }
+  uint8_t sorted[6];
+  memcpy(sorted, mpm, 6);
+  std::sort(sorted, sorted + 6);
+  int rem = mode;
+  for (int i = 5; i >= 0; i--)
+    if (rem > sorted[i]) rem--;
+  e.bin(false, m.models[kCtxIntraLumaMpmFlag]);
+  e.trunc_bin((uint32_t)rem, 61);
+}
+
+// slice.rs:1718-1754 encode_chroma_intra_mode without CCLM; false when the
+// mode is neither DM nor a Table 24 candidate.
+bool write_chroma_mode(Encoder& e, CtxStore& m, int chroma, int luma) {
+  if (chroma == luma) {
+    e.bin(false, m.models[kCtxIntraChromaPredMode]);
+    return true;
+  }
+  static const int cand[4] = {0, 50, 18, 1};
+  for (int i = 0; i < 4; i++)
+    if ((cand[i] == luma ? 66 : cand[i]) == chroma) {
+      e.bin(true, m.models[kCtxIntraChromaPredMode]);
+      e.bypass_bins((uint32_t)i, 2);
+      return true;
+    }
+  return false;
+}
+
+// slice.rs:1782-1806 encode_mvd
+void write_mvd(Encoder& e, CtxStore& m, const int32_t mvd[2]) {
+  for (int i = 0; i < 2; i++) e.bin(mvd[i] != 0, m.models[kCtxMvd]);
+  for (int i = 0; i < 2; i++)
+    if (mvd[i] != 0) e.bin(std::abs(mvd[i]) > 1, m.models[kCtxMvd + 1]);
+  for (int i = 0; i < 2; i++)
+    if (mvd[i] != 0) {
+      if (std::abs(mvd[i]) > 1) e.rem_abs((uint32_t)std::abs(mvd[i]) - 2, 1, 0, 17);
+      e.bypass(mvd[i] < 0);
+    }
+}
+
+// A coded TB's levels (n of them, at least one nonzero) and its
+// transform_skip_flag and residual syntax.
+int write_tb(Encoder& e, CtxStore& m, const CScan& s, const int16_t* levels, uint64_t num_levels, int32_t off, int n,
+             bool luma, bool ts, bool dq, bool sdh, std::vector<int32_t>& c) {
+  if (off < 0 || (uint64_t)off + n > num_levels) return -4;
+  c.assign(n, 0);
+  bool any = false;
+  for (int i = 0; i < n; i++) {
+    c[i] = levels[off + i];
+    any |= c[i] != 0;
+  }
+  if (!any) return -5;
+  e.bin(ts, m.models[kCtxTransformSkipFlag + (luma ? 0 : 1)]);
+  if (ts)
+    write_ts(e, m, s, c.data());
+  else
+    write_residual(e, m, s, c.data(), luma, dq, sdh);
+  return 0;
+}
+
 }  // namespace
+
+// The slice data encode_picture_multitool writes (slice.rs:2867-2960 with
+// every optional tool but dep_quant / sign_data_hiding off) for 32 x 32
+// coding units in raster order: luma mode against the MPM list of the left
+// neighbour's mode, chroma mode, cbfs (Cb, Cr, Y), then per coded TB its
+// transform_skip_flag and residual. Returns 0, or a negative code for
+// records the syntax cannot carry.
+int mt_write(const vvcg_cu_rec* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+             uint32_t opts, std::vector<uint8_t>* out) {
+  if (w % 32 || h % 32 || w <= 0 || h <= 0) return -1;
+  const bool dq = opts & VVCG_SLICE_DEP_QUANT, sdh = opts & VVCG_SLICE_SIGN_HIDING;
+  const CScan ls = coeff_scan(32, 32), cs = coeff_scan(16, 16);
+  Encoder e;
+  CtxStore m(qp);
+  std::vector<int32_t> c;
+  const int gw = w / 32, gh = h / 32;
+  for (int k = 0; k < gw * gh; k++) {
+    const vvcg_cu_rec& r = cus[k];
+    if (r.luma_mode > 66 || (r.tu_tools >> 3)) return -2;
+    uint8_t mpm[6];
+    derive_intra_mpms(k % gw ? cus[k - 1].luma_mode : -1, -1, mpm);
+    write_full_luma_mode(e, m, r.luma_mode, mpm);
+    if (!write_chroma_mode(e, m, r.chroma_mode, r.luma_mode)) return -3;
+    const bool cbf[3] = {(r.cbf & 1) != 0, (r.cbf & 2) != 0, (r.cbf & 4) != 0};
+    e.bin(cbf[1], m.models[kCtxQtCbfCb]);
+    e.bin(cbf[2], m.models[kCtxQtCbfCr + (cbf[1] ? 1 : 0)]);
+    e.bin(cbf[0], m.models[kCtxQtCbfY]);
+    for (int q = 0; q < 3; q++) {
+      if (!cbf[q]) continue;
+      const int rc = write_tb(e, m, q ? cs : ls, levels, num_levels, r.level_off[q], q ? 256 : 1024, q == 0,
+                              (r.tu_tools >> q) & 1, dq, sdh, c);
+      if (rc) return rc;
+    }
+  }
+  e.terminate(true);
+  *out = e.finish_and_align();
+  return 0;
+}
+
+// The slice data encode_inter_picture writes (slice.rs:3451-3536, P slice,
+// SAO / ALF / joint Cb-Cr off) for one coding unit per 32 x 32 CTU: the skip
+// flag (context from the left and above CTUs' skip flags), and unless
+// skipped pred_mode_flag (inter), general_merge_flag, for AMVP coding units
+// the mvd, mvp_l0_flag and rqt_root_cbf, then the cbfs (tu_y_coded_flag only
+// when a chroma cbf is set, else inferred 1) and each coded TB's
+// transform_skip_flag and residual. A record is a skip coding unit when it
+// is merge with no cbf. A record with flags bit 0x80 (not a vvcg_inter_cu
+// flag) writes pred_mode_flag 1 instead, an intra coding unit, and ends the
+// slice data there: the input of the parser's rejection test. Returns 0, or
+// a negative code for records the syntax cannot carry.
+int p_write(const vvcg_inter_cu* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+            uint32_t opts, std::vector<uint8_t>* out) {
+  if (w % 32 || h % 32 || w <= 0 || h <= 0) return -1;
+  const bool dq = opts & VVCG_SLICE_DEP_QUANT, sdh = opts & VVCG_SLICE_SIGN_HIDING;
+  const CScan ls = coeff_scan(32, 32), cs = coeff_scan(16, 16);
+  Encoder e;
+  CtxStore m(qp, kCtxInitP);
+  std::vector<int32_t> c;
+  const int gw = w / 32, gh = h / 32;
+  std::vector<char> skip(gw * gh, 0);
+  for (int k = 0; k < gw * gh; k++) {
+    const vvcg_inter_cu& r = cus[k];
+    const int gx = k % gw, gy = k / gw;
+    const bool merge = (r.flags & VVCG_INTER_CU_MERGE) != 0, any_cbf = (r.cbf & 7) != 0;
+    const bool cu_skip = merge && !any_cbf;
+    if (((r.flags & VVCG_INTER_CU_SKIP) != 0) != cu_skip || (r.tu_tools >> 3) || r.mvp_idx > 1) return -2;
+    const int sctx = kCtxSkipFlag + (gx > 0 && skip[k - 1]) + (gy > 0 && skip[k - gw]);
+    if (r.flags & 0x80) {  // test hook: an intra coding unit (pred_mode_flag 1), where the syntax ends
+      e.bin(false, m.models[sctx]);
+      e.bin(true, m.models[kCtxPredMode]);
+      break;
+    }
+    e.bin(cu_skip, m.models[sctx]);
+    skip[k] = cu_skip;
+    if (cu_skip) continue;
+    e.bin(false, m.models[kCtxPredMode]);
+    e.bin(merge, m.models[kCtxMergeFlag]);
+    if (!merge) {
+      write_mvd(e, m, r.mvd);
+      e.bin(r.mvp_idx != 0, m.models[kCtxMvpIdx]);
+      e.bin(any_cbf, m.models[kCtxQtRootCbf]);
+    }
+    if (!any_cbf) continue;
+    const bool cbf[3] = {(r.cbf & 1) != 0, (r.cbf & 2) != 0, (r.cbf & 4) != 0};
+    e.bin(cbf[1], m.models[kCtxQtCbfCb]);
+    e.bin(cbf[2], m.models[kCtxQtCbfCr + (cbf[1] ? 1 : 0)]);
+    if (cbf[1] || cbf[2])
+      e.bin(cbf[0], m.models[kCtxQtCbfY]);
+    else if (!cbf[0])
+      return -3;  // cannot happen: any_cbf
+    for (int q = 0; q < 3; q++) {
+      if (!cbf[q]) continue;
+      const int rc = write_tb(e, m, q ? cs : ls, levels, num_levels, r.level_off[q], q ? 256 : 1024, q == 0,
+                              (r.tu_tools >> q) & 1, dq, sdh, c);
+      if (rc) return rc;
+    }
+  }
+  e.terminate(true);
+  *out = e.finish_and_align();
+  return 0;
+}
 
 // The slice data encode_picture writes (slice.rs:407-455) for records in the
 // frame path's strict layout. Returns 0, or a negative code for records the

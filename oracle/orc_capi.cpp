@@ -329,3 +329,51 @@ extern "C" int orc_block_write(const int32_t* c, int w, int h, int luma, int dq,
   return 0;
 }
 
+
+// The multi-tool stream (orc_multitool.cpp, orc_cabac.cpp). refs: 3 * num_refs
+// plane pointers (Y, Cb, Cr of each L0 picture).
+extern "C" int orc_mt_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp, int ctu_log2,
+                             uint32_t opts, void* cus, int16_t* levels, uint64_t* num_levels, uint8_t* ry,
+                             uint8_t* ru, uint8_t* rv) {
+  return orc::mt_encode(y, u, v, w, h, qp, ctu_log2, opts, (vvcg_cu_rec*)cus, levels, num_levels, ry, ru, rv);
+}
+extern "C" int orc_mt_decode(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                             int ctu_log2, uint32_t opts, uint8_t* ry, uint8_t* ru, uint8_t* rv) {
+  return orc::mt_decode((const vvcg_cu_rec*)cus, levels, num_levels, w, h, qp, ctu_log2, opts, ry, ru, rv);
+}
+extern "C" int orc_inter_encode(const uint8_t* y, const uint8_t* u, const uint8_t* v, int w, int h, int qp,
+                                int ctu_log2, uint32_t opts, const uint8_t* const* refs, int num_refs, void* cus,
+                                int16_t* levels, uint64_t* num_levels, uint8_t* ry, uint8_t* ru, uint8_t* rv) {
+  return orc::inter_encode(y, u, v, w, h, qp, ctu_log2, opts, refs, num_refs, (vvcg_inter_cu*)cus, levels, num_levels,
+                           ry, ru, rv);
+}
+extern "C" int orc_inter_resolve_motion(void* cus, int w, int h, int ctu_log2) {
+  return orc::inter_resolve_motion((vvcg_inter_cu*)cus, w, h, ctu_log2);
+}
+extern "C" int orc_inter_decode(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                                int ctu_log2, uint32_t opts, const uint8_t* const* refs, int num_refs, uint8_t* ry,
+                                uint8_t* ru, uint8_t* rv) {
+  return orc::inter_decode((const vvcg_inter_cu*)cus, levels, num_levels, w, h, qp, ctu_log2, opts, refs, num_refs,
+                           ry, ru, rv);
+}
+extern "C" void orc_derive_intra_mpms(int left, int above, uint8_t* mpm) { orc::derive_intra_mpms(left, above, mpm); }
+extern "C" int orc_mt_write(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                            uint32_t opts, uint8_t* out, uint64_t cap, uint64_t* size) {
+  std::vector<uint8_t> b;
+  const int rc = orc::mt_write((const vvcg_cu_rec*)cus, levels, num_levels, w, h, qp, opts, &b);
+  if (rc) return rc;
+  if (b.size() > cap) return -1000;
+  memcpy(out, b.data(), b.size());
+  *size = b.size();
+  return 0;
+}
+extern "C" int orc_p_write(const void* cus, const int16_t* levels, uint64_t num_levels, int w, int h, int qp,
+                           uint32_t opts, uint8_t* out, uint64_t cap, uint64_t* size) {
+  std::vector<uint8_t> b;
+  const int rc = orc::p_write((const vvcg_inter_cu*)cus, levels, num_levels, w, h, qp, opts, &b);
+  if (rc) return rc;
+  if (b.size() > cap) return -1000;
+  memcpy(out, b.data(), b.size());
+  *size = b.size();
+  return 0;
+}

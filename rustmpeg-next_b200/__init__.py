@@ -129,6 +129,15 @@ GEN_PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("vis_width", "<u
 TOOL_DEP_QUANT, TOOL_DEBLOCK, TOOL_SAO, TOOL_ALF = 1, 2, 4, 8
 TOOL_ENC_FULL_INTRA, TOOL_ENC_CCLM, TOOL_SPARSE_LEVELS, TOOL_TU_TOOLS = 16, 32, 64, 128
 CU_TS_Y, CU_TS_CB, CU_TS_CR, CU_MTS_SHIFT, CU_LFNST_SHIFT = 1, 2, 4, 3, 6
+# the multi-tool stream (vvcg.h VVCG_SLICE_*, VVCG_INTER_CU_*, vvcg_inter_cu, vvcg_p_pic)
+SLICE_DEP_QUANT, SLICE_SIGN_HIDING, SLICE_DEBLOCK, SLICE_FULL_INTRA_MODES = 1, 2, 4, 8
+INTER_CU_MERGE, INTER_CU_SKIP, INTER_CU_ALT_HPEL = 1, 2, 4
+INTER_CU_DTYPE = np.dtype([("mv", "<i4", (2, 2)), ("mvd", "<i4", (2,)), ("ref_idx", "i1", (2,)), ("inter_dir", "u1"),
+                           ("bcw_idx", "u1"), ("flags", "u1"), ("mvp_idx", "u1"), ("cbf", "u1"), ("tu_tools", "u1"),
+                           ("level_off", "<i4", (3,)), ("reserved", "<u4")])
+P_PIC_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("qp", "u1"), ("options", "u1"), ("num_refs", "u1"),
+                        ("sparse", "u1"), ("ref_slot", "<i4", (4,)), ("out_slot", "<i4"), ("cu_offset", "<u4")])
+assert INTER_CU_DTYPE.itemsize == 48 and P_PIC_DTYPE.itemsize == 36
 TU_DEP_QUANT, TU_TRANSFORM_SKIP, TU_BDPCM_HOR, TU_BDPCM_VER, TU_IMPLICIT_MTS, TU_INTER = 1, 2, 4, 8, 16, 32
 STAGE_RECON, STAGE_DEBLOCK, STAGE_SAO, STAGE_ALF, STAGE_ALL = 1, 2, 4, 8, 15
 MC_BI, MC_AFFINE, MC_ALT_HPEL = 1, 2, 4
@@ -191,6 +200,12 @@ class _StrictSubstream(C.Structure):
     _fields_ = [("data", C.c_void_p), ("size", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32),
                 ("qp", C.c_uint8), ("reserved", C.c_uint8 * 3), ("cu_offset", C.c_uint32),
                 ("level_offset", C.c_uint64), ("level_cap", C.c_uint64)]
+
+
+class _SliceSubstream(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("qp", C.c_uint8), ("ctu_log2", C.c_uint8), ("options", C.c_uint8), ("reserved", C.c_uint8),
+                ("cu_offset", C.c_uint32), ("level_offset", C.c_uint64), ("level_cap", C.c_uint64)]
 
 
 class _PlaneOut(C.Structure):
@@ -311,6 +326,14 @@ def lib():
         L.vvcg_gen_levels.restype = u32
         L.vvcg_parse_strict.argtypes = [vp, u32, u32, u32, vp, u64, vp, u64, vp, C.c_char_p, C.c_size_t]
         L.vvcg_parse_residual_block.argtypes = [vp, u64, u32, u32, u32, u32, vp]
+        L.vvcg_parse_multitool_idr.argtypes = [vp, u32, u32, u32, vp, u64, vp, u64, vp, C.c_char_p, C.c_size_t]
+        L.vvcg_parse_multitool_p.argtypes = [vp, u32, u32, u32, vp, u64, vp, u64, vp, C.c_char_p, C.c_size_t]
+        L.vvcg_dpb_reserve.argtypes = [vp, u32, u32, u32]
+        L.vvcg_dpb_store.argtypes = [vp, u32, u32]
+        L.vvcg_dpb_upload.argtypes = [vp, u32, vp]
+        L.vvcg_dpb_download.argtypes = [vp, u32, vp]
+        L.vvcg_dpb_plane.argtypes = [vp, u32, u32, vp, vp]
+        L.vvcg_decode_p_batch.argtypes = [vp, vp, u32, vp, u32, vp, u64]
         _lib = L
     return _lib
 
@@ -485,6 +508,77 @@ class Context:
         self._keep = (batch, outs, po, st)
         self._check(self._L.vvcg_decode_general_batch(self._h, C.byref(st), po))
         return outs
+
+    # -- the multi-tool stream: picture buffer and P pictures --
+    def dpb_reserve(self, slots, width, height):
+        """Device picture buffer of `slots` 8-bit 4:2:0 pictures (vvcg_dpb_reserve)."""
+        self._check(self._L.vvcg_dpb_reserve(self._h, slots, width, height))
+        self._dpb_size = (width, height)
+
+    def dpb_store(self, pic, slot):
+        """Picture `pic` of the last frame-path batch into a slot (on the device)."""
+        self._check(self._L.vvcg_dpb_store(self._h, pic, slot))
+
+    def dpb_upload(self, slot, planes):
+        """(y, u, v) host planes (uint8 or uint16 samples) into a slot."""
+        arrs = [np.ascontiguousarray(a, dtype=np.uint16) for a in planes]
+        pin = (_PlaneIn * 3)(*[_PlaneIn(_ptr(a), a.shape[1], 0) for a in arrs])
+        self._check(self._L.vvcg_dpb_upload(self._h, slot, pin))
+
+    def dpb_download(self, slot, outs=None):
+        """A slot's (y, u, v) planes as host uint16 arrays."""
+        w, h = self._dpb_size
+        if outs is None:
+            outs = (np.zeros((h, w), np.uint16), np.zeros((h // 2, w // 2), np.uint16),
+                    np.zeros((h // 2, w // 2), np.uint16))
+        self._check(self._L.vvcg_dpb_download(self._h, slot, self._plane_outs([outs])))
+        return outs
+
+    def decode_p_batch(self, pics, cus, levels):
+        """P pictures (P_PIC_DTYPE) with their INTER_CU_DTYPE records and levels
+        into their picture-buffer slots, in order (vvcg_decode_p_batch)."""
+        pics = np.ascontiguousarray(pics, dtype=P_PIC_DTYPE)
+        cus = np.ascontiguousarray(cus, dtype=INTER_CU_DTYPE)
+        levels = np.ascontiguousarray(levels, dtype=np.int16)
+        self._check(self._L.vvcg_decode_p_batch(self._h, _ptr(pics), len(pics), _ptr(cus), len(cus), _ptr(levels),
+                                                levels.size))
+
+    def decode_multitool_stream(self, streams, sparse=False, threads=0):
+        """Decode the multi-tool stream's pictures (VvcMultiToolEncoder: IDR
+        and P pictures, each P picture predicting from the picture before it,
+        the DPB's build_ref_lists, inter.rs:481) from their slice data.
+
+        streams: [(kind "I" / "P", bytes, width, height, qp, options)] in
+        decoding order, one size. The IDR pictures are parsed and decoded on
+        the frame path in one batch, the P pictures parsed in parallel and
+        decoded in order from the picture buffer. Returns [(y, u, v)] uint16
+        planes."""
+        if not streams:
+            return []
+        w, h = streams[0][2], streams[0][3]
+        if any((s[2], s[3]) != (w, h) for s in streams):
+            raise InvalidInput("the pictures of a stream share one size")
+        idx_i = [k for k, s in enumerate(streams) if s[0] == "I"]
+        idx_p = [k for k, s in enumerate(streams) if s[0] != "I"]
+        if idx_p and idx_p[0] < (idx_i[0] if idx_i else len(streams)):
+            raise InvalidInput("a P picture needs a picture before it")
+        self.dpb_reserve(len(streams), w, h)
+        if idx_i:
+            pics, cus, levels, _ = parse_multitool([streams[k] for k in idx_i], "I", sparse, threads)
+            ctus = np.zeros(len(idx_i) * (w // 32) * (h // 32), CTU_DTYPE)
+            pics["ctu_offset"] = np.arange(len(idx_i)) * (w // 32) * (h // 32)
+            batch = Batch(pics, cus, levels, ctus)
+            self.decode_batch(batch)
+            for j, k in enumerate(idx_i):
+                self.dpb_store(j, k)
+        if idx_p:
+            pp, pcus, plevels, _ = parse_multitool([streams[k] for k in idx_p], "P", sparse, threads)
+            for j, k in enumerate(idx_p):
+                pp[j]["ref_slot"][:] = k - 1
+                pp[j]["num_refs"] = 1
+                pp[j]["out_slot"] = k
+            self.decode_p_batch(pp, pcus, plevels)
+        return [self.dpb_download(k) for k in range(len(streams))]
 
     def decode_batch_async(self, batch: Batch, outs):
         """decode_batch without the wait: sync() waits and reports the status.
@@ -1150,6 +1244,74 @@ def parse_strict(streams, sparse=False, threads=0):
         p["alf_aps"] = -1
         p["cu_offset"] = subs[i].cu_offset
     return pics, cus, levels, used[:n].copy()
+
+
+def parse_multitool(streams, kind, sparse=False, threads=0):
+    """Parse the multi-tool stream's slice data on the host.
+
+    streams: [(kind, bytes, width, height, qp, options)] (kind is ignored;
+    every entry is parsed as `kind`: "I" with vvcg_parse_multitool_idr, "P"
+    with vvcg_parse_multitool_p). Returns (pics, cus, levels, used): for "I"
+    a PIC_DTYPE batch for the frame path (8-bit 4:2:0, CTU 32, TU_TOOLS, plus
+    DEP_QUANT / SPARSE_LEVELS as the options ask) with CU_DTYPE records; for
+    "P" P_PIC_DTYPE pictures (slots to fill in) with INTER_CU_DTYPE records.
+    Each picture's levels are compacted into one pool."""
+    L = lib()
+    is_p = kind != "I"
+    n = len(streams)
+    subs = (_SliceSubstream * max(1, n))()
+    bufs, cu_at, lv_at = [], 0, 0
+    for i, (_, data, w, h, qp, opts) in enumerate(streams):
+        buf = np.frombuffer(bytes(data), np.uint8)
+        bufs.append(buf)
+        ncu = (w // 32) * (h // 32)
+        cap = (w * h * 3) // 2 * (2 if sparse else 1) + 8 * ncu
+        subs[i] = _SliceSubstream(_ptr(buf) if buf.size else None, buf.size, w, h, qp, 5, opts, 0, cu_at, lv_at, cap)
+        cu_at += ncu
+        lv_at += cap + (cap & 1)
+    cus = np.zeros(cu_at, INTER_CU_DTYPE if is_p else CU_DTYPE)
+    levels = np.zeros(max(1, lv_at), np.int16)
+    used = np.zeros(max(1, n), np.uint64)
+    err = C.create_string_buffer(256)
+    fn = L.vvcg_parse_multitool_p if is_p else L.vvcg_parse_multitool_idr
+    st = fn(subs, n, int(sparse), threads, _ptr(cus), len(cus), _ptr(levels), levels.size, _ptr(used), err, 256)
+    if st != OK:
+        raise _ERRORS.get(st, Execution)(err.value.decode())
+    pool_n, starts = 0, []
+    for i in range(n):
+        pool_n += pool_n & 1
+        starts.append(pool_n)
+        pool_n += int(used[i])
+    pool = np.zeros(max(1, pool_n), np.int16)
+    for i in range(n):
+        a, m = int(subs[i].level_offset), int(used[i])
+        pool[starts[i]:starts[i] + m] = levels[a:a + m]
+        c0, w, h = int(subs[i].cu_offset), streams[i][2], streams[i][3]
+        rec = cus[c0:c0 + (w // 32) * (h // 32)]
+        lo = rec["level_off"].astype(np.int64)
+        rec["level_off"] = np.where(lo >= 0, lo - a + starts[i], -1).astype(np.int32)
+    if is_p:
+        pics = np.zeros(n, P_PIC_DTYPE)
+        for i, (_, _, w, h, qp, opts) in enumerate(streams):
+            pics[i]["width"], pics[i]["height"], pics[i]["qp"] = w, h, qp
+            pics[i]["options"], pics[i]["sparse"] = opts & (SLICE_DEP_QUANT | SLICE_DEBLOCK), int(sparse)
+            pics[i]["num_refs"], pics[i]["cu_offset"] = 1, subs[i].cu_offset
+    else:
+        pics = np.zeros(n, PIC_DTYPE)
+        for i, (_, _, w, h, qp, opts) in enumerate(streams):
+            p = pics[i:i + 1]
+            p["width"], p["height"], p["visible_width"], p["visible_height"] = w, h, w, h
+            # decode_picture_multitool reconstructs and deblocks at max(QP, 4)
+            # and max(derived_chroma_qp, 4) (slice.rs:3029-3031, :3290-3297)
+            lqp = max(qp, 4)
+            p["bit_depth"], p["chroma_format"], p["ctu_log2"], p["slice_qp"] = 8, CHROMA_420, 5, lqp
+            p["chroma_qp_scaled"] = min(63, lqp if lqp <= 26 else lqp - 1)  # derived_chroma_qp (hls.rs:778)
+            p["tools"] = (TOOL_TU_TOOLS | (TOOL_SPARSE_LEVELS if sparse else 0) |
+                          (TOOL_DEP_QUANT if opts & SLICE_DEP_QUANT else 0) |
+                          (TOOL_DEBLOCK if opts & SLICE_DEBLOCK else 0))
+            p["alf_aps"] = -1
+            p["cu_offset"] = subs[i].cu_offset
+    return pics, cus, pool, used[:n].copy()
 
 
 def parse_residual_block(data, w, h, flags, qp):

@@ -64,10 +64,12 @@ inline Model model_init(int qp, int init_id, int log2_window) {
 
 struct Models {
   Model m[kNumContexts];
-  void init_i_slice(int qp) {
+  // cabac.rs:276-308: one of the I / P / B initialisation tables at qp
+  void init(int qp, const uint8_t (*table)[2]) {
     qp = std::min(63, std::max(0, qp));
-    for (int i = 0; i < kNumContexts; i++) m[i] = model_init(qp, kCtxInitI[i][0], kCtxInitI[i][1]);
+    for (int i = 0; i < kNumContexts; i++) m[i] = model_init(qp, table[i][0], table[i][1]);
   }
+  void init_i_slice(int qp) { init(qp, kCtxInitI); }
   Model& operator[](int i) { return m[i]; }
 };
 
@@ -261,7 +263,7 @@ inline Scan make_scan(int w, int h) {
 }
 
 // ------------------------------------------------------- residual_coding --
-enum ParseError { kOk = 0, kBadLast = 1, kBadRange = 2, kBadSyntax = 3, kTruncated = 4, kBadEnd = 5 };
+enum ParseError { kOk = 0, kBadLast = 1, kBadRange = 2, kBadSyntax = 3, kTruncated = 4, kBadEnd = 5, kIntraInP = 6 };
 
 struct Template {  // the last significance context's neighbourhood
   int diag = -1, sum1 = 0;

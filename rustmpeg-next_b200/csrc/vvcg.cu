@@ -98,6 +98,8 @@ struct PicLayout {
 
 struct GenPass;  // the general decoder's picture pass (gen_picture.cuh)
 void gen_pass_free(GenPass* g);
+struct PState;  // picture buffer and P-picture state (p_picture.cuh)
+void p_state_free(PState* s);
 
 struct vvcg_ctx {
   int device = 0;
@@ -151,6 +153,7 @@ struct vvcg_ctx {
   PinnedBuf stage, stage_cus;
   size_t stage_used = 0;
   GenPass* gen = nullptr;  // state of vvcg_gen_prepare / vvcg_gen_run
+  PState* p = nullptr;     // picture buffer and P-picture state (vvcg_dpb_*, vvcg_decode_p_batch)
 };
 
 namespace {
@@ -471,6 +474,7 @@ void vvcg_ctx_destroy(vvcg_ctx* ctx) {
   if (ctx->graph) cudaGraphDestroy(ctx->graph);
   for (vvcg_ctx* l : ctx->lanes) vvcg_ctx_destroy(l);
   gen_pass_free(ctx->gen);
+  p_state_free(ctx->p);
   ctx->stage.release();
   ctx->stage_cus.release();
   for (DevBuf* b : {&ctx->planes, &ctx->flags, &ctx->d_pics, &ctx->d_items, &ctx->d_dbf[0],
@@ -2807,6 +2811,7 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
 }
 
 #include "gen_picture.cuh"
+#include "p_picture.cuh"
 
 // ---------------------------------------------------------------------------
 // CABAC parse of strict-profile pictures on the host (vvcg_parse_strict).
@@ -2815,6 +2820,41 @@ extern "C" vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const
 #include <thread>
 
 #include "cabac_parse.h"
+#include "mt_parse.h"
+
+namespace {
+
+// Runs parse(i, &levels_used[i]) for every picture on `threads` host
+// threads (pictures taken in turn from a shared counter) and reports the
+// first picture that failed.
+template <class F>
+vvcg_status parse_pictures(uint32_t num_pics, uint32_t threads, uint64_t* levels_used, char* err, size_t err_cap,
+                           F parse) {
+  std::atomic<uint32_t> next{0};
+  std::vector<int> code(num_pics, 0);
+  auto work = [&]() {
+    for (uint32_t i; (i = next.fetch_add(1)) < num_pics;) code[i] = parse(i, &levels_used[i]);
+  };
+  const uint32_t n = std::max<uint32_t>(1, std::min<uint32_t>(threads ? threads : 1, num_pics));
+  std::vector<std::thread> pool;
+  for (uint32_t t = 1; t < n; t++) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  static const char* kWhy[] = {"",
+                               "last position outside the block",
+                               "level outside 16 bits",
+                               "syntax",
+                               "level capacity exceeded",
+                               "no end of slice or alignment",
+                               "intra coding unit inside an inter slice"};
+  for (uint32_t i = 0; i < num_pics; i++)
+    if (code[i])
+      return static_fail(err, err_cap, code[i] == vvcg_parse::kTruncated ? VVCG_LIMIT_EXCEEDED : VVCG_INVALID_INPUT,
+                         "picture %u: %s", i, kWhy[std::min(code[i], 6)]);
+  return VVCG_OK;
+}
+
+}  // namespace
 
 extern "C" vvcg_status vvcg_parse_strict(const vvcg_strict_substream* pics, uint32_t num_pics, uint32_t sparse,
                                          uint32_t threads, vvcg_cu_rec* cus, uint64_t num_cus, int16_t* levels,
@@ -2834,29 +2874,84 @@ extern "C" vvcg_status vvcg_parse_strict(const vvcg_strict_substream* pics, uint
     if (p.level_offset + p.level_cap > num_levels || (sparse && (p.level_offset & 1)))
       return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: level range", i);
   }
-  std::atomic<uint32_t> next{0};
-  std::vector<int> code(num_pics, 0);
-  auto work = [&]() {
-    for (uint32_t i; (i = next.fetch_add(1)) < num_pics;) {
-      const vvcg_strict_substream& p = pics[i];
-      vvcg_parse::LevelSink sink{levels + p.level_offset, p.level_cap, 0, sparse != 0};
-      code[i] = vvcg_parse::parse_strict_picture(p.data, p.size, p.qp, (int)p.width, (int)p.height,
-                                                 cus + p.cu_offset, sink, (int64_t)p.level_offset);
-      levels_used[i] = sink.at;
-    }
-  };
-  const uint32_t n = std::max<uint32_t>(1, std::min<uint32_t>(threads ? threads : 1, num_pics));
-  std::vector<std::thread> pool;
-  for (uint32_t t = 1; t < n; t++) pool.emplace_back(work);
-  work();
-  for (auto& t : pool) t.join();
-  static const char* kWhy[] = {"", "last position outside the block", "level outside 16 bits", "syntax",
-                               "level capacity exceeded", "no end of slice or alignment"};
-  for (uint32_t i = 0; i < num_pics; i++)
-    if (code[i])
-      return static_fail(err, err_cap, code[i] == 4 ? VVCG_LIMIT_EXCEEDED : VVCG_INVALID_INPUT,
-                         "picture %u: %s", i, kWhy[std::min(code[i], 5)]);
+  return parse_pictures(num_pics, threads, levels_used, err, err_cap, [&](uint32_t i, uint64_t* used) {
+    const vvcg_strict_substream& p = pics[i];
+    vvcg_parse::LevelSink sink{levels + p.level_offset, p.level_cap, 0, sparse != 0};
+    const int code = vvcg_parse::parse_strict_picture(p.data, p.size, p.qp, (int)p.width, (int)p.height,
+                                                      cus + p.cu_offset, sink, (int64_t)p.level_offset);
+    *used = sink.at;
+    return code;
+  });
+}
+
+namespace {
+
+// Checks of one multi-tool substream: CTU 32, options, record and level ranges.
+vvcg_status check_slice_substream(const vvcg_slice_substream& p, uint32_t i, uint32_t sparse, uint64_t num_cus,
+                                  uint64_t num_levels, uint32_t allowed, char* err, size_t err_cap) {
+  if (!p.data && p.size) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: missing data", i);
+  if (p.ctu_log2 != 5) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: CTU size must be 32", i);
+  if (!p.width || !p.height || p.width % 32 || p.height % 32 || p.width > 16384 || p.height > 16384)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: coded size not a multiple of 32", i);
+  if (p.qp > 63) return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: slice QP above 63", i);
+  if (p.options & ~allowed)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: unsupported slice options 0x%x", i, p.options);
+  if ((uint64_t)p.cu_offset + (uint64_t)(p.width / 32) * (p.height / 32) > num_cus)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: records past the array", i);
+  if (p.level_offset + p.level_cap > num_levels || (sparse && (p.level_offset & 1)))
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "picture %u: level range", i);
   return VVCG_OK;
+}
+
+}  // namespace
+
+extern "C" vvcg_status vvcg_parse_multitool_idr(const vvcg_slice_substream* pics, uint32_t num_pics, uint32_t sparse,
+                                                uint32_t threads, vvcg_cu_rec* cus, uint64_t num_cus, int16_t* levels,
+                                                uint64_t num_levels, uint64_t* levels_used, char* err,
+                                                size_t err_cap) {
+  if (err && err_cap) err[0] = 0;
+  if (!num_pics) return VVCG_OK;
+  if (!pics || !cus || !levels || !levels_used)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "missing pictures, records, levels or counts");
+  const uint32_t allowed =
+      VVCG_SLICE_DEP_QUANT | VVCG_SLICE_SIGN_HIDING | VVCG_SLICE_FULL_INTRA_MODES | VVCG_SLICE_DEBLOCK;
+  for (uint32_t i = 0; i < num_pics; i++) {
+    vvcg_status st = check_slice_substream(pics[i], i, sparse, num_cus, num_levels, allowed, err, err_cap);
+    if (st != VVCG_OK) return st;
+  }
+  return parse_pictures(num_pics, threads, levels_used, err, err_cap, [&](uint32_t i, uint64_t* used) {
+    const vvcg_slice_substream& p = pics[i];
+    vvcg_parse::LevelSink sink{levels + p.level_offset, p.level_cap, 0, sparse != 0};
+    const int code = vvcg_parse::parse_mt_idr_picture(
+        p.data, p.size, p.qp, (int)p.width, (int)p.height, (p.options & VVCG_SLICE_DEP_QUANT) != 0,
+        (p.options & VVCG_SLICE_SIGN_HIDING) != 0, cus + p.cu_offset, sink, (int64_t)p.level_offset);
+    *used = sink.at;
+    return code;
+  });
+}
+
+extern "C" vvcg_status vvcg_parse_multitool_p(const vvcg_slice_substream* pics, uint32_t num_pics, uint32_t sparse,
+                                              uint32_t threads, vvcg_inter_cu* cus, uint64_t num_cus, int16_t* levels,
+                                              uint64_t num_levels, uint64_t* levels_used, char* err, size_t err_cap) {
+  if (err && err_cap) err[0] = 0;
+  if (!num_pics) return VVCG_OK;
+  if (!pics || !cus || !levels || !levels_used)
+    return static_fail(err, err_cap, VVCG_INVALID_INPUT, "missing pictures, records, levels or counts");
+  const uint32_t allowed =
+      VVCG_SLICE_DEP_QUANT | VVCG_SLICE_SIGN_HIDING | VVCG_SLICE_FULL_INTRA_MODES | VVCG_SLICE_DEBLOCK;
+  for (uint32_t i = 0; i < num_pics; i++) {
+    vvcg_status st = check_slice_substream(pics[i], i, sparse, num_cus, num_levels, allowed, err, err_cap);
+    if (st != VVCG_OK) return st;
+  }
+  return parse_pictures(num_pics, threads, levels_used, err, err_cap, [&](uint32_t i, uint64_t* used) {
+    const vvcg_slice_substream& p = pics[i];
+    vvcg_parse::LevelSink sink{levels + p.level_offset, p.level_cap, 0, sparse != 0};
+    const int code = vvcg_parse::parse_mt_p_picture(
+        p.data, p.size, p.qp, (int)p.width, (int)p.height, (p.options & VVCG_SLICE_DEP_QUANT) != 0,
+        (p.options & VVCG_SLICE_SIGN_HIDING) != 0, cus + p.cu_offset, sink, (int64_t)p.level_offset);
+    *used = sink.at;
+    return code;
+  });
 }
 
 extern "C" vvcg_status vvcg_parse_residual_block(const uint8_t* data, uint64_t size, uint32_t w, uint32_t h,

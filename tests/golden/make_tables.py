@@ -41,7 +41,7 @@ TABLES = [
     ("predict.rs", "ANG_TABLE"), ("predict.rs", "INV_ANG_TABLE"), ("predict.rs", "INTRA_FILTER_THRESHOLD"),
     ("predict.rs", "CHROMA_FILTER_4TAP"), ("predict.rs", "CCLM_DIV_SIG_TABLE"),
     ("predict.rs", "MIP_MATRIX_4X4"), ("predict.rs", "MIP_MATRIX_8X8"), ("predict.rs", "MIP_MATRIX_16X16"),
-    ("cabac.rs", "CTX_INIT_I"), ("cabac.rs", "RENORM_LPS"),
+    ("cabac.rs", "CTX_INIT_I"), ("cabac.rs", "CTX_INIT_P"), ("cabac.rs", "CTX_INIT_B"), ("cabac.rs", "RENORM_LPS"),
     ("residual.rs", "PREFIX_CTX"), ("residual.rs", "MIN_IN_GROUP"), ("residual.rs", "GROUP_IDX"),
     ("residual.rs", "GO_RICE_PARS_COEFF"),
 ]

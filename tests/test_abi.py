@@ -125,6 +125,7 @@ RECORDS = {
     "BDOF_REQ_DTYPE": "vvcg_bdof_req", "DMVR_REQ_DTYPE": "vvcg_dmvr_req", "AFFINE_REQ_DTYPE": "vvcg_affine_req",
     "PROF_REQ_DTYPE": "vvcg_prof_req", "CIIP_REQ_DTYPE": "vvcg_ciip_req", "GPM_REQ_DTYPE": "vvcg_gpm_req",
     "GEN_TB_DTYPE": "vvcg_gen_tb", "GEN_PIC_DTYPE": "vvcg_gen_pic",
+    "INTER_CU_DTYPE": "vvcg_inter_cu", "P_PIC_DTYPE": "vvcg_p_pic",
 }
 
 

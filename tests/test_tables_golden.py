@@ -40,7 +40,8 @@ PAIRS = {
     "kCclmDivSig": ["CCLM_DIV_SIG_TABLE"],
     "kMip4x4": ["MIP_MATRIX_4X4"], "kMip8x8": ["MIP_MATRIX_8X8"], "kMip16x16": ["MIP_MATRIX_16X16"],
     # vvc_cabac.h
-    "kCtxInitI": ["CTX_INIT_I"], "kRenormLps": ["RENORM_LPS"], "kPrefixCtx": ["PREFIX_CTX"],
+    "kCtxInitI": ["CTX_INIT_I"], "kCtxInitP": ["CTX_INIT_P"], "kCtxInitB": ["CTX_INIT_B"],
+    "kRenormLps": ["RENORM_LPS"], "kPrefixCtx": ["PREFIX_CTX"],
     "kMinInGroup": ["MIN_IN_GROUP"], "kGroupIdx": ["GROUP_IDX"], "kGoRicePars": ["GO_RICE_PARS_COEFF"],
 }
 CABAC_HDR = os.path.join(ROOT, "rustmpeg-next_b200", "csrc", "vvc_cabac.h")
