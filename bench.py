@@ -371,6 +371,8 @@ def main():
     ap.add_argument("--general-streams", type=int, default=64)
     ap.add_argument("--no-streams", action="store_true", help="skip the slice-data (CABAC parse) section")
     ap.add_argument("--stream-pictures", type=int, default=64)
+    ap.add_argument("--no-multitool", action="store_true", help="skip the multi-tool stream (IDR + P) section")
+    ap.add_argument("--multitool-reps", type=int, default=8, help="copies of the four 1080p multi-tool streams")
     ap.add_argument("--no-graph", action="store_true", help="launch the stages directly, not from a CUDA graph")
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
@@ -606,6 +608,8 @@ def main():
         line["general"] = bench_general(pkg, dev, stream, args, timed)
     if world == 1 and not args.no_streams:
         line["streams"] = bench_streams(pkg, dev, stream, args, timed)
+    if world == 1 and not args.no_multitool:
+        line["multitool"] = bench_multitool(pkg, dev, stream, args, timed)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt, n = cpu_baseline_oracle(pics_d, cus_d, levels_d, ctus, aps, args.cpu_sample)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": "Mpx/s", "cores": 1, "kind": "port",
@@ -1043,6 +1047,104 @@ def bench_streams(pkg, dev, stream, args, timed):
             "slice_data_to_pixels_mpx_s": round(px / (e2e_ms * 1e-3) / 1e6, 1),
             "parity": {"checked": len(outs) * 3, "mismatches": int(bad + bad_e2e),
                        "against": "SHA-256 of the encoder reconstruction of each picture (fixture)"}}
+
+
+MULTITOOL_STREAMS = os.path.join(ROOT, "tests", "golden", "multitool_streams.npz")
+
+
+def bench_multitool(pkg, dev, stream, args, timed):
+    """Slice data to pixels for the multi-tool stream (IDR + P pictures, the
+    reference's VvcMultiToolEncoder with default options), from the committed
+    slice data (tests/golden/multitool_streams.npz): the small-picture
+    configuration's I P P sequence (64x64, QP 26) as one call, and four
+    independent 1920x1088 I P P P streams (QP 22..37) repeated to a batch:
+    IDR pictures on the frame path in one batch, every P picture in one
+    vvcg_decode_p_batch call (one launch per dependency level). Every decoded
+    picture is hashed against the encoder reconstruction the fixture holds."""
+    import hashlib
+
+    import torch
+
+    z = np.load(MULTITOOL_STREAMS)
+
+    def pictures(name, reps=1):
+        data, offs = z[f"{name}_data"], z[f"{name}_offsets"]
+        w, h = (int(x) for x in z[f"{name}_size"])
+        base = [(str(z[f"{name}_kind"][i]), data[offs[i]:offs[i + 1]].tobytes(), w, h, int(z[f"{name}_qp"][i]), 0)
+                for i in range(len(offs) - 1)]
+        sid0 = [int(x) for x in z[f"{name}_stream"]]
+        nstreams = max(sid0) + 1
+        pics, sid, hashes = [], [], []
+        for r in range(reps):  # the streams repeated as further independent streams
+            pics += base
+            sid += [s_ + r * nstreams for s_ in sid0]
+            hashes += [str(x) for x in z[f"{name}_sha256"]]
+        return pics, sid, hashes, w, h
+
+    def sha(planes):
+        hh = hashlib.sha256()
+        for p in planes:
+            hh.update(p.astype(np.uint8).tobytes())
+        return hh.hexdigest()
+
+    ctx = pkg.Context(dev.index)
+    ctx.set_stream(stream)
+    out = {"what": "multi-tool stream (IDR + P pictures, default slice options) from CABAC slice data: host parse "
+                   "(merge / AMVP / HMVP motion derivation), IDR pictures on the frame path, P pictures by the "
+                   "P-picture kernel (8-tap / 4-tap motion compensation + DCT-2 residual per 32x32 CTU) from the "
+                   "device picture buffer; every picture's SHA-256 checked against the encoder reconstruction in "
+                   "the fixture"}
+    bad, checked = 0, 0
+    # the small-picture configuration: one I P P sequence per call, host pixels out
+    pics, sid, hashes, w, h = pictures("small")
+    got = ctx.decode_multitool_stream(pics, threads=1, stream_ids=sid)
+    bad += sum(sha(g) != hashes[i] for i, g in enumerate(got))
+    checked += len(got)
+    k = max(20, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        ctx.decode_multitool_stream(pics, threads=1, stream_ids=sid)
+    small_ms = (time.perf_counter() - t0) * 1e3 / k
+    out["small"] = {"pictures": "64x64 8-bit 4:2:0, I P P at QP 26", "slice_data_to_host_pixels_ms": round(small_ms, 3),
+                    "fps": round(3 / (small_ms * 1e-3), 1)}
+    # HD: independent streams, one call per step
+    reps = max(1, args.multitool_reps)
+    pics, sid, hashes, w, h = pictures("hd", reps)
+    threads = os.cpu_count() or 1
+    got = ctx.decode_multitool_stream(pics, threads=threads, stream_ids=sid)
+    bad += sum(sha(g) != hashes[i] for i, g in enumerate(got))
+    checked += len(got)
+    px = len(pics) * w * h
+    k = max(3, args.steps // 10)
+    t0 = time.perf_counter()
+    for _ in range(k):
+        ctx.decode_multitool_stream(pics, threads=threads, stream_ids=sid, download=False)
+    torch.cuda.synchronize(dev)
+    call_ms = (time.perf_counter() - t0) * 1e3 / k
+    # the P pictures alone: their parsed records through vvcg_decode_p_batch
+    idx_p = [i for i, p in enumerate(pics) if p[0] != "I"]
+    pp, pc, pl, _ = pkg.parse_multitool([pics[i] for i in idx_p], "P", threads=threads)
+    prev, ref_of = {}, {}
+    for i in range(len(pics)):
+        if pics[i][0] != "I":
+            ref_of[i] = prev[sid[i]]
+        prev[sid[i]] = i
+    for j, i in enumerate(idx_p):
+        pp[j]["ref_slot"][:] = ref_of[i]
+        pp[j]["out_slot"] = i
+    p_ms = timed(lambda: ctx.decode_p_batch(pp, pc, pl), k)
+    p_px = len(idx_p) * w * h
+    out["hd"] = {"pictures": len(pics), "p_pictures": len(idx_p), "size": f"{w}x{h}", "streams": max(sid) + 1,
+                 "slice_data_bytes": int(sum(len(p[1]) for p in pics)),
+                 "slice_data_to_device_pictures_ms": round(call_ms, 2),
+                 "slice_data_to_device_pictures_mpx_s": round(px / (call_ms * 1e-3) / 1e6, 1),
+                 "p_batch_ms": round(p_ms, 3), "p_batch_mpx_s": round(p_px / (p_ms * 1e-3) / 1e6, 1),
+                 "p_batch": "host records and levels in (uploads inside the call), pictures left in the device "
+                            "picture buffer; CUDA events on the call's stream"}
+    out["parity"] = {"checked": int(checked), "mismatches": int(bad),
+                     "against": "SHA-256 of the encoder reconstruction of each picture (fixture)"}
+    ctx.close()
+    return out
 
 
 def _cpu_model():

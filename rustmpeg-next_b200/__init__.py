@@ -514,6 +514,7 @@ class Context:
         """Device picture buffer of `slots` 8-bit 4:2:0 pictures (vvcg_dpb_reserve)."""
         self._check(self._L.vvcg_dpb_reserve(self._h, slots, width, height))
         self._dpb_size = (width, height)
+        self._dpb_slots = slots
 
     def dpb_store(self, pic, slot):
         """Picture `pic` of the last frame-path batch into a slot (on the device)."""
@@ -543,26 +544,35 @@ class Context:
         self._check(self._L.vvcg_decode_p_batch(self._h, _ptr(pics), len(pics), _ptr(cus), len(cus), _ptr(levels),
                                                 levels.size))
 
-    def decode_multitool_stream(self, streams, sparse=False, threads=0):
+    def decode_multitool_stream(self, streams, sparse=False, threads=0, stream_ids=None, download=True):
         """Decode the multi-tool stream's pictures (VvcMultiToolEncoder: IDR
-        and P pictures, each P picture predicting from the picture before it,
-        the DPB's build_ref_lists, inter.rs:481) from their slice data.
+        and P pictures, each P picture predicting from the picture before it
+        in its stream, the DPB's build_ref_lists, inter.rs:481) from their
+        slice data.
 
         streams: [(kind "I" / "P", bytes, width, height, qp, options)] in
-        decoding order, one size. The IDR pictures are parsed and decoded on
+        decoding order, one size; stream_ids (optional) tells the pictures of
+        independent streams apart. The IDR pictures are parsed and decoded on
         the frame path in one batch, the P pictures parsed in parallel and
-        decoded in order from the picture buffer. Returns [(y, u, v)] uint16
-        planes."""
+        decoded in one call from the picture buffer (slot k holds picture k).
+        Returns [(y, u, v)] uint16 planes, or None with download=False."""
         if not streams:
             return []
         w, h = streams[0][2], streams[0][3]
         if any((s[2], s[3]) != (w, h) for s in streams):
             raise InvalidInput("the pictures of a stream share one size")
+        sid = list(stream_ids) if stream_ids is not None else [0] * len(streams)
         idx_i = [k for k, s in enumerate(streams) if s[0] == "I"]
         idx_p = [k for k, s in enumerate(streams) if s[0] != "I"]
-        if idx_p and idx_p[0] < (idx_i[0] if idx_i else len(streams)):
-            raise InvalidInput("a P picture needs a picture before it")
-        self.dpb_reserve(len(streams), w, h)
+        prev, ref_of = {}, {}
+        for k, s in enumerate(streams):
+            if s[0] != "I":
+                if sid[k] not in prev:
+                    raise InvalidInput("a P picture needs a picture before it")
+                ref_of[k] = prev[sid[k]]
+            prev[sid[k]] = k
+        if getattr(self, "_dpb_size", None) != (w, h) or getattr(self, "_dpb_slots", 0) < len(streams):
+            self.dpb_reserve(len(streams), w, h)
         if idx_i:
             pics, cus, levels, _ = parse_multitool([streams[k] for k in idx_i], "I", sparse, threads)
             ctus = np.zeros(len(idx_i) * (w // 32) * (h // 32), CTU_DTYPE)
@@ -574,10 +584,12 @@ class Context:
         if idx_p:
             pp, pcus, plevels, _ = parse_multitool([streams[k] for k in idx_p], "P", sparse, threads)
             for j, k in enumerate(idx_p):
-                pp[j]["ref_slot"][:] = k - 1
+                pp[j]["ref_slot"][:] = ref_of[k]
                 pp[j]["num_refs"] = 1
                 pp[j]["out_slot"] = k
             self.decode_p_batch(pp, pcus, plevels)
+        if not download:
+            return None
         return [self.dpb_download(k) for k in range(len(streams))]
 
     def decode_batch_async(self, batch: Batch, outs):

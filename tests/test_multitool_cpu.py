@@ -226,3 +226,40 @@ def test_unsupported_options_and_ctu_sizes_are_rejected(pkg, orc):
         pkg.parse_multitool([("I", st[0]["data"], 64, 64, 26, 16)], "I")  # an option outside VVCG_SLICE_*
     with pytest.raises(pkg.InvalidInput):
         pkg.parse_multitool([("I", st[0]["data"], 64, 48, 26, 0)], "I")  # not a multiple of 32
+
+
+def _fixture_pictures(name):
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "multitool_streams.npz"))
+    data, offs = z[f"{name}_data"], z[f"{name}_offsets"]
+    w, h = (int(x) for x in z[f"{name}_size"])
+    pics = [(str(z[f"{name}_kind"][i]), data[offs[i]:offs[i + 1]].tobytes(), w, h, int(z[f"{name}_qp"][i]), 0)
+            for i in range(len(offs) - 1)]
+    return pics, [int(x) for x in z[f"{name}_stream"]], [str(x) for x in z[f"{name}_sha256"]]
+
+
+def _sha(planes):
+    import hashlib
+
+    hh = hashlib.sha256()
+    for p in planes:
+        hh.update(np.ascontiguousarray(p, dtype=np.uint8).tobytes())
+    return hh.hexdigest()
+
+
+@pytest.mark.parametrize("name", ["small", "hd"])
+def test_committed_streams_parse_and_decode_to_their_hashes(pkg, orc, name):
+    """tests/golden/multitool_streams.npz: the parser's records, decoded by
+    the oracle picture after picture (each P picture from the previous
+    picture of its stream), give the committed reconstruction hashes."""
+    pics, sid, hashes = _fixture_pictures(name)
+    prev = {}
+    for i, (kind, data, w, h, qp, opts) in enumerate(pics):
+        _, cus, levels, _ = pkg.parse_multitool([(kind, data, w, h, qp, opts)], kind, threads=1)
+        if kind == "I":
+            dec = orc.mt_decode(cus, levels, w, h, qp, opts)
+        else:
+            dec = orc.inter_decode(cus, levels, w, h, qp, [prev[sid[i]]], opts)
+        assert _sha(dec) == hashes[i], i
+        prev[sid[i]] = dec

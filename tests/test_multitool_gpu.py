@@ -234,3 +234,17 @@ def test_picture_buffer_round_trip_and_store(ctx, pkg, orc):
     ctx.decode_batch(batch)
     ctx.dpb_store(0, 0)
     _assert_same(ctx.dpb_download(0), rec, "frame-path picture stored")
+
+
+@pytest.mark.parametrize("name", ["small", "hd"])
+@pytest.mark.parametrize("sparse", [False, True])
+def test_committed_streams_decode_to_their_hashes(ctx, pkg, name, sparse):
+    """tests/golden/multitool_streams.npz (the small-picture I P P sequence;
+    four 1920x1088 I P P P streams at QP 22..37) from slice data to pixels in
+    one call: every picture's SHA-256 equals the committed reconstruction's."""
+    from test_multitool_cpu import _fixture_pictures, _sha
+
+    pics, sid, hashes = _fixture_pictures(name)
+    got = ctx.decode_multitool_stream(pics, sparse=sparse, threads=4, stream_ids=sid)
+    for i, g in enumerate(got):
+        assert _sha(g) == hashes[i], i
