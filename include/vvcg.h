@@ -1109,7 +1109,7 @@ vvcg_status vvcg_parse_multitool_p(const vvcg_slice_substream* pics, uint32_t nu
 /* The context's picture buffer: device pictures of 8-bit 4:2:0 samples in
  * 16-bit planes (stride a multiple of 64 samples), the reference pictures of
  * P pictures (the reference decoder's DecodedPictureBuffer, inter.rs:446,
- * kept on the device). vvcg_dpb_reserve makes `slots` slots of width x
+ * kept on the device). vvcg_dpb_reserve makes `slots` (1..1024) slots of width x
  * height (contents undefined; earlier slots are released). */
 vvcg_status vvcg_dpb_reserve(vvcg_ctx* ctx, uint32_t slots, uint32_t width, uint32_t height);
 /* Copies picture `pic` of the last frame-path batch (vvcg_decode_batch or

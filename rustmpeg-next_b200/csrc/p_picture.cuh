@@ -189,8 +189,8 @@ static_assert(sizeof(vvcg_p_pic) == 36, "P picture layout");
 
 extern "C" vvcg_status vvcg_dpb_reserve(vvcg_ctx* ctx, uint32_t slots, uint32_t width, uint32_t height) {
   if (!ctx) return VVCG_INVALID_INPUT;
-  if (!slots || slots > 64 || !width || !height || (width & 1) || (height & 1))
-    return fail(ctx, VVCG_INVALID_INPUT, "picture buffer: 1..64 slots of a nonzero even size");
+  if (!slots || slots > 1024 || !width || !height || (width & 1) || (height & 1))
+    return fail(ctx, VVCG_INVALID_INPUT, "picture buffer: 1..1024 slots of a nonzero even size");
   if ((uint64_t)width * height > kMaxLumaSamples) return fail(ctx, VVCG_LIMIT_EXCEEDED, "picture too large");
   CK(cudaSetDevice(ctx->device), "cudaSetDevice");
   CK(cudaStreamSynchronize(ctx->stream), "sync");
