@@ -1111,19 +1111,19 @@ def bench_multitool(pkg, dev, stream, args, timed):
     reps = max(1, args.multitool_reps)
     pics, sid, hashes, w, h = pictures("hd", reps)
     threads = os.cpu_count() or 1
-    got = ctx.decode_multitool_stream(pics, threads=threads, stream_ids=sid)
+    got = ctx.decode_multitool_stream(pics, sparse=True, threads=threads, stream_ids=sid)
     bad += sum(sha(g) != hashes[i] for i, g in enumerate(got))
     checked += len(got)
     px = len(pics) * w * h
     k = max(3, args.steps // 10)
     t0 = time.perf_counter()
     for _ in range(k):
-        ctx.decode_multitool_stream(pics, threads=threads, stream_ids=sid, download=False)
+        ctx.decode_multitool_stream(pics, sparse=True, threads=threads, stream_ids=sid, download=False)
     torch.cuda.synchronize(dev)
     call_ms = (time.perf_counter() - t0) * 1e3 / k
     # the P pictures alone: their parsed records through vvcg_decode_p_batch
     idx_p = [i for i, p in enumerate(pics) if p[0] != "I"]
-    pp, pc, pl, _ = pkg.parse_multitool([pics[i] for i in idx_p], "P", threads=threads)
+    pp, pc, pl, _ = pkg.parse_multitool([pics[i] for i in idx_p], "P", sparse=True, threads=threads)
     prev, ref_of = {}, {}
     for i in range(len(pics)):
         if pics[i][0] != "I":
@@ -1139,8 +1139,9 @@ def bench_multitool(pkg, dev, stream, args, timed):
                  "slice_data_to_device_pictures_ms": round(call_ms, 2),
                  "slice_data_to_device_pictures_mpx_s": round(px / (call_ms * 1e-3) / 1e6, 1),
                  "p_batch_ms": round(p_ms, 3), "p_batch_mpx_s": round(p_px / (p_ms * 1e-3) / 1e6, 1),
-                 "p_batch": "host records and levels in (uploads inside the call), pictures left in the device "
-                            "picture buffer; CUDA events on the call's stream"}
+                 "p_batch_level_bytes": int(pl.nbytes),
+                 "p_batch": "host records and sparse levels in (uploads inside the call), pictures left in the "
+                            "device picture buffer; CUDA events on the call's stream"}
     out["parity"] = {"checked": int(checked), "mismatches": int(bad),
                      "against": "SHA-256 of the encoder reconstruction of each picture (fixture)"}
     ctx.close()
