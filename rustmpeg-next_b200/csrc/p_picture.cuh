@@ -110,11 +110,14 @@ __device__ void p_mc_component(const PPicDev& P, const vvcg_inter_cu& rec, int c
 }
 
 // Grid: (CTUs of the largest picture of the level, pictures of the level).
-__global__ void __launch_bounds__(kPWarps * 32)
+__global__ void __launch_bounds__(kPWarps * 32, 8)
 k_p_cu(const PPicDev* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels, uint32_t* status) {
   __shared__ __align__(16) union {
-    int32_t ws[3][2][1024 + kTuPad];  // residual transforms, one pair per component warp
-    PMcSmem mc;                       // then the prediction windows
+    struct {
+      int32_t luma[2][1024 + kTuPad];    // the luma warp's transform tiles
+      int32_t chroma[2][2][256 + kTuPad];  // the chroma warps' tiles
+    } ws;
+    PMcSmem mc;  // then the prediction windows
   } U;
   __shared__ __align__(16) int16_t res[1024 + 2 * 256];
   __shared__ __align__(16) int16_t dense[3][1024];
@@ -153,7 +156,9 @@ k_p_cu(const PPicDev* __restrict__ pics, const int16_t* __restrict__ levels, uin
         t.flags = ts ? VVCG_TU_TRANSFORM_SKIP : ((P.flags & 1) ? VVCG_TU_DEP_QUANT : 0);
         t.mts_idx = t.lfnst_idx = t.lfnst_mode = 0;
         t.in_off = t.out_off = 0;
-        warp_tu_inverse(t, src, r, U.ws[c][0], U.ws[c][1], lane);
+        int32_t* A = c ? U.ws.chroma[c - 1][0] : U.ws.luma[0];
+        int32_t* B = c ? U.ws.chroma[c - 1][1] : U.ws.luma[1];
+        warp_tu_inverse(t, src, r, A, B, lane);
       }
     }
     if (!coded)
