@@ -677,6 +677,60 @@ __device__ __noinline__ void alf_classify_tile(const uint16_t (&t)[kAlfH][kAlfW]
 // The 7x7 diamond (apply_alf_luma_plane_16, filter.rs:2045-2124) on the
 // staged tile after alf_classify_tile: each of the 256 threads filters one
 // 4-sample row of a block and stores it to dst.
+// The 7x7 diamond of four horizontally adjacent outputs (row ty, columns
+// tx0..tx0+3, tx0 a multiple of 4) with every coefficient in a signed byte.
+// Each row of the diamond is read once as 8-byte words (columns tx0-4 ..
+// tx0+7); for each output and coefficient the two symmetric samples are
+// packed into one register (byte permute), their differences to the centre
+// clipped as two 16-bit lanes (vmaxs2 / vmins2) and both multiplied by the
+// coefficient and summed by one dp2a. The sums are exact integers, equal to
+// the scalar loop's: sum_k f_k * (clip(p0 - c) + clip(p1 - c)).
+__device__ __forceinline__ void alf_filter4_packed(const uint16_t (&t)[kAlfH][kAlfW], int tx0, int ty,
+                                                   const int (&fc)[12], const int (&fcl)[12], int maxv, int (&out)[4]) {
+  // (column, row) offset of the first sample of each coefficient's pair; the
+  // second is its mirror (filter.rs:2045 apply_alf_luma_plane_16 order)
+  constexpr int kAx[12] = {0, 1, 0, -1, 2, 1, 0, -1, -2, 3, 2, 1};
+  constexpr int kAy[12] = {3, 2, 2, 2, 1, 1, 1, 1, 1, 0, 0, 0};
+  uint32_t R[7][6];  // R[dy + 3][w]: samples tx0 - 4 + 2w (low half) and tx0 - 3 + 2w (high half)
+#pragma unroll
+  for (int dy = -3; dy <= 3; dy++) {
+    const uint2* row = reinterpret_cast<const uint2*>(&t[ty + dy][tx0 - 4]);
+#pragma unroll
+    for (int g = 0; g < 3; g++) {
+      const uint2 v = row[g];
+      R[dy + 3][2 * g] = v.x;
+      R[dy + 3][2 * g + 1] = v.y;
+    }
+  }
+  uint32_t pcl[12], ncl[12], cb[6];
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    pcl[k] = ((uint32_t)fcl[k] & 0xFFFFu) * 0x10001u;
+    ncl[k] = ((uint32_t)(-fcl[k]) & 0xFFFFu) * 0x10001u;
+  }
+#pragma unroll
+  for (int m = 0; m < 6; m++)
+    cb[m] = ((uint32_t)(uint8_t)fc[2 * m] * 0x0101u) | (((uint32_t)(uint8_t)fc[2 * m + 1] * 0x0101u) << 16);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int jc = i + 4;  // the centre's column index within R's 12 samples
+    const uint32_t hc = 2 * (jc & 1);
+    const uint32_t cc = __byte_perm(R[3][jc >> 1], 0, hc | ((hc + 1) << 4) | (hc << 8) | ((hc + 1) << 12));
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      const int ja = jc + kAx[k], jb = jc - kAx[k];
+      const uint32_t ha = 2 * (ja & 1), hb = 2 * (jb & 1) + 4;
+      const uint32_t pair = __byte_perm(R[3 + kAy[k]][ja >> 1], R[3 - kAy[k]][jb >> 1],
+                                        ha | ((ha + 1) << 4) | (hb << 8) | ((hb + 1) << 12));
+      const uint32_t d = __vmins2(__vmaxs2(__vsub2(pair, cc), ncl[k]), pcl[k]);
+      s = (k & 1) ? __dp2a_hi((int)d, (int)cb[k >> 1], s) : __dp2a_lo((int)d, (int)cb[k >> 1], s);
+    }
+    const int c = (int)(cc & 0xFFFFu);
+    out[i] = clampi(c + ((s + 64) >> 7), 0, maxv);
+  }
+}
+
 __device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW], int x0, int y0, int w, int h, int bd,
                                                 const AlfTileWs& ws, uint16_t* dst, int stride, uint32_t* status) {
   auto g = [&](int tx, int ty) -> int { return t[ty][tx]; };
@@ -697,6 +751,12 @@ __device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW
       fcl[k] = ws.fcl[b][k];
     }
     const int maxv = (1 << bd) - 1;
+    bool narrow = true;  // every coefficient fits a signed byte (the packed path's dp2a operand)
+#pragma unroll
+    for (int k = 0; k < 12; k++) narrow &= fc[k] >= -128 && fc[k] <= 127;
+    if (narrow) {
+      alf_filter4_packed(t, tx0, ty, fc, fcl, maxv, out);
+    } else {
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       const int tx = tx0 + i;
@@ -717,6 +777,7 @@ __device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW
       s += fc[11] * ca(fcl[11], g(tx + 1, ty), g(tx - 1, ty));
       out[i] = clampi(c + ((s + 64) >> 7), 0, maxv);
     }
+    }
   }
   *reinterpret_cast<uint2*>(dst + (size_t)y * stride + x) =
       make_uint2((uint32_t)out[0] | ((uint32_t)out[1] << 16), (uint32_t)out[2] | ((uint32_t)out[3] << 16));
@@ -728,7 +789,7 @@ __device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW
 // halo lies inside the plane needs no clamping and is staged with 8-byte
 // loads. Then the blocks are classified and filtered (alf_classify_tile,
 // alf_filter_tile).
-__global__ void __launch_bounds__(256) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
+__global__ void __launch_bounds__(256, 5) k_alf_luma(const AlfPass* __restrict__ passes, uint32_t* status) {
   const AlfPass& A = passes[blockIdx.z];
   __shared__ __align__(16) uint16_t t[kAlfH][kAlfW];
   __shared__ AlfTileWs ws;
@@ -814,7 +875,7 @@ __device__ __forceinline__ int sao_at(const uint16_t (*d)[kSaStW], int ox, int o
   return c;
 }
 
-__global__ void __launch_bounds__(256) k_sao_alf_luma(const SaoAlfPass* __restrict__ passes, uint32_t spin_limit,
+__global__ void __launch_bounds__(256, 5) k_sao_alf_luma(const SaoAlfPass* __restrict__ passes, uint32_t spin_limit,
                                                       uint32_t* status) {
   const SaoAlfPass& S = passes[blockIdx.z];
   __shared__ __align__(128) uint16_t d[kSaStH][kSaStW];
