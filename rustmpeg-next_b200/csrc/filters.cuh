@@ -674,9 +674,6 @@ __device__ __noinline__ void alf_classify_tile(const uint16_t (&t)[kAlfH][kAlfW]
   if (q == 0) ws.abort[b] = abort ? 1 : 0;
 }
 
-// The 7x7 diamond (apply_alf_luma_plane_16, filter.rs:2045-2124) on the
-// staged tile after alf_classify_tile: each of the 256 threads filters one
-// 4-sample row of a block and stores it to dst.
 // The 7x7 diamond of four horizontally adjacent outputs (row ty, columns
 // tx0..tx0+3, tx0 a multiple of 4) with every coefficient in a signed byte.
 // Each row of the diamond is read once as 8-byte words (columns tx0-4 ..
@@ -731,6 +728,9 @@ __device__ __forceinline__ void alf_filter4_packed(const uint16_t (&t)[kAlfH][kA
   }
 }
 
+// The 7x7 diamond (apply_alf_luma_plane_16, filter.rs:2045-2124) on the
+// staged tile after alf_classify_tile: each of the 256 threads filters one
+// 4-sample row of a block and stores it to dst.
 __device__ __forceinline__ void alf_filter_tile(const uint16_t (&t)[kAlfH][kAlfW], int x0, int y0, int w, int h, int bd,
                                                 const AlfTileWs& ws, uint16_t* dst, int stride, uint32_t* status) {
   auto g = [&](int tx, int ty) -> int { return t[ty][tx]; };
