@@ -634,7 +634,7 @@ CNN_FLOP_PER_BLOCK = 2 * 1024 * 32 * 9 * (2 + 3 * 32)  # conv1 (2 inputs) + 3 x 
 # needs a bitstream); all are reported. The first also gives the
 # no-fallback comparison of the trained and an untrained network.
 PRUNE_POLICIES = ((6, 2, 0.7), (3, 2, 0.0), (6, 3, 0.7), (6, 2, 0.75), (6, 3, 0.75), (6, 2, 0.8), (6, 3, 0.8),
-                  (3, 3, 0.8), (6, 3, 0.85))
+                  (3, 3, 0.8), (6, 3, 0.85), (6, 3, 0.77), (6, 3, 0.78), (6, 3, 0.79), (6, 4, 0.78))
 COST_BOUND_PCT = 1.0
 
 
