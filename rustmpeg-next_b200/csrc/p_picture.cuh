@@ -9,10 +9,11 @@
 // (reconstruct_component_full, slice.rs:1920: DCT-2 or transform skip,
 // regular or dependent dequantisation) and the clipped sum. Every CTU of a
 // picture depends only on the reference pictures, so one CTA per CTU runs
-// them all at once: its first three warps turn the Y, Cb and Cr levels into
-// residuals in shared memory (the TU path's warp_tu_inverse), then all four
-// warps stage each component's reference window, filter it and store the
-// reconstruction into the picture's buffer slot. apply_inter_loop_filters'
+// them all at once: warp 0 turns the Y levels into the residual (the TU
+// path's warp_tu_inverse) while warps 1 and 2 do Cb and Cr and then, with
+// warp 3, stage each component's reference window and filter it into a
+// prediction in shared memory; all four warps then store the clipped sums
+// into the picture's buffer slot. apply_inter_loop_filters'
 // CTU-boundary deblocking (slice.rs:2291) follows for pictures that enable
 // it. Pictures are grouped into levels by their slots (a picture waits for
 // the pictures before it that write a slot it reads or writes, or read the
@@ -32,26 +33,29 @@ struct PPicDev {
 };
 
 // The MC window of one component (the luma 39 x 39, or chroma 19 x 19) and
-// the horizontal pass's rows.
+// the horizontal pass's rows. 16 bits suffice: samples are 8-bit and the
+// horizontal sums of the 8-tap / 4-tap filters stay within +-32767.
 struct PMcSmem {
-  int win[39][40];
-  int tmp[39][32];
+  int16_t win[39][40];
+  int16_t tmp[39][32];
 };
 
-// One component of a coding unit: prediction from the reference window,
-// plus the residual, clipped to 8 bits, into the slot plane.
-__device__ void p_mc_component(const PPicDev& P, const vvcg_inter_cu& rec, int comp, int bx, int by,
-                               const int16_t* __restrict__ res, PMcSmem& S) {
+// Barrier of warps 1..3, the prediction warps of a CTA.
+__device__ __forceinline__ void p_mc_sync() { asm volatile("bar.sync 1, 96;" ::: "memory"); }
+
+// The inter prediction of one component of a coding unit into `pred` (int16,
+// n x n raster), by the prediction warps (thread `tid` of 96).
+__device__ void p_predict_component(const PPicDev& P, const vvcg_inter_cu& rec, int comp, int bx, int by,
+                                    int16_t* __restrict__ pred, PMcSmem& S, int tid) {
+  constexpr int nth = 96;
   const bool luma = comp == 0;
   const int n = luma ? 32 : 16, ntap = luma ? 8 : 4, half = luma ? 3 : 1;
   const int pw = luma ? P.w : P.w / 2, ph = luma ? P.h : P.h / 2;
   const int x0 = luma ? bx : bx / 2, y0 = luma ? by : by / 2;
-  uint16_t* out = P.out[comp] + (size_t)y0 * P.stride[comp] + x0;
-  const int ostride = P.stride[comp];
+  const int rstride = P.stride[comp];
   const bool has = (rec.inter_dir & 1) && rec.ref_idx[0] >= 0;
   if (!has) {  // predict_inter_pu without a usable list: 128
-    for (int i = threadIdx.x; i < n * n; i += blockDim.x)
-      out[(size_t)(i / n) * ostride + (i % n)] = (uint16_t)clampi(128 + res[i], 0, 255);
+    for (int i = tid; i < n * n; i += nth) pred[i] = 128;
     return;
   }
   const uint16_t* ref = P.ref[min((int)rec.ref_idx[0], P.num_refs - 1)][comp];
@@ -71,23 +75,23 @@ __device__ void p_mc_component(const PPicDev& P, const vvcg_inter_cu& rec, int c
     }
   }
   const int wx0 = x0 + dx - half, wy0 = y0 + dy - half, ww = n + ntap - 1;
-  __syncthreads();  // the window buffer is free
-  for (int i = threadIdx.x; i < ww * ww; i += blockDim.x) {
+  p_mc_sync();  // the window buffer is free
+  for (int i = tid; i < ww * ww; i += nth) {
     const int yy = i / ww, xx = i % ww;
     const int gx = clampi(wx0 + xx, 0, pw - 1), gy = clampi(wy0 + yy, 0, ph - 1);
-    S.win[yy][xx] = ref[(size_t)gy * ostride + gx];
+    S.win[yy][xx] = (int16_t)ref[(size_t)gy * rstride + gx];
   }
-  __syncthreads();
+  p_mc_sync();
   if (fx != 0 && fy != 0) {  // horizontal pass over every window row (shift1 is 0 at 8 bits)
-    for (int i = threadIdx.x; i < n * ww; i += blockDim.x) {
+    for (int i = tid; i < n * ww; i += nth) {
       const int x = i % n, yy = i / n;
       int s = 0;
       for (int k = 0; k < ntap; k++) s += fh[k] * S.win[yy][x + k];
-      S.tmp[yy][x] = s;
+      S.tmp[yy][x] = (int16_t)s;
     }
-    __syncthreads();
+    p_mc_sync();
   }
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+  for (int i = tid; i < n * n; i += nth) {
     const int x = i % n, y = i / n;
     int p;
     if (fx == 0 && fy == 0) {
@@ -105,22 +109,22 @@ __device__ void p_mc_component(const PPicDev& P, const vvcg_inter_cu& rec, int c
       for (int k = 0; k < ntap; k++) s += fv[k] * S.tmp[y + k][x];
       p = clampi((s + 2048) >> 12, 0, 255);
     }
-    out[(size_t)y * ostride + x] = (uint16_t)clampi(p + res[i], 0, 255);
+    pred[i] = (int16_t)p;
   }
 }
 
 // Grid: (CTUs of the largest picture of the level, pictures of the level).
-__global__ void __launch_bounds__(kPWarps * 32, 8)
+// Warp 0 turns the luma levels into the residual while warps 1 and 2 do the
+// chroma ones and then, with warp 3, the three predictions; all four warps
+// then add, clip and store.
+__global__ void __launch_bounds__(kPWarps * 32, 7)
 k_p_cu(const PPicDev* __restrict__ pics, const int16_t* __restrict__ levels, uint64_t n_levels, uint32_t* status) {
-  __shared__ __align__(16) union {
-    struct {
-      int32_t luma[2][1024 + kTuPad];    // the luma warp's transform tiles
-      int32_t chroma[2][2][256 + kTuPad];  // the chroma warps' tiles
-    } ws;
-    PMcSmem mc;  // then the prediction windows
-  } U;
+  __shared__ __align__(16) int32_t ws_luma[2][1024 + kTuPad];     // the luma warp's transform tiles
+  __shared__ __align__(16) int32_t ws_chroma[2][2][256 + kTuPad];  // the chroma warps' tiles
+  __shared__ __align__(16) PMcSmem mc;
   __shared__ __align__(16) int16_t res[1024 + 2 * 256];
-  __shared__ __align__(16) int16_t dense[3][1024];
+  __shared__ __align__(16) int16_t pred[1024 + 2 * 256];
+  __shared__ __align__(16) int16_t dense[1024 + 2 * 256];  // sparse TBs expanded (same layout as res)
   const PPicDev& P = pics[blockIdx.y];
   const int cu = blockIdx.x;
   if (cu >= P.gw * P.gh) return;
@@ -138,8 +142,8 @@ k_p_cu(const PPicDev* __restrict__ pics, const int16_t* __restrict__ levels, uin
       if (ok && (P.flags & 2)) {  // sparse: count, unused word, (index, level) pairs
         const int cnt = (off & 1) || (uint64_t)off + 2 > n_levels ? -1 : levels[off];
         ok = cnt >= 0 && cnt <= n && (uint64_t)off + 2 + 2 * (uint64_t)cnt <= n_levels &&
-             expand_sparse(levels + off, cnt, n, dense[c], lane);
-        src = dense[c];
+             expand_sparse(levels + off, cnt, n, dense + off_res, lane);
+        src = dense + off_res;
       } else if (ok) {
         ok = (uint64_t)off + (uint64_t)n <= n_levels;
       }
@@ -156,15 +160,32 @@ k_p_cu(const PPicDev* __restrict__ pics, const int16_t* __restrict__ levels, uin
         t.flags = ts ? VVCG_TU_TRANSFORM_SKIP : ((P.flags & 1) ? VVCG_TU_DEP_QUANT : 0);
         t.mts_idx = t.lfnst_idx = t.lfnst_mode = 0;
         t.in_off = t.out_off = 0;
-        int32_t* A = c ? U.ws.chroma[c - 1][0] : U.ws.luma[0];
-        int32_t* B = c ? U.ws.chroma[c - 1][1] : U.ws.luma[1];
+        int32_t* A = c ? ws_chroma[c - 1][0] : ws_luma[0];
+        int32_t* B = c ? ws_chroma[c - 1][1] : ws_luma[1];
         warp_tu_inverse(t, src, r, A, B, lane);
       }
     }
     if (!coded)
       for (int i = lane; i < n; i += 32) r[i] = 0;
   }
-  for (int c = 0; c < 3; c++) p_mc_component(P, rec, c, bx, by, res + (c == 0 ? 0 : (c == 1 ? 1024 : 1280)), U.mc);
+  if (wid >= 1)
+    for (int c = 0; c < 3; c++)
+      p_predict_component(P, rec, c, bx, by, pred + (c == 0 ? 0 : (c == 1 ? 1024 : 1280)), mc, threadIdx.x - 32);
+  __syncthreads();
+  // reconstruction: clip(prediction + residual), two samples per store
+  for (int i = threadIdx.x; i < (1024 + 512) / 2; i += blockDim.x) {
+    const int e = 2 * i;
+    const int comp = e < 1024 ? 0 : (e < 1280 ? 1 : 2);
+    const int n = comp ? 16 : 32, base = comp == 0 ? 0 : (comp == 1 ? 1024 : 1280);
+    const int k = e - base, x = k % n, y = k / n;
+    const int x0 = comp ? bx / 2 : bx, y0 = comp ? by / 2 : by;
+    const uint32_t pv = *reinterpret_cast<const uint32_t*>(&pred[e]);
+    const uint32_t rv = *reinterpret_cast<const uint32_t*>(&res[e]);
+    const int v0 = clampi((int)(int16_t)(pv & 0xFFFFu) + (int)(int16_t)(rv & 0xFFFFu), 0, 255);
+    const int v1 = clampi((int)(int16_t)(pv >> 16) + (int)(int16_t)(rv >> 16), 0, 255);
+    *reinterpret_cast<uint32_t*>(P.out[comp] + (size_t)(y0 + y) * P.stride[comp] + x0 + x) =
+        (uint32_t)v0 | ((uint32_t)v1 << 16);
+  }
 }
 
 }  // namespace vvcg
