@@ -377,6 +377,8 @@ def main():
     ap.add_argument("--no-encode", action="store_true", help="skip the encoder (full vs CNN-pruned search) section")
     ap.add_argument("--train-frames", type=int, default=26, help="1080p frames per QP labelled for training")
     ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--train-lr", type=float, default=1e-3)
+    ap.add_argument("--train-schedule", default="constant", choices=["constant", "cosine"])
     ap.add_argument("--eval-frames", type=int, default=8, help="held-out 1080p frames per QP for the encoder")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -674,7 +676,8 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
     n_train = sum(int(d[1].shape[0]) for d in data)
     cnn.train(ctx, data, steps=2, batch=1024, lr=1e-3, seed=11)  # warm-up (fresh parameters below)
     t1 = time.perf_counter()
-    params, losses = cnn.train(ctx, data, steps=args.train_steps, batch=1024, lr=1e-3, seed=11)
+    params, losses = cnn.train(ctx, data, steps=args.train_steps, batch=1024, lr=args.train_lr, seed=11,
+                               schedule=args.train_schedule, lr_min=args.train_lr * 0.05)
     train_s = time.perf_counter() - t1
     del data
     # held-out frames
@@ -767,7 +770,8 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
             "cnn_inference": {"blocks": 4096, "ms": round(ms4, 4), "tflops": round(tflops, 1),
                               "peak": bf16_peak, "frac": round(tflops / bf16_peak, 4),
                               "flop_per_block": CNN_FLOP_PER_BLOCK},
-            "training": {"ctus_labelled": n_train, "label_s": round(label_s, 2), "steps": args.train_steps,
+            "training": {"ctus_labelled": n_train, "label_s": round(label_s, 2), "steps": args.train_steps, "lr": args.train_lr,
+                         "schedule": args.train_schedule,
                          "batch": 1024, "s": round(train_s, 2), "first_loss": round(losses[0], 4),
                          "final_loss": round(float(np.mean(losses[-20:])), 4)}}
 

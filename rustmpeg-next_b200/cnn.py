@@ -139,9 +139,10 @@ def _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed):
             out.append((plane, xy, lab, qp))
 
 
-def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None):
+def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None, schedule="constant", lr_min=0.0):
     """Adam on the labelled blocks of training_set (batches drawn from one
-    frame at a time); returns (params CUDA tensor, losses)."""
+    frame at a time); returns (params CUDA tensor, losses). schedule
+    "cosine" decays the step size from lr to lr_min over the steps."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -152,7 +153,9 @@ def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None):
         for step in range(1, steps + 1):
             plane, xy, lab, qp = data[int(rng.integers(0, len(data)))]
             idx = torch.from_numpy(rng.choice(xy.shape[0], min(batch, xy.shape[0]), replace=False)).cuda()
-            loss, _ = ctx.cnn_train_step(plane, 10, qp, xy[idx], lab[idx], p, m, v, step, lr, sync=False)
+            lr_t = lr if schedule == "constant" else \
+                lr_min + (lr - lr_min) * 0.5 * (1.0 + np.cos(np.pi * (step - 1) / max(1, steps)))
+            loss, _ = ctx.cnn_train_step(plane, 10, qp, xy[idx], lab[idx], p, m, v, step, float(lr_t), sync=False)
             losses.append(loss)
         torch.cuda.synchronize()
     return p, [float(x.item()) for x in losses]
