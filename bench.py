@@ -379,6 +379,9 @@ def main():
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--train-lr", type=float, default=1e-3)
     ap.add_argument("--train-schedule", default="constant", choices=["constant", "cosine"])
+    ap.add_argument("--soft-labels", type=float, default=None,
+                    help="train the mode head on softmax(-(cost - best) / (T * lambda)) of the full search's "
+                         "67 mode costs instead of its best mode")
     ap.add_argument("--eval-frames", type=int, default=8, help="held-out 1080p frames per QP for the encoder")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -671,7 +674,7 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
         return e0.elapsed_time(e1)
 
     t0 = time.perf_counter()
-    data = cnn.training_set(ctx, n_frames=args.train_frames, qps=QPS, seed=11)
+    data = cnn.training_set(ctx, n_frames=args.train_frames, qps=QPS, seed=11, soft_t=args.soft_labels)
     label_s = time.perf_counter() - t0
     n_train = sum(int(d[1].shape[0]) for d in data)
     cnn.train(ctx, data, steps=2, batch=1024, lr=1e-3, seed=11)  # warm-up (fresh parameters below)
@@ -771,7 +774,7 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
                               "peak": bf16_peak, "frac": round(tflops / bf16_peak, 4),
                               "flop_per_block": CNN_FLOP_PER_BLOCK},
             "training": {"ctus_labelled": n_train, "label_s": round(label_s, 2), "steps": args.train_steps, "lr": args.train_lr,
-                         "schedule": args.train_schedule,
+                         "schedule": args.train_schedule, "soft_labels": args.soft_labels,
                          "batch": 1024, "s": round(train_s, 2), "first_loss": round(losses[0], 4),
                          "final_loss": round(float(np.mean(losses[-20:])), 4)}}
 

@@ -751,6 +751,15 @@ vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64
                                     const uint8_t* labels, uint32_t num_blocks, float* params, float* adam_m,
                                     float* adam_v, uint32_t step, float lr, float* grads, float* loss,
                                     uint32_t* status);
+/* vvcg_cnn_train_step_dev with a target distribution for the mode head
+ * (soft_modes: device memory, num_blocks x 67 fp32, each row summing to 1):
+ * its cross-entropy loss and gradient p - target; the split head keeps the
+ * labels' split type. */
+vvcg_status vvcg_cnn_train_step_soft_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                         uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
+                                         const uint8_t* labels, const float* soft_modes, uint32_t num_blocks,
+                                         float* params, float* adam_m, float* adam_v, uint32_t step, float lr,
+                                         float* grads, float* loss, uint32_t* status);
 
 /* ---- tensor-core self-test ---------------------------------------------------- */
 
@@ -775,6 +784,16 @@ vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint6
                                        const uint32_t* ctu_xy, uint32_t num_ctus, const float* logits,
                                        uint32_t top_modes, uint32_t top_splits, float threshold,
                                        vvcg_ctu_search_res* res);
+
+/* The full CTU search of vvcg_ctu_search_pruned_dev (no pruning) that also
+ * writes, per CTU, the cost (SATD + lambda * mode bits) of each of the 67
+ * luma modes for the unsplit 32x32 coding unit: mode_costs, device memory,
+ * num_ctus x 67 uint32. The training targets of the pruner's mode head are
+ * built from them (a near-tie between modes costs little to miss). No
+ * counterpart in the reference, whose encoder keeps only the best mode. */
+vvcg_status vvcg_ctu_search_costs_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                      uint32_t height, uint8_t bit_depth, uint32_t lambda_q8, const uint32_t* ctu_xy,
+                                      uint32_t num_ctus, vvcg_ctu_search_res* res, uint32_t* mode_costs);
 
 /* ---- general-decoder intra prediction -------------------------------------- */
 

@@ -303,10 +303,13 @@ def lib():
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
         L.vvcg_ctu_search_pruned_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, u32, u32, C.c_float, vp]
+        L.vvcg_ctu_search_costs_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, vp]
         L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
         L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, u32, vp, vp, vp, vp, vp]
         L.vvcg_cnn_train_step_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, vp, u32, vp, vp, vp, u32, C.c_float,
                                               vp, vp, vp]
+        L.vvcg_cnn_train_step_soft_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, vp, vp, u32, vp, vp, vp, u32,
+                                                   C.c_float, vp, vp, vp]
         L.vvcg_gen_intra_predict_dev.argtypes = [vp, vp, vp, u32, vp, u64]
         L.vvcg_gen_intra_recon_dev.argtypes = [vp, vp, vp, u32, vp, u32, vp, vp, u64]
         L.vvcg_deblock_general_dev.argtypes = [vp, vp, vp, u32, u32, u8, u32, vp, u32, u32, vp, u32, u32, vp]
@@ -820,10 +823,11 @@ class Context:
         return logits, gap, acts
 
     def cnn_train_step(self, plane, bit_depth, qp, xy, labels, params, adam_m=None, adam_v=None, step=0, lr=0.0,
-                       sync=True):
+                       sync=True, soft=None):
         """One training step on the blocks xy ((n, 2) int32 CUDA) with labels
-        ((n, 2) uint8 CUDA: intra mode, split type). Updates params (and the
-        Adam moments) in place when lr > 0. Returns (loss, grads) CUDA
+        ((n, 2) uint8 CUDA: intra mode, split type), or with soft ((n, 67)
+        fp32 CUDA) the mode head's target distribution. Updates params (and
+        the Adam moments) in place when lr > 0. Returns (loss, grads) CUDA
         tensors (one fp32; CNN_PARAMS fp32)."""
         import torch
 
@@ -832,10 +836,17 @@ class Context:
         loss = torch.empty(1, dtype=torch.float32, device=dev)
         st = torch.zeros(1, dtype=torch.int32, device=dev)
         h, w = plane.shape
-        self._check(self._L.vvcg_cnn_train_step_dev(self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, qp,
-                                                    _ptr(xy.contiguous()), _ptr(labels.contiguous()), int(xy.shape[0]),
-                                                    _ptr(params), _ptr(adam_m), _ptr(adam_v), step, lr, _ptr(grads),
-                                                    _ptr(loss), _ptr(st)))
+        if soft is None:
+            self._check(self._L.vvcg_cnn_train_step_dev(
+                self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, qp, _ptr(xy.contiguous()),
+                _ptr(labels.contiguous()), int(xy.shape[0]), _ptr(params), _ptr(adam_m), _ptr(adam_v), step, lr,
+                _ptr(grads), _ptr(loss), _ptr(st)))
+        else:
+            soft = soft.contiguous()
+            self._check(self._L.vvcg_cnn_train_step_soft_dev(
+                self._h, _ptr(plane), plane.stride(0), w, h, bit_depth, qp, _ptr(xy.contiguous()),
+                _ptr(labels.contiguous()), _ptr(soft), int(xy.shape[0]), _ptr(params), _ptr(adam_m), _ptr(adam_v),
+                step, lr, _ptr(grads), _ptr(loss), _ptr(st)))
         if sync:
             torch.cuda.synchronize(dev)
             code = int(st.item())
@@ -882,6 +893,21 @@ class Context:
             return None
         torch.cuda.synchronize(src.device)
         return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:n]
+
+    def ctu_search_costs(self, src, bit_depth, lambda_q8, xy):
+        """The full CTU search over device positions xy with every luma mode's
+        cost of each unsplit 32x32 CU (vvcg_ctu_search_costs_dev): returns
+        (CTU_SEARCH_RES_DTYPE results, (n, 67) int64 CUDA tensor of costs)."""
+        import torch
+
+        n = int(xy.shape[0])
+        h, w = src.shape
+        dst = torch.empty(max(n, 1) * CTU_SEARCH_RES_DTYPE.itemsize, dtype=torch.uint8, device=src.device)
+        costs = torch.empty((max(n, 1), 67), dtype=torch.int32, device=src.device)
+        self._check(self._L.vvcg_ctu_search_costs_dev(self._h, _ptr(src), src.stride(0), w, h, bit_depth, lambda_q8,
+                                                      _ptr(xy.contiguous()), n, _ptr(dst), _ptr(costs)))
+        torch.cuda.synchronize(src.device)
+        return dst.cpu().numpy().view(CTU_SEARCH_RES_DTYPE)[:n], costs[:n].to(torch.int64)
 
     # -- general-decoder intra prediction --
     def gen_intra_predict(self, planes, dec_y, dec_c, bit_depth, ctu, reqs, out_count, vert_collocated=False):

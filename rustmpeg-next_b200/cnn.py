@@ -88,16 +88,18 @@ def reference_forward(blocks, bit_depth, params, qp):
     return logits, gap, acts
 
 
-def reference_loss_and_grads(blocks, labels, bit_depth, params, qp):
+def reference_loss_and_grads(blocks, labels, bit_depth, params, qp, soft=None):
     """Mean cross-entropy of both heads and its gradient w.r.t. the
     parameter vector, by autograd through reference_forward (fp32 with the
-    kernels' bf16 roundings)."""
+    kernels' bf16 roundings). `soft` (N x 67 rows summing to 1) replaces the
+    mode head's one-hot target."""
     import torch
 
     p = torch.tensor(np.asarray(params, np.float32), requires_grad=True)
     logits, _, _ = reference_forward(blocks, bit_depth, p, qp)
     lab = torch.as_tensor(np.asarray(labels), dtype=torch.long)
-    loss = torch.nn.functional.cross_entropy(logits[:, :MODES], lab[:, 0]) + \
+    mode_target = lab[:, 0] if soft is None else torch.as_tensor(np.asarray(soft, np.float32))
+    loss = torch.nn.functional.cross_entropy(logits[:, :MODES], mode_target) + \
         torch.nn.functional.cross_entropy(logits[:, MODES:], lab[:, 1])
     loss.backward()
     return float(loss.detach()), p.grad.numpy()
@@ -109,12 +111,15 @@ def search_lambda_q8(qp, bit_depth=10):
     return int(round(256.0 * np.sqrt(0.57 * 2.0 ** ((qp - 12) / 3.0)) * 2.0 ** (bit_depth - 8)))
 
 
-def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37), seed=0):
+def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37), seed=0, soft_t=None):
     """Labelled 32x32 luma blocks for the pruner: value-noise 10-bit frames
     (the 1080p synthetic content), every CTU labelled by the full search at
     each QP (intra mode of the unsplit CU, best split type). Returns a list
     of (plane (H, W) int16 CUDA, xy (n, 2) int32 CUDA, labels (n, 2) uint8
-    CUDA, qp) per frame and QP."""
+    CUDA, qp, soft) per frame and QP. With soft_t, soft ((n, 67) fp32 CUDA)
+    is each CTU's target over the 67 modes of the unsplit CU,
+    softmax(-(cost - best cost) / (soft_t * lambda)): modes within a few
+    lambda-weighted bits of the best share the probability; else None."""
     import torch
 
     from . import synth
@@ -123,20 +128,27 @@ def training_set(ctx, n_frames=8, width=1920, height=1080, qps=(22, 27, 32, 37),
     with ctx.torch_stream_scope():
         xs, ys = np.meshgrid(np.arange(0, width - 31, 32), np.arange(0, height - 31, 32))
         xy = torch.from_numpy(np.stack([xs.ravel(), ys.ravel()], 1).astype(np.int32)).cuda()
-        _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed)
+        _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed, soft_t)
     return out
 
 
-def _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed):
+def _label_frames(ctx, synth, xy, out, n_frames, width, height, qps, seed, soft_t):
     import torch
 
     for f in range(n_frames):
         y, _, _ = synth.value_noise_frame(width, height, 10, frame=seed * 1000 + f)
         plane = torch.from_numpy(np.ascontiguousarray(y.astype(np.uint16)).view(np.int16)).cuda()
         for qp in qps:
-            r = ctx.ctu_search_xy(plane, 10, search_lambda_q8(qp), xy)
+            lam = search_lambda_q8(qp)
+            soft = None
+            if soft_t is None:
+                r = ctx.ctu_search_xy(plane, 10, lam, xy)
+            else:
+                r, costs = ctx.ctu_search_costs(plane, 10, lam, xy)
+                rel = (costs - costs.min(dim=1, keepdim=True).values).to(torch.float32)
+                soft = torch.softmax(-rel / (soft_t * lam / 256.0), dim=1).contiguous()
             lab = torch.from_numpy(np.stack([r["cu_mode"], r["split"]], 1).astype(np.uint8)).cuda()
-            out.append((plane, xy, lab, qp))
+            out.append((plane, xy, lab, qp, soft))
 
 
 def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None, schedule="constant", lr_min=0.0):
@@ -151,11 +163,12 @@ def train(ctx, data, steps=300, batch=1024, lr=1e-3, seed=0, params=None, schedu
         m, v = torch.zeros_like(p), torch.zeros_like(p)
         losses = []
         for step in range(1, steps + 1):
-            plane, xy, lab, qp = data[int(rng.integers(0, len(data)))]
+            plane, xy, lab, qp, soft = data[int(rng.integers(0, len(data)))]
             idx = torch.from_numpy(rng.choice(xy.shape[0], min(batch, xy.shape[0]), replace=False)).cuda()
             lr_t = lr if schedule == "constant" else \
                 lr_min + (lr - lr_min) * 0.5 * (1.0 + np.cos(np.pi * (step - 1) / max(1, steps)))
-            loss, _ = ctx.cnn_train_step(plane, 10, qp, xy[idx], lab[idx], p, m, v, step, float(lr_t), sync=False)
+            loss, _ = ctx.cnn_train_step(plane, 10, qp, xy[idx], lab[idx], p, m, v, step, float(lr_t), sync=False,
+                                         soft=None if soft is None else soft[idx])
             losses.append(loss)
         torch.cuda.synchronize()
     return p, [float(x.item()) for x in losses]

@@ -288,6 +288,7 @@ struct CnnBwdArgs {
   const uint32_t* ctu_xy;
   const uint8_t* labels;  // n x (mode, split)
   const float* params;
+  const float* soft;       // optional n x kCnnModes target distribution of the mode head (else the label)
   const uint16_t* packT;  // flipped packed weights of layers 2..4
   const float* logits;
   const float* gap;
@@ -358,11 +359,19 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
       float se = 0.0f;
       for (int j = lane; j < n_out; j += 32) se += __expf(lg[base + j] - mx);
       for (int o = 16; o > 0; o >>= 1) se += __shfl_xor_sync(0xFFFFFFFFu, se, o);
+      // soft targets of the mode head: cross-entropy against the given
+      // distribution, the loss summed in a fixed order (shuffles of lanes)
+      const float* tg = (warp == 0 && A.soft) ? A.soft + (size_t)blk * kCnnModes : nullptr;
+      float ce = 0.0f;
       for (int j = lane; j < n_out; j += 32) {
         const float pj = __expf(lg[base + j] - mx) / se;
-        dlog[base + j] = (pj - (j == label ? 1.0f : 0.0f)) * A.inv_batch;
+        const float yj = tg ? tg[j] : (j == label ? 1.0f : 0.0f);
+        dlog[base + j] = (pj - yj) * A.inv_batch;
+        if (tg) ce += yj * (logf(se) + mx - lg[base + j]);
       }
-      if (lane == 0) dlog[kCnnOut + warp] = (logf(se) + mx - lg[base + label]) * A.inv_batch;
+      if (tg)
+        for (int o = 16; o > 0; o >>= 1) ce += __shfl_xor_sync(0xFFFFFFFFu, ce, o);
+      if (lane == 0) dlog[kCnnOut + warp] = (tg ? ce : (logf(se) + mx - lg[base + label])) * A.inv_batch;
     }
     __syncthreads();
     // the two heads' losses, added in a fixed order (training is deterministic)

@@ -406,6 +406,7 @@ struct CostArgs {
   const CostReq* reqs;
   uint32_t* block_cost;  // [ctu][15]
   uint8_t* block_mode;   // [ctu][15]
+  uint32_t* mode_costs;  // optional [ctu][67]: every mode's cost of the unsplit CU (slot 0, full set)
 };
 
 // 8x8 Hadamard SATD of a w x h residual block (w, h multiples of 8) in the
@@ -504,6 +505,8 @@ __global__ void __launch_bounds__(kIsrWarps * 32) k_cost_search(const __grid_con
       A.block_cost[(size_t)R.ctu * 15 + R.slot] = best;
       A.block_mode[(size_t)R.ctu * 15 + R.slot] = (uint8_t)bm;
     }
+    if (A.mode_costs && R.slot == 0 && R.n_cand == 0)
+      for (int c = t; c < 67; c += blockDim.x) A.mode_costs[(size_t)R.ctu * 67 + c] = S.cost[c];
     __syncthreads();
   }
 }

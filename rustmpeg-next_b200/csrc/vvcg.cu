@@ -1634,11 +1634,34 @@ extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, u
 // ---------------------------------------------------------------------------
 // CTU search from device positions, full or CNN-pruned (vvcg_ctu_search_pruned_dev).
 // ---------------------------------------------------------------------------
+static vvcg_status ctu_search_xy(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                 uint32_t height, uint8_t bit_depth, uint32_t lambda_q8, const uint32_t* ctu_xy,
+                                 uint32_t num_ctus, const float* logits, uint32_t top_modes, uint32_t top_splits,
+                                 float threshold, vvcg_ctu_search_res* res, uint32_t* mode_costs);
+
 extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride,
                                                   uint32_t width, uint32_t height, uint8_t bit_depth,
                                                   uint32_t lambda_q8, const uint32_t* ctu_xy, uint32_t num_ctus,
                                                   const float* logits, uint32_t top_modes, uint32_t top_splits,
                                                   float threshold, vvcg_ctu_search_res* res) {
+  return ctu_search_xy(ctx, src, stride, width, height, bit_depth, lambda_q8, ctu_xy, num_ctus, logits, top_modes,
+                       top_splits, threshold, res, nullptr);
+}
+
+extern "C" vvcg_status vvcg_ctu_search_costs_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                                 uint32_t height, uint8_t bit_depth, uint32_t lambda_q8,
+                                                 const uint32_t* ctu_xy, uint32_t num_ctus, vvcg_ctu_search_res* res,
+                                                 uint32_t* mode_costs) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (num_ctus && !mode_costs) return fail(ctx, VVCG_INVALID_INPUT, "missing mode costs");
+  return ctu_search_xy(ctx, src, stride, width, height, bit_depth, lambda_q8, ctu_xy, num_ctus, nullptr, 6, 2, 0.0f,
+                       res, mode_costs);
+}
+
+static vvcg_status ctu_search_xy(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                 uint32_t height, uint8_t bit_depth, uint32_t lambda_q8, const uint32_t* ctu_xy,
+                                 uint32_t num_ctus, const float* logits, uint32_t top_modes, uint32_t top_splits,
+                                 float threshold, vvcg_ctu_search_res* res, uint32_t* mode_costs) {
   if (!ctx) return VVCG_INVALID_INPUT;
   if (!num_ctus) return VVCG_OK;
   if (!src || !ctu_xy || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, positions or results");
@@ -1659,7 +1682,7 @@ extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t*
   CK(cudaGetLastError(), "prune launch");
   CostArgs A{src, (int64_t)stride, (int32_t)width, (int32_t)height, bit_depth, (int32_t)nb, lambda_q8,
              (const CostReq*)ctx->d_search_reqs.p, (uint32_t*)ctx->d_search_cost.p,
-             (uint8_t*)ctx->d_search_mode.p};
+             (uint8_t*)ctx->d_search_mode.p, mode_costs};
   k_cost_search<<<(uint32_t)std::min<size_t>(nb, (size_t)ctx->num_sms * 8), kIsrWarps * 32, 0, ctx->stream>>>(A);
   CK(cudaGetLastError(), "search launch");
   k_ctu_search_combine<<<(num_ctus + 127) / 128, 128, 0, ctx->stream>>>(
@@ -1719,11 +1742,38 @@ extern "C" vvcg_status vvcg_cnn_forward_dev(vvcg_ctx* ctx, const uint16_t* plane
 // ---------------------------------------------------------------------------
 // CNN pruner training step (vvcg_cnn_train_step_dev).
 // ---------------------------------------------------------------------------
+static vvcg_status cnn_train_step(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                  uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
+                                  const uint8_t* labels, const float* soft, uint32_t num_blocks, float* params,
+                                  float* adam_m, float* adam_v, uint32_t step, float lr, float* grads, float* loss,
+                                  uint32_t* status);
+
 extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride,
                                                uint32_t width, uint32_t height, uint8_t bit_depth, uint8_t qp,
                                                const uint32_t* ctu_xy, const uint8_t* labels, uint32_t num_blocks,
                                                float* params, float* adam_m, float* adam_v, uint32_t step, float lr,
                                                float* grads, float* loss, uint32_t* status) {
+  return cnn_train_step(ctx, plane, stride, width, height, bit_depth, qp, ctu_xy, labels, nullptr, num_blocks, params,
+                        adam_m, adam_v, step, lr, grads, loss, status);
+}
+
+extern "C" vvcg_status vvcg_cnn_train_step_soft_dev(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride,
+                                                    uint32_t width, uint32_t height, uint8_t bit_depth, uint8_t qp,
+                                                    const uint32_t* ctu_xy, const uint8_t* labels,
+                                                    const float* soft_modes, uint32_t num_blocks, float* params,
+                                                    float* adam_m, float* adam_v, uint32_t step, float lr,
+                                                    float* grads, float* loss, uint32_t* status) {
+  if (!ctx) return VVCG_INVALID_INPUT;
+  if (num_blocks && !soft_modes) return fail(ctx, VVCG_INVALID_INPUT, "missing mode targets");
+  return cnn_train_step(ctx, plane, stride, width, height, bit_depth, qp, ctu_xy, labels, soft_modes, num_blocks,
+                        params, adam_m, adam_v, step, lr, grads, loss, status);
+}
+
+static vvcg_status cnn_train_step(vvcg_ctx* ctx, const uint16_t* plane, uint64_t stride, uint32_t width,
+                                  uint32_t height, uint8_t bit_depth, uint8_t qp, const uint32_t* ctu_xy,
+                                  const uint8_t* labels, const float* soft, uint32_t num_blocks, float* params,
+                                  float* adam_m, float* adam_v, uint32_t step, float lr, float* grads, float* loss,
+                                  uint32_t* status) {
   if (!ctx) return VVCG_INVALID_INPUT;
   if (!num_blocks) return VVCG_OK;
   if (!plane || !ctu_xy || !labels || !params || !grads || !loss || !status)
@@ -1757,7 +1807,8 @@ extern "C" vvcg_status vvcg_cnn_train_step_dev(vvcg_ctx* ctx, const uint16_t* pl
   k_cnn_forward<<<grid, kCnnThreads, kCnnSmem, ctx->stream>>>(F);
   CK(cudaGetLastError(), "cnn forward launch");
   CnnBwdArgs B{plane, (int64_t)stride, (int32_t)width, (int32_t)height, (1 << bit_depth) - 1, (int32_t)num_blocks,
-               cnn_qp_input(qp), ctu_xy, labels, params, (const uint16_t*)ctx->d_cnn_packT.p, (const float*)ctx->d_cnn_logits.p,
+               cnn_qp_input(qp), ctu_xy, labels, params, soft, (const uint16_t*)ctx->d_cnn_packT.p,
+               (const float*)ctx->d_cnn_logits.p,
                (const float*)ctx->d_cnn_gap.p, (const uint16_t*)ctx->d_cnn_acts.p, (float*)ctx->d_cnn_partial.p,
                1.0f / (float)num_blocks, status};
   k_cnn_backward<<<grid, kCnnThreads, kCnnBwdSmem, ctx->stream>>>(B);

@@ -78,6 +78,41 @@ def test_cnn_gradients_match_autograd(ctx, pkg, n, seed):
     assert torch.equal(p.cpu(), torch.from_numpy(params))
 
 
+@pytest.mark.parametrize("n,seed", [(5, 3), (150, 4)])
+def test_cnn_soft_target_gradients_match_autograd(ctx, pkg, n, seed):
+    """The mode head trained against a distribution over the 67 modes (the
+    softmax of negated search costs): loss and gradients against autograd."""
+    import torch
+    from rustmpeg_next_b200 import cnn
+
+    plane, xy, blocks = _blocks(n, 10, seed)
+    rng = np.random.default_rng(seed)
+    labels = np.stack([rng.integers(0, 67, n), rng.integers(0, 6, n)], axis=1).astype(np.uint8)
+    z = rng.normal(0.0, 2.0, (n, 67))
+    soft = (np.exp(z - z.max(1, keepdims=True)) / np.exp(z - z.max(1, keepdims=True)).sum(1, keepdims=True))
+    soft = soft.astype(np.float32)
+    params = cnn.init_params(seed)
+    p = torch.from_numpy(params).cuda()
+    loss, grads = ctx.cnn_train_step(plane, 10, 27, xy, torch.from_numpy(labels).cuda(), p,
+                                     soft=torch.from_numpy(soft).cuda())
+    ref_loss, ref = cnn.reference_loss_and_grads(blocks, labels, 10, params, 27, soft=soft)
+    assert abs(float(loss.item()) - ref_loss) <= 1e-3 * max(1.0, abs(ref_loss))
+    g = grads.cpu().numpy()
+    for name, off, cnt in [("w1", cnn.OFF_W1, 576), ("wi", cnn.OFF_WI, 67 * 32), ("bi", cnn.OFF_BI, 67),
+                           ("ws", cnn.OFF_WS, 192), ("w4", cnn.off_w(4), 9216)]:
+        a, b = g[off:off + cnt], ref[off:off + cnt]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert rel < 3e-2, (name, rel)
+    # a one-hot soft target is the hard label
+    onehot = np.zeros((n, 67), np.float32)
+    onehot[np.arange(n), labels[:, 0]] = 1.0
+    l1, g1 = ctx.cnn_train_step(plane, 10, 27, xy, torch.from_numpy(labels).cuda(), p,
+                                soft=torch.from_numpy(onehot).cuda())
+    l0, g0 = ctx.cnn_train_step(plane, 10, 27, xy, torch.from_numpy(labels).cuda(), p)
+    assert abs(float(l1.item()) - float(l0.item())) <= 1e-5 * max(1.0, abs(float(l0.item())))
+    assert torch.allclose(g1, g0, rtol=1e-4, atol=1e-7)
+
+
 def test_cnn_adam_steps_reduce_the_loss(ctx, pkg):
     import torch
     from rustmpeg_next_b200 import cnn

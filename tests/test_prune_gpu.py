@@ -94,3 +94,24 @@ def test_trained_pruner_stays_close_to_full_search(ctx, pkg):
     inc_t = forced_t["cost"].astype(np.float64).sum() / total - 1.0
     inc_u = forced_u["cost"].astype(np.float64).sum() / total - 1.0
     assert inc_t < 0.8 * inc_u, (inc_t, inc_u)
+
+
+def test_mode_costs_of_the_unsplit_cu(ctx, pkg, orc):
+    """vvcg_ctu_search_costs_dev: the same results as the full search, every
+    mode's cost of the unsplit CU equal to the oracle's search restricted to
+    that one mode, and the minimum over the 67 costs is the unsplit cost."""
+    y, plane = _plane(192, 128, 5)
+    a, xy = _xy(192, 128)
+    want = ctx.ctu_search_xy(plane, 10, 280, xy)
+    got, costs = ctx.ctu_search_costs(plane, 10, 280, xy)
+    assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+    c = costs.cpu().numpy()
+    assert c.shape == (len(a), 67)
+    # the unsplit cost adds the split flag's one bit at lambda to the best mode's
+    assert np.array_equal(c.min(1) + (280 * 1 >> 8), got["split_cost"][:, 0].astype(np.int64))
+    assert np.array_equal(c.argmin(1), got["cu_mode"])
+    rng = np.random.default_rng(5)
+    for k in rng.choice(len(a), 4, replace=False):
+        for m in (0, 1, int(rng.integers(2, 67)), int(c[k].argmin())):
+            r = orc.ctu_search(y, 10, int(a[k, 0]), int(a[k, 1]), 280, split_mask=1, cand=(m,))
+            assert r["split_cost"][0] == c[k, m] + (280 >> 8), (k, m)
