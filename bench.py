@@ -379,9 +379,9 @@ def main():
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--train-lr", type=float, default=1e-3)
     ap.add_argument("--train-schedule", default="constant", choices=["constant", "cosine"])
-    ap.add_argument("--soft-labels", type=float, default=None,
-                    help="train the mode head on softmax(-(cost - best) / (T * lambda)) of the full search's "
-                         "67 mode costs instead of its best mode")
+    ap.add_argument("--soft-labels", type=float, default=2.0,
+                    help="T: train the mode head on softmax(-(cost - best) / (T * lambda)) of the full search's "
+                         "67 mode costs; 0 trains on its best mode alone")
     ap.add_argument("--eval-frames", type=int, default=8, help="held-out 1080p frames per QP for the encoder")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -658,8 +658,10 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
     top modes and split types of the pruner's softmax; a head keeps its full
     set when those hold less than the threshold of its probability mass),
     with the pruner trained here on full-search labels (Adam, lr 1e-3, batch
-    1024) from frames other than the evaluated ones. Pruned times include the
-    CNN forward pass."""
+    1024) from frames other than the evaluated ones: the best split type, and
+    for the mode head a softmax over the 67 modes' costs of the unsplit CU, so
+    that a near-tie costs little to miss. Pruned times include the CNN forward
+    pass."""
     import torch
 
     from rustmpeg_next_b200 import cnn
@@ -674,7 +676,8 @@ def bench_encoder(pkg, ctx, stream, dev, args, peaks):
         return e0.elapsed_time(e1)
 
     t0 = time.perf_counter()
-    data = cnn.training_set(ctx, n_frames=args.train_frames, qps=QPS, seed=11, soft_t=args.soft_labels)
+    data = cnn.training_set(ctx, n_frames=args.train_frames, qps=QPS, seed=11,
+                            soft_t=args.soft_labels if args.soft_labels > 0 else None)
     label_s = time.perf_counter() - t0
     n_train = sum(int(d[1].shape[0]) for d in data)
     cnn.train(ctx, data, steps=2, batch=1024, lr=1e-3, seed=11)  # warm-up (fresh parameters below)
