@@ -78,8 +78,10 @@ struct CnnFwdArgs {
 };
 
 // Issues the 144 MMAs of one 3x3 32->32 layer reading image `xin` with the
-// packed weights `w` into TMEM columns tile * 32, then commits to mbar.
-__device__ __forceinline__ void cnn_issue_layer(uint32_t tmem, uint32_t xin, uint32_t w, uint64_t* mbar) {
+// packed weights `w` into TMEM columns tile * 32, then (with commit) commits
+// to mbar.
+__device__ __forceinline__ void cnn_issue_layer(uint32_t tmem, uint32_t xin, uint32_t w, uint64_t* mbar,
+                                                bool commit = true) {
   for (int tile = 0; tile < 8; tile++) {
     const int xg = tile & 3, yh = tile >> 2;
     for (int tap = 0; tap < 9; tap++) {
@@ -92,7 +94,7 @@ __device__ __forceinline__ void cnn_issue_layer(uint32_t tmem, uint32_t xin, uin
       }
     }
   }
-  umma_commit(mbar);
+  if (commit) umma_commit(mbar);
 }
 
 __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_forward(const __grid_constant__ CnnFwdArgs A) {
@@ -271,10 +273,10 @@ namespace vvcg {
 //  * its input gradient dA_{l-1} = conv(dZ_l, flipped W_l) is 144 tcgen05
 //    MMAs exactly as in the forward pass (the taps of the transposed
 //    convolution are the mirrored address offsets);
-//  * meanwhile the CUDA cores form the weight gradient
-//    dW_l[co][ci][tap] = sum_p dZ_l[p][co] a_{l-1}[p + tap][ci] (the 32
-//    channels of one tap are too few rows for a tensor-core operand) and
-//    the bias gradient;
+//  * behind them, the weight gradient
+//    dW_l[co][ci][tap] = sum_p dZ_l[p][co] a_{l-1}[p + tap][ci] is 576 more
+//    MMAs (cnn_issue_dw): the 1024 pixels are the K dimension and both
+//    images are MN-major operands as they lie;
 //  * the epilogue masks dA_{l-1} by a_{l-1} > 0 into dZ_{l-1}, in place of
 //    a_{l-1}.
 // Layer 1's weight gradient uses the bf16 input. Gradients and the loss
@@ -297,16 +299,55 @@ struct CnnBwdArgs {
   float inv_batch;
   uint32_t* status;
 };
-constexpr int kCnnBwdMisc = (1024 + 32 + 32 * 8 + 96) * 4;
+constexpr int kXPad = 34 * 34;  // the input zero-padded by one pixel
+constexpr int kCnnBwdMisc = (2 * kXPad + 32 + 32 * 8 + 96) * 4;
+// M = 64, N = 32, both operands MN-major
+constexpr uint32_t kCnnIdescW = umma_idesc_bf16(64, 32) | (1u << 15) | (1u << 16);
+constexpr int kCnnBwdCols = 512;  // dA_{l-1}: columns 0..255; dW_l: 256..415
+
+// Issues the weight-gradient MMAs of one 3x3 32->32 layer and returns
+// without committing. Per tap t, D_t (M = 64, N = 32) += L * H_t^T over the
+// 1024 pixels, 16 of one image row per MMA (K), with L the image at `lo`
+// and H the one at `hi`: as MN-major operands without swizzle a core matrix
+// is 8 pixels (K, 16 B apart) x 8 channels (16 B), LBO = 128 B steps the
+// next 8 pixels and SBO = one channel plane the next 8 channels. Only L's
+// 32 channels are rows of interest: rows 32..63 read the 4 planes that
+// follow L, which must be the other image (lo is the lower of the two
+// buffers), and are never read back. The tap's pixel offset applies to the
+// activation image: to L when lo_tap, else to H. D_t sits in the TMEM lanes
+// 16 (t & 1) + {0..15, 32..47} of columns (t >> 1) * 32 + 0..31 (two M = 64
+// accumulators share columns in the two half sub-partitions).
+__device__ __forceinline__ void cnn_issue_dw(uint32_t tmem, uint32_t lo, uint32_t hi, bool lo_tap) {
+  // the start address is the descriptor's low field in 16-byte units (one
+  // pixel): every operand is a base descriptor plus a pixel offset
+  const uint64_t da0 = umma_desc(lo, 128, kPlane), db0 = umma_desc(hi, 128, kPlane);
+  for (int y = 0; y < 32; y++)
+    for (int h = 0; h < 2; h++) {
+      const int base = (y + 1) * kImgW + 1 + 16 * h;
+#pragma unroll
+      for (int tap = 0; tap < 9; tap++) {
+        const int sh = (tap / 3 - 1) * kImgW + tap % 3 - 1;
+        umma_bf16(tmem + ((uint32_t)(16 * (tap & 1)) << 16) + (tap >> 1) * 32,
+                  da0 + (uint64_t)(base + (lo_tap ? sh : 0)), db0 + (uint64_t)(base + (lo_tap ? 0 : sh)),
+                  kCnnIdescW, (y | h) != 0);
+      }
+    }
+}
 constexpr int kCnnBwdSmem = 2 * kImg + kPackL + kCnnBwdMisc + 64;
 
 // Loads activation image `layer` (0..3) of block blk from global into an
 // image buffer (interior only; the halo stays zero).
 __device__ __forceinline__ void cnn_load_act(uint8_t* img, const uint16_t* acts, int blk, int layer) {
   const uint4* src = (const uint4*)(acts + ((size_t)blk * 4 + layer) * 1024 * 32);
-  for (int i = threadIdx.x; i < 1024 * 4; i += kCnnThreads) {
-    const int p = i >> 2, g = i & 3;
-    *(uint4*)(img + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = src[i];
+  for (int i0 = threadIdx.x; i0 < 1024 * 4; i0 += 4 * kCnnThreads) {
+    uint4 v[4];  // four loads in flight before the stores
+#pragma unroll
+    for (int k = 0; k < 4; k++) v[k] = src[i0 + k * kCnnThreads];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int i = i0 + k * kCnnThreads, p = i >> 2, g = i & 3;
+      *(uint4*)(img + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = v[k];
+    }
   }
 }
 
@@ -315,8 +356,9 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
   uint8_t* P = smem;
   uint8_t* Q = smem + kImg;
   uint8_t* Wt = smem + 2 * kImg;
-  float* xin = (float*)(Wt + kPackL);  // bf16-rounded normalised input
-  float* dgap = xin + 1024;
+  // (bf16-rounded normalised input, 1) inside the block, (0, 0) in the halo
+  float2* xpad = (float2*)(Wt + kPackL);
+  float* dgap = (float*)(xpad + kXPad);
   float* dbp = dgap + 32;   // [8 warps][32] bias-gradient partials
   float* dlog = dbp + 256;  // [73] logit gradients (+ pad)
   uint64_t* mbar = (uint64_t*)(dlog + 96);
@@ -325,8 +367,9 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
   float* part = A.partial + (size_t)blockIdx.x * (kCnnParams + 1);
   for (int i = t; i < kCnnParams + 1; i += kCnnThreads) part[i] = 0.0f;
   for (int i = t; i < 2 * kImg / 16; i += kCnnThreads) ((uint4*)P)[i] = make_uint4(0, 0, 0, 0);
+  for (int i = t; i < kXPad; i += kCnnThreads) xpad[i] = make_float2(0.0f, 0.0f);
   if (warp == 0) {
-    tmem_alloc(tslot, 256);
+    tmem_alloc(tslot, kCnnBwdCols);
     tmem_relinquish();
   }
   if (t == 0) {
@@ -339,7 +382,6 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
   const uint32_t tmem = *tslot;
   uint32_t phase = 0;
   bool ok = true;
-  const int co4 = t >> 5, ci = t & 31;  // weight-gradient ownership: 4 output channels x 1 input channel
 
   for (int blk = blockIdx.x; blk < A.n && ok; blk += gridDim.x) {
     const uint32_t ux = A.ctu_xy[2 * blk], uy = A.ctu_xy[2 * blk + 1];
@@ -378,8 +420,19 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
     if (t == 0) part[kCnnParams] += dlog[kCnnOut] + dlog[kCnnOut + 1];
     const float inv = 1.0f / (float)A.maxv;
     const int bx = (int)ux, by = (int)uy;
-    for (int i = t; i < 1024; i += kCnnThreads)
-      xin[i] = bf2f(f2bf((float)A.plane[(int64_t)(by + (i >> 5)) * A.stride + bx + (i & 31)] * inv));
+    {
+      uint16_t pv[1024 / kCnnThreads];  // the loads first, then the stores
+#pragma unroll
+      for (int u = 0; u < 1024 / kCnnThreads; u++) {
+        const int i = t + u * kCnnThreads;
+        pv[u] = A.plane[(int64_t)(by + (i >> 5)) * A.stride + bx + (i & 31)];
+      }
+#pragma unroll
+      for (int u = 0; u < 1024 / kCnnThreads; u++) {
+        const int i = t + u * kCnnThreads;
+        xpad[((i >> 5) + 1) * 34 + (i & 31) + 1] = make_float2(bf2f(f2bf((float)pv[u] * inv)), 1.0f);
+      }
+    }
     __syncthreads();
     const float* gp = A.gap + (size_t)blk * 32;
     if (t < 32) {
@@ -388,9 +441,19 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
       for (int j = 0; j < kCnnSplits; j++) s = fmaf(A.params[kOffWs + j * 32 + t], dlog[kCnnModes + j], s);
       dgap[t] = s;
     }
-    for (int i = t; i < kCnnOut * 32; i += kCnnThreads) {
-      const int j = i >> 5, c = i & 31;
-      part[(j < kCnnModes ? kOffWi : kOffWs - kCnnModes * 32) + i] += dlog[j] * gp[c];
+    {
+      constexpr int kR = (kCnnOut * 32 + kCnnThreads - 1) / kCnnThreads;
+      float o[kR];  // the loads first, then the stores
+#pragma unroll
+      for (int k = 0; k < kR; k++) {
+        const int i = t + k * kCnnThreads;
+        if (i < kCnnOut * 32) o[k] = part[((i >> 5) < kCnnModes ? kOffWi : kOffWs - kCnnModes * 32) + i];
+      }
+#pragma unroll
+      for (int k = 0; k < kR; k++) {
+        const int i = t + k * kCnnThreads, j = i >> 5;
+        if (i < kCnnOut * 32) part[(j < kCnnModes ? kOffWi : kOffWs - kCnnModes * 32) + i] = o[k] + dlog[j] * gp[i & 31];
+      }
     }
     if (t < kCnnOut) part[t < kCnnModes ? kOffBi + t : kOffBs + t - kCnnModes] += dlog[t];
     __syncthreads();
@@ -399,19 +462,26 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
       const uint4* a4 = (const uint4*)(A.acts + ((size_t)blk * 4 + 3) * 1024 * 32);
       float dbs[8];
       for (int k = 0; k < 8; k++) dbs[k] = 0.0f;
-      for (int i = t; i < 1024 * 4; i += kCnnThreads) {
-        const int p = i >> 2, g = i & 3;  // g is fixed per thread (stride 256)
-        const uint4 av = a4[i];
-        const uint32_t aw[4] = {av.x, av.y, av.z, av.w};
-        uint32_t o[4];
-        for (int k = 0; k < 4; k++) {
-          const float d0 = (aw[k] & 0xFFFFu) && !(aw[k] & 0x8000u) ? dgap[g * 8 + 2 * k] * (1.0f / 1024.0f) : 0.0f;
-          const float d1 = (aw[k] >> 16) && !(aw[k] & 0x80000000u) ? dgap[g * 8 + 2 * k + 1] * (1.0f / 1024.0f) : 0.0f;
-          dbs[2 * k] += d0;
-          dbs[2 * k + 1] += d1;
-          o[k] = (uint32_t)f2bf(d0) | ((uint32_t)f2bf(d1) << 16);
+      for (int i0 = t; i0 < 1024 * 4; i0 += 8 * kCnnThreads) {
+        uint4 avs[8];  // eight loads in flight
+#pragma unroll
+        for (int u = 0; u < 8; u++) avs[u] = a4[i0 + u * kCnnThreads];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const int i = i0 + u * kCnnThreads, p = i >> 2, g = i & 3;  // g is fixed per thread (stride 256)
+          const uint32_t aw[4] = {avs[u].x, avs[u].y, avs[u].z, avs[u].w};
+          uint32_t o[4];
+          for (int k = 0; k < 4; k++) {
+            const float d0 = (aw[k] & 0xFFFFu) && !(aw[k] & 0x8000u) ? dgap[g * 8 + 2 * k] * (1.0f / 1024.0f) : 0.0f;
+            const float d1 =
+                (aw[k] >> 16) && !(aw[k] & 0x80000000u) ? dgap[g * 8 + 2 * k + 1] * (1.0f / 1024.0f) : 0.0f;
+            dbs[2 * k] += d0;
+            dbs[2 * k + 1] += d1;
+            o[k] = (uint32_t)f2bf(d0) | ((uint32_t)f2bf(d1) << 16);
+          }
+          *(uint4*)(P + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) =
+              make_uint4(o[0], o[1], o[2], o[3]);
         }
-        *(uint4*)(P + g * kPlane + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16) = make_uint4(o[0], o[1], o[2], o[3]);
       }
       // the 64 threads with the same g hold that plane's sums: reduced over
       // the warp's lanes of equal g, then over the warps in a fixed order
@@ -432,46 +502,55 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
     uint8_t* act = Q; // a_{l-1}, becomes dZ_{l-1}
     for (int layer = 4; layer >= 2 && ok; layer--) {
       const int li = layer - 2;
-      for (int i = t; i < kPackL / 16; i += kCnnThreads)
-        ((uint4*)Wt)[i] = ((const uint4*)(A.packT + (size_t)li * (kPackL / 2)))[i];
+      {
+        constexpr int kN = kPackL / 16, kU = (kN + kCnnThreads - 1) / kCnnThreads;
+        const uint4* src = (const uint4*)(A.packT + (size_t)li * (kPackL / 2));
+        uint4 wv[kU];  // the loads first, then the stores
+#pragma unroll
+        for (int u = 0; u < kU; u++)
+          if (t + u * kCnnThreads < kN) wv[u] = src[t + u * kCnnThreads];
+#pragma unroll
+        for (int u = 0; u < kU; u++)
+          if (t + u * kCnnThreads < kN) ((uint4*)Wt)[t + u * kCnnThreads] = wv[u];
+      }
       fence_async_smem();
       tc_fence_before();
       __syncthreads();
       tc_fence_after();
-      if (t == 0) cnn_issue_layer(tmem, smem_u32(dz), smem_u32(Wt), mbar);
-      // weight gradient on the CUDA cores while the tensor cores run
-      {
-        float acc[4][9];
-        for (int k = 0; k < 4; k++)
-          for (int tp = 0; tp < 9; tp++) acc[k][tp] = 0.0f;
-        const uint8_t* ap = act + (ci >> 3) * kPlane + (ci & 7) * 2;
-        const uint8_t* zp = dz + (co4 >> 1) * kPlane + (co4 & 1) * 8;
-        for (int iy = 0; iy < 32; iy++) {
-          float w[3][3];
-          for (int dy = 0; dy < 3; dy++)
-            for (int dx = 0; dx < 2; dx++) w[dy][dx + 1] = bf2f(*(const uint16_t*)(ap + ((iy + dy) * kImgW + dx) * 16));
-          for (int ix = 0; ix < 32; ix++) {
-            for (int dy = 0; dy < 3; dy++) {
-              w[dy][0] = w[dy][1];
-              w[dy][1] = w[dy][2];
-              w[dy][2] = bf2f(*(const uint16_t*)(ap + ((iy + dy) * kImgW + ix + 2) * 16));
-            }
-            const uint2 zv = *(const uint2*)(zp + ((iy + 1) * kImgW + ix + 1) * 16);
-            const float z[4] = {bf2f(zv.x & 0xFFFFu), bf2f(zv.x >> 16), bf2f(zv.y & 0xFFFFu), bf2f(zv.y >> 16)};
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-#pragma unroll
-              for (int tp = 0; tp < 9; tp++) acc[k][tp] = fmaf(z[k], w[tp / 3][tp % 3], acc[k][tp]);
-          }
-        }
-        float* gw = part + cnn_off_w(layer);
-        for (int k = 0; k < 4; k++)
-          for (int tp = 0; tp < 9; tp++) gw[((co4 * 4 + k) * kCnnCh + ci) * 9 + tp] += acc[k][tp];
+      if (t == 0) {
+        cnn_issue_layer(tmem, smem_u32(dz), smem_u32(Wt), mbar, false);
+        cnn_issue_dw(tmem + 256, smem_u32(P), smem_u32(Q), act == P);
+        umma_commit(mbar);
       }
       ok = __syncthreads_and(mbar_wait(mbar, phase, 1u << 26));
       phase ^= 1;
       tc_fence_after();
       if (!ok) break;
+      // weight gradient out of TMEM: warps of lane quarters 0 and 1 hold
+      // rows 0..31 (the channels of the image at P); a thread takes tap
+      // 2g + lane / 16 of row 16 q + lane % 16 and its 32 columns (the other
+      // image's channels)
+      if ((warp & 3) < 2) {
+        float* gw = part + cnn_off_w(layer);
+        const bool rows_co = dz == P;
+        const int r = 16 * (warp & 3) + (lane & 15);
+        for (int g = warp < 4 ? 0 : 3; g < (warp < 4 ? 3 : 5); g++) {
+          const int tp = 2 * g + (lane >> 4);
+          const uint32_t ta = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + 256 + g * 32;
+          float v[32];
+          tmem_ld16(ta, v);
+          tmem_ld16(ta + 16, v + 16);
+          if (tp < 9) {  // the 32 loads first, then the 32 stores (one round trip, not 32)
+            float* g0 = gw + (rows_co ? r * kCnnCh * 9 : r * 9) + tp;
+            const int st = rows_co ? 9 : kCnnCh * 9;
+            float o[32];
+#pragma unroll
+            for (int n = 0; n < 32; n++) o[n] = g0[n * st];
+#pragma unroll
+            for (int n = 0; n < 32; n++) g0[n * st] = o[n] + v[n];
+          }
+        }
+      }
       // epilogue: dZ_{l-1} = dA_{l-1} where a_{l-1} > 0, in place of a_{l-1}
       float dbs[32];
       for (int c = 0; c < 32; c++) dbs[c] = 0.0f;
@@ -518,27 +597,56 @@ __global__ void __launch_bounds__(kCnnThreads, 1) k_cnn_backward(const __grid_co
       __syncthreads();
     }
     if (!ok) break;
-    // layer 1: dW1[co][input][tap] = sum_p dZ1[p][co] in[p + tap] (dZ1 is in dz)
-    for (int o = t; o < 288; o += kCnnThreads) {
-      const int co = o / 9, tp = o % 9, dy = tp / 3 - 1, dx = tp % 3 - 1;
-      const uint8_t* zp = dz + (co >> 3) * kPlane + (co & 7) * 2;
-      float s = 0.0f, sq = 0.0f;
-      for (int p = 0; p < 1024; p++) {
-        const int y = (p >> 5) + dy, x = (p & 31) + dx;
-        if (y < 0 || y >= 32 || x < 0 || x >= 32) continue;
-        const float z = bf2f(*(const uint16_t*)(zp + (((p >> 5) + 1) * kImgW + (p & 31) + 1) * 16));
-        s = fmaf(z, xin[y * 32 + x], s);
-        sq += z;
+    // layer 1: dW1[co][input][tap] = sum_p dZ1[p][co] in[p + tap] (dZ1 is in
+    // dz; the second input is the constant QP plane, zero in the halo). Warp
+    // w takes rows 4w..4w+3 and lane the output channel, over a sliding 3x3
+    // window of (input, inside) pairs; the 8 row groups' sums meet in the
+    // weight buffer (free until the next block) and are added in a fixed order.
+    {
+      const uint8_t* zp = dz + (lane >> 3) * kPlane + (lane & 7) * 2;
+      float sx[9], sq[9];
+#pragma unroll
+      for (int k = 0; k < 9; k++) sx[k] = sq[k] = 0.0f;
+      for (int y = 4 * warp; y < 4 * warp + 4; y++) {
+        float2 w[3][3];
+#pragma unroll
+        for (int dy = 0; dy < 3; dy++)
+#pragma unroll
+          for (int dx = 0; dx < 2; dx++) w[dy][dx + 1] = xpad[(y + dy) * 34 + dx];
+        for (int x = 0; x < 32; x++) {
+#pragma unroll
+          for (int dy = 0; dy < 3; dy++) {
+            w[dy][0] = w[dy][1];
+            w[dy][1] = w[dy][2];
+            w[dy][2] = xpad[(y + dy) * 34 + x + 2];
+          }
+          const float z = bf2f(*(const uint16_t*)(zp + ((y + 1) * kImgW + x + 1) * 16));
+#pragma unroll
+          for (int k = 0; k < 9; k++) {
+            sx[k] = fmaf(z, w[k / 3][k % 3].x, sx[k]);
+            sq[k] = fmaf(z, w[k / 3][k % 3].y, sq[k]);
+          }
+        }
       }
-      part[kOffW1 + co * 18 + tp] += s;
-      part[kOffW1 + co * 18 + 9 + tp] += sq * A.qp_in;
+      float* red = (float*)Wt;  // [8 row groups][32 channels][18]
+#pragma unroll
+      for (int k = 0; k < 9; k++) {
+        red[(warp * 32 + lane) * 18 + k] = sx[k];
+        red[(warp * 32 + lane) * 18 + 9 + k] = sq[k];
+      }
+      __syncthreads();
+      for (int o = t; o < 32 * 18; o += kCnnThreads) {
+        float v = 0.0f;
+        for (int g = 0; g < 8; g++) v += red[g * 32 * 18 + o];
+        part[kOffW1 + o] += (o % 18) < 9 ? v : v * A.qp_in;
+      }
     }
     __syncthreads();
   }
   if (!ok && t == 0) atomicOr(A.status, 1u);
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, 256);
+  if (warp == 0) tmem_dealloc(tmem, kCnnBwdCols);
 }
 
 // grads[i] = sum over the CTA slices; loss[0] = sum of the loss slots.
