@@ -1346,8 +1346,7 @@ vvcg_status vvcg_plane_metrics_16_dev(vvcg_ctx* ctx, const uint16_t* ref, uint64
  * the stream has finished the picture.
  *
  * The first call on a device does the set-up (it loads the tables, finds the
- * array's address and sets the kernels' attributes); make that first call
- * before any stream capture begins. Every call copies the picture's header
+ * array's address and sets the kernels' attributes). Every call copies the picture's header
  * from host memory into the array, reads the status word back and waits for
  * `cuda_stream` before it returns. Every call shares the array and leaves the previous call's
  * contents in it; each call clears the parts that must start at zero. Calls
