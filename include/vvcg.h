@@ -1357,6 +1357,70 @@ vvcg_status vvcg_recon_picture_static(const vvcg_pic_desc* pic, const vvcg_cu_re
                                       uint64_t num_levels, const vvcg_plane_out* planes,
                                       void* cuda_stream, char* err, size_t err_cap);
 
+/* ---- Annex-B access units around the slice data -----------------------
+ *
+ * Host-side bitstream assembly of the reference encoder's default stream
+ * (8-bit 4:2:0, 32x32 CTUs; MTS, LFNST and transform skip enabled, every
+ * other tool off) and its reverse, so that slice data parsed by
+ * vvcg_parse_strict can come from, and go to, an H.266 Annex-B byte stream.
+ * No GPU is involved. */
+
+/* The stream configuration the parameter sets describe (replaces hls.rs
+ * VvcStreamConfig, crates/rustmpeg-video/src/vvc/hls.rs:94-107). */
+typedef struct vvcg_stream_cfg {
+  uint32_t width, height;            /* coded size in luma samples */
+  uint32_t crop_right, crop_bottom;  /* conformance-window crop in luma samples, even */
+  uint8_t qp, level_idc, ctu_log2, min_cb_log2, ts_log2;
+  uint8_t reserved[3];
+} vvcg_stream_cfg;
+
+typedef enum vvcg_hls_kind {
+  VVCG_HLS_AUD = 0,          /* hls.rs:756 build_aud_rbsp_pic_type; arg = aud_pic_type */
+  VVCG_HLS_VPS = 1,          /* hls.rs:353 build_vps_rbsp */
+  VVCG_HLS_SPS = 2,          /* hls.rs:373 build_sps_rbsp */
+  VVCG_HLS_PPS = 3,          /* hls.rs:529 build_pps_rbsp */
+  VVCG_HLS_PH = 4,           /* hls.rs:571 build_ph_rbsp; arg = POC LSB */
+  VVCG_HLS_SLICE_HEADER = 5  /* hls.rs:598 build_slice_header_bits; arg = sh_qp_delta */
+} vvcg_hls_kind;
+
+/* One RBSP (before emulation prevention) of the default stream into `out`
+ * (cap bytes). *size receives its length; VVCG_LIMIT_EXCEEDED when it does
+ * not fit (nothing written), VVCG_INVALID_INPUT for an unknown kind or a
+ * configuration the syntax cannot carry (ctu_log2 outside 5..7, odd crop,
+ * min_cb_log2 or ts_log2 below 2). */
+vvcg_status vvcg_hls_rbsp(const vvcg_stream_cfg* cfg, uint32_t kind, int32_t arg, uint8_t* out, size_t cap,
+                          size_t* size);
+
+/* The IDR access unit VvcEncoder::encode_i420 emits for a picture of
+ * width x height visible luma samples coded at qp (mod.rs:582-616): AUD,
+ * VPS, SPS, PPS, picture header, then one IDR_N_LP slice NAL unit holding
+ * the slice header and `slice_data` (what vvcg_parse_strict reads), each
+ * behind a 4-byte start code with emulation prevention. The coded size is
+ * the visible size rounded up to whole CTUs (mod.rs:300-318), the level the
+ * smallest whose picture size holds it (hls.rs:182). *size receives the
+ * length; VVCG_LIMIT_EXCEEDED when it exceeds cap (nothing written). */
+vvcg_status vvcg_annexb_idr(uint32_t width, uint32_t height, uint8_t qp, const uint8_t* slice_data, size_t n,
+                            uint8_t* out, size_t cap, size_t* size);
+
+typedef struct vvcg_annexb_info {
+  uint32_t width, height;  /* coded size (from the PPS) */
+  int32_t qp;              /* slice QP: 26 + pps_init_qp_minus26 + sh_qp_delta */
+  uint32_t num_nals;       /* NAL units in the access unit */
+  uint32_t slice_nal_type; /* nal_unit_type of the slice (7 or 8: IDR) */
+  uint32_t reserved;
+} vvcg_annexb_info;
+
+/* The reverse for one access unit of that stream: splits the byte stream at
+ * its start codes, reads the coded size and initial QP from the PPS, then
+ * the IDR slice's header, and writes the slice data after it (emulation
+ * prevention removed) to `slice_data`; *size receives its length.
+ * VVCG_INVALID_INPUT when no PPS or IDR slice is present, or a syntax
+ * element differs from the default stream's layout (pps_no_pic_partition,
+ * a picture header in the slice header, an unterminated slice header);
+ * VVCG_LIMIT_EXCEEDED when the slice data exceeds cap. */
+vvcg_status vvcg_annexb_read_idr(const uint8_t* au, size_t n, vvcg_annexb_info* info, uint8_t* slice_data,
+                                 size_t cap, size_t* size);
+
 #ifdef __cplusplus
 }
 #endif

@@ -337,6 +337,9 @@ def lib():
         L.vvcg_dpb_download.argtypes = [vp, u32, vp]
         L.vvcg_dpb_plane.argtypes = [vp, u32, u32, vp, vp]
         L.vvcg_decode_p_batch.argtypes = [vp, vp, u32, vp, u32, vp, u64]
+        L.vvcg_hls_rbsp.argtypes = [vp, u32, C.c_int32, vp, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.vvcg_annexb_idr.argtypes = [u32, u32, u8, vp, C.c_size_t, vp, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.vvcg_annexb_read_idr.argtypes = [vp, C.c_size_t, vp, vp, C.c_size_t, C.POINTER(C.c_size_t)]
         _lib = L
     return _lib
 
@@ -1225,6 +1228,59 @@ def lmcs_build(aps, bit_depth):
 
 
 PARSE_LUMA, PARSE_DEP_QUANT, PARSE_SIGN_HIDING, PARSE_TRANSFORM_SKIP = 1, 2, 4, 8
+
+
+# -- Annex-B access units (include/vvcg.h "Annex-B access units") --
+STREAM_CFG_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("crop_right", "<u4"), ("crop_bottom", "<u4"),
+                             ("qp", "u1"), ("level_idc", "u1"), ("ctu_log2", "u1"), ("min_cb_log2", "u1"),
+                             ("ts_log2", "u1"), ("reserved", "u1", (3,))])
+ANNEXB_INFO_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("qp", "<i4"), ("num_nals", "<u4"),
+                              ("slice_nal_type", "<u4"), ("reserved", "<u4")])
+HLS_AUD, HLS_VPS, HLS_SPS, HLS_PPS, HLS_PH, HLS_SLICE_HEADER = range(6)
+
+
+def _sized_call(fn, *args):
+    """Calls fn(*args, out, cap, &size) twice: once for the size, once into a
+    buffer of that size; returns the bytes."""
+    size = C.c_size_t(0)
+    st = fn(*args, None, 0, C.byref(size))
+    if st not in (OK, LIMIT_EXCEEDED):
+        raise _ERRORS.get(st, Execution)(f"{fn.__name__} rejected its input")
+    out = np.zeros(max(1, size.value), np.uint8)
+    st = fn(*args, _ptr(out), out.size, C.byref(size))
+    if st != OK:
+        raise _ERRORS.get(st, Execution)(f"{fn.__name__} rejected its input")
+    return out[:size.value].tobytes()
+
+
+def hls_rbsp(kind, width, height, qp, level_idc, ctu_log2=5, min_cb_log2=5, ts_log2=5, crop_right=0,
+             crop_bottom=0, arg=0):
+    """One RBSP of the default stream's parameter sets or headers
+    (vvcg_hls_rbsp): kind HLS_AUD / VPS / SPS / PPS / PH / SLICE_HEADER, arg
+    the AUD picture type, the POC LSB or the slice QP delta; bytes."""
+    cfg = np.zeros(1, STREAM_CFG_DTYPE)
+    for k, v in dict(width=width, height=height, crop_right=crop_right, crop_bottom=crop_bottom, qp=qp,
+                     level_idc=level_idc, ctu_log2=ctu_log2, min_cb_log2=min_cb_log2, ts_log2=ts_log2).items():
+        cfg[k] = v
+    return _sized_call(lib().vvcg_hls_rbsp, _ptr(cfg), kind, arg)
+
+
+def annexb_idr(slice_data, width, height, qp):
+    """The reference encoder's IDR access unit (AUD, VPS, SPS, PPS, picture
+    header, IDR slice) around strict-profile slice data, for a picture of
+    width x height visible samples at qp (vvcg_annexb_idr); bytes."""
+    buf = np.frombuffer(bytes(slice_data), np.uint8)
+    return _sized_call(lib().vvcg_annexb_idr, width, height, qp, _ptr(buf) if buf.size else None, buf.size)
+
+
+def annexb_read_idr(au):
+    """The slice data of an IDR access unit of the default stream and what
+    the PPS and slice header say (vvcg_annexb_read_idr): returns (slice
+    data bytes, width, height, qp), ready for parse_strict."""
+    buf = np.frombuffer(bytes(au), np.uint8)
+    info = np.zeros(1, ANNEXB_INFO_DTYPE)
+    data = _sized_call(lib().vvcg_annexb_read_idr, _ptr(buf) if buf.size else None, buf.size, _ptr(info))
+    return data, int(info["width"][0]), int(info["height"][0]), int(info["qp"][0])
 
 
 def parse_strict(streams, sparse=False, threads=0):

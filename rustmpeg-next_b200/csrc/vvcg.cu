@@ -13,6 +13,7 @@
 
 #include "../../include/vvcg.h"
 #include "alf_general.cuh"
+#include "annexb.h"
 #include "cnn.cuh"
 #include "dbk_general.cuh"
 #include "enc.cuh"
@@ -3027,3 +3028,88 @@ extern "C" vvcg_status vvcg_parse_residual_block(const uint8_t* data, uint64_t s
   return VVCG_OK;
 }
 
+
+// ---- Annex-B access units (host only) ----------------------------------------
+
+static vvcg_status copy_out(const std::vector<uint8_t>& v, uint8_t* out, size_t cap, size_t* size) {
+  if (size) *size = v.size();
+  if (v.size() > cap) return VVCG_LIMIT_EXCEEDED;
+  if (!v.empty()) {
+    if (!out) return VVCG_INVALID_INPUT;
+    memcpy(out, v.data(), v.size());
+  }
+  return VVCG_OK;
+}
+
+extern "C" vvcg_status vvcg_hls_rbsp(const vvcg_stream_cfg* cfg, uint32_t kind, int32_t arg, uint8_t* out,
+                                     size_t cap, size_t* size) {
+  namespace ab = vvcg::annexb;
+  if (!cfg || !size) return VVCG_INVALID_INPUT;
+  if (cfg->ctu_log2 < 5 || cfg->ctu_log2 > 7 || (cfg->crop_right & 1) || (cfg->crop_bottom & 1) ||
+      cfg->min_cb_log2 < 2 || cfg->ts_log2 < 2)
+    return VVCG_INVALID_INPUT;
+  const ab::StreamCfg c{cfg->width,    cfg->height,    cfg->crop_right,  cfg->crop_bottom, cfg->qp,
+                        cfg->level_idc, cfg->ctu_log2, cfg->min_cb_log2, cfg->ts_log2};
+  switch (kind) {
+    case VVCG_HLS_AUD: return copy_out(ab::aud_rbsp((uint8_t)arg), out, cap, size);
+    case VVCG_HLS_VPS: return copy_out(ab::vps_rbsp(c), out, cap, size);
+    case VVCG_HLS_SPS: return copy_out(ab::sps_rbsp(c), out, cap, size);
+    case VVCG_HLS_PPS: return copy_out(ab::pps_rbsp(c), out, cap, size);
+    case VVCG_HLS_PH: return copy_out(ab::ph_rbsp((uint32_t)arg), out, cap, size);
+    case VVCG_HLS_SLICE_HEADER: return copy_out(ab::slice_header(arg), out, cap, size);
+    default: return VVCG_INVALID_INPUT;
+  }
+}
+
+extern "C" vvcg_status vvcg_annexb_idr(uint32_t width, uint32_t height, uint8_t qp, const uint8_t* slice_data,
+                                       size_t n, uint8_t* out, size_t cap, size_t* size) {
+  if (!size || !width || !height || width > (1u << 16) || height > (1u << 16) || qp > 63 || (n && !slice_data))
+    return VVCG_INVALID_INPUT;
+  const vvcg::annexb::StreamCfg c = vvcg::annexb::encoder_cfg(width, height, qp);
+  return copy_out(vvcg::annexb::idr_access_unit(c, slice_data, n), out, cap, size);
+}
+
+extern "C" vvcg_status vvcg_annexb_read_idr(const uint8_t* au, size_t n, vvcg_annexb_info* info,
+                                            uint8_t* slice_data, size_t cap, size_t* size) {
+  namespace ab = vvcg::annexb;
+  if (!au || !info || !size) return VVCG_INVALID_INPUT;
+  const std::vector<ab::Nal> nals = ab::split(au, n);
+  memset(info, 0, sizeof(*info));
+  info->num_nals = (uint32_t)nals.size();
+  bool have_pps = false;
+  int32_t init_qp = 0;
+  for (const ab::Nal& x : nals) {
+    if (x.type == ab::kNalPps) {  // hls.rs:529-564
+      const std::vector<uint8_t> r = ab::unescape(au + x.begin, x.end - x.begin);
+      ab::Reader b(r.data(), r.size());
+      b.u(6); b.u(4); b.u(1);  // PPS id, SPS id, mixed NALU types
+      info->width = b.ue();
+      info->height = b.ue();
+      b.u(1); b.u(1); b.u(1);  // conformance window, scaling window, output flag (0 in this layout)
+      if (b.u(1) != 1) return VVCG_INVALID_INPUT;  // pps_no_pic_partition_flag
+      b.u(1); b.u(1);          // subpic id mapping, CABAC init present
+      b.ue(); b.ue();          // default active ref idx L0 / L1
+      b.u(1); b.u(1); b.u(1); b.u(1);
+      init_qp = 26 + b.se();
+      if (!b.ok()) return VVCG_INVALID_INPUT;
+      have_pps = true;
+    } else if (x.type == 7 || x.type == ab::kNalIdrNLp) {  // hls.rs:598-637
+      if (!have_pps) return VVCG_INVALID_INPUT;
+      const std::vector<uint8_t> r = ab::unescape(au + x.begin, x.end - x.begin);
+      ab::Reader b(r.data(), r.size());
+      if (b.u(1) != 0) return VVCG_INVALID_INPUT;  // sh_picture_header_in_slice_header_flag
+      b.u(1);                                      // sh_no_output_of_prior_pics_flag
+      const int32_t qp_delta = b.se();
+      b.u(1);                                      // sh_ts_residual_coding_disabled_flag
+      if (b.u(1) != 1) return VVCG_INVALID_INPUT;  // byte_alignment(): the one bit ...
+      while (b.ok() && (b.pos() & 7))
+        if (b.u(1) != 0) return VVCG_INVALID_INPUT;  // ... then zeros
+      if (!b.ok()) return VVCG_INVALID_INPUT;
+      info->qp = init_qp + qp_delta;
+      info->slice_nal_type = x.type;
+      const std::vector<uint8_t> data(r.begin() + (ptrdiff_t)(b.pos() >> 3), r.end());
+      return copy_out(data, slice_data, cap, size);
+    }
+  }
+  return VVCG_INVALID_INPUT;
+}

@@ -126,6 +126,7 @@ RECORDS = {
     "PROF_REQ_DTYPE": "vvcg_prof_req", "CIIP_REQ_DTYPE": "vvcg_ciip_req", "GPM_REQ_DTYPE": "vvcg_gpm_req",
     "GEN_TB_DTYPE": "vvcg_gen_tb", "GEN_PIC_DTYPE": "vvcg_gen_pic",
     "INTER_CU_DTYPE": "vvcg_inter_cu", "P_PIC_DTYPE": "vvcg_p_pic",
+    "STREAM_CFG_DTYPE": "vvcg_stream_cfg", "ANNEXB_INFO_DTYPE": "vvcg_annexb_info",
 }
 
 

@@ -152,3 +152,33 @@ def test_strict_bitstreams_decode_on_the_gpu(ctx, pkg, orc, sparse):
     got = ctx.decode_batch(pkg.Batch(pics, cus, levels, ctus))
     for k, (g, rec) in enumerate(zip(got, recs)):
         _assert_planes(g, rec, f"stream {k}")
+
+
+def test_annexb_access_units_decode_on_the_gpu(ctx, pkg, orc):
+    """From Annex-B access units to pixels: the oracle encoder's slice data
+    wrapped as the reference encoder's IDR access units (vvcg_annexb_idr),
+    read back (vvcg_annexb_read_idr: size and QP from the PPS and slice
+    header), parsed and decoded on the GPU, equal to the encoder's
+    reconstruction."""
+    from rustmpeg_next_b200 import synth
+
+    aus, recs = [], []
+    rng = np.random.default_rng(8)
+    for k, qp in enumerate((26, 37, 22)):
+        if k < 2:
+            y, u, v = synth.config1_frame(k)
+        else:  # 96x64 noise: a second coded size in the batch
+            y = rng.integers(0, 256, (64, 96), dtype=np.uint8)
+            u, v = (rng.integers(0, 256, (32, 48), dtype=np.uint8) for _ in range(2))
+        cus, levels, rec = orc.strict_encode(y, u, v, qp)
+        h, w = y.shape
+        aus.append(pkg.annexb_idr(orc.strict_write(cus, levels, w, h, qp), w, h, qp))
+        recs.append(rec)
+    streams = [pkg.annexb_read_idr(au) for au in aus]
+    assert [(w, h, qp) for _, w, h, qp in streams] == [(64, 64, 26), (64, 64, 37), (96, 64, 22)]
+    pics, cus, levels, _ = pkg.parse_strict(streams, threads=2)
+    n_ctu = [(int(p["width"]) // 32) * (int(p["height"]) // 32) for p in pics]
+    pics["ctu_offset"] = np.concatenate([[0], np.cumsum(n_ctu)[:-1]])
+    got = ctx.decode_batch(pkg.Batch(pics, cus, levels, np.zeros(sum(n_ctu), pkg.CTU_DTYPE)))
+    for k, (g, rec) in enumerate(zip(got, recs)):
+        _assert_planes(g, rec, f"access unit {k}")
