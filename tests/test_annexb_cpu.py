@@ -31,6 +31,27 @@ def test_parameter_sets_match_the_reference_vectors(pkg):
     assert pkg.hls_rbsp(pkg.HLS_SLICE_HEADER, **REF_CFG, arg=0) == bytes([0x28])
 
 
+def _ue(bits, pos):
+    z = 0
+    while bits[pos + z] == "0":
+        z += 1
+    return int(bits[pos + z:pos + 2 * z + 1], 2) - 1, pos + 2 * z + 1
+
+
+def test_sps_parses_as_the_reference_reads_it(pkg):
+    """What the reference's own test reads back from its SPS
+    (hls.rs:5504-5508: 128x128, level 16, profile 1): profile and level in
+    the PTL, then after sps_gdr_enabled_flag and
+    sps_ref_pic_resampling_enabled_flag the two sizes as ue(v)."""
+    sps = pkg.hls_rbsp(pkg.HLS_SPS, **REF_CFG)
+    bits = "".join(f"{b:08b}" for b in sps)
+    assert int(bits[16:23], 2) == 1 and int(bits[24:32], 2) == 16  # general_profile_idc, general_level_idc
+    w, pos = _ue(bits, 16 + 14 * 8 + 2)
+    h, pos = _ue(bits, pos)
+    assert (w, h) == (128, 128)
+    assert bits[pos] == "0"  # no conformance window
+
+
 def test_sps_carries_the_size_and_the_conformance_window(pkg):
     a = pkg.hls_rbsp(pkg.HLS_SPS, **REF_CFG)
     b = pkg.hls_rbsp(pkg.HLS_SPS, **dict(REF_CFG, crop_right=8, crop_bottom=4))
