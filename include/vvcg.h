@@ -785,6 +785,18 @@ vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint6
                                        uint32_t top_modes, uint32_t top_splits, float threshold,
                                        vvcg_ctu_search_res* res);
 
+/* Fallback rules of vvcg_ctu_search_pruned_rule_dev: a head keeps its full
+ * set when its chosen entries hold less than the threshold of its softmax
+ * mass (VVCG_PRUNE_MASS, the rule of vvcg_ctu_search_pruned_dev), or when
+ * its most probable entry does (VVCG_PRUNE_MAX_PROB: "full-search fallback
+ * when max softmax < threshold"). */
+enum { VVCG_PRUNE_MASS = 0, VVCG_PRUNE_MAX_PROB = 1 };
+vvcg_status vvcg_ctu_search_pruned_rule_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
+                                            uint32_t height, uint8_t bit_depth, uint32_t lambda_q8,
+                                            const uint32_t* ctu_xy, uint32_t num_ctus, const float* logits,
+                                            uint32_t top_modes, uint32_t top_splits, float threshold, uint32_t rule,
+                                            vvcg_ctu_search_res* res);
+
 /* The full CTU search of vvcg_ctu_search_pruned_dev (no pruning) that also
  * writes, per CTU, the cost (SATD + lambda * mode bits) of each of the 67
  * luma modes for the unsplit 32x32 coding unit: mode_costs, device memory,

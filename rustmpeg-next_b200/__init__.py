@@ -303,6 +303,8 @@ def lib():
         L.vvcg_luma_intra_search_8_dev.argtypes = [vp, vp, u64, vp, u64, u32, u32, vp, u32, vp]
         L.vvcg_ctu_search_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp]
         L.vvcg_ctu_search_pruned_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, u32, u32, C.c_float, vp]
+        L.vvcg_ctu_search_pruned_rule_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, u32, u32,
+                                                      C.c_float, u32, vp]
         L.vvcg_ctu_search_costs_dev.argtypes = [vp, vp, u64, u32, u32, u8, u32, vp, u32, vp, vp]
         L.vvcg_tc_selftest_dev.argtypes = [vp, vp, vp, vp, vp]
         L.vvcg_cnn_forward_dev.argtypes = [vp, vp, u64, u32, u32, u8, u8, vp, u32, vp, vp, vp, vp, vp]
@@ -876,11 +878,12 @@ class Context:
         return d
 
     def ctu_search_xy(self, src, bit_depth, lambda_q8, xy, logits=None, top_modes=6, top_splits=2,
-                      threshold=0.7, out=None, sync=True):
+                      threshold=0.7, out=None, sync=True, rule=0):
         """The CTU search over device positions xy ((n, 2) int32 CUDA), full
         (logits None) or pruned by the CNN's logits ((n, 73) fp32 CUDA): the
         top_modes / top_splits most probable entries of each head, or its full
-        set when they hold less than threshold of its softmax mass.
+        set when they hold less than threshold of its softmax mass (rule
+        PRUNE_MASS) or when its most probable entry does (PRUNE_MAX_PROB).
         Returns CTU_SEARCH_RES_DTYPE results, or fills the CUDA uint8 tensor
         out (n x 36 bytes) without synchronising when sync is False."""
         import torch
@@ -889,9 +892,9 @@ class Context:
         h, w = src.shape
         dst = out if out is not None else torch.empty(max(n, 1) * CTU_SEARCH_RES_DTYPE.itemsize, dtype=torch.uint8,
                                                       device=src.device)
-        self._check(self._L.vvcg_ctu_search_pruned_dev(self._h, _ptr(src), src.stride(0), w, h, bit_depth, lambda_q8,
-                                                       _ptr(xy.contiguous()), n, _ptr(logits), top_modes, top_splits,
-                                                       threshold, _ptr(dst)))
+        self._check(self._L.vvcg_ctu_search_pruned_rule_dev(
+            self._h, _ptr(src), src.stride(0), w, h, bit_depth, lambda_q8, _ptr(xy.contiguous()), n, _ptr(logits),
+            top_modes, top_splits, threshold, rule, _ptr(dst)))
         if not sync:
             return None
         torch.cuda.synchronize(src.device)
@@ -1237,6 +1240,7 @@ STREAM_CFG_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("crop_right",
 ANNEXB_INFO_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("qp", "<i4"), ("num_nals", "<u4"),
                               ("slice_nal_type", "<u4"), ("reserved", "<u4")])
 HLS_AUD, HLS_VPS, HLS_SPS, HLS_PPS, HLS_PH, HLS_SLICE_HEADER = range(6)
+PRUNE_MASS, PRUNE_MAX_PROB = 0, 1  # fallback rules of vvcg_ctu_search_pruned_rule_dev
 
 
 def _sized_call(fn, *args):

@@ -3,8 +3,9 @@
 // top_splits most probable) that the full search of intra_search.cuh then
 // evaluates; a head whose chosen candidates hold less than the threshold of
 // its softmax probability mass (for a calibrated network: the chance that
-// the full search's choice is among them) keeps its full set (all 67 modes /
-// all 6 splits). Everything
+// the full search's choice is among them), or under the max-probability
+// rule whose most probable entry is below the threshold, keeps its full set
+// (all 67 modes / all 6 splits). Everything
 // stays on the device: requests are built from the logits by one thread per
 // CTU and expanded into the 15 block slots of the search.
 #pragma once
@@ -43,8 +44,8 @@ __device__ __forceinline__ float top_mass(const float* v, int n, const uint8_t* 
 }
 
 __global__ void k_prune_requests(const float* __restrict__ logits, const uint32_t* __restrict__ xy, int n, int width,
-                                 int height, int top_modes, int top_splits, float thr, vvcg_ctu_search_req* reqs,
-                                 CostReq* blocks) {
+                                 int height, int top_modes, int top_splits, float thr, bool max_prob,
+                                 vvcg_ctu_search_req* reqs, CostReq* blocks) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   vvcg_ctu_search_req r{};
@@ -57,13 +58,13 @@ __global__ void k_prune_requests(const float* __restrict__ logits, const uint32_
     const float* lg = logits + (size_t)i * kCnnOut;
     uint8_t cand[6];
     top_k(lg, kCnnModes, top_modes, cand);
-    if (top_mass(lg, kCnnModes, cand, top_modes) >= thr) {
+    if (top_mass(lg, kCnnModes, cand, max_prob ? 1 : top_modes) >= thr) {
       r.n_cand = (uint8_t)top_modes;
       for (int k = 0; k < top_modes; k++) r.cand[k] = cand[k];
     }
     uint8_t sp[6];
     top_k(lg + kCnnModes, kCnnSplits, top_splits, sp);
-    if (top_mass(lg + kCnnModes, kCnnSplits, sp, top_splits) >= thr) {
+    if (top_mass(lg + kCnnModes, kCnnSplits, sp, max_prob ? 1 : top_splits) >= thr) {
       r.split_mask = 0;
       for (int k = 0; k < top_splits; k++) r.split_mask |= (uint8_t)(1u << sp[k]);
     }

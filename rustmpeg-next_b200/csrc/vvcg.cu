@@ -1638,7 +1638,7 @@ extern "C" vvcg_status vvcg_ctu_search_dev(vvcg_ctx* ctx, const uint16_t* src, u
 static vvcg_status ctu_search_xy(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
                                  uint32_t height, uint8_t bit_depth, uint32_t lambda_q8, const uint32_t* ctu_xy,
                                  uint32_t num_ctus, const float* logits, uint32_t top_modes, uint32_t top_splits,
-                                 float threshold, vvcg_ctu_search_res* res, uint32_t* mode_costs);
+                                 float threshold, uint32_t rule, vvcg_ctu_search_res* res, uint32_t* mode_costs);
 
 extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride,
                                                   uint32_t width, uint32_t height, uint8_t bit_depth,
@@ -1646,7 +1646,17 @@ extern "C" vvcg_status vvcg_ctu_search_pruned_dev(vvcg_ctx* ctx, const uint16_t*
                                                   const float* logits, uint32_t top_modes, uint32_t top_splits,
                                                   float threshold, vvcg_ctu_search_res* res) {
   return ctu_search_xy(ctx, src, stride, width, height, bit_depth, lambda_q8, ctu_xy, num_ctus, logits, top_modes,
-                       top_splits, threshold, res, nullptr);
+                       top_splits, threshold, VVCG_PRUNE_MASS, res, nullptr);
+}
+
+extern "C" vvcg_status vvcg_ctu_search_pruned_rule_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride,
+                                                       uint32_t width, uint32_t height, uint8_t bit_depth,
+                                                       uint32_t lambda_q8, const uint32_t* ctu_xy, uint32_t num_ctus,
+                                                       const float* logits, uint32_t top_modes, uint32_t top_splits,
+                                                       float threshold, uint32_t rule, vvcg_ctu_search_res* res) {
+  if (ctx && rule > VVCG_PRUNE_MAX_PROB) return fail(ctx, VVCG_INVALID_INPUT, "unknown fallback rule");
+  return ctu_search_xy(ctx, src, stride, width, height, bit_depth, lambda_q8, ctu_xy, num_ctus, logits, top_modes,
+                       top_splits, threshold, rule, res, nullptr);
 }
 
 extern "C" vvcg_status vvcg_ctu_search_costs_dev(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
@@ -1656,13 +1666,13 @@ extern "C" vvcg_status vvcg_ctu_search_costs_dev(vvcg_ctx* ctx, const uint16_t* 
   if (!ctx) return VVCG_INVALID_INPUT;
   if (num_ctus && !mode_costs) return fail(ctx, VVCG_INVALID_INPUT, "missing mode costs");
   return ctu_search_xy(ctx, src, stride, width, height, bit_depth, lambda_q8, ctu_xy, num_ctus, nullptr, 6, 2, 0.0f,
-                       res, mode_costs);
+                       VVCG_PRUNE_MASS, res, mode_costs);
 }
 
 static vvcg_status ctu_search_xy(vvcg_ctx* ctx, const uint16_t* src, uint64_t stride, uint32_t width,
                                  uint32_t height, uint8_t bit_depth, uint32_t lambda_q8, const uint32_t* ctu_xy,
                                  uint32_t num_ctus, const float* logits, uint32_t top_modes, uint32_t top_splits,
-                                 float threshold, vvcg_ctu_search_res* res, uint32_t* mode_costs) {
+                                 float threshold, uint32_t rule, vvcg_ctu_search_res* res, uint32_t* mode_costs) {
   if (!ctx) return VVCG_INVALID_INPUT;
   if (!num_ctus) return VVCG_OK;
   if (!src || !ctu_xy || !res) return fail(ctx, VVCG_INVALID_INPUT, "missing plane, positions or results");
@@ -1679,7 +1689,7 @@ static vvcg_status ctu_search_xy(vvcg_ctx* ctx, const uint16_t* src, uint64_t st
   CK(ctx->d_search_mode.reserve(nb), "cudaMalloc");
   k_prune_requests<<<(num_ctus + 127) / 128, 128, 0, ctx->stream>>>(
       logits, ctu_xy, (int)num_ctus, (int)width, (int)height, (int)top_modes, (int)top_splits, threshold,
-      (vvcg_ctu_search_req*)ctx->d_search_ctus.p, (CostReq*)ctx->d_search_reqs.p);
+      rule == VVCG_PRUNE_MAX_PROB, (vvcg_ctu_search_req*)ctx->d_search_ctus.p, (CostReq*)ctx->d_search_reqs.p);
   CK(cudaGetLastError(), "prune launch");
   CostArgs A{src, (int64_t)stride, (int32_t)width, (int32_t)height, bit_depth, (int32_t)nb, lambda_q8,
              (const CostReq*)ctx->d_search_reqs.p, (uint32_t*)ctx->d_search_cost.p,

@@ -115,3 +115,37 @@ def test_mode_costs_of_the_unsplit_cu(ctx, pkg, orc):
         for m in (0, 1, int(rng.integers(2, 67)), int(c[k].argmin())):
             r = orc.ctu_search(y, 10, int(a[k, 0]), int(a[k, 1]), 280, split_mask=1, cand=(m,))
             assert r["split_cost"][0] == c[k, m] + (280 >> 8), (k, m)
+
+
+def test_max_probability_rule_matches_oracle(ctx, pkg, orc):
+    """The encoder configuration's own policy: top-3 modes, top-2 splits and
+    the full set for a head whose most probable entry is below 0.4
+    (PRUNE_MAX_PROB), against the oracle's search on those candidates."""
+    import torch
+
+    y, plane = _plane(160, 96, 9)
+    a, xy = _xy(160, 96)
+    rng = np.random.default_rng(9)
+    logits = rng.normal(0, 1.0, (len(a), 73)).astype(np.float32)
+    logits[np.arange(len(a)), rng.integers(0, 67, len(a))] += rng.uniform(0.0, 9.0, len(a)).astype(np.float32)
+    logits[np.arange(len(a)), 67 + rng.integers(0, 6, len(a))] += rng.uniform(0.0, 3.0, len(a)).astype(np.float32)
+    got = ctx.ctu_search_xy(plane, 10, 250, xy, torch.from_numpy(logits).cuda(), 3, 2, 0.4, rule=pkg.PRUNE_MAX_PROB)
+
+    def top(v, k):
+        return [int(i) for i in sorted(range(len(v)), key=lambda j: (-v[j], j))[:k]]
+
+    def pmax(v):
+        e = np.exp(v.astype(np.float64) - v.max())
+        return 1.0 / e.sum()
+
+    kept = 0
+    for i, (x, yy) in enumerate(a):
+        li, ls = logits[i, :67], logits[i, 67:]
+        cand = tuple(top(li, 3)) if pmax(li) >= 0.4 else ()
+        mask = sum(1 << s for s in top(ls, 2)) if pmax(ls) >= 0.4 else 0x3F
+        kept += bool(cand) + (mask != 0x3F)
+        want = orc.ctu_search(y, 10, int(x), int(yy), 250, mask, cand)
+        g = got[i]
+        assert (int(g["cost"]), int(g["split"]), [int(v) for v in g["modes"]]) == \
+            (want["cost"], want["split"], want["modes"]), i
+    assert 0 < kept < 2 * len(a)  # both pruned and fallback heads occur
